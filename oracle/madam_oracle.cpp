@@ -1,0 +1,2466 @@
+// CPU ORACLE for the Madam destriping solve -- TEST INFRASTRUCTURE ONLY.
+//
+// This file is a loop-for-loop C++17/OpenMP restatement of the reference
+// Fortran destriper (hpc4cmb/libmadam) on the destripe() path.  It exists to
+// check the CUDA product and to serve as the timed CPU baseline.  Only tests/,
+// __graft_entry__.smoke() and bench.py's CPU legs load it; the product library
+// (libmadam_b200) never links, loads or calls it.
+//
+// Parity status: the reference (Fortran + MPI + FFTW + LAPACK) cannot be
+// compiled in this environment (no Fortran compiler, MPI, FFTW or LAPACK), so
+// this restatement is pinned (a) against the known-answer relations of the
+// reference's own tests (python/tests/test_libmadam.py:120-174,
+// test_libmadam_mc.py:194-208: exact hit map, binned map = sum/hits), and
+// (b) its third-party arithmetic (FFTW r2c/c2r, LAPACK dsyev/dpbtrf/dpbtrs/
+// dpotrf/dpotri) is pinned against numpy.fft / scipy.linalg.lapack in the
+// test-suite.  The destriped map and baselines have no golden values in the
+// reference; they are compared product-vs-oracle.
+//
+// Reference files followed (paths inside the reference project):
+//   src/smadam.F90           destripe 64-590, destripe_with_cache 593-918,
+//                            clear_caches 921-951
+//   src/inputparam.f90       read_parameters 24-67, read_detectors 73-163,
+//                            read_line 169-371, parse_detset 375-434,
+//                            parse_survey 438-492, check_missing 498-505
+//   src/commonparam.f90      set_parameter_defaults 200-305
+//   src/parameter_control.f90 init_parameters 27-409, init_parallelization
+//                            415-482, start_timeloop 752-950,
+//                            baseline_times 956-977
+//   src/read_data.f90        flag_bad_baselines 30-74, check_files 203-325
+//   src/pointing.f90         init_pointing 37-64, reduce_pixels 115-163,
+//                            restore_pixels 168-191
+//   src/maptod_transfer.f90  update_maptod_transfer 49-124, collect_map
+//                            461-625, collect_cc 631-799, collect_hits
+//                            804-936, scatter_map 942-1113 (single rank)
+//   src/smadam_routines.f90  pixel_matrix 111-246, bin_tod 252-343,
+//                            count_hits 349-422, initialize_a 428-671,
+//                            iterate_a 677-1483, subtract_baselines_a
+//                            1489-1539, clean_tod 1545-1585
+//   src/noise_routines.f90   measure_noise_weights 65-127, interpolate_psd
+//                            130-190, psd_index 193-208, psd_index_det
+//                            211-236, init_filter 242-292, build_filter
+//                            367-739, trim_interval 764-813,
+//                            convolve_interval 816-857, convolve_pp 861-913,
+//                            construct_preconditioner 920-1153,
+//                            preconditioning_band 1159-1256,
+//                            apply_cholesky_decomposition 1259-1275,
+//                            get_cholesky_decomposition 1279-1301,
+//                            apply_CG_preconditioner 1305-1409
+//   src/map_routines.f90     ccmultiply 24-77, invert_pixelmatrix_cross
+//                            83-212, invert_pixelmatrix_map 218-321,
+//                            makemaps 327-357
+//   src/matrix.f90           test_decoupling 15-51, invert_eig 53-126,
+//                            invert_eig_s 132-179, invert_LU 287-327
+//   src/fourier_fftw_2003.f90 dfft 101-109, dfftinv 113-123
+//
+// Third-party arithmetic restated from published algorithms (the reference
+// links whatever FFTW3 / LAPACK the system provides; no version is pinned):
+//   * FFTW r2c / c2r: iterative radix-2 Cooley-Tukey complex FFT of length
+//     n/2 plus the standard real-to-half-complex split; inverse scaled 1/n.
+//   * LAPACK DSYEV (symmetric eigen): cyclic Jacobi rotations.
+//   * LAPACK DPBTRF / DPBTRS (lower, band): unblocked band Cholesky
+//     (the DPBTF2 column algorithm) and the two banded triangular solves.
+//   * LAPACK DPOTRF / DPOTRI (upper): Cholesky factor, triangular inverse,
+//     product U^-1 U^-T.
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <vector>
+#include <omp.h>
+
+namespace {
+
+const double kPi = 3.141592653589793238462643383279502884197;
+
+// Fortran default-real (single precision) literals used by the reference as
+// thresholds and defaults, e.g. `1e-12` in matrix.f90:110 is the float
+// 1e-12 widened to double.
+inline constexpr double F(float x) { return (double)x; }
+const double kTiny30 = F(1e-30f);
+const double kRcondSing = F(1e-12f);
+
+struct OracleError : std::runtime_error {
+  explicit OracleError(const std::string &m) : std::runtime_error(m) {}
+};
+
+[[noreturn]] void fail(const std::string &msg) { throw OracleError(msg); }
+
+// ---------------------------------------------------------------- FFT -----
+// Real FFT of power-of-two length n.  rfft returns n/2+1 complex values;
+// irfft takes n/2+1 values (imag parts of bins 0 and n/2 ignored) and returns
+// n reals scaled by 1/n, matching fourier_fftw_2003.f90:101-123.
+struct RealFFT {
+  long n = 0;
+  std::vector<std::complex<double>> tw;    // exp(-2 pi i k / (n/2)), k < n/4
+  std::vector<std::complex<double>> tw2;   // exp(-2 pi i k / n), k <= n/2
+  std::vector<long> rev;
+
+  explicit RealFFT(long n_) : n(n_) {
+    if (n < 2 || (n & (n - 1))) fail("FFT length must be a power of two >= 2");
+    long h = n / 2;
+    tw.resize(std::max(1L, h / 2));
+    for (long k = 0; k < (long)tw.size(); ++k) {
+      double a = -2.0 * kPi * (double)k / (double)h;
+      tw[k] = {std::cos(a), std::sin(a)};
+    }
+    tw2.resize(h + 1);
+    for (long k = 0; k <= h; ++k) {
+      double a = -2.0 * kPi * (double)k / (double)n;
+      tw2[k] = {std::cos(a), std::sin(a)};
+    }
+    rev.resize(h);
+    int bits = 0;
+    while ((1L << bits) < h) ++bits;
+    for (long i = 0; i < h; ++i) {
+      long r = 0;
+      for (int b = 0; b < bits; ++b)
+        if (i & (1L << b)) r |= 1L << (bits - 1 - b);
+      rev[i] = r;
+    }
+  }
+
+  // in-place complex FFT of length h = n/2; sign -1 forward, +1 inverse
+  void cfft(std::complex<double> *a, int sign) const {
+    long h = n / 2;
+    for (long i = 0; i < h; ++i)
+      if (rev[i] > i) std::swap(a[i], a[rev[i]]);
+    for (long len = 2; len <= h; len <<= 1) {
+      long half = len / 2, step = h / len;
+      for (long s = 0; s < h; s += len) {
+        for (long j = 0; j < half; ++j) {
+          std::complex<double> w = tw[j * step];
+          if (sign > 0) w = std::conj(w);
+          std::complex<double> u = a[s + j], v = a[s + j + half] * w;
+          a[s + j] = u + v;
+          a[s + j + half] = u - v;
+        }
+      }
+    }
+  }
+
+  void rfft(const double *x, std::complex<double> *X,
+            std::vector<std::complex<double>> &work) const {
+    long h = n / 2;
+    work.resize(h);
+    for (long m = 0; m < h; ++m) work[m] = {x[2 * m], x[2 * m + 1]};
+    cfft(work.data(), -1);
+    const std::complex<double> I(0, 1);
+    for (long k = 0; k <= h; ++k) {
+      std::complex<double> zk = work[k % h];
+      std::complex<double> zc = std::conj(work[(h - k) % h]);
+      std::complex<double> e = 0.5 * (zk + zc);
+      std::complex<double> o = -0.5 * I * (zk - zc);
+      X[k] = e + tw2[k] * o;
+    }
+  }
+
+  void irfft(const std::complex<double> *X, double *x,
+             std::vector<std::complex<double>> &work) const {
+    long h = n / 2;
+    work.resize(h);
+    const std::complex<double> I(0, 1);
+    std::complex<double> X0(X[0].real(), 0.0), Xh(X[h].real(), 0.0);
+    for (long k = 0; k < h; ++k) {
+      std::complex<double> a = (k == 0) ? X0 : X[k];
+      std::complex<double> b = (k == 0) ? Xh : std::conj(X[h - k]);
+      std::complex<double> e = 0.5 * (a + b);
+      std::complex<double> o = 0.5 * (a - b) * std::conj(tw2[k]);
+      work[k] = e + I * o;
+    }
+    cfft(work.data(), +1);
+    double s = 1.0 / (double)n;
+    for (long m = 0; m < h; ++m) {
+      x[2 * m] = 2.0 * work[m].real() * s;
+      x[2 * m + 1] = 2.0 * work[m].imag() * s;
+    }
+  }
+};
+
+// ------------------------------------------------------- small linalg -----
+// Symmetric eigen-decomposition by cyclic Jacobi (replaces LAPACK DSYEV,
+// matrix.f90:102,149; smadam_routines.f90:608).  a is n x n column-major;
+// only the upper triangle is read (DSYEV 'U').  On return w holds the
+// eigenvalues in ascending order and v the eigenvectors as columns.
+int sym_eig(int n, const double *a, double *w, double *v) {
+  std::vector<double> A(n * n);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i <= j; ++i) {
+      A[i + n * j] = a[i + n * j];
+      A[j + n * i] = a[i + n * j];
+    }
+  for (int i = 0; i < n * n; ++i) v[i] = 0;
+  for (int i = 0; i < n; ++i) v[i + n * i] = 1;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0, diag = 0;
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        if (i != j) off += A[i + n * j] * A[i + n * j];
+        else diag += A[i + n * j] * A[i + n * j];
+      }
+    if (off == 0 || off <= 1e-34 * diag) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        double apq = A[p + n * q];
+        if (apq == 0) continue;
+        double app = A[p + n * p], aqq = A[q + n * q];
+        double theta = (aqq - app) / (2 * apq);
+        double t = (theta >= 0 ? 1.0 : -1.0) /
+                   (std::fabs(theta) + std::sqrt(theta * theta + 1));
+        if (std::isinf(theta)) t = 0.5 / theta;
+        double c = 1 / std::sqrt(t * t + 1), s = t * c;
+        for (int k = 0; k < n; ++k) {
+          double akp = A[k + n * p], akq = A[k + n * q];
+          A[k + n * p] = c * akp - s * akq;
+          A[k + n * q] = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {
+          double apk = A[p + n * k], aqk = A[q + n * k];
+          A[p + n * k] = c * apk - s * aqk;
+          A[q + n * k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          double vkp = v[k + n * p], vkq = v[k + n * q];
+          v[k + n * p] = c * vkp - s * vkq;
+          v[k + n * q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  for (int i = 0; i < n; ++i) w[i] = A[i + n * i];
+  // sort ascending (selection sort, carrying eigenvectors)
+  for (int i = 0; i < n; ++i) {
+    int m = i;
+    for (int j = i + 1; j < n; ++j)
+      if (w[j] < w[m]) m = j;
+    if (m != i) {
+      std::swap(w[i], w[m]);
+      for (int k = 0; k < n; ++k) std::swap(v[k + n * i], v[k + n * m]);
+    }
+  }
+  for (int i = 0; i < n; ++i)
+    if (std::isnan(w[i])) return 1;
+  return 0;
+}
+
+// invert_eig (matrix.f90:53-126) with incomplete_matrices handling.
+// cc is an n x n column-major block inside a larger matrix with leading
+// dimension ld.
+void invert_eig(double *cc, int ld, int n, bool incomplete, double &cdet,
+                double &rcond, bool &sing) {
+  std::vector<int> good;
+  if (incomplete) {
+    for (int i = 0; i < n; ++i)
+      if (std::fabs(cc[i + ld * i]) > kTiny30) good.push_back(i);
+    if (good.empty()) good.push_back(0);
+  } else {
+    for (int i = 0; i < n; ++i) good.push_back(i);
+  }
+  int nf = (int)good.size();
+  std::vector<double> a(nf * nf), w(nf), v(nf * nf);
+  for (int j = 0; j < nf; ++j)
+    for (int i = 0; i < nf; ++i) a[i + nf * j] = cc[good[i] + ld * good[j]];
+  int info = sym_eig(nf, a.data(), w.data(), v.data());
+  cdet = 1;
+  for (int i = 0; i < nf; ++i) cdet *= w[i];
+  double mn = w[0], mx = w[0];
+  for (int i = 1; i < nf; ++i) {
+    mn = std::min(mn, w[i]);
+    mx = std::max(mx, w[i]);
+  }
+  rcond = mn / mx;
+  if (info != 0 || mx < kTiny30 || rcond < kRcondSing) {
+    sing = true;
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) cc[i + ld * j] = 0;
+    cdet = 0;
+    rcond = 0;
+    return;
+  }
+  sing = false;
+  // cc(good, good) = matmul(V / lambda, V^T)
+  for (int j = 0; j < nf; ++j)
+    for (int i = 0; i < nf; ++i) {
+      double s = 0;
+      for (int k = 0; k < nf; ++k) s += (v[i + nf * k] / w[k]) * v[j + nf * k];
+      cc[good[i] + ld * good[j]] = s;
+    }
+}
+
+// invert_eig_s (matrix.f90:132-179)
+void invert_eig_s(double *cc, int ld, int n, double plim, double &cdet,
+                  double &rcond, int &noeig) {
+  std::vector<double> a(n * n), w(n), v(n * n);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) a[i + n * j] = cc[i + ld * j];
+  int info = sym_eig(n, a.data(), w.data(), v.data());
+  cdet = 1;
+  double mn = w[0], mx = w[0];
+  for (int i = 0; i < n; ++i) {
+    cdet *= w[i];
+    mn = std::min(mn, w[i]);
+    mx = std::max(mx, w[i]);
+  }
+  rcond = mn / mx;
+  if (info != 0 || mx < kTiny30) {
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) cc[i + ld * j] = 0;
+    cdet = 0;
+    rcond = 0;
+    noeig = 0;
+    return;
+  }
+  double lim = std::fabs(plim * mx);
+  noeig = 0;
+  for (int i = 0; i < n; ++i) {
+    if (w[i] < lim) w[i] = 0;
+    else {
+      w[i] = 1 / w[i];
+      ++noeig;
+    }
+  }
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      double s = 0;
+      for (int k = 0; k < n; ++k) s += (v[i + n * k] * w[k]) * v[j + n * k];
+      cc[i + ld * j] = s;
+    }
+}
+
+// invert_LU (matrix.f90:287-327): DPOTRF('U') + DPOTRI('U') + symmetrise.
+void invert_LU(double *cc, int ld, int n, double &cdet, bool &sing) {
+  // Cholesky A = U^T U, upper triangle in place
+  for (int j = 0; j < n; ++j) {
+    double s = cc[j + ld * j];
+    for (int k = 0; k < j; ++k) s -= cc[k + ld * j] * cc[k + ld * j];
+    if (!(s > 0)) {
+      sing = true;
+      return;
+    }
+    double ujj = std::sqrt(s);
+    cc[j + ld * j] = ujj;
+    for (int i = j + 1; i < n; ++i) {
+      double t = cc[j + ld * i];
+      for (int k = 0; k < j; ++k) t -= cc[k + ld * j] * cc[k + ld * i];
+      cc[j + ld * i] = t / ujj;
+    }
+  }
+  cdet = 1;
+  for (int i = 0; i < n; ++i) cdet *= cc[i + ld * i];
+  // inverse of U (upper), then A^-1 = U^-1 U^-T
+  std::vector<double> ui(n * n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    ui[j + n * j] = 1 / cc[j + ld * j];
+    for (int i = j - 1; i >= 0; --i) {
+      double s = 0;
+      for (int k = i + 1; k <= j; ++k) s += cc[i + ld * k] * ui[k + n * j];
+      ui[i + n * j] = -s / cc[i + ld * i];
+    }
+  }
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i <= j; ++i) {
+      double s = 0;
+      for (int k = j; k < n; ++k) s += ui[i + n * k] * ui[j + n * k];
+      cc[i + ld * j] = s;
+    }
+  for (int i = 0; i < n; ++i)
+    for (int j = i + 1; j < n; ++j) cc[j + ld * i] = cc[i + ld * j];
+  sing = false;
+}
+
+// test_decoupling (matrix.f90:15-51)
+int test_decoupling(double *cc, int n, bool allow_decoupling) {
+  if (!allow_decoupling) return 1;
+  int istart = 2;
+  for (int i = 0; i < n; ++i) {
+    double cii = cc[i + n * i];
+    if (cii > kTiny30) {
+      for (int j = 1; j < n; ++j)
+        if (std::fabs(cc[0 + n * j]) / cii > F(1e-10f)) istart = 1;
+    }
+  }
+  bool any = false;
+  for (int i = 1; i < n; ++i)
+    if (std::fabs(cc[i + n * 0]) > F(1e-10f)) any = true;
+  istart = any ? 1 : 2;
+  if (istart == 2 && cc[0] > kTiny30) {
+    cc[0] = 1 / cc[0];
+    for (int i = 1; i < n; ++i) {
+      cc[i] = 0;
+      cc[0 + n * i] = 0;
+    }
+  }
+  return istart;
+}
+
+// Band Cholesky, lower, ldab = kd+1 (DPBTRF 'L' via the DPBTF2 algorithm).
+// ab[j*(kd+1) + d] = A(j+d, j).  Returns 0 or the 1-based failing column.
+int pbtrf_lower(long n, long kd, double *ab) {
+  long ld = kd + 1;
+  for (long j = 0; j < n; ++j) {
+    double ajj = ab[j * ld];
+    if (!(ajj > 0)) return (int)std::min<long>(j + 1, 2147483647L);
+    ajj = std::sqrt(ajj);
+    ab[j * ld] = ajj;
+    long kn = std::min(kd, n - j - 1);
+    if (kn > 0) {
+      double r = 1.0 / ajj;
+      for (long i = 1; i <= kn; ++i) ab[j * ld + i] *= r;
+      for (long c = 0; c < kn; ++c) {
+        double xc = ab[j * ld + 1 + c];
+        double *col = ab + (j + 1 + c) * ld;
+        for (long r2 = c; r2 < kn; ++r2) col[r2 - c] -= ab[j * ld + 1 + r2] * xc;
+      }
+    }
+  }
+  return 0;
+}
+
+// DPBTRS 'L' with one right-hand side: solve L L^T x = b in place.
+void pbtrs_lower(long n, long kd, const double *ab, double *b) {
+  long ld = kd + 1;
+  for (long j = 0; j < n; ++j) {
+    double bj = b[j] / ab[j * ld];
+    b[j] = bj;
+    long kn = std::min(kd, n - j - 1);
+    for (long i = 1; i <= kn; ++i) b[j + i] -= bj * ab[j * ld + i];
+  }
+  for (long j = n - 1; j >= 0; --j) {
+    double t = b[j];
+    long kn = std::min(kd, n - j - 1);
+    for (long i = 1; i <= kn; ++i) t -= ab[j * ld + i] * b[j + i];
+    b[j] = t / ab[j * ld];
+  }
+}
+
+// ------------------------------------------------ Fortran-style parsing ---
+std::string trim(const std::string &s) {
+  size_t a = s.find_first_not_of(" \t\r\n");
+  if (a == std::string::npos) return "";
+  size_t b = s.find_last_not_of(" \t\r\n");
+  return s.substr(a, b - a + 1);
+}
+
+// first list-directed token (blank, comma or slash terminates it)
+std::string first_token(const std::string &v) {
+  std::string t = trim(v);
+  size_t e = t.find_first_of(" ,/\t");
+  return e == std::string::npos ? t : t.substr(0, e);
+}
+
+bool read_int(const std::string &v, long &out) {
+  std::string t = first_token(v);
+  if (t.empty()) return false;
+  size_t i = 0;
+  if (t[0] == '+' || t[0] == '-') i = 1;
+  if (i >= t.size()) return false;
+  for (size_t k = i; k < t.size(); ++k)
+    if (!isdigit((unsigned char)t[k])) return false;
+  out = std::strtol(t.c_str(), nullptr, 10);
+  return true;
+}
+
+bool read_real(const std::string &v, double &out) {
+  std::string t = first_token(v);
+  if (t.empty()) return false;
+  for (auto &c : t)
+    if (c == 'd' || c == 'D') c = 'e';
+  char *end = nullptr;
+  out = std::strtod(t.c_str(), &end);
+  return end && *end == '\0' && end != t.c_str();
+}
+
+bool read_logical(const std::string &v, bool &out) {
+  std::string t = first_token(v);
+  size_t i = 0;
+  if (i < t.size() && t[i] == '.') ++i;
+  if (i >= t.size()) return false;
+  char c = t[i];
+  if (c == 'T' || c == 't') { out = true; return true; }
+  if (c == 'F' || c == 'f') { out = false; return true; }
+  return false;
+}
+
+struct Detector {
+  std::string name;
+  int npsd = 1;
+  std::vector<double> psdstarts, psdfreqs, sigmas, weights, plateaus;
+  std::vector<std::vector<double>> psds;   // psds[ipsd][bin]
+  bool has_psd = false;
+};
+
+struct Params {
+  // commonparam.f90:200-305 defaults
+  double fsample = 1;
+  bool concatenate_messages = true, allreduce = false, reassign_submaps = true;
+  bool noise_weights_from_psd = false, radiometers = true;
+  long psd_downsample = 10, psdlen = 1000000;
+  long nsubchunk = 0, isubchunk = 0;
+  bool checknan = false;
+  double diagfilter = 0;
+  bool sync_output = true, skip_existing = false, write_cut = false;
+  bool binary_output = false;
+  long nwrite_binary = 10;
+  int basis_func = 4;  // legendre
+  long basis_order = 0;
+  bool bin_subsets = false, mcmode = false;
+  double good_baseline_fraction = 0;
+  bool incomplete_matrices = false;
+  long info = 2;
+  long nside_map = 512, nside_cross = -1, nside_submap = 16;
+  double time_unit = -5;
+  long pixmode_map = 2, pixmode_cross = 2;
+  double pixlim_map = F(1e-6f), pixlim_cross = F(1e-3f);
+  bool allow_decoupling = false;
+  double dnshort = -1;
+  long nshort = -1;
+  bool kfirst = true, kfilter = false, unaligned_fft = false;
+  double cglimit = F(1e-12f);
+  long iter_min = 3, iter_max = 1000;
+  long precond_width_min = 10, precond_width_max = 100;
+  bool use_fprecond = false, use_cgprecond = false;
+  long mode_detweight = 0;
+  bool rm_monopole = false, temperature_only = false;
+  bool flag_by_horn = false, force_pol = false;
+  std::string file_inmask, file_spectrum, file_gap, file_root = "madam",
+      path_output, unit_tod = "unknown", file_gap_out, file_mc, file_covmat;
+  bool write_tod = false;
+  bool do_map = true, do_binmap = false, do_hits = false, do_mask = false,
+       do_matrix = false, do_wcov = false, do_base = false,
+       do_leakmatrix = false;
+  long nthreads = 1;
+  int ndetset = 0, nsurvey = 0;
+};
+
+void parse_detset(Params &p, const std::string &value) {
+  size_t i = value.find(':');
+  if (i == std::string::npos)
+    fail("Failed to parse: " + trim(value) + " for valid detector set name");
+  std::string name = trim(value.substr(0, i));
+  if (name.empty()) fail("Empty detset name");
+  std::string line = trim(value.substr(i + 1));
+  while (true) {
+    size_t c = line.find(',');
+    std::string det = trim(c == std::string::npos ? line : line.substr(0, c));
+    if (det.empty() || det == "all" || det == "All" || det == "ALL") return;
+    if (c == std::string::npos) break;
+    line = trim(line.substr(c + 1));
+  }
+  p.ndetset += 1;
+}
+
+void parse_survey(Params &p, const std::string &value) {
+  size_t i = value.find(':');
+  if (i == std::string::npos)
+    fail("Failed to parse: " + trim(value) + " for valid survey name");
+  std::string name = trim(value.substr(0, i));
+  if (name.empty()) fail("Empty survey name");
+  std::string line = trim(value.substr(i + 1));
+  while (true) {
+    size_t d = line.find('-');
+    if (d == std::string::npos) {
+      if (line.empty() || line == "all" || line == "All" || line == "ALL")
+        return;
+      fail("Failed to parse: " + line + " for valid survey span marker (-)");
+    }
+    double a, b;
+    if (!read_real(line.substr(0, d), a))
+      fail("Failed to parse: " + line + " for valid survey start");
+    line = trim(line.substr(d + 1));
+    if (!read_real(line, b))
+      fail("Failed to parse: " + line + " for valid survey stop");
+    size_t c = line.find(',');
+    if (c == std::string::npos) break;
+    line = trim(line.substr(c + 1));
+  }
+  p.nsurvey += 1;
+}
+
+// read_line (inputparam.f90:169-371)
+void read_line(Params &p, const std::string &line_in) {
+  std::string line = trim(line_in);
+  if (line.empty()) return;
+  size_t eq = line.find('=');
+  if (line[0] == '#') return;
+  if (eq == std::string::npos)
+    fail("Syntax error in parameter definition: " + line);
+  std::string key = trim(line.substr(0, eq)).substr(0, 40);
+  std::string value = trim(line.substr(eq + 1)).substr(0, 200);
+  size_t h = value.find('#');
+  if (h != std::string::npos) value = value.substr(0, h);
+  if (key.compare(0, 8, "detector") == 0) key = "detector";
+  if (trim(value).empty() && key.compare(0, 4, "file") != 0) return;
+
+  bool ok = true;
+  long iv;
+  double dv;
+  bool bv;
+  auto I = [&](long &dst) { ok = read_int(value, iv); if (ok) dst = iv; };
+  auto D = [&](double &dst) { ok = read_real(value, dv); if (ok) dst = dv; };
+  auto L = [&](bool &dst) { ok = read_logical(value, bv); if (ok) dst = bv; };
+  std::string tv = trim(value);
+
+  if (key == "info") I(p.info);
+  else if (key == "nthreads") I(p.nthreads);
+  else if (key == "nsubchunk") I(p.nsubchunk);
+  else if (key == "isubchunk") I(p.isubchunk);
+  else if (key == "time_unit") {
+    if (!tv.empty() && (tv[0] == 'p' || tv[0] == 'P')) p.time_unit = -5;
+    else D(p.time_unit);
+  } else if (key == "base_first" || key == "nshort") D(p.dnshort);
+  else if (key == "nside_map") I(p.nside_map);
+  else if (key == "nside_cross") I(p.nside_cross);
+  else if (key == "nside_submap") I(p.nside_submap);
+  else if (key == "good_baseline_fraction") D(p.good_baseline_fraction);
+  else if (key == "concatenate_messages") L(p.concatenate_messages);
+  else if (key == "allreduce") L(p.allreduce);
+  else if (key == "reassign_submaps") L(p.reassign_submaps);
+  else if (key == "pixmode_map") I(p.pixmode_map);
+  else if (key == "pixmode_cross") I(p.pixmode_cross);
+  else if (key == "pixlim_map") D(p.pixlim_map);
+  else if (key == "pixlim_cross") D(p.pixlim_cross);
+  else if (key == "incomplete_matrices") L(p.incomplete_matrices);
+  else if (key == "allow_decoupling") L(p.allow_decoupling);
+  else if (key == "kfirst") L(p.kfirst);
+  else if (key == "basis_func") {
+    std::string v4 = tv.substr(0, 4);
+    if (v4 == "poly") p.basis_func = 1;
+    else if (v4 == "four") p.basis_func = 2;
+    else if (v4 == "cheb") p.basis_func = 3;
+    else if (v4 == "lege") p.basis_func = 4;
+    else fail("Unknown function basis : " + tv);
+  } else if (key == "basis_order") {
+    I(p.basis_order);
+    if (ok && p.basis_order < 0) fail("basis order must be nonnegative");
+  } else if (key == "iter_min") I(p.iter_min);
+  else if (key == "iter_max") I(p.iter_max);
+  else if (key == "cglimit") D(p.cglimit);
+  else if (key == "fsample") D(p.fsample);
+  else if (key == "mode_detweight") I(p.mode_detweight);
+  else if (key == "flag_by_horn") L(p.flag_by_horn);
+  else if (key == "write_cut") L(p.write_cut);
+  else if (key == "checknan") L(p.checknan);
+  else if (key == "sync_output") L(p.sync_output);
+  else if (key == "skip_existing") L(p.skip_existing);
+  else if (key == "temperature_only") L(p.temperature_only);
+  else if (key == "force_pol") L(p.force_pol);
+  else if (key == "noise_weights_from_psd") L(p.noise_weights_from_psd);
+  else if (key == "radiometers") L(p.radiometers);
+  else if (key == "psdlen") I(p.psdlen);
+  else if (key == "psd_down" || key == "psd_downsample") I(p.psd_downsample);
+  else if (key == "kfilter") L(p.kfilter);
+  else if (key == "diagfilter") D(p.diagfilter);
+  else if (key == "unaligned_fft") L(p.unaligned_fft);
+  else if (key == "precond_width_min") I(p.precond_width_min);
+  else if (key == "precond_width_max") I(p.precond_width_max);
+  else if (key == "use_fprecond") L(p.use_fprecond);
+  else if (key == "use_cgprecond") L(p.use_cgprecond);
+  else if (key == "rm_monopole") L(p.rm_monopole);
+  else if (key == "path_output") p.path_output = tv;
+  else if (key == "file_root") p.file_root = tv;
+  else if (key == "write_map") L(p.do_map);
+  else if (key == "write_binmap") L(p.do_binmap);
+  else if (key == "write_hits") L(p.do_hits);
+  else if (key == "write_matrix") L(p.do_matrix);
+  else if (key == "write_wcov") L(p.do_wcov);
+  else if (key == "write_base") L(p.do_base);
+  else if (key == "write_mask") L(p.do_mask);
+  else if (key == "write_leakmatrix") L(p.do_leakmatrix);
+  else if (key == "unit_tod") p.unit_tod = tv;
+  else if (key == "file_gap_out") p.file_gap_out = tv;
+  else if (key == "file_mc") p.file_mc = tv;
+  else if (key == "write_tod") L(p.write_tod);
+  else if (key == "file_inmask") p.file_inmask = tv;
+  else if (key == "file_spectrum") p.file_spectrum = tv;
+  else if (key == "file_gap") p.file_gap = tv;
+  else if (key == "binary_output") L(p.binary_output);
+  else if (key == "nwrite_binary") I(p.nwrite_binary);
+  else if (key == "file_covmat") p.file_covmat = tv;
+  else if (key == "detset") parse_detset(p, value);
+  else if (key == "detset_nopol") parse_detset(p, value);
+  else if (key == "survey") parse_survey(p, value);
+  else if (key == "bin_subsets") L(p.bin_subsets);
+  else if (key == "mcmode") L(p.mcmode);
+  else fail("Unknown parameter: " + key);
+  if (!ok) fail("Failed to parse " + key + " from " + tv);
+}
+
+// read_parameters (inputparam.f90:24-67) + check_missing_parameters (498-505)
+Params read_parameters(const char *parstring) {
+  Params p;
+  std::string s(parstring ? parstring : "");
+  size_t start = 0;
+  while (start < s.size()) {
+    size_t stop = s.find(';', start);
+    if (stop == std::string::npos) stop = s.size();
+    read_line(p, s.substr(start, stop - start));
+    start = stop + 1;
+  }
+  p.dnshort = std::round(p.dnshort * p.fsample);  // nint: half away from 0
+  if (p.kfirst && p.dnshort < 0) p.dnshort = 1e10;
+  return p;
+}
+
+// --------------------------------------------------------------- state ----
+struct BandPrec {
+  long nband = 0, noba = 0;
+  std::vector<double> data;  // (nband, noba) column-major
+};
+
+struct State {
+  Params par;
+  bool cached = false;
+  long ndet = 0, nsamp = 0, nnz = 0;
+  int nmap = 0;
+  std::vector<Detector> dets;
+  int nthreads = 1;
+
+  // layout
+  long nside_max = 0, nosubmaps_tot = 0, nosubpix_max = 0, nosubpix_map = 0,
+       nosubpix_cross = 0, nopix_map = 0, nopix_cross = 0;
+  long ninterval = 0;
+  std::vector<long> intervals, noba_short_pp, kstart_pp;
+  long noba_short = 0, noba_short_pp_max = 0;
+  std::vector<long> bstart, bstop;  // 0-based inclusive sample index
+  std::vector<double> btime;
+  double dnshort = 0;
+  long nshort = 0;
+
+  // pointing (caller memory)
+  int32_t *pixels = nullptr;
+  float *weights = nullptr;
+  double *tod = nullptr;
+  double *times = nullptr;
+  std::vector<char> ksubmap;
+  std::vector<long> subtable1, subtable2;
+  long dummy_pixel = -1;
+  long nolocmaps = 0, nsize_locmap = -1;
+  std::vector<char> flagged;  // samples that became dummy (for restore)
+
+  // maps
+  std::vector<double> locmap, loccc;
+  std::vector<int> lochits;
+  std::vector<double> map, binmap, cc, cca, wamap;
+  std::vector<int> nohits, outmask;
+  std::vector<float> crit;
+
+  // baselines
+  std::vector<double> aa, yba, nna, nna_inv;
+
+  // filter
+  long nof = -1;
+  long npsdtot = 0;
+  std::vector<double> fcov;  // (nof/2+1) x npsdtot, real valued
+  std::vector<int> psddet;
+  std::vector<double> psdstart, psdstop;
+  std::vector<double> fprecond, invcov;
+  bool use_diagonal = false;
+  std::vector<double> prec_diag;
+  std::map<std::tuple<long, long, long>, BandPrec> bandprec;
+  RealFFT *fft = nullptr;
+
+  // diagnostics
+  long noiter = 0;
+  std::vector<double> rr_history;
+  double rrinit = 0, rr_final = 0;
+  long n_band_ok = 0, n_band_fail = 0;
+  std::vector<long> band_widths;
+  double t_iterate = 0, t_total = 0;
+  bool tod_cleaned = false;
+
+  ~State() { delete fft; }
+};
+
+State *g_state = nullptr;
+std::string g_error;
+
+inline double &CC(std::vector<double> &a, int nmap, long ip, int r, int c) {
+  return a[(size_t)ip * nmap * nmap + (size_t)c * nmap + r];
+}
+
+// ------------------------------------------------------- noise helpers ---
+// interpolate_psd (noise_routines.f90:130-190)
+void interpolate_psd(const std::vector<double> &freq,
+                     const std::vector<double> &psd, const double *target,
+                     double *out, long nout) {
+  long nin = (long)freq.size();
+  if ((long)psd.size() != nin) fail("freq and psd do not have the same shape");
+  bool allzero = true;
+  for (double f : freq)
+    if (f != 0) allzero = false;
+  if (allzero) fail("input freqs are all zero.");
+  long startbin = 0;
+  while (freq[startbin] == 0) ++startbin;
+  std::vector<double> lf(nin), lp(nin);
+  for (long i = 0; i < nin; ++i) {
+    lf[i] = std::log(freq[i]);
+    lp[i] = std::log(psd[i]);
+  }
+  long j = startbin;  // 0-based; Fortran j = startbin+1
+  for (long i = 0; i < nout; ++i) {
+    if (target[i] == 0) {
+      out[i] = 0;
+      continue;
+    }
+    double flog = std::log(target[i]);
+    if (j < nin - 2) {
+      while (lf[j + 1] < flog) {
+        ++j;
+        if (j == nin - 2) break;
+      }
+    }
+    if (psd[j] > 0 && psd[j + 1] > 0) {
+      double r = (flog - lf[j]) / (lf[j + 1] - lf[j]);
+      out[i] = std::exp(lp[j] * (1.0 - r) + lp[j + 1] * r);
+    } else {
+      double r = (target[i] - freq[j]) / (freq[j + 1] - freq[j]);
+      out[i] = psd[j] * (1.0 - r) + psd[j + 1] * r;
+    }
+  }
+}
+
+// psd_index_det (noise_routines.f90:211-236): 0-based, -1 when none
+int psd_index_det(const State &S, long idet, double t) {
+  const Detector &d = S.dets[idet];
+  if (!d.has_psd && d.npsd == 1) return 0;
+  int ipsd = 0;
+  while (true) {
+    if (ipsd == d.npsd - 1) {
+      if (d.psdstarts[ipsd] > t) ipsd = -1;
+      return ipsd;
+    }
+    if (d.psdstarts[ipsd + 1] > t) return ipsd;
+    ++ipsd;
+  }
+}
+
+// psd_index (noise_routines.f90:193-208): global index or -1
+int psd_index(const State &S, long idet, double t) {
+  for (long i = 0; i < S.npsdtot; ++i)
+    if (S.psddet[i] == idet && S.psdstart[i] <= t && S.psdstop[i] >= t)
+      return (int)i;
+  return -1;
+}
+
+// measure_noise_weights (noise_routines.f90:65-127)
+void measure_noise_weights(State &S, bool radiometers) {
+  double fs = S.par.fsample;
+  if (radiometers) {
+    double f = fs / 2, v;
+    for (auto &d : S.dets)
+      for (int i = 0; i < d.npsd; ++i) {
+        interpolate_psd(d.psdfreqs, d.psds[i], &f, &v, 1);
+        d.sigmas[i] = std::sqrt(v * fs);
+        d.plateaus[i] = v;
+      }
+  } else {
+    long nbin = 10000;
+    double fstep = fs * .5 / nbin;
+    std::vector<double> freqs(nbin), data(nbin);
+    for (long i = 0; i < nbin; ++i) freqs[i] = fstep * (i + 1);
+    double fbase = 1 / (S.par.dnshort / fs);
+    long ibase = (long)(fbase / fstep);
+    long ilower = (long)(1 / fstep), iupper = (long)(10 / fstep);
+    for (auto &d : S.dets)
+      for (int ip = 0; ip < d.npsd; ++ip) {
+        interpolate_psd(d.psdfreqs, d.psds[ip], freqs.data(), data.data(), nbin);
+        double plateau = data[ilower - 1];
+        for (long i = ilower - 1; i <= iupper - 1; ++i)
+          plateau = std::min(plateau, data[i]);
+        double rms = ibase * plateau;
+        for (long i = ibase; i < nbin; ++i) rms += data[i];
+        rms = std::sqrt(rms / nbin * fs);
+        d.sigmas[ip] = rms;
+        d.plateaus[ip] = plateau;
+        d.weights[ip] = 1 / (plateau * fs);
+      }
+  }
+}
+
+// trim_interval (noise_routines.f90:764-813); kstart/kstop are 0-based with
+// the Fortran meaning (segment = baselines kstart+1..kstop, 1-based), i.e.
+// 0-based baselines [kstart, kstop).
+void trim_interval(const State &S, long &kstart, long &kstop, long &noba,
+                   long idet) {
+  const double *nna = S.nna.data() + idet * S.noba_short;
+  bool allzero = true;
+  for (long k = kstart; k < kstop; ++k)
+    if (nna[k] != 0) { allzero = false; break; }
+  if (allzero) {
+    noba = 0;
+    return;
+  }
+  while (kstart < kstop) {
+    if (nna[kstart] != 0) break;
+    ++kstart;
+  }
+  while (kstop > kstart) {
+    if (nna[kstop - 1] != 0) break;
+    --kstop;
+  }
+  noba = kstop - kstart;
+  long gapmin = (long)(60 * S.par.fsample / S.dnshort + 1);
+  long gaplen = 0;
+  for (long i = kstart; i < kstop; ++i) {  // Fortran i = kstart+1..kstop
+    if (nna[i] != 0) gaplen = 0;
+    else {
+      ++gaplen;
+      if (gaplen == gapmin) {
+        noba = (i + 1) - gaplen - kstart;
+        return;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------ routines ---
+void check_files(State &S, long nperiod, const long *periods) {
+  S.ninterval = nperiod;
+  S.intervals.assign(nperiod, 0);
+  for (long ip = 0; ip < nperiod; ++ip) {
+    long len = (ip < nperiod - 1) ? periods[ip + 1] - periods[ip]
+                                  : S.nsamp - periods[ip];
+    if (S.par.basis_order > 0 && len < S.par.basis_order + 1)
+      fail("Too short period");
+    S.intervals[ip] = len;
+  }
+  for (long d = 0; d < S.ndet; ++d)
+    for (long i = 0; i < S.nsamp; ++i) {
+      const float *w = S.weights + ((size_t)d * S.nsamp + i) * S.nnz;
+      bool allz = true;
+      for (long j = 0; j < S.nnz; ++j)
+        if (w[j] != 0) allz = false;
+      int32_t &px = S.pixels[(size_t)d * S.nsamp + i];
+      if (allz && !(px < 0)) px = -1;
+    }
+  long istart = 0;
+  for (long ip = 0; ip < nperiod; ++ip) {
+    long istop = istart + S.intervals[ip];
+    for (long d = 0; d < S.ndet; ++d) {
+      int32_t *px = S.pixels + (size_t)d * S.nsamp;
+      long ngood = 0;
+      for (long i = istart; i < istop; ++i)
+        if (px[i] >= 0) ++ngood;
+      if (ngood == 0) continue;
+      double frac = (double)ngood / (double)S.intervals[ip];
+      if (frac < F(1e-3f))
+        for (long i = istart; i < istop; ++i) px[i] = -1;
+    }
+    istart = istop;
+  }
+}
+
+bool is_pow2(long n) { return n > 0 && (n & (n - 1)) == 0; }
+
+void init_parameters(State &S) {
+  Params &p = S.par;
+  if (!p.radiometers) {
+    for (auto &d : S.dets)
+      for (int ip = 0; ip < d.npsd && d.has_psd; ++ip) {
+        auto &psd = d.psds[ip];
+        long im = 0;
+        for (long i = 1; i < (long)psd.size(); ++i)
+          if (psd[i] > psd[im]) im = i;
+        double mx = psd[im];
+        for (long i = 0; i < im; ++i) psd[i] = mx;
+      }
+  }
+  if (p.noise_weights_from_psd) measure_noise_weights(S, p.radiometers);
+  if (p.nsubchunk < 2) {
+    p.nsubchunk = 0;
+    p.isubchunk = 0;
+  }
+  if (p.nsubchunk > 1) fail("nsubchunk > 1 is not supported");
+  if (p.good_baseline_fraction < 0 || p.good_baseline_fraction > 1)
+    fail("ERROR: good_baseline_fraction must be in 0..1");
+  if (p.nside_cross < 0) p.nside_cross = p.nside_map;
+  if (!is_pow2(p.nside_map)) fail("nside_map must be a power of two.");
+  if (!is_pow2(p.nside_submap)) fail("nside_submap must be a power of two.");
+  if (!is_pow2(p.nside_cross)) fail("nside_cross must be a power of two.");
+  if (p.nside_map < p.nside_cross)
+    fail("nside_cross > nside_map not supported by Madam/TOAST");
+  if (p.pixlim_cross < 0) p.pixlim_cross = p.pixlim_map;
+  if (p.pixmode_map < 0 || p.pixmode_map > 2)
+    fail("Pixmode_map must be in range [0-2]");
+  if (p.pixmode_cross < 0 || p.pixmode_cross > 4)
+    fail("Pixmode_cross must be in range [0-4]");
+  if (!p.file_inmask.empty()) fail("file_inmask is not supported");
+  if (!p.file_spectrum.empty()) fail("file_spectrum is not supported");
+  if (!p.file_covmat.empty()) fail("file_covmat is not supported");
+  if (S.nmap == 1) p.temperature_only = true;
+  else if (p.temperature_only) S.nmap = 1;
+  if (S.nmap != 1 && S.nmap != 3) fail("only nnz = 1 or nnz = 3 is supported");
+  if (p.mode_detweight == 0) {
+    for (auto &d : S.dets)
+      for (int i = 0; i < d.npsd; ++i)
+        d.weights[i] = (d.sigmas[i] == 0) ? 0 : 1.0 / d.plateaus[i] / p.fsample;
+  } else if (p.mode_detweight == 1) {
+    for (auto &d : S.dets)
+      for (int i = 0; i < d.npsd; ++i) d.weights[i] = 1;
+  } else if (p.mode_detweight == 2) {
+    auto horn = [](const std::string &n) -> long {
+      long h;
+      std::string s = n.compare(0, 3, "LFI") == 0 ? n.substr(3, 2)
+                                                   : (n.size() > 4 ? n.substr(4, 1) : "");
+      if (!read_int(s, h)) fail("ERROR : Failed to extract horn from " + n);
+      return h;
+    };
+    for (size_t a = 0; a + 1 < S.dets.size(); ++a) {
+      long h1 = horn(S.dets[a].name);
+      for (size_t b = a + 1; b < S.dets.size(); ++b) {
+        if (horn(S.dets[b].name) != h1) continue;
+        auto &d1 = S.dets[a];
+        auto &d2 = S.dets[b];
+        if (d1.npsd != d2.npsd)
+          fail("Detectors in the same horn do not have the same number of PSDs");
+        std::vector<double> w(d1.npsd);
+        for (int i = 0; i < d1.npsd; ++i)
+          w[i] = (d1.plateaus[i] == 0 || d2.plateaus[i] == 0)
+                     ? 0
+                     : 2 / (d1.plateaus[i] + d2.plateaus[i]) / p.fsample;
+        d1.weights = w;
+        d2.weights = w;
+      }
+    }
+  } else {
+    fail("bad mode_detweight");
+  }
+  S.nside_max = std::max(p.nside_map, p.nside_cross);
+  p.nside_submap = std::min({p.nside_submap, p.nside_map, p.nside_cross});
+  S.nosubmaps_tot = 12 * p.nside_submap * p.nside_submap;
+  S.nshort = (long)(p.dnshort + .5);
+  if (!p.kfirst) {
+    p.dnshort = 1e6;
+    S.nshort = (long)(p.dnshort + .5);
+    p.precond_width_min = 0;
+    p.precond_width_max = 0;
+    p.kfilter = false;
+  } else {
+    p.precond_width_max = std::max(p.precond_width_min, p.precond_width_max);
+  }
+  if (p.basis_order > 0 && p.kfilter)
+    fail("Filter only implemented for basis_order==0");
+  if (p.basis_order > 0) fail("basis_order > 0 is not supported");
+  S.dnshort = p.dnshort;
+  if (S.ninterval <= 0) fail("ERROR: intervals not known.");
+  S.noba_short_pp.assign(S.ninterval, 0);
+  S.kstart_pp.assign(S.ninterval, 0);
+  S.noba_short = 0;
+  for (long i = 0; i < S.ninterval; ++i) {
+    if (S.intervals[i] <= 0) fail("empty pointing period");
+    S.noba_short_pp[i] = (long)((double)(S.intervals[i] - 1) / S.dnshort) + 1;
+    S.kstart_pp[i] = S.noba_short;
+    S.noba_short += S.noba_short_pp[i];
+  }
+  long nsm = p.nside_submap;
+  S.nosubpix_max = S.nside_max * S.nside_max / (nsm * nsm);
+  S.nosubpix_map = p.nside_map * p.nside_map / (nsm * nsm);
+  S.nosubpix_cross = p.nside_cross * p.nside_cross / (nsm * nsm);
+  S.noba_short_pp_max = 0;
+  for (long v : S.noba_short_pp) S.noba_short_pp_max = std::max(S.noba_short_pp_max, v);
+  S.nopix_map = S.nosubmaps_tot * S.nosubpix_map;
+  S.nopix_cross = S.nosubmaps_tot * S.nosubpix_cross;
+}
+
+// start_timeloop (parameter_control.f90:752-950) + baseline_times (956-977)
+void start_timeloop(State &S) {
+  std::vector<long> len(S.noba_short);
+  long m = 0;
+  for (long i = 0; i < S.ninterval; ++i) {
+    double dn = 0;
+    long n = 0;
+    for (long k = 0; k < S.noba_short_pp[i] - 1; ++k) {
+      double dn0 = dn;
+      long n0 = n;
+      dn = dn0 + S.dnshort;
+      n = (long)(dn + .5);
+      len[m++] = n - n0;
+    }
+    len[m] = S.intervals[i] - n;
+    if (S.par.kfirst && (len[m] < 0 || len[m] > (long)S.dnshort + 1))
+      fail("ERROR in start_timeloop: Lengths do not match.");
+    ++m;
+  }
+  S.bstart.assign(S.noba_short, 0);
+  S.bstop.assign(S.noba_short, 0);
+  for (long k = 0; k < S.noba_short; ++k) {
+    if (k > 0) S.bstart[k] = S.bstart[k - 1] + len[k - 1];
+    S.bstop[k] = S.bstart[k] + len[k] - 1;
+  }
+  S.btime.assign(S.noba_short, 0);
+  for (long k = 0; k < S.noba_short; ++k) S.btime[k] = S.times[S.bstart[k]];
+}
+
+// init_filter (noise_routines.f90:242-292)
+void init_filter(State &S) {
+  if (!S.par.kfilter) return;
+  long nof_min = 2 * S.noba_short_pp_max;
+  if (S.par.precond_width_max > nof_min - 1) nof_min = S.par.precond_width_max + 1;
+  long nof = 1;
+  while (nof < nof_min) nof *= 2;
+  if (nof < 2) nof = 2;
+  S.nof = nof;
+  delete S.fft;
+  S.fft = new RealFFT(nof);
+}
+
+// build_filter (noise_routines.f90:367-739) with get_spectrum_interp
+void build_filter(State &S) {
+  if (!S.par.kfilter) return;
+  Params &p = S.par;
+  S.npsdtot = 0;
+  for (auto &d : S.dets) S.npsdtot += d.npsd;
+  long nof = S.nof, nh = nof / 2 + 1;
+  S.fcov.assign((size_t)nh * S.npsdtot, 0.0);
+  S.psddet.assign(S.npsdtot, 0);
+  S.psdstart.assign(S.npsdtot, 0);
+  S.psdstop.assign(S.npsdtot, 0);
+  double fa = p.fsample / (double)S.nshort;
+  std::vector<std::pair<long, int>> tasks;
+  for (long d = 0; d < S.ndet; ++d) {
+    if (!S.dets[d].has_psd)
+      fail("All detectors must have at least one PSD to build the filter");
+    for (int ip = 0; ip < S.dets[d].npsd; ++ip) tasks.push_back({d, ip});
+  }
+  std::string err;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(S.nthreads)
+  for (long it = 0; it < (long)tasks.size(); ++it) {
+    try {
+      long d = tasks[it].first;
+      int ip = tasks[it].second;
+      Detector &det = S.dets[d];
+      S.psddet[it] = (int)d;
+      S.psdstart[it] = det.psdstarts[ip];
+      S.psdstop[it] = (ip < det.npsd - 1) ? det.psdstarts[ip + 1] : F(1e30f);
+      double sigma = det.sigmas[ip];
+      std::vector<double> aspec(nh, 0.0), f(nof), g(nof), spec(nof);
+      for (int k = 0; k <= 2; ++k) {
+        for (long i = 0; i < nof; ++i)
+          f[i] = k * fa + (double)i * fa / (double)nof;
+        // get_spectrum_interp
+        interpolate_psd(det.psdfreqs, det.psds[ip], f.data(), spec.data(), nof);
+        double plateau;
+        if (p.noise_weights_from_psd) {
+          plateau = det.plateaus[ip];
+        } else {
+          if (p.radiometers) {
+            double ff = p.fsample / 2;
+            interpolate_psd(det.psdfreqs, det.psds[ip], &ff, &plateau, 1);
+          } else {
+            std::vector<double> fr(1000), dt(1000);
+            for (int i = 0; i < 1000; ++i) fr[i] = 1 + (double)(i * 10) / 1000;
+            interpolate_psd(det.psdfreqs, det.psds[ip], fr.data(), dt.data(), 1000);
+            plateau = *std::min_element(dt.begin(), dt.end());
+          }
+          det.sigmas[ip] = std::sqrt(plateau * p.fsample);
+        }
+        double margin = p.radiometers ? F(1e-6f) : F(1e-3f);
+        bool anyneg = false;
+        for (long i = 0; i < nof; ++i) {
+          if (spec[i] > plateau * (1 + margin)) spec[i] = spec[i] - plateau;
+          else spec[i] = spec[i] * margin;
+          if (spec[i] <= 0) anyneg = true;
+        }
+        if (anyneg) {
+          for (long i = 0; i < nof; ++i) {
+            if (spec[i] <= 0) {
+              bool found = false;
+              for (long j = i + 1; j < nof; ++j)
+                if (spec[j] > 0) { spec[i] = spec[j]; found = true; break; }
+              if (found) continue;
+            }
+            if (spec[i] <= 0) {
+              for (long j = i - 1; j >= 0; --j)
+                if (spec[j] > 0) { spec[i] = spec[j]; break; }
+            }
+          }
+        }
+        if (f[0] == 0) spec[0] = 0;
+        for (long i = 0; i < nof; ++i) {
+          double x = kPi * f[i] / fa;
+          g[i] = (x < kTiny30) ? 1.0 : std::sin(x) * std::sin(x) / (x * x);
+        }
+        if (k == 0) aspec[0] = spec[0];
+        else aspec[0] = aspec[0] + 2 * spec[0] * g[0];
+        for (long i = 1; i < nh; ++i)  // Fortran i = 2..nof/2+1
+          aspec[i] = aspec[i] + spec[i] * g[i] + spec[nof - i] * g[nof - i];
+      }
+      for (long i = 0; i < nh; ++i)
+        aspec[i] = (std::fabs(aspec[i]) > sigma * kTiny30) ? 1.0 / (fa * aspec[i]) : 0.0;
+      aspec[0] = 0;
+      for (long i = 0; i < nh; ++i) {
+        if (std::isnan(aspec[i])) fail("NaN in fcov. Check input PSD and sigma.");
+        S.fcov[(size_t)it * nh + i] = aspec[i];
+      }
+    } catch (const std::exception &e) {
+#pragma omp critical
+      err = e.what();
+    }
+  }
+  if (!err.empty()) fail(err);
+}
+
+// reduce_pixels (pointing.f90:115-163)
+void reduce_pixels(State &S) {
+  S.ksubmap.assign(S.nosubmaps_tot + 1, 0);
+  size_t ntot = (size_t)S.ndet * S.nsamp;
+  for (size_t i = 0; i < ntot; ++i) S.ksubmap[S.pixels[i] / S.nosubpix_max] = 1;
+  S.ksubmap[S.nosubmaps_tot] = 1;
+  S.subtable1.assign(S.nosubmaps_tot + 1, -1);
+  S.subtable2.assign(S.nosubmaps_tot + 1, -1);
+  long k = -1;
+  for (long i = 0; i <= S.nosubmaps_tot; ++i)
+    if (S.ksubmap[i]) {
+      ++k;
+      S.subtable1[i] = i - k;
+      S.subtable2[k] = i - k;
+    }
+#pragma omp parallel for num_threads(S.nthreads)
+  for (size_t i = 0; i < ntot; ++i) {
+    long ip = S.pixels[i] / S.nosubpix_max;
+    S.pixels[i] = (int32_t)(S.pixels[i] - S.subtable1[ip] * S.nosubpix_max);
+  }
+  S.dummy_pixel = (S.nosubmaps_tot - S.subtable1[S.nosubmaps_tot]) * S.nosubpix_max;
+}
+
+void restore_pixels(State &S) {
+  size_t ntot = (size_t)S.ndet * S.nsamp;
+#pragma omp parallel for num_threads(S.nthreads)
+  for (size_t i = 0; i < ntot; ++i) {
+    long ip = S.pixels[i] / S.nosubpix_max;
+    S.pixels[i] = (int32_t)(S.pixels[i] + S.subtable2[ip] * S.nosubpix_max);
+  }
+  S.dummy_pixel = 12 * S.nside_max * S.nside_max;
+}
+
+// update_maptod_transfer (maptod_transfer.f90:49-124), single rank
+void update_maptod_transfer(State &S) {
+  S.nolocmaps = 0;
+  for (long i = 0; i < S.nosubmaps_tot; ++i) S.nolocmaps += S.ksubmap[i] ? 1 : 0;
+  long nolocpix = S.nolocmaps * S.nosubpix_max;
+  if (S.nsize_locmap < nolocpix) S.nsize_locmap = nolocpix;
+  S.locmap.assign((size_t)S.nmap * (S.nsize_locmap + 1), 0.0);
+  S.loccc.assign((size_t)S.nmap * S.nmap * (S.nsize_locmap + 1), 0.0);
+  S.lochits.assign(S.nsize_locmap + 1, 0);
+}
+
+// collect_map (maptod_transfer.f90:461-625), single rank: map += locmap
+void collect_map(State &S, std::vector<double> &map, long nosubpix) {
+  long ndegrade = S.nosubpix_max / nosubpix;
+  int nmap = S.nmap;
+  long k = 0;
+  for (long i = 0; i < S.nosubmaps_tot; ++i) {
+    if (!S.ksubmap[i]) continue;
+    for (long n = 0; n < nosubpix; ++n) {
+      long j0 = k * nosubpix * ndegrade + n * ndegrade;
+      for (int c = 0; c < nmap; ++c) {
+        double s = 0;
+        for (long d = 0; d < ndegrade; ++d) s += S.locmap[(size_t)(j0 + d) * nmap + c];
+        if (ndegrade == 1) s = S.locmap[(size_t)j0 * nmap + c];
+        map[(size_t)(i * nosubpix + n) * nmap + c] += s;
+      }
+    }
+    ++k;
+  }
+}
+
+void collect_cc(State &S, std::vector<double> &cc, long nosubpix) {
+  long ndegrade = S.nosubpix_max / nosubpix;
+  int nmap = S.nmap, nn = nmap * nmap;
+  long k = 0;
+  for (long i = 0; i < S.nosubmaps_tot; ++i) {
+    if (!S.ksubmap[i]) continue;
+    for (long n = 0; n < nosubpix; ++n) {
+      long j0 = k * nosubpix * ndegrade + n * ndegrade;
+      for (int e = 0; e < nn; ++e) {
+        double s = 0;
+        for (long d = 0; d < ndegrade; ++d) s += S.loccc[(size_t)(j0 + d) * nn + e];
+        if (ndegrade == 1) s = S.loccc[(size_t)j0 * nn + e];
+        cc[(size_t)(i * nosubpix + n) * nn + e] += s;
+      }
+    }
+    ++k;
+  }
+}
+
+void collect_hits(State &S, std::vector<int> &hits, long nosubpix) {
+  long ndegrade = S.nosubpix_max / nosubpix;
+  long k = 0;
+  for (long i = 0; i < S.nosubmaps_tot; ++i) {
+    if (!S.ksubmap[i]) continue;
+    for (long n = 0; n < nosubpix; ++n) {
+      long j0 = k * nosubpix * ndegrade + n * ndegrade;
+      int s = 0;
+      for (long d = 0; d < ndegrade; ++d) s += S.lochits[j0 + d];
+      hits[i * nosubpix + n] += s;
+    }
+    ++k;
+  }
+}
+
+// scatter_map (maptod_transfer.f90:942-1113), single rank: locmap = map
+void scatter_map(State &S, const std::vector<double> &map, long nosubpix) {
+  long ndegrade = S.nosubpix_max / nosubpix;
+  int nmap = S.nmap;
+  std::fill(S.locmap.begin(), S.locmap.end(), 0.0);
+  long k = 0;
+  for (long i = 0; i < S.nosubmaps_tot; ++i) {
+    if (!S.ksubmap[i]) continue;
+    for (long n = 0; n < nosubpix; ++n)
+      for (long d = 0; d < ndegrade; ++d)
+        for (int c = 0; c < nmap; ++c)
+          S.locmap[(size_t)(k * nosubpix * ndegrade + n * ndegrade + d) * nmap + c] =
+              map[(size_t)(i * nosubpix + n) * nmap + c];
+    ++k;
+  }
+}
+
+// Thread-local pixel range used by the scatter routines (pixel-range
+// ownership: smadam_routines.f90:144-147)
+inline void pix_range(const State &S, int tid, int nth, long &first, long &last) {
+  first = (long)tid * S.nsize_locmap / nth;
+  last = (long)(tid + 1) * S.nsize_locmap / nth - 1;
+  last = std::min(last, S.dummy_pixel - 1);
+}
+
+// pixel_matrix (smadam_routines.f90:111-246)
+void pixel_matrix(State &S) {
+  std::fill(S.loccc.begin(), S.loccc.end(), 0.0);
+  int nmap = S.nmap, nn = nmap * nmap;
+#pragma omp parallel num_threads(S.nthreads)
+  {
+    int tid = omp_get_thread_num(), nth = omp_get_num_threads();
+    long first, last;
+    pix_range(S, tid, nth, first, last);
+    for (long d = 0; d < S.ndet; ++d) {
+      for (long iv = 0; iv < S.ninterval; ++iv) {
+        long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
+        int ipsd = psd_index_det(S, d, S.btime[ks]);
+        if (ipsd < 0) continue;
+        double detw = S.dets[d].weights[ipsd];
+        if (detw == 0) continue;
+        double sqw = std::sqrt(detw);
+        for (long k = ks; k < ks + noba; ++k)
+          for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+            long ip = S.pixels[(size_t)d * S.nsamp + i];
+            if (ip < first || ip > last) continue;
+            double *c = &S.loccc[(size_t)ip * nn];
+            if (nmap == 1) {
+              c[0] += detw;
+            } else {
+              const float *wf = S.weights + ((size_t)d * S.nsamp + i) * S.nnz;
+              double w0 = (double)wf[0] * sqw, w1 = (double)wf[1] * sqw,
+                     w2 = (double)wf[2] * sqw;
+              c[0 + 3 * 0] += w0 * w0;
+              c[0 + 3 * 1] += w0 * w1;
+              c[0 + 3 * 2] += w0 * w2;
+              c[1 + 3 * 1] += w1 * w1;
+              c[1 + 3 * 2] += w1 * w2;
+              c[2 + 3 * 2] += w2 * w2;
+            }
+          }
+      }
+    }
+  }
+  collect_cc(S, S.cc, S.nosubpix_map);
+  if (S.par.kfirst) collect_cc(S, S.cca, S.nosubpix_cross);
+}
+
+// count_hits (smadam_routines.f90:349-422); counted regardless of write_hits
+void count_hits(State &S) {
+  std::fill(S.lochits.begin(), S.lochits.end(), 0);
+  for (long d = 0; d < S.ndet; ++d) {
+#pragma omp parallel num_threads(S.nthreads)
+    {
+      int tid = omp_get_thread_num(), nth = omp_get_num_threads();
+      long first, last;
+      pix_range(S, tid, nth, first, last);
+      for (long iv = 0; iv < S.ninterval; ++iv) {
+        long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
+        int ipsd = psd_index_det(S, d, S.btime[ks]);
+        if (ipsd < 0) continue;
+        if (S.dets[d].weights[ipsd] == 0) continue;
+        for (long k = ks; k < ks + noba; ++k)
+          for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+            long ip = S.pixels[(size_t)d * S.nsamp + i];
+            if (ip < first || ip > last) continue;
+            S.lochits[ip] += 1;
+          }
+      }
+    }
+  }
+  collect_hits(S, S.nohits, S.nosubpix_map);
+}
+
+// bin_tod (smadam_routines.f90:252-343)
+void bin_tod(State &S) {
+  std::fill(S.locmap.begin(), S.locmap.end(), 0.0);
+  int nmap = S.nmap;
+#pragma omp parallel num_threads(S.nthreads)
+  {
+    int tid = omp_get_thread_num(), nth = omp_get_num_threads();
+    long first, last;
+    pix_range(S, tid, nth, first, last);
+    for (long d = 0; d < S.ndet; ++d)
+      for (long iv = 0; iv < S.ninterval; ++iv) {
+        long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
+        int ipsd = psd_index_det(S, d, S.btime[ks]);
+        if (ipsd < 0) continue;
+        double detw = S.dets[d].weights[ipsd];
+        if (detw == 0) continue;
+        for (long k = ks; k < ks + noba; ++k)
+          for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+            size_t s = (size_t)d * S.nsamp + i;
+            long ip = S.pixels[s];
+            if (ip < first || ip > last) continue;
+            double t = S.tod[s];
+            if (nmap == 1) {
+              S.locmap[ip] += t * detw;
+            } else {
+              const float *wf = S.weights + s * S.nnz;
+              for (int c = 0; c < 3; ++c)
+                S.locmap[(size_t)ip * 3 + c] += (double)wf[c] * t * detw;
+            }
+          }
+      }
+  }
+  if (S.par.kfirst) collect_map(S, S.map, S.nosubpix_map);
+  collect_map(S, S.binmap, S.nosubpix_map);  // binned map always kept
+  if (S.par.kfirst) collect_map(S, S.wamap, S.nosubpix_cross);
+}
+
+// ccmultiply (map_routines.f90:24-77)
+void ccmultiply(const State &S, const std::vector<double> &cc,
+                std::vector<double> &map, long nopix) {
+  int nmap = S.nmap;
+#pragma omp parallel for num_threads(S.nthreads)
+  for (long ip = 0; ip < nopix; ++ip) {
+    const double *c = &cc[(size_t)ip * nmap * nmap];
+    double *m = &map[(size_t)ip * nmap];
+    if (c[0] == 0) {
+      for (int j = 0; j < nmap; ++j) m[j] = 0;
+    } else if (nmap == 1) {
+      m[0] = c[0] * m[0];
+    } else {
+      double tm = c[0] * m[0] + c[1] * m[1] + c[2] * m[2];
+      double qm = c[1] * m[0] + c[4] * m[1] + c[5] * m[2];
+      double um = c[2] * m[0] + c[5] * m[1] + c[8] * m[2];
+      m[0] = tm;
+      m[1] = qm;
+      m[2] = um;
+    }
+  }
+}
+
+// invert_pixelmatrix_cross (map_routines.f90:83-212)
+void invert_pixelmatrix_cross(State &S) {
+  int nmap = S.nmap, nn = nmap * nmap;
+  Params &p = S.par;
+  if (nmap == 1) {
+    for (long ip = 0; ip < S.nopix_cross; ++ip) {
+      double &c = S.cca[ip];
+      c = (c != 0) ? 1.0 / c : 0.0;
+    }
+    return;
+  }
+#pragma omp parallel for num_threads(S.nthreads)
+  for (long ip = 0; ip < S.nopix_cross; ++ip) {
+    double *c = &S.cca[(size_t)ip * nn];
+    bool allz = true;
+    for (int e = 0; e < nn; ++e)
+      if (c[e] != 0) allz = false;
+    if (allz) continue;
+    int istart = test_decoupling(c, nmap, p.allow_decoupling) - 1;
+    int ns = nmap - istart;
+    double *sub = c + istart + nmap * istart;
+    double cdet = 0, rcnd = 0, trace, tracen;
+    bool sing = false;
+    int noeig;
+    switch (p.pixmode_cross) {
+      case 0:
+        invert_LU(sub, nmap, ns, cdet, sing);
+        if (cdet < p.pixlim_cross || sing) std::fill(c, c + nn, 0.0);
+        break;
+      case 1:
+        trace = 0;
+        for (int i = istart; i < nmap; ++i) trace += c[i + nmap * i];
+        tracen = (std::fabs(trace) < kTiny30) ? 0 : std::pow(nmap / trace, nmap);
+        invert_LU(sub, nmap, ns, cdet, sing);
+        if (cdet * tracen < p.pixlim_cross || sing) std::fill(c, c + nn, 0.0);
+        break;
+      case 2:
+        invert_eig(sub, nmap, ns, p.incomplete_matrices, cdet, rcnd, sing);
+        if (rcnd < p.pixlim_cross || sing) std::fill(c, c + nn, 0.0);
+        break;
+      case 3:
+        if (c[0] > kTiny30) {
+          if (istart == 0) c[0] = 1.0 / c[0];
+          for (int j = 1; j < nmap; ++j)
+            for (int i = 0; i < nmap; ++i) c[i + nmap * j] = 0;
+          for (int i = 1; i < nmap; ++i) c[i] = 0;
+        } else {
+          std::fill(c, c + nn, 0.0);
+        }
+        break;
+      case 4:
+        invert_eig_s(sub, nmap, ns, p.pixlim_cross, cdet, rcnd, noeig);
+        break;
+    }
+  }
+}
+
+// invert_pixelmatrix_map (map_routines.f90:218-321)
+void invert_pixelmatrix_map(State &S) {
+  int nmap = S.nmap, nn = nmap * nmap;
+  Params &p = S.par;
+  S.outmask.assign(S.nopix_map, 0);
+  S.crit.assign(S.nopix_map, 0.0f);
+  if (nmap == 1) {
+    for (long ip = 0; ip < S.nopix_map; ++ip) {
+      double &c = S.cc[ip];
+      if (c != 0) {
+        c = 1.0 / c;
+        S.outmask[ip] = 1;
+      } else {
+        c = 0;
+        S.outmask[ip] = 0;
+      }
+    }
+    return;
+  }
+#pragma omp parallel for num_threads(S.nthreads)
+  for (long ip = 0; ip < S.nopix_map; ++ip) {
+    double *c = &S.cc[(size_t)ip * nn];
+    bool allz = true;
+    for (int e = 0; e < nn; ++e)
+      if (c[e] != 0) allz = false;
+    if (allz) continue;
+    int istart = test_decoupling(c, nmap, p.allow_decoupling) - 1;
+    int ns = nmap - istart;
+    double *sub = c + istart + nmap * istart;
+    double cdet = 0, rcnd = 0, pcrit = 0, trace, tracen;
+    bool sing = false;
+    switch (p.pixmode_map) {
+      case 0:
+        invert_LU(sub, nmap, ns, cdet, sing);
+        pcrit = cdet;
+        break;
+      case 1:
+        trace = 0;
+        for (int i = istart; i < nmap; ++i) trace += c[i + nmap * i];
+        tracen = (std::fabs(trace) < kTiny30) ? 0 : std::pow(nmap / trace, nmap);
+        invert_LU(sub, nmap, ns, cdet, sing);
+        pcrit = cdet * tracen;
+        break;
+      default:
+        invert_eig(sub, nmap, ns, p.incomplete_matrices, cdet, rcnd, sing);
+        pcrit = rcnd;
+        break;
+    }
+    if (pcrit < p.pixlim_map || sing) {
+      std::fill(c, c + nn, 0.0);
+      S.outmask[ip] = 0;
+    } else {
+      S.outmask[ip] = 1;
+    }
+    S.crit[ip] = (float)pcrit;
+  }
+}
+
+// initialize_a (smadam_routines.f90:428-671), basis_order = 0
+void initialize_a(State &S) {
+  ccmultiply(S, S.cca, S.wamap, S.nopix_cross);
+  scatter_map(S, S.wamap, S.nosubpix_cross);
+  int nmap = S.nmap;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(S.nthreads)
+  for (long d = 0; d < S.ndet; ++d) {
+    for (long iv = 0; iv < S.ninterval; ++iv) {
+      long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
+      int ipsd = psd_index_det(S, d, S.btime[ks]);
+      if (ipsd < 0) continue;
+      double detw = S.dets[d].weights[ipsd];
+      if (detw == 0) continue;
+      for (long k = ks; k < ks + noba; ++k) {
+        double y = 0, n = 0;
+        for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+          size_t s = (size_t)d * S.nsamp + i;
+          long ip = S.pixels[s];
+          if (ip == S.dummy_pixel) continue;
+          const double *lm = &S.locmap[(size_t)ip * nmap];
+          bool allz = true;
+          for (int c = 0; c < nmap; ++c)
+            if (lm[c] != 0) allz = false;
+          if (allz) continue;
+          y = y + 1.0 * S.tod[s];
+          n = n + 1.0 * 1.0;
+          if (nmap == 1) {
+            y = y - 1.0 * lm[0];
+          } else {
+            const float *wf = S.weights + s * S.nnz;
+            double dp = lm[0] * (double)wf[0] + lm[1] * (double)wf[1] + lm[2] * (double)wf[2];
+            y = y - 1.0 * dp;
+          }
+        }
+        S.yba[d * S.noba_short + k] = y * detw;
+        S.nna[d * S.noba_short + k] = n * detw;
+      }
+    }
+  }
+  // invert the 1x1 F^T F blocks (dsyev on a 1x1 block)
+  for (long d = 0; d < S.ndet; ++d)
+    for (long iv = 0; iv < S.ninterval; ++iv) {
+      long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
+      int ipsd = psd_index_det(S, d, S.btime[ks]);
+      if (ipsd < 0) continue;
+      if (S.dets[d].weights[ipsd] == 0) continue;
+      for (long k = ks; k < ks + noba; ++k) {
+        size_t o = d * S.noba_short + k;
+        S.nna_inv[o] = 0;
+        double ev = (std::fabs(S.nna[o]) < kTiny30) ? 0.0 : S.nna[o];
+        if (ev == 0) {
+          S.nna[o] = 0;
+          S.yba[o] = 0;
+          continue;
+        }
+        S.nna_inv[o] = 1.0 / ev;
+      }
+    }
+}
+
+// ----------------------------------------------------- FFT convolution ---
+struct FFTWork {
+  std::vector<double> xx;
+  std::vector<std::complex<double>> fx, work;
+};
+
+// convolve_interval core: y = filter(x) over noba values with spectrum fc
+void convolve_segment(const State &S, const double *x, double *y, long noba,
+                      const double *fc, FFTWork &w) {
+  long nof = S.nof, nh = nof / 2 + 1;
+  w.xx.assign(nof, 0.0);
+  w.fx.resize(nh);
+  double s = 0;
+  for (long i = 0; i < noba; ++i) s += x[i];
+  double mean = s / noba;
+  for (long i = 0; i < noba; ++i) w.xx[i] = x[i] - mean;
+  S.fft->rfft(w.xx.data(), w.fx.data(), w.work);
+  for (long i = 0; i < nh; ++i) w.fx[i] *= fc[i];
+  S.fft->irfft(w.fx.data(), w.xx.data(), w.work);
+  s = 0;
+  for (long i = 0; i < noba; ++i) s += w.xx[i];
+  mean = s / noba;
+  for (long i = 0; i < noba; ++i) y[i] = w.xx[i] - mean;
+}
+
+// convolve_pp (noise_routines.f90:861-913) with convolve_interval (816-857)
+void convolve_pp(State &S, std::vector<double> &y, const std::vector<double> &x,
+                 const std::vector<double> &fc) {
+  y = x;
+  long nh = S.nof / 2 + 1;
+  long ntask = S.ndet * S.ninterval;
+#pragma omp parallel num_threads(S.nthreads)
+  {
+    FFTWork w;
+#pragma omp for schedule(static, 1)
+    for (long t = 0; t < ntask; ++t) {
+      long d = t / S.ninterval, iv = t % S.ninterval;
+      long ks = S.kstart_pp[iv], kstop = ks + S.noba_short_pp[iv];
+      int ipsd = psd_index(S, d, S.btime[ks]);
+      if (ipsd == -1) continue;
+      while (true) {
+        long noba;
+        trim_interval(S, ks, kstop, noba, d);
+        if (noba == 0) break;
+        convolve_segment(S, &x[d * S.noba_short + ks], &y[d * S.noba_short + ks],
+                         noba, &fc[(size_t)ipsd * nh], w);
+        ks += noba;
+      }
+    }
+  }
+}
+
+// construct_preconditioner (noise_routines.f90:920-1153)
+void construct_preconditioner(State &S) {
+  Params &p = S.par;
+  S.bandprec.clear();
+  S.band_widths.clear();
+  S.n_band_ok = S.n_band_fail = 0;
+  if (p.precond_width_max < 1) return;
+  if (!p.kfilter || p.precond_width_max == 1) {
+    S.use_diagonal = true;
+    S.prec_diag.assign((size_t)S.noba_short * S.ndet, 0.0);
+    for (long d = 0; d < S.ndet; ++d)
+      for (long iv = 0; iv < S.ninterval; ++iv) {
+        long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
+        int ipd = psd_index_det(S, d, S.btime[ks]);
+        for (long k = ks; k < ks + noba; ++k) {
+          size_t o = d * S.noba_short + k;
+          if (ipd < 0) S.prec_diag[o] = 1.;
+          else if (S.nna[o] == 0) S.prec_diag[o] = 1. / S.dets[d].weights[ipd];
+          else S.prec_diag[o] = 1. / S.nna[o];
+        }
+      }
+    return;
+  }
+  S.use_diagonal = false;
+  long nof = S.nof, nh = nof / 2 + 1;
+  S.fprecond.assign((size_t)nh * S.npsdtot, 0.0);
+  {
+    long ip = 0;
+    for (long d = 0; d < S.ndet; ++d)
+      for (int k = 0; k < S.dets[d].npsd; ++k, ++ip)
+        for (long i = 0; i < nh; ++i)
+          S.fprecond[(size_t)ip * nh + i] =
+              1.0 / ((double)S.nshort * S.dets[d].weights[k] + S.fcov[(size_t)ip * nh + i]);
+  }
+  if (p.use_fprecond) return;
+  S.invcov.assign((size_t)nof * S.npsdtot, 0.0);
+  for (long ip = 0; ip < S.npsdtot; ++ip) {
+    std::vector<std::complex<double>> fx(nh), work;
+    for (long i = 0; i < nh; ++i) fx[i] = S.fcov[(size_t)ip * nh + i];
+    S.fft->irfft(fx.data(), &S.invcov[(size_t)ip * nof], work);
+  }
+  if (p.use_cgprecond) return;
+  // enumerate segments, then factor in parallel
+  struct Seg { long d, iv, isub, ks, noba; int ipsd; };
+  std::vector<Seg> segs;
+  for (long d = 0; d < S.ndet; ++d)
+    for (long iv = 0; iv < S.ninterval; ++iv) {
+      long ks = S.kstart_pp[iv], kstop = ks + S.noba_short_pp[iv];
+      long isub = 0;
+      while (true) {
+        long noba;
+        trim_interval(S, ks, kstop, noba, d);
+        if (noba == 0) break;
+        int ipsd = psd_index(S, d, S.btime[ks]);
+        bool empty = (ipsd == -1 || noba < 1);
+        if (!empty) {
+          bool allz = true;
+          for (long k = ks; k < ks + noba; ++k)
+            if (S.nna[d * S.noba_short + k] != 0) allz = false;
+          empty = allz;
+        }
+        if (!empty) segs.push_back({d, iv, isub, ks, noba, ipsd});
+        ks += noba;
+        ++isub;
+      }
+    }
+  std::vector<BandPrec> res(segs.size());
+  std::vector<char> okv(segs.size(), 0);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(S.nthreads)
+  for (long si = 0; si < (long)segs.size(); ++si) {
+    const Seg &g = segs[si];
+    const double *ic = &S.invcov[(size_t)g.ipsd * nof];
+    double p_tot = 0;
+    for (long i = 0; i < nof / 2; ++i) p_tot += ic[i] * ic[i];
+    const double plim = (double)(1.0f - 1e-5f);
+    long tr = 1, nband = 0;
+    int ierr = -1;
+    while (true) {
+      nband = std::min(g.noba, tr * p.precond_width_min);
+      nband = std::min(nband, p.precond_width_max);
+      double pp = 0;
+      for (long i = 0; i < nband; ++i) pp += ic[i] * ic[i];
+      if (pp > plim * p_tot) { ierr = 0; break; }
+      if (nband == g.noba || nband == p.precond_width_max) break;
+      if (tr == 1000) break;
+      ++tr;
+    }
+    if (ierr == 0) {
+      while (true) {
+        BandPrec b;
+        b.nband = nband;
+        b.noba = g.noba;
+        b.data.assign((size_t)nband * g.noba, 0.0);
+        for (long j = 0; j < g.noba; ++j) {
+          for (long r = 0; r < nband; ++r) b.data[(size_t)j * nband + r] = ic[r];
+          b.data[(size_t)j * nband] += S.nna[g.d * S.noba_short + g.ks + j];
+        }
+        ierr = pbtrf_lower(g.noba, nband - 1, b.data.data());
+        if (ierr == 0) {
+          res[si] = std::move(b);
+          break;
+        }
+        if (tr == 1000) break;
+        if (nband == g.noba || nband == p.precond_width_max) break;
+        ++tr;
+        nband = std::min(nband + p.precond_width_min, p.precond_width_max);
+      }
+    }
+    okv[si] = (ierr == 0);
+  }
+  for (size_t si = 0; si < segs.size(); ++si) {
+    if (okv[si]) {
+      S.band_widths.push_back(res[si].nband);
+      S.bandprec[{segs[si].isub, segs[si].iv, segs[si].d}] = std::move(res[si]);
+      ++S.n_band_ok;
+    } else {
+      ++S.n_band_fail;
+    }
+  }
+}
+
+// apply_CG_preconditioner (noise_routines.f90:1305-1409)
+void apply_cg_preconditioner(const State &S, long noba, const double *fc,
+                             const double *nna, double *x, const double *b,
+                             const double *ic, FFTWork &w) {
+  std::vector<double> resid(noba), prop(noba), Aprop(noba), zres(noba), prec(noba);
+  for (long i = 0; i < noba; ++i) x[i] = 0;
+  for (long i = 0; i < noba; ++i) resid[i] = b[i] - x[i];
+  double rr = 0;
+  for (long i = 0; i < noba; ++i) rr += resid[i] * resid[i];
+  if (rr == 0) return;
+  double rr0 = rr;
+  for (long i = 0; i < noba; ++i) {
+    prec[i] = nna[i] + ic[0];
+    if (prec[i] != 0) prec[i] = 1 / prec[i];
+  }
+  for (long i = 0; i < noba; ++i) zres[i] = prec[i] * resid[i];
+  double rz = 0;
+  for (long i = 0; i < noba; ++i) rz += resid[i] * zres[i];
+  prop = zres;
+  int iter = 1;
+  while (true) {
+    convolve_segment(S, prop.data(), Aprop.data(), noba, fc, w);
+    for (long i = 0; i < noba; ++i) Aprop[i] = Aprop[i] + nna[i] * prop[i];
+    double an = 0;
+    for (long i = 0; i < noba; ++i) an += prop[i] * Aprop[i];
+    double alpha = rz / an;
+    for (long i = 0; i < noba; ++i) x[i] = x[i] + alpha * prop[i];
+    for (long i = 0; i < noba; ++i) resid[i] = resid[i] - alpha * Aprop[i];
+    rr = 0;
+    for (long i = 0; i < noba; ++i) rr += resid[i] * resid[i];
+    if (rr / rr0 < F(1e-6f) || iter == 100) break;
+    for (long i = 0; i < noba; ++i) zres[i] = prec[i] * resid[i];
+    double rz_old = rz;
+    rz = 0;
+    for (long i = 0; i < noba; ++i) rz += resid[i] * zres[i];
+    double beta = rz / rz_old;
+    for (long i = 0; i < noba; ++i) prop[i] = zres[i] + beta * prop[i];
+    ++iter;
+  }
+}
+
+// preconditioning_band (noise_routines.f90:1159-1256)
+void apply_preconditioner(State &S, std::vector<double> &z,
+                          const std::vector<double> &r) {
+  z = r;
+  Params &p = S.par;
+  if (p.precond_width_max < 1) return;
+  if (S.use_diagonal) {
+    for (size_t i = 0; i < z.size(); ++i) z[i] = r[i] * S.prec_diag[i];
+    return;
+  }
+  if (p.use_fprecond) {
+    convolve_pp(S, z, r, S.fprecond);
+    return;
+  }
+  long nof = S.nof, nh = nof / 2 + 1;
+  struct Seg { long d, iv, isub, ks, noba; };
+  std::vector<Seg> segs;
+  for (long d = 0; d < S.ndet; ++d)
+    for (long iv = 0; iv < S.ninterval; ++iv) {
+      long ks = S.kstart_pp[iv], kstop = ks + S.noba_short_pp[iv];
+      long isub = 0;
+      while (true) {
+        long noba;
+        trim_interval(S, ks, kstop, noba, d);
+        if (noba == 0) break;
+        segs.push_back({d, iv, isub, ks, noba});
+        ks += noba;
+        ++isub;
+      }
+    }
+#pragma omp parallel num_threads(S.nthreads)
+  {
+    FFTWork w;
+#pragma omp for schedule(static, 1)
+    for (long si = 0; si < (long)segs.size(); ++si) {
+      const Seg &g = segs[si];
+      int ipd = psd_index_det(S, g.d, S.btime[g.ks]);
+      if (ipd < 0) continue;
+      if (S.dets[g.d].weights[ipd] == 0) continue;
+      int ipsd = psd_index(S, g.d, S.btime[g.ks]);
+      size_t o = g.d * S.noba_short + g.ks;
+      auto it = S.bandprec.find({g.isub, g.iv, g.d});
+      if (it != S.bandprec.end()) {
+        for (long i = 0; i < g.noba; ++i) z[o + i] = r[o + i];
+        pbtrs_lower(g.noba, it->second.nband - 1, it->second.data.data(), &z[o]);
+      } else {
+        apply_cg_preconditioner(S, g.noba, &S.fcov[(size_t)ipsd * nh], &S.nna[o],
+                                &z[o], &r[o], &S.invcov[(size_t)ipsd * nof], w);
+      }
+    }
+  }
+}
+
+// iterate_a (smadam_routines.f90:677-983), basis_order = 0
+void iterate_a(State &S) {
+  Params &p = S.par;
+  long nb = S.noba_short * S.ndet;
+  int nmap = S.nmap;
+  std::vector<double> r(nb, 0), pv(nb, 0), z(nb, 0), ap(nb, 0), ro(nb, 0);
+  std::vector<char> rmask(nb, 0);
+  for (long d = 0; d < S.ndet; ++d)
+    for (long iv = 0; iv < S.ninterval; ++iv) {
+      long ks = S.kstart_pp[iv], kstop = ks + S.noba_short_pp[iv];
+      while (true) {
+        long noba;
+        trim_interval(S, ks, kstop, noba, d);
+        if (noba == 0) break;
+        for (long k = ks; k < ks + noba; ++k) rmask[d * S.noba_short + k] = 1;
+        ks += noba;
+      }
+    }
+  std::fill(S.aa.begin(), S.aa.end(), 0.0);
+  r = S.yba;
+  apply_preconditioner(S, z, r);
+  pv = z;
+  auto mdot = [&](const std::vector<double> &a, const std::vector<double> &b) {
+    double s = 0;
+    for (long i = 0; i < nb; ++i)
+      if (rmask[i]) s += a[i] * b[i];
+    return s;
+  };
+  double rz = mdot(r, z), rr = mdot(r, r);
+  double rzinit = rz, rrinit = rr;
+  S.rrinit = rrinit;
+  S.rr_history.clear();
+  S.noiter = 0;
+  if (rzinit < kTiny30) return;
+  if (std::isnan(rz)) return;
+  long istep = 0;
+  // per-baseline detector weight (0 when the interval is skipped)
+  std::vector<double> bw(nb, 0.0);
+  for (long d = 0; d < S.ndet; ++d)
+    for (long iv = 0; iv < S.ninterval; ++iv) {
+      long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
+      int ipsd = psd_index_det(S, d, S.btime[ks]);
+      if (ipsd < 0) continue;
+      double detw = S.dets[d].weights[ipsd];
+      for (long k = ks; k < ks + noba; ++k) bw[d * S.noba_short + k] = detw;
+    }
+  double t0 = omp_get_wtime();
+  while (true) {
+    if (istep >= p.iter_max) break;
+    ++istep;
+    // baseline_to_map_order0_* (smadam_routines.f90:1049-1111)
+    std::fill(S.locmap.begin(), S.locmap.end(), 0.0);
+    long npix_thread;
+#pragma omp parallel num_threads(S.nthreads)
+    {
+      int tid = omp_get_thread_num(), nth = omp_get_num_threads();
+      npix_thread = (S.nsize_locmap + nth - 1) / nth;
+      long first = tid * npix_thread;
+      long last = std::min(first + npix_thread - 1, S.dummy_pixel - 1);
+      for (long d = 0; d < S.ndet; ++d)
+        for (long iv = 0; iv < S.ninterval; ++iv) {
+          long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
+          double detw = bw[d * S.noba_short + ks];
+          if (detw == 0) continue;
+          for (long k = ks; k < ks + noba; ++k) {
+            double pw = pv[d * S.noba_short + k] * detw;
+            for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+              size_t s = (size_t)d * S.nsamp + i;
+              long ip = S.pixels[s];
+              if (ip < first || ip > last) continue;
+              if (nmap == 1) {
+                S.locmap[ip] += pw;
+              } else {
+                const float *wf = S.weights + s * S.nnz;
+                S.locmap[(size_t)ip * 3 + 0] += (double)wf[0] * pw;
+                S.locmap[(size_t)ip * 3 + 1] += (double)wf[1] * pw;
+                S.locmap[(size_t)ip * 3 + 2] += (double)wf[2] * pw;
+              }
+            }
+          }
+        }
+    }
+    std::fill(S.wamap.begin(), S.wamap.end(), 0.0);
+    collect_map(S, S.wamap, S.nosubpix_cross);
+    ccmultiply(S, S.cca, S.wamap, S.nopix_cross);
+    scatter_map(S, S.wamap, S.nosubpix_cross);
+    if (p.kfilter) {
+      convolve_pp(S, ap, pv, S.fcov);
+    } else {
+      std::fill(ap.begin(), ap.end(), 0.0);
+      if (p.diagfilter != 0)
+        for (long i = 0; i < nb; ++i) ap[i] = S.nna[i] * pv[i] * p.diagfilter;
+    }
+    // map_to_baseline_order0_* (smadam_routines.f90:1232-1329)
+#pragma omp parallel for schedule(static, 1) num_threads(S.nthreads)
+    for (long t = 0; t < S.ndet * S.ninterval; ++t) {
+      long d = t / S.ninterval, iv = t % S.ninterval;
+      long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
+      double detw = bw[d * S.noba_short + ks];
+      if (detw == 0) continue;
+      for (long k = ks; k < ks + noba; ++k) {
+        double apn = 0;
+        for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+          size_t s = (size_t)d * S.nsamp + i;
+          long ip = S.pixels[s];
+          if (ip == S.dummy_pixel) continue;
+          if (nmap == 1) {
+            apn = apn + S.locmap[ip];
+          } else {
+            const float *wf = S.weights + s * S.nnz;
+            const double *lm = &S.locmap[(size_t)ip * 3];
+            apn = apn + (double)wf[0] * lm[0] + (double)wf[1] * lm[1] +
+                  (double)wf[2] * lm[2];
+          }
+        }
+        size_t o = d * S.noba_short + k;
+        apn = S.nna[o] * pv[o] - apn * detw;
+        ap[o] = ap[o] + apn;
+      }
+    }
+    double pap = mdot(pv, ap);
+    double alpha = rz / pap;
+    ro = r;
+    for (long i = 0; i < nb; ++i) S.aa[i] = S.aa[i] + alpha * pv[i];
+    for (long i = 0; i < nb; ++i) r[i] = r[i] - alpha * ap[i];
+    apply_preconditioner(S, z, r);
+    double rzo = rz;
+    rz = mdot(r, z);
+    double rz2 = mdot(ro, z);
+    rr = mdot(r, r);
+    double beta = (rz - rz2) / rzo;
+    S.rr_history.push_back(rr / rrinit);
+    S.noiter = istep;
+    if (rr / rrinit > 1e3) fail("CG is diverging");
+    if (rr / rrinit < p.cglimit && istep > p.iter_min) break;
+    if (rz == 0) break;
+    for (long i = 0; i < nb; ++i) pv[i] = z[i] + beta * pv[i];
+  }
+  S.t_iterate = omp_get_wtime() - t0;
+  S.rr_final = rr / rrinit;
+}
+
+// subtract_baselines_a (smadam_routines.f90:1489-1539)
+void subtract_baselines_a(State &S) {
+  std::fill(S.locmap.begin(), S.locmap.end(), 0.0);
+  int nmap = S.nmap;
+  for (long d = 0; d < S.ndet; ++d)
+    for (long iv = 0; iv < S.ninterval; ++iv) {
+      long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
+      int ipsd = psd_index_det(S, d, S.btime[ks]);
+      if (ipsd < 0) continue;
+      double detw = S.dets[d].weights[ipsd];
+      if (detw == 0) continue;
+      for (long k = ks; k < ks + noba; ++k)
+        for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+          size_t s = (size_t)d * S.nsamp + i;
+          long ip = S.pixels[s];
+          if (ip == S.dummy_pixel) continue;
+          double aw = (1.0 * S.aa[d * S.noba_short + k]) * detw;
+          if (nmap == 1) {
+            S.locmap[ip] = S.locmap[ip] - aw;
+          } else {
+            const float *wf = S.weights + s * S.nnz;
+            for (int c = 0; c < 3; ++c)
+              S.locmap[(size_t)ip * 3 + c] = S.locmap[(size_t)ip * 3 + c] - aw * (double)wf[c];
+          }
+        }
+    }
+  collect_map(S, S.map, S.nosubpix_map);
+}
+
+// makemaps (map_routines.f90:327-357)
+void makemaps(State &S, std::vector<double> &map) {
+  ccmultiply(S, S.cc, map, S.nopix_map);
+  if (!S.par.rm_monopole) return;
+  long cover = 0;
+  for (int v : S.outmask)
+    if (v > 0) ++cover;
+  if (cover == 0) return;
+  double mono = 0;
+  for (long ip = 0; ip < S.nopix_map; ++ip) mono += map[(size_t)ip * S.nmap];
+  mono /= cover;
+  for (long ip = 0; ip < S.nopix_map; ++ip)
+    if (S.outmask[ip] > 0) map[(size_t)ip * S.nmap] -= mono;
+}
+
+// clean_tod (smadam_routines.f90:1545-1585)
+void clean_tod(State &S) {
+  const Params &p = S.par;
+  if (!p.write_tod && p.ndetset == 0 && p.nsurvey == 0) return;
+  if (!p.kfirst) return;
+  if (S.tod_cleaned) return;
+  for (long d = 0; d < S.ndet; ++d)
+    for (long k = 0; k < S.noba_short; ++k)
+      for (long i = S.bstart[k]; i <= S.bstop[k]; ++i)
+        S.tod[(size_t)d * S.nsamp + i] =
+            S.tod[(size_t)d * S.nsamp + i] - 1.0 * S.aa[d * S.noba_short + k];
+  S.tod_cleaned = true;
+}
+
+void allocate_maps(State &S) {
+  int nmap = S.nmap;
+  S.map.assign((size_t)nmap * S.nopix_map, 0.0);
+  S.cc.assign((size_t)nmap * nmap * S.nopix_map, 0.0);
+  S.outmask.assign(S.nopix_map, 0);
+  S.binmap.assign((size_t)nmap * S.nopix_map, 0.0);
+  S.nohits.assign(S.nopix_map, 0);
+  S.crit.assign(S.nopix_map, 0.0f);
+  if (S.par.kfirst) {
+    S.cca.assign((size_t)nmap * nmap * S.nopix_cross, 0.0);
+    S.wamap.assign((size_t)nmap * S.nopix_cross, 0.0);
+  }
+}
+
+// flag_bad_baselines (read_data.f90:30-74)
+void flag_bad_baselines(State &S) {
+  if (S.par.good_baseline_fraction == 0 || S.par.kfilter) return;
+  for (long d = 0; d < S.ndet; ++d)
+    for (long k = 0; k < S.noba_short; ++k) {
+      long ngood = 0;
+      for (long i = S.bstart[k]; i <= S.bstop[k]; ++i)
+        if (S.pixels[(size_t)d * S.nsamp + i] != S.dummy_pixel) ++ngood;
+      long len = S.bstop[k] - S.bstart[k] + 1;
+      if (ngood > 0 && ngood < S.par.good_baseline_fraction * len)
+        for (long i = S.bstart[k]; i <= S.bstop[k]; ++i)
+          S.pixels[(size_t)d * S.nsamp + i] = (int32_t)S.dummy_pixel;
+    }
+}
+
+void read_detectors(State &S, const char *detstring, long ndet,
+                    const double *detweights, const long *npsd, long npsdtot,
+                    const double *psdstarts, long npsdbin, const double *psdfreqs,
+                    long npsdval, const double *psdvals) {
+  S.dets.assign(ndet, Detector());
+  std::string s(detstring ? detstring : "");
+  size_t start = 0;
+  long idet = 0, ipsd = 0, off = 0;
+  while (start < s.size()) {
+    size_t stop = s.find(';', start);
+    if (stop == std::string::npos) stop = s.size();
+    if (idet >= ndet) fail("Too many detectors");
+    Detector &d = S.dets[idet];
+    d.name = trim(s.substr(start, stop - start)).substr(0, 20);
+    long nint = npsd[idet];
+    d.npsd = nint == 0 ? 1 : (int)nint;
+    double w = detweights[idet];
+    d.weights.assign(d.npsd, w);
+    d.sigmas.assign(d.npsd, w > 0 ? 1.0 / std::sqrt(w) : 0.0);
+    d.plateaus.assign(d.npsd, 0.0);
+    for (int i = 0; i < d.npsd; ++i) d.plateaus[i] = d.sigmas[i] * d.sigmas[i] / S.par.fsample;
+    d.psdstarts.assign(d.npsd, 0.0);
+    if (nint > 0) {
+      d.has_psd = true;
+      d.psdfreqs.assign(psdfreqs, psdfreqs + npsdbin);
+      d.psds.assign(nint, std::vector<double>(npsdbin));
+      for (long i = 0; i < nint; ++i) {
+        if (ipsd >= npsdtot || off + npsdbin > npsdval) fail("PSD arrays too short");
+        d.psdstarts[i] = psdstarts[ipsd];
+        std::copy(psdvals + off, psdvals + off + npsdbin, d.psds[i].begin());
+        off += npsdbin;
+        ++ipsd;
+      }
+    }
+    ++idet;
+    start = stop + 1;
+  }
+}
+
+void bind_tod(State &S, long ndet, long nsamp, long nnz, double *timestamps,
+              int32_t *pix, float *pixweights, double *signal) {
+  S.ndet = ndet;
+  S.nsamp = nsamp;
+  S.nnz = nnz;
+  S.times = timestamps;
+  S.pixels = pix;
+  S.weights = pixweights;
+  S.tod = signal;
+}
+
+void run_destripe(State &S, long nperiod, const long *periods) {
+  double t0 = omp_get_wtime();
+  Params &p = S.par;
+  // pixel range check (smadam.F90:156-171)
+  long pmin = 0, pmax = 0;
+  size_t ntot = (size_t)S.ndet * S.nsamp;
+  if (ntot > 0) {
+    pmin = pmax = S.pixels[0];
+    for (size_t i = 0; i < ntot; ++i) {
+      pmin = std::min<long>(pmin, S.pixels[i]);
+      pmax = std::max<long>(pmax, S.pixels[i]);
+    }
+  }
+  long nside_max = std::max(p.nside_map, p.nside_cross);
+  if (pmin < -1) fail("Too small pixel number");
+  if (pmax > 12 * nside_max * nside_max - 1) fail("Too large pixel number");
+  check_files(S, nperiod, periods);
+  init_parameters(S);
+  // init_pointing + where (pixels < 0) pixels = dummy_pixel
+  S.dummy_pixel = 12 * S.nside_max * S.nside_max;
+  S.flagged.assign(ntot, 0);
+  for (size_t i = 0; i < ntot; ++i)
+    if (S.pixels[i] < 0) {
+      S.pixels[i] = (int32_t)S.dummy_pixel;
+      S.flagged[i] = 1;
+    }
+  init_filter(S);
+  build_filter(S);
+  start_timeloop(S);
+  reduce_pixels(S);
+  update_maptod_transfer(S);
+  S.dummy_pixel = 12 * S.nside_max * S.nside_max;
+  S.aa.assign((size_t)S.noba_short * S.ndet, 0.0);
+  S.yba.assign((size_t)S.noba_short * S.ndet, 0.0);
+  S.nna.assign((size_t)S.noba_short * S.ndet, 0.0);
+  S.nna_inv.assign((size_t)S.noba_short * S.ndet, 0.0);
+  allocate_maps(S);
+  if (p.kfirst) flag_bad_baselines(S);
+  pixel_matrix(S);
+  count_hits(S);
+  bin_tod(S);
+  if (p.kfirst) {
+    invert_pixelmatrix_cross(S);
+    initialize_a(S);
+    construct_preconditioner(S);
+    iterate_a(S);
+    subtract_baselines_a(S);
+  }
+  invert_pixelmatrix_map(S);
+  makemaps(S, S.binmap);
+  makemaps(S, S.map);
+  S.tod_cleaned = false;
+  clean_tod(S);
+  S.t_total = omp_get_wtime() - t0;
+}
+
+void run_cached(State &S) {
+  double t0 = omp_get_wtime();
+  Params &p = S.par;
+  size_t ntot = (size_t)S.ndet * S.nsamp;
+  S.flagged.assign(ntot, 0);
+  for (size_t i = 0; i < ntot; ++i)
+    if (S.pixels[i] < 0) {
+      S.pixels[i] = (int32_t)S.dummy_pixel;
+      S.flagged[i] = 1;
+    }
+  std::fill(S.aa.begin(), S.aa.end(), 0.0);
+  std::fill(S.yba.begin(), S.yba.end(), 0.0);
+  std::fill(S.nna.begin(), S.nna.end(), 0.0);
+  std::fill(S.nna_inv.begin(), S.nna_inv.end(), 0.0);
+  reduce_pixels(S);
+  update_maptod_transfer(S);
+  std::fill(S.map.begin(), S.map.end(), 0.0);
+  std::fill(S.binmap.begin(), S.binmap.end(), 0.0);
+  S.dummy_pixel = 12 * S.nside_max * S.nside_max;
+  if (p.kfirst) flag_bad_baselines(S);
+  bin_tod(S);  // note: wamap keeps its previous contents (smadam.F90:719-732)
+  if (p.kfirst) {
+    initialize_a(S);
+    iterate_a(S);
+    subtract_baselines_a(S);
+  }
+  makemaps(S, S.binmap);
+  makemaps(S, S.map);
+  S.tod_cleaned = false;
+  clean_tod(S);
+  S.t_total = omp_get_wtime() - t0;
+}
+
+}  // namespace
+
+// ======================================================== C interface ====
+extern "C" {
+
+const char *oracle_last_error(void) { return g_error.c_str(); }
+
+// Same arguments as destripe() (madam.h:1-2).  Returns 0 on success, nonzero
+// on any condition where the reference would call abort_mpi / stop.
+int oracle_destripe(int comm, const char *parstring, long ndet,
+                    const char *detstring, const double *detweights, long nsamp,
+                    long nnz, double *timestamps, int32_t *pix,
+                    float *pixweights, double *signal, long nperiod,
+                    const long *periods, const long *npsd, long npsdtot,
+                    const double *psdstarts, long npsdbin,
+                    const double *psdfreqs, long npsdval,
+                    const double *psdvals) {
+  (void)comm;
+  g_error.clear();
+  try {
+    Params p = read_parameters(parstring);
+    if (g_state && p.mcmode && g_state->cached)
+      fail("Destripe called while caches are not empty.");
+    if (p.temperature_only && nnz != 1)
+      fail("temperature_only=T but pointing weights are polarized");
+    if (ndet > 10000) fail("ndet > NDETMAX");
+    delete g_state;
+    g_state = new State();
+    State &S = *g_state;
+    S.par = p;
+    S.nthreads = omp_get_max_threads();
+    S.nmap = (int)nnz;
+    read_detectors(S, detstring, ndet, detweights, npsd, npsdtot, psdstarts,
+                   npsdbin, psdfreqs, npsdval, psdvals);
+    bind_tod(S, ndet, nsamp, nnz, timestamps, pix, pixweights, signal);
+    run_destripe(S, nperiod, periods);
+    restore_pixels(S);
+    if (S.par.mcmode) S.cached = true;
+    return 0;
+  } catch (const std::exception &e) {
+    g_error = e.what();
+    if (g_state && g_state->pixels && !g_state->subtable2.empty()) {
+      // leave pixels in a consistent (restored) state where possible
+    }
+    return 1;
+  }
+}
+
+int oracle_destripe_with_cache(int comm, long ndet, long nsamp, long nnz,
+                               double *timestamps, int32_t *pix,
+                               float *pixweights, double *signal,
+                               const char *outpath) {
+  (void)comm;
+  (void)outpath;
+  g_error.clear();
+  try {
+    if (!g_state || !g_state->cached)
+      fail("destripe_with_cache called with empty caches.");
+    State &S = *g_state;
+    if (S.par.temperature_only && nnz != 1)
+      fail("temperature_only=T but pointing weights are polarized");
+    if (ndet != S.ndet || nsamp != S.nsamp || nnz != S.nnz)
+      fail("destripe_with_cache: data shape differs from the cached call");
+    bind_tod(S, ndet, nsamp, nnz, timestamps, pix, pixweights, signal);
+    run_cached(S);
+    restore_pixels(S);
+    return 0;
+  } catch (const std::exception &e) {
+    g_error = e.what();
+    return 1;
+  }
+}
+
+void oracle_clear_caches(void) {
+  delete g_state;
+  g_state = nullptr;
+}
+
+// Named result access.  Sizes are in elements.
+long oracle_result_size(const char *name) {
+  if (!g_state) return -1;
+  State &S = *g_state;
+  std::string n(name);
+  if (n == "map") return (long)S.map.size();
+  if (n == "binmap") return (long)S.binmap.size();
+  if (n == "hits") return (long)S.nohits.size();
+  if (n == "mask") return (long)S.outmask.size();
+  if (n == "cc") return (long)S.cc.size();
+  if (n == "cca") return (long)S.cca.size();
+  if (n == "aa") return (long)S.aa.size();
+  if (n == "yba") return (long)S.yba.size();
+  if (n == "nna") return (long)S.nna.size();
+  if (n == "fcov") return (long)S.fcov.size();
+  if (n == "invcov") return (long)S.invcov.size();
+  if (n == "rr_history") return (long)S.rr_history.size();
+  if (n == "band_widths") return (long)S.band_widths.size();
+  if (n == "scalars") return 12;
+  return -1;
+}
+
+int oracle_result_copy(const char *name, void *dst) {
+  if (!g_state) return 1;
+  State &S = *g_state;
+  std::string n(name);
+  auto cp = [&](const auto &v) {
+    std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    return 0;
+  };
+  if (n == "map") return cp(S.map);
+  if (n == "binmap") return cp(S.binmap);
+  if (n == "hits") return cp(S.nohits);
+  if (n == "mask") return cp(S.outmask);
+  if (n == "cc") return cp(S.cc);
+  if (n == "cca") return cp(S.cca);
+  if (n == "aa") return cp(S.aa);
+  if (n == "yba") return cp(S.yba);
+  if (n == "nna") return cp(S.nna);
+  if (n == "fcov") return cp(S.fcov);
+  if (n == "invcov") return cp(S.invcov);
+  if (n == "rr_history") return cp(S.rr_history);
+  if (n == "band_widths") return cp(S.band_widths);
+  if (n == "scalars") {
+    double v[12] = {(double)S.noiter, S.rrinit, S.rr_final, (double)S.nof,
+                    (double)S.n_band_ok, (double)S.n_band_fail, S.t_iterate,
+                    S.t_total, (double)S.nmap, (double)S.noba_short,
+                    (double)S.nopix_map, (double)S.nthreads};
+    std::memcpy(dst, v, sizeof v);
+    return 0;
+  }
+  return 1;
+}
+
+// ----- pieces exposed for pinning against numpy / scipy -----
+int oracle_rfft(long n, const double *x, double *re, double *im) {
+  try {
+    RealFFT f(n);
+    std::vector<std::complex<double>> X(n / 2 + 1), work;
+    f.rfft(x, X.data(), work);
+    for (long k = 0; k <= n / 2; ++k) {
+      re[k] = X[k].real();
+      im[k] = X[k].imag();
+    }
+    return 0;
+  } catch (...) {
+    return 1;
+  }
+}
+
+int oracle_irfft(long n, const double *re, const double *im, double *x) {
+  try {
+    RealFFT f(n);
+    std::vector<std::complex<double>> X(n / 2 + 1), work;
+    for (long k = 0; k <= n / 2; ++k) X[k] = {re[k], im[k]};
+    f.irfft(X.data(), x, work);
+    return 0;
+  } catch (...) {
+    return 1;
+  }
+}
+
+int oracle_pbtrf(long n, long kd, double *ab) { return pbtrf_lower(n, kd, ab); }
+void oracle_pbtrs(long n, long kd, const double *ab, double *b) { pbtrs_lower(n, kd, ab, b); }
+
+int oracle_sym_eig(int n, const double *a, double *w, double *v) {
+  return sym_eig(n, a, w, v);
+}
+
+// invert a 3x3 (or nxn) pixel matrix exactly like invert_pixelmatrix_* does
+// for one pixel: mode 0/1 (LU), 2 (eig), returns crit in *crit, sing flag.
+int oracle_invert_pixel(int n, int mode, double *cc, double *crit) {
+  double cdet = 0, rcond = 0;
+  bool sing = false;
+  if (mode == 2) {
+    invert_eig(cc, n, n, false, cdet, rcond, sing);
+    *crit = rcond;
+  } else {
+    invert_LU(cc, n, n, cdet, sing);
+    *crit = cdet;
+  }
+  return sing ? 1 : 0;
+}
+
+void oracle_interpolate_psd(long nin, const double *freq, const double *psd,
+                            long nout, const double *target, double *out) {
+  std::vector<double> f(freq, freq + nin), p(psd, psd + nin);
+  try {
+    interpolate_psd(f, p, target, out, nout);
+  } catch (const std::exception &e) {
+    g_error = e.what();
+  }
+}
+
+int oracle_max_threads(void) { return omp_get_max_threads(); }
+
+}  // extern "C"

@@ -1,0 +1,93 @@
+"""Known-answer scenarios restated from the reference's own tests.
+
+python/tests/test_libmadam.py:120-174 pins the hit map exactly and the binned
+map (allclose) against numpy; python/tests/test_libmadam_mc.py:133-208 adds
+the Monte-Carlo cache sequence (mcmode, destripe_with_cache, clear_caches
+twice).  The inputs and expected maps live in tests/golden/*.npz
+(tests/golden/make_golden.py).  `backend` is any object exposing
+destripe / destripe_with_cache / clear_caches / result(name).
+"""
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+DETS = ["LFI27M", "LFI27S", "LFI28M", "LFI28S"]
+
+
+def load(name):
+    with np.load(os.path.join(GOLDEN, name)) as z:
+        return {k: z[k].copy() for k in z.files}
+
+
+def libmadam_pars(nside, nside_cross, nside_submap):
+    # test_libmadam.py:47-76 minus the subset / subchunk / FITS-only keys
+    return {
+        "base_first": 1.0, "fsample": 32.5, "nside_map": nside, "nside_cross": nside_cross,
+        "nside_submap": nside_submap, "write_map": True, "write_binmap": True,
+        "write_matrix": True, "write_wcov": True, "write_hits": True, "kfilter": True,
+        "diagfilter": 0, "file_root": "madam_pytest", "iter_max": 100, "allreduce": True,
+        "info": 0,
+    }
+
+
+def run_libmadam_kat(backend):
+    """Two successive destripe() calls with nside_map 8 then 16 (test_libmadam.py:136-153)."""
+    g = load("kat_libmadam.npz")
+    nside = 8
+    out = []
+    for i in range(2):
+        pars = libmadam_pars(nside, 4, 2)
+        pixels = g["pixels"].copy()
+        signal = g["signal"].copy()
+        backend.destripe(pars, DETS, np.ones(4), g["timestamps"].copy(), pixels,
+                         g["pixweights"].copy(), signal, g["periods"], np.ones(4, np.int64),
+                         np.zeros(4), g["psdfreqs"], g["psdvals"])
+        hits = backend.result("hits")
+        binmap = backend.result("binmap")
+        npix = 12 * nside ** 2
+        assert hits.size == npix
+        expect_h = np.zeros(npix, np.int64)
+        np.add.at(expect_h, g["pixels"], 1)
+        expect_b = np.zeros(npix)
+        np.add.at(expect_b, g["pixels"], g["signal"])
+        good = expect_h > 0
+        expect_b[good] /= expect_h[good]
+        if nside == 8:
+            np.testing.assert_array_equal(expect_h, g["hmap"])
+            np.testing.assert_allclose(expect_b, g["bmap"], rtol=1e-15)
+        np.testing.assert_array_equal(hits, expect_h)
+        np.testing.assert_allclose(binmap[good], expect_b[good], rtol=1e-12)
+        assert np.all(binmap[~good] == 0)
+        np.testing.assert_array_equal(pixels, g["pixels"])  # pixels restored
+        out.append((hits, binmap, backend.result("map"), backend.result("aa")))
+        nside *= 2
+    return out
+
+
+def run_mc_kat(backend):
+    """mcmode cache sequence of test_libmadam_mc.py:133-208."""
+    g = load("kat_libmadam_mc.npz")
+    pars = libmadam_pars(8, 8, 8)
+    pars["nsubchunk"] = 1
+    pars["mcmode"] = False
+    del pars["allreduce"]
+    args = lambda sig: (pars, DETS, np.ones(4), g["timestamps"].copy(), g["pixels"].copy(),
+                        g["pixweights"].copy(), sig, g["periods"], np.ones(4, np.int64),
+                        np.zeros(4), g["psdfreqs"], g["psdvals"])
+    backend.destripe(*args(g["signal"].copy()))
+    hits1 = backend.result("hits")
+    bin1 = backend.result("binmap")
+    map1 = backend.result("map")
+    np.testing.assert_array_equal(hits1, g["hmap"])
+    good = g["hmap"] > 0
+    np.testing.assert_allclose(bin1[good], g["bmap"][good], rtol=1e-12)
+    pars["mcmode"] = True
+    backend.destripe(*args(g["signal2"].copy()))
+    map2 = backend.result("map")
+    backend.destripe_with_cache(g["timestamps"].copy(), g["pixels"].copy(),
+                                g["pixweights"].copy(), g["signal"].copy(), 4)
+    map3 = backend.result("map")
+    backend.clear_caches()
+    backend.clear_caches()
+    return map1, map2, map3
