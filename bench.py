@@ -1,0 +1,323 @@
+"""Benchmark of the B200 destriping solve.
+
+Metric: TOD samples per second per PCG iteration (N_samples / t_iteration)
+on the "plain destripe on one B200" workload: nside 512, nside_submap 16,
+16 detectors x 4 observations x 2^23 samples at 100 Hz, IQU, 1/f noise
+(fknee 0.05 Hz, alpha -1.5), base_first 0.5 s, kfilter, cglimit 1e-12.
+Synthetic inputs of that shape are generated on the GPU with a fixed seed.
+
+  value      device-resident PCG iterations (bench_iterations through the
+             C-ABI), CUDA events on the library's stream, max over ranks
+  e2e        destripe() through the C-ABI with pinned HOST buffers: host->
+             device copies, setup, PCG to cglimit and the read-back of the map
+             inside the timed region; samples x iterations / wall time
+  roofline   dominant kernel of the iteration against measured HBM bandwidth
+  cpu_baseline  the CPU oracle (C++/OpenMP restatement of the reference;
+             the Fortran reference cannot be built here) on a bounded sample
+
+--impl reference times that CPU restatement alone (the reference arm).
+Multi-GPU: every rank solves its own replica (the north-star path does not
+shard); value is the sum over ranks divided by the slowest rank's time.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q,
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def config_for(name):
+    from libmadam_b200 import synthetic as syn
+    if name == "2":
+        return syn.config2(), "plain destripe nside512 16det x 4obs x 2^23 @100Hz IQU"
+    if name == "1":
+        return syn.config1(), "plain destripe nside64 4det x 2^20 @10Hz IQU"
+    cfg = syn.small_config(ndet=4, nsamp_obs=1 << 18, nobs=2, nside=64, seed=5)
+    return cfg, "small ring scan nside64 4det x 2 x 2^18"
+
+
+def cpu_sample_config(cfg):
+    """A bounded sample of the workload for the CPU restatement: the first
+    group of 4 detectors (0/45/90/135 deg) over the first observation."""
+    from libmadam_b200 import synthetic as syn
+    s = syn.ScanConfig(**{k: getattr(cfg, k) for k in cfg.__dataclass_fields__})
+    s.ndet = min(4, cfg.ndet)
+    s.nobs = 1
+    s.extra_pars = dict(cfg.extra_pars)
+    return s
+
+
+def run_cpu(cfg):
+    """Time the CPU restatement on the bounded sample: samples/s per PCG iteration."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_api as O
+    from libmadam_b200 import synthetic as syn
+    s = cpu_sample_config(cfg)
+    dev = "cuda" if _has_cuda() else "cpu"
+    d = syn.to_numpy(syn.generate(s, device=dev))
+    O.destripe(d["pars"], d["dets"], d["detweights"], d["timestamps"], d["pixels"],
+               d["pixweights"], d["signal"], d["periods"], d["npsd"], d["psdstarts"],
+               d["psdfreqs"], d["psdvals"])
+    sc = O.scalars()
+    n = s.ndet * s.nsamp
+    it = max(1, int(sc["noiter"]))
+    t_iter = sc["t_iterate"] / it
+    return {"value": n / t_iter, "unit": "samples/s per PCG iteration",
+            "cores": int(sc["nthreads"]), "kind": "port",
+            "sample": "{} detectors x {} samples of the workload ({} PCG iterations, "
+                      "{:.1f} ms/iteration, setup+solve {:.1f} s)".format(
+                          s.ndet, s.nsamp, it, 1e3 * t_iter, sc["t_total"]),
+            "iterations": it, "ms_per_iteration": 1e3 * t_iter}
+
+
+def _has_cuda():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def reduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    cfg, wname = config_for(args.config)
+    res = run_cpu(cfg)
+    line = {"impl": "reference", "metric": "TOD samples/s per PCG iteration",
+            "value": res["value"], "unit": "samples/s per PCG iteration", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res["ms_per_iteration"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wname, "sample": res["sample"]},
+            "cpu_baseline": {"value": res["value"], "unit": res["unit"], "cores": res["cores"],
+                             "kind": res["kind"], "sample": res["sample"]},
+            "e2e": {"value": res["value"], "unit": res["unit"], "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": "reference Fortran/MPI/FFTW build unavailable (no Fortran compiler, MPI, "
+                    "FFTW or LAPACK in the image); the C++/OpenMP restatement of its "
+                    "destripe path is timed instead"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="2", choices=["2", "1", "small"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        rc = reference_arm(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return rc
+
+    import torch
+    from libmadam_b200 import libmadam_wrapper as W
+    from libmadam_b200 import synthetic as syn
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    cfg, wname = config_for(args.config)
+    cfg.seed += 1000 * rank
+    t0 = time.time()
+    d = syn.generate(cfg, device="cuda")
+    torch.cuda.synchronize()
+    t_gen = time.time() - t0
+    n = cfg.ndet * cfg.nsamp
+    pix = d["pixels"].reshape(-1)
+    wts = d["pixweights"].reshape(-1)
+    sig = d["signal"].reshape(-1)
+    common = (d["pars"], d["dets"], d["detweights"])
+    psd = (d["periods"], d["npsd"], d["psdstarts"], d["psdfreqs"], d["psdvals"])
+
+    # full solve with inputs resident in HBM: time to cglimit
+    W.destripe(None, *common, d["timestamps"], pix, wts, sig, *psd)
+    tim = W.timings()
+    sca = W.scalars()
+    noiter = int(sca["noiter"])
+
+    # timed PCG iterations (the step)
+    barrier(world)
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    l0 = W.kernel_launches()
+    b = W.bench_iterations(args.warmup, args.steps)
+    launches = W.kernel_launches() - l0
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = clk.stop()
+    ms_iter = reduce_max(b["ms_per_iter"], world)
+    value = world * n / (ms_iter * 1e-3)
+
+    # end to end through the C-ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        h = {k: d[k].cpu().pin_memory() for k in ("timestamps", "pixels", "pixweights", "signal")}
+        hn = {k: v.numpy().reshape(-1) for k, v in h.items()}
+        barrier(world)
+        t1 = time.perf_counter()
+        W.destripe(None, *common, hn["timestamps"], hn["pixels"], hn["pixweights"], hn["signal"],
+                   *psd)
+        m = W.get_result("map")
+        t_e2e = time.perf_counter() - t1
+        t_e2e = reduce_max(t_e2e, world)
+        it_e2e = int(W.scalars()["noiter"])
+        h2d = sum(v.numel() * v.element_size() for v in h.values())
+        e2e = {"value": world * n * it_e2e / t_e2e, "unit": "samples/s per PCG iteration",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(m.nbytes),
+               "seconds": t_e2e, "iterations": it_e2e}
+        del h, hn
+
+    # roofline of the dominant kernel (algorithmic bytes per launch / duration)
+    hbm, peak_kind = peaks()
+    nb = cfg.ndet * int(sca["noba_short"])
+    npix_hit = int(sca["nloc"])
+    phases = {"scatter": b["scatter_ms"], "gather": b["gather_ms"], "filter": b["filter_ms"],
+              "precond": b["precond_ms"]}
+    algo = {"scatter": 16.0 * n + 8.0 * n / max(1, cfg.base_first * cfg.fsample),
+            "gather": 16.0 * n + 5 * 8.0 * nb + 24.0 * npix_hit,
+            "filter": None, "precond": None}
+    dom = max(("scatter", "gather"), key=lambda k: phases[k])
+    achieved = algo[dom] / (phases[dom] * 1e-3) / 1e9
+    b_iter = 32.0 * n + 8.0 * (16 + 20) * nb + (4 * 3 * 8 + 48) * npix_hit
+    roofline = {"bound": "hbm", "kernel": "k_" + dom, "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
+                "traffic": None,
+                "iteration": {"algorithmic_bytes": b_iter,
+                              "achieved_gbs": b_iter / (ms_iter * 1e-3) / 1e9,
+                              "frac": b_iter / (ms_iter * 1e-3) / 1e9 / hbm}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cpu = run_cpu(cfg)
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as e:  # the CPU leg never blocks the GPU line
+            cpu = {"value": None, "unit": "samples/s per PCG iteration", "cores": None,
+                   "kind": "port", "sample": "failed: {}".format(e)}
+
+    if rank == 0:
+        line = {
+            "metric": "TOD samples/s per PCG iteration", "value": value,
+            "unit": "samples/s per PCG iteration", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_iter, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": wname, "samples": n, "baselines": nb,
+                       "hit_pixels": npix_hit, "nside": cfg.nside,
+                       "l2": "inputs larger than L2 (pointing {:.1f} GB)".format(16e-9 * n),
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "e2e": e2e,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "time_to_cglimit_ms": tim["iterate_ms"], "iterations_to_cglimit": noiter,
+            "destripe_device_ms": tim["total_ms"], "setup_ms": tim["setup_ms"],
+            "phases_ms_per_iteration": phases, "generate_s": t_gen,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,65 @@
+/* Extensions of the B200 destriping library (libmadam_b200/libmadam.so).
+ *
+ * The reference has no status codes (errors call abort_mpi,
+ * src/mpi_wrappers.f90:120-137) and returns its products only as FITS files
+ * (src/output.f90).  These entry points return a status (0 = success) and
+ * give the products of the last call as arrays.
+ */
+#ifndef MADAM_B200_H
+#define MADAM_B200_H
+
+#include "madam.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* destripe() with a status (reference src/smadam.F90:64-590). */
+int madam_b200_destripe(int comm, char *parstring, long ndet, char *detstring,
+                        double *detweights, long nsamp, long nnz, void *timestamps, void *pix,
+                        void *pixweights, void *signal, long nperiod, long *periods, long *npsd,
+                        long npsdtot, double *psdstarts, long npsdbin, double *psdfreqs,
+                        long npsdval, double *psdvals);
+
+/* destripe_with_cache() with a status (reference src/smadam.F90:593-918). */
+int madam_b200_destripe_with_cache(int comm, long ndet, long nsamp, long nnz, void *timestamps,
+                                   void *pix, void *pixweights, void *signal, char *outpath);
+
+/* clear_caches() with a status (reference src/smadam.F90:921-951). */
+int madam_b200_clear_caches(void);
+
+/* Status of the last call (0 = success) and its error message; replaces the
+ * reference's abort_mpi messages (src/mpi_wrappers.f90:120-137). */
+int madam_b200_last_error(char *buf, long buflen);
+
+/* Products of the last call, in place of the FITS writers of
+ * src/output.f90:114-1180.  Names: "map", "binmap" (float64 [npix][nmap],
+ * full sky, NESTED, nside_map), "hits", "mask" (int32 [npix]), "crit"
+ * (float32 [npix]), "cc", "cca" (float64 [npix][nmap][nmap], inverse pixel
+ * matrices at nside_map / nside_cross), "aa", "yba", "nna" (float64
+ * [ndet][noba]: baselines, RHS, F^T N^-1 F), "fcov" (float64
+ * [npsdtot][nof/2+1]), "invcov" (float64 [npsdtot][nof]), "rr_history"
+ * (float64 [niter]), "band_widths" (int64), "scalars" (float64 [16]),
+ * "timings" (float64 [9], milliseconds).  result_size returns elements or
+ * -1; result_copy fails when nbytes is too small. */
+long madam_b200_result_size(const char *name);
+int madam_b200_result_copy(const char *name, void *dst, long nbytes);
+
+/* Times `iters` PCG iterations (after `warmup`) restarted from the RHS of the
+ * last solve, inputs resident in HBM; out[0..7] = total ms, ms per
+ * iteration, kernel launches per iteration, scatter / filter / gather /
+ * preconditioner / update ms per iteration.  No reference counterpart. */
+int madam_b200_bench_iterations(int warmup, int iters, double *out, long nout);
+
+/* Number of kernels the library has launched.  No reference counterpart. */
+unsigned long long madam_b200_kernel_launches(void);
+
+/* Host check of the integer division used in the kernels (0 = pass).  No
+ * reference counterpart. */
+int madam_b200_selftest_fastdiv(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,186 @@
+// C-ABI of libmadam.so.
+//
+// destripe, destripe_with_cache and clear_caches keep the reference's exact
+// signatures (madam.h:1-2; smadam.F90:64-101, 593-609, 921), so a program
+// or the ctypes wrapper that loads the reference library can load this one.
+// Like the reference, the library keeps module state between calls
+// (the Monte-Carlo caches) and is not reentrant: calls are serialised.
+// Where the reference calls abort_mpi the replacement returns instead; the
+// void entry points print the message on stderr and record it, the
+// madam_b200_* entry points return a status and madam_b200_last_error
+// gives the message.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+
+#include "engine.h"
+#include "params.h"
+
+using madam::Engine;
+
+namespace {
+
+std::mutex g_mutex;
+std::unique_ptr<Engine> g_engine;
+std::string g_last_error;
+int g_last_status = 0;
+
+bool is_device_pointer(const void *p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+template <typename F>
+int guarded(F &&f) {
+  try {
+    f();
+    g_last_status = 0;
+    g_last_error.clear();
+  } catch (const std::exception &e) {
+    g_last_status = 1;
+    g_last_error = e.what();
+  }
+  return g_last_status;
+}
+
+Engine &engine() {
+  if (!g_engine) g_engine.reset(new Engine());
+  return *g_engine;
+}
+
+void report(const char *who) {
+  if (g_last_status != 0) std::fprintf(stderr, "%s: ERROR: %s\n", who, g_last_error.c_str());
+}
+
+}  // namespace
+
+extern "C" {
+
+int madam_b200_destripe(int comm, char *parstring, long ndet, char *detstring,
+                        double *detweights, long nsamp, long nnz, void *timestamps, void *pix,
+                        void *pixweights, void *signal, long nperiod, long *periods, long *npsd,
+                        long npsdtot, double *psdstarts, long npsdbin, double *psdfreqs,
+                        long npsdval, double *psdvals) {
+  (void)comm;  // single rank: the communicator handle is accepted and ignored
+  std::lock_guard<std::mutex> lock(g_mutex);
+  return guarded([&] {
+    madam::Params par = madam::parse_parstring(parstring);
+    if (par.mcmode && g_engine && g_engine->cached())
+      madam::fail("Destripe called while caches are not empty.");
+    if (par.mcmode && par.nsubchunk > 1) madam::fail("MCMode is not compatible with nsubchunk > 1.");
+    if (par.temperature_only && nnz != 1)
+      madam::fail("temperature_only=T but pointing weights are polarized");
+    if (ndet > 10000) madam::fail("ndet > NDETMAX");
+    if (ndet <= 0 || nsamp <= 0 || nnz <= 0) madam::fail("empty data");
+    auto dets = madam::read_detectors(par, detstring, ndet, detweights, npsd, npsdtot, psdstarts,
+                                      npsdbin, psdfreqs, npsdval, psdvals);
+    const bool dev = is_device_pointer(pix);
+    engine().run(par, std::move(dets), ndet, nsamp, nnz, (double *)timestamps, (int32_t *)pix,
+                 (float *)pixweights, (double *)signal, nperiod, periods, dev);
+  });
+}
+
+int madam_b200_destripe_with_cache(int comm, long ndet, long nsamp, long nnz, void *timestamps,
+                                   void *pix, void *pixweights, void *signal, char *outpath) {
+  (void)comm;
+  (void)outpath;  // output files are not written by this library
+  std::lock_guard<std::mutex> lock(g_mutex);
+  return guarded([&] {
+    if (!g_engine || !g_engine->cached())
+      madam::fail("destripe_with_cache called with empty caches.");
+    const bool dev = is_device_pointer(pix);
+    g_engine->run_cached(ndet, nsamp, nnz, (double *)timestamps, (int32_t *)pix,
+                         (float *)pixweights, (double *)signal, dev);
+  });
+}
+
+int madam_b200_clear_caches(void) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  return guarded([&] { g_engine.reset(); });
+}
+
+void destripe(int comm, char *parstring, long ndet, char *detstring, double *detweights,
+              long nsamp, long nnz, void *timestamps, void *pix, void *pixweights, void *signal,
+              long nperiod, long *periods, long *npsd, long npsdtot, double *psdstarts,
+              long npsdbin, double *psdfreqs, long npsdval, double *psdvals) {
+  madam_b200_destripe(comm, parstring, ndet, detstring, detweights, nsamp, nnz, timestamps, pix,
+                      pixweights, signal, nperiod, periods, npsd, npsdtot, psdstarts, npsdbin,
+                      psdfreqs, npsdval, psdvals);
+  report("destripe");
+}
+
+void destripe_with_cache(int comm, long ndet, long nsamp, long nnz, void *timestamps, void *pix,
+                         void *pixweights, void *signal, char *outpath) {
+  madam_b200_destripe_with_cache(comm, ndet, nsamp, nnz, timestamps, pix, pixweights, signal,
+                                 outpath);
+  report("destripe_with_cache");
+}
+
+void clear_caches(void) {
+  madam_b200_clear_caches();
+}
+
+int madam_b200_last_error(char *buf, long buflen) {
+  if (buf && buflen > 0) {
+    std::strncpy(buf, g_last_error.c_str(), (size_t)buflen - 1);
+    buf[buflen - 1] = '\0';
+  }
+  return g_last_status;
+}
+
+long madam_b200_result_size(const char *name) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  if (!g_engine || !name) return -1;
+  long n = -1;
+  guarded([&] { n = g_engine->result_size(name); });
+  return n;
+}
+
+int madam_b200_result_copy(const char *name, void *dst, long nbytes) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  return guarded([&] {
+    if (!g_engine) madam::fail("no results: destripe has not run");
+    g_engine->result_copy(name, dst, nbytes);
+  });
+}
+
+int madam_b200_bench_iterations(int warmup, int iters, double *out, long nout) {
+  std::lock_guard<std::mutex> lock(g_mutex);
+  return guarded([&] {
+    if (!g_engine) madam::fail("no solve state: destripe has not run");
+    std::vector<double> v;
+    g_engine->bench_iterations(warmup, iters, v);
+    for (long i = 0; i < nout && i < (long)v.size(); ++i) out[i] = v[i];
+  });
+}
+
+unsigned long long madam_b200_kernel_launches(void) { return madam::g_kernel_launches; }
+
+// Host-side check of the invariant-divisor division used by the kernels.
+int madam_b200_selftest_fastdiv(void) {
+  const uint32_t divs[] = {1, 2, 3, 5, 7, 10, 49, 50, 51, 100, 1000, 65535, 65536, 1u << 20,
+                           123456789u, 2147483647u, 4294967295u};
+  const uint32_t nums[] = {0, 1, 2, 3, 49, 50, 99, 100, 101, 65535, 65536, 1u << 24, 2147483647u,
+                           2147483648u, 4000000000u, 4294967295u};
+  for (uint32_t d : divs) {
+    madam::FastDiv f(d);
+    for (uint32_t n : nums)
+      if (f.div(n) != n / d) return 1;
+    for (uint32_t k = 0; k < 100000; ++k) {
+      const uint32_t n = k * 2654435761u;
+      if (f.div(n) != n / d) return 1;
+    }
+  }
+  return 0;
+}
+
+}  // extern "C"

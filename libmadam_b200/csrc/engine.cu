@@ -1,0 +1,836 @@
+// Destriping engine: setup, PCG iteration and finalisation on sm_100a.
+//
+// Data layout in HBM
+//   pointing  float4 {w_I, w_Q, w_U, compacted pixel} per sample, [det][sample]
+//             (int32 compacted pixel only, for temperature-only data)
+//   signal    float64 [det][sample]
+//   maps      compacted pixel space (hit submaps only), pixel-major
+//             (cc / cca: 6 doubles = symmetric 3x3; maps: 3 doubles)
+//   baselines float64 [det][baseline] (the reference's aa(0, k, idet) order)
+// Scatter passes (map <- samples) run over "runs": maximal stretches of one
+// detector's samples inside one tile of <= 1024 compacted pixels.  Runs are
+// bucketed by tile, each CTA accumulates a tile in shared memory and flushes
+// it with one global atomic per touched pixel value.  Gather passes
+// (baselines <- samples) use one warp per baseline in time order.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <omp.h>
+
+#include "engine.h"
+#include "fft.cuh"
+#include "kernels.cuh"
+#include "pixmat.cuh"
+#include "band2.cuh"
+#include "precond.cuh"
+
+namespace madam {
+
+unsigned long long g_kernel_launches = 0;
+
+namespace {
+
+constexpr int kTileMax = 1024;        // pixels per scatter tile (fine res)
+constexpr uint32_t kRunMax = 1024;    // samples per run
+constexpr long long kItemSamples = 1 << 16;  // samples per scatter work item
+constexpr int kRedBlocks = 1184;      // 148 SMs x 8, fixed for determinism
+
+enum Scal { S_RZ = 0, S_RR, S_PAP, S_RZ2, S_RZO, S_ALPHA, S_BETA, S_NSCAL = 16 };
+
+__device__ __forceinline__ int find_iv(const long long *istart, int niv, long long s) {
+  int lo = 0, hi = niv - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (istart[mid] <= s) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// global baseline index (det * noba_short + k) of sample s of detector det
+__device__ __forceinline__ long long baseline_of(const SampleMap &m, long long det,
+                                                 long long s) {
+  const int iv = find_iv(m.istart, m.ninterval, s);
+  return det * m.noba_short + m.kstart[iv] + m.fdn.div((uint32_t)(s - m.istart[iv]));
+}
+
+template <int NNZ>
+__device__ __forceinline__ int sample_pix(const float4 *p4, const int32_t *pc, long long i) {
+  if (NNZ == 3) return point_pix(p4[i]);
+  return pc[i];
+}
+
+// ---------------------------------------------------------------- setup --
+__global__ void k_minmax(const int32_t *pix, long long n, int *out) {
+  int mn = INT_MAX, mx = INT_MIN;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int v = pix[i];
+    mn = min(mn, v);
+    mx = max(mx, v);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(out, mn);
+    atomicMax(out + 1, mx);
+  }
+}
+
+// check_files: samples whose weights are all zero get pixel -1
+// (read_data.f90:243-252)
+__global__ void k_flag_zero_weight(int32_t *pix, const float *w, int nnz, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    bool allz = true;
+    for (int j = 0; j < nnz; ++j)
+      if (w[i * nnz + j] != 0.0f) allz = false;
+    if (allz && !(pix[i] < 0)) pix[i] = -1;
+  }
+}
+
+__global__ void k_count_good(const int32_t *pix, long long n, SampleMap sm, int niv,
+                             unsigned long long *counts) {
+  for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < n;
+       i0 += (long long)gridDim.x * blockDim.x) {
+    const long long i = i0 + threadIdx.x;
+    int key = -1;
+    bool good = false;
+    if (i < n) {
+      const long long det = i / sm.nsamp, s = i - det * sm.nsamp;
+      key = (int)(det * niv + find_iv(sm.istart, sm.ninterval, s));
+      good = pix[i] >= 0;
+    }
+    const unsigned grp = __match_any_sync(0xffffffffu, key);
+    const unsigned ball = __ballot_sync(0xffffffffu, good);
+    const int lane = threadIdx.x & 31;
+    if (key >= 0 && lane == __ffs(grp) - 1) {
+      const unsigned c = __popc(grp & ball);
+      if (c) atomicAdd(counts + key, (unsigned long long)c);
+    }
+  }
+}
+
+// check_files: periods with less than 0.1 % good samples are flagged
+// (read_data.f90:255-272)
+__global__ void k_flag_sparse(int32_t *pix, long long n, SampleMap sm, int niv,
+                              const unsigned long long *counts, const long long *ivlen) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long det = i / sm.nsamp, s = i - det * sm.nsamp;
+    const int iv = find_iv(sm.istart, sm.ninterval, s);
+    const unsigned long long c = counts[det * niv + iv];
+    if (c == 0) continue;
+    if ((double)c / (double)ivlen[iv] < fsp(1e-3f)) pix[i] = -1;
+  }
+}
+
+// where (pixels < 0) pixels = dummy_pixel; hit-submap flags (pointing.f90:125-131)
+__global__ void k_dummy_ksub(int32_t *pix, long long n, int dummy, int nosubpix, int *ksub) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    int v = pix[i];
+    if (v < 0) {
+      v = dummy;
+      pix[i] = v;
+    }
+    const int sm = v / nosubpix;
+    if (ksub[sm] == 0) ksub[sm] = 1;
+  }
+}
+
+// reduce_pixels compaction (pointing.f90:150-156) and packing of the pointing
+template <int NNZ>
+__global__ void k_compact(int32_t *pix, const float *w, long long n, const int *sub1,
+                          int nosubpix, float4 *p4, int32_t *pc) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int v = pix[i];
+    const int c = v - sub1[v / nosubpix] * nosubpix;
+    pix[i] = c;
+    if (NNZ == 3) {
+      p4[i] = make_float4(w[3 * i], w[3 * i + 1], w[3 * i + 2], __int_as_float(c));
+    } else {
+      pc[i] = c;
+    }
+  }
+}
+
+// per-baseline detector weight, 0 for (det, period) pairs the reference skips
+__global__ void k_baseline_weights(double *bw, long long nb, long noba, const int *kstart,
+                                   int niv, const double *detw_iv) {
+  for (long long b = blockIdx.x * (long long)blockDim.x + threadIdx.x; b < nb;
+       b += (long long)gridDim.x * blockDim.x) {
+    const long long det = b / noba, k = b - det * noba;
+    int lo = 0, hi = niv - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (kstart[mid] <= k) lo = mid;
+      else hi = mid - 1;
+    }
+    bw[b] = detw_iv[det * niv + lo];
+  }
+}
+
+// flag_bad_baselines (read_data.f90:30-74): one warp per baseline
+template <int NNZ>
+__global__ void k_bad_baselines(int32_t *pix, float4 *p4, int32_t *pc, long long nb,
+                                long noba, long long nsamp, const uint32_t *bstart,
+                                int dummy_global, double frac) {
+  const long long b = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (b >= nb) return;
+  const long long det = b / noba, k = b - det * noba;
+  const long long s0 = bstart[k], s1 = bstart[k + 1];
+  int ngood = 0;
+  for (long long s = s0 + lane; s < s1; s += 32)
+    if (pix[det * nsamp + s] != dummy_global) ++ngood;
+  ngood = warp_sum(ngood);
+  const long long len = s1 - s0;
+  if (ngood > 0 && ngood < frac * len) {
+    for (long long s = s0 + lane; s < s1; s += 32) {
+      const long long i = det * nsamp + s;
+      pix[i] = dummy_global;
+      if (NNZ == 3) p4[i].w = __int_as_float(dummy_global);
+      else pc[i] = dummy_global;
+    }
+  }
+}
+
+// run boundaries: a sample is inside a run if its pixel is a real compacted
+// pixel and its (det, period) is not skipped
+template <int NNZ>
+__global__ void k_run_flags(const float4 *p4, const int32_t *pc, long long n, SampleMap sm,
+                            const double *bw, int nloc, int tile_shift, uint8_t *sflag,
+                            uint8_t *eflag) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long det = i / sm.nsamp, s = i - det * sm.nsamp;
+    const int iv = find_iv(sm.istart, sm.ninterval, s);
+    const int px = sample_pix<NNZ>(p4, pc, i);
+    const bool valid = px < nloc && bw[det * sm.noba_short + sm.kstart[iv]] != 0.0;
+    uint8_t st = 0, en = 0;
+    if (valid) {
+      const int tile = px >> tile_shift;
+      // previous sample
+      if (s == 0 || s == sm.istart[iv]) {
+        st = 1;
+      } else {
+        const int pp = sample_pix<NNZ>(p4, pc, i - 1);
+        st = !(pp < nloc && (pp >> tile_shift) == tile);
+      }
+      const long long ivend = sm.istart[iv + 1];
+      if (s + 1 == sm.nsamp || s + 1 == ivend) {
+        en = 1;
+      } else {
+        const int pn = sample_pix<NNZ>(p4, pc, i + 1);
+        en = !(pn < nloc && (pn >> tile_shift) == tile);
+      }
+    }
+    sflag[i] = st;
+    eflag[i] = en;
+  }
+}
+
+__global__ void k_run_pieces(const long long *starts, const long long *ends, long long nr,
+                             long long *pieces) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < nr;
+       r += (long long)gridDim.x * blockDim.x) {
+    const long long len = ends[r] - starts[r] + 1;
+    pieces[r] = (len + kRunMax - 1) / kRunMax;
+  }
+}
+
+template <int NNZ>
+__global__ void k_run_emit(const long long *starts, const long long *ends,
+                           const long long *piece_off, long long nr, SampleMap sm,
+                           const float4 *p4, const int32_t *pc, int tile_shift, Run *runs,
+                           int *keys, int *lens) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < nr;
+       r += (long long)gridDim.x * blockDim.x) {
+    const long long a = starts[r], e = ends[r];
+    long long o = piece_off[r];
+    for (long long s0 = a; s0 <= e; s0 += kRunMax, ++o) {
+      const uint32_t len = (uint32_t)min((long long)kRunMax, e - s0 + 1);
+      const long long det = s0 / sm.nsamp, s = s0 - det * sm.nsamp;
+      const int iv = find_iv(sm.istart, sm.ninterval, s);
+      Run R;
+      R.s_lo = (uint32_t)(s0 & 0xffffffffu);
+      R.hi_len = ((uint32_t)(s0 >> 32) << 24) | len;
+      R.kbase = (int32_t)(det * sm.noba_short + sm.kstart[iv]);
+      R.offiv = (uint32_t)(s - sm.istart[iv]);
+      runs[o] = R;
+      keys[o] = sample_pix<NNZ>(p4, pc, s0) >> tile_shift;
+      lens[o] = (int)len;
+    }
+  }
+}
+
+__global__ void k_gather_runs(const int *perm, const Run *in, const int *lens_in, long long n,
+                              Run *out, int *lens_out) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+       r += (long long)gridDim.x * blockDim.x) {
+    out[r] = in[perm[r]];
+    lens_out[r] = lens_in[perm[r]];
+  }
+}
+
+__global__ void k_item_flags(const int *keys, const long long *pref, long long n, uint8_t *f) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < n;
+       r += (long long)gridDim.x * blockDim.x) {
+    f[r] = (r == 0 || keys[r] != keys[r - 1] ||
+            pref[r] / kItemSamples != pref[r - 1] / kItemSamples);
+  }
+}
+
+__global__ void k_item_tiles(const long long *begins, long long nitem, const int *keys,
+                             int *item_begin, int *item_tile) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nitem;
+       t += (long long)gridDim.x * blockDim.x) {
+    item_begin[t] = (int)begins[t];
+    item_tile[t] = keys[begins[t]];
+  }
+}
+
+// pixel_matrix + count_hits + bin_tod (smadam_routines.f90:111-422), fused,
+// shared-memory privatised per tile, at the map (fine) resolution
+template <int NMAP>
+__global__ void k_setup_scatter(const int *item_begin, const int *item_tile, const Run *runs,
+                                const float4 *p4, const int32_t *pc, const double *tod,
+                                const double *bw, FastDiv fdn, int tile_shift, double *cc,
+                                double *bin, int *hits) {
+  constexpr int NCC = NMAP == 3 ? 6 : 1;
+  extern __shared__ double sm[];
+  const int T = 1 << tile_shift;
+  double *scc = sm;
+  double *sbin = sm + NCC * T;
+  int *shits = (int *)(sbin + NMAP * T);
+  for (int e = threadIdx.x; e < NCC * T; e += blockDim.x) scc[e] = 0;
+  for (int e = threadIdx.x; e < NMAP * T; e += blockDim.x) sbin[e] = 0;
+  for (int e = threadIdx.x; e < T; e += blockDim.x) shits[e] = 0;
+  __syncthreads();
+  const int it = blockIdx.x;
+  const int rb = item_begin[it], re = item_begin[it + 1];
+  const int tile = item_tile[it];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int r = rb + wid; r < re; r += nw) {
+    const Run R = runs[r];
+    const uint64_t s0 = run_start(R);
+    const uint32_t len = run_len(R);
+    const double detw = bw[R.kbase];
+    const double sqw = sqrt(detw);
+    for (uint32_t u = lane; u < len; u += 32) {
+      const uint64_t i = s0 + u;
+      const double t = tod[i];
+      if (NMAP == 3) {
+        const float4 q = p4[i];
+        const int loc = point_pix(q) & (T - 1);
+        const double w0 = (double)q.x * sqw, w1 = (double)q.y * sqw, w2 = (double)q.z * sqw;
+        double *c = scc + 6 * loc;
+        atomicAdd(c + 0, w0 * w0);
+        atomicAdd(c + 1, w0 * w1);
+        atomicAdd(c + 2, w0 * w2);
+        atomicAdd(c + 3, w1 * w1);
+        atomicAdd(c + 4, w1 * w2);
+        atomicAdd(c + 5, w2 * w2);
+        double *bm = sbin + 3 * loc;
+        atomicAdd(bm + 0, (double)q.x * t * detw);
+        atomicAdd(bm + 1, (double)q.y * t * detw);
+        atomicAdd(bm + 2, (double)q.z * t * detw);
+        atomicAdd(shits + loc, 1);
+      } else {
+        const int loc = pc[i] & (T - 1);
+        atomicAdd(scc + loc, detw);
+        atomicAdd(sbin + loc, t * detw);
+        atomicAdd(shits + loc, 1);
+      }
+    }
+  }
+  __syncthreads();
+  const long long base = (long long)tile * T;
+  for (int p = threadIdx.x; p < T; p += blockDim.x) {
+    if (shits[p] == 0) continue;
+    atomicAdd(hits + base + p, shits[p]);
+    for (int j = 0; j < NCC; ++j) atomicAdd(cc + (base + p) * NCC + j, scc[NCC * p + j]);
+    for (int j = 0; j < NMAP; ++j) atomicAdd(bin + (base + p) * NMAP + j, sbin[NMAP * p + j]);
+  }
+}
+
+// collect to the cross resolution: sum groups of ndeg consecutive pixels
+__global__ void k_degrade(const double *fine, double *coarse, long long ncoarse, int nv,
+                          int ndeg) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ncoarse * nv;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long p = e / nv;
+    const int j = (int)(e - p * nv);
+    double s = 0;
+    for (int d = 0; d < ndeg; ++d) s += fine[(p * ndeg + d) * nv + j];
+    coarse[e] = s;
+  }
+}
+
+template <int NMAP>
+__global__ void k_invert_cross(double *cc, long long n, MatrixRules mr) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x) {
+    if (NMAP == 1) {
+      const double c = cc[p];
+      cc[p] = (c != 0) ? 1.0 / c : 0.0;
+    } else {
+      double s6[6];
+      for (int j = 0; j < 6; ++j) s6[j] = cc[p * 6 + j];
+      invert_cross_pixel(s6, mr.pixmode, mr.pixlim, mr.allow_decoupling, mr.incomplete);
+      for (int j = 0; j < 6; ++j) cc[p * 6 + j] = s6[j];
+    }
+  }
+}
+
+template <int NMAP>
+__global__ void k_invert_map(double *cc, long long n, MatrixRules mr, int *mask, float *crit) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x) {
+    if (NMAP == 1) {
+      const double c = cc[p];
+      if (c != 0) {
+        cc[p] = 1.0 / c;
+        mask[p] = 1;
+      } else {
+        cc[p] = 0;
+        mask[p] = 0;
+      }
+    } else {
+      double s6[6];
+      for (int j = 0; j < 6; ++j) s6[j] = cc[p * 6 + j];
+      float cr = 0.0f;
+      mask[p] = invert_map_pixel(s6, mr.pixmode, mr.pixlim, mr.allow_decoupling, mr.incomplete,
+                                 cr);
+      crit[p] = cr;
+      for (int j = 0; j < 6; ++j) cc[p * 6 + j] = s6[j];
+    }
+  }
+}
+
+// ccmultiply (map_routines.f90:24-77)
+template <int NMAP>
+__global__ void k_ccmult(const double *cc, double *m, long long n) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x) {
+    if (NMAP == 1) {
+      const double c = cc[p];
+      m[p] = (c == 0) ? 0.0 : c * m[p];
+    } else {
+      const double *c = cc + p * 6;
+      double *v = m + p * 3;
+      if (c[0] == 0) {
+        v[0] = v[1] = v[2] = 0;
+      } else {
+        const double a = v[0], b = v[1], d = v[2];
+        const double tm = c[0] * a + c[1] * b + c[2] * d;
+        const double qm = c[1] * a + c[3] * b + c[4] * d;
+        const double um = c[2] * a + c[4] * b + c[5] * d;
+        v[0] = tm;
+        v[1] = qm;
+        v[2] = um;
+      }
+    }
+  }
+}
+
+// initialize_a (smadam_routines.f90:508-653): one warp per baseline
+template <int NMAP>
+__global__ void k_init_a(const float4 *p4, const int32_t *pc, const double *tod,
+                         const uint32_t *bstart, long long nb, long noba, long long nsamp,
+                         const double *bw, const double *wamap, int deg_shift, int nloc,
+                         double *yba, double *nna) {
+  const long long b = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (b >= nb) return;
+  const double detw = bw[b];
+  if (detw == 0) return;
+  const long long det = b / noba, k = b - det * noba;
+  const long long i0 = det * nsamp + bstart[k], i1 = det * nsamp + bstart[k + 1];
+  double y = 0, cnt = 0;
+  for (long long i = i0 + lane; i < i1; i += 32) {
+    int px;
+    float4 q;
+    if (NMAP == 3) {
+      q = p4[i];
+      px = point_pix(q);
+    } else {
+      px = pc[i];
+    }
+    if (px >= nloc) continue;
+    const long long pcr = px >> deg_shift;
+    if (NMAP == 3) {
+      const double m0 = wamap[pcr * 3], m1 = wamap[pcr * 3 + 1], m2 = wamap[pcr * 3 + 2];
+      if (m0 == 0 && m1 == 0 && m2 == 0) continue;
+      y += tod[i] - (m0 * (double)q.x + m1 * (double)q.y + m2 * (double)q.z);
+    } else {
+      const double m0 = wamap[pcr];
+      if (m0 == 0) continue;
+      y += tod[i] - m0;
+    }
+    cnt += 1.0;
+  }
+  y = warp_sum(y);
+  cnt = warp_sum(cnt);
+  if (lane == 0) {
+    double n = cnt * detw, yy = y * detw;
+    if (fabs(n) < fsp(1e-30f)) {
+      n = 0;
+      yy = 0;
+    }
+    yba[b] = yy;
+    nna[b] = n;
+  }
+}
+
+// baseline_to_map (smadam_routines.f90:1074-1111) / subtract_baselines_a
+// (1489-1539): target[pix] += w * pw[k], privatised per tile
+template <int NMAP>
+__global__ void k_scatter(const int *item_begin, const int *item_tile, const Run *runs,
+                          const float4 *p4, const int32_t *pc, const double *pw, FastDiv fdn,
+                          int tile_shift, int deg_shift, int tilec, double *target) {
+  extern __shared__ double sacc[];
+  for (int e = threadIdx.x; e < tilec * NMAP; e += blockDim.x) sacc[e] = 0;
+  __syncthreads();
+  const int it = blockIdx.x;
+  const int rb = item_begin[it], re = item_begin[it + 1];
+  const long long base_c = ((long long)item_tile[it] << tile_shift) >> deg_shift;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int r = rb + wid; r < re; r += nw) {
+    const Run R = runs[r];
+    const uint64_t s0 = run_start(R);
+    const uint32_t len = run_len(R);
+    for (uint32_t u = lane; u < len; u += 32) {
+      const uint64_t i = s0 + u;
+      const double v = pw[R.kbase + fdn.div(R.offiv + u)];
+      if (NMAP == 3) {
+        const float4 q = p4[i];
+        const int loc = (int)((point_pix(q) >> deg_shift) - base_c);
+        atomicAdd(sacc + 3 * loc + 0, (double)q.x * v);
+        atomicAdd(sacc + 3 * loc + 1, (double)q.y * v);
+        atomicAdd(sacc + 3 * loc + 2, (double)q.z * v);
+      } else {
+        const int loc = (int)((pc[i] >> deg_shift) - base_c);
+        atomicAdd(sacc + loc, v);
+      }
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < tilec * NMAP; e += blockDim.x) {
+    const double v = sacc[e];
+    if (v != 0) atomicAdd(target + base_c * NMAP + e, v);
+  }
+}
+
+// map_to_baseline (smadam_routines.f90:1282-1329) + "ap = ap + ..." (870)
+// and the partial p.ap of the PCG (877): one warp per baseline
+template <int NMAP>
+__global__ void k_gather(const float4 *p4, const int32_t *pc, const uint32_t *bstart,
+                         long long nb, long noba, long long nsamp, const double *bw,
+                         const double *p, const double *nna, const double *m, int deg_shift,
+                         int nloc, const uint8_t *rmask, double *ap, double *part) {
+  const int lane = threadIdx.x & 31;
+  const long long warp0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  double pap = 0;
+  for (long long b = warp0; b < nb; b += nwarps) {
+    const double detw = bw[b];
+    if (detw != 0) {
+      const long long det = b / noba, k = b - det * noba;
+      const long long i0 = det * nsamp + bstart[k], i1 = det * nsamp + bstart[k + 1];
+      double apn = 0;
+      for (long long i = i0 + lane; i < i1; i += 32) {
+        if (NMAP == 3) {
+          const float4 q = p4[i];
+          const int px = point_pix(q);
+          if (px >= nloc) continue;
+          const double *mm = m + (long long)(px >> deg_shift) * 3;
+          apn += (double)q.x * mm[0] + (double)q.y * mm[1] + (double)q.z * mm[2];
+        } else {
+          const int px = pc[i];
+          if (px >= nloc) continue;
+          apn += m[px >> deg_shift];
+        }
+      }
+      apn = warp_sum(apn);
+      if (lane == 0) {
+        const double v = ap[b] + (nna[b] * p[b] - apn * detw);
+        ap[b] = v;
+        if (rmask[b]) pap += p[b] * v;
+      }
+    } else if (lane == 0 && rmask[b]) {
+      pap += p[b] * ap[b];
+    }
+  }
+  double v[1] = {pap};
+  block_sum<1>(v);
+  if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+
+// masked dot products sum_i mask_i a_i b_i for up to 3 pairs
+__global__ void k_dots(const double *a0, const double *b0, const double *a1, const double *b1,
+                       const double *a2, const double *b2, int nd, const uint8_t *mask,
+                       long long n, double *part) {
+  double v[3] = {0, 0, 0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (!mask[i]) continue;
+    v[0] += a0[i] * b0[i];
+    if (nd > 1) v[1] += a1[i] * b1[i];
+    if (nd > 2) v[2] += a2[i] * b2[i];
+  }
+  block_sum<3>(v);
+  if (threadIdx.x == 0)
+    for (int j = 0; j < 3; ++j) part[j * gridDim.x + blockIdx.x] = v[j];
+}
+
+// deterministic final sums; mode 0: scal[slots] = sums
+// mode 1 (pap): scal[S_PAP] = s0, scal[S_ALPHA] = rz / pap
+// mode 2 (rz, rz2, rr): rzo = rz, then beta = (rz - rz2) / rzo
+__global__ void k_finish(const double *part, int nblk, int nd, double *scal, int mode,
+                         int slot0) {
+  double v[3] = {0, 0, 0};
+  for (int j = 0; j < nd; ++j)
+    for (int i = threadIdx.x; i < nblk; i += blockDim.x) v[j] += part[j * nblk + i];
+  block_sum<3>(v);
+  if (threadIdx.x != 0) return;
+  if (mode == 0) {
+    for (int j = 0; j < nd; ++j) scal[slot0 + j] = v[j];
+  } else if (mode == 1) {
+    scal[S_PAP] = v[0];
+    scal[S_ALPHA] = scal[S_RZ] / v[0];
+  } else {
+    scal[S_RZO] = scal[S_RZ];
+    scal[S_RZ] = v[0];
+    scal[S_RZ2] = v[1];
+    scal[S_RR] = v[2];
+    scal[S_BETA] = (v[0] - v[1]) / scal[S_RZO];
+  }
+}
+
+// aa += alpha p; ro = r; r -= alpha ap (smadam_routines.f90:882-889)
+__global__ void k_update_ar(double *aa, double *r, double *ro, const double *p, const double *ap,
+                            long long n, const double *scal) {
+  const double alpha = scal[S_ALPHA];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    aa[i] = aa[i] + alpha * p[i];
+    const double ri = r[i];
+    ro[i] = ri;
+    r[i] = ri - alpha * ap[i];
+  }
+}
+
+// p = z + beta p (922); pw = p * detw for the next scatter
+__global__ void k_update_p(double *p, const double *z, double *pw, const double *bw, long long n,
+                           const double *scal, int first) {
+  const double beta = first ? 0.0 : scal[S_BETA];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double v = first ? z[i] : z[i] + beta * p[i];
+    p[i] = v;
+    pw[i] = v * bw[i];
+  }
+}
+
+__global__ void k_scale_neg(const double *a, const double *bw, double *out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    out[i] = -(a[i] * bw[i]);
+}
+
+__global__ void k_mul(double *z, const double *r, const double *d, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    z[i] = r[i] * d[i];
+}
+
+__global__ void k_diagfilter(double *ap, const double *nna, const double *p, double f,
+                             long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    ap[i] = nna[i] * p[i] * f;
+}
+
+__global__ void k_add(double *a, const double *b, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    a[i] = a[i] + b[i];
+}
+
+// clean_tod (smadam_routines.f90:1545-1585): every sample, no pixel test
+__global__ void k_clean_tod(double *tod, long long n, SampleMap sm, const double *aa) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long det = i / sm.nsamp, s = i - det * sm.nsamp;
+    tod[i] = tod[i] - 1.0 * aa[baseline_of(sm, det, s)];
+  }
+}
+
+// restore_pixels (pointing.f90:168-191) and the list of samples whose value
+// differs from the caller's input
+__global__ void k_restore(const int32_t *pixc, const int32_t *orig, long long n, const int *sub2,
+                          int nosubpix, int32_t *final_pix, long long *idx, int32_t *val,
+                          unsigned long long *count, long long cap) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int c = pixc[i];
+    const int v = c + sub2[c / nosubpix] * nosubpix;
+    if (final_pix) final_pix[i] = v;
+    if (orig && v != orig[i]) {
+      const unsigned long long o = atomicAdd(count, 1ull);
+      if ((long long)o < cap) {
+        idx[o] = i;
+        val[o] = v;
+      }
+    }
+  }
+}
+
+__global__ void k_monopole(const double *map, const int *mask, long long n, int nmap,
+                           double *part) {
+  double v[2] = {0, 0};
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x) {
+    v[0] += map[p * nmap];
+    v[1] += mask[p] > 0 ? 1.0 : 0.0;
+  }
+  block_sum<2>(v);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = v[0];
+    part[gridDim.x + blockIdx.x] = v[1];
+  }
+}
+
+__global__ void k_sub_monopole(double *map, const int *mask, long long n, int nmap,
+                               const double *scal) {
+  const double cover = scal[1];
+  if (cover == 0) return;
+  const double mono = scal[0] / cover;
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x)
+    if (mask[p] > 0) map[p * nmap] -= mono;
+}
+
+// --- CG fallback preconditioner (apply_CG_preconditioner,
+// noise_routines.f90:1305-1409), one CTA per segment
+struct CgpSeg {
+  long long k0;
+  int n;
+  int spec;
+};
+
+__global__ void k_cgp_init(const CgpSeg *segs, const double *r, double *x, double *resid,
+                           double *prop, double *zres, double *prec, const double *nna,
+                           const double *invcov, long long nof, double *st, int *done) {
+  const CgpSeg g = segs[blockIdx.x];
+  const double ic0 = invcov[(long long)g.spec * nof];
+  double v[2] = {0, 0};
+  for (int i = threadIdx.x; i < g.n; i += blockDim.x) {
+    const long long k = g.k0 + i;
+    x[k] = 0;
+    const double rr = r[k];
+    resid[k] = rr;
+    double pc = nna[k] + ic0;
+    if (pc != 0) pc = 1 / pc;
+    prec[k] = pc;
+    const double zz = pc * rr;
+    zres[k] = zz;
+    prop[k] = zz;
+    v[0] += rr * rr;
+    v[1] += rr * zz;
+  }
+  block_sum<2>(v);
+  if (threadIdx.x == 0) {
+    st[4 * blockIdx.x + 0] = v[0];  // rr
+    st[4 * blockIdx.x + 1] = v[0];  // rr0
+    st[4 * blockIdx.x + 2] = v[1];  // rz
+    done[blockIdx.x] = (v[0] == 0);
+  }
+}
+
+__global__ void k_cgp_step(const CgpSeg *segs, double *x, double *resid, double *prop,
+                           double *aprop, double *zres, const double *prec, const double *nna,
+                           double *st, int *done, int iter, int *active) {
+  if (done[blockIdx.x]) return;
+  const CgpSeg g = segs[blockIdx.x];
+  __shared__ double sh[2];
+  double v[2] = {0, 0};
+  for (int i = threadIdx.x; i < g.n; i += blockDim.x) {
+    const long long k = g.k0 + i;
+    const double a = aprop[k] + nna[k] * prop[k];
+    aprop[k] = a;
+    v[0] += prop[k] * a;
+  }
+  block_sum<2>(v);
+  if (threadIdx.x == 0) sh[0] = st[4 * blockIdx.x + 2] / v[0];
+  __syncthreads();
+  const double alpha = sh[0];
+  v[0] = 0;
+  for (int i = threadIdx.x; i < g.n; i += blockDim.x) {
+    const long long k = g.k0 + i;
+    x[k] = x[k] + alpha * prop[k];
+    const double rs = resid[k] - alpha * aprop[k];
+    resid[k] = rs;
+    v[0] += rs * rs;
+  }
+  v[1] = 0;
+  block_sum<2>(v);
+  if (threadIdx.x == 0) {
+    st[4 * blockIdx.x + 0] = v[0];
+    const bool fin = (v[0] / st[4 * blockIdx.x + 1] < fsp(1e-6f)) || iter == 100;
+    done[blockIdx.x] = fin;
+    sh[1] = fin;
+  }
+  __syncthreads();
+  if (sh[1] != 0) return;
+  v[0] = 0;
+  v[1] = 0;
+  for (int i = threadIdx.x; i < g.n; i += blockDim.x) {
+    const long long k = g.k0 + i;
+    const double zz = prec[k] * resid[k];
+    zres[k] = zz;
+    v[0] += resid[k] * zz;
+  }
+  block_sum<2>(v);
+  if (threadIdx.x == 0) {
+    const double rz_old = st[4 * blockIdx.x + 2];
+    st[4 * blockIdx.x + 2] = v[0];
+    sh[0] = v[0] / rz_old;
+    atomicAdd(active, 1);
+  }
+  __syncthreads();
+  const double beta = sh[0];
+  for (int i = threadIdx.x; i < g.n; i += blockDim.x) {
+    const long long k = g.k0 + i;
+    prop[k] = zres[k] + beta * prop[k];
+  }
+}
+
+__global__ void k_copy_seg(const CgpSeg *segs, const double *x, double *z) {
+  const CgpSeg g = segs[blockIdx.x];
+  for (int i = threadIdx.x; i < g.n; i += blockDim.x) z[g.k0 + i] = x[g.k0 + i];
+}
+
+unsigned grid_for(long long n, int block = 256) {
+  long long g = (n + block - 1) / block;
+  return (unsigned)std::max(1LL, std::min(g, 148LL * 32));
+}
+
+double now_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+#include "engine_host.inl"
+
+}  // namespace madam

@@ -1,0 +1,246 @@
+// The destriping engine: state of one destripe() solve on one GPU.
+//
+// Host orchestration follows destripe() (smadam.F90:64-590) and
+// destripe_with_cache() (smadam.F90:593-918).  All sample- and map-domain
+// work runs as CUDA kernels; the host keeps the small tables (baseline layout,
+// PSDs, trimmed filter segments) and drives the PCG loop.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "band2.cuh"
+#include "common.cuh"
+#include "params.h"
+
+namespace madam {
+
+// Owning device allocation.
+template <typename T>
+struct DevBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    if (count == n && p) return;
+    reset();
+    if (count == 0) return;
+    MADAM_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void zero(cudaStream_t s) {
+    if (n) MADAM_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+  }
+  T *get() const { return p; }
+};
+
+// A filtered / preconditioned piece of one (detector, period): the baselines
+// kept by trim_interval (noise_routines.f90:764-813).
+struct Segment {
+  int det, iv, isub;
+  long k0;       // first baseline, index into the [det][noba_short] vectors
+  long noba;
+  int psd_filter;  // psd_index at the period start (convolve_interval)
+  int psd_prec;    // psd_index at the segment start (preconditioning_band)
+  int prec_ok;     // psd_index_det >= 0 and detector weight != 0
+};
+
+// Device table entry of the batched FFT convolution.
+struct ConvSeg {
+  long long x_off;   // input offset into the source vector
+  long long y_off;   // output offset into the destination vector
+  int n_in;          // input length (zero padded to the FFT length)
+  int n_out;         // output length
+  int spec;          // spectrum row
+  int flags;         // bit 0: subtract input mean, bit 1: subtract output mean
+};
+
+// Per-segment band Cholesky factor location.
+struct BandSeg {
+  long long k0;      // first baseline of the segment
+  long long l_off;   // offset of the factor in the band store
+  int n;             // rows
+  int nband;         // band width (kd + 1)
+};
+
+struct Timings {
+  double setup_ms = 0, iterate_ms = 0, finalize_ms = 0, total_ms = 0;
+  double scatter_ms = 0, gather_ms = 0, filter_ms = 0, precond_ms = 0, other_ms = 0;
+};
+
+struct FFTPlan;  // fft.cu
+struct CgpWork;  // engine_host.inl
+
+class Engine {
+ public:
+  Engine();
+  ~Engine();
+
+  // Full destripe().  Pointers are host or device memory (is_device).
+  void run(const Params &par, std::vector<Detector> dets, long ndet, long nsamp,
+           long nnz, double *timestamps, int32_t *pix, float *pixweights,
+           double *signal, long nperiod, const long *periods, bool is_device);
+  // destripe_with_cache(): new TOD, cached pixel matrices / filter / preconditioner
+  void run_cached(long ndet, long nsamp, long nnz, double *timestamps,
+                  int32_t *pix, float *pixweights, double *signal,
+                  bool is_device);
+
+  bool cached() const { return cached_; }
+  const Params &params() const { return par_; }
+
+  // Named results (host copies).  Maps are full sky at nside_map.
+  long result_size(const std::string &name);
+  void result_copy(const std::string &name, void *dst, long nbytes);
+
+  // Times `iters` PCG iterations on the state of the last solve (bench).
+  void bench_iterations(int warmup, int iters, std::vector<double> &out);
+
+  Timings timings;
+  long noiter = 0;
+  double rrinit = 0, rr_final = 0;
+  std::vector<double> rr_history;
+  unsigned long long launches_iter = 0;
+
+ private:
+  // --- setup phases
+  void bind_inputs(double *timestamps, int32_t *pix, float *pixweights,
+                   double *signal, bool is_device, bool first_call);
+  void init_layout(long nperiod, const long *periods);
+  void flag_and_compact(bool first_call);
+  void build_runs();
+  void setup_scatter();
+  void map_side_setup();
+  void initialize_a();
+  void build_segments();
+  void build_filter();
+  void construct_preconditioner();
+  void iterate();
+  void finalize(bool first_call);
+  void writeback_host();
+
+  // --- iteration pieces
+  void apply_A(const double *p, const double *pw, double *ap, bool timed);
+  void bin_tod(bool accumulate_wamap);
+  void subtract_baselines();
+  void clean_tod();
+  void apply_preconditioner(const double *r, double *z);
+  void scatter_baselines(const double *pw, double *target, bool fine);
+  void convolve(const double *x, double *y, const std::vector<ConvSeg> &segs,
+                const double *spectra, DevBuf<ConvSeg> &dsegs);
+  void cg_preconditioner_segments(const double *r, double *z);
+  void finish_dots(int nd, int mode, int slot0);
+
+  Params par_;
+  std::vector<Detector> dets_;
+  bool cached_ = false;
+  cudaStream_t st_ = nullptr;
+  cudaEvent_t ev_[8];
+
+  // sizes
+  long ndet_ = 0, nsamp_ = 0, nnz_ = 0;
+  int nmap_ = 0;
+  long nside_max_ = 0, nosubmaps_tot_ = 0, nosubpix_max_ = 0, nosubpix_map_ = 0,
+       nosubpix_cross_ = 0, ndeg_cross_ = 1, ndeg_shift_ = 0;
+  long ninterval_ = 0, noba_short_ = 0, noba_pp_max_ = 0, nshort_ = 0;
+  double dnshort_ = 0;
+  FastDiv fdn_;
+  std::vector<long> intervals_, istart_iv_, noba_pp_, kstart_pp_;
+  std::vector<uint32_t> bstart_;  // noba_short + 1
+  std::vector<double> btime_;
+  std::vector<double> detw_iv_;   // [det * ninterval + iv], 0 = skipped
+  std::vector<double> bw_host_;   // per baseline detector weight
+
+  // compaction
+  std::vector<int> ksubmap_;
+  std::vector<long> subtable1_, subtable2_;
+  long nolocmaps_ = 0, nloc_ = 0, nloc_map_ = 0, nloc_cross_ = 0;
+  long dummy_local_ = 0, dummy_global_ = 0;
+  int tile_shift_ = 0;
+  long ntiles_ = 0;
+
+  // inputs
+  bool in_device_ = false;
+  int32_t *d_pix_caller_ = nullptr;
+  double *h_signal_ = nullptr;
+  int32_t *h_pix_ = nullptr;
+  double *d_tod_ = nullptr;   // device signal (caller's or ours)
+  DevBuf<double> tod_own_;
+  DevBuf<int32_t> pix_;       // working pixel numbers
+  DevBuf<float> wraw_;        // staging copy of host weights
+  const float *d_w_ = nullptr;
+  DevBuf<float4> point4_;     // nnz = 3: {w0, w1, w2, compacted pixel}
+  DevBuf<int32_t> pixc_;      // nnz = 1: compacted pixel
+  DevBuf<uint32_t> bstart_d_;
+  DevBuf<double> bw_;         // per-baseline detector weight
+  DevBuf<uint8_t> rmask_;
+  DevBuf<double> times_d_;
+
+  // runs for the privatised scatters
+  DevBuf<Run> runs_;
+  DevBuf<int> item_begin_;   // nwork + 1 run offsets
+  DevBuf<int> item_tile_;    // tile of each work item
+  long nruns_ = 0, nwork_ = 0;
+  DevBuf<long long> istart_d_;
+  DevBuf<int> kstart_d_;
+  DevBuf<int32_t> pix_orig_;
+
+  // map domain (compacted)
+  DevBuf<double> cc_, cca_, map_, binmap_, wamap_, lmap_, lmap_fine_;
+  DevBuf<int> hits_, mask_;
+  DevBuf<float> crit_;
+  DevBuf<int> flagcount_;
+
+  // baseline domain
+  DevBuf<double> aa_, yba_, nna_, r_, p_, z_, ap_, ro_, pw_, tmpv_;
+  std::vector<double> nna_host_;
+  DevBuf<double> part_, scal_;
+  std::vector<double> scal_host_;
+
+  // filter / preconditioner
+  long nof_ = -1, npsdtot_ = 0;
+  std::vector<int> psddet_;
+  std::vector<double> psdstart_, psdstop_;
+  std::vector<double> fcov_host_, invcov_host_;
+  DevBuf<double> fcov_, fprec_, invcov_, delta_;
+  std::vector<Segment> segs_;
+  std::vector<ConvSeg> filt_segs_, fprec_segs_;
+  DevBuf<ConvSeg> filt_segs_d_, fprec_segs_d_, tmp_segs_d_;
+  bool use_diagonal_ = false;
+  DevBuf<double> prec_diag_;
+  std::vector<BandSeg> band_segs_;
+  DevBuf<BandSeg> band_segs_d_;
+  DevBuf<double> band_;
+  std::vector<int> cg_prec_segs_;   // segments without a band factor
+  std::vector<long> band_widths_;
+  DevBuf<PSeg> p2segs_;
+  DevBuf<PRun> p2runs_;
+  DevBuf<PChunk> p2ch_;
+  DevBuf<double> p2rows_, p2T_, p2wp_, p2ws_;
+  int p2nseg_ = 0, p2nch_ = 0;
+  long long band2_rows_ = 0;
+  long band2_ntrans_ = 0;
+  long n_band_fail_ = 0;
+  std::unique_ptr<FFTPlan> fft_;
+  std::unique_ptr<CgpWork> cgp_;
+
+  // pixels flagged during the call (host write-back)
+  DevBuf<long long> flagged_idx_;
+  DevBuf<int32_t> flagged_val_;
+  std::vector<int32_t> orig_pix_values_;
+  bool tod_cleaned_ = false;
+};
+
+}  // namespace madam

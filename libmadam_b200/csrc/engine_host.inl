@@ -1,0 +1,1796 @@
+// Engine methods: host orchestration of the destriping solve.  Included at
+// the end of engine.cu so the kernels there are visible.
+
+// Work vectors of the CG fallback preconditioner.
+struct CgpWork {
+  DevBuf<CgpSeg> segs;
+  DevBuf<double> x, resid, prop, aprop, zres, prec, st;
+  DevBuf<int> done, active;
+  DevBuf<ConvSeg> csegs;
+  std::vector<ConvSeg> hcsegs;
+  long nseg = 0;
+};
+
+Engine::Engine() {
+  MADAM_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+  for (auto &e : ev_) MADAM_CUDA(cudaEventCreate(&e));
+}
+
+Engine::~Engine() {
+  for (auto &e : ev_) cudaEventDestroy(e);
+  if (st_) cudaStreamDestroy(st_);
+}
+
+static SampleMap sample_map(const long long *istart, const int *kstart, int niv,
+                            long long nsamp, long noba, FastDiv fdn) {
+  SampleMap m;
+  m.istart = istart;
+  m.kstart = kstart;
+  m.ninterval = niv;
+  m.nsamp = nsamp;
+  m.noba_short = noba;
+  m.fdn = fdn;
+  return m;
+}
+
+void Engine::bind_inputs(double *timestamps, int32_t *pix, float *pixweights, double *signal,
+                         bool is_device, bool first_call) {
+  (void)first_call;
+  (void)timestamps;
+  const long long n = (long long)ndet_ * nsamp_;
+  in_device_ = is_device;
+  h_pix_ = is_device ? nullptr : pix;
+  h_signal_ = is_device ? nullptr : signal;
+  const cudaMemcpyKind kind = is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  pix_.alloc(n);
+  pix_orig_.alloc(n);
+  MADAM_CUDA(cudaMemcpyAsync(pix_orig_.get(), pix, n * sizeof(int32_t), kind, st_));
+  MADAM_CUDA(cudaMemcpyAsync(pix_.get(), pix_orig_.get(), n * sizeof(int32_t),
+                             cudaMemcpyDeviceToDevice, st_));
+  if (is_device) {
+    d_w_ = pixweights;
+    d_tod_ = signal;
+  } else {
+    wraw_.alloc(n * nnz_);
+    MADAM_CUDA(cudaMemcpyAsync(wraw_.get(), pixweights, n * nnz_ * sizeof(float),
+                               cudaMemcpyHostToDevice, st_));
+    d_w_ = wraw_.get();
+    tod_own_.alloc(n);
+    MADAM_CUDA(cudaMemcpyAsync(tod_own_.get(), signal, n * sizeof(double),
+                               cudaMemcpyHostToDevice, st_));
+    d_tod_ = tod_own_.get();
+  }
+}
+
+void Engine::init_layout(long nperiod, const long *periods) {
+  Params &p = par_;
+  // check_files: interval lengths (read_data.f90:221-239)
+  ninterval_ = nperiod;
+  if (nperiod <= 0) fail("ERROR: intervals not known.");
+  intervals_.assign(nperiod, 0);
+  for (long ip = 0; ip < nperiod; ++ip) {
+    const long len = (ip < nperiod - 1) ? periods[ip + 1] - periods[ip] : nsamp_ - periods[ip];
+    if (p.basis_order > 0 && len < p.basis_order + 1) fail("Too short period");
+    intervals_[ip] = len;
+  }
+  // init_parameters (parameter_control.f90:27-409)
+  if (!p.radiometers) {
+    for (auto &d : dets_)
+      for (int ip = 0; ip < d.npsd && d.has_psd; ++ip) {
+        auto &psd = d.psds[ip];
+        size_t im = 0;
+        for (size_t i = 1; i < psd.size(); ++i)
+          if (psd[i] > psd[im]) im = i;
+        for (size_t i = 0; i < im; ++i) psd[i] = psd[im];
+      }
+  }
+  if (p.noise_weights_from_psd) {
+    // measure_noise_weights (noise_routines.f90:65-127)
+    const double fs = p.fsample;
+    if (p.radiometers) {
+      const double f = fs / 2;
+      for (auto &d : dets_)
+        for (int i = 0; i < d.npsd; ++i) {
+          double v;
+          interpolate_psd(d.psdfreqs, d.psds[i], &f, &v, 1);
+          d.sigmas[i] = std::sqrt(v * fs);
+          d.plateaus[i] = v;
+        }
+    } else {
+      const long nbin = 10000;
+      const double fstep = fs * .5 / nbin;
+      std::vector<double> fr(nbin), dv(nbin);
+      for (long i = 0; i < nbin; ++i) fr[i] = fstep * (i + 1);
+      const double fbase = 1 / (p.dnshort / fs);
+      const long ibase = (long)(fbase / fstep);
+      const long ilo = (long)(1 / fstep), ihi = (long)(10 / fstep);
+      for (auto &d : dets_)
+        for (int ip = 0; ip < d.npsd; ++ip) {
+          interpolate_psd(d.psdfreqs, d.psds[ip], fr.data(), dv.data(), nbin);
+          double plateau = dv[ilo - 1];
+          for (long i = ilo - 1; i <= ihi - 1; ++i) plateau = std::min(plateau, dv[i]);
+          double rms = ibase * plateau;
+          for (long i = ibase; i < nbin; ++i) rms += dv[i];
+          d.sigmas[ip] = std::sqrt(rms / nbin * fs);
+          d.plateaus[ip] = plateau;
+          d.weights[ip] = 1 / (plateau * fs);
+        }
+    }
+  }
+  if (p.nsubchunk < 2) {
+    p.nsubchunk = 0;
+    p.isubchunk = 0;
+  }
+  if (p.nsubchunk > 1) fail("nsubchunk > 1 is not supported");
+  if (p.good_baseline_fraction < 0 || p.good_baseline_fraction > 1)
+    fail("ERROR: good_baseline_fraction must be in 0..1");
+  if (p.nside_cross < 0) p.nside_cross = p.nside_map;
+  auto pow2 = [](long v) { return v > 0 && (v & (v - 1)) == 0; };
+  if (!pow2(p.nside_map)) fail("nside_map must be a power of two.");
+  if (!pow2(p.nside_submap)) fail("nside_submap must be a power of two.");
+  if (!pow2(p.nside_cross)) fail("nside_cross must be a power of two.");
+  if (p.nside_map < p.nside_cross) fail("nside_cross > nside_map not supported by Madam/TOAST");
+  if (p.pixlim_cross < 0) p.pixlim_cross = p.pixlim_map;
+  if (p.pixmode_map < 0 || p.pixmode_map > 2) fail("Pixmode_map must be in range [0-2]");
+  if (p.pixmode_cross < 0 || p.pixmode_cross > 4) fail("Pixmode_cross must be in range [0-4]");
+  if (!p.file_inmask.empty()) fail("file_inmask is not supported");
+  if (!p.file_spectrum.empty()) fail("file_spectrum is not supported");
+  if (!p.file_covmat.empty()) fail("file_covmat is not supported");
+  if (nmap_ == 1) p.temperature_only = true;
+  else if (p.temperature_only) nmap_ = 1;
+  if (nmap_ != 1 && nmap_ != 3) fail("only nnz = 1 or nnz = 3 is supported");
+  if (p.mode_detweight == 0) {
+    for (auto &d : dets_)
+      for (int i = 0; i < d.npsd; ++i)
+        d.weights[i] = (d.sigmas[i] == 0) ? 0 : 1.0 / d.plateaus[i] / p.fsample;
+  } else if (p.mode_detweight == 1) {
+    for (auto &d : dets_) std::fill(d.weights.begin(), d.weights.end(), 1.0);
+  } else if (p.mode_detweight == 2) {
+    auto horn = [](const std::string &nm) -> long {
+      std::string s = nm.compare(0, 3, "LFI") == 0 ? nm.substr(3, 2)
+                                                    : (nm.size() > 4 ? nm.substr(4, 1) : "");
+      char *end = nullptr;
+      const long h = std::strtol(s.c_str(), &end, 10);
+      if (s.empty() || !end || *end != '\0') fail("ERROR : Failed to extract horn from " + nm);
+      return h;
+    };
+    for (size_t a = 0; a + 1 < dets_.size(); ++a) {
+      const long h1 = horn(dets_[a].name);
+      for (size_t b = a + 1; b < dets_.size(); ++b) {
+        if (horn(dets_[b].name) != h1) continue;
+        auto &d1 = dets_[a];
+        auto &d2 = dets_[b];
+        if (d1.npsd != d2.npsd)
+          fail("Detectors in the same horn do not have the same number of PSDs");
+        std::vector<double> w(d1.npsd);
+        for (int i = 0; i < d1.npsd; ++i)
+          w[i] = (d1.plateaus[i] == 0 || d2.plateaus[i] == 0)
+                     ? 0
+                     : 2 / (d1.plateaus[i] + d2.plateaus[i]) / p.fsample;
+        d1.weights = w;
+        d2.weights = w;
+      }
+    }
+  } else {
+    fail("bad mode_detweight");
+  }
+  nside_max_ = std::max(p.nside_map, p.nside_cross);
+  p.nside_submap = std::min({p.nside_submap, p.nside_map, p.nside_cross});
+  nosubmaps_tot_ = 12 * p.nside_submap * p.nside_submap;
+  nshort_ = (long)(p.dnshort + .5);
+  if (!p.kfirst) {
+    p.dnshort = 1e6;
+    nshort_ = (long)(p.dnshort + .5);
+    p.precond_width_min = 0;
+    p.precond_width_max = 0;
+    p.kfilter = false;
+  } else {
+    p.precond_width_max = std::max(p.precond_width_min, p.precond_width_max);
+  }
+  if (p.basis_order > 0 && p.kfilter) fail("Filter only implemented for basis_order==0");
+  if (p.basis_order > 0) fail("basis_order > 0 is not supported");
+  dnshort_ = p.dnshort;
+  noba_pp_.assign(ninterval_, 0);
+  kstart_pp_.assign(ninterval_ + 1, 0);
+  istart_iv_.assign(ninterval_ + 1, 0);
+  noba_short_ = 0;
+  long long acc = 0;
+  for (long i = 0; i < ninterval_; ++i) {
+    if (intervals_[i] <= 0) fail("empty pointing period");
+    noba_pp_[i] = (long)((double)(intervals_[i] - 1) / dnshort_) + 1;
+    kstart_pp_[i] = noba_short_;
+    istart_iv_[i] = acc;
+    noba_short_ += noba_pp_[i];
+    acc += intervals_[i];
+  }
+  kstart_pp_[ninterval_] = noba_short_;
+  istart_iv_[ninterval_] = acc;
+  if (acc != nsamp_) fail("pointing periods do not cover the samples");
+  if ((long long)ndet_ * noba_short_ >= (1LL << 31)) fail("too many baselines");
+  if (nsamp_ >= (1LL << 32) - 1) fail("too many samples per detector");
+  const long nsm = p.nside_submap;
+  nosubpix_max_ = nside_max_ * nside_max_ / (nsm * nsm);
+  nosubpix_map_ = p.nside_map * p.nside_map / (nsm * nsm);
+  nosubpix_cross_ = p.nside_cross * p.nside_cross / (nsm * nsm);
+  ndeg_cross_ = nosubpix_max_ / nosubpix_cross_;
+  ndeg_shift_ = 0;
+  while ((1L << ndeg_shift_) < ndeg_cross_) ++ndeg_shift_;
+  noba_pp_max_ = 0;
+  for (long v : noba_pp_) noba_pp_max_ = std::max(noba_pp_max_, v);
+  // start_timeloop (parameter_control.f90:752-846): baseline lengths
+  bstart_.assign(noba_short_ + 1, 0);
+  long m = 0;
+  long long pos = 0;
+  for (long i = 0; i < ninterval_; ++i) {
+    double dn = 0;
+    long nn = 0;
+    for (long k = 0; k < noba_pp_[i] - 1; ++k) {
+      const double dn0 = dn;
+      const long n0 = nn;
+      dn = dn0 + dnshort_;
+      nn = (long)(dn + .5);
+      bstart_[m++] = (uint32_t)pos;
+      pos += nn - n0;
+    }
+    const long last = intervals_[i] - nn;
+    if (p.kfirst && (last < 0 || last > (long)dnshort_ + 1))
+      fail("ERROR in start_timeloop: Lengths do not match.");
+    bstart_[m++] = (uint32_t)pos;
+    pos += last;
+  }
+  bstart_[m] = (uint32_t)pos;
+  // every baseline but the last of a period has length dnshort
+  const double dnc = std::min(dnshort_, 4294967295.0);
+  fdn_ = FastDiv((uint32_t)std::max(1.0, dnc));
+  // device copies of the layout tables
+  istart_d_.alloc(ninterval_ + 1);
+  kstart_d_.alloc(ninterval_ + 1);
+  std::vector<long long> is(istart_iv_.begin(), istart_iv_.end());
+  std::vector<int> ks(kstart_pp_.begin(), kstart_pp_.end());
+  MADAM_CUDA(cudaMemcpyAsync(istart_d_.get(), is.data(), is.size() * sizeof(long long),
+                             cudaMemcpyHostToDevice, st_));
+  MADAM_CUDA(cudaMemcpyAsync(kstart_d_.get(), ks.data(), ks.size() * sizeof(int),
+                             cudaMemcpyHostToDevice, st_));
+  bstart_d_.alloc(noba_short_ + 1);
+  MADAM_CUDA(cudaMemcpyAsync(bstart_d_.get(), bstart_.data(), bstart_.size() * sizeof(uint32_t),
+                             cudaMemcpyHostToDevice, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+}
+
+void Engine::flag_and_compact(bool first_call) {
+  const long long n = (long long)ndet_ * nsamp_;
+  const SampleMap sm = sample_map(istart_d_.get(), kstart_d_.get(), (int)ninterval_, nsamp_,
+                                  noba_short_, fdn_);
+  if (first_call && n > 0) {
+    // check_files (read_data.f90:241-272)
+    MADAM_LAUNCH(k_flag_zero_weight, grid_for(n), 256, 0, st_, pix_.get(), d_w_, (int)nnz_, n);
+    DevBuf<unsigned long long> cnt;
+    cnt.alloc((size_t)ndet_ * ninterval_);
+    cnt.zero(st_);
+    MADAM_LAUNCH(k_count_good, grid_for(n), 256, 0, st_, pix_.get(), n, sm, (int)ninterval_,
+                 cnt.get());
+    DevBuf<long long> ivlen;
+    ivlen.alloc(ninterval_);
+    std::vector<long long> il(intervals_.begin(), intervals_.end());
+    MADAM_CUDA(cudaMemcpyAsync(ivlen.get(), il.data(), il.size() * sizeof(long long),
+                               cudaMemcpyHostToDevice, st_));
+    MADAM_LAUNCH(k_flag_sparse, grid_for(n), 256, 0, st_, pix_.get(), n, sm, (int)ninterval_,
+                 cnt.get(), ivlen.get());
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+  }
+  // init_pointing + where (pixels < 0) pixels = dummy_pixel + reduce_pixels
+  dummy_global_ = 12 * nside_max_ * nside_max_;
+  DevBuf<int> ksub;
+  ksub.alloc(nosubmaps_tot_ + 1);
+  ksub.zero(st_);
+  if (n > 0)
+    MADAM_LAUNCH(k_dummy_ksub, grid_for(n), 256, 0, st_, pix_.get(), n, (int)dummy_global_,
+                 (int)nosubpix_max_, ksub.get());
+  std::vector<int> ks(nosubmaps_tot_ + 1);
+  MADAM_CUDA(cudaMemcpyAsync(ks.data(), ksub.get(), ks.size() * sizeof(int),
+                             cudaMemcpyDeviceToHost, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  ks[nosubmaps_tot_] = 1;
+  if (first_call) {
+    ksubmap_ = ks;
+    subtable1_.assign(nosubmaps_tot_ + 1, -1);
+    subtable2_.assign(nosubmaps_tot_ + 1, -1);
+    long k = -1;
+    for (long i = 0; i <= nosubmaps_tot_; ++i)
+      if (ksubmap_[i]) {
+        ++k;
+        subtable1_[i] = i - k;
+        subtable2_[k] = i - k;
+      }
+    nolocmaps_ = 0;
+    for (long i = 0; i < nosubmaps_tot_; ++i) nolocmaps_ += ksubmap_[i] ? 1 : 0;
+    nloc_ = nolocmaps_ * nosubpix_max_;
+    nloc_map_ = nloc_;
+    nloc_cross_ = nolocmaps_ * nosubpix_cross_;
+    dummy_local_ = (nosubmaps_tot_ - subtable1_[nosubmaps_tot_]) * nosubpix_max_;
+    if (nloc_ >= (1L << 30)) fail("map too large");
+    int ts = 0;
+    while ((1L << (ts + 1)) <= std::min<long>(nosubpix_max_, kTileMax)) ++ts;
+    tile_shift_ = ts;
+    ntiles_ = (nloc_ + (1L << ts) - 1) >> ts;
+  } else {
+    for (long i = 0; i <= nosubmaps_tot_; ++i)
+      if ((ks[i] != 0) != (ksubmap_[i] != 0))
+        fail("destripe_with_cache: the pointing hits other submaps than the cached call");
+  }
+  DevBuf<int> sub1;
+  sub1.alloc(nosubmaps_tot_ + 1);
+  std::vector<int> s1(subtable1_.begin(), subtable1_.end());
+  MADAM_CUDA(cudaMemcpyAsync(sub1.get(), s1.data(), s1.size() * sizeof(int),
+                             cudaMemcpyHostToDevice, st_));
+  if (nmap_ == 3 && nnz_ == 3) {
+    point4_.alloc(n);
+    if (n > 0)
+      MADAM_LAUNCH(k_compact<3>, grid_for(n), 256, 0, st_, pix_.get(), d_w_, n, sub1.get(),
+                   (int)nosubpix_max_, point4_.get(), nullptr);
+  } else {
+    pixc_.alloc(n);
+    if (n > 0)
+      MADAM_LAUNCH(k_compact<1>, grid_for(n), 256, 0, st_, pix_.get(), d_w_, n, sub1.get(),
+                   (int)nosubpix_max_, nullptr, pixc_.get());
+  }
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  if (!in_device_) wraw_.reset();
+  // detector weights per (det, period) and per baseline
+  if (first_call) {
+    detw_iv_.assign((size_t)ndet_ * ninterval_, 0.0);
+    for (long d = 0; d < ndet_; ++d)
+      for (long iv = 0; iv < ninterval_; ++iv) {
+        const int ipsd = psd_index_det(dets_[d], btime_[kstart_pp_[iv]]);
+        if (ipsd < 0) continue;
+        detw_iv_[d * ninterval_ + iv] = dets_[d].weights[ipsd];
+      }
+    DevBuf<double> dw;
+    dw.alloc(detw_iv_.size());
+    MADAM_CUDA(cudaMemcpyAsync(dw.get(), detw_iv_.data(), detw_iv_.size() * sizeof(double),
+                               cudaMemcpyHostToDevice, st_));
+    const long long nb = (long long)ndet_ * noba_short_;
+    bw_.alloc(nb);
+    MADAM_LAUNCH(k_baseline_weights, grid_for(nb), 256, 0, st_, bw_.get(), nb, noba_short_,
+                 kstart_d_.get(), (int)ninterval_, dw.get());
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+  }
+  // flag_bad_baselines (read_data.f90:30-74)
+  if (par_.kfirst && par_.good_baseline_fraction != 0 && !par_.kfilter) {
+    const long long nb = (long long)ndet_ * noba_short_;
+    const unsigned grid = (unsigned)((nb * 32 + 255) / 256);
+    if (nmap_ == 3)
+      MADAM_LAUNCH(k_bad_baselines<3>, grid, 256, 0, st_, pix_.get(), point4_.get(), nullptr, nb,
+                   noba_short_, nsamp_, bstart_d_.get(), (int)dummy_global_,
+                   par_.good_baseline_fraction);
+    else
+      MADAM_LAUNCH(k_bad_baselines<1>, grid, 256, 0, st_, pix_.get(), nullptr, pixc_.get(), nb,
+                   noba_short_, nsamp_, bstart_d_.get(), (int)dummy_global_,
+                   par_.good_baseline_fraction);
+  }
+}
+
+void Engine::build_runs() {
+  const long long n = (long long)ndet_ * nsamp_;
+  const SampleMap sm = sample_map(istart_d_.get(), kstart_d_.get(), (int)ninterval_, nsamp_,
+                                  noba_short_, fdn_);
+  nruns_ = 0;
+  nwork_ = 0;
+  item_begin_.alloc(1);
+  item_begin_.zero(st_);
+  if (n == 0) return;
+  DevBuf<uint8_t> sflag, eflag;
+  sflag.alloc(n);
+  eflag.alloc(n);
+  const float4 *p4 = point4_.get();
+  const int32_t *pc = pixc_.get();
+  if (nmap_ == 3)
+    MADAM_LAUNCH(k_run_flags<3>, grid_for(n), 256, 0, st_, p4, pc, n, sm, bw_.get(), (int)nloc_,
+                 tile_shift_, sflag.get(), eflag.get());
+  else
+    MADAM_LAUNCH(k_run_flags<1>, grid_for(n), 256, 0, st_, p4, pc, n, sm, bw_.get(), (int)nloc_,
+                 tile_shift_, sflag.get(), eflag.get());
+  // select run starts / ends
+  DevBuf<long long> starts, ends, nsel;
+  starts.alloc(n);
+  ends.alloc(n);
+  nsel.alloc(2);
+  cub::CountingInputIterator<long long> it(0);
+  size_t tmpb = 0;
+  MADAM_CUDA(cub::DeviceSelect::Flagged(nullptr, tmpb, it, sflag.get(), starts.get(), nsel.get(),
+                                        n, st_));
+  DevBuf<uint8_t> tmp;
+  tmp.alloc(tmpb);
+  MADAM_CUDA(cub::DeviceSelect::Flagged(tmp.get(), tmpb, it, sflag.get(), starts.get(),
+                                        nsel.get(), n, st_));
+  MADAM_CUDA(cub::DeviceSelect::Flagged(tmp.get(), tmpb, it, eflag.get(), ends.get(),
+                                        nsel.get() + 1, n, st_));
+  long long cnt[2];
+  MADAM_CUDA(cudaMemcpyAsync(cnt, nsel.get(), sizeof cnt, cudaMemcpyDeviceToHost, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  sflag.reset();
+  eflag.reset();
+  if (cnt[0] != cnt[1]) fail("internal: unpaired run boundaries");
+  const long long nr0 = cnt[0];
+  if (nr0 == 0) return;
+  // split long runs
+  DevBuf<long long> pieces, poff;
+  pieces.alloc(nr0);
+  poff.alloc(nr0 + 1);
+  MADAM_LAUNCH(k_run_pieces, grid_for(nr0), 256, 0, st_, starts.get(), ends.get(), nr0,
+               pieces.get());
+  tmpb = 0;
+  MADAM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmpb, pieces.get(), poff.get(), nr0, st_));
+  tmp.alloc(std::max<size_t>(tmpb, tmp.n));
+  MADAM_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tmpb, pieces.get(), poff.get(), nr0, st_));
+  long long lastoff, lastp;
+  MADAM_CUDA(cudaMemcpyAsync(&lastoff, poff.get() + nr0 - 1, sizeof(long long),
+                             cudaMemcpyDeviceToHost, st_));
+  MADAM_CUDA(cudaMemcpyAsync(&lastp, pieces.get() + nr0 - 1, sizeof(long long),
+                             cudaMemcpyDeviceToHost, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  const long long nr = lastoff + lastp;
+  if (nr >= (1LL << 31)) fail("too many runs");
+  DevBuf<Run> runs0;
+  DevBuf<int> keys, lens, keys_sorted, idx, idx_sorted, lens_sorted;
+  runs0.alloc(nr);
+  keys.alloc(nr);
+  lens.alloc(nr);
+  if (nmap_ == 3)
+    MADAM_LAUNCH(k_run_emit<3>, grid_for(nr0), 256, 0, st_, starts.get(), ends.get(), poff.get(),
+                 nr0, sm, p4, pc, tile_shift_, runs0.get(), keys.get(), lens.get());
+  else
+    MADAM_LAUNCH(k_run_emit<1>, grid_for(nr0), 256, 0, st_, starts.get(), ends.get(), poff.get(),
+                 nr0, sm, p4, pc, tile_shift_, runs0.get(), keys.get(), lens.get());
+  starts.reset();
+  ends.reset();
+  // bucket runs by tile (stable radix sort keeps time order inside a tile)
+  idx.alloc(nr);
+  idx_sorted.alloc(nr);
+  keys_sorted.alloc(nr);
+  {
+    // idx = 0..nr-1
+    std::vector<int> h(nr);
+    for (long long i = 0; i < nr; ++i) h[i] = (int)i;
+    MADAM_CUDA(cudaMemcpyAsync(idx.get(), h.data(), nr * sizeof(int), cudaMemcpyHostToDevice, st_));
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+  }
+  int endbit = 1;
+  while ((1L << endbit) <= ntiles_) ++endbit;
+  tmpb = 0;
+  MADAM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmpb, keys.get(), keys_sorted.get(),
+                                             idx.get(), idx_sorted.get(), (int)nr, 0, endbit, st_));
+  tmp.alloc(std::max<size_t>(tmpb, tmp.n));
+  MADAM_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tmpb, keys.get(), keys_sorted.get(),
+                                             idx.get(), idx_sorted.get(), (int)nr, 0, endbit, st_));
+  runs_.alloc(nr);
+  lens_sorted.alloc(nr);
+  MADAM_LAUNCH(k_gather_runs, grid_for(nr), 256, 0, st_, idx_sorted.get(), runs0.get(),
+               lens.get(), nr, runs_.get(), lens_sorted.get());
+  runs0.reset();
+  // work items: <= kItemSamples samples of one tile
+  DevBuf<long long> lens64, pref;
+  lens64.alloc(nr);
+  pref.alloc(nr);
+  tmpb = 0;
+  cub::TransformInputIterator<long long, cub::CastOp<long long>, const int *> wide(
+      lens_sorted.get(), cub::CastOp<long long>());
+  MADAM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmpb, wide, pref.get(), nr, st_));
+  tmp.alloc(std::max<size_t>(tmpb, tmp.n));
+  MADAM_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tmpb, wide, pref.get(), nr, st_));
+  DevBuf<uint8_t> iflag;
+  iflag.alloc(nr);
+  MADAM_LAUNCH(k_item_flags, grid_for(nr), 256, 0, st_, keys_sorted.get(), pref.get(), nr,
+               iflag.get());
+  DevBuf<long long> ibeg, nitem;
+  ibeg.alloc(nr);
+  nitem.alloc(1);
+  cub::CountingInputIterator<long long> it2(0);
+  tmpb = 0;
+  MADAM_CUDA(cub::DeviceSelect::Flagged(nullptr, tmpb, it2, iflag.get(), ibeg.get(), nitem.get(),
+                                        nr, st_));
+  tmp.alloc(std::max<size_t>(tmpb, tmp.n));
+  MADAM_CUDA(cub::DeviceSelect::Flagged(tmp.get(), tmpb, it2, iflag.get(), ibeg.get(),
+                                        nitem.get(), nr, st_));
+  long long ni;
+  MADAM_CUDA(cudaMemcpyAsync(&ni, nitem.get(), sizeof ni, cudaMemcpyDeviceToHost, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  item_begin_.alloc(ni + 1);
+  item_tile_.alloc(ni);
+  MADAM_LAUNCH(k_item_tiles, grid_for(ni), 256, 0, st_, ibeg.get(), ni, keys_sorted.get(),
+               item_begin_.get(), item_tile_.get());
+  const int nrr = (int)nr;
+  MADAM_CUDA(cudaMemcpyAsync(item_begin_.get() + ni, &nrr, sizeof(int), cudaMemcpyHostToDevice,
+                             st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  nruns_ = nr;
+  nwork_ = ni;
+}
+
+void Engine::bin_tod(bool accumulate_wamap) {
+  // pixel_matrix + count_hits + bin_tod (smadam_routines.f90:111-422)
+  const int ncc = nmap_ == 3 ? 6 : 1;
+  const int T = 1 << tile_shift_;
+  const size_t smem = (size_t)(ncc + nmap_) * T * sizeof(double) + T * sizeof(int);
+  static bool attr = false;
+  if (!attr) {
+    MADAM_CUDA(cudaFuncSetAttribute(k_setup_scatter<3>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+    MADAM_CUDA(cudaFuncSetAttribute(k_setup_scatter<1>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+    attr = true;
+  }
+  DevBuf<double> ccacc, bin;
+  DevBuf<int> hits;
+  ccacc.alloc((size_t)nloc_ * ncc);
+  ccacc.zero(st_);
+  bin.alloc((size_t)nloc_ * nmap_);
+  bin.zero(st_);
+  hits.alloc(nloc_);
+  hits.zero(st_);
+  if (nwork_ > 0) {
+    if (nmap_ == 3)
+      MADAM_LAUNCH(k_setup_scatter<3>, (unsigned)nwork_, 256, smem, st_, item_begin_.get(),
+                   item_tile_.get(), runs_.get(), point4_.get(), pixc_.get(), d_tod_, bw_.get(),
+                   fdn_, tile_shift_, ccacc.get(), bin.get(), hits.get());
+    else
+      MADAM_LAUNCH(k_setup_scatter<1>, (unsigned)nwork_, 256, smem, st_, item_begin_.get(),
+                   item_tile_.get(), runs_.get(), point4_.get(), pixc_.get(), d_tod_, bw_.get(),
+                   fdn_, tile_shift_, ccacc.get(), bin.get(), hits.get());
+  }
+  const long long nv = (long long)nloc_ * nmap_;
+  if (!accumulate_wamap) {
+    // first call: cc, cca, hits, map, binmap, wamap from scratch
+    cc_.alloc((size_t)nloc_ * ncc);
+    MADAM_CUDA(cudaMemcpyAsync(cc_.get(), ccacc.get(), cc_.n * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st_));
+    hits_.alloc(nloc_);
+    MADAM_CUDA(cudaMemcpyAsync(hits_.get(), hits.get(), nloc_ * sizeof(int),
+                               cudaMemcpyDeviceToDevice, st_));
+    cca_.alloc((size_t)nloc_cross_ * ncc);
+    wamap_.alloc((size_t)nloc_cross_ * nmap_);
+    wamap_.zero(st_);
+    if (ndeg_cross_ == 1) {
+      MADAM_CUDA(cudaMemcpyAsync(cca_.get(), ccacc.get(), cca_.n * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, st_));
+    } else {
+      MADAM_LAUNCH(k_degrade, grid_for(nloc_cross_ * ncc), 256, 0, st_, ccacc.get(), cca_.get(),
+                   (long long)nloc_cross_, ncc, (int)ndeg_cross_);
+    }
+  }
+  map_.alloc(nv);
+  binmap_.alloc(nv);
+  if (par_.kfirst) {
+    MADAM_CUDA(cudaMemcpyAsync(map_.get(), bin.get(), nv * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st_));
+  } else {
+    map_.zero(st_);
+  }
+  MADAM_CUDA(cudaMemcpyAsync(binmap_.get(), bin.get(), nv * sizeof(double),
+                             cudaMemcpyDeviceToDevice, st_));
+  if (par_.kfirst) {
+    // collect_map(wamap) adds to whatever wamap holds
+    DevBuf<double> wc;
+    wc.alloc((size_t)nloc_cross_ * nmap_);
+    if (ndeg_cross_ == 1)
+      MADAM_CUDA(cudaMemcpyAsync(wc.get(), bin.get(), wc.n * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, st_));
+    else
+      MADAM_LAUNCH(k_degrade, grid_for(nloc_cross_ * nmap_), 256, 0, st_, bin.get(), wc.get(),
+                   (long long)nloc_cross_, nmap_, (int)ndeg_cross_);
+    MADAM_LAUNCH(k_add, grid_for(wc.n), 256, 0, st_, wamap_.get(), wc.get(), (long long)wc.n);
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+  }
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+}
+
+void Engine::setup_scatter() { bin_tod(false); }
+
+void Engine::map_side_setup() {
+  // invert_pixelmatrix_cross (map_routines.f90:83-212)
+  MatrixRules mr{(int)par_.pixmode_cross, par_.pixlim_cross, par_.allow_decoupling ? 1 : 0,
+                 par_.incomplete_matrices ? 1 : 0};
+  if (nloc_cross_ == 0) return;
+  if (nmap_ == 3)
+    MADAM_LAUNCH(k_invert_cross<3>, grid_for(nloc_cross_), 128, 0, st_, cca_.get(),
+                 (long long)nloc_cross_, mr);
+  else
+    MADAM_LAUNCH(k_invert_cross<1>, grid_for(nloc_cross_), 128, 0, st_, cca_.get(),
+                 (long long)nloc_cross_, mr);
+}
+
+void Engine::initialize_a() {
+  // initialize_a (smadam_routines.f90:428-671)
+  const long long nb = (long long)ndet_ * noba_short_;
+  if (nloc_cross_ > 0) {
+    if (nmap_ == 3)
+      MADAM_LAUNCH(k_ccmult<3>, grid_for(nloc_cross_), 256, 0, st_, cca_.get(), wamap_.get(),
+                   (long long)nloc_cross_);
+    else
+      MADAM_LAUNCH(k_ccmult<1>, grid_for(nloc_cross_), 256, 0, st_, cca_.get(), wamap_.get(),
+                   (long long)nloc_cross_);
+  }
+  yba_.alloc(nb);
+  nna_.alloc(nb);
+  aa_.alloc(nb);
+  yba_.zero(st_);
+  nna_.zero(st_);
+  aa_.zero(st_);
+  const unsigned grid = (unsigned)((nb * 32 + 255) / 256);
+  if (nb > 0) {
+    if (nmap_ == 3)
+      MADAM_LAUNCH(k_init_a<3>, grid, 256, 0, st_, point4_.get(), pixc_.get(), d_tod_,
+                   bstart_d_.get(), nb, noba_short_, nsamp_, bw_.get(), wamap_.get(),
+                   (int)ndeg_shift_, (int)nloc_, yba_.get(), nna_.get());
+    else
+      MADAM_LAUNCH(k_init_a<1>, grid, 256, 0, st_, point4_.get(), pixc_.get(), d_tod_,
+                   bstart_d_.get(), nb, noba_short_, nsamp_, bw_.get(), wamap_.get(),
+                   (int)ndeg_shift_, (int)nloc_, yba_.get(), nna_.get());
+  }
+  nna_host_.resize(nb);
+  MADAM_CUDA(cudaMemcpyAsync(nna_host_.data(), nna_.get(), nb * sizeof(double),
+                             cudaMemcpyDeviceToHost, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+}
+
+namespace {
+// psd_index (noise_routines.f90:193-208)
+int psd_index_global(const std::vector<int> &psddet, const std::vector<double> &start,
+                     const std::vector<double> &stop, long det, double t) {
+  for (size_t i = 0; i < psddet.size(); ++i)
+    if (psddet[i] == det && start[i] <= t && stop[i] >= t) return (int)i;
+  return -1;
+}
+}  // namespace
+
+void Engine::build_segments() {
+  // trim_interval (noise_routines.f90:764-813) over every (det, period)
+  segs_.clear();
+  const long gapmin = (long)(60 * par_.fsample / dnshort_ + 1);
+  const long long nb = (long long)ndet_ * noba_short_;
+  std::vector<uint8_t> rm(nb, 0);
+  for (long d = 0; d < ndet_; ++d) {
+    const double *nna = nna_host_.data() + d * noba_short_;
+    for (long iv = 0; iv < ninterval_; ++iv) {
+      long ks = kstart_pp_[iv], kstop = ks + noba_pp_[iv];
+      const int pf = par_.kfilter ? psd_index_global(psddet_, psdstart_, psdstop_, d, btime_[ks])
+                                  : -1;
+      int isub = 0;
+      for (;;) {
+        long noba = 0;
+        bool allz = true;
+        for (long k = ks; k < kstop; ++k)
+          if (nna[k] != 0) { allz = false; break; }
+        if (!allz) {
+          while (ks < kstop && nna[ks] == 0) ++ks;
+          while (kstop > ks && nna[kstop - 1] == 0) --kstop;
+          noba = kstop - ks;
+          long gap = 0;
+          for (long i = ks; i < kstop; ++i) {
+            if (nna[i] != 0) gap = 0;
+            else if (++gap == gapmin) {
+              noba = (i + 1) - gap - ks;
+              break;
+            }
+          }
+        }
+        if (noba == 0) break;
+        Segment s;
+        s.det = (int)d;
+        s.iv = (int)iv;
+        s.isub = isub++;
+        s.k0 = d * noba_short_ + ks;
+        s.noba = noba;
+        s.psd_filter = pf;
+        s.psd_prec = par_.kfilter ? psd_index_global(psddet_, psdstart_, psdstop_, d, btime_[ks])
+                                  : -1;
+        const int ipd = psd_index_det(dets_[d], btime_[ks]);
+        s.prec_ok = (ipd >= 0 && dets_[d].weights[ipd] != 0) ? 1 : 0;
+        segs_.push_back(s);
+        for (long k = 0; k < noba; ++k) rm[s.k0 + k] = 1;
+        ks += noba;
+      }
+    }
+  }
+  rmask_.alloc(nb);
+  MADAM_CUDA(cudaMemcpyAsync(rmask_.get(), rm.data(), nb, cudaMemcpyHostToDevice, st_));
+  // convolve_interval segments (noise_routines.f90:816-857)
+  filt_segs_.clear();
+  for (const Segment &s : segs_) {
+    if (s.psd_filter < 0) continue;
+    if (s.noba > 2147483647L) fail("segment too long");
+    ConvSeg c;
+    c.x_off = s.k0;
+    c.y_off = s.k0;
+    c.n_in = (int)s.noba;
+    c.n_out = (int)s.noba;
+    c.spec = s.psd_filter;
+    c.flags = 3;
+    filt_segs_.push_back(c);
+  }
+  filt_segs_d_.alloc(std::max<size_t>(1, filt_segs_.size()));
+  if (!filt_segs_.empty())
+    MADAM_CUDA(cudaMemcpyAsync(filt_segs_d_.get(), filt_segs_.data(),
+                               filt_segs_.size() * sizeof(ConvSeg), cudaMemcpyHostToDevice, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+}
+
+void Engine::build_filter() {
+  // init_filter (noise_routines.f90:242-292) + build_filter (367-739)
+  if (!par_.kfilter) return;
+  long nof_min = 2 * noba_pp_max_;
+  if (par_.precond_width_max > nof_min - 1) nof_min = par_.precond_width_max + 1;
+  long nof = 1;
+  while (nof < nof_min) nof *= 2;
+  nof_ = std::max(4L, nof);
+  npsdtot_ = 0;
+  for (auto &d : dets_) npsdtot_ += d.npsd;
+  const long nh = nof_ / 2 + 1;
+  fcov_host_.assign((size_t)nh * npsdtot_, 0.0);
+  psddet_.assign(npsdtot_, 0);
+  psdstart_.assign(npsdtot_, 0.0);
+  psdstop_.assign(npsdtot_, 0.0);
+  std::vector<std::pair<long, int>> tasks;
+  for (long d = 0; d < ndet_; ++d) {
+    if (!dets_[d].has_psd) fail("All detectors must have at least one PSD to build the filter");
+    for (int ip = 0; ip < dets_[d].npsd; ++ip) tasks.push_back({d, ip});
+  }
+  const double fa = par_.fsample / (double)nshort_;
+  const double kPi = 3.141592653589793238462643383279502884197;
+  std::string err;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long it = 0; it < (long)tasks.size(); ++it) {
+    try {
+      const long d = tasks[it].first;
+      const int ip = tasks[it].second;
+      Detector &det = dets_[d];
+      psddet_[it] = (int)d;
+      psdstart_[it] = det.psdstarts[ip];
+      psdstop_[it] = (ip < det.npsd - 1) ? det.psdstarts[ip + 1] : fsp(1e30f);
+      const double sigma = det.sigmas[ip];
+      std::vector<double> aspec(nh, 0.0), f(nof_), g(nof_), spec(nof_);
+      for (int k = 0; k <= 2; ++k) {
+        for (long i = 0; i < nof_; ++i) f[i] = k * fa + (double)i * fa / (double)nof_;
+        // get_spectrum_interp (noise_routines.f90:638-737)
+        interpolate_psd(det.psdfreqs, det.psds[ip], f.data(), spec.data(), nof_);
+        double plateau;
+        if (par_.noise_weights_from_psd) {
+          plateau = det.plateaus[ip];
+        } else {
+          if (par_.radiometers) {
+            const double ff = par_.fsample / 2;
+            interpolate_psd(det.psdfreqs, det.psds[ip], &ff, &plateau, 1);
+          } else {
+            std::vector<double> fr(1000), dt(1000);
+            for (int i = 0; i < 1000; ++i) fr[i] = 1 + (double)(i * 10) / 1000;
+            interpolate_psd(det.psdfreqs, det.psds[ip], fr.data(), dt.data(), 1000);
+            plateau = *std::min_element(dt.begin(), dt.end());
+          }
+          det.sigmas[ip] = std::sqrt(plateau * par_.fsample);
+        }
+        const double margin = par_.radiometers ? fsp(1e-6f) : fsp(1e-3f);
+        bool anyneg = false;
+        for (long i = 0; i < nof_; ++i) {
+          spec[i] = (spec[i] > plateau * (1 + margin)) ? spec[i] - plateau : spec[i] * margin;
+          if (spec[i] <= 0) anyneg = true;
+        }
+        if (anyneg) {
+          for (long i = 0; i < nof_; ++i) {
+            if (spec[i] <= 0) {
+              bool found = false;
+              for (long j = i + 1; j < nof_; ++j)
+                if (spec[j] > 0) { spec[i] = spec[j]; found = true; break; }
+              if (found) continue;
+            }
+            if (spec[i] <= 0)
+              for (long j = i - 1; j >= 0; --j)
+                if (spec[j] > 0) { spec[i] = spec[j]; break; }
+          }
+        }
+        if (f[0] == 0) spec[0] = 0;
+        for (long i = 0; i < nof_; ++i) {
+          const double x = kPi * f[i] / fa;
+          g[i] = (x < fsp(1e-30f)) ? 1.0 : std::sin(x) * std::sin(x) / (x * x);
+        }
+        if (k == 0) aspec[0] = spec[0];
+        else aspec[0] = aspec[0] + 2 * spec[0] * g[0];
+        for (long i = 1; i < nh; ++i)
+          aspec[i] = aspec[i] + spec[i] * g[i] + spec[nof_ - i] * g[nof_ - i];
+      }
+      for (long i = 0; i < nh; ++i)
+        aspec[i] = (std::fabs(aspec[i]) > sigma * fsp(1e-30f)) ? 1.0 / (fa * aspec[i]) : 0.0;
+      aspec[0] = 0;
+      for (long i = 0; i < nh; ++i) {
+        if (std::isnan(aspec[i])) fail("NaN in fcov. Check input PSD and sigma.");
+        fcov_host_[(size_t)it * nh + i] = aspec[i];
+      }
+    } catch (const std::exception &e) {
+#pragma omp critical
+      err = e.what();
+    }
+  }
+  if (!err.empty()) fail(err);
+  fcov_.alloc(fcov_host_.size());
+  MADAM_CUDA(cudaMemcpyAsync(fcov_.get(), fcov_host_.data(), fcov_host_.size() * sizeof(double),
+                             cudaMemcpyHostToDevice, st_));
+  fft_.reset(new FFTPlan(nof_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+}
+
+void Engine::construct_preconditioner() {
+  // construct_preconditioner (noise_routines.f90:920-1153)
+  band_segs_.clear();
+  cg_prec_segs_.clear();
+  band_widths_.clear();
+  n_band_fail_ = 0;
+  use_diagonal_ = false;
+  const long long nb = (long long)ndet_ * noba_short_;
+  if (par_.precond_width_max < 1) return;
+  if (!par_.kfilter || par_.precond_width_max == 1) {
+    use_diagonal_ = true;
+    std::vector<double> pd(nb, 0.0);
+    for (long d = 0; d < ndet_; ++d)
+      for (long iv = 0; iv < ninterval_; ++iv) {
+        const long ks = kstart_pp_[iv];
+        const int ipd = psd_index_det(dets_[d], btime_[ks]);
+        for (long k = ks; k < ks + noba_pp_[iv]; ++k) {
+          const size_t o = d * noba_short_ + k;
+          if (ipd < 0) pd[o] = 1.;
+          else if (nna_host_[o] == 0) pd[o] = 1. / dets_[d].weights[ipd];
+          else pd[o] = 1. / nna_host_[o];
+        }
+      }
+    prec_diag_.alloc(nb);
+    MADAM_CUDA(cudaMemcpyAsync(prec_diag_.get(), pd.data(), nb * sizeof(double),
+                               cudaMemcpyHostToDevice, st_));
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    return;
+  }
+  const long nh = nof_ / 2 + 1;
+  {
+    std::vector<double> fp((size_t)nh * npsdtot_);
+    long ip = 0;
+    for (long d = 0; d < ndet_; ++d)
+      for (int k = 0; k < dets_[d].npsd; ++k, ++ip)
+        for (long i = 0; i < nh; ++i)
+          fp[(size_t)ip * nh + i] =
+              1.0 / ((double)nshort_ * dets_[d].weights[k] + fcov_host_[(size_t)ip * nh + i]);
+    fprec_.alloc(fp.size());
+    MADAM_CUDA(cudaMemcpyAsync(fprec_.get(), fp.data(), fp.size() * sizeof(double),
+                               cudaMemcpyHostToDevice, st_));
+  }
+  if (par_.use_fprecond) {
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    return;
+  }
+  // invcov = c2r(fcov): convolution of a unit impulse without mean removal
+  invcov_.alloc((size_t)nof_ * npsdtot_);
+  delta_.alloc(1);
+  const double one = 1.0;
+  MADAM_CUDA(cudaMemcpyAsync(delta_.get(), &one, sizeof one, cudaMemcpyHostToDevice, st_));
+  std::vector<ConvSeg> ic(npsdtot_);
+  for (long ip = 0; ip < npsdtot_; ++ip) {
+    ic[ip].x_off = 0;
+    ic[ip].y_off = ip * nof_;
+    ic[ip].n_in = 1;
+    ic[ip].n_out = (int)nof_;
+    ic[ip].spec = (int)ip;
+    ic[ip].flags = 0;
+  }
+  convolve(delta_.get(), invcov_.get(), ic, fcov_.get(), tmp_segs_d_);
+  invcov_host_.resize((size_t)nof_ * npsdtot_);
+  MADAM_CUDA(cudaMemcpyAsync(invcov_host_.data(), invcov_.get(),
+                             invcov_host_.size() * sizeof(double), cudaMemcpyDeviceToHost, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  // candidate segments
+  std::vector<int> cand;
+  for (int i = 0; i < (int)segs_.size(); ++i) {
+    const Segment &s = segs_[i];
+    if (s.psd_prec == -1) continue;  // nothing is built (preconditioning falls back to CG)
+    cand.push_back(i);
+  }
+  if (par_.use_cgprecond) {
+    for (int i : cand) cg_prec_segs_.push_back(i);
+    return;
+  }
+  const double plim = (double)(1.0f - 1e-5f);
+  struct Try { int seg; long nband; int tr; };
+  std::vector<Try> todo;
+  for (int i : cand) {
+    const Segment &s = segs_[i];
+    const double *icv = invcov_host_.data() + (size_t)s.psd_prec * nof_;
+    double p_tot = 0;
+    for (long k = 0; k < nof_ / 2; ++k) p_tot += icv[k] * icv[k];
+    long tr = 1, nband = 0;
+    bool ok = false;
+    for (;;) {
+      nband = std::min(s.noba, tr * par_.precond_width_min);
+      nband = std::min(nband, par_.precond_width_max);
+      double pp = 0;
+      for (long k = 0; k < nband; ++k) pp += icv[k] * icv[k];
+      if (pp > plim * p_tot) { ok = true; break; }
+      if (nband == s.noba || nband == par_.precond_width_max) break;
+      if (tr == 1000) break;
+      ++tr;
+    }
+    if (ok) todo.push_back({i, nband, (int)tr});
+    else {
+      cg_prec_segs_.push_back(i);
+      ++n_band_fail_;
+    }
+  }
+  // factor; segments that are not positive definite get a wider band
+  // (noise_routines.f90:1092-1120).  Band widths up to kBand2MaxWidth use the
+  // deduplicated factor (band2.cu), wider ones the plain column store.
+  struct Done2 { int seg; PSeg ps; size_t round; int nu, nr; };
+  struct Done1 { int seg; BandSeg bs; size_t round; };
+  std::vector<std::unique_ptr<DevBuf<double>>> rows_r;
+  std::vector<std::unique_ptr<DevBuf<PRun>>> runs_r;
+  std::vector<std::unique_ptr<DevBuf<double>>> band_r;
+  std::vector<Done2> done2;
+  std::vector<Done1> done1;
+  while (!todo.empty()) {
+    std::vector<Try> t2, t1, next;
+    for (const Try &t : todo) (t.nband <= kBand2MaxWidth ? t2 : t1).push_back(t);
+    std::vector<int> stat2, stat1, nu2, nr2;
+    std::vector<PSeg> ps(t2.size());
+    std::vector<BandSeg> bs(t1.size());
+    if (!t2.empty()) {
+      std::vector<int> spec(t2.size());
+      long long roff = 0;
+      int runoff = 0;
+      for (size_t t = 0; t < t2.size(); ++t) {
+        const Segment &sg = segs_[t2[t].seg];
+        ps[t] = PSeg{sg.k0, roff, (int)sg.noba, (int)t2[t].nband, runoff, 0, 0, 0};
+        spec[t] = sg.psd_prec;
+        roff += (long long)sg.noba * t2[t].nband;
+        runoff += (int)sg.noba;
+      }
+      DevBuf<PSeg> dps;
+      DevBuf<int> dspec, dstat, dnu, dnr;
+      rows_r.emplace_back(new DevBuf<double>());
+      runs_r.emplace_back(new DevBuf<PRun>());
+      rows_r.back()->alloc(std::max<long long>(1, roff));
+      runs_r.back()->alloc(std::max(1, runoff));
+      dps.alloc(ps.size());
+      dspec.alloc(ps.size());
+      dstat.alloc(ps.size());
+      dnu.alloc(ps.size());
+      dnr.alloc(ps.size());
+      MADAM_CUDA(cudaMemcpyAsync(dps.get(), ps.data(), ps.size() * sizeof(PSeg),
+                                 cudaMemcpyHostToDevice, st_));
+      MADAM_CUDA(cudaMemcpyAsync(dspec.get(), spec.data(), spec.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice, st_));
+      band2_factor(st_, dps.get(), (int)ps.size(), dspec.get(), invcov_.get(), nof_, nna_.get(),
+                   rows_r.back()->get(), runs_r.back()->get(), dstat.get(), dnu.get(), dnr.get());
+      stat2.resize(ps.size());
+      nu2.resize(ps.size());
+      nr2.resize(ps.size());
+      MADAM_CUDA(cudaMemcpyAsync(stat2.data(), dstat.get(), ps.size() * sizeof(int),
+                                 cudaMemcpyDeviceToHost, st_));
+      MADAM_CUDA(cudaMemcpyAsync(nu2.data(), dnu.get(), ps.size() * sizeof(int),
+                                 cudaMemcpyDeviceToHost, st_));
+      MADAM_CUDA(cudaMemcpyAsync(nr2.data(), dnr.get(), ps.size() * sizeof(int),
+                                 cudaMemcpyDeviceToHost, st_));
+      MADAM_CUDA(cudaStreamSynchronize(st_));
+    }
+    if (!t1.empty()) {
+      std::vector<int> spec(t1.size());
+      long long off = 0;
+      for (size_t t = 0; t < t1.size(); ++t) {
+        const Segment &sg = segs_[t1[t].seg];
+        bs[t] = BandSeg{sg.k0, off, (int)sg.noba, (int)t1[t].nband};
+        spec[t] = sg.psd_prec;
+        off += (long long)sg.noba * t1[t].nband;
+      }
+      DevBuf<BandSeg> dbs;
+      DevBuf<int> dspec, dstat;
+      band_r.emplace_back(new DevBuf<double>());
+      band_r.back()->alloc(off);
+      dbs.alloc(bs.size());
+      dspec.alloc(bs.size());
+      dstat.alloc(bs.size());
+      MADAM_CUDA(cudaMemcpyAsync(dbs.get(), bs.data(), bs.size() * sizeof(BandSeg),
+                                 cudaMemcpyHostToDevice, st_));
+      MADAM_CUDA(cudaMemcpyAsync(dspec.get(), spec.data(), spec.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice, st_));
+      band_factor(st_, dbs.get(), (int)bs.size(), dspec.get(), invcov_.get(), nof_, nna_.get(),
+                  band_r.back()->get(), dstat.get());
+      stat1.resize(bs.size());
+      MADAM_CUDA(cudaMemcpyAsync(stat1.data(), dstat.get(), stat1.size() * sizeof(int),
+                                 cudaMemcpyDeviceToHost, st_));
+      MADAM_CUDA(cudaStreamSynchronize(st_));
+    }
+    auto retry = [&](Try nt) {
+      const Segment &sg = segs_[nt.seg];
+      if (nt.tr == 1000 || nt.nband == sg.noba || nt.nband == par_.precond_width_max) {
+        cg_prec_segs_.push_back(nt.seg);
+        ++n_band_fail_;
+      } else {
+        ++nt.tr;
+        nt.nband = std::min(nt.nband + par_.precond_width_min, par_.precond_width_max);
+        next.push_back(nt);
+      }
+    };
+    for (size_t t = 0; t < t2.size(); ++t) {
+      if (stat2[t] == 0) {
+        done2.push_back({t2[t].seg, ps[t], rows_r.size() - 1, nu2[t], nr2[t]});
+        band_widths_.push_back(t2[t].nband);
+      } else {
+        retry(t2[t]);
+      }
+    }
+    for (size_t t = 0; t < t1.size(); ++t) {
+      if (stat1[t] == 0) {
+        done1.push_back({t1[t].seg, bs[t], band_r.size() - 1});
+        band_widths_.push_back(t1[t].nband);
+      } else {
+        retry(t1[t]);
+      }
+    }
+    todo.swap(next);
+  }
+  // pack the deduplicated factors the apply step uses (prec_ok segments)
+  std::vector<PSeg> pseg;
+  std::vector<PRun> pruns;
+  long long nrows_total = 0;
+  std::vector<std::pair<const Done2 *, long long>> copies;
+  for (const Done2 &dn : done2) {
+    if (!segs_[dn.seg].prec_ok) continue;
+    std::vector<PRun> rl(dn.nr);
+    MADAM_CUDA(cudaMemcpy(rl.data(), runs_r[dn.round]->get() + dn.ps.run_off,
+                          dn.nr * sizeof(PRun), cudaMemcpyDeviceToHost));
+    PSeg q = dn.ps;
+    q.row_off = nrows_total;
+    q.run_off = (int)pruns.size();
+    q.nrun = dn.nr;
+    for (PRun r : rl) {
+      r.row_off = r.row_off - dn.ps.row_off + nrows_total;
+      pruns.push_back(r);
+    }
+    copies.push_back({&dn, nrows_total});
+    nrows_total += (long long)dn.nu * dn.ps.nb;
+    pseg.push_back(q);
+  }
+  p2rows_.alloc(std::max<long long>(1, nrows_total));
+  for (auto &cp : copies)
+    MADAM_CUDA(cudaMemcpyAsync(p2rows_.get() + cp.second, rows_r[cp.first->round]->get() +
+                                                              cp.first->ps.row_off,
+                               (size_t)cp.first->nu * cp.first->ps.nb * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st_));
+  // chunks and transfer matrices
+  std::vector<PChunk> chunks;
+  std::vector<PTrans> trans;
+  std::map<std::tuple<long long, int, int>, long long> tcache;
+  long long toff = 0;
+  for (size_t si = 0; si < pseg.size(); ++si) {
+    PSeg &q = pseg[si];
+    const int w = q.nb - 1;
+    const int C = kBand2Chunk;
+    q.nch = (q.n + C - 1) / C;
+    q.ch_off = (int)chunks.size();
+    auto run_of = [&](int row) {
+      int lo = q.run_off, hi = q.run_off + q.nrun - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (pruns[mid].start <= row) lo = mid;
+        else hi = mid - 1;
+      }
+      return lo;
+    };
+    for (int c = 0; c < q.nch; ++c) {
+      PChunk k;
+      k.seg = (int)si;
+      k.a = c * C;
+      k.b = std::min(q.n, k.a + C);
+      k.run = run_of(k.a);
+      k.run_hi = run_of(std::min(k.b + w, q.n) - 1);
+      k.first = c == 0;
+      k.last = c == q.nch - 1;
+      k.tf = k.tb = 0;
+      if (!k.first && !k.last && w > 0) {
+        const int ci = (int)chunks.size();
+        const bool steady_f = run_of(k.b - 1) == k.run && k.b - k.a == C;
+        const bool steady_b = k.run_hi == k.run && k.b - k.a == C && k.b + w <= q.n;
+        for (int dir = 0; dir < 2; ++dir) {
+          const bool steady = dir == 0 ? steady_f : steady_b;
+          long long off = -1;
+          std::tuple<long long, int, int> key{pruns[k.run].row_off, dir, q.nb};
+          if (steady) {
+            auto it = tcache.find(key);
+            if (it != tcache.end()) off = it->second;
+          }
+          if (off < 0) {
+            off = toff;
+            toff += (long long)w * w;
+            trans.push_back({ci, dir, off});
+            if (steady) tcache[key] = off;
+          }
+          (dir == 0 ? k.tf : k.tb) = (int)off;
+        }
+      }
+      chunks.push_back(k);
+    }
+  }
+  if (toff >= (1LL << 31)) fail("too many band transfer matrices");
+  p2nseg_ = (int)pseg.size();
+  p2nch_ = (int)chunks.size();
+  p2segs_.alloc(std::max<size_t>(1, pseg.size()));
+  p2runs_.alloc(std::max<size_t>(1, pruns.size()));
+  p2ch_.alloc(std::max<size_t>(1, chunks.size()));
+  p2T_.alloc(std::max<long long>(1, toff));
+  p2wp_.alloc((size_t)std::max(1, p2nch_) * 128);
+  p2ws_.alloc((size_t)std::max(1, p2nch_) * 128);
+  if (!pseg.empty()) {
+    MADAM_CUDA(cudaMemcpyAsync(p2segs_.get(), pseg.data(), pseg.size() * sizeof(PSeg),
+                               cudaMemcpyHostToDevice, st_));
+    MADAM_CUDA(cudaMemcpyAsync(p2runs_.get(), pruns.data(), pruns.size() * sizeof(PRun),
+                               cudaMemcpyHostToDevice, st_));
+    MADAM_CUDA(cudaMemcpyAsync(p2ch_.get(), chunks.data(), chunks.size() * sizeof(PChunk),
+                               cudaMemcpyHostToDevice, st_));
+    DevBuf<PTrans> dtr;
+    dtr.alloc(std::max<size_t>(1, trans.size()));
+    if (!trans.empty()) {
+      MADAM_CUDA(cudaMemcpyAsync(dtr.get(), trans.data(), trans.size() * sizeof(PTrans),
+                                 cudaMemcpyHostToDevice, st_));
+      band2_transfer(st_, p2segs_.get(), p2ch_.get(), dtr.get(), (int)trans.size(),
+                     p2runs_.get(), p2rows_.get(), p2T_.get());
+    }
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+  }
+  band2_rows_ = nrows_total;
+  band2_ntrans_ = (long)trans.size();
+  // plain column store for the wide bands
+  long long total = 0;
+  band_segs_.clear();
+  std::vector<const Done1 *> keep;
+  for (const Done1 &dn : done1) {
+    if (!segs_[dn.seg].prec_ok) continue;
+    BandSeg b = dn.bs;
+    b.l_off = total;
+    total += (long long)b.n * b.nband;
+    band_segs_.push_back(b);
+    keep.push_back(&dn);
+  }
+  band_.alloc(std::max<long long>(1, total));
+  for (size_t j = 0; j < keep.size(); ++j)
+    MADAM_CUDA(cudaMemcpyAsync(band_.get() + band_segs_[j].l_off,
+                               band_r[keep[j]->round]->get() + keep[j]->bs.l_off,
+                               (size_t)band_segs_[j].n * band_segs_[j].nband * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st_));
+  band_segs_d_.alloc(std::max<size_t>(1, band_segs_.size()));
+  if (!band_segs_.empty())
+    MADAM_CUDA(cudaMemcpyAsync(band_segs_d_.get(), band_segs_.data(),
+                               band_segs_.size() * sizeof(BandSeg), cudaMemcpyHostToDevice, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  // segments without a factor that the apply step reaches use the CG fallback
+  std::vector<int> cgk;
+  for (int i : cg_prec_segs_)
+    if (segs_[i].prec_ok) cgk.push_back(i);
+  cg_prec_segs_ = cgk;
+}
+
+void Engine::finish_dots(int nd, int mode, int slot0) {
+  MADAM_LAUNCH(k_finish, 1, 1024, 0, st_, part_.get(), kRedBlocks, nd, scal_.get(), mode, slot0);
+}
+
+void Engine::scatter_baselines(const double *pw, double *target, bool fine) {
+  if (nwork_ == 0) return;
+  const int T = 1 << tile_shift_;
+  const int deg = fine ? 0 : (int)ndeg_shift_;
+  const int tilec = std::max(1, T >> deg);
+  const size_t smem = (size_t)tilec * nmap_ * sizeof(double);
+  if (nmap_ == 3)
+    MADAM_LAUNCH(k_scatter<3>, (unsigned)nwork_, 256, smem, st_, item_begin_.get(),
+                 item_tile_.get(), runs_.get(), point4_.get(), pixc_.get(), pw, fdn_, tile_shift_,
+                 deg, tilec, target);
+  else
+    MADAM_LAUNCH(k_scatter<1>, (unsigned)nwork_, 256, smem, st_, item_begin_.get(),
+                 item_tile_.get(), runs_.get(), point4_.get(), pixc_.get(), pw, fdn_, tile_shift_,
+                 deg, tilec, target);
+}
+
+void Engine::convolve(const double *x, double *y, const std::vector<ConvSeg> &segs,
+                      const double *spectra, DevBuf<ConvSeg> &dsegs) {
+  if (segs.empty()) return;
+  if (dsegs.n < segs.size()) dsegs.alloc(segs.size());
+  MADAM_CUDA(cudaMemcpyAsync(dsegs.get(), segs.data(), segs.size() * sizeof(ConvSeg),
+                             cudaMemcpyHostToDevice, st_));
+  fft_->convolve(st_, dsegs.get(), (long)segs.size(), spectra, x, y);
+}
+
+void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) {
+  const long long nb = (long long)ndet_ * noba_short_;
+  // 1) baseline -> map, collect, ccmultiply, scatter back (iterate_a 798-827)
+  MADAM_CUDA(cudaMemsetAsync(lmap_.get(), 0, lmap_.n * sizeof(double), st_));
+  if (timed) MADAM_CUDA(cudaEventRecord(ev_[0], st_));
+  scatter_baselines(pw, lmap_.get(), false);
+  if (timed) MADAM_CUDA(cudaEventRecord(ev_[1], st_));
+  if (nloc_cross_ > 0) {
+    if (nmap_ == 3)
+      MADAM_LAUNCH(k_ccmult<3>, grid_for(nloc_cross_), 256, 0, st_, cca_.get(), lmap_.get(),
+                   (long long)nloc_cross_);
+    else
+      MADAM_LAUNCH(k_ccmult<1>, grid_for(nloc_cross_), 256, 0, st_, cca_.get(), lmap_.get(),
+                   (long long)nloc_cross_);
+  }
+  // 2) noise prior: ap = C_a^-1 p (cinvmul, 829-845)
+  if (timed) MADAM_CUDA(cudaEventRecord(ev_[2], st_));
+  if (par_.kfilter) {
+    MADAM_CUDA(cudaMemcpyAsync(ap, p, nb * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+    if (!filt_segs_.empty())
+      fft_->convolve(st_, filt_segs_d_.get(), (long)filt_segs_.size(), fcov_.get(), p, ap);
+  } else if (par_.diagfilter != 0) {
+    MADAM_LAUNCH(k_diagfilter, grid_for(nb), 256, 0, st_, ap, nna_.get(), p, par_.diagfilter, nb);
+  } else {
+    MADAM_CUDA(cudaMemsetAsync(ap, 0, nb * sizeof(double), st_));
+  }
+  if (timed) MADAM_CUDA(cudaEventRecord(ev_[3], st_));
+  // 3) map -> baseline and p.ap (849-878)
+  if (nmap_ == 3)
+    MADAM_LAUNCH(k_gather<3>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
+                 bstart_d_.get(), nb, noba_short_, nsamp_, bw_.get(), p, nna_.get(), lmap_.get(),
+                 (int)ndeg_shift_, (int)nloc_, rmask_.get(), ap, part_.get());
+  else
+    MADAM_LAUNCH(k_gather<1>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
+                 bstart_d_.get(), nb, noba_short_, nsamp_, bw_.get(), p, nna_.get(), lmap_.get(),
+                 (int)ndeg_shift_, (int)nloc_, rmask_.get(), ap, part_.get());
+  finish_dots(1, 1, 0);
+  if (timed) MADAM_CUDA(cudaEventRecord(ev_[4], st_));
+}
+
+void Engine::cg_preconditioner_segments(const double *r, double *z) {
+  if (cg_prec_segs_.empty()) return;
+  const long long nb = (long long)ndet_ * noba_short_;
+  if (!cgp_) cgp_.reset(new CgpWork());
+  CgpWork &w = *cgp_;
+  if (w.nseg != (long)cg_prec_segs_.size()) {
+    std::vector<CgpSeg> hs;
+    w.hcsegs.clear();
+    for (int i : cg_prec_segs_) {
+      const Segment &s = segs_[i];
+      hs.push_back({s.k0, (int)s.noba, s.psd_prec});
+      ConvSeg c;
+      c.x_off = s.k0;
+      c.y_off = s.k0;
+      c.n_in = (int)s.noba;
+      c.n_out = (int)s.noba;
+      c.spec = s.psd_prec;
+      c.flags = 3;
+      w.hcsegs.push_back(c);
+    }
+    w.nseg = (long)hs.size();
+    w.segs.alloc(hs.size());
+    MADAM_CUDA(cudaMemcpyAsync(w.segs.get(), hs.data(), hs.size() * sizeof(CgpSeg),
+                               cudaMemcpyHostToDevice, st_));
+    w.csegs.alloc(w.hcsegs.size());
+    MADAM_CUDA(cudaMemcpyAsync(w.csegs.get(), w.hcsegs.data(), w.hcsegs.size() * sizeof(ConvSeg),
+                               cudaMemcpyHostToDevice, st_));
+    for (auto *b : {&w.x, &w.resid, &w.prop, &w.aprop, &w.zres, &w.prec}) b->alloc(nb);
+    w.st.alloc(4 * w.nseg);
+    w.done.alloc(w.nseg);
+    w.active.alloc(1);
+  }
+  const unsigned ns = (unsigned)w.nseg;
+  MADAM_LAUNCH(k_cgp_init, ns, 256, 0, st_, w.segs.get(), r, w.x.get(), w.resid.get(),
+               w.prop.get(), w.zres.get(), w.prec.get(), nna_.get(), invcov_.get(),
+               (long long)nof_, w.st.get(), w.done.get());
+  for (int iter = 1; iter <= 100; ++iter) {
+    fft_->convolve(st_, w.csegs.get(), w.nseg, fcov_.get(), w.prop.get(), w.aprop.get());
+    MADAM_CUDA(cudaMemsetAsync(w.active.get(), 0, sizeof(int), st_));
+    MADAM_LAUNCH(k_cgp_step, ns, 256, 0, st_, w.segs.get(), w.x.get(), w.resid.get(),
+                 w.prop.get(), w.aprop.get(), w.zres.get(), w.prec.get(), nna_.get(), w.st.get(),
+                 w.done.get(), iter, w.active.get());
+    int active = 0;
+    MADAM_CUDA(cudaMemcpyAsync(&active, w.active.get(), sizeof(int), cudaMemcpyDeviceToHost, st_));
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    if (active == 0) break;
+  }
+  MADAM_LAUNCH(k_copy_seg, ns, 256, 0, st_, w.segs.get(), w.x.get(), z);
+}
+
+void Engine::apply_preconditioner(const double *r, double *z) {
+  // preconditioning_band (noise_routines.f90:1159-1256)
+  const long long nb = (long long)ndet_ * noba_short_;
+  if (par_.precond_width_max < 1) {
+    MADAM_CUDA(cudaMemcpyAsync(z, r, nb * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+    return;
+  }
+  if (use_diagonal_) {
+    MADAM_LAUNCH(k_mul, grid_for(nb), 256, 0, st_, z, r, prec_diag_.get(), nb);
+    return;
+  }
+  MADAM_CUDA(cudaMemcpyAsync(z, r, nb * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+  if (par_.use_fprecond) {
+    if (!filt_segs_.empty())
+      fft_->convolve(st_, filt_segs_d_.get(), (long)filt_segs_.size(), fprec_.get(), r, z);
+    return;
+  }
+  band2_solve(st_, p2segs_.get(), p2nseg_, p2ch_.get(), p2nch_, p2runs_.get(), p2rows_.get(),
+              p2T_.get(), r, z, p2wp_.get(), p2ws_.get());
+  band_solve(st_, band_segs_d_.get(), (int)band_segs_.size(), band_.get(), r, z);
+  cg_preconditioner_segments(r, z);
+}
+
+void Engine::iterate() {
+  // iterate_a (smadam_routines.f90:677-983)
+  const double t0 = now_ms();
+  const long long nb = (long long)ndet_ * noba_short_;
+  for (auto *b : {&r_, &p_, &z_, &ap_, &ro_, &pw_}) b->alloc(nb);
+  part_.alloc(3 * kRedBlocks);
+  scal_.alloc(S_NSCAL);
+  scal_.zero(st_);
+  lmap_.alloc((size_t)std::max<long>(1, nloc_cross_) * nmap_);
+  MADAM_CUDA(cudaMemcpyAsync(r_.get(), yba_.get(), nb * sizeof(double), cudaMemcpyDeviceToDevice,
+                             st_));
+  aa_.zero(st_);
+  apply_preconditioner(r_.get(), z_.get());
+  MADAM_LAUNCH(k_update_p, grid_for(nb), 256, 0, st_, p_.get(), z_.get(), pw_.get(), bw_.get(),
+               nb, scal_.get(), 1);
+  MADAM_LAUNCH(k_dots, kRedBlocks, 256, 0, st_, r_.get(), z_.get(), r_.get(), r_.get(), nullptr,
+               nullptr, 2, rmask_.get(), nb, part_.get());
+  finish_dots(2, 0, S_RZ);
+  scal_host_.assign(S_NSCAL, 0.0);
+  MADAM_CUDA(cudaMemcpyAsync(scal_host_.data(), scal_.get(), S_NSCAL * sizeof(double),
+                             cudaMemcpyDeviceToHost, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  const double rzinit = scal_host_[S_RZ];
+  rrinit = scal_host_[S_RR];
+  rr_final = 1.0;
+  noiter = 0;
+  if (rzinit < fsp(1e-30f) || std::isnan(rzinit)) {
+    timings.iterate_ms = now_ms() - t0;
+    return;
+  }
+  long istep = 0;
+  float tm[4];
+  while (istep < par_.iter_max) {
+    ++istep;
+    apply_A(p_.get(), pw_.get(), ap_.get(), true);
+    MADAM_LAUNCH(k_update_ar, grid_for(nb), 256, 0, st_, aa_.get(), r_.get(), ro_.get(), p_.get(),
+                 ap_.get(), nb, scal_.get());
+    MADAM_CUDA(cudaEventRecord(ev_[5], st_));
+    apply_preconditioner(r_.get(), z_.get());
+    MADAM_CUDA(cudaEventRecord(ev_[6], st_));
+    MADAM_LAUNCH(k_dots, kRedBlocks, 256, 0, st_, r_.get(), z_.get(), ro_.get(), z_.get(),
+                 r_.get(), r_.get(), 3, rmask_.get(), nb, part_.get());
+    finish_dots(3, 2, 0);
+    MADAM_CUDA(cudaMemcpyAsync(scal_host_.data(), scal_.get(), S_NSCAL * sizeof(double),
+                               cudaMemcpyDeviceToHost, st_));
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    MADAM_CUDA(cudaEventElapsedTime(&tm[0], ev_[0], ev_[1]));
+    MADAM_CUDA(cudaEventElapsedTime(&tm[1], ev_[2], ev_[3]));
+    MADAM_CUDA(cudaEventElapsedTime(&tm[2], ev_[3], ev_[4]));
+    MADAM_CUDA(cudaEventElapsedTime(&tm[3], ev_[5], ev_[6]));
+    timings.scatter_ms += tm[0];
+    timings.filter_ms += tm[1];
+    timings.gather_ms += tm[2];
+    timings.precond_ms += tm[3];
+    const double rz = scal_host_[S_RZ], rr = scal_host_[S_RR];
+    rr_history.push_back(rr / rrinit);
+    rr_final = rr / rrinit;
+    noiter = istep;
+    if (rr / rrinit > 1e3) fail("CG is diverging");
+    if (rr / rrinit < par_.cglimit && istep > par_.iter_min) break;
+    if (rz == 0) break;
+    MADAM_LAUNCH(k_update_p, grid_for(nb), 256, 0, st_, p_.get(), z_.get(), pw_.get(), bw_.get(),
+                 nb, scal_.get(), 0);
+  }
+  // iterate_a leaves wamap holding the last A.p map (collect_map + ccmultiply
+  // on wamap, smadam_routines.f90:818-822); destripe_with_cache adds the new
+  // binned map onto it (smadam.F90:719-732)
+  if (istep > 0)
+    MADAM_CUDA(cudaMemcpyAsync(wamap_.get(), lmap_.get(), wamap_.n * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  timings.iterate_ms = now_ms() - t0;
+}
+
+void Engine::subtract_baselines() {
+  // subtract_baselines_a (smadam_routines.f90:1489-1539)
+  const long long nb = (long long)ndet_ * noba_short_;
+  tmpv_.alloc(nb);
+  MADAM_LAUNCH(k_scale_neg, grid_for(nb), 256, 0, st_, aa_.get(), bw_.get(), tmpv_.get(), nb);
+  lmap_fine_.alloc((size_t)std::max<long>(1, nloc_) * nmap_);
+  lmap_fine_.zero(st_);
+  scatter_baselines(tmpv_.get(), lmap_fine_.get(), true);
+  const long long nv = (long long)nloc_ * nmap_;
+  if (nv > 0) MADAM_LAUNCH(k_add, grid_for(nv), 256, 0, st_, map_.get(), lmap_fine_.get(), nv);
+}
+
+void Engine::clean_tod() {
+  // clean_tod (smadam_routines.f90:1545-1585)
+  if (!par_.write_tod && par_.ndetset == 0 && par_.nsurvey == 0) return;
+  if (!par_.kfirst || tod_cleaned_) return;
+  const long long n = (long long)ndet_ * nsamp_;
+  const SampleMap sm = sample_map(istart_d_.get(), kstart_d_.get(), (int)ninterval_, nsamp_,
+                                  noba_short_, fdn_);
+  if (n > 0) MADAM_LAUNCH(k_clean_tod, grid_for(n), 256, 0, st_, d_tod_, n, sm, aa_.get());
+  tod_cleaned_ = true;
+}
+
+void Engine::finalize(bool first_call) {
+  if (par_.kfirst) subtract_baselines();
+  const long long nm = nloc_;
+  if (first_call) {
+    // invert_pixelmatrix_map (map_routines.f90:218-321)
+    mask_.alloc(std::max<long long>(1, nm));
+    mask_.zero(st_);
+    crit_.alloc(std::max<long long>(1, nm));
+    crit_.zero(st_);
+    MatrixRules mr{(int)par_.pixmode_map, par_.pixlim_map, par_.allow_decoupling ? 1 : 0,
+                   par_.incomplete_matrices ? 1 : 0};
+    if (nm > 0) {
+      if (nmap_ == 3)
+        MADAM_LAUNCH(k_invert_map<3>, grid_for(nm), 128, 0, st_, cc_.get(), nm, mr, mask_.get(),
+                     crit_.get());
+      else
+        MADAM_LAUNCH(k_invert_map<1>, grid_for(nm), 128, 0, st_, cc_.get(), nm, mr, mask_.get(),
+                     crit_.get());
+    }
+  }
+  // makemaps (map_routines.f90:327-357)
+  if (nm > 0) {
+    for (double *m : {binmap_.get(), map_.get()}) {
+      if (nmap_ == 3) MADAM_LAUNCH(k_ccmult<3>, grid_for(nm), 256, 0, st_, cc_.get(), m, nm);
+      else MADAM_LAUNCH(k_ccmult<1>, grid_for(nm), 256, 0, st_, cc_.get(), m, nm);
+      if (par_.rm_monopole) {
+        part_.alloc(std::max<size_t>(part_.n, 3 * kRedBlocks));
+        scal_.alloc(std::max<size_t>(scal_.n, S_NSCAL));
+        MADAM_LAUNCH(k_monopole, kRedBlocks, 256, 0, st_, m, mask_.get(), nm, nmap_, part_.get());
+        finish_dots(2, 0, 8);
+        MADAM_LAUNCH(k_sub_monopole, grid_for(nm), 256, 0, st_, m, mask_.get(), nm, nmap_,
+                     scal_.get() + 8);
+      }
+    }
+  }
+  clean_tod();
+  writeback_host();
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+}
+
+void Engine::writeback_host() {
+  // restore_pixels (pointing.f90:168-191): the caller's pixel buffer shows the
+  // reference's edits (flagged samples become 12 nside_max^2)
+  const long long n = (long long)ndet_ * nsamp_;
+  if (n == 0) return;
+  DevBuf<int> sub2;
+  sub2.alloc(nosubmaps_tot_ + 1);
+  std::vector<int> s2(subtable2_.begin(), subtable2_.end());
+  MADAM_CUDA(cudaMemcpyAsync(sub2.get(), s2.data(), s2.size() * sizeof(int),
+                             cudaMemcpyHostToDevice, st_));
+  const long long cap = std::max<long long>(1024, n / 16);
+  DevBuf<long long> idx;
+  DevBuf<int32_t> val;
+  DevBuf<unsigned long long> cnt;
+  idx.alloc(cap);
+  val.alloc(cap);
+  cnt.alloc(1);
+  cnt.zero(st_);
+  MADAM_LAUNCH(k_restore, grid_for(n), 256, 0, st_, pix_.get(), pix_orig_.get(), n, sub2.get(),
+               (int)nosubpix_max_, in_device_ ? d_pix_caller_ : (int32_t *)nullptr, idx.get(),
+               val.get(), cnt.get(), cap);
+  if (!in_device_) {
+    unsigned long long c = 0;
+    MADAM_CUDA(cudaMemcpyAsync(&c, cnt.get(), sizeof c, cudaMemcpyDeviceToHost, st_));
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    if ((long long)c <= cap) {
+      std::vector<long long> hi(c);
+      std::vector<int32_t> hv(c);
+      if (c) {
+        MADAM_CUDA(cudaMemcpyAsync(hi.data(), idx.get(), c * sizeof(long long),
+                                   cudaMemcpyDeviceToHost, st_));
+        MADAM_CUDA(cudaMemcpyAsync(hv.data(), val.get(), c * sizeof(int32_t),
+                                   cudaMemcpyDeviceToHost, st_));
+        MADAM_CUDA(cudaStreamSynchronize(st_));
+      }
+      for (size_t i = 0; i < c; ++i) h_pix_[hi[i]] = hv[i];
+    } else {
+      DevBuf<int32_t> fin;
+      fin.alloc(n);
+      MADAM_LAUNCH(k_restore, grid_for(n), 256, 0, st_, pix_.get(), (const int32_t *)nullptr, n,
+                   sub2.get(), (int)nosubpix_max_, fin.get(), idx.get(), val.get(), cnt.get(), 0LL);
+      MADAM_CUDA(cudaMemcpyAsync(h_pix_, fin.get(), n * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                 st_));
+    }
+    if (tod_cleaned_)
+      MADAM_CUDA(cudaMemcpyAsync(h_signal_, d_tod_, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                 st_));
+  }
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+}
+
+void Engine::run(const Params &par, std::vector<Detector> dets, long ndet, long nsamp, long nnz,
+                 double *timestamps, int32_t *pix, float *pixweights, double *signal,
+                 long nperiod, const long *periods, bool is_device) {
+  const double t0 = now_ms();
+  timings = Timings();
+  rr_history.clear();
+  noiter = 0;
+  rrinit = 0;
+  rr_final = 0;
+  par_ = par;
+  dets_ = std::move(dets);
+  ndet_ = ndet;
+  nsamp_ = nsamp;
+  nnz_ = nnz;
+  nmap_ = (int)nnz;
+  cached_ = false;
+  tod_cleaned_ = false;
+  cgp_.reset();
+  d_pix_caller_ = is_device ? pix : nullptr;
+  const long long n = (long long)ndet * nsamp;
+  bind_inputs(timestamps, pix, pixweights, signal, is_device, true);
+  // pixel range check (smadam.F90:156-171)
+  {
+    DevBuf<int> mm;
+    mm.alloc(2);
+    const int init[2] = {INT_MAX, INT_MIN};
+    MADAM_CUDA(cudaMemcpyAsync(mm.get(), init, sizeof init, cudaMemcpyHostToDevice, st_));
+    if (n > 0) MADAM_LAUNCH(k_minmax, grid_for(n), 256, 0, st_, pix_.get(), n, mm.get());
+    int out[2];
+    MADAM_CUDA(cudaMemcpyAsync(out, mm.get(), sizeof out, cudaMemcpyDeviceToHost, st_));
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    const long nside_max = std::max(par_.nside_map, par_.nside_cross);
+    if (n > 0 && out[0] < -1) fail("Too small pixel number");
+    if (n > 0 && (long)out[1] > 12 * nside_max * nside_max - 1) fail("Too large pixel number");
+  }
+  init_layout(nperiod, periods);
+  // baseline start times (baseline_times, parameter_control.f90:956-977)
+  btime_.assign(noba_short_, 0.0);
+  if (is_device) {
+    std::vector<double> all(nsamp);
+    MADAM_CUDA(cudaMemcpyAsync(all.data(), timestamps, nsamp * sizeof(double),
+                               cudaMemcpyDeviceToHost, st_));
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    for (long k = 0; k < noba_short_; ++k) btime_[k] = all[bstart_[k]];
+  } else {
+    for (long k = 0; k < noba_short_; ++k) btime_[k] = timestamps[bstart_[k]];
+  }
+  build_filter();
+  flag_and_compact(true);
+  build_runs();
+  setup_scatter();
+  if (par_.kfirst) {
+    map_side_setup();
+    initialize_a();
+    build_segments();
+    construct_preconditioner();
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    timings.setup_ms = now_ms() - t0;
+    iterate();
+  } else {
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    timings.setup_ms = now_ms() - t0;
+  }
+  const double tf = now_ms();
+  finalize(true);
+  timings.finalize_ms = now_ms() - tf;
+  if (par_.mcmode) cached_ = true;
+  timings.total_ms = now_ms() - t0;
+}
+
+void Engine::run_cached(long ndet, long nsamp, long nnz, double *timestamps, int32_t *pix,
+                        float *pixweights, double *signal, bool is_device) {
+  // destripe_with_cache (smadam.F90:593-918)
+  if (!cached_) fail("destripe_with_cache called with empty caches.");
+  if (par_.temperature_only && nnz != 1)
+    fail("temperature_only=T but pointing weights are polarized");
+  if (ndet != ndet_ || nsamp != nsamp_ || nnz != nnz_)
+    fail("destripe_with_cache: data shape differs from the cached call");
+  const double t0 = now_ms();
+  timings = Timings();
+  rr_history.clear();
+  noiter = 0;
+  tod_cleaned_ = false;
+  d_pix_caller_ = is_device ? pix : nullptr;
+  (void)timestamps;
+  bind_inputs(timestamps, pix, pixweights, signal, is_device, false);
+  flag_and_compact(false);
+  build_runs();
+  bin_tod(true);
+  if (par_.kfirst) {
+    std::vector<Segment> old = segs_;
+    initialize_a();
+    build_segments();
+    bool same = old.size() == segs_.size();
+    for (size_t i = 0; same && i < old.size(); ++i)
+      same = old[i].k0 == segs_[i].k0 && old[i].noba == segs_[i].noba;
+    if (!same) fail("destripe_with_cache: flagging differs from the cached call");
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    timings.setup_ms = now_ms() - t0;
+    iterate();
+  }
+  const double tf = now_ms();
+  finalize(false);
+  timings.finalize_ms = now_ms() - tf;
+  timings.total_ms = now_ms() - t0;
+}
+
+// --------------------------------------------------------------- results --
+namespace {
+enum RKind { RK_DOUBLE, RK_INT, RK_FLOAT, RK_LONG };
+}
+
+long Engine::result_size(const std::string &name) {
+  const long npm = 12 * par_.nside_map * par_.nside_map;
+  const long npc = 12 * par_.nside_cross * par_.nside_cross;
+  const long nb = ndet_ * noba_short_;
+  if (name == "map" || name == "binmap") return npm * nmap_;
+  if (name == "hits" || name == "mask" || name == "crit") return npm;
+  if (name == "cc") return npm * nmap_ * nmap_;
+  if (name == "cca") return npc * nmap_ * nmap_;
+  if (name == "aa" || name == "yba" || name == "nna") return nb;
+  if (name == "fcov") return (long)fcov_host_.size();
+  if (name == "invcov") return (long)invcov_host_.size();
+  if (name == "rr_history") return (long)rr_history.size();
+  if (name == "band_widths") return (long)band_widths_.size();
+  if (name == "scalars") return 16;
+  if (name == "timings") return 9;
+  return -1;
+}
+
+void Engine::result_copy(const std::string &name, void *dst, long nbytes) {
+  const long sz = result_size(name);
+  if (sz < 0) fail("unknown result: " + name);
+  auto need = [&](size_t elem) {
+    if ((size_t)nbytes < (size_t)sz * elem) fail("result buffer too small for " + name);
+  };
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  // expand compacted per-pixel arrays to the full sky
+  auto expand = [&](const void *dev, size_t elem, long per_pix, long nosubpix, void *out) {
+    const long nloc_pix = nolocmaps_ * nosubpix;
+    std::vector<char> h((size_t)nloc_pix * per_pix * elem);
+    if (nloc_pix)
+      MADAM_CUDA(cudaMemcpy(h.data(), dev, h.size(), cudaMemcpyDeviceToHost));
+    const long total = nosubmaps_tot_ * nosubpix;
+    std::memset(out, 0, (size_t)total * per_pix * elem);
+    for (long j = 0; j < nolocmaps_; ++j) {
+      const long g = j + subtable2_[j];
+      std::memcpy((char *)out + (size_t)g * nosubpix * per_pix * elem,
+                  h.data() + (size_t)j * nosubpix * per_pix * elem,
+                  (size_t)nosubpix * per_pix * elem);
+    }
+  };
+  auto sym = [&](const std::vector<double> &s6, long npix, double *out) {
+    for (long p = 0; p < npix; ++p) {
+      double *o = out + p * nmap_ * nmap_;
+      if (nmap_ == 1) {
+        o[0] = s6[p];
+        continue;
+      }
+      const double *c = &s6[p * 6];
+      o[0] = c[0]; o[1] = c[1]; o[2] = c[2];
+      o[3] = c[1]; o[4] = c[3]; o[5] = c[4];
+      o[6] = c[2]; o[7] = c[4]; o[8] = c[5];
+    }
+  };
+  const long ncc = nmap_ == 3 ? 6 : 1;
+  if (name == "map" || name == "binmap") {
+    need(sizeof(double));
+    expand(name == "map" ? map_.get() : binmap_.get(), sizeof(double), nmap_, nosubpix_map_, dst);
+  } else if (name == "hits") {
+    need(sizeof(int));
+    expand(hits_.get(), sizeof(int), 1, nosubpix_map_, dst);
+  } else if (name == "mask") {
+    need(sizeof(int));
+    expand(mask_.get(), sizeof(int), 1, nosubpix_map_, dst);
+  } else if (name == "crit") {
+    need(sizeof(float));
+    expand(crit_.get(), sizeof(float), 1, nosubpix_map_, dst);
+  } else if (name == "cc" || name == "cca") {
+    need(sizeof(double));
+    const bool cross = name == "cca";
+    const long nsp = cross ? nosubpix_cross_ : nosubpix_map_;
+    std::vector<double> s6((size_t)nosubmaps_tot_ * nsp * ncc);
+    expand(cross ? cca_.get() : cc_.get(), sizeof(double), ncc, nsp, s6.data());
+    sym(s6, nosubmaps_tot_ * nsp, (double *)dst);
+  } else if (name == "aa" || name == "yba" || name == "nna") {
+    need(sizeof(double));
+    const double *src = name == "aa" ? aa_.get() : name == "yba" ? yba_.get() : nna_.get();
+    if (sz) MADAM_CUDA(cudaMemcpy(dst, src, sz * sizeof(double), cudaMemcpyDeviceToHost));
+  } else if (name == "fcov") {
+    need(sizeof(double));
+    std::memcpy(dst, fcov_host_.data(), sz * sizeof(double));
+  } else if (name == "invcov") {
+    need(sizeof(double));
+    std::memcpy(dst, invcov_host_.data(), sz * sizeof(double));
+  } else if (name == "rr_history") {
+    need(sizeof(double));
+    std::memcpy(dst, rr_history.data(), sz * sizeof(double));
+  } else if (name == "band_widths") {
+    need(sizeof(long));
+    std::memcpy(dst, band_widths_.data(), sz * sizeof(long));
+  } else if (name == "scalars") {
+    need(sizeof(double));
+    const double v[16] = {(double)noiter, rrinit, rr_final, (double)nof_,
+                          (double)band_widths_.size(), (double)n_band_fail_, timings.iterate_ms,
+                          timings.total_ms, (double)nmap_, (double)noba_short_,
+                          (double)(12 * par_.nside_map * par_.nside_map), (double)nruns_,
+                          (double)nwork_, (double)nloc_, (double)segs_.size(),
+                          (double)cg_prec_segs_.size()};
+    std::memcpy(dst, v, sizeof v);
+  } else if (name == "timings") {
+    need(sizeof(double));
+    const double v[9] = {timings.setup_ms, timings.iterate_ms, timings.finalize_ms,
+                         timings.total_ms, timings.scatter_ms, timings.gather_ms,
+                         timings.filter_ms, timings.precond_ms, timings.other_ms};
+    std::memcpy(dst, v, sizeof v);
+  }
+}
+
+// K timed PCG iterations restarted from the solve's right-hand side.  The
+// solution of the last solve is kept.  out: [total_ms, ms_per_iter,
+// launches_per_iter, scatter_ms, filter_ms, gather_ms, precond_ms, update_ms]
+void Engine::bench_iterations(int warmup, int iters, std::vector<double> &out) {
+  if (!par_.kfirst || noba_short_ == 0) fail("no solve state to benchmark");
+  const long long nb = (long long)ndet_ * noba_short_;
+  DevBuf<double> aa_keep;
+  aa_keep.alloc(nb);
+  MADAM_CUDA(cudaMemcpyAsync(aa_keep.get(), aa_.get(), nb * sizeof(double),
+                             cudaMemcpyDeviceToDevice, st_));
+  auto restart = [&]() {
+    MADAM_CUDA(cudaMemcpyAsync(r_.get(), yba_.get(), nb * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st_));
+    aa_.zero(st_);
+    apply_preconditioner(r_.get(), z_.get());
+    MADAM_LAUNCH(k_update_p, grid_for(nb), 256, 0, st_, p_.get(), z_.get(), pw_.get(), bw_.get(),
+                 nb, scal_.get(), 1);
+    MADAM_LAUNCH(k_dots, kRedBlocks, 256, 0, st_, r_.get(), z_.get(), r_.get(), r_.get(), nullptr,
+                 nullptr, 2, rmask_.get(), nb, part_.get());
+    finish_dots(2, 0, S_RZ);
+  };
+  auto one = [&](bool timed) {
+    apply_A(p_.get(), pw_.get(), ap_.get(), timed);
+    MADAM_LAUNCH(k_update_ar, grid_for(nb), 256, 0, st_, aa_.get(), r_.get(), ro_.get(), p_.get(),
+                 ap_.get(), nb, scal_.get());
+    if (timed) MADAM_CUDA(cudaEventRecord(ev_[5], st_));
+    apply_preconditioner(r_.get(), z_.get());
+    if (timed) MADAM_CUDA(cudaEventRecord(ev_[6], st_));
+    MADAM_LAUNCH(k_dots, kRedBlocks, 256, 0, st_, r_.get(), z_.get(), ro_.get(), z_.get(),
+                 r_.get(), r_.get(), 3, rmask_.get(), nb, part_.get());
+    finish_dots(3, 2, 0);
+    MADAM_LAUNCH(k_update_p, grid_for(nb), 256, 0, st_, p_.get(), z_.get(), pw_.get(), bw_.get(),
+                 nb, scal_.get(), 0);
+    if (timed) MADAM_CUDA(cudaEventRecord(ev_[7], st_));
+  };
+  restart();
+  for (int i = 0; i < warmup; ++i) one(false);
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  cudaEvent_t a, b;
+  MADAM_CUDA(cudaEventCreate(&a));
+  MADAM_CUDA(cudaEventCreate(&b));
+  const unsigned long long l0 = g_kernel_launches;
+  MADAM_CUDA(cudaEventRecord(a, st_));
+  for (int i = 0; i < iters; ++i) one(false);
+  MADAM_CUDA(cudaEventRecord(b, st_));
+  MADAM_CUDA(cudaEventSynchronize(b));
+  const unsigned long long l1 = g_kernel_launches;
+  float total = 0;
+  MADAM_CUDA(cudaEventElapsedTime(&total, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  // per-phase breakdown on separate iterations
+  double sc = 0, fi = 0, ga = 0, pr = 0, up = 0;
+  const int nbrk = std::max(1, std::min(iters, 5));
+  for (int i = 0; i < nbrk; ++i) {
+    one(true);
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    float t[5];
+    MADAM_CUDA(cudaEventElapsedTime(&t[0], ev_[0], ev_[1]));
+    MADAM_CUDA(cudaEventElapsedTime(&t[1], ev_[2], ev_[3]));
+    MADAM_CUDA(cudaEventElapsedTime(&t[2], ev_[3], ev_[4]));
+    MADAM_CUDA(cudaEventElapsedTime(&t[3], ev_[5], ev_[6]));
+    MADAM_CUDA(cudaEventElapsedTime(&t[4], ev_[6], ev_[7]));
+    sc += t[0];
+    fi += t[1];
+    ga += t[2];
+    pr += t[3];
+    up += t[4];
+  }
+  MADAM_CUDA(cudaMemcpyAsync(aa_.get(), aa_keep.get(), nb * sizeof(double),
+                             cudaMemcpyDeviceToDevice, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  out = {total, total / std::max(1, iters), (double)(l1 - l0) / std::max(1, iters), sc / nbrk,
+         fi / nbrk, ga / nbrk, pr / nbrk, up / nbrk};
+}

@@ -1,0 +1,385 @@
+// Batched real-FFT convolution for sm_100a (see fft.cuh).
+//
+// A real vector of length nof is packed into N = nof/2 complex values
+// z[m] = x[2m] + i x[2m+1]; the complex transform is split N = R x C
+// (four-step: length-R column FFTs, twiddles w_N^{n2 k1}, length-C row
+// FFTs).  The spectrum is never transposed: the row pass holds rows k1 and
+// R-k1 together, which contain every conjugate pair (k, N-k) of the real
+// transform, so the real-spectrum split, the multiplication by H and the
+// re-packing for the inverse happen in shared memory between the forward and
+// the inverse row FFTs.  The inverse column pass then writes the real output.
+// Shared-memory FFTs are radix-2: decimation in time (bit-reversed load) for
+// the forward transforms and decimation in frequency (bit-reversed store) for
+// the inverse ones, so no separate permutation pass is needed.
+#include "engine.h"
+#include "fft.cuh"
+
+namespace madam {
+namespace {
+
+typedef double2 cplx;
+
+__device__ __forceinline__ cplx cmul(cplx a, cplx b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ cplx cconj(cplx a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ cplx cadd(cplx a, cplx b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ cplx csub(cplx a, cplx b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ cplx cscale(cplx a, double s) { return make_double2(a.x * s, a.y * s); }
+
+// exp(-2 pi i num / den) computed with sincospi for full double accuracy
+__device__ __forceinline__ cplx twiddle(long long num, long long den) {
+  long long r = num % den;
+  double s, c;
+  sincospi(-2.0 * (double)r / (double)den, &s, &c);
+  return make_double2(c, s);
+}
+
+__device__ __forceinline__ unsigned bitrev(unsigned v, int bits) {
+  return __brev(v) >> (32 - bits);
+}
+
+// table[j] = exp(-2 pi i j / L), j < L/2
+__device__ void fill_twiddles(cplx *table, int L) {
+  for (int j = threadIdx.x; j < L / 2; j += blockDim.x) table[j] = twiddle(j, L);
+}
+
+// nfft independent length-L transforms stored contiguously in s (s[f*L + i]),
+// input in bit-reversed order, output natural order; sign -1 forward.
+__device__ void fft_dit(cplx *s, int L, int nfft, const cplx *tw, bool inverse) {
+  const int half_total = nfft * (L / 2);
+  for (int len = 2; len <= L; len <<= 1) {
+    const int half = len >> 1, stride = L / len;
+    for (int b = threadIdx.x; b < half_total; b += blockDim.x) {
+      const int f = b / (L / 2), j = b % (L / 2);
+      const int g = j / half, pos = j % half;
+      const int i0 = f * L + g * len + pos, i1 = i0 + half;
+      cplx w = tw[pos * stride];
+      if (inverse) w = cconj(w);
+      const cplx t = cmul(s[i1], w), u = s[i0];
+      s[i0] = cadd(u, t);
+      s[i1] = csub(u, t);
+    }
+    __syncthreads();
+  }
+}
+
+// natural-order input, bit-reversed output
+__device__ void fft_dif(cplx *s, int L, int nfft, const cplx *tw, bool inverse) {
+  const int half_total = nfft * (L / 2);
+  for (int len = L; len >= 2; len >>= 1) {
+    const int half = len >> 1, stride = L / len;
+    for (int b = threadIdx.x; b < half_total; b += blockDim.x) {
+      const int f = b / (L / 2), j = b % (L / 2);
+      const int g = j / half, pos = j % half;
+      const int i0 = f * L + g * len + pos, i1 = i0 + half;
+      cplx w = tw[pos * stride];
+      if (inverse) w = cconj(w);
+      const cplx u = s[i0], v = s[i1];
+      s[i0] = cadd(u, v);
+      s[i1] = cmul(csub(u, v), w);
+    }
+    __syncthreads();
+  }
+}
+
+// Real-spectrum split of the packed transform for the pair (k, N-k), product
+// with the real spectrum H and re-packing for the inverse transform.
+// A = Z[k], B = Z[N-k]; on return A = Z'[k], B = Z'[N-k].  k == 0 handles
+// the DC / Nyquist pair (B is ignored and set equal to A).
+__device__ __forceinline__ void spectral_pair(cplx &A, cplx &B, long long k, long long N,
+                                              const double *H) {
+  if (k == 0) {
+    const double x0 = A.x + A.y, xn = A.x - A.y;
+    const double y0 = x0 * H[0], yn = xn * H[N];
+    A = make_double2(0.5 * (y0 + yn), 0.5 * (y0 - yn));
+    B = A;
+    return;
+  }
+  const cplx W = twiddle(k, 2 * N);  // exp(-i pi k / N)
+  const cplx Bc = cconj(B);
+  const cplx E = cscale(cadd(A, Bc), 0.5);
+  const cplx D = csub(A, Bc);
+  const cplx O = make_double2(0.5 * D.y, -0.5 * D.x);  // -i/2 (A - conj B)
+  const cplx WO = cmul(W, O);
+  const cplx Xk = cadd(E, WO);
+  const cplx Xnk = cconj(csub(E, WO));
+  const cplx Yk = cscale(Xk, H[k]);
+  const cplx Ynk = cscale(Xnk, H[N - k]);
+  // re-pack: Z'[k] = 1/2 (Yk + conj Ynk) + i/2 (Yk - conj Ynk) conj(W^k)
+  const cplx Wc = cconj(W);
+  const cplx e1 = cscale(cadd(Yk, cconj(Ynk)), 0.5);
+  const cplx o1 = cmul(cscale(csub(Yk, cconj(Ynk)), 0.5), Wc);
+  A = make_double2(e1.x - o1.y, e1.y + o1.x);
+  // Z'[N-k] uses conj(W^{N-k}) = -W^k
+  const cplx Wn = make_double2(-W.x, -W.y);
+  const cplx e2 = cscale(cadd(Ynk, cconj(Yk)), 0.5);
+  const cplx o2 = cmul(cscale(csub(Ynk, cconj(Yk)), 0.5), Wn);
+  B = make_double2(e2.x - o2.y, e2.y + o2.x);
+}
+
+__device__ __forceinline__ double seg_input(const double *x, const ConvSeg &sg, long long i,
+                                            double mean) {
+  return i < sg.n_in ? x[sg.x_off + i] - mean : 0.0;
+}
+
+// ---------------------------------------------------------------- means --
+__global__ void k_seg_mean_in(const ConvSeg *segs, const double *x, double *means) {
+  const ConvSeg sg = segs[blockIdx.x];
+  double v[1] = {0.0};
+  if (sg.flags & 1)
+    for (long long i = threadIdx.x; i < sg.n_in; i += blockDim.x) v[0] += x[sg.x_off + i];
+  block_sum<1>(v);
+  if (threadIdx.x == 0) means[blockIdx.x] = (sg.flags & 1) ? v[0] / sg.n_in : 0.0;
+}
+
+__global__ void k_seg_mean_out(const ConvSeg *segs, double *y) {
+  const ConvSeg sg = segs[blockIdx.x];
+  if (!(sg.flags & 2)) return;
+  double v[1] = {0.0};
+  for (long long i = threadIdx.x; i < sg.n_out; i += blockDim.x) v[0] += y[sg.y_off + i];
+  block_sum<1>(v);
+  __shared__ double m;
+  if (threadIdx.x == 0) m = v[0] / sg.n_out;
+  __syncthreads();
+  const double mm = m;
+  for (long long i = threadIdx.x; i < sg.n_out; i += blockDim.x) y[sg.y_off + i] -= mm;
+}
+
+// ------------------------------------------------------ single-CTA path --
+// One CTA per segment; N complex values in shared memory.
+__global__ void k_conv_small(const ConvSeg *segs, const double *spectra, long long spec_len,
+                             const double *x, double *y, const double *means, int N, int logN) {
+  extern __shared__ double2 sm[];
+  cplx *s = sm;
+  cplx *tw = sm + N;
+  const ConvSeg sg = segs[blockIdx.x];
+  const double mean = means[blockIdx.x];
+  fill_twiddles(tw, N);
+  for (int m = threadIdx.x; m < N; m += blockDim.x) {
+    const double a = seg_input(x, sg, 2LL * m, mean);
+    const double b = seg_input(x, sg, 2LL * m + 1, mean);
+    s[bitrev(m, logN)] = make_double2(a, b);
+  }
+  __syncthreads();
+  fft_dit(s, N, 1, tw, false);
+  const double *H = spectra + (long long)sg.spec * spec_len;
+  for (int k = threadIdx.x; k <= N / 2; k += blockDim.x) {
+    const int nk = (N - k) % N;
+    cplx A = s[k], B = s[nk];
+    spectral_pair(A, B, k, N, H);
+    s[k] = A;
+    if (nk != k) s[nk] = B;
+  }
+  __syncthreads();
+  fft_dif(s, N, 1, tw, true);
+  const double scale = 1.0 / (double)N;  // 1/nof times the factor 2 of the packing
+  for (int m = threadIdx.x; m < N; m += blockDim.x) {
+    const cplx v = s[bitrev(m, logN)];
+    const long long i0 = 2LL * m;
+    if (i0 < sg.n_out) y[sg.y_off + i0] = v.x * scale;
+    if (i0 + 1 < sg.n_out) y[sg.y_off + i0 + 1] = v.y * scale;
+  }
+}
+
+// ------------------------------------------------------- four-step path --
+// Pass 1: forward column FFTs (length R) of G adjacent columns, twiddled.
+__global__ void k_conv_cols_fwd(const ConvSeg *segs, const double *x, const double *means,
+                                double2 *work, int R, int logR, int C, int G) {
+  extern __shared__ double2 sm[];
+  cplx *s = sm;            // G columns x R
+  cplx *tw = sm + G * R;   // R/2
+  const int seg = blockIdx.y;
+  const ConvSeg sg = segs[seg];
+  const double mean = means[seg];
+  const int c0 = blockIdx.x * G;
+  fill_twiddles(tw, R);
+  for (int e = threadIdx.x; e < G * R; e += blockDim.x) {
+    const int c = e % G, n1 = e / G;
+    const long long m = (long long)C * n1 + c0 + c;
+    const double a = seg_input(x, sg, 2 * m, mean);
+    const double b = seg_input(x, sg, 2 * m + 1, mean);
+    s[c * R + bitrev(n1, logR)] = make_double2(a, b);
+  }
+  __syncthreads();
+  fft_dit(s, R, G, tw, false);
+  const long long N = (long long)R * C;
+  double2 *W = work + (long long)seg * N;
+  for (int e = threadIdx.x; e < G * R; e += blockDim.x) {
+    const int c = e % G, k1 = e / G;
+    const int n2 = c0 + c;
+    W[(long long)k1 * C + n2] = cmul(s[c * R + k1], twiddle((long long)n2 * k1, N));
+  }
+}
+
+// Pass 2: forward row FFTs of rows k1 and R-k1, spectral product, inverse
+// row FFTs, inverse twiddles.
+__global__ void k_conv_rows(const ConvSeg *segs, const double *spectra, long long spec_len,
+                            double2 *work, int R, int C, int logC) {
+  extern __shared__ double2 sm[];
+  cplx *tw = sm;               // C/2
+  cplx *s = sm + C / 2;        // 2 rows x C
+  const int seg = blockIdx.y;
+  const ConvSeg sg = segs[seg];
+  const long long N = (long long)R * C;
+  double2 *W = work + (long long)seg * N;
+  const int j = blockIdx.x;            // 0 .. R/2
+  const int ka = j, kb = (R - j) % R;  // row pair (equal for j = 0, R/2)
+  const int nrows = (ka == kb) ? 1 : 2;
+  fill_twiddles(tw, C);
+  for (int e = threadIdx.x; e < nrows * C; e += blockDim.x) {
+    const int r = e / C, n2 = e % C;
+    const int k1 = r ? kb : ka;
+    s[r * C + bitrev(n2, logC)] = W[(long long)k1 * C + n2];
+  }
+  __syncthreads();
+  fft_dit(s, C, nrows, tw, false);
+  const double *H = spectra + (long long)sg.spec * spec_len;
+  if (ka == 0) {
+    // row 0: (0, k2) <-> (0, C - k2)
+    for (int k2 = threadIdx.x; k2 <= C / 2; k2 += blockDim.x) {
+      const int p2 = (C - k2) % C;
+      cplx A = s[k2], B = s[p2];
+      spectral_pair(A, B, (long long)R * k2, N, H);
+      s[k2] = A;
+      if (p2 != k2) s[p2] = B;
+    }
+  } else if (ka == kb) {
+    // row R/2: (R/2, k2) <-> (R/2, C - 1 - k2)
+    for (int k2 = threadIdx.x; k2 < C / 2; k2 += blockDim.x) {
+      const int p2 = C - 1 - k2;
+      cplx A = s[k2], B = s[p2];
+      spectral_pair(A, B, ka + (long long)R * k2, N, H);
+      s[k2] = A;
+      s[p2] = B;
+    }
+  } else {
+    // rows ka, kb = R - ka: (ka, k2) <-> (kb, C - 1 - k2)
+    for (int k2 = threadIdx.x; k2 < C; k2 += blockDim.x) {
+      const int p2 = C - 1 - k2;
+      cplx A = s[k2], B = s[C + p2];
+      spectral_pair(A, B, ka + (long long)R * k2, N, H);
+      s[k2] = A;
+      s[C + p2] = B;
+    }
+  }
+  __syncthreads();
+  fft_dif(s, C, nrows, tw, true);
+  for (int e = threadIdx.x; e < nrows * C; e += blockDim.x) {
+    const int r = e / C, n2 = e % C;
+    const int k1 = r ? kb : ka;
+    const cplx v = s[r * C + bitrev(n2, logC)];
+    W[(long long)k1 * C + n2] = cmul(v, cconj(twiddle((long long)n2 * k1, N)));
+  }
+}
+
+// Pass 3: inverse column FFTs and real output.
+__global__ void k_conv_cols_inv(const ConvSeg *segs, const double2 *work, double *y, int R,
+                                int logR, int C, int G) {
+  extern __shared__ double2 sm[];
+  cplx *s = sm;
+  cplx *tw = sm + G * R;
+  const int seg = blockIdx.y;
+  const ConvSeg sg = segs[seg];
+  const int c0 = blockIdx.x * G;
+  const long long N = (long long)R * C;
+  const double2 *W = work + (long long)seg * N;
+  // rows n1 whose outputs are needed: 2 (C n1 + n2) < n_out
+  const int rows_needed = (int)min((long long)R, ((long long)sg.n_out + 2LL * C - 1) / (2LL * C));
+  fill_twiddles(tw, R);
+  for (int e = threadIdx.x; e < G * R; e += blockDim.x) {
+    const int c = e % G, k1 = e / G;
+    s[c * R + k1] = W[(long long)k1 * C + c0 + c];
+  }
+  __syncthreads();
+  fft_dif(s, R, G, tw, true);
+  const double scale = 1.0 / (double)N;
+  for (int e = threadIdx.x; e < G * rows_needed; e += blockDim.x) {
+    const int c = e % G, n1 = e / G;
+    const cplx v = s[c * R + bitrev(n1, logR)];
+    const long long m = (long long)C * n1 + c0 + c;
+    if (2 * m < sg.n_out) y[sg.y_off + 2 * m] = v.x * scale;
+    if (2 * m + 1 < sg.n_out) y[sg.y_off + 2 * m + 1] = v.y * scale;
+  }
+}
+
+int ilog2(long v) {
+  int l = 0;
+  while ((1L << l) < v) ++l;
+  return l;
+}
+
+}  // namespace
+
+FFTPlan::FFTPlan(long nof_) : nof(nof_), N(nof_ / 2) {
+  if (nof < 4 || (nof & (nof - 1))) fail("FFT length must be a power of two >= 4");
+  if (N > (1L << 24)) fail("FFT length too large");
+  if (N > 2048) {
+    int l = ilog2(N);
+    R = 1 << (l / 2);
+    C = (int)(N / R);
+    G = std::max(1, std::min(16, 4096 / R));
+    if (G > C) G = C;
+  }
+}
+
+FFTPlan::~FFTPlan() {
+  if (work) cudaFree(work);
+  if (means) cudaFree(means);
+}
+
+void FFTPlan::reserve(long nseg) {
+  if (nseg <= nseg_max) return;
+  if (work) cudaFree(work);
+  if (means) cudaFree(means);
+  work = nullptr;
+  means = nullptr;
+  if (R) MADAM_CUDA(cudaMalloc(&work, (size_t)nseg * N * sizeof(double2)));
+  MADAM_CUDA(cudaMalloc(&means, (size_t)nseg * sizeof(double)));
+  nseg_max = nseg;
+}
+
+void FFTPlan::convolve(cudaStream_t st, const ConvSeg *segs, long nseg, const double *spectra,
+                       const double *x, double *y) {
+  if (nseg == 0) return;
+  if (nseg > 65535) fail("too many filter segments in one batch");
+  reserve(nseg);
+  const long long spec_len = N + 1;
+  MADAM_LAUNCH(k_seg_mean_in, (unsigned)nseg, 256, 0, st, segs, x, means);
+  if (R == 0) {
+    const int logN = ilog2(N);
+    size_t smem = (size_t)(N + N / 2) * sizeof(double2);
+    static bool attr_small = false;
+    if (!attr_small) {
+      MADAM_CUDA(cudaFuncSetAttribute(k_conv_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      64 * 1024));
+      attr_small = true;
+    }
+    MADAM_LAUNCH(k_conv_small, (unsigned)nseg, 256, smem, st, segs, spectra, spec_len, x, y,
+                 means, (int)N, logN);
+  } else {
+    const int logR = ilog2(R), logC = ilog2(C);
+    size_t smem_cols = (size_t)(G * R + R / 2) * sizeof(double2);
+    size_t smem_rows = (size_t)(2 * C + C / 2) * sizeof(double2);
+    static bool attr = false;
+    if (!attr) {
+      MADAM_CUDA(cudaFuncSetAttribute(k_conv_cols_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      200 * 1024));
+      MADAM_CUDA(cudaFuncSetAttribute(k_conv_cols_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      200 * 1024));
+      MADAM_CUDA(cudaFuncSetAttribute(k_conv_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      200 * 1024));
+      attr = true;
+    }
+    dim3 gc(C / G, (unsigned)nseg), gr(R / 2 + 1, (unsigned)nseg);
+    MADAM_LAUNCH(k_conv_cols_fwd, gc, 256, smem_cols, st, segs, x, means, (double2 *)work, R, logR,
+                 C, G);
+    MADAM_LAUNCH(k_conv_rows, gr, 256, smem_rows, st, segs, spectra, spec_len, (double2 *)work, R, C,
+                 logC);
+    MADAM_LAUNCH(k_conv_cols_inv, gc, 256, smem_cols, st, segs, (const double2 *)work, y, R, logR,
+                 C, G);
+  }
+  MADAM_LAUNCH(k_seg_mean_out, (unsigned)nseg, 256, 0, st, segs, y);
+}
+
+}  // namespace madam

@@ -1,0 +1,102 @@
+"""The C-ABI boundary: symbols, loading, argument validation without a GPU."""
+import ctypes as ct
+import os
+import re
+
+import numpy as np
+import pytest
+
+import libmadam_b200
+from libmadam_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    names = []
+    for h in ("madam.h", "madam_b200.h"):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names += re.findall(r"\b([a-z_0-9]+)\s*\(", src)
+    return sorted(set(n for n in names if n not in ("if", "sizeof")))
+
+
+def test_library_builds_and_loads():
+    libmadam_b200.build()
+    L = _lib.load()
+    assert os.path.exists(_lib.LIB_PATH)
+    assert L is not None
+
+
+def test_every_declared_symbol_is_exported():
+    L = _lib.load()
+    names = _declared()
+    assert {"destripe", "destripe_with_cache", "clear_caches"} <= set(names)
+    for n in names:
+        assert hasattr(L, n), n
+
+
+def test_reference_symbols_have_c_linkage():
+    # the reference exports unmangled names (bind(c), smadam.F90:68,611,921)
+    out = os.popen("nm -D --defined-only " + _lib.LIB_PATH).read()
+    for n in ("destripe", "destripe_with_cache", "clear_caches"):
+        assert re.search(r"\bT {}\b".format(n), out), n
+
+
+def test_fastdiv_selftest():
+    assert _lib.load().madam_b200_selftest_fastdiv() == 0
+
+
+def test_parameter_errors_are_reported_not_aborted():
+    from libmadam_b200 import libmadam_wrapper as W
+    d = np.zeros(4)
+    with pytest.raises(RuntimeError, match="Unknown parameter: bogus_key"):
+        W.destripe(None, {"bogus_key": 1}, ["a"], np.ones(1), np.zeros(4), np.zeros(4, np.int32),
+                   np.ones(4, np.float32), np.zeros(4), np.array([0]), np.ones(1, np.int64),
+                   np.zeros(1), np.array([1.0, 2.0]), np.ones(2))
+    with pytest.raises(RuntimeError, match="Failed to parse nside_map from x"):
+        W.destripe(None, {"nside_map": "x"}, ["a"], np.ones(1), np.zeros(4),
+                   np.zeros(4, np.int32), np.ones(4, np.float32), np.zeros(4), np.array([0]),
+                   np.ones(1, np.int64), np.zeros(1), np.array([1.0, 2.0]), np.ones(2))
+    with pytest.raises(RuntimeError, match="temperature_only=T but pointing weights are polarized"):
+        W.destripe(None, {"temperature_only": True}, ["a"], np.ones(1), np.zeros(4),
+                   np.zeros(4, np.int32), np.ones(12, np.float32), np.zeros(4), np.array([0]),
+                   np.ones(1, np.int64), np.zeros(1), np.array([1.0, 2.0]), np.ones(2))
+    status, msg = _lib.last_error()
+    assert status == 1 and "polarized" in msg
+    del d
+
+
+def test_destripe_with_cache_without_cache_fails():
+    from libmadam_b200 import libmadam_wrapper as W
+    W.clear_caches()
+    with pytest.raises(RuntimeError, match="empty caches"):
+        W.destripe_with_cache(None, np.zeros(4), np.zeros(4, np.int32), np.ones(4, np.float32),
+                              np.zeros(4), b"")
+
+
+def test_void_entry_points_do_not_abort():
+    L = _lib.load()
+    p = ct.c_void_p
+    z = np.zeros(8)
+    L.destripe.argtypes = [ct.c_int, ct.c_char_p, ct.c_long, ct.c_char_p, p, ct.c_long, ct.c_long,
+                           p, p, p, p, ct.c_long, p, p, ct.c_long, p, ct.c_long, p, ct.c_long, p]
+    ptr = z.ctypes.data_as(p)
+    per = np.zeros(1, np.int64)
+    L.destripe(0, b"nside_map = 3;", 1, b"d;", ptr, 4, 1, ptr, ptr, ptr, ptr, 1,
+               per.ctypes.data_as(p), per.ctypes.data_as(p), 1, ptr, 1, ptr, 1, ptr)
+    status, msg = _lib.last_error()
+    assert status == 1 and msg
+
+
+def test_no_cpu_fallback_without_gpu():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from libmadam_b200 import libmadam_wrapper as W
+    from libmadam_b200 import synthetic as syn
+    d = syn.to_numpy(syn.generate(syn.small_config(nsamp_obs=256, nobs=1)))
+    with pytest.raises(RuntimeError, match="CUDA"):
+        W.destripe(None, d["pars"], d["dets"], d["detweights"], d["timestamps"], d["pixels"],
+                   d["pixweights"], d["signal"], d["periods"], d["npsd"], d["psdstarts"],
+                   d["psdfreqs"], d["psdvals"])
