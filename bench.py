@@ -90,6 +90,11 @@ def config_for(name):
         return syn.config2(), "plain destripe nside512 16det x 4obs x 2^23 @100Hz IQU"
     if name == "1":
         return syn.config1(), "plain destripe nside64 4det x 2^20 @10Hz IQU"
+    if name == "mid":
+        cfg = syn.config2()
+        cfg.nobs = 1
+        cfg.nsamp_obs = 1 << 21
+        return cfg, "nside512 16det x 1obs x 2^21 @100Hz IQU (profiling size)"
     cfg = syn.small_config(ndet=4, nsamp_obs=1 << 18, nobs=2, nside=64, seed=5)
     return cfg, "small ring scan nside64 4det x 2 x 2^18"
 
@@ -195,7 +200,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="2", choices=["2", "1", "small"])
+    ap.add_argument("--config", default="2", choices=["2", "1", "mid", "small"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
@@ -231,6 +236,7 @@ def main():
     W.destripe(None, *common, d["timestamps"], pix, wts, sig, *psd)
     tim = W.timings()
     sca = W.scalars()
+    marks = W.setup_marks()
     noiter = int(sca["noiter"])
 
     # timed PCG iterations (the step)
@@ -311,6 +317,8 @@ def main():
             "time_to_cglimit_ms": tim["iterate_ms"], "iterations_to_cglimit": noiter,
             "destripe_device_ms": tim["total_ms"], "setup_ms": tim["setup_ms"],
             "phases_ms_per_iteration": phases, "generate_s": t_gen,
+            "setup_marks_ms": marks,
+            "band": {k: sca[k] for k in ("band_rows", "band_transfers", "band_chunks", "nseg")},
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -198,41 +198,67 @@ __global__ void k_band2_transfer(const PSeg *segs, const PChunk *ch, const PTran
 // State propagation across chunks, one warp per segment.
 // dir 0: s[c] = p[c] + T_c s[c-1] for c = c0+1 .. c0+n-2 (s[c0] = p[c0])
 // dir 1: s[c] = p[c] + T_c s[c+1] for c = c0+n-2 .. c0+1 (s[last] = p[last])
+// The particular states and transfer offsets of the next kScanBlock chunks are
+// staged in shared memory before the sequential steps, so a step waits only on
+// the w x w product.
+constexpr int kScanBlock = 16;
+constexpr int kScanWarps = 2;
+
 __global__ void k_band2_scan(const PSeg *segs, int nseg, const PChunk *ch, const double *T,
                              const double *p, double *s, int dir) {
-  const int seg = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  __shared__ double pbuf[kScanWarps][kScanBlock][kRing];
+  __shared__ double curb[kScanWarps][kRing];
+  __shared__ int toffb[kScanWarps][kScanBlock];
+  const int wl = threadIdx.x >> 5;
+  const int seg = blockIdx.x * kScanWarps + wl;
   const int lane = threadIdx.x & 31;
-  extern __shared__ double sh[];
-  double *cur = sh + (threadIdx.x >> 5) * kRing;
   if (seg >= nseg) return;
   const PSeg g = segs[seg];
   const int w = g.nb - 1;
-  if (g.nch <= 1) return;
+  if (g.nch <= 1 || w <= 0) return;
+  double *cur = curb[wl];
   const int c0 = g.ch_off, cl = g.ch_off + g.nch - 1;
   const int start = dir == 0 ? c0 : cl;
+  const int stop = dir == 0 ? cl : c0;  // exclusive
+  const int step = dir == 0 ? 1 : -1;
   for (int i = lane; i < w; i += 32) {
     const double v = p[(long long)start * kRing + i];
     cur[i] = v;
     s[(long long)start * kRing + i] = v;
   }
   __syncwarp();
-  const int step = dir == 0 ? 1 : -1;
-  for (int c = start + step; c != (dir == 0 ? cl : c0); c += step) {
-    const double *Tm = T + (dir == 0 ? ch[c].tf : ch[c].tb);
-    double v[4];
-    int ni = 0;
-    for (int i = lane; i < w; i += 32, ++ni) {
-      double acc = p[(long long)c * kRing + i];
-      for (int q = 0; q < w; ++q) acc += Tm[(long long)i * w + q] * cur[q];
-      v[ni] = acc;
+  for (int cb = start + step; cb != stop;) {
+    int nblk = 0;
+    for (int u = 0, c = cb; u < kScanBlock && c != stop; ++u, c += step) ++nblk;
+    for (int e = lane; e < nblk * w; e += 32) {
+      const int u = e / w, i = e - u * w;
+      pbuf[wl][u][i] = p[(long long)(cb + u * step) * kRing + i];
+    }
+    if (lane < nblk) {
+      const int c = cb + lane * step;
+      toffb[wl][lane] = dir == 0 ? ch[c].tf : ch[c].tb;
     }
     __syncwarp();
-    ni = 0;
-    for (int i = lane; i < w; i += 32, ++ni) {
-      cur[i] = v[ni];
-      s[(long long)c * kRing + i] = v[ni];
+    for (int u = 0; u < nblk; ++u) {
+      const double *Tm = T + toffb[wl][u];
+      double v[kRing / 32];
+      int ni = 0;
+      for (int i = lane; i < w; i += 32, ++ni) {
+        double acc = pbuf[wl][u][i];
+        const double *Ti = Tm + (long long)i * w;
+        for (int q = 0; q < w; ++q) acc += Ti[q] * cur[q];
+        v[ni] = acc;
+      }
+      __syncwarp();
+      ni = 0;
+      const long long c = cb + u * step;
+      for (int i = lane; i < w; i += 32, ++ni) {
+        cur[i] = v[ni];
+        s[c * kRing + i] = v[ni];
+      }
+      __syncwarp();
     }
-    __syncwarp();
+    cb += nblk * step;
   }
 }
 
@@ -257,18 +283,16 @@ void band2_solve(cudaStream_t st, const PSeg *segs, int nseg, const PChunk *ch, 
                  double *z, double *work_p, double *work_s) {
   if (nch == 0) return;
   const unsigned gc = (nch + 127) / 128;
-  const int wpb = 4;
-  const unsigned gs = (nseg + wpb - 1) / wpb;
-  const size_t shs = (size_t)wpb * kRing * sizeof(double);
+  const unsigned gs = (nseg + kScanWarps - 1) / kScanWarps;
   // forward: particular, state scan, final
   MADAM_LAUNCH(k_band2_fwd, gc, 128, 0, st, segs, ch, nch, runs, urows, r, nullptr, nullptr,
                work_p);
-  MADAM_LAUNCH(k_band2_scan, gs, 32 * wpb, shs, st, segs, nseg, ch, T, work_p, work_s, 0);
+  MADAM_LAUNCH(k_band2_scan, gs, 32 * kScanWarps, 0, st, segs, nseg, ch, T, work_p, work_s, 0);
   MADAM_LAUNCH(k_band2_fwd, gc, 128, 0, st, segs, ch, nch, runs, urows, r, work_s, z, nullptr);
   // backward, in place on z
   MADAM_LAUNCH(k_band2_bwd, gc, 128, 0, st, segs, ch, nch, runs, urows, z, nullptr, nullptr,
                work_p);
-  MADAM_LAUNCH(k_band2_scan, gs, 32 * wpb, shs, st, segs, nseg, ch, T, work_p, work_s, 1);
+  MADAM_LAUNCH(k_band2_scan, gs, 32 * kScanWarps, 0, st, segs, nseg, ch, T, work_p, work_s, 1);
   MADAM_LAUNCH(k_band2_bwd, gc, 128, 0, st, segs, ch, nch, runs, urows, z, work_s, z, nullptr);
 }
 

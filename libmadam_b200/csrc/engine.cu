@@ -22,6 +22,7 @@
 
 #include "engine.h"
 #include "fft.cuh"
+#include "fits.h"
 #include "kernels.cuh"
 #include "pixmat.cuh"
 #include "band2.cuh"
@@ -572,6 +573,199 @@ __global__ void k_gather(const float4 *p4, const int32_t *pc, const uint32_t *bs
   double v[1] = {pap};
   block_sum<1>(v);
   if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+
+// map_to_baseline, block-tiled: a CTA takes `kb` consecutive baselines of one
+// detector (<= kGatherTile samples), streams their samples once (coalesced
+// float4 loads, four independent loads in flight per thread), stages w.m per
+// sample in shared memory and sums each baseline with one warp.  Used when
+// every baseline is at most kGatherTile / 2 samples long.
+constexpr int kGatherTile = 2048;
+constexpr int kGatherUnroll = 4;
+constexpr int kScatterUnroll = 8;
+
+template <int NMAP>
+__device__ __forceinline__ double wm_sample(const float4 *__restrict__ p4,
+                                            const int32_t *__restrict__ pc,
+                                            const double *__restrict__ m, long long i,
+                                            int deg_shift, int nloc) {
+  if (NMAP == 3) {
+    const float4 q = __ldcs(p4 + i);
+    const int px = point_pix(q);
+    if (px >= nloc) return 0.0;
+    const double *mm = m + (long long)(px >> deg_shift) * 3;
+    return (double)q.x * mm[0] + (double)q.y * mm[1] + (double)q.z * mm[2];
+  } else {
+    const int px = __ldcs(pc + i);
+    if (px >= nloc) return 0.0;
+    return m[px >> deg_shift];
+  }
+}
+
+template <int NMAP>
+__global__ void __launch_bounds__(256) k_gather_tiled(
+    const float4 *__restrict__ p4, const int32_t *__restrict__ pc,
+    const uint32_t *__restrict__ bstart, long noba, long long nsamp, int kb,
+    long long ntiles_det, int ndet, const double *__restrict__ bw, const double *__restrict__ p,
+    const double *__restrict__ nna, const double *__restrict__ m, int deg_shift, int nloc,
+    const uint8_t *__restrict__ rmask, double *__restrict__ ap, double *__restrict__ part) {
+  __shared__ double vals[kGatherTile];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double pap = 0;
+  const long long ntiles = ntiles_det * ndet;
+  for (long long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const long long det = t / ntiles_det;
+    const long long k0 = (t - det * ntiles_det) * kb;
+    const long long k1 = min(k0 + kb, (long long)noba);
+    const int s0 = (int)bstart[k0], ns = (int)(bstart[k1] - bstart[k0]);
+    const long long base = det * nsamp + s0;
+    for (int u0 = threadIdx.x; u0 < ns; u0 += kGatherUnroll * blockDim.x) {
+      double v[kGatherUnroll];
+#pragma unroll
+      for (int r = 0; r < kGatherUnroll; ++r) {
+        const int u = u0 + r * blockDim.x;
+        v[r] = u < ns ? wm_sample<NMAP>(p4, pc, m, base + u, deg_shift, nloc) : 0.0;
+      }
+#pragma unroll
+      for (int r = 0; r < kGatherUnroll; ++r) {
+        const int u = u0 + r * blockDim.x;
+        if (u < ns) vals[u] = v[r];
+      }
+    }
+    __syncthreads();
+    for (long long k = k0 + wid; k < k1; k += nw) {
+      const long long b = det * noba + k;
+      const double detw = bw[b];
+      if (detw == 0) {
+        if (lane == 0 && rmask[b]) pap += p[b] * ap[b];
+        continue;
+      }
+      const int a0 = (int)(bstart[k] - s0), a1 = (int)(bstart[k + 1] - s0);
+      double apn = 0;
+      for (int i = a0 + lane; i < a1; i += 32) apn += vals[i];
+      apn = warp_sum(apn);
+      if (lane == 0) {
+        const double v = ap[b] + (nna[b] * p[b] - apn * detw);
+        ap[b] = v;
+        if (rmask[b]) pap += p[b] * v;
+      }
+    }
+    __syncthreads();
+  }
+  double v[1] = {pap};
+  block_sum<1>(v);
+  if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+
+// baseline_to_map (smadam_routines.f90:1074-1111) as a pixel-major gather:
+// the pointing is also stored sorted by cross pixel (time order inside a
+// pixel) as {w_I, w_Q, w_U, global baseline}; one warp sums a pixel's samples
+// and stores the pixel's value.  No atomics, deterministic.
+template <int NMAP>
+__global__ void __launch_bounds__(256) k_scatter_csr(
+    const int *__restrict__ off, long long npix, const float4 *__restrict__ sp4,
+    const int2 *__restrict__ sp2, const double *__restrict__ pw, double *__restrict__ target) {
+  const int lane = threadIdx.x & 31;
+  const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long p = w0; p < npix; p += nwarps) {
+    const int a = off[p], e = off[p + 1];
+    double acc0 = 0, acc1 = 0, acc2 = 0;
+    for (int i0 = a + lane; i0 < e; i0 += 32 * kScatterUnroll) {
+      if (NMAP == 3) {
+        float4 q[kScatterUnroll];
+#pragma unroll
+        for (int r = 0; r < kScatterUnroll; ++r) {
+          const int i = i0 + 32 * r;
+          q[r] = i < e ? __ldcs(sp4 + i) : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+        }
+        double v[kScatterUnroll];
+#pragma unroll
+        for (int r = 0; r < kScatterUnroll; ++r) {
+          const int k = __float_as_int(q[r].w);
+          v[r] = k >= 0 ? pw[k] : 0.0;
+        }
+#pragma unroll
+        for (int r = 0; r < kScatterUnroll; ++r) {
+          acc0 += (double)q[r].x * v[r];
+          acc1 += (double)q[r].y * v[r];
+          acc2 += (double)q[r].z * v[r];
+        }
+      } else {
+        int k[kScatterUnroll];
+#pragma unroll
+        for (int r = 0; r < kScatterUnroll; ++r) {
+          const int i = i0 + 32 * r;
+          k[r] = i < e ? __ldcs(&sp2[i].x) : -1;
+        }
+#pragma unroll
+        for (int r = 0; r < kScatterUnroll; ++r) acc0 += k[r] >= 0 ? pw[k[r]] : 0.0;
+      }
+    }
+    acc0 = warp_sum(acc0);
+    if (NMAP == 3) {
+      acc1 = warp_sum(acc1);
+      acc2 = warp_sum(acc2);
+    }
+    if (lane == 0) {
+      if (NMAP == 3) {
+        target[p * 3] = acc0;
+        target[p * 3 + 1] = acc1;
+        target[p * 3 + 2] = acc2;
+      } else {
+        target[p] = acc0;
+      }
+    }
+  }
+}
+
+// CSR construction: sort key (cross pixel, or nloc_cross for samples the
+// scatter skips) for every sample
+template <int NNZ>
+__global__ void k_csr_keys(const float4 *p4, const int32_t *pc, long long n, SampleMap sm,
+                           const double *bw, int nloc, int deg_shift, int sentinel, int *keys,
+                           uint32_t *vals, unsigned long long *nvalid) {
+  for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < n;
+       i0 += (long long)gridDim.x * blockDim.x) {
+    const long long i = i0 + threadIdx.x;
+    bool valid = false;
+    if (i < n) {
+      const long long det = i / sm.nsamp, s = i - det * sm.nsamp;
+      const int px = sample_pix<NNZ>(p4, pc, i);
+      const long long b = baseline_of(sm, det, s);
+      valid = px < nloc && bw[b] != 0.0;
+      keys[i] = valid ? (px >> deg_shift) : sentinel;
+      vals[i] = (uint32_t)i;
+    }
+    const unsigned ball = __ballot_sync(0xffffffffu, valid);
+    if ((threadIdx.x & 31) == 0 && ball) atomicAdd(nvalid, (unsigned long long)__popc(ball));
+  }
+}
+
+template <int NNZ>
+__global__ void k_csr_fill(const int *keys, const uint32_t *idx, long long nvalid,
+                           const float4 *p4, SampleMap sm, float4 *sp4, int2 *sp2, int *off) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nvalid;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long src = idx[i];
+    const long long det = src / sm.nsamp, s = src - det * sm.nsamp;
+    const int b = (int)baseline_of(sm, det, s);
+    if (NNZ == 3) {
+      const float4 q = p4[src];
+      sp4[i] = make_float4(q.x, q.y, q.z, __int_as_float(b));
+    } else {
+      sp2[i] = make_int2(b, 0);
+    }
+    const int key = keys[i];
+    const int prev = i == 0 ? -1 : keys[i - 1];
+    for (int p = prev + 1; p <= key; ++p) off[p] = (int)i;
+  }
+}
+
+__global__ void k_fill_int(int *a, long long n, int v) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    a[i] = v;
 }
 
 // masked dot products sum_i mask_i a_i b_i for up to 3 pairs

@@ -109,6 +109,7 @@ class Engine {
   void bench_iterations(int warmup, int iters, std::vector<double> &out);
 
   Timings timings;
+  double setup_marks_[9] = {0};
   long noiter = 0;
   double rrinit = 0, rr_final = 0;
   std::vector<double> rr_history;
@@ -121,6 +122,7 @@ class Engine {
   void init_layout(long nperiod, const long *periods);
   void flag_and_compact(bool first_call);
   void build_runs();
+  void build_csr();
   void setup_scatter();
   void map_side_setup();
   void initialize_a();
@@ -130,6 +132,7 @@ class Engine {
   void iterate();
   void finalize(bool first_call);
   void writeback_host();
+  void write_fits(bool first_call);
 
   // --- iteration pieces
   void apply_A(const double *p, const double *pw, double *ap, bool timed);
@@ -157,6 +160,8 @@ class Engine {
   long ninterval_ = 0, noba_short_ = 0, noba_pp_max_ = 0, nshort_ = 0;
   double dnshort_ = 0;
   FastDiv fdn_;
+  int gather_kb_ = 0;
+  long long gather_tiles_det_ = 0;
   std::vector<long> intervals_, istart_iv_, noba_pp_, kstart_pp_;
   std::vector<uint32_t> bstart_;  // noba_short + 1
   std::vector<double> btime_;
@@ -193,6 +198,10 @@ class Engine {
   DevBuf<int> item_begin_;   // nwork + 1 run offsets
   DevBuf<int> item_tile_;    // tile of each work item
   long nruns_ = 0, nwork_ = 0;
+  DevBuf<float4> sp4_;        // pixel-sorted pointing {w, baseline}
+  DevBuf<int2> sp2_;          // pixel-sorted baseline (temperature only)
+  DevBuf<int> csr_off_;       // nloc_cross + 1 offsets
+  long long csr_nvalid_ = 0;
   DevBuf<long long> istart_d_;
   DevBuf<int> kstart_d_;
   DevBuf<int32_t> pix_orig_;
@@ -206,6 +215,7 @@ class Engine {
   // baseline domain
   DevBuf<double> aa_, yba_, nna_, r_, p_, z_, ap_, ro_, pw_, tmpv_;
   std::vector<double> nna_host_;
+  std::vector<double> cc_raw_host_;
   DevBuf<double> part_, scal_;
   std::vector<double> scal_host_;
 

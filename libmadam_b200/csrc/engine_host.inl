@@ -239,6 +239,17 @@ void Engine::init_layout(long nperiod, const long *periods) {
     pos += last;
   }
   bstart_[m] = (uint32_t)pos;
+  // gather tiling: kb baselines per CTA tile when baselines are short
+  {
+    long maxlen = 0;
+    for (long k = 0; k < noba_short_; ++k) maxlen = std::max<long>(maxlen, bstart_[k + 1] - bstart_[k]);
+    gather_kb_ = 0;
+    if (maxlen > 0 && maxlen <= kGatherTile / 2) {
+      gather_kb_ = (int)std::max<long>(1, kGatherTile / maxlen);
+      gather_kb_ = std::min(gather_kb_, 256);
+      gather_tiles_det_ = (noba_short_ + gather_kb_ - 1) / gather_kb_;
+    }
+  }
   // every baseline but the last of a period has length dnshort
   const double dnc = std::min(dnshort_, 4294967295.0);
   fdn_ = FastDiv((uint32_t)std::max(1.0, dnc));
@@ -505,6 +516,68 @@ void Engine::build_runs() {
   MADAM_CUDA(cudaStreamSynchronize(st_));
   nruns_ = nr;
   nwork_ = ni;
+}
+
+void Engine::build_csr() {
+  // pixel-sorted copy of the pointing for the PCG scatter (k_scatter_csr)
+  const long long n = (long long)ndet_ * nsamp_;
+  csr_nvalid_ = 0;
+  csr_off_.alloc((size_t)nloc_cross_ + 1);
+  if (n == 0 || nloc_cross_ == 0) {
+    csr_off_.zero(st_);
+    return;
+  }
+  if (n >= (1LL << 31)) fail("too many samples for the pixel-sorted pointing");
+  const SampleMap sm = sample_map(istart_d_.get(), kstart_d_.get(), (int)ninterval_, nsamp_,
+                                  noba_short_, fdn_);
+  DevBuf<int> keys, keys_s;
+  DevBuf<uint32_t> vals, vals_s;
+  DevBuf<unsigned long long> cnt;
+  keys.alloc(n);
+  vals.alloc(n);
+  cnt.alloc(1);
+  cnt.zero(st_);
+  const int sentinel = (int)nloc_cross_;
+  if (nmap_ == 3)
+    MADAM_LAUNCH(k_csr_keys<3>, grid_for(n), 256, 0, st_, point4_.get(), pixc_.get(), n, sm,
+                 bw_.get(), (int)nloc_, (int)ndeg_shift_, sentinel, keys.get(), vals.get(),
+                 cnt.get());
+  else
+    MADAM_LAUNCH(k_csr_keys<1>, grid_for(n), 256, 0, st_, point4_.get(), pixc_.get(), n, sm,
+                 bw_.get(), (int)nloc_, (int)ndeg_shift_, sentinel, keys.get(), vals.get(),
+                 cnt.get());
+  unsigned long long nv = 0;
+  MADAM_CUDA(cudaMemcpyAsync(&nv, cnt.get(), sizeof nv, cudaMemcpyDeviceToHost, st_));
+  keys_s.alloc(n);
+  vals_s.alloc(n);
+  int endbit = 1;
+  while ((1L << endbit) <= sentinel) ++endbit;
+  size_t tmpb = 0;
+  MADAM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmpb, keys.get(), keys_s.get(), vals.get(),
+                                             vals_s.get(), (int)n, 0, endbit, st_));
+  DevBuf<uint8_t> tmp;
+  tmp.alloc(tmpb);
+  MADAM_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tmpb, keys.get(), keys_s.get(),
+                                             vals.get(), vals_s.get(), (int)n, 0, endbit, st_));
+  tmp.reset();
+  keys.reset();
+  vals.reset();
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  csr_nvalid_ = (long long)nv;
+  MADAM_LAUNCH(k_fill_int, grid_for(nloc_cross_ + 1), 256, 0, st_, csr_off_.get(),
+               (long long)nloc_cross_ + 1, (int)csr_nvalid_);
+  if (nmap_ == 3) {
+    sp4_.alloc(std::max<long long>(1, csr_nvalid_));
+    if (csr_nvalid_)
+      MADAM_LAUNCH(k_csr_fill<3>, grid_for(csr_nvalid_), 256, 0, st_, keys_s.get(), vals_s.get(),
+                   csr_nvalid_, point4_.get(), sm, sp4_.get(), (int2 *)nullptr, csr_off_.get());
+  } else {
+    sp2_.alloc(std::max<long long>(1, csr_nvalid_));
+    if (csr_nvalid_)
+      MADAM_LAUNCH(k_csr_fill<1>, grid_for(csr_nvalid_), 256, 0, st_, keys_s.get(), vals_s.get(),
+                   csr_nvalid_, point4_.get(), sm, (float4 *)nullptr, sp2_.get(), csr_off_.get());
+  }
+  MADAM_CUDA(cudaStreamSynchronize(st_));
 }
 
 void Engine::bin_tod(bool accumulate_wamap) {
@@ -1202,9 +1275,15 @@ void Engine::convolve(const double *x, double *y, const std::vector<ConvSeg> &se
 void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) {
   const long long nb = (long long)ndet_ * noba_short_;
   // 1) baseline -> map, collect, ccmultiply, scatter back (iterate_a 798-827)
-  MADAM_CUDA(cudaMemsetAsync(lmap_.get(), 0, lmap_.n * sizeof(double), st_));
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[0], st_));
-  scatter_baselines(pw, lmap_.get(), false);
+  if (nloc_cross_ > 0) {
+    if (nmap_ == 3)
+      MADAM_LAUNCH(k_scatter_csr<3>, kRedBlocks, 256, 0, st_, csr_off_.get(),
+                   (long long)nloc_cross_, sp4_.get(), sp2_.get(), pw, lmap_.get());
+    else
+      MADAM_LAUNCH(k_scatter_csr<1>, kRedBlocks, 256, 0, st_, csr_off_.get(),
+                   (long long)nloc_cross_, sp4_.get(), sp2_.get(), pw, lmap_.get());
+  }
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[1], st_));
   if (nloc_cross_ > 0) {
     if (nmap_ == 3)
@@ -1227,14 +1306,26 @@ void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) 
   }
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[3], st_));
   // 3) map -> baseline and p.ap (849-878)
-  if (nmap_ == 3)
+  if (gather_kb_ > 0) {
+    if (nmap_ == 3)
+      MADAM_LAUNCH(k_gather_tiled<3>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
+                   bstart_d_.get(), noba_short_, nsamp_, gather_kb_, gather_tiles_det_,
+                   (int)ndet_, bw_.get(), p, nna_.get(), lmap_.get(), (int)ndeg_shift_,
+                   (int)nloc_, rmask_.get(), ap, part_.get());
+    else
+      MADAM_LAUNCH(k_gather_tiled<1>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
+                   bstart_d_.get(), noba_short_, nsamp_, gather_kb_, gather_tiles_det_,
+                   (int)ndet_, bw_.get(), p, nna_.get(), lmap_.get(), (int)ndeg_shift_,
+                   (int)nloc_, rmask_.get(), ap, part_.get());
+  } else if (nmap_ == 3) {
     MADAM_LAUNCH(k_gather<3>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
                  bstart_d_.get(), nb, noba_short_, nsamp_, bw_.get(), p, nna_.get(), lmap_.get(),
                  (int)ndeg_shift_, (int)nloc_, rmask_.get(), ap, part_.get());
-  else
+  } else {
     MADAM_LAUNCH(k_gather<1>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
                  bstart_d_.get(), nb, noba_short_, nsamp_, bw_.get(), p, nna_.get(), lmap_.get(),
                  (int)ndeg_shift_, (int)nloc_, rmask_.get(), ap, part_.get());
+  }
   finish_dots(1, 1, 0);
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[4], st_));
 }
@@ -1412,6 +1503,11 @@ void Engine::clean_tod() {
 void Engine::finalize(bool first_call) {
   if (par_.kfirst) subtract_baselines();
   const long long nm = nloc_;
+  if (first_call && par_.do_matrix) {
+    // the pixel matrices before inversion (write_matrix(cc), smadam.F90:389)
+    cc_raw_host_.assign((size_t)12 * par_.nside_map * par_.nside_map * nmap_ * nmap_, 0.0);
+    result_copy("cc", cc_raw_host_.data(), (long)(cc_raw_host_.size() * sizeof(double)));
+  }
   if (first_call) {
     // invert_pixelmatrix_map (map_routines.f90:218-321)
     mask_.alloc(std::max<long long>(1, nm));
@@ -1447,6 +1543,46 @@ void Engine::finalize(bool first_call) {
   clean_tod();
   writeback_host();
   MADAM_CUDA(cudaStreamSynchronize(st_));
+  write_fits(first_call);
+}
+
+void Engine::write_fits(bool first_call) {
+  // write_map / write_binmap / write_mask / write_hits / write_matrix
+  // (smadam.F90:401-422, 756-764)
+  const bool any = par_.do_map || par_.do_binmap ||
+                   (first_call && (par_.do_hits || par_.do_mask || par_.do_matrix || par_.do_wcov));
+  if (!any) return;
+  const long npix = 12 * par_.nside_map * par_.nside_map;
+  std::vector<double> map((size_t)npix * nmap_), bin((size_t)npix * nmap_), ccinv;
+  std::vector<int> hits(npix), mask(npix);
+  std::vector<float> crit(npix);
+  result_copy("mask", mask.data(), (long)(mask.size() * sizeof(int)));
+  if (par_.do_map) result_copy("map", map.data(), (long)(map.size() * sizeof(double)));
+  if (par_.do_binmap) result_copy("binmap", bin.data(), (long)(bin.size() * sizeof(double)));
+  if (first_call) {
+    result_copy("hits", hits.data(), (long)(hits.size() * sizeof(int)));
+    result_copy("crit", crit.data(), (long)(crit.size() * sizeof(float)));
+    if (par_.do_wcov) {
+      ccinv.resize((size_t)npix * nmap_ * nmap_);
+      result_copy("cc", ccinv.data(), (long)(ccinv.size() * sizeof(double)));
+    }
+  }
+  FitsInput in;
+  in.par = &par_;
+  in.nosubpix_map = nosubpix_map_;
+  in.nosubmaps_tot = nosubmaps_tot_;
+  in.ndet = ndet_;
+  in.nmap = nmap_;
+  in.first_call = first_call;
+  in.map = par_.do_map ? map.data() : nullptr;
+  in.binmap = par_.do_binmap ? bin.data() : nullptr;
+  in.hits = hits.data();
+  in.mask = mask.data();
+  in.crit = crit.data();
+  in.cc_raw = cc_raw_host_.empty() ? nullptr : cc_raw_host_.data();
+  in.cc_inv = ccinv.empty() ? nullptr : ccinv.data();
+  write_products(in);
+  cc_raw_host_.clear();
 }
 
 void Engine::writeback_host() {
@@ -1547,15 +1683,29 @@ void Engine::run(const Params &par, std::vector<Detector> dets, long ndet, long 
   } else {
     for (long k = 0; k < noba_short_; ++k) btime_[k] = timestamps[bstart_[k]];
   }
+  auto mark = [&](int i) {
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    setup_marks_[i] = now_ms() - t0;
+  };
+  mark(0);
   build_filter();
+  mark(1);
   flag_and_compact(true);
+  mark(2);
   build_runs();
+  mark(3);
   setup_scatter();
+  mark(4);
+  if (par_.kfirst) build_csr();
+  mark(5);
   if (par_.kfirst) {
     map_side_setup();
     initialize_a();
+    mark(6);
     build_segments();
+    mark(7);
     construct_preconditioner();
+    mark(8);
     MADAM_CUDA(cudaStreamSynchronize(st_));
     timings.setup_ms = now_ms() - t0;
     iterate();
@@ -1589,6 +1739,7 @@ void Engine::run_cached(long ndet, long nsamp, long nnz, double *timestamps, int
   flag_and_compact(false);
   build_runs();
   bin_tod(true);
+  if (par_.kfirst) build_csr();
   if (par_.kfirst) {
     std::vector<Segment> old = segs_;
     initialize_a();
@@ -1625,8 +1776,9 @@ long Engine::result_size(const std::string &name) {
   if (name == "invcov") return (long)invcov_host_.size();
   if (name == "rr_history") return (long)rr_history.size();
   if (name == "band_widths") return (long)band_widths_.size();
-  if (name == "scalars") return 16;
+  if (name == "scalars") return 20;
   if (name == "timings") return 9;
+  if (name == "setup_marks") return 9;
   return -1;
 }
 
@@ -1703,13 +1855,17 @@ void Engine::result_copy(const std::string &name, void *dst, long nbytes) {
     std::memcpy(dst, band_widths_.data(), sz * sizeof(long));
   } else if (name == "scalars") {
     need(sizeof(double));
-    const double v[16] = {(double)noiter, rrinit, rr_final, (double)nof_,
+    const double v[20] = {(double)noiter, rrinit, rr_final, (double)nof_,
                           (double)band_widths_.size(), (double)n_band_fail_, timings.iterate_ms,
                           timings.total_ms, (double)nmap_, (double)noba_short_,
                           (double)(12 * par_.nside_map * par_.nside_map), (double)nruns_,
                           (double)nwork_, (double)nloc_, (double)segs_.size(),
-                          (double)cg_prec_segs_.size()};
+                          (double)cg_prec_segs_.size(), (double)band2_rows_,
+                          (double)band2_ntrans_, (double)p2nch_, (double)csr_nvalid_};
     std::memcpy(dst, v, sizeof v);
+  } else if (name == "setup_marks") {
+    need(sizeof(double));
+    std::memcpy(dst, setup_marks_, sizeof setup_marks_);
   } else if (name == "timings") {
     need(sizeof(double));
     const double v[9] = {timings.setup_ms, timings.iterate_ms, timings.finalize_ms,

@@ -35,26 +35,69 @@ __device__ __forceinline__ cplx twiddle(long long num, long long den) {
   return make_double2(c, s);
 }
 
+// T2[m] = exp(-2 pi i m / (2N)), m < 2N, precomputed once per plan
+__device__ __forceinline__ cplx tw_n(const cplx *T2, long long num, long long N) {
+  return T2[2 * (num % N)];
+}
+
+__global__ void k_fill_table(cplx *T2, long long n2) {
+  for (long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x; m < n2;
+       m += (long long)gridDim.x * blockDim.x)
+    T2[m] = twiddle(m, n2);
+}
+
 __device__ __forceinline__ unsigned bitrev(unsigned v, int bits) {
   return __brev(v) >> (32 - bits);
 }
 
-// table[j] = exp(-2 pi i j / L), j < L/2
-__device__ void fill_twiddles(cplx *table, int L) {
-  for (int j = threadIdx.x; j < L / 2; j += blockDim.x) table[j] = twiddle(j, L);
+// table[j] = exp(-2 pi i j / L), j < L/2, from the plan table of length 2N
+__device__ void fill_twiddles(cplx *table, int L, const cplx *T2, long long N) {
+  const long long step = 2 * N / L;
+  for (int j = threadIdx.x; j < L / 2; j += blockDim.x) table[j] = T2[j * step];
 }
 
 // nfft independent length-L transforms stored contiguously in s (s[f*L + i]),
 // input in bit-reversed order, output natural order; sign -1 forward.
+// Two radix-2 stages (spans h and 2h) are done per round in registers on the
+// four elements i, i+h, i+2h, i+3h; a single radix-2 stage finishes odd
+// lengths.
 __device__ void fft_dit(cplx *s, int L, int nfft, const cplx *tw, bool inverse) {
-  const int half_total = nfft * (L / 2);
-  for (int len = 2; len <= L; len <<= 1) {
-    const int half = len >> 1, stride = L / len;
-    for (int b = threadIdx.x; b < half_total; b += blockDim.x) {
-      const int f = b / (L / 2), j = b % (L / 2);
-      const int g = j / half, pos = j % half;
-      const int i0 = f * L + g * len + pos, i1 = i0 + half;
-      cplx w = tw[pos * stride];
+  int h = 1;
+  for (; 4 * h <= L; h *= 4) {
+    const int quarter = L / 4, total = nfft * quarter;
+    const int st1 = L / (2 * h), st2 = L / (4 * h);
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+      const int f = b / quarter, j = b - f * quarter;
+      const int g = j / h, pos = j - g * h;
+      const int i0 = f * L + g * 4 * h + pos;
+      cplx w1 = tw[pos * st1], w2 = tw[pos * st2], w3 = tw[(pos + h) * st2];
+      if (inverse) {
+        w1 = cconj(w1);
+        w2 = cconj(w2);
+        w3 = cconj(w3);
+      }
+      cplx a0 = s[i0], a1 = s[i0 + h], a2 = s[i0 + 2 * h], a3 = s[i0 + 3 * h];
+      cplx t = cmul(a1, w1);
+      a1 = csub(a0, t);
+      a0 = cadd(a0, t);
+      t = cmul(a3, w1);
+      a3 = csub(a2, t);
+      a2 = cadd(a2, t);
+      t = cmul(a2, w2);
+      s[i0 + 2 * h] = csub(a0, t);
+      s[i0] = cadd(a0, t);
+      t = cmul(a3, w3);
+      s[i0 + 3 * h] = csub(a1, t);
+      s[i0 + h] = cadd(a1, t);
+    }
+    __syncthreads();
+  }
+  if (h < L) {  // last radix-2 stage, span h = L/2
+    const int half = h, total = nfft * (L / 2), stride = L / (2 * h);
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+      const int f = b / (L / 2), j = b - f * (L / 2);
+      const int i0 = f * L + j, i1 = i0 + half;
+      cplx w = tw[j * stride];
       if (inverse) w = cconj(w);
       const cplx t = cmul(s[i1], w), u = s[i0];
       s[i0] = cadd(u, t);
@@ -64,20 +107,55 @@ __device__ void fft_dit(cplx *s, int L, int nfft, const cplx *tw, bool inverse) 
   }
 }
 
-// natural-order input, bit-reversed output
+// natural-order input, bit-reversed output (decimation in frequency); stages
+// with spans 2h then h are fused per round
 __device__ void fft_dif(cplx *s, int L, int nfft, const cplx *tw, bool inverse) {
-  const int half_total = nfft * (L / 2);
-  for (int len = L; len >= 2; len >>= 1) {
-    const int half = len >> 1, stride = L / len;
-    for (int b = threadIdx.x; b < half_total; b += blockDim.x) {
-      const int f = b / (L / 2), j = b % (L / 2);
-      const int g = j / half, pos = j % half;
-      const int i0 = f * L + g * len + pos, i1 = i0 + half;
-      cplx w = tw[pos * stride];
+  int lg = 0;
+  while ((1 << lg) < L) ++lg;
+  int h;
+  if (lg & 1) {  // first radix-2 stage, span L/2
+    const int half = L / 2, total = nfft * half;
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+      const int f = b / half, j = b - f * half;
+      const int i0 = f * L + j, i1 = i0 + half;
+      cplx w = tw[j];
       if (inverse) w = cconj(w);
       const cplx u = s[i0], v = s[i1];
       s[i0] = cadd(u, v);
       s[i1] = cmul(csub(u, v), w);
+    }
+    __syncthreads();
+    h = L / 8;
+  } else {
+    h = L / 4;
+  }
+  for (; h >= 1; h /= 4) {
+    const int quarter = L / 4, total = nfft * quarter;
+    const int st1 = L / (2 * h), st2 = L / (4 * h);
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+      const int f = b / quarter, j = b - f * quarter;
+      const int g = j / h, pos = j - g * h;
+      const int i0 = f * L + g * 4 * h + pos;
+      cplx w1 = tw[pos * st1], w2 = tw[pos * st2], w3 = tw[(pos + h) * st2];
+      if (inverse) {
+        w1 = cconj(w1);
+        w2 = cconj(w2);
+        w3 = cconj(w3);
+      }
+      cplx a0 = s[i0], a1 = s[i0 + h], a2 = s[i0 + 2 * h], a3 = s[i0 + 3 * h];
+      // span 2h: (a0, a2) with w2, (a1, a3) with w3
+      cplx u = a0, v = a2;
+      a0 = cadd(u, v);
+      a2 = cmul(csub(u, v), w2);
+      u = a1;
+      v = a3;
+      a1 = cadd(u, v);
+      a3 = cmul(csub(u, v), w3);
+      // span h: (a0, a1) and (a2, a3) with w1
+      s[i0] = cadd(a0, a1);
+      s[i0 + h] = cmul(csub(a0, a1), w1);
+      s[i0 + 2 * h] = cadd(a2, a3);
+      s[i0 + 3 * h] = cmul(csub(a2, a3), w1);
     }
     __syncthreads();
   }
@@ -88,7 +166,7 @@ __device__ void fft_dif(cplx *s, int L, int nfft, const cplx *tw, bool inverse) 
 // A = Z[k], B = Z[N-k]; on return A = Z'[k], B = Z'[N-k].  k == 0 handles
 // the DC / Nyquist pair (B is ignored and set equal to A).
 __device__ __forceinline__ void spectral_pair(cplx &A, cplx &B, long long k, long long N,
-                                              const double *H) {
+                                              const double *H, const cplx *T2) {
   if (k == 0) {
     const double x0 = A.x + A.y, xn = A.x - A.y;
     const double y0 = x0 * H[0], yn = xn * H[N];
@@ -96,7 +174,7 @@ __device__ __forceinline__ void spectral_pair(cplx &A, cplx &B, long long k, lon
     B = A;
     return;
   }
-  const cplx W = twiddle(k, 2 * N);  // exp(-i pi k / N)
+  const cplx W = T2[k];  // exp(-i pi k / N)
   const cplx Bc = cconj(B);
   const cplx E = cscale(cadd(A, Bc), 0.5);
   const cplx D = csub(A, Bc);
@@ -124,38 +202,51 @@ __device__ __forceinline__ double seg_input(const double *x, const ConvSeg &sg, 
 }
 
 // ---------------------------------------------------------------- means --
-__global__ void k_seg_mean_in(const ConvSeg *segs, const double *x, double *means) {
-  const ConvSeg sg = segs[blockIdx.x];
-  double v[1] = {0.0};
-  if (sg.flags & 1)
-    for (long long i = threadIdx.x; i < sg.n_in; i += blockDim.x) v[0] += x[sg.x_off + i];
-  block_sum<1>(v);
-  if (threadIdx.x == 0) means[blockIdx.x] = (sg.flags & 1) ? v[0] / sg.n_in : 0.0;
+// Segment sums in two stages: kMeanBlocks CTAs per segment write partial sums;
+// consumers add the partials of their segment.
+constexpr int kMeanBlocks = 32;
+
+__global__ void k_seg_sum(const ConvSeg *segs, const double *v, int out, double *part) {
+  const ConvSeg sg = segs[blockIdx.y];
+  const bool on = out ? (sg.flags & 2) : (sg.flags & 1);
+  const long long n = out ? sg.n_out : sg.n_in;
+  const long long off = out ? sg.y_off : sg.x_off;
+  double acc[1] = {0.0};
+  if (on) {
+    const long long a = n * blockIdx.x / gridDim.x, e = n * (blockIdx.x + 1) / gridDim.x;
+    for (long long i = a + threadIdx.x; i < e; i += blockDim.x) acc[0] += v[off + i];
+  }
+  block_sum<1>(acc);
+  if (threadIdx.x == 0) part[(long long)blockIdx.y * gridDim.x + blockIdx.x] = acc[0];
 }
 
-__global__ void k_seg_mean_out(const ConvSeg *segs, double *y) {
-  const ConvSeg sg = segs[blockIdx.x];
+__device__ __forceinline__ double seg_mean(const double *part, int seg, long long n, bool on) {
+  if (!on || n == 0) return 0.0;
+  double s = 0;
+  for (int b = 0; b < kMeanBlocks; ++b) s += part[(long long)seg * kMeanBlocks + b];
+  return s / (double)n;
+}
+
+__global__ void k_seg_sub_mean(const ConvSeg *segs, double *y, const double *part) {
+  const ConvSeg sg = segs[blockIdx.y];
   if (!(sg.flags & 2)) return;
-  double v[1] = {0.0};
-  for (long long i = threadIdx.x; i < sg.n_out; i += blockDim.x) v[0] += y[sg.y_off + i];
-  block_sum<1>(v);
-  __shared__ double m;
-  if (threadIdx.x == 0) m = v[0] / sg.n_out;
-  __syncthreads();
-  const double mm = m;
-  for (long long i = threadIdx.x; i < sg.n_out; i += blockDim.x) y[sg.y_off + i] -= mm;
+  const double m = seg_mean(part, blockIdx.y, sg.n_out, true);
+  const long long n = sg.n_out;
+  const long long a = n * blockIdx.x / gridDim.x, e = n * (blockIdx.x + 1) / gridDim.x;
+  for (long long i = a + threadIdx.x; i < e; i += blockDim.x) y[sg.y_off + i] -= m;
 }
 
 // ------------------------------------------------------ single-CTA path --
 // One CTA per segment; N complex values in shared memory.
 __global__ void k_conv_small(const ConvSeg *segs, const double *spectra, long long spec_len,
-                             const double *x, double *y, const double *means, int N, int logN) {
+                             const double *x, double *y, const double *part, int N, int logN,
+                             const cplx *T2) {
   extern __shared__ double2 sm[];
   cplx *s = sm;
   cplx *tw = sm + N;
   const ConvSeg sg = segs[blockIdx.x];
-  const double mean = means[blockIdx.x];
-  fill_twiddles(tw, N);
+  const double mean = seg_mean(part, blockIdx.x, sg.n_in, sg.flags & 1);
+  fill_twiddles(tw, N, T2, N);
   for (int m = threadIdx.x; m < N; m += blockDim.x) {
     const double a = seg_input(x, sg, 2LL * m, mean);
     const double b = seg_input(x, sg, 2LL * m + 1, mean);
@@ -167,7 +258,7 @@ __global__ void k_conv_small(const ConvSeg *segs, const double *spectra, long lo
   for (int k = threadIdx.x; k <= N / 2; k += blockDim.x) {
     const int nk = (N - k) % N;
     cplx A = s[k], B = s[nk];
-    spectral_pair(A, B, k, N, H);
+    spectral_pair(A, B, k, N, H, T2);
     s[k] = A;
     if (nk != k) s[nk] = B;
   }
@@ -184,16 +275,16 @@ __global__ void k_conv_small(const ConvSeg *segs, const double *spectra, long lo
 
 // ------------------------------------------------------- four-step path --
 // Pass 1: forward column FFTs (length R) of G adjacent columns, twiddled.
-__global__ void k_conv_cols_fwd(const ConvSeg *segs, const double *x, const double *means,
-                                double2 *work, int R, int logR, int C, int G) {
+__global__ void k_conv_cols_fwd(const ConvSeg *segs, const double *x, const double *part,
+                                double2 *work, int R, int logR, int C, int G, const cplx *T2) {
   extern __shared__ double2 sm[];
   cplx *s = sm;            // G columns x R
   cplx *tw = sm + G * R;   // R/2
   const int seg = blockIdx.y;
   const ConvSeg sg = segs[seg];
-  const double mean = means[seg];
+  const double mean = seg_mean(part, seg, sg.n_in, sg.flags & 1);
   const int c0 = blockIdx.x * G;
-  fill_twiddles(tw, R);
+  fill_twiddles(tw, R, T2, (long long)R * C);
   for (int e = threadIdx.x; e < G * R; e += blockDim.x) {
     const int c = e % G, n1 = e / G;
     const long long m = (long long)C * n1 + c0 + c;
@@ -208,14 +299,14 @@ __global__ void k_conv_cols_fwd(const ConvSeg *segs, const double *x, const doub
   for (int e = threadIdx.x; e < G * R; e += blockDim.x) {
     const int c = e % G, k1 = e / G;
     const int n2 = c0 + c;
-    W[(long long)k1 * C + n2] = cmul(s[c * R + k1], twiddle((long long)n2 * k1, N));
+    W[(long long)k1 * C + n2] = cmul(s[c * R + k1], tw_n(T2, (long long)n2 * k1, N));
   }
 }
 
 // Pass 2: forward row FFTs of rows k1 and R-k1, spectral product, inverse
 // row FFTs, inverse twiddles.
 __global__ void k_conv_rows(const ConvSeg *segs, const double *spectra, long long spec_len,
-                            double2 *work, int R, int C, int logC) {
+                            double2 *work, int R, int C, int logC, const cplx *T2) {
   extern __shared__ double2 sm[];
   cplx *tw = sm;               // C/2
   cplx *s = sm + C / 2;        // 2 rows x C
@@ -226,7 +317,7 @@ __global__ void k_conv_rows(const ConvSeg *segs, const double *spectra, long lon
   const int j = blockIdx.x;            // 0 .. R/2
   const int ka = j, kb = (R - j) % R;  // row pair (equal for j = 0, R/2)
   const int nrows = (ka == kb) ? 1 : 2;
-  fill_twiddles(tw, C);
+  fill_twiddles(tw, C, T2, N);
   for (int e = threadIdx.x; e < nrows * C; e += blockDim.x) {
     const int r = e / C, n2 = e % C;
     const int k1 = r ? kb : ka;
@@ -240,7 +331,7 @@ __global__ void k_conv_rows(const ConvSeg *segs, const double *spectra, long lon
     for (int k2 = threadIdx.x; k2 <= C / 2; k2 += blockDim.x) {
       const int p2 = (C - k2) % C;
       cplx A = s[k2], B = s[p2];
-      spectral_pair(A, B, (long long)R * k2, N, H);
+      spectral_pair(A, B, (long long)R * k2, N, H, T2);
       s[k2] = A;
       if (p2 != k2) s[p2] = B;
     }
@@ -249,7 +340,7 @@ __global__ void k_conv_rows(const ConvSeg *segs, const double *spectra, long lon
     for (int k2 = threadIdx.x; k2 < C / 2; k2 += blockDim.x) {
       const int p2 = C - 1 - k2;
       cplx A = s[k2], B = s[p2];
-      spectral_pair(A, B, ka + (long long)R * k2, N, H);
+      spectral_pair(A, B, ka + (long long)R * k2, N, H, T2);
       s[k2] = A;
       s[p2] = B;
     }
@@ -258,7 +349,7 @@ __global__ void k_conv_rows(const ConvSeg *segs, const double *spectra, long lon
     for (int k2 = threadIdx.x; k2 < C; k2 += blockDim.x) {
       const int p2 = C - 1 - k2;
       cplx A = s[k2], B = s[C + p2];
-      spectral_pair(A, B, ka + (long long)R * k2, N, H);
+      spectral_pair(A, B, ka + (long long)R * k2, N, H, T2);
       s[k2] = A;
       s[C + p2] = B;
     }
@@ -269,13 +360,13 @@ __global__ void k_conv_rows(const ConvSeg *segs, const double *spectra, long lon
     const int r = e / C, n2 = e % C;
     const int k1 = r ? kb : ka;
     const cplx v = s[r * C + bitrev(n2, logC)];
-    W[(long long)k1 * C + n2] = cmul(v, cconj(twiddle((long long)n2 * k1, N)));
+    W[(long long)k1 * C + n2] = cmul(v, cconj(tw_n(T2, (long long)n2 * k1, N)));
   }
 }
 
 // Pass 3: inverse column FFTs and real output.
 __global__ void k_conv_cols_inv(const ConvSeg *segs, const double2 *work, double *y, int R,
-                                int logR, int C, int G) {
+                                int logR, int C, int G, const cplx *T2) {
   extern __shared__ double2 sm[];
   cplx *s = sm;
   cplx *tw = sm + G * R;
@@ -286,7 +377,7 @@ __global__ void k_conv_cols_inv(const ConvSeg *segs, const double2 *work, double
   const double2 *W = work + (long long)seg * N;
   // rows n1 whose outputs are needed: 2 (C n1 + n2) < n_out
   const int rows_needed = (int)min((long long)R, ((long long)sg.n_out + 2LL * C - 1) / (2LL * C));
-  fill_twiddles(tw, R);
+  fill_twiddles(tw, R, T2, N);
   for (int e = threadIdx.x; e < G * R; e += blockDim.x) {
     const int c = e % G, k1 = e / G;
     s[c * R + k1] = W[(long long)k1 * C + c0 + c];
@@ -324,6 +415,7 @@ FFTPlan::FFTPlan(long nof_) : nof(nof_), N(nof_ / 2) {
 }
 
 FFTPlan::~FFTPlan() {
+  if (table) cudaFree(table);
   if (work) cudaFree(work);
   if (means) cudaFree(means);
 }
@@ -335,17 +427,24 @@ void FFTPlan::reserve(long nseg) {
   work = nullptr;
   means = nullptr;
   if (R) MADAM_CUDA(cudaMalloc(&work, (size_t)nseg * N * sizeof(double2)));
-  MADAM_CUDA(cudaMalloc(&means, (size_t)nseg * sizeof(double)));
+  MADAM_CUDA(cudaMalloc(&means, (size_t)nseg * kMeanBlocks * sizeof(double)));
   nseg_max = nseg;
 }
 
 void FFTPlan::convolve(cudaStream_t st, const ConvSeg *segs, long nseg, const double *spectra,
                        const double *x, double *y) {
   if (nseg == 0) return;
+  if (!table) {
+    MADAM_CUDA(cudaMalloc(&table, (size_t)2 * N * sizeof(double2)));
+    MADAM_LAUNCH(k_fill_table, (unsigned)std::min<long long>(4096, (2 * N + 255) / 256), 256, 0,
+                 st, (double2 *)table, 2LL * N);
+  }
+  const cplx *T2 = (const cplx *)table;
   if (nseg > 65535) fail("too many filter segments in one batch");
   reserve(nseg);
   const long long spec_len = N + 1;
-  MADAM_LAUNCH(k_seg_mean_in, (unsigned)nseg, 256, 0, st, segs, x, means);
+  const dim3 gm(kMeanBlocks, (unsigned)nseg);
+  MADAM_LAUNCH(k_seg_sum, gm, 256, 0, st, segs, x, 0, means);
   if (R == 0) {
     const int logN = ilog2(N);
     size_t smem = (size_t)(N + N / 2) * sizeof(double2);
@@ -356,7 +455,7 @@ void FFTPlan::convolve(cudaStream_t st, const ConvSeg *segs, long nseg, const do
       attr_small = true;
     }
     MADAM_LAUNCH(k_conv_small, (unsigned)nseg, 256, smem, st, segs, spectra, spec_len, x, y,
-                 means, (int)N, logN);
+                 means, (int)N, logN, T2);
   } else {
     const int logR = ilog2(R), logC = ilog2(C);
     size_t smem_cols = (size_t)(G * R + R / 2) * sizeof(double2);
@@ -373,13 +472,14 @@ void FFTPlan::convolve(cudaStream_t st, const ConvSeg *segs, long nseg, const do
     }
     dim3 gc(C / G, (unsigned)nseg), gr(R / 2 + 1, (unsigned)nseg);
     MADAM_LAUNCH(k_conv_cols_fwd, gc, 256, smem_cols, st, segs, x, means, (double2 *)work, R, logR,
-                 C, G);
+                 C, G, T2);
     MADAM_LAUNCH(k_conv_rows, gr, 256, smem_rows, st, segs, spectra, spec_len, (double2 *)work, R, C,
-                 logC);
+                 logC, T2);
     MADAM_LAUNCH(k_conv_cols_inv, gc, 256, smem_cols, st, segs, (const double2 *)work, y, R, logR,
-                 C, G);
+                 C, G, T2);
   }
-  MADAM_LAUNCH(k_seg_mean_out, (unsigned)nseg, 256, 0, st, segs, y);
+  MADAM_LAUNCH(k_seg_sum, gm, 256, 0, st, segs, y, 1, means);
+  MADAM_LAUNCH(k_seg_sub_mean, gm, 256, 0, st, segs, y, means);
 }
 
 }  // namespace madam

@@ -20,6 +20,7 @@ struct FFTPlan {
   int R = 0, C = 0; // four-step split N = R * C (0 for the single-CTA path)
   int G = 0;        // columns per CTA in the column passes
   double *work = nullptr;   // nseg_max * N complex values
+  double *table = nullptr;  // 2N complex twiddles exp(-2 pi i m / (2N))
   double *means = nullptr;  // nseg_max
   long nseg_max = 0;
   explicit FFTPlan(long nof_);

@@ -1,0 +1,270 @@
+// FITS products of destripe(): HEALPix binary tables like the reference's
+// output.f90 (write_map 114-375, write_binmap 526-786, write_mask 792-912,
+// write_hits 918-1025, write_matrix 1031-1175, headers 1376-1591).
+//
+// Layout (full sky, NESTED): one row per submap, one column per map
+// component with nosubpix values per row ('E' float32 maps, 'J' hits and
+// mask, 'D' pixel matrices); unobserved map pixels hold the HEALPix
+// undefined value -1.6375e30.  Files are named <path_output><file_root>
+// _map.fits, _bmap.fits, _hmap.fits, _mask.fits, _wcov_inv.fits, _wcov.fits;
+// an existing file gets a _001, _002, ... suffix unless the name starts with
+// '!' (check_outfile, output.f90:1329-1366).
+#include "fits.h"
+
+#include <sys/stat.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace madam {
+namespace {
+
+const float kUndef = -1.6375e30f;
+
+bool exists(const std::string &f) {
+  struct stat st;
+  return stat(f.c_str(), &st) == 0;
+}
+
+std::string resolve(std::string f) {
+  if (!f.empty() && f[0] == '!') return f.substr(1);
+  if (!exists(f)) return f;
+  const size_t dot = f.rfind('.');
+  const std::string stem = dot == std::string::npos ? f : f.substr(0, dot);
+  const std::string ext = dot == std::string::npos ? "" : f.substr(dot);
+  for (int k = 1; k < 1000; ++k) {
+    char s[8];
+    std::snprintf(s, sizeof s, "_%03d", k);
+    const std::string c = stem + s + ext;
+    if (!exists(c)) return c;
+  }
+  return "";
+}
+
+class Header {
+ public:
+  void raw(const std::string &c) {
+    std::string s = c.substr(0, 80);
+    s.resize(80, ' ');
+    cards_.push_back(s);
+  }
+  void str(const std::string &k, const std::string &v, const std::string &cm = "") {
+    std::string q = "'" + v;
+    while (q.size() < 9) q += ' ';
+    q += "'";
+    kv(k, q, cm, false);
+  }
+  void integer(const std::string &k, long long v, const std::string &cm = "") {
+    kv(k, std::to_string(v), cm, true);
+  }
+  void real(const std::string &k, double v, const std::string &cm = "") {
+    char b[32];
+    std::snprintf(b, sizeof b, "%.10E", v);
+    kv(k, b, cm, true);
+  }
+  void logical(const std::string &k, bool v, const std::string &cm = "") {
+    kv(k, v ? "T" : "F", cm, true);
+  }
+  void comment(const std::string &t) { raw("COMMENT " + t); }
+  void write(FILE *f) {
+    raw("END");
+    for (auto &c : cards_) std::fwrite(c.data(), 1, 80, f);
+    const size_t n = cards_.size() * 80;
+    const size_t pad = (2880 - n % 2880) % 2880;
+    std::string sp(pad, ' ');
+    std::fwrite(sp.data(), 1, pad, f);
+    cards_.clear();
+  }
+
+ private:
+  void kv(const std::string &k, const std::string &v, const std::string &cm, bool right) {
+    std::string key = k;
+    for (auto &ch : key) ch = (char)toupper(ch);
+    key.resize(8, ' ');
+    std::string val = v;
+    if (right && val.size() < 20) val = std::string(20 - val.size(), ' ') + val;
+    std::string c = key + "= " + val;
+    if (!cm.empty()) c += " / " + cm;
+    raw(c);
+  }
+  std::vector<std::string> cards_;
+};
+
+template <typename T>
+void put_be(std::vector<unsigned char> &out, T v) {
+  unsigned char b[sizeof(T)];
+  std::memcpy(b, &v, sizeof(T));
+  for (int i = (int)sizeof(T) - 1; i >= 0; --i) out.push_back(b[i]);
+}
+
+struct Col {
+  std::string name, tform, unit;
+  int bytes;  // per row
+};
+
+// One BINTABLE file: empty primary HDU + table.  row(r, buf) appends row r.
+template <typename KeyFn, typename RowFn>
+void write_table(const std::string &fname, const std::vector<Col> &cols, long long nrows,
+                 KeyFn keys, RowFn row) {
+  FILE *f = std::fopen(fname.c_str(), "wb");
+  if (!f) fail("cannot open " + fname + " for writing");
+  Header p;
+  p.logical("SIMPLE", true, "file does conform to FITS standard");
+  p.integer("BITPIX", 8, "number of bits per data pixel");
+  p.integer("NAXIS", 0, "number of data axes");
+  p.logical("EXTEND", true, "FITS dataset may contain extensions");
+  p.write(f);
+  long long rowbytes = 0;
+  for (auto &c : cols) rowbytes += c.bytes;
+  Header h;
+  h.str("XTENSION", "BINTABLE", "binary table extension");
+  h.integer("BITPIX", 8, "8-bit bytes");
+  h.integer("NAXIS", 2, "2-dimensional binary table");
+  h.integer("NAXIS1", rowbytes, "width of table in bytes");
+  h.integer("NAXIS2", nrows, "number of rows in table");
+  h.integer("PCOUNT", 0, "size of special data area");
+  h.integer("GCOUNT", 1, "one data group (required keyword)");
+  h.integer("TFIELDS", (long long)cols.size(), "number of fields in each row");
+  for (size_t i = 0; i < cols.size(); ++i) {
+    const std::string n = std::to_string(i + 1);
+    h.str("TTYPE" + n, cols[i].name, "label for field");
+    h.str("TFORM" + n, cols[i].tform, "data format of field");
+    if (!cols[i].unit.empty()) h.str("TUNIT" + n, cols[i].unit, "physical unit of field");
+  }
+  keys(h);
+  std::vector<unsigned char> buf;
+  h.write(f);
+  long long total = 0;
+  for (long long r = 0; r < nrows; ++r) {
+    buf.clear();
+    row(r, buf);
+    std::fwrite(buf.data(), 1, buf.size(), f);
+    total += (long long)buf.size();
+  }
+  const long long pad = (2880 - total % 2880) % 2880;
+  std::vector<unsigned char> z(pad, 0);
+  std::fwrite(z.data(), 1, pad, f);
+  std::fclose(f);
+}
+
+}  // namespace
+
+void write_products(const FitsInput &in) {
+  const Params &p = *in.par;
+  std::string root = p.file_root;
+  std::string path = p.path_output;
+  if (!path.empty() && path.back() != '/') path += '/';
+  auto name = [&](const std::string &suffix) {
+    std::string f = root + suffix;
+    if (!f.empty() && f[0] == '!') return "!" + path + f.substr(1);
+    return path + f;
+  };
+  const long nsub = in.nosubpix_map, nsm = in.nosubmaps_tot, npix = nsub * nsm;
+  const int nmap = in.nmap;
+  const char *mapnames[3] = {"TEMPERATURE", "Q-POLARISATION", "U-POLARISATION"};
+  auto healpix = [&](Header &h) {
+    h.str("PIXTYPE", "HEALPIX", "HEALPIX Pixelisation");
+    h.str("ORDERING", "NESTED", "Pixel ordering scheme");
+    h.integer("NSIDE", p.nside_map, "Resolution parameter for HEALPIX");
+    h.integer("FIRSTPIX", 0, "First pixel # (0 based)");
+    h.integer("LASTPIX", 12LL * p.nside_map * p.nside_map - 1, "Last pixel # (0 based)");
+    h.logical("POLAR", nmap != 1, "Polarisation included (True/False)");
+    h.str("POLCCONV", "COSMO", "Coord. convention for polarisation (COSMO/IAU)");
+    h.str("EXTNAME", "FULL SKY MAP");
+    h.str("OBJECT", "FULLSKY");
+    h.str("INDXSCHM", "IMPLICIT", "Indexing : IMPLICIT or EXPLICIT");
+    h.integer("GRAIN", 0, "Grain of pixel indexing");
+    h.str("CREATOR", "Madam", "Software creating FITS file");
+    h.integer("NODET", in.ndet, "Number of detectors");
+    h.real("FSAMPLE", p.fsample, "Sampling frequency (Hz)");
+    h.integer("NSIDESUB", p.nside_submap, "Submap resolution");
+    h.integer("NSIDECR", p.nside_cross, "Crossing point resolution");
+  };
+  auto map_file = [&](const std::string &suffix, const double *m, const char *objtype) {
+    const std::string f = resolve(name(suffix));
+    if (f.empty()) return;
+    std::vector<Col> cols;
+    for (int j = 0; j < nmap; ++j)
+      cols.push_back({nmap == 3 ? mapnames[j] : "TEMPERATURE", std::to_string(nsub) + "E",
+                      p.unit_tod, (int)(4 * nsub)});
+    auto keys = [&](Header &h) {
+      h.str("OBJTYPE", objtype, "Object type");
+      healpix(h);
+      h.logical("MONOPOLE", p.rm_monopole, "Monopole removed (T map)");
+    };
+    write_table(f, cols, nsm, keys, [&](long long r, std::vector<unsigned char> &b) {
+      for (int j = 0; j < nmap; ++j)
+        for (long i = 0; i < nsub; ++i) {
+          const long px = r * nsub + i;
+          const float v = in.mask[px] > 0 ? (float)m[px * nmap + j] : kUndef;
+          put_be(b, v);
+        }
+    });
+  };
+  if (p.do_map && in.map) map_file("_map.fits", in.map, "madam.map");
+  if (p.do_binmap && in.binmap) map_file("_bmap.fits", in.binmap, "madam.binmap");
+  if (in.first_call && p.do_hits && in.hits) {
+    const std::string f = resolve(name("_hmap.fits"));
+    if (!f.empty()) {
+      long rep = std::max<long>(12 * 1024, nsub);
+      rep = std::min<long>(rep, npix);
+      const long nrows = (npix + rep - 1) / rep;
+      std::vector<Col> cols = {{"Total hits", std::to_string(rep) + "J", "", (int)(4 * rep)}};
+      auto keys = [&](Header &h) {
+        h.str("OBJTYPE", "madam.hits", "Object type");
+        healpix(h);
+      };
+      write_table(f, cols, nrows, keys, [&](long long r, std::vector<unsigned char> &b) {
+        for (long i = 0; i < rep; ++i) {
+          const long px = r * rep + i;
+          put_be(b, (int32_t)(px < npix ? in.hits[px] : 0));
+        }
+      });
+    }
+  }
+  if (in.first_call && p.do_mask && in.mask) {
+    const std::string f = resolve(name("_mask.fits"));
+    if (!f.empty()) {
+      std::vector<Col> cols = {{"Mask", std::to_string(nsub) + "J", "", (int)(4 * nsub)},
+                               {"criterion", std::to_string(nsub) + "E", "", (int)(4 * nsub)}};
+      auto keys = [&](Header &h) {
+        h.str("OBJTYPE", "madam.mask", "Object type");
+        healpix(h);
+      };
+      write_table(f, cols, nsm, keys, [&](long long r, std::vector<unsigned char> &b) {
+        for (long i = 0; i < nsub; ++i) put_be(b, (int32_t)in.mask[r * nsub + i]);
+        for (long i = 0; i < nsub; ++i) put_be(b, in.crit ? in.crit[r * nsub + i] : 0.0f);
+      });
+    }
+  }
+  auto matrix_file = [&](const std::string &suffix, const double *cc) {
+    const std::string f = resolve(name(suffix));
+    if (f.empty()) return;
+    std::vector<Col> cols;
+    std::vector<std::pair<int, int>> ij;
+    for (int i = 0; i < nmap; ++i)
+      for (int j = i; j < nmap; ++j) {
+        cols.push_back({"cc(" + std::to_string(i + 1) + "," + std::to_string(j + 1) + ")",
+                        std::to_string(nsub) + "D", "", (int)(8 * nsub)});
+        ij.push_back({i, j});
+      }
+    auto keys = [&](Header &h) {
+      h.str("OBJTYPE", "madam.matrix", "Object type");
+      healpix(h);
+    };
+    write_table(f, cols, nsm, keys, [&](long long r, std::vector<unsigned char> &b) {
+      for (auto e : ij)
+        for (long q = 0; q < nsub; ++q) {
+          const long px = r * nsub + q;
+          put_be(b, cc[(size_t)px * nmap * nmap + e.second * nmap + e.first]);
+        }
+    });
+  };
+  if (in.first_call && p.do_matrix && in.cc_raw) matrix_file("_wcov_inv.fits", in.cc_raw);
+  if (in.first_call && p.do_wcov && in.cc_inv) matrix_file("_wcov.fits", in.cc_inv);
+}
+
+}  // namespace madam

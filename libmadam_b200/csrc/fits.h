@@ -1,0 +1,25 @@
+// FITS products of destripe() (fits.cpp).
+#pragma once
+
+#include "params.h"
+
+namespace madam {
+
+// Full-sky host arrays at nside_map; null pointers skip the product.
+struct FitsInput {
+  const Params *par = nullptr;
+  long nosubpix_map = 0, nosubmaps_tot = 0, ndet = 0;
+  int nmap = 0;
+  bool first_call = true;          // destripe (all products) or destripe_with_cache (maps)
+  const double *map = nullptr;     // [npix][nmap]
+  const double *binmap = nullptr;  // [npix][nmap]
+  const int *hits = nullptr;       // [npix]
+  const int *mask = nullptr;       // [npix]
+  const float *crit = nullptr;     // [npix]
+  const double *cc_raw = nullptr;  // [npix][nmap][nmap] before inversion
+  const double *cc_inv = nullptr;  // [npix][nmap][nmap] after inversion
+};
+
+void write_products(const FitsInput &in);
+
+}  // namespace madam

@@ -176,7 +176,7 @@ _RESULT_DTYPES = dict(map=np.float64, binmap=np.float64, hits=np.int32, mask=np.
                       crit=np.float32, cc=np.float64, cca=np.float64, aa=np.float64,
                       yba=np.float64, nna=np.float64, fcov=np.float64, invcov=np.float64,
                       rr_history=np.float64, band_widths=np.int64, scalars=np.float64,
-                      timings=np.float64)
+                      timings=np.float64, setup_marks=np.float64)
 
 
 def get_result(name):
@@ -201,7 +201,7 @@ def get_result(name):
 def scalars():
     keys = ["noiter", "rrinit", "rr_final", "nof", "n_band", "n_band_fail", "iterate_ms",
             "total_ms", "nmap", "noba_short", "npix_map", "nruns", "nwork", "nloc", "nseg",
-            "n_cg_prec"]
+            "n_cg_prec", "band_rows", "band_transfers", "band_chunks", "scatter_samples"]
     return dict(zip(keys, get_result("scalars").tolist()))
 
 
@@ -209,6 +209,14 @@ def timings():
     keys = ["setup_ms", "iterate_ms", "finalize_ms", "total_ms", "scatter_ms", "gather_ms",
             "filter_ms", "precond_ms", "other_ms"]
     return dict(zip(keys, get_result("timings").tolist()))
+
+
+def setup_marks():
+    """Cumulative host time (ms) after each setup phase of the last destripe:
+    start, filter, flagging+compaction, runs, binning, pixel-sorted pointing,
+    RHS, segments, preconditioner."""
+    keys = ["start", "filter", "compact", "runs", "bin", "csr", "rhs", "segments", "precond"]
+    return dict(zip(keys, get_result("setup_marks").tolist()))
 
 
 def bench_iterations(warmup, iters):

@@ -167,7 +167,7 @@ def pars_for(cfg: ScanConfig) -> dict:
         nside_map=cfg.nside, nside_cross=cfg.nside, nside_submap=cfg.nside_submap,
         fsample=cfg.fsample, base_first=cfg.base_first, kfilter=True,
         temperature_only=cfg.temperature_only, info=0,
-        write_map=True, write_binmap=True, write_hits=True,
+        write_map=False, write_binmap=False, write_hits=False,
     )
     pars.update(cfg.extra_pars)
     return pars

@@ -8,6 +8,7 @@ twice).  The inputs and expected maps live in tests/golden/*.npz
 destripe / destripe_with_cache / clear_caches / result(name).
 """
 import os
+import tempfile
 
 import numpy as np
 
@@ -27,12 +28,14 @@ def libmadam_pars(nside, nside_cross, nside_submap):
         "nside_submap": nside_submap, "write_map": True, "write_binmap": True,
         "write_matrix": True, "write_wcov": True, "write_hits": True, "kfilter": True,
         "diagfilter": 0, "file_root": "madam_pytest", "iter_max": 100, "allreduce": True,
-        "info": 0,
+        "info": 0, "path_output": tempfile.mkdtemp(prefix="madam_kat_"),
     }
 
 
-def run_libmadam_kat(backend):
-    """Two successive destripe() calls with nside_map 8 then 16 (test_libmadam.py:136-153)."""
+def run_libmadam_kat(backend, check_files=False):
+    """Two successive destripe() calls with nside_map 8 then 16 (test_libmadam.py:136-153).
+    With check_files, the hit and binned maps are also read back from the FITS
+    files, as the reference test does with healpy (test_libmadam.py:164-169)."""
     g = load("kat_libmadam.npz")
     nside = 8
     out = []
@@ -60,6 +63,21 @@ def run_libmadam_kat(backend):
         np.testing.assert_allclose(binmap[good], expect_b[good], rtol=1e-12)
         assert np.all(binmap[~good] == 0)
         np.testing.assert_array_equal(pixels, g["pixels"])  # pixels restored
+        if check_files:
+            from fits_reader import read_table
+            hh, hc = read_table(os.path.join(pars["path_output"], "madam_pytest_hmap.fits"))
+            assert hh["NSIDE"] == nside and hh["ORDERING"] == "NESTED"
+            np.testing.assert_array_equal(hc["Total hits"], expect_h)
+            bh, bc = read_table(os.path.join(pars["path_output"], "madam_pytest_bmap.fits"))
+            fb = bc["TEMPERATURE"]
+            np.testing.assert_allclose(fb[good], expect_b[good].astype(np.float32), rtol=1e-7)
+            assert np.all(fb[~good] == np.float32(-1.6375e30))
+            mh, mc = read_table(os.path.join(pars["path_output"], "madam_pytest_map.fits"))
+            assert mh["OBJTYPE"] == "madam.map"
+            np.testing.assert_allclose(mc["TEMPERATURE"][good],
+                                       backend.result("map")[good].astype(np.float32), rtol=1e-6)
+            for suffix in ("_wcov_inv.fits", "_wcov.fits"):
+                assert os.path.exists(os.path.join(pars["path_output"], "madam_pytest" + suffix))
         out.append((hits, binmap, backend.result("map"), backend.result("aa")))
         nside *= 2
     return out

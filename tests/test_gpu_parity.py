@@ -81,7 +81,7 @@ def compare(ro, rp, nmap, iters_exact=True):
 
 def test_reference_kat_hits_and_binned_map(W):
     from product_api import ProductBackend
-    kat.run_libmadam_kat(ProductBackend())
+    kat.run_libmadam_kat(ProductBackend(), check_files=True)
 
 
 def test_reference_kat_mc_sequence(W):
