@@ -58,6 +58,31 @@ unsigned long long madam_b200_kernel_launches(void);
  * reference counterpart. */
 int madam_b200_selftest_fastdiv(void);
 
+/* Hit counts and inverse pixel matrices (the "hits" and "cc" products of
+ * destripe) of a pointing that is already in device memory, computed
+ * without allocating any device memory.  No counterpart in the reference
+ * (whose pixel_matrix / count_hits, src/smadam_routines.f90:111-246,
+ * 349-422, and invert_pixelmatrix_map, src/map_routines.f90:218-321, run
+ * inside destripe).
+ *
+ * All arrays are device memory owned by the caller: detweights [ndet],
+ * pix int64 [ndet][nsamp] (NESTED at nside; negative = flagged, skipped),
+ * pixweights float64 [ndet][nsamp][nnz], hits int32 [12 nside^2], cc
+ * float64 [12 nside^2][nnz][nnz] (zero where the rcond cut of pixmode /
+ * pixlim rejects the pixel).  Work is queued on `stream` (NULL = legacy
+ * default stream) and is complete once that stream is synchronised.
+ * Limits: nside <= 64 (the accumulators are a fixed 2.75 MB device array of
+ * 49152 pixels; larger maps return status 1 and say so); nnz 1 or 3.  The
+ * first call on a device looks up that array's address (make it before
+ * any stream capture).  Calls that overlap on one device share the array
+ * and race.  Returns 0, 1 (invalid argument) or 2 (CUDA error); the message
+ * goes to err (errlen bytes, may be NULL). */
+int madam_b200_pixel_matrices_noalloc(long nside, long nnz, long ndet, long nsamp,
+                                      const double *detweights, const long long *pix,
+                                      const double *pixweights, long pixmode, double pixlim,
+                                      int *hits, double *cc, void *stream, char *err,
+                                      long errlen);
+
 #ifdef __cplusplus
 }
 #endif
