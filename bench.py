@@ -90,6 +90,10 @@ def config_for(name):
         return syn.config2(), "plain destripe nside512 16det x 4obs x 2^23 @100Hz IQU"
     if name == "1":
         return syn.config1(), "plain destripe nside64 4det x 2^20 @10Hz IQU"
+    if name == "prof":
+        cfg = syn.config2()
+        cfg.nobs = 1
+        return cfg, "nside512 16det x 1obs x 2^23 @100Hz IQU (per-segment shapes of config 2)"
     if name == "mid":
         cfg = syn.config2()
         cfg.nobs = 1
@@ -200,7 +204,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="2", choices=["2", "1", "mid", "small"])
+    ap.add_argument("--config", default="2", choices=["2", "1", "prof", "mid", "small"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

@@ -6,21 +6,31 @@
 //
 // Factor.  Row j of L is R_j[d] = L(j, j-d), d = 0..w (w = nband - 1), and
 // depends only on rows j-w..j-1 and on nna_j.  Computed left-looking, in the
-// update order of DPBTF2 (m increasing), rows settle to a bitwise fixed point
-// after ~100 rows wherever nna is constant; once w+1 consecutive rows are
-// identical and nna_j == nna_{j-1} the next row is a copy, so it is not
-// recomputed.  The factor is stored as a table of distinct rows plus a run
-// list (first row, table entry).  Exact: every stored row is the row the
-// column algorithm would produce for that input.
+// update order of DPBTF2 (m increasing), rows settle to a fixed point after
+// ~100 rows wherever nna is constant.  A row that agrees with its
+// predecessor to 4 ulp in every entry is taken to be that row (in FMA
+// arithmetic the fixed point can end in a last-bit limit cycle instead of a
+// bitwise fixed point), and once w+1 consecutive rows are one row and
+// nna_j == nna_{j-1} the next row is that row without recomputation.  The
+// factor is stored as a table of distinct rows plus a run list (first row,
+// table entry).
 //
-// Solve.  The forward recurrence y_j = (r_j - sum_d R_j[d] y_{j-d}) / R_j[0]
-// is cut into chunks.  Pass 1 solves every chunk with a zero initial state;
-// a warp per segment then propagates the true state across chunks with the
-// w x w transfer matrices T_c (homogeneous response of the chunk's last w rows
-// to its w initial values, precomputed, shared between chunks whose rows are
-// one run); pass 2 re-solves every chunk from its true initial state.  The
-// backward solve L^T x = y does the same from the end of the segment.
+// Solve.  Both triangular solves are one recurrence over positions p,
+//   v_p = (in_p - sum_{d=w..1} K_p[d] v_{p-d}) * (1 / K_p[0]),
+// forward with p = j and K_p = row j of L (DTBSV 'L','N' order: d = w first),
+// backward with p = n-1-j and K_p = column j of L, K_p[d] = L(j+d, j)
+// (DTBSV 'L','T' order).  A column inside a run of equal rows is that row;
+// the w columns before each run boundary and at the segment end are
+// assembled into extra entries.  The positions are cut into chunks; pass 1
+// solves every chunk from a zero state, a warp per segment propagates the
+// true state across chunks with the w x w transfer matrices T_c (the
+// response of the chunk's last w values to its w initial values,
+// precomputed, one per distinct coefficient entry for chunks inside one
+// run), and pass 2 re-solves each chunk from its true state.  The forward
+// final pass and the backward pass 1 of a chunk run in one thread.  Widths
+// up to 32 keep the recurrence window and the coefficients in registers.
 #include <algorithm>
+#include <climits>
 
 #include "band2.cuh"
 #include "engine.h"
@@ -28,33 +38,32 @@
 namespace madam {
 namespace {
 
-constexpr int kRing = 128;  // >= w + 1
+constexpr int kRing = 128;               // generic window (>= w + 1)
+constexpr double kFreezeTol = 0x1p-50;   // 4 ulp relative
 
-// One thread per segment.  urows: worst-case region of n * nb doubles at
-// seg.row_off; runs: worst-case n entries at seg.run_off.
+// One thread per segment.  rows: worst-case region of n * (nb + 1) doubles
+// at seg.row_off; runs: worst-case n entries at seg.run_off.
 __global__ void k_band2_factor(const PSeg *segs, int nseg, const int *spec, const double *invcov,
-                               long long nof, const double *nna, double *urows, PRun *runs,
+                               long long nof, const double *nna, double *rows, PRun *runs,
                                int *status, int *nunique, int *nruns) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nseg) return;
   const PSeg g = segs[s];
-  const int nb = g.nb, w = nb - 1;
+  const int nb = g.nb, w = nb - 1, S = nb + 1;
   const double *ic = invcov + (long long)spec[s] * nof;
   const double *nn = nna + g.k0;
-  double *rowbase = urows + g.row_off;
+  double *rowbase = rows + g.row_off;
   PRun *rl = runs + g.run_off;
-  // window of the last w rows (pointers into the unique table)
-  const double *win[kRing];
+  const double *win[kRing];  // the last w rows (pointers into the table)
   int nu = 0, nr = 0, same = 0;
   const double *prev = nullptr;
   for (int j = 0; j < g.n; ++j) {
     if (prev && same >= w + 1 && nn[j] == nn[j - 1]) {
-      // steady state: row j equals row j-1
       win[j & (kRing - 1)] = prev;
       ++same;
       continue;
     }
-    double *R = rowbase + (long long)nu * nb;
+    double *R = rowbase + (long long)nu * S;
     for (int d = 0; d < nb; ++d) R[d] = 0.0;
     // off-diagonal entries, d = w..1 (k = j - d increasing)
     for (int d = min(w, j); d >= 1; --d) {
@@ -76,13 +85,18 @@ __global__ void k_band2_factor(const PSeg *segs, int nseg, const int *spec, cons
     bool eq = prev != nullptr;
     if (eq)
       for (int d = 0; d < nb; ++d)
-        if (R[d] != prev[d]) { eq = false; break; }
+        if (!(fabs(R[d] - prev[d]) <= kFreezeTol * fabs(prev[d]))) {
+          eq = false;
+          break;
+        }
     if (eq) {
       win[j & (kRing - 1)] = prev;
       ++same;
     } else {
+      R[nb] = 1.0 / R[0];
       rl[nr].start = j;
-      rl[nr].row_off = g.row_off + (long long)nu * nb;
+      rl[nr].fill = 0;
+      rl[nr].off = g.row_off + (long long)nu * S;
       ++nr;
       ++nu;
       prev = R;
@@ -95,90 +109,183 @@ __global__ void k_band2_factor(const PSeg *segs, int nseg, const int *spec, cons
   nruns[s] = nr;
 }
 
-// Forward solve of rows [a, b) of one segment.  state: y_{a-w..a-1} (or
-// nullptr for zeros); writes y (if out) and the last w values (if tail).
-__device__ void fwd_rows(const PSeg &g, const PRun *runs, const double *urows, int run,
-                         int a, int b, const double *r, const double *state, double *out,
-                         double *tail) {
+// Backward entries: column j of L, C[d] = L(j+d, j) = R_{j+d}[d] (zero past
+// the segment end), C[w+1] = 1 / C[0].  Block row y = segment.
+__global__ void k_band2_columns(const PSeg *segs, const PRun *runs, const PRun *cruns,
+                                double *tab) {
+  const PSeg g = segs[blockIdx.y];
   const int w = g.nb - 1;
-  double ring[kRing];
-  for (int i = 0; i < w; ++i) ring[(a - w + i) & (kRing - 1)] = state ? state[i] : 0.0;
-  const int rend = g.run_off + g.nrun;
-  int next = (run + 1 < rend) ? runs[run + 1].start : 0x7fffffff;
-  const double *R = urows + runs[run].row_off;
-  for (int j = a; j < b; ++j) {
-    while (j >= next) {
-      ++run;
-      R = urows + runs[run].row_off;
-      next = (run + 1 < rend) ? runs[run + 1].start : 0x7fffffff;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < g.ncrun; e += gridDim.x * blockDim.x) {
+    const PRun c = cruns[g.crun_off + e];
+    if (!c.fill) continue;
+    const int j = g.n - 1 - c.start;
+    double *C = tab + c.off;
+    for (int d = 0; d <= w; ++d) {
+      const int row = j + d;
+      if (row >= g.n) {
+        C[d] = 0.0;
+        continue;
+      }
+      int lo = g.run_off, hi = g.run_off + g.nrun - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (runs[mid].start <= row) lo = mid;
+        else hi = mid - 1;
+      }
+      const double *Rr = tab + runs[lo].off;
+      C[d] = Rr[d];
+      if (d == 0) C[w + 1] = Rr[w + 1];
     }
-    double acc = r ? r[g.k0 + j] : 0.0;
-    for (int d = w; d >= 1; --d) acc -= R[d] * ring[(j - d) & (kRing - 1)];
-    const double y = acc / R[0];
-    ring[j & (kRing - 1)] = y;
-    if (out) out[g.k0 + j] = y;
+  }
+}
+
+// One direction of one segment: run list, entry table and the map from
+// position p to the vector index gbase + gstep * p.
+struct Seq {
+  const PRun *runs;
+  int rend;  // one past the segment's last run
+  const double *tab;
+  long long gbase;
+  int gstep;
+};
+
+__device__ __forceinline__ Seq fwd_seq(const PSeg &g, const PRun *runs, const double *tab) {
+  return Seq{runs, g.run_off + g.nrun, tab, g.k0, 1};
+}
+
+__device__ __forceinline__ Seq bwd_seq(const PSeg &g, const PRun *cruns, const double *tab) {
+  return Seq{cruns, g.crun_off + g.ncrun, tab, g.k0 + g.n - 1, -1};
+}
+
+// Positions [p0, p1), window of any width w <= kRing - 1 in local memory.
+// state: v_{p0-w..p0-1} (nullptr = zeros); writes v (if out) and the last w
+// values (if tail).
+__device__ void recur_generic(int w, const Seq &q, int run, int p0, int p1, const double *in,
+                              const double *state, double *out, double *tail) {
+  double ring[kRing];
+  for (int i = 0; i < w; ++i) ring[(p0 - w + i) & (kRing - 1)] = state ? state[i] : 0.0;
+  int next = (run + 1 < q.rend) ? q.runs[run + 1].start : INT_MAX;
+  const double *K = q.tab + q.runs[run].off;
+  for (int p = p0; p < p1; ++p) {
+    while (p >= next) {
+      ++run;
+      K = q.tab + q.runs[run].off;
+      next = (run + 1 < q.rend) ? q.runs[run + 1].start : INT_MAX;
+    }
+    const long long gi = q.gbase + (long long)q.gstep * p;
+    double acc = in ? in[gi] : 0.0;
+    for (int d = w; d >= 1; --d) acc -= K[d] * ring[(p - d) & (kRing - 1)];
+    const double v = acc * K[w + 1];
+    ring[p & (kRing - 1)] = v;
+    if (out) out[gi] = v;
   }
   if (tail)
-    for (int i = 0; i < w; ++i) tail[i] = (b - w + i >= a - w) ? ring[(b - w + i) & (kRing - 1)] : 0.0;
+    for (int i = 0; i < w; ++i) tail[i] = ring[(p1 - w + i) & (kRing - 1)];
 }
 
-// Backward solve of rows [a, b) (descending).  state: x_{b..b+w-1} (zeros
-// beyond the segment end, or nullptr); writes x (if out) and the first w
-// values (if head).  run_hi: the run containing row min(b + w, n) - 1.
-__device__ void bwd_rows(const PSeg &g, const PRun *runs, const double *urows, int run_hi,
-                         int a, int b, const double *y, const double *state, double *out,
-                         double *head) {
-  const int w = g.nb - 1;
-  double xr[kRing];
-  const double *pr[kRing];
-  int rr = run_hi;
-  const int top = min(b + w, g.n) - 1;
-  for (int q = top; q >= a; --q) {
-    // row pointer of q
-    while (q < runs[rr].start) --rr;
-    pr[q & (kRing - 1)] = urows + runs[rr].row_off;
-    if (q >= b) xr[q & (kRing - 1)] = state ? state[q - b] : 0.0;
-    if (q < b) {
-      const int j = q;
-      double t = y ? y[g.k0 + j] : 0.0;
-      const int dmax = min(w, g.n - 1 - j);
-      for (int d = 1; d <= dmax; ++d) t -= pr[(j + d) & (kRing - 1)][d] * xr[(j + d) & (kRing - 1)];
-      const double x = t / pr[j & (kRing - 1)][0];
-      xr[j & (kRing - 1)] = x;
-      if (out) out[g.k0 + j] = x;
+// The same recurrence with a compile-time window W >= w held in registers:
+// the loop is unrolled by W + 1 so every window slot is a fixed register;
+// taps d > w have zero coefficients.
+template <int W>
+__device__ __forceinline__ void recur_reg(int w, const Seq &q, int run, int p0, int p1,
+                                          const double *in, const double *state,
+                                          double *out, double *tail) {
+  constexpr int R = W + 1;
+  double v[R];  // slot of position p: (p - p0) mod R
+#pragma unroll
+  for (int s = 0; s < R; ++s) {
+    const int m = R - s;  // slot s >= 1 holds v_{p0-m}
+    v[s] = (s >= 1 && m <= w && state) ? state[w - m] : 0.0;
+  }
+  double K[W + 1];
+  double kinv;
+  int next;
+  auto load = [&](int rr) {
+    const double *E = q.tab + q.runs[rr].off;
+#pragma unroll
+    for (int d = 1; d <= W; ++d) K[d] = d <= w ? E[d] : 0.0;
+    kinv = E[w + 1];
+    next = (rr + 1 < q.rend) ? q.runs[rr + 1].start : INT_MAX;
+  };
+  load(run);
+  for (int pb = p0; pb < p1; pb += R) {
+#pragma unroll
+    for (int t = 0; t < R; ++t) {
+      const int p = pb + t;
+      if (p < p1) {
+        if (p >= next) {
+          while (p >= next) {
+            ++run;
+            next = (run + 1 < q.rend) ? q.runs[run + 1].start : INT_MAX;
+          }
+          load(run);
+        }
+        const long long gi = q.gbase + (long long)q.gstep * p;
+        double acc = in ? in[gi] : 0.0;
+#pragma unroll
+        for (int d = W; d >= 1; --d) acc -= K[d] * v[(t - d + 2 * R) % R];
+        v[t] = acc * kinv;
+        if (out) out[gi] = v[t];
+      }
     }
   }
-  if (head)
-    for (int i = 0; i < w; ++i) head[i] = (a + i < b) ? xr[(a + i) & (kRing - 1)] : 0.0;
+  if (tail) {
+    const int base = (((p1 - p0 - w) % R) + R) % R;  // slot of v_{p1-w}
+#pragma unroll
+    for (int s = 0; s < R; ++s) {
+      int i = s - base;
+      if (i < 0) i += R;
+      if (i < w) tail[i] = v[s];
+    }
+  }
 }
 
-__global__ void k_band2_fwd(const PSeg *segs, const PChunk *ch, int nch, const PRun *runs,
-                            const double *urows, const double *r, const double *tstate,
-                            double *out, double *tails) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nch) return;
+template <int W>
+__device__ __forceinline__ void recur(int w, const Seq &q, int run, int p0, int p1,
+                                      const double *in, const double *state, double *out,
+                                      double *tail) {
+  if (W == 0) recur_generic(w, q, run, p0, p1, in, state, out, tail);
+  else recur_reg<(W > 0 ? W : 1)>(w, q, run, p0, p1, in, state, out, tail);
+}
+
+// mode 0: forward pass 1 (tails -> wp)
+// mode 1: forward pass 2 (state ws[c-1], writes z), then backward pass 1 on
+//         the chunk's own rows of z (tails -> wp)
+// mode 2: backward pass 2 (state ws[c+1], z in place)
+template <int W>
+__global__ void __launch_bounds__(64) k_band2_pass(const PSeg *segs, const PChunk *ch, int c0,
+                                                   int c1, const PRun *runs, const PRun *cruns,
+                                                   const double *tab, int mode, const double *r,
+                                                   double *z, const double *ws, double *wp) {
+  const int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= c1) return;
   const PChunk k = ch[c];
   const PSeg g = segs[k.seg];
-  const double *st = (tstate && k.first == 0) ? tstate + (long long)(c - 1) * kRing : nullptr;
-  double *tl = (tails && k.last == 0) ? tails + (long long)c * kRing : nullptr;
-  fwd_rows(g, runs, urows, k.run, k.a, k.b, r, st, out, tl);
+  const int w = g.nb - 1;
+  if (mode <= 1) {
+    const Seq f = fwd_seq(g, runs, tab);
+    if (mode == 0) {
+      recur<W>(w, f, k.run_f, k.a, k.b, r, nullptr, nullptr,
+               k.last ? nullptr : wp + (long long)c * kBand2State);
+      return;
+    }
+    recur<W>(w, f, k.run_f, k.a, k.b, r, k.first ? nullptr : ws + (long long)(c - 1) * kBand2State,
+             z, nullptr);
+    const Seq b = bwd_seq(g, cruns, tab);
+    recur<W>(w, b, k.run_b, g.n - k.b, g.n - k.a, z, nullptr, nullptr,
+             k.first ? nullptr : wp + (long long)c * kBand2State);
+    return;
+  }
+  const Seq b = bwd_seq(g, cruns, tab);
+  recur<W>(w, b, k.run_b, g.n - k.b, g.n - k.a, z,
+           k.last ? nullptr : ws + (long long)(c + 1) * kBand2State, z, nullptr);
 }
 
-__global__ void k_band2_bwd(const PSeg *segs, const PChunk *ch, int nch, const PRun *runs,
-                            const double *urows, const double *y, const double *hstate,
-                            double *out, double *heads) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nch) return;
-  const PChunk k = ch[c];
-  const PSeg g = segs[k.seg];
-  const double *st = (hstate && k.last == 0) ? hstate + (long long)(c + 1) * kRing : nullptr;
-  double *hd = (heads && k.first == 0) ? heads + (long long)c * kRing : nullptr;
-  bwd_rows(g, runs, urows, k.run_hi, k.a, k.b, y, st, out, hd);
-}
-
-// Transfer matrices: column q of T = response to the unit state e_q.
+// Transfer matrices: column q of T = response of the tail to the unit state
+// e_q with zero input.
 __global__ void k_band2_transfer(const PSeg *segs, const PChunk *ch, const PTrans *tr, int ntr,
-                                 const PRun *runs, const double *urows, double *T) {
+                                 const PRun *runs, const PRun *cruns, const double *tab,
+                                 double *T) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ntr) return;
   const PTrans e = tr[t];
@@ -187,10 +294,11 @@ __global__ void k_band2_transfer(const PSeg *segs, const PChunk *ch, const PTran
   const int w = g.nb - 1;
   double unit[kRing], res[kRing];
   double *Tm = T + e.off;
+  const Seq f = fwd_seq(g, runs, tab), b = bwd_seq(g, cruns, tab);
   for (int q = 0; q < w; ++q) {
     for (int i = 0; i < w; ++i) unit[i] = (i == q) ? 1.0 : 0.0;
-    if (e.dir == 0) fwd_rows(g, runs, urows, k.run, k.a, k.b, nullptr, unit, nullptr, res);
-    else bwd_rows(g, runs, urows, k.run_hi, k.a, k.b, nullptr, unit, nullptr, res);
+    if (e.dir == 0) recur_generic(w, f, k.run_f, k.a, k.b, nullptr, unit, nullptr, res);
+    else recur_generic(w, b, k.run_b, g.n - k.b, g.n - k.a, nullptr, unit, nullptr, res);
     for (int i = 0; i < w; ++i) Tm[(long long)i * w + q] = res[i];
   }
 }
@@ -206,8 +314,8 @@ constexpr int kScanWarps = 2;
 
 __global__ void k_band2_scan(const PSeg *segs, int nseg, const PChunk *ch, const double *T,
                              const double *p, double *s, int dir) {
-  __shared__ double pbuf[kScanWarps][kScanBlock][kRing];
-  __shared__ double curb[kScanWarps][kRing];
+  __shared__ double pbuf[kScanWarps][kScanBlock][kBand2State];
+  __shared__ double curb[kScanWarps][kBand2State];
   __shared__ int toffb[kScanWarps][kScanBlock];
   const int wl = threadIdx.x >> 5;
   const int seg = blockIdx.x * kScanWarps + wl;
@@ -222,9 +330,9 @@ __global__ void k_band2_scan(const PSeg *segs, int nseg, const PChunk *ch, const
   const int stop = dir == 0 ? cl : c0;  // exclusive
   const int step = dir == 0 ? 1 : -1;
   for (int i = lane; i < w; i += 32) {
-    const double v = p[(long long)start * kRing + i];
+    const double v = p[(long long)start * kBand2State + i];
     cur[i] = v;
-    s[(long long)start * kRing + i] = v;
+    s[(long long)start * kBand2State + i] = v;
   }
   __syncwarp();
   for (int cb = start + step; cb != stop;) {
@@ -232,7 +340,7 @@ __global__ void k_band2_scan(const PSeg *segs, int nseg, const PChunk *ch, const
     for (int u = 0, c = cb; u < kScanBlock && c != stop; ++u, c += step) ++nblk;
     for (int e = lane; e < nblk * w; e += 32) {
       const int u = e / w, i = e - u * w;
-      pbuf[wl][u][i] = p[(long long)(cb + u * step) * kRing + i];
+      pbuf[wl][u][i] = p[(long long)(cb + u * step) * kBand2State + i];
     }
     if (lane < nblk) {
       const int c = cb + lane * step;
@@ -241,7 +349,7 @@ __global__ void k_band2_scan(const PSeg *segs, int nseg, const PChunk *ch, const
     __syncwarp();
     for (int u = 0; u < nblk; ++u) {
       const double *Tm = T + toffb[wl][u];
-      double v[kRing / 32];
+      double v[kBand2State / 32];
       int ni = 0;
       for (int i = lane; i < w; i += 32, ++ni) {
         double acc = pbuf[wl][u][i];
@@ -254,7 +362,7 @@ __global__ void k_band2_scan(const PSeg *segs, int nseg, const PChunk *ch, const
       const long long c = cb + u * step;
       for (int i = lane; i < w; i += 32, ++ni) {
         cur[i] = v[ni];
-        s[c * kRing + i] = v[ni];
+        s[c * kBand2State + i] = v[ni];
       }
       __syncwarp();
     }
@@ -262,38 +370,88 @@ __global__ void k_band2_scan(const PSeg *segs, int nseg, const PChunk *ch, const
   }
 }
 
+template <int W>
+void launch_pass(cudaStream_t st, const PSeg *segs, const PChunk *ch, int c0, int c1,
+                 const PRun *runs, const PRun *cruns, const double *tab, int mode, const double *r,
+                 double *z, const double *ws, double *wp) {
+  const unsigned grid = (unsigned)((c1 - c0 + 63) / 64);
+  MADAM_LAUNCH(k_band2_pass<W>, grid, 64, 0, st, segs, ch, c0, c1, runs, cruns, tab, mode, r, z,
+               ws, wp);
+}
+
+// Register widths compiled: the band widths precond_width_min = 10 gives
+// (10, 20, 30) exactly, others padded to the next width.
+constexpr int kWidths[] = {1, 2, 4, 8, 9, 12, 16, 19, 24, 29, 32};
+
+void pass_class(int W, cudaStream_t st, const PSeg *segs, const PChunk *ch, int c0, int c1,
+                const PRun *runs, const PRun *cruns, const double *tab, int mode, const double *r,
+                double *z, const double *ws, double *wp) {
+  switch (W) {
+#define MADAM_BAND2_CASE(X) \
+  case X: launch_pass<X>(st, segs, ch, c0, c1, runs, cruns, tab, mode, r, z, ws, wp); break;
+    MADAM_BAND2_CASE(1)
+    MADAM_BAND2_CASE(2)
+    MADAM_BAND2_CASE(4)
+    MADAM_BAND2_CASE(8)
+    MADAM_BAND2_CASE(9)
+    MADAM_BAND2_CASE(12)
+    MADAM_BAND2_CASE(16)
+    MADAM_BAND2_CASE(19)
+    MADAM_BAND2_CASE(24)
+    MADAM_BAND2_CASE(29)
+    MADAM_BAND2_CASE(32)
+#undef MADAM_BAND2_CASE
+    default: launch_pass<0>(st, segs, ch, c0, c1, runs, cruns, tab, mode, r, z, ws, wp); break;
+  }
+}
+
 }  // namespace
 
+int band2_class_width(int w) {
+  for (int W : kWidths)
+    if (W >= w) return W;
+  return 0;
+}
+
 void band2_factor(cudaStream_t st, const PSeg *segs, int nseg, const int *spec,
-                  const double *invcov, long long nof, const double *nna, double *urows,
+                  const double *invcov, long long nof, const double *nna, double *rows,
                   PRun *runs, int *status, int *nunique, int *nruns) {
   if (nseg == 0) return;
   MADAM_LAUNCH(k_band2_factor, (nseg + 31) / 32, 32, 0, st, segs, nseg, spec, invcov, nof, nna,
-               urows, runs, status, nunique, nruns);
+               rows, runs, status, nunique, nruns);
+}
+
+void band2_columns(cudaStream_t st, const PSeg *segs, int nseg, int max_ncrun, const PRun *runs,
+                   const PRun *cruns, double *tab) {
+  if (nseg == 0 || max_ncrun == 0) return;
+  const dim3 grid((unsigned)std::min(64, (max_ncrun + 255) / 256), (unsigned)nseg);
+  MADAM_LAUNCH(k_band2_columns, grid, 256, 0, st, segs, runs, cruns, tab);
 }
 
 void band2_transfer(cudaStream_t st, const PSeg *segs, const PChunk *ch, const PTrans *tr, int ntr,
-                    const PRun *runs, const double *urows, double *T) {
+                    const PRun *runs, const PRun *cruns, const double *tab, double *T) {
   if (ntr == 0) return;
-  MADAM_LAUNCH(k_band2_transfer, (ntr + 63) / 64, 64, 0, st, segs, ch, tr, ntr, runs, urows, T);
+  MADAM_LAUNCH(k_band2_transfer, (ntr + 63) / 64, 64, 0, st, segs, ch, tr, ntr, runs, cruns, tab,
+               T);
 }
 
 void band2_solve(cudaStream_t st, const PSeg *segs, int nseg, const PChunk *ch, int nch,
-                 const PRun *runs, const double *urows, const double *T, const double *r,
-                 double *z, double *work_p, double *work_s) {
+                 const int *cls_w, const int *cls_begin, int ncls, const PRun *runs,
+                 const PRun *cruns, const double *tab, const double *T, const double *r, double *z,
+                 double *work_p, double *work_s) {
   if (nch == 0) return;
-  const unsigned gc = (nch + 127) / 128;
   const unsigned gs = (nseg + kScanWarps - 1) / kScanWarps;
-  // forward: particular, state scan, final
-  MADAM_LAUNCH(k_band2_fwd, gc, 128, 0, st, segs, ch, nch, runs, urows, r, nullptr, nullptr,
-               work_p);
+  auto passes = [&](int mode) {
+    for (int i = 0; i < ncls; ++i)
+      if (cls_begin[i + 1] > cls_begin[i])
+        pass_class(cls_w[i], st, segs, ch, cls_begin[i], cls_begin[i + 1], runs, cruns, tab, mode,
+                   r, z, work_s, work_p);
+  };
+  passes(0);
   MADAM_LAUNCH(k_band2_scan, gs, 32 * kScanWarps, 0, st, segs, nseg, ch, T, work_p, work_s, 0);
-  MADAM_LAUNCH(k_band2_fwd, gc, 128, 0, st, segs, ch, nch, runs, urows, r, work_s, z, nullptr);
-  // backward, in place on z
-  MADAM_LAUNCH(k_band2_bwd, gc, 128, 0, st, segs, ch, nch, runs, urows, z, nullptr, nullptr,
-               work_p);
+  passes(1);
   MADAM_LAUNCH(k_band2_scan, gs, 32 * kScanWarps, 0, st, segs, nseg, ch, T, work_p, work_s, 1);
-  MADAM_LAUNCH(k_band2_bwd, gc, 128, 0, st, segs, ch, nch, runs, urows, z, work_s, z, nullptr);
+  passes(2);
 }
 
 }  // namespace madam

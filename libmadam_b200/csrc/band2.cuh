@@ -5,50 +5,63 @@
 
 namespace madam {
 
-// One factored segment.  row_off / run_off locate its distinct rows and runs.
+// One factored segment of n baselines with band width nb = w + 1.
+// Coefficient entries are nb + 1 doubles: the nb band values and the
+// reciprocal of the first one.
 struct PSeg {
   long long k0;       // first baseline of the segment
-  long long row_off;  // offset (doubles) of its row table
+  long long row_off;  // offset (doubles) of its entry table while factoring
   int n;              // rows
   int nb;             // band width (w + 1)
-  int run_off;        // first run
-  int nrun;           // runs
-  int ch_off;         // first chunk
-  int nch;            // chunks
+  int run_off, nrun;  // forward runs (rows of L, position p = row j)
+  int crun_off, ncrun;  // backward runs (columns of L, position p = n - 1 - j)
+  int ch_off, nch;    // chunks
 };
 
-// Rows [start, next run's start) share the distinct row at row_off.
+// Positions [start, next run's start) of one direction share the entry at
+// off.  fill = 1 marks a backward entry that a kernel assembles from rows.
 struct PRun {
   int start;
-  int pad;
-  long long row_off;
+  int fill;
+  long long off;
 };
 
-// A chunk of rows [a, b) of segment seg.
+// Rows [a, b) of segment seg; the forward pass visits them ascending, the
+// backward pass descending.
 struct PChunk {
   int seg, a, b;
-  int run;     // run containing row a
-  int run_hi;  // run containing row min(b + w, n) - 1
+  int run_f;   // forward run containing row a
+  int run_b;   // backward run containing position n - b (row b - 1)
   int first, last;
   int tf, tb;  // offsets (doubles) of the forward / backward transfer matrices
 };
 
 struct PTrans {
-  int chunk;       // representative chunk
-  int dir;         // 0 forward, 1 backward
-  long long off;   // offset of the w x w matrix
+  int chunk;  // representative chunk
+  int dir;    // 0 forward, 1 backward
+  long long off;  // offset of the w x w matrix
 };
 
 constexpr int kBand2MaxWidth = 128;
-constexpr int kBand2Chunk = 256;
+constexpr int kBand2State = 128;  // doubles per chunk state slot (>= w)
 
+// Factor one segment per thread; rows: worst case n * (nb + 1) doubles at
+// seg.row_off, runs: worst case n at seg.run_off.
 void band2_factor(cudaStream_t st, const PSeg *segs, int nseg, const int *spec,
-                  const double *invcov, long long nof, const double *nna, double *urows,
+                  const double *invcov, long long nof, const double *nna, double *rows,
                   PRun *runs, int *status, int *nunique, int *nruns);
+// Assemble the backward entries flagged in the column runs.
+void band2_columns(cudaStream_t st, const PSeg *segs, int nseg, int max_ncrun, const PRun *runs,
+                   const PRun *cruns, double *tab);
 void band2_transfer(cudaStream_t st, const PSeg *segs, const PChunk *ch, const PTrans *tr, int ntr,
-                    const PRun *runs, const double *urows, double *T);
+                    const PRun *runs, const PRun *cruns, const double *tab, double *T);
+// Solve L L^T z = r on every factored segment.  classes: chunk ranges
+// [cls_begin[i], cls_begin[i + 1]) whose segments have w <= cls_w[i].
 void band2_solve(cudaStream_t st, const PSeg *segs, int nseg, const PChunk *ch, int nch,
-                 const PRun *runs, const double *urows, const double *T, const double *r,
-                 double *z, double *work_p, double *work_s);
+                 const int *cls_w, const int *cls_begin, int ncls, const PRun *runs,
+                 const PRun *cruns, const double *tab, const double *T, const double *r, double *z,
+                 double *work_p, double *work_s);
+// Smallest compiled register width >= w (0 when w needs the generic path).
+int band2_class_width(int w);
 
 }  // namespace madam

@@ -236,12 +236,14 @@ class Engine {
   std::vector<int> cg_prec_segs_;   // segments without a band factor
   std::vector<long> band_widths_;
   DevBuf<PSeg> p2segs_;
-  DevBuf<PRun> p2runs_;
+  DevBuf<PRun> p2runs_, p2cruns_;
   DevBuf<PChunk> p2ch_;
   DevBuf<double> p2rows_, p2T_, p2wp_, p2ws_;
   int p2nseg_ = 0, p2nch_ = 0;
   long long band2_rows_ = 0;
   long band2_ntrans_ = 0;
+  int band2_chunk_ = 0;
+  std::vector<int> band2_cls_w_, band2_cls_begin_;
   long n_band_fail_ = 0;
   std::unique_ptr<FFTPlan> fft_;
   std::unique_ptr<CgpWork> cgp_;

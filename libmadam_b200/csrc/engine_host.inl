@@ -1014,9 +1014,9 @@ void Engine::construct_preconditioner() {
       int runoff = 0;
       for (size_t t = 0; t < t2.size(); ++t) {
         const Segment &sg = segs_[t2[t].seg];
-        ps[t] = PSeg{sg.k0, roff, (int)sg.noba, (int)t2[t].nband, runoff, 0, 0, 0};
+        ps[t] = PSeg{sg.k0, roff, (int)sg.noba, (int)t2[t].nband, runoff, 0, 0, 0, 0, 0};
         spec[t] = sg.psd_prec;
-        roff += (long long)sg.noba * t2[t].nband;
+        roff += (long long)sg.noba * (t2[t].nband + 1);
         runoff += (int)sg.noba;
       }
       DevBuf<PSeg> dps;
@@ -1103,81 +1103,115 @@ void Engine::construct_preconditioner() {
     }
     todo.swap(next);
   }
-  // pack the deduplicated factors the apply step uses (prec_ok segments)
-  std::vector<PSeg> pseg;
-  std::vector<PRun> pruns;
-  long long nrows_total = 0;
-  std::vector<std::pair<const Done2 *, long long>> copies;
+  // pack the deduplicated factors the apply step uses (prec_ok segments),
+  // ordered by register width class so that each class's chunks are contiguous
+  struct Pack { const Done2 *dn; std::vector<PRun> rl; int W; };
+  std::vector<Pack> packs;
+  long nmax = 0;
   for (const Done2 &dn : done2) {
     if (!segs_[dn.seg].prec_ok) continue;
-    std::vector<PRun> rl(dn.nr);
-    MADAM_CUDA(cudaMemcpy(rl.data(), runs_r[dn.round]->get() + dn.ps.run_off,
+    Pack pk{&dn, std::vector<PRun>(dn.nr), band2_class_width(dn.ps.nb - 1)};
+    MADAM_CUDA(cudaMemcpy(pk.rl.data(), runs_r[dn.round]->get() + dn.ps.run_off,
                           dn.nr * sizeof(PRun), cudaMemcpyDeviceToHost));
-    PSeg q = dn.ps;
-    q.row_off = nrows_total;
-    q.run_off = (int)pruns.size();
-    q.nrun = dn.nr;
-    for (PRun r : rl) {
-      r.row_off = r.row_off - dn.ps.row_off + nrows_total;
-      pruns.push_back(r);
-    }
-    copies.push_back({&dn, nrows_total});
-    nrows_total += (long long)dn.nu * dn.ps.nb;
-    pseg.push_back(q);
+    nmax = std::max<long>(nmax, dn.ps.n);
+    packs.push_back(std::move(pk));
   }
-  p2rows_.alloc(std::max<long long>(1, nrows_total));
-  for (auto &cp : copies)
-    MADAM_CUDA(cudaMemcpyAsync(p2rows_.get() + cp.second, rows_r[cp.first->round]->get() +
-                                                              cp.first->ps.row_off,
-                               (size_t)cp.first->nu * cp.first->ps.nb * sizeof(double),
-                               cudaMemcpyDeviceToDevice, st_));
-  // chunks and transfer matrices
+  auto cls_key = [](int W) { return W == 0 ? INT_MAX : W; };
+  std::stable_sort(packs.begin(), packs.end(),
+                   [&](const Pack &a, const Pack &b) { return cls_key(a.W) < cls_key(b.W); });
+  // chunk length ~ sqrt(4 n): balances the chunk passes against the
+  // sequential state scan
+  int C = 64;
+  while (C < 4096 && (long)C * C < 4 * nmax) C *= 2;
+  std::vector<PSeg> pseg;
+  std::vector<PRun> pruns, cruns;
   std::vector<PChunk> chunks;
   std::vector<PTrans> trans;
-  std::map<std::tuple<long long, int, int>, long long> tcache;
+  long long tab_end = 0, nunique = 0;
+  for (const Pack &pk : packs) {
+    PSeg q = pk.dn->ps;
+    q.row_off = tab_end;
+    tab_end += (long long)pk.dn->nu * (q.nb + 1);
+    nunique += pk.dn->nu;
+    pseg.push_back(q);
+  }
+  band2_cls_w_.clear();
+  band2_cls_begin_.clear();
+  int max_ncrun = 0;
+  std::map<std::pair<long long, int>, long long> tcache;
   long long toff = 0;
-  for (size_t si = 0; si < pseg.size(); ++si) {
+  for (size_t si = 0; si < packs.size(); ++si) {
+    const Pack &pk = packs[si];
     PSeg &q = pseg[si];
-    const int w = q.nb - 1;
-    const int C = kBand2Chunk;
-    q.nch = (q.n + C - 1) / C;
-    q.ch_off = (int)chunks.size();
-    auto run_of = [&](int row) {
-      int lo = q.run_off, hi = q.run_off + q.nrun - 1;
+    const int n = q.n, w = q.nb - 1, S = q.nb + 1;
+    if (band2_cls_w_.empty() || band2_cls_w_.back() != pk.W) {
+      band2_cls_w_.push_back(pk.W);
+      band2_cls_begin_.push_back((int)chunks.size());
+    }
+    q.run_off = (int)pruns.size();
+    q.nrun = pk.dn->nr;
+    for (PRun r : pk.rl) {
+      r.off = r.off - pk.dn->ps.row_off + q.row_off;
+      r.fill = 0;
+      pruns.push_back(r);
+    }
+    // backward runs (p = n - 1 - j ascending): column j is row j's entry
+    // while rows j..j+w are one run; the w columns before each run's end
+    // (and the segment end) are assembled
+    q.crun_off = (int)cruns.size();
+    for (int ri = q.nrun - 1; ri >= 0; --ri) {
+      const int s0 = pruns[q.run_off + ri].start;
+      const int e0 = ri + 1 < q.nrun ? pruns[q.run_off + ri + 1].start : n;
+      for (int j = e0 - 1; j >= std::max(s0, e0 - w); --j) {
+        cruns.push_back({n - 1 - j, 1, tab_end});
+        tab_end += S;
+      }
+      if (e0 - w - 1 >= s0) cruns.push_back({n - 1 - (e0 - w - 1), 0, pruns[q.run_off + ri].off});
+    }
+    q.ncrun = (int)cruns.size() - q.crun_off;
+    max_ncrun = std::max(max_ncrun, q.ncrun);
+    auto find = [](const std::vector<PRun> &v, int lo, int hi, int pos) {
       while (lo < hi) {
         const int mid = (lo + hi + 1) / 2;
-        if (pruns[mid].start <= row) lo = mid;
+        if (v[mid].start <= pos) lo = mid;
         else hi = mid - 1;
       }
       return lo;
     };
+    q.nch = (n + C - 1) / C;
+    q.ch_off = (int)chunks.size();
     for (int c = 0; c < q.nch; ++c) {
       PChunk k;
       k.seg = (int)si;
       k.a = c * C;
-      k.b = std::min(q.n, k.a + C);
-      k.run = run_of(k.a);
-      k.run_hi = run_of(std::min(k.b + w, q.n) - 1);
+      k.b = std::min(n, k.a + C);
+      k.run_f = find(pruns, q.run_off, q.run_off + q.nrun - 1, k.a);
+      k.run_b = find(cruns, q.crun_off, q.crun_off + q.ncrun - 1, n - k.b);
       k.first = c == 0;
       k.last = c == q.nch - 1;
       k.tf = k.tb = 0;
       if (!k.first && !k.last && w > 0) {
         const int ci = (int)chunks.size();
-        const bool steady_f = run_of(k.b - 1) == k.run && k.b - k.a == C;
-        const bool steady_b = k.run_hi == k.run && k.b - k.a == C && k.b + w <= q.n;
+        // a chunk inside one run has the transfer matrix of that entry and
+        // length, whichever direction
+        const bool steady_f =
+            find(pruns, q.run_off, q.run_off + q.nrun - 1, k.b - 1) == k.run_f && k.b - k.a == C;
+        const bool steady_b =
+            find(cruns, q.crun_off, q.crun_off + q.ncrun - 1, n - k.a - 1) == k.run_b &&
+            k.b - k.a == C;
         for (int dir = 0; dir < 2; ++dir) {
           const bool steady = dir == 0 ? steady_f : steady_b;
+          const long long eoff = dir == 0 ? pruns[k.run_f].off : cruns[k.run_b].off;
           long long off = -1;
-          std::tuple<long long, int, int> key{pruns[k.run].row_off, dir, q.nb};
           if (steady) {
-            auto it = tcache.find(key);
+            auto it = tcache.find({eoff, q.nb});
             if (it != tcache.end()) off = it->second;
           }
           if (off < 0) {
             off = toff;
             toff += (long long)w * w;
             trans.push_back({ci, dir, off});
-            if (steady) tcache[key] = off;
+            if (steady) tcache[{eoff, q.nb}] = off;
           }
           (dir == 0 ? k.tf : k.tb) = (int)off;
         }
@@ -1185,34 +1219,49 @@ void Engine::construct_preconditioner() {
       chunks.push_back(k);
     }
   }
+  band2_cls_begin_.push_back((int)chunks.size());
   if (toff >= (1LL << 31)) fail("too many band transfer matrices");
   p2nseg_ = (int)pseg.size();
   p2nch_ = (int)chunks.size();
   p2segs_.alloc(std::max<size_t>(1, pseg.size()));
   p2runs_.alloc(std::max<size_t>(1, pruns.size()));
+  p2cruns_.alloc(std::max<size_t>(1, cruns.size()));
   p2ch_.alloc(std::max<size_t>(1, chunks.size()));
+  p2rows_.alloc(std::max<long long>(1, tab_end));
   p2T_.alloc(std::max<long long>(1, toff));
-  p2wp_.alloc((size_t)std::max(1, p2nch_) * 128);
-  p2ws_.alloc((size_t)std::max(1, p2nch_) * 128);
+  p2wp_.alloc((size_t)std::max(1, p2nch_) * kBand2State);
+  p2ws_.alloc((size_t)std::max(1, p2nch_) * kBand2State);
   if (!pseg.empty()) {
+    for (size_t si = 0; si < packs.size(); ++si) {
+      const Done2 &dn = *packs[si].dn;
+      MADAM_CUDA(cudaMemcpyAsync(p2rows_.get() + pseg[si].row_off,
+                                 rows_r[dn.round]->get() + dn.ps.row_off,
+                                 (size_t)dn.nu * (dn.ps.nb + 1) * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, st_));
+    }
     MADAM_CUDA(cudaMemcpyAsync(p2segs_.get(), pseg.data(), pseg.size() * sizeof(PSeg),
                                cudaMemcpyHostToDevice, st_));
     MADAM_CUDA(cudaMemcpyAsync(p2runs_.get(), pruns.data(), pruns.size() * sizeof(PRun),
                                cudaMemcpyHostToDevice, st_));
+    MADAM_CUDA(cudaMemcpyAsync(p2cruns_.get(), cruns.data(), cruns.size() * sizeof(PRun),
+                               cudaMemcpyHostToDevice, st_));
     MADAM_CUDA(cudaMemcpyAsync(p2ch_.get(), chunks.data(), chunks.size() * sizeof(PChunk),
                                cudaMemcpyHostToDevice, st_));
+    band2_columns(st_, p2segs_.get(), p2nseg_, max_ncrun, p2runs_.get(), p2cruns_.get(),
+                  p2rows_.get());
     DevBuf<PTrans> dtr;
     dtr.alloc(std::max<size_t>(1, trans.size()));
     if (!trans.empty()) {
       MADAM_CUDA(cudaMemcpyAsync(dtr.get(), trans.data(), trans.size() * sizeof(PTrans),
                                  cudaMemcpyHostToDevice, st_));
       band2_transfer(st_, p2segs_.get(), p2ch_.get(), dtr.get(), (int)trans.size(),
-                     p2runs_.get(), p2rows_.get(), p2T_.get());
+                     p2runs_.get(), p2cruns_.get(), p2rows_.get(), p2T_.get());
     }
     MADAM_CUDA(cudaStreamSynchronize(st_));
   }
-  band2_rows_ = nrows_total;
+  band2_rows_ = nunique;
   band2_ntrans_ = (long)trans.size();
+  band2_chunk_ = C;
   // plain column store for the wide bands
   long long total = 0;
   band_segs_.clear();
@@ -1397,8 +1446,9 @@ void Engine::apply_preconditioner(const double *r, double *z) {
       fft_->convolve(st_, filt_segs_d_.get(), (long)filt_segs_.size(), fprec_.get(), r, z);
     return;
   }
-  band2_solve(st_, p2segs_.get(), p2nseg_, p2ch_.get(), p2nch_, p2runs_.get(), p2rows_.get(),
-              p2T_.get(), r, z, p2wp_.get(), p2ws_.get());
+  band2_solve(st_, p2segs_.get(), p2nseg_, p2ch_.get(), p2nch_, band2_cls_w_.data(),
+              band2_cls_begin_.data(), (int)band2_cls_w_.size(), p2runs_.get(), p2cruns_.get(),
+              p2rows_.get(), p2T_.get(), r, z, p2wp_.get(), p2ws_.get());
   band_solve(st_, band_segs_d_.get(), (int)band_segs_.size(), band_.get(), r, z);
   cg_preconditioner_segments(r, z);
 }
