@@ -41,12 +41,18 @@ namespace {
 constexpr int kRing = 128;               // generic window (>= w + 1)
 constexpr double kFreezeTol = 0x1p-50;   // 4 ulp relative
 
-// One thread per segment.  rows: worst-case region of n * (nb + 1) doubles
-// at seg.row_off; runs: worst-case n entries at seg.run_off.
+// One warp per segment: lane 0 computes the rows; where the factor has
+// reached its steady state the warp scans nna for the next change (8 values
+// per lane per step) and the rows in between are copies.  rows: worst-case
+// region of n * (nb + 1) doubles at seg.row_off; runs: worst-case n entries
+// at seg.run_off.
+constexpr int kScanPerLane = 8;
+
 __global__ void k_band2_factor(const PSeg *segs, int nseg, const int *spec, const double *invcov,
                                long long nof, const double *nna, double *rows, PRun *runs,
                                int *status, int *nunique, int *nruns) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (s >= nseg) return;
   const PSeg g = segs[s];
   const int nb = g.nb, w = nb - 1, S = nb + 1;
@@ -54,59 +60,94 @@ __global__ void k_band2_factor(const PSeg *segs, int nseg, const int *spec, cons
   const double *nn = nna + g.k0;
   double *rowbase = rows + g.row_off;
   PRun *rl = runs + g.run_off;
-  const double *win[kRing];  // the last w rows (pointers into the table)
+  const double *win[kRing];  // lane 0: the last w rows (pointers into the table)
   int nu = 0, nr = 0, same = 0;
   const double *prev = nullptr;
-  for (int j = 0; j < g.n; ++j) {
-    if (prev && same >= w + 1 && nn[j] == nn[j - 1]) {
-      win[j & (kRing - 1)] = prev;
-      ++same;
-      continue;
-    }
-    double *R = rowbase + (long long)nu * S;
-    for (int d = 0; d < nb; ++d) R[d] = 0.0;
-    // off-diagonal entries, d = w..1 (k = j - d increasing)
-    for (int d = min(w, j); d >= 1; --d) {
-      const double *Rk = win[(j - d) & (kRing - 1)];
-      double acc = ic[d];
-      // subtract L(j, m) L(k, m) for m = j-w .. k-1 in increasing m
-      for (int e = min(w, j); e > d; --e) acc -= R[e] * Rk[e - d];
-      R[d] = acc * (1.0 / Rk[0]);
-    }
-    double dg = ic[0] + nn[j];
-    for (int e = min(w, j); e >= 1; --e) dg -= R[e] * R[e];
-    if (!(dg > 0)) {
-      status[s] = j + 1;
-      nunique[s] = 0;
-      nruns[s] = 0;
-      return;
-    }
-    R[0] = sqrt(dg);
-    bool eq = prev != nullptr;
-    if (eq)
-      for (int d = 0; d < nb; ++d)
-        if (!(fabs(R[d] - prev[d]) <= kFreezeTol * fabs(prev[d]))) {
-          eq = false;
+  int j = 0;
+  while (j < g.n) {
+    int jn = j;
+    if (lane == 0) {
+      for (; jn < g.n; ++jn) {
+        if (prev && same >= w + 1 && nn[jn] == nn[jn - 1]) break;  // steady: warp scan
+        double *R = rowbase + (long long)nu * S;
+        for (int d = 0; d < nb; ++d) R[d] = 0.0;
+        // off-diagonal entries, d = w..1 (k = jn - d increasing)
+        for (int d = min(w, jn); d >= 1; --d) {
+          const double *Rk = win[(jn - d) & (kRing - 1)];
+          double acc = ic[d];
+          // subtract L(jn, m) L(k, m) for m = jn-w .. k-1 in increasing m
+          for (int e = min(w, jn); e > d; --e) acc -= R[e] * Rk[e - d];
+          R[d] = acc * (1.0 / Rk[0]);
+        }
+        double dg = ic[0] + nn[jn];
+        for (int e = min(w, jn); e >= 1; --e) dg -= R[e] * R[e];
+        if (!(dg > 0)) {
+          status[s] = jn + 1;
+          nunique[s] = 0;
+          nruns[s] = 0;
+          jn = -1;
           break;
         }
-    if (eq) {
-      win[j & (kRing - 1)] = prev;
-      ++same;
-    } else {
-      R[nb] = 1.0 / R[0];
-      rl[nr].start = j;
-      rl[nr].fill = 0;
-      rl[nr].off = g.row_off + (long long)nu * S;
-      ++nr;
-      ++nu;
-      prev = R;
-      win[j & (kRing - 1)] = R;
-      same = 1;
+        R[0] = sqrt(dg);
+        bool eq = prev != nullptr;
+        if (eq)
+          for (int d = 0; d < nb; ++d)
+            if (!(fabs(R[d] - prev[d]) <= kFreezeTol * fabs(prev[d]))) {
+              eq = false;
+              break;
+            }
+        if (eq) {
+          win[jn & (kRing - 1)] = prev;
+          ++same;
+        } else {
+          R[nb] = 1.0 / R[0];
+          rl[nr].start = jn;
+          rl[nr].fill = 0;
+          rl[nr].off = g.row_off + (long long)nu * S;
+          ++nr;
+          ++nu;
+          prev = R;
+          win[jn & (kRing - 1)] = R;
+          same = 1;
+        }
+      }
     }
+    jn = __shfl_sync(0xffffffffu, jn, 0);
+    if (jn < 0) return;
+    if (jn >= g.n) break;
+    // rows jn.. repeat the previous row while nna keeps its value
+    const double v0 = nn[jn - 1];
+    int je = jn;
+    for (;;) {
+      unsigned stop = 0;
+#pragma unroll
+      for (int u = 0; u < kScanPerLane; ++u) {
+        const int idx = je + u * 32 + lane;
+        if (idx >= g.n || nn[idx] != v0) stop |= 1u << u;
+      }
+      int first = INT_MAX;
+#pragma unroll
+      for (int u = 0; u < kScanPerLane; ++u) {
+        const unsigned ball = __ballot_sync(0xffffffffu, (stop >> u) & 1u);
+        if (ball && first == INT_MAX) first = je + u * 32 + __ffs(ball) - 1;
+      }
+      if (first != INT_MAX) {
+        je = min(first, g.n);
+        break;
+      }
+      je += kScanPerLane * 32;
+    }
+    if (lane == 0) {
+      same += je - jn;
+      for (int r = max(jn, je - w); r < je; ++r) win[r & (kRing - 1)] = prev;
+    }
+    j = je;
   }
-  status[s] = 0;
-  nunique[s] = nu;
-  nruns[s] = nr;
+  if (lane == 0) {
+    status[s] = 0;
+    nunique[s] = nu;
+    nruns[s] = nr;
+  }
 }
 
 // Backward entries: column j of L, C[d] = L(j+d, j) = R_{j+d}[d] (zero past
@@ -185,12 +226,15 @@ __device__ void recur_generic(int w, const Seq &q, int run, int p0, int p1, cons
 
 // The same recurrence with a compile-time window W >= w held in registers:
 // the loop is unrolled by W + 1 so every window slot is a fixed register;
-// taps d > w have zero coefficients.
-template <int W>
+// taps d > w have zero coefficients.  A block of W + 1 positions that lies in
+// one run and in [p0, p1) runs without branches; the inputs of the next
+// block are loaded while the current one is computed (W <= 16).
+template <int W, bool HAS_IN, bool HAS_OUT>
 __device__ __forceinline__ void recur_reg(int w, const Seq &q, int run, int p0, int p1,
-                                          const double *in, const double *state,
-                                          double *out, double *tail) {
+                                          const double *in, const double *state, double *out,
+                                          double *tail) {
   constexpr int R = W + 1;
+  constexpr bool kAhead = W <= 16;
   double v[R];  // slot of position p: (p - p0) mod R
 #pragma unroll
   for (int s = 0; s < R; ++s) {
@@ -208,24 +252,56 @@ __device__ __forceinline__ void recur_reg(int w, const Seq &q, int run, int p0, 
     next = (rr + 1 < q.rend) ? q.runs[rr + 1].start : INT_MAX;
   };
   load(run);
-  for (int pb = p0; pb < p1; pb += R) {
+  const long long gs = q.gstep;
+  double buf[kAhead ? R : 1];
+  auto fetch = [&](int pb) {
 #pragma unroll
     for (int t = 0; t < R; ++t) {
       const int p = pb + t;
-      if (p < p1) {
-        if (p >= next) {
-          while (p >= next) {
-            ++run;
-            next = (run + 1 < q.rend) ? q.runs[run + 1].start : INT_MAX;
-          }
-          load(run);
-        }
-        const long long gi = q.gbase + (long long)q.gstep * p;
-        double acc = in ? in[gi] : 0.0;
+      buf[t] = (HAS_IN && p < p1) ? in[q.gbase + gs * p] : 0.0;
+    }
+  };
+  if (kAhead) fetch(p0);
+  for (int pb = p0; pb < p1; pb += R) {
+    double cur[R];
+    if (kAhead) {
+#pragma unroll
+      for (int t = 0; t < R; ++t) cur[t] = buf[t];
+      fetch(pb + R);
+    } else {
+#pragma unroll
+      for (int t = 0; t < R; ++t) {
+        const int p = pb + t;
+        cur[t] = (HAS_IN && p < p1) ? in[q.gbase + gs * p] : 0.0;
+      }
+    }
+    if (pb + R <= p1 && pb + R <= next) {
+#pragma unroll
+      for (int t = 0; t < R; ++t) {
+        double acc = cur[t];
 #pragma unroll
         for (int d = W; d >= 1; --d) acc -= K[d] * v[(t - d + 2 * R) % R];
         v[t] = acc * kinv;
-        if (out) out[gi] = v[t];
+        if (HAS_OUT) out[q.gbase + gs * (pb + t)] = v[t];
+      }
+    } else {
+#pragma unroll
+      for (int t = 0; t < R; ++t) {
+        const int p = pb + t;
+        if (p < p1) {
+          if (p >= next) {
+            while (p >= next) {
+              ++run;
+              next = (run + 1 < q.rend) ? q.runs[run + 1].start : INT_MAX;
+            }
+            load(run);
+          }
+          double acc = cur[t];
+#pragma unroll
+          for (int d = W; d >= 1; --d) acc -= K[d] * v[(t - d + 2 * R) % R];
+          v[t] = acc * kinv;
+          if (HAS_OUT) out[q.gbase + gs * p] = v[t];
+        }
       }
     }
   }
@@ -240,12 +316,13 @@ __device__ __forceinline__ void recur_reg(int w, const Seq &q, int run, int p0, 
   }
 }
 
-template <int W>
+template <int W, bool HAS_IN, bool HAS_OUT>
 __device__ __forceinline__ void recur(int w, const Seq &q, int run, int p0, int p1,
                                       const double *in, const double *state, double *out,
                                       double *tail) {
-  if (W == 0) recur_generic(w, q, run, p0, p1, in, state, out, tail);
-  else recur_reg<(W > 0 ? W : 1)>(w, q, run, p0, p1, in, state, out, tail);
+  if (W == 0) recur_generic(w, q, run, p0, p1, HAS_IN ? in : nullptr, state,
+                            HAS_OUT ? out : nullptr, tail);
+  else recur_reg<(W > 0 ? W : 1), HAS_IN, HAS_OUT>(w, q, run, p0, p1, in, state, out, tail);
 }
 
 // mode 0: forward pass 1 (tails -> wp)
@@ -265,42 +342,47 @@ __global__ void __launch_bounds__(64) k_band2_pass(const PSeg *segs, const PChun
   if (mode <= 1) {
     const Seq f = fwd_seq(g, runs, tab);
     if (mode == 0) {
-      recur<W>(w, f, k.run_f, k.a, k.b, r, nullptr, nullptr,
-               k.last ? nullptr : wp + (long long)c * kBand2State);
+      recur<W, true, false>(w, f, k.run_f, k.a, k.b, r, nullptr, nullptr,
+                            k.last ? nullptr : wp + (long long)c * kBand2State);
       return;
     }
-    recur<W>(w, f, k.run_f, k.a, k.b, r, k.first ? nullptr : ws + (long long)(c - 1) * kBand2State,
-             z, nullptr);
+    recur<W, true, true>(w, f, k.run_f, k.a, k.b, r,
+                         k.first ? nullptr : ws + (long long)(c - 1) * kBand2State, z, nullptr);
     const Seq b = bwd_seq(g, cruns, tab);
-    recur<W>(w, b, k.run_b, g.n - k.b, g.n - k.a, z, nullptr, nullptr,
-             k.first ? nullptr : wp + (long long)c * kBand2State);
+    recur<W, true, false>(w, b, k.run_b, g.n - k.b, g.n - k.a, z, nullptr, nullptr,
+                          k.first ? nullptr : wp + (long long)c * kBand2State);
     return;
   }
   const Seq b = bwd_seq(g, cruns, tab);
-  recur<W>(w, b, k.run_b, g.n - k.b, g.n - k.a, z,
-           k.last ? nullptr : ws + (long long)(c + 1) * kBand2State, z, nullptr);
+  recur<W, true, true>(w, b, k.run_b, g.n - k.b, g.n - k.a, z,
+                       k.last ? nullptr : ws + (long long)(c + 1) * kBand2State, z, nullptr);
 }
 
 // Transfer matrices: column q of T = response of the tail to the unit state
-// e_q with zero input.
-__global__ void k_band2_transfer(const PSeg *segs, const PChunk *ch, const PTrans *tr, int ntr,
-                                 const PRun *runs, const PRun *cruns, const double *tab,
+// e_q with zero input; one thread per (matrix, q).
+template <int W>
+__global__ void k_band2_transfer(const PSeg *segs, const PChunk *ch, const PTrans *tr, int t0,
+                                 int t1, const PRun *runs, const PRun *cruns, const double *tab,
                                  double *T) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ntr) return;
+  constexpr int WS = W > 0 ? W : kRing - 1;
+  const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long t = t0 + gid / WS;
+  const int qq = (int)(gid % WS);
+  if (t >= t1) return;
   const PTrans e = tr[t];
   const PChunk k = ch[e.chunk];
   const PSeg g = segs[k.seg];
   const int w = g.nb - 1;
-  double unit[kRing], res[kRing];
-  double *Tm = T + e.off;
-  const Seq f = fwd_seq(g, runs, tab), b = bwd_seq(g, cruns, tab);
-  for (int q = 0; q < w; ++q) {
-    for (int i = 0; i < w; ++i) unit[i] = (i == q) ? 1.0 : 0.0;
-    if (e.dir == 0) recur_generic(w, f, k.run_f, k.a, k.b, nullptr, unit, nullptr, res);
-    else recur_generic(w, b, k.run_b, g.n - k.b, g.n - k.a, nullptr, unit, nullptr, res);
-    for (int i = 0; i < w; ++i) Tm[(long long)i * w + q] = res[i];
-  }
+  if (qq >= w) return;
+  double unit[WS], res[WS];
+  for (int i = 0; i < w; ++i) unit[i] = (i == qq) ? 1.0 : 0.0;
+  if (e.dir == 0)
+    recur<W, false, false>(w, fwd_seq(g, runs, tab), k.run_f, k.a, k.b, nullptr, unit, nullptr,
+                           res);
+  else
+    recur<W, false, false>(w, bwd_seq(g, cruns, tab), k.run_b, g.n - k.b, g.n - k.a, nullptr,
+                           unit, nullptr, res);
+  for (int i = 0; i < w; ++i) T[e.off + (long long)i * w + qq] = res[i];
 }
 
 // State propagation across chunks, one warp per segment.
@@ -370,6 +452,58 @@ __global__ void k_band2_scan(const PSeg *segs, int nseg, const PChunk *ch, const
   }
 }
 
+// The same propagation with the state in registers (lane i holds s_i,
+// w <= W <= 32): lane i keeps row i of the current T_c in registers (reloaded
+// only when the matrix changes) and gathers the state by shuffles; the next
+// chunk's particular state and matrix offset are loaded one step ahead.
+template <int W>
+__global__ void k_band2_scan_reg(const PSeg *segs, int s0, int s1, const PChunk *ch,
+                                 const double *T, const double *p, double *s, int dir) {
+  const int seg = s0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (seg >= s1) return;
+  const PSeg g = segs[seg];
+  const int w = g.nb - 1;
+  if (g.nch <= 1 || w <= 0) return;
+  const bool on = lane < w;
+  const int c0 = g.ch_off, cl = g.ch_off + g.nch - 1;
+  const int start = dir == 0 ? c0 : cl;
+  const int stop = dir == 0 ? cl : c0;  // exclusive
+  const int step = dir == 0 ? 1 : -1;
+  double cur = on ? p[(long long)start * kBand2State + lane] : 0.0;
+  if (on) s[(long long)start * kBand2State + lane] = cur;
+  double Tr[W];
+  int tcur = -1;
+  int c = start + step;
+  if (c == stop) return;
+  double pn = on ? p[(long long)c * kBand2State + lane] : 0.0;
+  int tn = dir == 0 ? ch[c].tf : ch[c].tb;
+  for (; c != stop; c += step) {
+    const double pc = pn;
+    const int tc = tn;
+    const int cn = c + step;
+    if (cn != stop) {
+      pn = on ? p[(long long)cn * kBand2State + lane] : 0.0;
+      tn = dir == 0 ? ch[cn].tf : ch[cn].tb;
+    }
+    if (tc != tcur) {
+#pragma unroll
+      for (int qq = 0; qq < W; ++qq) Tr[qq] = (on && qq < w) ? T[tc + (long long)lane * w + qq] : 0.0;
+      tcur = tc;
+    }
+    double a0 = pc, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+    for (int qq = 0; qq < W; qq += 4) {
+      a0 += Tr[qq] * __shfl_sync(0xffffffffu, cur, qq);
+      if (qq + 1 < W) a1 += Tr[qq + 1] * __shfl_sync(0xffffffffu, cur, qq + 1);
+      if (qq + 2 < W) a2 += Tr[qq + 2] * __shfl_sync(0xffffffffu, cur, qq + 2);
+      if (qq + 3 < W) a3 += Tr[qq + 3] * __shfl_sync(0xffffffffu, cur, qq + 3);
+    }
+    cur = on ? (a0 + a1) + (a2 + a3) : 0.0;
+    if (on) s[(long long)c * kBand2State + lane] = cur;
+  }
+}
+
 template <int W>
 void launch_pass(cudaStream_t st, const PSeg *segs, const PChunk *ch, int c0, int c1,
                  const PRun *runs, const PRun *cruns, const double *tab, int mode, const double *r,
@@ -417,7 +551,7 @@ void band2_factor(cudaStream_t st, const PSeg *segs, int nseg, const int *spec,
                   const double *invcov, long long nof, const double *nna, double *rows,
                   PRun *runs, int *status, int *nunique, int *nruns) {
   if (nseg == 0) return;
-  MADAM_LAUNCH(k_band2_factor, (nseg + 31) / 32, 32, 0, st, segs, nseg, spec, invcov, nof, nna,
+  MADAM_LAUNCH(k_band2_factor, (unsigned)nseg, 32, 0, st, segs, nseg, spec, invcov, nof, nna,
                rows, runs, status, nunique, nruns);
 }
 
@@ -428,29 +562,86 @@ void band2_columns(cudaStream_t st, const PSeg *segs, int nseg, int max_ncrun, c
   MADAM_LAUNCH(k_band2_columns, grid, 256, 0, st, segs, runs, cruns, tab);
 }
 
-void band2_transfer(cudaStream_t st, const PSeg *segs, const PChunk *ch, const PTrans *tr, int ntr,
-                    const PRun *runs, const PRun *cruns, const double *tab, double *T) {
-  if (ntr == 0) return;
-  MADAM_LAUNCH(k_band2_transfer, (ntr + 63) / 64, 64, 0, st, segs, ch, tr, ntr, runs, cruns, tab,
-               T);
+void band2_transfer(cudaStream_t st, const PSeg *segs, const PChunk *ch, const PTrans *tr,
+                    const int *cls_w, const int *tcls_begin, int ncls, const PRun *runs,
+                    const PRun *cruns, const double *tab, double *T) {
+  for (int i = 0; i < ncls; ++i) {
+    const int t0 = tcls_begin[i], t1 = tcls_begin[i + 1];
+    if (t1 <= t0) continue;
+    const int W = cls_w[i];
+    const long long nthr = (long long)(t1 - t0) * (W > 0 ? W : kRing - 1);
+    const unsigned grid = (unsigned)((nthr + 63) / 64);
+    switch (W) {
+#define MADAM_BAND2_CASE(X)                                                                 \
+  case X:                                                                                   \
+    MADAM_LAUNCH(k_band2_transfer<X>, grid, 64, 0, st, segs, ch, tr, t0, t1, runs, cruns, tab, \
+                 T);                                                                        \
+    break;
+      MADAM_BAND2_CASE(1)
+      MADAM_BAND2_CASE(2)
+      MADAM_BAND2_CASE(4)
+      MADAM_BAND2_CASE(8)
+      MADAM_BAND2_CASE(9)
+      MADAM_BAND2_CASE(12)
+      MADAM_BAND2_CASE(16)
+      MADAM_BAND2_CASE(19)
+      MADAM_BAND2_CASE(24)
+      MADAM_BAND2_CASE(29)
+      MADAM_BAND2_CASE(32)
+#undef MADAM_BAND2_CASE
+      default:
+        MADAM_LAUNCH(k_band2_transfer<0>, grid, 64, 0, st, segs, ch, tr, t0, t1, runs, cruns, tab,
+                     T);
+        break;
+    }
+  }
 }
 
 void band2_solve(cudaStream_t st, const PSeg *segs, int nseg, const PChunk *ch, int nch,
-                 const int *cls_w, const int *cls_begin, int ncls, const PRun *runs,
-                 const PRun *cruns, const double *tab, const double *T, const double *r, double *z,
-                 double *work_p, double *work_s) {
+                 const int *cls_w, const int *cls_begin, const int *cls_seg, int ncls,
+                 const PRun *runs, const PRun *cruns, const double *tab, const double *T,
+                 const double *r, double *z, double *work_p, double *work_s) {
   if (nch == 0) return;
-  const unsigned gs = (nseg + kScanWarps - 1) / kScanWarps;
   auto passes = [&](int mode) {
     for (int i = 0; i < ncls; ++i)
       if (cls_begin[i + 1] > cls_begin[i])
         pass_class(cls_w[i], st, segs, ch, cls_begin[i], cls_begin[i + 1], runs, cruns, tab, mode,
                    r, z, work_s, work_p);
   };
+  auto scans = [&](int dir) {
+    for (int i = 0; i < ncls; ++i) {
+      const int s0 = cls_seg[i], s1 = cls_seg[i + 1];
+      if (s1 <= s0) continue;
+      const unsigned grid = (unsigned)((s1 - s0 + 1) / 2);
+      switch (cls_w[i]) {
+#define MADAM_BAND2_CASE(X)                                                                   \
+  case X:                                                                                     \
+    MADAM_LAUNCH(k_band2_scan_reg<X>, grid, 64, 0, st, segs, s0, s1, ch, T, work_p, work_s,    \
+                 dir);                                                                        \
+    break;
+        MADAM_BAND2_CASE(1)
+        MADAM_BAND2_CASE(2)
+        MADAM_BAND2_CASE(4)
+        MADAM_BAND2_CASE(8)
+        MADAM_BAND2_CASE(9)
+        MADAM_BAND2_CASE(12)
+        MADAM_BAND2_CASE(16)
+        MADAM_BAND2_CASE(19)
+        MADAM_BAND2_CASE(24)
+        MADAM_BAND2_CASE(29)
+        MADAM_BAND2_CASE(32)
+#undef MADAM_BAND2_CASE
+        default:
+          MADAM_LAUNCH(k_band2_scan, (unsigned)((s1 - s0 + kScanWarps - 1) / kScanWarps),
+                       32 * kScanWarps, 0, st, segs + s0, s1 - s0, ch, T, work_p, work_s, dir);
+          break;
+      }
+    }
+  };
   passes(0);
-  MADAM_LAUNCH(k_band2_scan, gs, 32 * kScanWarps, 0, st, segs, nseg, ch, T, work_p, work_s, 0);
+  scans(0);
   passes(1);
-  MADAM_LAUNCH(k_band2_scan, gs, 32 * kScanWarps, 0, st, segs, nseg, ch, T, work_p, work_s, 1);
+  scans(1);
   passes(2);
 }
 

@@ -45,7 +45,7 @@ struct PTrans {
 constexpr int kBand2MaxWidth = 128;
 constexpr int kBand2State = 128;  // doubles per chunk state slot (>= w)
 
-// Factor one segment per thread; rows: worst case n * (nb + 1) doubles at
+// Factor one segment per warp; rows: worst case n * (nb + 1) doubles at
 // seg.row_off, runs: worst case n at seg.run_off.
 void band2_factor(cudaStream_t st, const PSeg *segs, int nseg, const int *spec,
                   const double *invcov, long long nof, const double *nna, double *rows,
@@ -53,14 +53,17 @@ void band2_factor(cudaStream_t st, const PSeg *segs, int nseg, const int *spec,
 // Assemble the backward entries flagged in the column runs.
 void band2_columns(cudaStream_t st, const PSeg *segs, int nseg, int max_ncrun, const PRun *runs,
                    const PRun *cruns, double *tab);
-void band2_transfer(cudaStream_t st, const PSeg *segs, const PChunk *ch, const PTrans *tr, int ntr,
-                    const PRun *runs, const PRun *cruns, const double *tab, double *T);
-// Solve L L^T z = r on every factored segment.  classes: chunk ranges
-// [cls_begin[i], cls_begin[i + 1]) whose segments have w <= cls_w[i].
+// Transfer matrices; tcls_begin: transfer ranges of the width classes.
+void band2_transfer(cudaStream_t st, const PSeg *segs, const PChunk *ch, const PTrans *tr,
+                    const int *cls_w, const int *tcls_begin, int ncls, const PRun *runs,
+                    const PRun *cruns, const double *tab, double *T);
+// Solve L L^T z = r on every factored segment.  Width class i: chunks
+// [cls_begin[i], cls_begin[i + 1]) of segments [cls_seg[i], cls_seg[i + 1])
+// with w <= cls_w[i] (host arrays).
 void band2_solve(cudaStream_t st, const PSeg *segs, int nseg, const PChunk *ch, int nch,
-                 const int *cls_w, const int *cls_begin, int ncls, const PRun *runs,
-                 const PRun *cruns, const double *tab, const double *T, const double *r, double *z,
-                 double *work_p, double *work_s);
+                 const int *cls_w, const int *cls_begin, const int *cls_seg, int ncls,
+                 const PRun *runs, const PRun *cruns, const double *tab, const double *T,
+                 const double *r, double *z, double *work_p, double *work_s);
 // Smallest compiled register width >= w (0 when w needs the generic path).
 int band2_class_width(int w);
 

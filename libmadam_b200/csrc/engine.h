@@ -243,7 +243,7 @@ class Engine {
   long long band2_rows_ = 0;
   long band2_ntrans_ = 0;
   int band2_chunk_ = 0;
-  std::vector<int> band2_cls_w_, band2_cls_begin_;
+  std::vector<int> band2_cls_w_, band2_cls_begin_, band2_cls_seg_;
   long n_band_fail_ = 0;
   std::unique_ptr<FFTPlan> fft_;
   std::unique_ptr<CgpWork> cgp_;

@@ -1137,6 +1137,8 @@ void Engine::construct_preconditioner() {
   }
   band2_cls_w_.clear();
   band2_cls_begin_.clear();
+  band2_cls_seg_.clear();
+  std::vector<int> tcls_begin;
   int max_ncrun = 0;
   std::map<std::pair<long long, int>, long long> tcache;
   long long toff = 0;
@@ -1147,6 +1149,8 @@ void Engine::construct_preconditioner() {
     if (band2_cls_w_.empty() || band2_cls_w_.back() != pk.W) {
       band2_cls_w_.push_back(pk.W);
       band2_cls_begin_.push_back((int)chunks.size());
+      band2_cls_seg_.push_back((int)si);
+      tcls_begin.push_back((int)trans.size());
     }
     q.run_off = (int)pruns.size();
     q.nrun = pk.dn->nr;
@@ -1220,6 +1224,8 @@ void Engine::construct_preconditioner() {
     }
   }
   band2_cls_begin_.push_back((int)chunks.size());
+  band2_cls_seg_.push_back((int)pseg.size());
+  tcls_begin.push_back((int)trans.size());
   if (toff >= (1LL << 31)) fail("too many band transfer matrices");
   p2nseg_ = (int)pseg.size();
   p2nch_ = (int)chunks.size();
@@ -1254,8 +1260,9 @@ void Engine::construct_preconditioner() {
     if (!trans.empty()) {
       MADAM_CUDA(cudaMemcpyAsync(dtr.get(), trans.data(), trans.size() * sizeof(PTrans),
                                  cudaMemcpyHostToDevice, st_));
-      band2_transfer(st_, p2segs_.get(), p2ch_.get(), dtr.get(), (int)trans.size(),
-                     p2runs_.get(), p2cruns_.get(), p2rows_.get(), p2T_.get());
+      band2_transfer(st_, p2segs_.get(), p2ch_.get(), dtr.get(), band2_cls_w_.data(),
+                     tcls_begin.data(), (int)band2_cls_w_.size(), p2runs_.get(), p2cruns_.get(),
+                     p2rows_.get(), p2T_.get());
     }
     MADAM_CUDA(cudaStreamSynchronize(st_));
   }
@@ -1447,8 +1454,9 @@ void Engine::apply_preconditioner(const double *r, double *z) {
     return;
   }
   band2_solve(st_, p2segs_.get(), p2nseg_, p2ch_.get(), p2nch_, band2_cls_w_.data(),
-              band2_cls_begin_.data(), (int)band2_cls_w_.size(), p2runs_.get(), p2cruns_.get(),
-              p2rows_.get(), p2T_.get(), r, z, p2wp_.get(), p2ws_.get());
+              band2_cls_begin_.data(), band2_cls_seg_.data(), (int)band2_cls_w_.size(),
+              p2runs_.get(), p2cruns_.get(), p2rows_.get(), p2T_.get(), r, z, p2wp_.get(),
+              p2ws_.get());
   band_solve(st_, band_segs_d_.get(), (int)band_segs_.size(), band_.get(), r, z);
   cg_preconditioner_segments(r, z);
 }

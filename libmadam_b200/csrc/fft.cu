@@ -273,43 +273,195 @@ __global__ void k_conv_small(const ConvSeg *segs, const double *spectra, long lo
   }
 }
 
+// ------------------------------------------------------ Stockham FFT --
+// Batched radix-8 Stockham transforms for the four-step passes.  Pass p
+// (sub-transform size Ns = 8^p) takes the eight elements j + k L/8 of a
+// length-L transform into registers, multiplies element k by the twiddle
+// w_L^{(j mod Ns) k L/(8 Ns)}, does an 8-point DFT in registers and writes
+// element k to (j / Ns) 8 Ns + (j mod Ns) + k Ns: natural order in and out,
+// no bit reversal.  A last radix-4 or radix-2 pass finishes lengths that are
+// not powers of 8.  Every thread holds eight values per pass; shared-memory
+// rows are padded one slot in nine (pad8) so that strided accesses spread
+// over the banks.  The first pass may read from global memory and the last
+// pass write to it through the load / store functors.
+__device__ __forceinline__ int pad8(int i) { return i + (i >> 3); }
+
+template <bool INV>
+__device__ __forceinline__ cplx tw_l(const cplx *T2, long long q, long long step) {
+  const cplx w = T2[q * step];  // exp(-2 pi i q / L), step = 2N / L
+  return INV ? cconj(w) : w;
+}
+
+template <bool INV>
+__device__ __forceinline__ cplx mul_mi(cplx a) {  // a * (-i), inverse a * i
+  return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+
+template <bool INV>
+__device__ __forceinline__ cplx mul_w8(cplx a) {  // a * exp(-+ 2 pi i / 8)
+  const double c = 0.70710678118654752440;
+  return INV ? make_double2(c * (a.x - a.y), c * (a.x + a.y))
+             : make_double2(c * (a.x + a.y), c * (a.y - a.x));
+}
+
+template <bool INV>
+__device__ __forceinline__ cplx mul_w83(cplx a) {  // a * exp(-+ 6 pi i / 8)
+  const double c = 0.70710678118654752440;
+  return INV ? make_double2(-c * (a.x + a.y), c * (a.x - a.y))
+             : make_double2(c * (a.y - a.x), -c * (a.x + a.y));
+}
+
+// 8-point DFT in registers, natural order in and out
+template <bool INV>
+__device__ __forceinline__ void dft8(cplx *v) {
+  const cplx a0 = cadd(v[0], v[4]), b0 = csub(v[0], v[4]);
+  const cplx a1 = cadd(v[1], v[5]), b1 = mul_w8<INV>(csub(v[1], v[5]));
+  const cplx a2 = cadd(v[2], v[6]), b2 = mul_mi<INV>(csub(v[2], v[6]));
+  const cplx a3 = cadd(v[3], v[7]), b3 = mul_w83<INV>(csub(v[3], v[7]));
+  const cplx c0 = cadd(a0, a2), d0 = csub(a0, a2), c1 = cadd(a1, a3);
+  const cplx d1 = mul_mi<INV>(csub(a1, a3));
+  v[0] = cadd(c0, c1);
+  v[4] = csub(c0, c1);
+  v[2] = cadd(d0, d1);
+  v[6] = csub(d0, d1);
+  const cplx e0 = cadd(b0, b2), f0 = csub(b0, b2), e1 = cadd(b1, b3);
+  const cplx f1 = mul_mi<INV>(csub(b1, b3));
+  v[1] = cadd(e0, e1);
+  v[5] = csub(e0, e1);
+  v[3] = cadd(f0, f1);
+  v[7] = csub(f0, f1);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(cplx *v) {
+  const cplx c0 = cadd(v[0], v[2]), d0 = csub(v[0], v[2]), c1 = cadd(v[1], v[3]);
+  const cplx d1 = mul_mi<INV>(csub(v[1], v[3]));
+  v[0] = cadd(c0, c1);
+  v[2] = csub(c0, c1);
+  v[1] = cadd(d0, d1);
+  v[3] = csub(d0, d1);
+}
+
+// Last radix-R pass (R = 2 or 4, Ns = L / R): butterflies j < L / R over the
+// elements j + k L / R; each thread takes 8 / R butterflies.
+template <int R, bool INV, bool FFAST, typename Store>
+__device__ __forceinline__ void last_pass(cplx *s, int S, int L, int nfft, const cplx *T2,
+                                          long long step, int nb8, Store store) {
+  constexpr int PER = 8 / R;
+  const int Lr = L / R, t = threadIdx.x;
+  cplx v[PER][R];
+  int ff[PER], jj[PER];
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int q = t + u * nb8;
+    ff[u] = -1;
+    jj[u] = 0;
+    if (q < nfft * Lr) {
+      ff[u] = FFAST ? q % nfft : q / Lr;
+      jj[u] = FFAST ? q / nfft : q % Lr;
+#pragma unroll
+      for (int k = 0; k < R; ++k) v[u][k] = s[ff[u] * S + pad8(jj[u] + k * Lr)];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    if (ff[u] < 0) continue;
+#pragma unroll
+    for (int k = 1; k < R; ++k) v[u][k] = cmul(v[u][k], tw_l<INV>(T2, (long long)jj[u] * k, step));
+    if (R == 4) {
+      dft4<INV>(v[u]);
+    } else {
+      const cplx a = v[u][0], b = v[u][1];
+      v[u][0] = cadd(a, b);
+      v[u][1] = csub(a, b);
+    }
+#pragma unroll
+    for (int k = 0; k < R; ++k) store(ff[u], jj[u] + k * Lr, v[u][k]);
+  }
+  __syncthreads();
+}
+
+// nfft transforms of length L (>= 64) at s + f * S; blockDim.x >= nfft L / 8.
+// FFAST: consecutive threads take consecutive transforms f (else consecutive
+// j).  load(f, i) gives input element i of transform f for the first pass;
+// store(f, i, v) takes output element i of the last pass.
+template <bool INV, bool FFAST, typename Load, typename Store>
+__device__ __forceinline__ void fft_block(cplx *s, int S, int L, int logL, int nfft,
+                                          const cplx *T2, long long N, Load load, Store store) {
+  const int L8 = L >> 3, n8 = logL / 3, rem = logL - 3 * n8;
+  const long long step = 2 * N / L;
+  const int nb8 = nfft * L8;
+  const int t = threadIdx.x;
+  int Ns = 1;
+  for (int pass = 0; pass < n8; ++pass) {
+    const bool first = pass == 0, last = pass == n8 - 1 && rem == 0;
+    const bool act = t < nb8;
+    const int f = FFAST ? t % nfft : t / L8;
+    const int j = FFAST ? t / nfft : t % L8;
+    cplx v[8];
+    if (act) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        v[k] = first ? load(f, j + k * L8) : s[f * S + pad8(j + k * L8)];
+    }
+    __syncthreads();
+    if (act) {
+      if (!first) {
+        const long long r = j & (Ns - 1);
+        const long long qs = r * (L / (8 * Ns));
+#pragma unroll
+        for (int k = 1; k < 8; ++k) v[k] = cmul(v[k], tw_l<INV>(T2, qs * k, step));
+      }
+      dft8<INV>(v);
+      if (last) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) store(f, j + k * L8, v[k]);
+      } else {
+        const int base = (j / Ns) * Ns * 8 + (j & (Ns - 1));
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s[f * S + pad8(base + k * Ns)] = v[k];
+      }
+    }
+    __syncthreads();
+    Ns *= 8;
+  }
+  if (rem == 1) last_pass<2, INV, FFAST>(s, S, L, nfft, T2, step, nb8, store);
+  else if (rem == 2) last_pass<4, INV, FFAST>(s, S, L, nfft, T2, step, nb8, store);
+}
+
 // ------------------------------------------------------- four-step path --
 // Pass 1: forward column FFTs (length R) of G adjacent columns, twiddled.
-__global__ void k_conv_cols_fwd(const ConvSeg *segs, const double *x, const double *part,
-                                double2 *work, int R, int logR, int C, int G, const cplx *T2) {
+__global__ void __launch_bounds__(512, 2) k_conv_cols_fwd(const ConvSeg *segs, const double *x,
+                                                       const double *part, double2 *work, int R,
+                                                       int logR, int C, int G, const cplx *T2) {
   extern __shared__ double2 sm[];
-  cplx *s = sm;            // G columns x R
-  cplx *tw = sm + G * R;   // R/2
+  const int S = pad8(R) + 1;
   const int seg = blockIdx.y;
   const ConvSeg sg = segs[seg];
   const double mean = seg_mean(part, seg, sg.n_in, sg.flags & 1);
   const int c0 = blockIdx.x * G;
-  fill_twiddles(tw, R, T2, (long long)R * C);
-  for (int e = threadIdx.x; e < G * R; e += blockDim.x) {
-    const int c = e % G, n1 = e / G;
-    const long long m = (long long)C * n1 + c0 + c;
-    const double a = seg_input(x, sg, 2 * m, mean);
-    const double b = seg_input(x, sg, 2 * m + 1, mean);
-    s[c * R + bitrev(n1, logR)] = make_double2(a, b);
-  }
-  __syncthreads();
-  fft_dit(s, R, G, tw, false);
   const long long N = (long long)R * C;
   double2 *W = work + (long long)seg * N;
-  for (int e = threadIdx.x; e < G * R; e += blockDim.x) {
-    const int c = e % G, k1 = e / G;
-    const int n2 = c0 + c;
-    W[(long long)k1 * C + n2] = cmul(s[c * R + k1], tw_n(T2, (long long)n2 * k1, N));
-  }
+  auto load = [&](int f, int n1) {
+    const long long m = (long long)C * n1 + c0 + f;
+    return make_double2(seg_input(x, sg, 2 * m, mean), seg_input(x, sg, 2 * m + 1, mean));
+  };
+  auto store = [&](int f, int k1, cplx v) {
+    const int n2 = c0 + f;
+    W[(long long)k1 * C + n2] = cmul(v, tw_n(T2, (long long)n2 * k1, N));
+  };
+  fft_block<false, true>(sm, S, R, logR, G, T2, N, load, store);
 }
 
 // Pass 2: forward row FFTs of rows k1 and R-k1, spectral product, inverse
 // row FFTs, inverse twiddles.
-__global__ void k_conv_rows(const ConvSeg *segs, const double *spectra, long long spec_len,
-                            double2 *work, int R, int C, int logC, const cplx *T2) {
+__global__ void __launch_bounds__(1024) k_conv_rows(const ConvSeg *segs, const double *spectra,
+                                                    long long spec_len, double2 *work, int R,
+                                                    int C, int logC, const cplx *T2) {
   extern __shared__ double2 sm[];
-  cplx *tw = sm;               // C/2
-  cplx *s = sm + C / 2;        // 2 rows x C
+  const int S = pad8(C) + 1;
+  cplx *s = sm;  // 2 rows
   const int seg = blockIdx.y;
   const ConvSeg sg = segs[seg];
   const long long N = (long long)R * C;
@@ -317,81 +469,67 @@ __global__ void k_conv_rows(const ConvSeg *segs, const double *spectra, long lon
   const int j = blockIdx.x;            // 0 .. R/2
   const int ka = j, kb = (R - j) % R;  // row pair (equal for j = 0, R/2)
   const int nrows = (ka == kb) ? 1 : 2;
-  fill_twiddles(tw, C, T2, N);
-  for (int e = threadIdx.x; e < nrows * C; e += blockDim.x) {
-    const int r = e / C, n2 = e % C;
-    const int k1 = r ? kb : ka;
-    s[r * C + bitrev(n2, logC)] = W[(long long)k1 * C + n2];
-  }
-  __syncthreads();
-  fft_dit(s, C, nrows, tw, false);
+  auto gload = [&](int f, int n2) { return W[(long long)(f ? kb : ka) * C + n2]; };
+  auto sload = [&](int f, int n2) { return s[f * S + pad8(n2)]; };
+  auto sstore = [&](int f, int n2, cplx v) { s[f * S + pad8(n2)] = v; };
+  fft_block<false, false>(s, S, C, logC, nrows, T2, N, gload, sstore);
   const double *H = spectra + (long long)sg.spec * spec_len;
+  auto at = [&](int f, int n2) -> cplx & { return s[f * S + pad8(n2)]; };
   if (ka == 0) {
     // row 0: (0, k2) <-> (0, C - k2)
     for (int k2 = threadIdx.x; k2 <= C / 2; k2 += blockDim.x) {
       const int p2 = (C - k2) % C;
-      cplx A = s[k2], B = s[p2];
+      cplx A = at(0, k2), B = at(0, p2);
       spectral_pair(A, B, (long long)R * k2, N, H, T2);
-      s[k2] = A;
-      if (p2 != k2) s[p2] = B;
+      at(0, k2) = A;
+      if (p2 != k2) at(0, p2) = B;
     }
   } else if (ka == kb) {
     // row R/2: (R/2, k2) <-> (R/2, C - 1 - k2)
     for (int k2 = threadIdx.x; k2 < C / 2; k2 += blockDim.x) {
       const int p2 = C - 1 - k2;
-      cplx A = s[k2], B = s[p2];
+      cplx A = at(0, k2), B = at(0, p2);
       spectral_pair(A, B, ka + (long long)R * k2, N, H, T2);
-      s[k2] = A;
-      s[p2] = B;
+      at(0, k2) = A;
+      at(0, p2) = B;
     }
   } else {
     // rows ka, kb = R - ka: (ka, k2) <-> (kb, C - 1 - k2)
     for (int k2 = threadIdx.x; k2 < C; k2 += blockDim.x) {
       const int p2 = C - 1 - k2;
-      cplx A = s[k2], B = s[C + p2];
+      cplx A = at(0, k2), B = at(1, p2);
       spectral_pair(A, B, ka + (long long)R * k2, N, H, T2);
-      s[k2] = A;
-      s[C + p2] = B;
+      at(0, k2) = A;
+      at(1, p2) = B;
     }
   }
   __syncthreads();
-  fft_dif(s, C, nrows, tw, true);
-  for (int e = threadIdx.x; e < nrows * C; e += blockDim.x) {
-    const int r = e / C, n2 = e % C;
-    const int k1 = r ? kb : ka;
-    const cplx v = s[r * C + bitrev(n2, logC)];
+  auto gstore = [&](int f, int n2, cplx v) {
+    const int k1 = f ? kb : ka;
     W[(long long)k1 * C + n2] = cmul(v, cconj(tw_n(T2, (long long)n2 * k1, N)));
-  }
+  };
+  fft_block<true, false>(s, S, C, logC, nrows, T2, N, sload, gstore);
 }
 
 // Pass 3: inverse column FFTs and real output.
-__global__ void k_conv_cols_inv(const ConvSeg *segs, const double2 *work, double *y, int R,
-                                int logR, int C, int G, const cplx *T2) {
+__global__ void __launch_bounds__(512, 2) k_conv_cols_inv(const ConvSeg *segs, const double2 *work,
+                                                       double *y, int R, int logR, int C, int G,
+                                                       const cplx *T2) {
   extern __shared__ double2 sm[];
-  cplx *s = sm;
-  cplx *tw = sm + G * R;
+  const int S = pad8(R) + 1;
   const int seg = blockIdx.y;
   const ConvSeg sg = segs[seg];
   const int c0 = blockIdx.x * G;
   const long long N = (long long)R * C;
   const double2 *W = work + (long long)seg * N;
-  // rows n1 whose outputs are needed: 2 (C n1 + n2) < n_out
-  const int rows_needed = (int)min((long long)R, ((long long)sg.n_out + 2LL * C - 1) / (2LL * C));
-  fill_twiddles(tw, R, T2, N);
-  for (int e = threadIdx.x; e < G * R; e += blockDim.x) {
-    const int c = e % G, k1 = e / G;
-    s[c * R + k1] = W[(long long)k1 * C + c0 + c];
-  }
-  __syncthreads();
-  fft_dif(s, R, G, tw, true);
   const double scale = 1.0 / (double)N;
-  for (int e = threadIdx.x; e < G * rows_needed; e += blockDim.x) {
-    const int c = e % G, n1 = e / G;
-    const cplx v = s[c * R + bitrev(n1, logR)];
-    const long long m = (long long)C * n1 + c0 + c;
+  auto load = [&](int f, int k1) { return W[(long long)k1 * C + c0 + f]; };
+  auto store = [&](int f, int n1, cplx v) {
+    const long long m = (long long)C * n1 + c0 + f;
     if (2 * m < sg.n_out) y[sg.y_off + 2 * m] = v.x * scale;
     if (2 * m + 1 < sg.n_out) y[sg.y_off + 2 * m + 1] = v.y * scale;
-  }
+  };
+  fft_block<true, true>(sm, S, R, logR, G, T2, N, load, store);
 }
 
 int ilog2(long v) {
@@ -412,6 +550,8 @@ FFTPlan::FFTPlan(long nof_) : nof(nof_), N(nof_ / 2) {
     G = std::max(1, std::min(16, 4096 / R));
     if (G > C) G = C;
   }
+  // column passes: G transforms of length R, G R / 8 threads; row pass: two
+  // rows of length C, C / 4 threads
 }
 
 FFTPlan::~FFTPlan() {
@@ -458,8 +598,11 @@ void FFTPlan::convolve(cudaStream_t st, const ConvSeg *segs, long nseg, const do
                  means, (int)N, logN, T2);
   } else {
     const int logR = ilog2(R), logC = ilog2(C);
-    size_t smem_cols = (size_t)(G * R + R / 2) * sizeof(double2);
-    size_t smem_rows = (size_t)(2 * C + C / 2) * sizeof(double2);
+    auto padded = [](long L) { return L + L / 8 + 1; };
+    size_t smem_cols = (size_t)(G * padded(R)) * sizeof(double2);
+    size_t smem_rows = (size_t)(2 * padded(C)) * sizeof(double2);
+    const unsigned tcols = (unsigned)std::max(32, G * R / 8);
+    const unsigned trows = (unsigned)std::max(32, C / 4);
     static bool attr = false;
     if (!attr) {
       MADAM_CUDA(cudaFuncSetAttribute(k_conv_cols_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -471,12 +614,12 @@ void FFTPlan::convolve(cudaStream_t st, const ConvSeg *segs, long nseg, const do
       attr = true;
     }
     dim3 gc(C / G, (unsigned)nseg), gr(R / 2 + 1, (unsigned)nseg);
-    MADAM_LAUNCH(k_conv_cols_fwd, gc, 256, smem_cols, st, segs, x, means, (double2 *)work, R, logR,
-                 C, G, T2);
-    MADAM_LAUNCH(k_conv_rows, gr, 256, smem_rows, st, segs, spectra, spec_len, (double2 *)work, R, C,
-                 logC, T2);
-    MADAM_LAUNCH(k_conv_cols_inv, gc, 256, smem_cols, st, segs, (const double2 *)work, y, R, logR,
-                 C, G, T2);
+    MADAM_LAUNCH(k_conv_cols_fwd, gc, tcols, smem_cols, st, segs, x, means, (double2 *)work, R,
+                 logR, C, G, T2);
+    MADAM_LAUNCH(k_conv_rows, gr, trows, smem_rows, st, segs, spectra, spec_len, (double2 *)work, R,
+                 C, logC, T2);
+    MADAM_LAUNCH(k_conv_cols_inv, gc, tcols, smem_cols, st, segs, (const double2 *)work, y, R,
+                 logR, C, G, T2);
   }
   MADAM_LAUNCH(k_seg_sum, gm, 256, 0, st, segs, y, 1, means);
   MADAM_LAUNCH(k_seg_sub_mean, gm, 256, 0, st, segs, y, means);
