@@ -20,6 +20,9 @@
 
 namespace madam {
 
+constexpr int kRedBlocks = 1184;      // 148 SMs x 8, fixed for determinism
+
+
 // Owning device allocation.
 template <typename T>
 struct DevBuf {
@@ -144,7 +147,7 @@ class Engine {
   void convolve(const double *x, double *y, const std::vector<ConvSeg> &segs,
                 const double *spectra, DevBuf<ConvSeg> &dsegs);
   void cg_preconditioner_segments(const double *r, double *z);
-  void finish_dots(int nd, int mode, int slot0);
+  void finish_dots(int nd, int mode, int slot0, int nblk = kRedBlocks);
 
   Params par_;
   std::vector<Detector> dets_;
@@ -201,6 +204,8 @@ class Engine {
   DevBuf<float4> sp4_;        // pixel-sorted pointing {w, baseline}
   DevBuf<int2> sp2_;          // pixel-sorted baseline (temperature only)
   DevBuf<int> csr_off_;       // nloc_cross + 1 offsets
+  DevBuf<int2> scatter_tiles_;  // pixel tiles {first, end} of the scatter
+  int nscatter_tiles_ = 0;
   long long csr_nvalid_ = 0;
   DevBuf<long long> istart_d_;
   DevBuf<int> kstart_d_;

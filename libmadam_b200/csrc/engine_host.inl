@@ -522,6 +522,7 @@ void Engine::build_csr() {
   // pixel-sorted copy of the pointing for the PCG scatter (k_scatter_csr)
   const long long n = (long long)ndet_ * nsamp_;
   csr_nvalid_ = 0;
+  nscatter_tiles_ = 0;
   csr_off_.alloc((size_t)nloc_cross_ + 1);
   if (n == 0 || nloc_cross_ == 0) {
     csr_off_.zero(st_);
@@ -576,6 +577,32 @@ void Engine::build_csr() {
     if (csr_nvalid_)
       MADAM_LAUNCH(k_csr_fill<1>, grid_for(csr_nvalid_), 256, 0, st_, keys_s.get(), vals_s.get(),
                    csr_nvalid_, point4_.get(), sm, (float4 *)nullptr, sp2_.get(), csr_off_.get());
+  }
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  // pixel tiles of the scatter: consecutive pixels with at most kGatherTile
+  // entries, or one pixel with more
+  {
+    std::vector<int> offh((size_t)nloc_cross_ + 1);
+    MADAM_CUDA(cudaMemcpy(offh.data(), csr_off_.get(), offh.size() * sizeof(int),
+                          cudaMemcpyDeviceToHost));
+    std::vector<int2> tl;
+    int pa = 0;
+    while (pa < (int)nloc_cross_) {
+      if (offh[pa + 1] - offh[pa] > kGatherTile) {
+        tl.push_back(make_int2(pa, pa + 1));
+        ++pa;
+        continue;
+      }
+      int pb = pa + 1;
+      while (pb < (int)nloc_cross_ && offh[pb + 1] - offh[pa] <= kGatherTile) ++pb;
+      tl.push_back(make_int2(pa, pb));
+      pa = pb;
+    }
+    nscatter_tiles_ = (int)tl.size();
+    scatter_tiles_.alloc(std::max<size_t>(1, tl.size()));
+    if (!tl.empty())
+      MADAM_CUDA(cudaMemcpyAsync(scatter_tiles_.get(), tl.data(), tl.size() * sizeof(int2),
+                                 cudaMemcpyHostToDevice, st_));
   }
   MADAM_CUDA(cudaStreamSynchronize(st_));
 }
@@ -1299,8 +1326,8 @@ void Engine::construct_preconditioner() {
   cg_prec_segs_ = cgk;
 }
 
-void Engine::finish_dots(int nd, int mode, int slot0) {
-  MADAM_LAUNCH(k_finish, 1, 1024, 0, st_, part_.get(), kRedBlocks, nd, scal_.get(), mode, slot0);
+void Engine::finish_dots(int nd, int mode, int slot0, int nblk) {
+  MADAM_LAUNCH(k_finish, 1, 1024, 0, st_, part_.get(), nblk, nd, scal_.get(), mode, slot0);
 }
 
 void Engine::scatter_baselines(const double *pw, double *target, bool fine) {
@@ -1332,13 +1359,20 @@ void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) 
   const long long nb = (long long)ndet_ * noba_short_;
   // 1) baseline -> map, collect, ccmultiply, scatter back (iterate_a 798-827)
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[0], st_));
-  if (nloc_cross_ > 0) {
+  static bool stream_attr = false;
+  if (!stream_attr) {
+    for (const void *f : {(const void *)k_scatter_tiled<3>, (const void *)k_scatter_tiled<1>})
+      MADAM_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kStreamSmem));
+    stream_attr = true;
+  }
+  if (nloc_cross_ > 0 && nscatter_tiles_ > 0) {
     if (nmap_ == 3)
-      MADAM_LAUNCH(k_scatter_csr<3>, kRedBlocks, 256, 0, st_, csr_off_.get(),
-                   (long long)nloc_cross_, sp4_.get(), sp2_.get(), pw, lmap_.get());
+      MADAM_LAUNCH(k_scatter_tiled<3>, kStreamBlocks, 256, kStreamSmem, st_, csr_off_.get(),
+                   scatter_tiles_.get(), nscatter_tiles_, sp4_.get(), sp2_.get(), pw, lmap_.get());
     else
-      MADAM_LAUNCH(k_scatter_csr<1>, kRedBlocks, 256, 0, st_, csr_off_.get(),
-                   (long long)nloc_cross_, sp4_.get(), sp2_.get(), pw, lmap_.get());
+      MADAM_LAUNCH(k_scatter_tiled<1>, kStreamBlocks, 256, kStreamSmem, st_, csr_off_.get(),
+                   scatter_tiles_.get(), nscatter_tiles_, sp4_.get(), sp2_.get(), pw, lmap_.get());
   }
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[1], st_));
   if (nloc_cross_ > 0) {
