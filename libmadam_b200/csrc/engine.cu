@@ -602,42 +602,6 @@ __device__ __forceinline__ double wm_sample(const float4 *__restrict__ p4,
   }
 }
 
-// Shared-memory staging of the streamed pointing: 16-byte (4-byte for pixel
-// numbers) cp.async copies with an L2 evict-first policy, so the stream does
-// not push the map and baseline vectors out of L2.
-__device__ __forceinline__ uint64_t evict_first_policy() {
-  uint64_t pol;
-  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(pol));
-  return pol;
-}
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, uint64_t pol) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;\n" ::"r"(s),
-               "l"(gmem), "l"(pol)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, uint64_t pol) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 8, %2;\n" ::"r"(s),
-               "l"(gmem), "l"(pol)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async4(void *smem, const void *gmem, uint64_t pol) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 4, %2;\n" ::"r"(s),
-               "l"(gmem), "l"(pol)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-constexpr int kStreamBlocks = 444;  // 148 SMs x 3 (64 KB of shared memory each)
-constexpr size_t kStreamSmem = 2 * kGatherTile * sizeof(float4);
 
 template <int NMAP>
 __global__ void __launch_bounds__(256) k_gather_tiled(
@@ -696,135 +660,81 @@ __global__ void __launch_bounds__(256) k_gather_tiled(
 
 // baseline_to_map (smadam_routines.f90:1074-1111) as a pixel-major gather:
 // the pointing is also stored sorted by cross pixel (time order inside a
-// pixel) as {w_I, w_Q, w_U, global baseline}.  Pixel tiles: pixels [pa, pb) whose pixel-sorted
-// entries fit kGatherTile (double-buffered in shared memory by cp.async), or
-// one pixel with more entries (read directly, all warps, rounds of the
-// block).  A warp sums each pixel of a tile with the pw loads of up to eight
-// entries per lane in flight.  No atomics, deterministic.
+// pixel) as {w_I, w_Q, w_U, global baseline}.  Each pixel's entries are cut
+// into fixed chunks of at most kScatterChunk; one warp sums a chunk with all
+// of its entry and pw loads in flight (8 per lane).  A pixel of one chunk is
+// written directly; the chunk sums of larger pixels go to `partial` and
+// k_scatter_combine adds them in chunk order.  No atomics, deterministic.
+constexpr int kScatterChunk = 256;
+
 template <int NMAP>
-__global__ void __launch_bounds__(256, 3) k_scatter_tiled(
-    const int *__restrict__ off, const int2 *__restrict__ tiles, int ntiles,
-    const float4 *__restrict__ sp4, const int2 *__restrict__ sp2, const double *__restrict__ pw,
-    double *__restrict__ target) {
-  extern __shared__ float4 gsm[];
-  __shared__ double red[3][8];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const uint64_t pol = evict_first_policy();
-  auto issue = [&](int t, int buf) {
-    const int2 tl = tiles[t];
-    const int e0 = off[tl.x], n = off[tl.y] - e0;
-    if (n > kGatherTile) return;
+__global__ void __launch_bounds__(256) k_scatter_chunks(
+    const int4 *__restrict__ chunks, long long nchunks, const float4 *__restrict__ sp4,
+    const int2 *__restrict__ sp2, const double *__restrict__ pw, double *__restrict__ target,
+    double *__restrict__ partial) {
+  const int lane = threadIdx.x & 31;
+  const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  constexpr int U = kScatterChunk / 32;
+  for (long long c = w0; c < nchunks; c += nwarps) {
+    const int4 ck = chunks[c];  // {pixel, first entry, entries, partial slot or -1}
+    double a0 = 0, a1 = 0, a2 = 0;
     if (NMAP == 3) {
-      for (int u = threadIdx.x; u < n; u += blockDim.x)
-        cp_async16(gsm + buf * kGatherTile + u, sp4 + e0 + u, pol);
-    } else {
-      int2 *dst = (int2 *)(gsm + buf * kGatherTile);
-      for (int u = threadIdx.x; u < n; u += blockDim.x) cp_async8(dst + u, sp2 + e0 + u, pol);
-    }
-  };
-  int buf = 0;
-  if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
-  cp_async_commit();
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, buf ^= 1) {
-    if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x, buf ^ 1);
-    cp_async_commit();
-    cp_async_wait<1>();
-    __syncthreads();
-    const int2 tl = tiles[t];
-    const int e0 = off[tl.x], n = off[tl.y] - e0;
-    if (n > kGatherTile) {
-      // one pixel: all warps, direct loads
-      const int p = tl.x;
-      double a0 = 0, a1 = 0, a2 = 0;
-      for (int i0 = e0 + threadIdx.x; i0 < e0 + n; i0 += 8 * blockDim.x) {
-        double wv[8];
-        float4 q[8];
+      float4 q[U];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          const int i = i0 + r * blockDim.x;
-          if (NMAP == 3) {
-            q[r] = i < e0 + n ? __ldcs(sp4 + i) : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
-            const int k = __float_as_int(q[r].w);
-            wv[r] = k >= 0 ? pw[k] : 0.0;
-          } else {
-            const int k = i < e0 + n ? __ldcs(&sp2[i].x) : -1;
-            wv[r] = k >= 0 ? pw[k] : 0.0;
-          }
-        }
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-          if (NMAP == 3) {
-            a0 += (double)q[r].x * wv[r];
-            a1 += (double)q[r].y * wv[r];
-            a2 += (double)q[r].z * wv[r];
-          } else {
-            a0 += wv[r];
-          }
-        }
+      for (int r = 0; r < U; ++r) {
+        const int i = r * 32 + lane;
+        q[r] = i < ck.z ? __ldcs(sp4 + ck.y + i) : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
       }
-      a0 = warp_sum(a0);
+      double wv[U];
+#pragma unroll
+      for (int r = 0; r < U; ++r) {
+        const int k = __float_as_int(q[r].w);
+        wv[r] = k >= 0 ? pw[k] : 0.0;
+      }
+#pragma unroll
+      for (int r = 0; r < U; ++r) {
+        a0 += (double)q[r].x * wv[r];
+        a1 += (double)q[r].y * wv[r];
+        a2 += (double)q[r].z * wv[r];
+      }
+    } else {
+      int k[U];
+#pragma unroll
+      for (int r = 0; r < U; ++r) {
+        const int i = r * 32 + lane;
+        k[r] = i < ck.z ? __ldcs(&sp2[ck.y + i].x) : -1;
+      }
+#pragma unroll
+      for (int r = 0; r < U; ++r) a0 += k[r] >= 0 ? pw[k[r]] : 0.0;
+    }
+    a0 = warp_sum(a0);
+    if (NMAP == 3) {
       a1 = warp_sum(a1);
       a2 = warp_sum(a2);
-      if (lane == 0) {
-        red[0][wid] = a0;
-        red[1][wid] = a1;
-        red[2][wid] = a2;
-      }
-      __syncthreads();
-      if (threadIdx.x < NMAP) {
-        double s = 0;
-        for (int w = 0; w < nw; ++w) s += red[threadIdx.x][w];
-        target[(long long)p * NMAP + threadIdx.x] = s;
-      }
-    } else {
-      const float4 *q4 = gsm + buf * kGatherTile;
-      const int2 *q2 = (const int2 *)(gsm + buf * kGatherTile);
-      for (int p = tl.x + wid; p < tl.y; p += nw) {
-        const int a = off[p] - e0, e = off[p + 1] - e0;
-        double a0 = 0, a1 = 0, a2 = 0;
-        for (int i0 = a + lane; i0 < e; i0 += 32 * 8) {
-          double wv[8];
-#pragma unroll
-          for (int r = 0; r < 8; ++r) {
-            const int i = i0 + 32 * r;
-            int k = -1;
-            if (i < e) k = NMAP == 3 ? __float_as_int(q4[i].w) : q2[i].x;
-            wv[r] = k >= 0 ? pw[k] : 0.0;
-          }
-#pragma unroll
-          for (int r = 0; r < 8; ++r) {
-            const int i = i0 + 32 * r;
-            if (i < e) {
-              if (NMAP == 3) {
-                const float4 q = q4[i];
-                a0 += (double)q.x * wv[r];
-                a1 += (double)q.y * wv[r];
-                a2 += (double)q.z * wv[r];
-              } else {
-                a0 += wv[r];
-              }
-            }
-          }
-        }
-        a0 = warp_sum(a0);
-        if (NMAP == 3) {
-          a1 = warp_sum(a1);
-          a2 = warp_sum(a2);
-        }
-        if (lane == 0) {
-          if (NMAP == 3) {
-            target[(long long)p * 3] = a0;
-            target[(long long)p * 3 + 1] = a1;
-            target[(long long)p * 3 + 2] = a2;
-          } else {
-            target[p] = a0;
-          }
-        }
+    }
+    if (lane == 0) {
+      double *o = ck.w < 0 ? target + (long long)ck.x * NMAP : partial + (long long)ck.w * NMAP;
+      o[0] = a0;
+      if (NMAP == 3) {
+        o[1] = a1;
+        o[2] = a2;
       }
     }
-    __syncthreads();
   }
-  cp_async_wait<0>();
+}
+
+// multi-chunk pixels: {pixel, first partial slot, chunks}
+template <int NMAP>
+__global__ void k_scatter_combine(const int4 *__restrict__ multi, int nmulti,
+                                  const double *__restrict__ partial, double *__restrict__ target) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nmulti; i += gridDim.x * blockDim.x) {
+    const int4 mp = multi[i];
+    double a[3] = {0, 0, 0};
+    for (int c = 0; c < mp.z; ++c)
+      for (int j = 0; j < NMAP; ++j) a[j] += partial[(long long)(mp.y + c) * NMAP + j];
+    for (int j = 0; j < NMAP; ++j) target[(long long)mp.x * NMAP + j] = a[j];
+  }
 }
 
 // CSR construction: sort key (cross pixel, or nloc_cross for samples the

@@ -204,8 +204,11 @@ class Engine {
   DevBuf<float4> sp4_;        // pixel-sorted pointing {w, baseline}
   DevBuf<int2> sp2_;          // pixel-sorted baseline (temperature only)
   DevBuf<int> csr_off_;       // nloc_cross + 1 offsets
-  DevBuf<int2> scatter_tiles_;  // pixel tiles {first, end} of the scatter
-  int nscatter_tiles_ = 0;
+  DevBuf<int4> scatter_chunks_;  // {pixel, first entry, entries, partial slot}
+  DevBuf<int4> scatter_multi_;   // {pixel, first slot, chunks} of multi-chunk pixels
+  DevBuf<double> scatter_partial_;
+  long long nscatter_chunks_ = 0;
+  int nscatter_multi_ = 0;
   long long csr_nvalid_ = 0;
   DevBuf<long long> istart_d_;
   DevBuf<int> kstart_d_;

@@ -522,7 +522,8 @@ void Engine::build_csr() {
   // pixel-sorted copy of the pointing for the PCG scatter (k_scatter_csr)
   const long long n = (long long)ndet_ * nsamp_;
   csr_nvalid_ = 0;
-  nscatter_tiles_ = 0;
+  nscatter_chunks_ = 0;
+  nscatter_multi_ = 0;
   csr_off_.alloc((size_t)nloc_cross_ + 1);
   if (n == 0 || nloc_cross_ == 0) {
     csr_off_.zero(st_);
@@ -579,29 +580,36 @@ void Engine::build_csr() {
                    csr_nvalid_, point4_.get(), sm, (float4 *)nullptr, sp2_.get(), csr_off_.get());
   }
   MADAM_CUDA(cudaStreamSynchronize(st_));
-  // pixel tiles of the scatter: consecutive pixels with at most kGatherTile
-  // entries, or one pixel with more
+  // scatter chunks: every pixel's entries cut into chunks of at most
+  // kScatterChunk; pixels of several chunks combine their partial sums
   {
     std::vector<int> offh((size_t)nloc_cross_ + 1);
     MADAM_CUDA(cudaMemcpy(offh.data(), csr_off_.get(), offh.size() * sizeof(int),
                           cudaMemcpyDeviceToHost));
-    std::vector<int2> tl;
-    int pa = 0;
-    while (pa < (int)nloc_cross_) {
-      if (offh[pa + 1] - offh[pa] > kGatherTile) {
-        tl.push_back(make_int2(pa, pa + 1));
-        ++pa;
+    std::vector<int4> ck, multi;
+    int slot = 0;
+    for (int p = 0; p < (int)nloc_cross_; ++p) {
+      const int e0 = offh[p], n = offh[p + 1] - offh[p];
+      const int nc = std::max(1, (n + kScatterChunk - 1) / kScatterChunk);
+      if (nc == 1) {
+        ck.push_back(make_int4(p, e0, n, -1));
         continue;
       }
-      int pb = pa + 1;
-      while (pb < (int)nloc_cross_ && offh[pb + 1] - offh[pa] <= kGatherTile) ++pb;
-      tl.push_back(make_int2(pa, pb));
-      pa = pb;
+      multi.push_back(make_int4(p, slot, nc, 0));
+      for (int c = 0; c < nc; ++c)
+        ck.push_back(make_int4(p, e0 + c * kScatterChunk, std::min(kScatterChunk, n - c * kScatterChunk),
+                               slot++));
     }
-    nscatter_tiles_ = (int)tl.size();
-    scatter_tiles_.alloc(std::max<size_t>(1, tl.size()));
-    if (!tl.empty())
-      MADAM_CUDA(cudaMemcpyAsync(scatter_tiles_.get(), tl.data(), tl.size() * sizeof(int2),
+    nscatter_chunks_ = (long long)ck.size();
+    nscatter_multi_ = (int)multi.size();
+    scatter_chunks_.alloc(std::max<size_t>(1, ck.size()));
+    scatter_multi_.alloc(std::max<size_t>(1, multi.size()));
+    scatter_partial_.alloc((size_t)std::max(1, slot) * nmap_);
+    if (!ck.empty())
+      MADAM_CUDA(cudaMemcpyAsync(scatter_chunks_.get(), ck.data(), ck.size() * sizeof(int4),
+                                 cudaMemcpyHostToDevice, st_));
+    if (!multi.empty())
+      MADAM_CUDA(cudaMemcpyAsync(scatter_multi_.get(), multi.data(), multi.size() * sizeof(int4),
                                  cudaMemcpyHostToDevice, st_));
   }
   MADAM_CUDA(cudaStreamSynchronize(st_));
@@ -1359,20 +1367,22 @@ void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) 
   const long long nb = (long long)ndet_ * noba_short_;
   // 1) baseline -> map, collect, ccmultiply, scatter back (iterate_a 798-827)
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[0], st_));
-  static bool stream_attr = false;
-  if (!stream_attr) {
-    for (const void *f : {(const void *)k_scatter_tiled<3>, (const void *)k_scatter_tiled<1>})
-      MADAM_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kStreamSmem));
-    stream_attr = true;
-  }
-  if (nloc_cross_ > 0 && nscatter_tiles_ > 0) {
-    if (nmap_ == 3)
-      MADAM_LAUNCH(k_scatter_tiled<3>, kStreamBlocks, 256, kStreamSmem, st_, csr_off_.get(),
-                   scatter_tiles_.get(), nscatter_tiles_, sp4_.get(), sp2_.get(), pw, lmap_.get());
-    else
-      MADAM_LAUNCH(k_scatter_tiled<1>, kStreamBlocks, 256, kStreamSmem, st_, csr_off_.get(),
-                   scatter_tiles_.get(), nscatter_tiles_, sp4_.get(), sp2_.get(), pw, lmap_.get());
+  if (nloc_cross_ > 0 && nscatter_chunks_ > 0) {
+    if (nmap_ == 3) {
+      MADAM_LAUNCH(k_scatter_chunks<3>, kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
+                   nscatter_chunks_, sp4_.get(), sp2_.get(), pw, lmap_.get(),
+                   scatter_partial_.get());
+      if (nscatter_multi_ > 0)
+        MADAM_LAUNCH(k_scatter_combine<3>, grid_for(nscatter_multi_), 256, 0, st_,
+                     scatter_multi_.get(), nscatter_multi_, scatter_partial_.get(), lmap_.get());
+    } else {
+      MADAM_LAUNCH(k_scatter_chunks<1>, kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
+                   nscatter_chunks_, sp4_.get(), sp2_.get(), pw, lmap_.get(),
+                   scatter_partial_.get());
+      if (nscatter_multi_ > 0)
+        MADAM_LAUNCH(k_scatter_combine<1>, grid_for(nscatter_multi_), 256, 0, st_,
+                     scatter_multi_.get(), nscatter_multi_, scatter_partial_.get(), lmap_.get());
+    }
   }
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[1], st_));
   if (nloc_cross_ > 0) {
