@@ -658,6 +658,98 @@ __global__ void __launch_bounds__(256) k_gather_tiled(
   if (threadIdx.x == 0) part[blockIdx.x] = v[0];
 }
 
+// map_to_baseline, warp chunks: a warp takes a chunk of consecutive
+// baselines of one detector (at most kGatherChunk samples, at most 32
+// baselines), loads all of its samples (8 per lane, coalesced) with their map
+// values in flight together, stages w.m in the warp's shared-memory slice and
+// lets lane j sum baseline j in time order; fused with the p.ap partial sums.
+// No block barriers: warps run independently.  Used when every baseline is
+// at most kGatherChunk samples long.
+constexpr int kGatherChunk = 256;
+
+template <int NMAP>
+__global__ void __launch_bounds__(256) k_gather_chunks(
+    const int2 *__restrict__ chunks, long long nchunks, const float4 *__restrict__ p4,
+    const int32_t *__restrict__ pc, const uint32_t *__restrict__ bstart, long noba,
+    long long nsamp, const double *__restrict__ bw, const double *__restrict__ p,
+    const double *__restrict__ nna, const double *__restrict__ m, int deg_shift, int nloc,
+    const uint8_t *__restrict__ rmask, double *__restrict__ ap, double *__restrict__ part) {
+  __shared__ double vbuf[8][kGatherChunk];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double *vb = vbuf[wid];
+  const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  constexpr int U = kGatherChunk / 32;
+  double pap = 0;
+  for (long long c = w0; c < nchunks; c += nwarps) {
+    const int2 ck = chunks[c];  // {first global baseline, baselines}
+    const long long det = ck.x / noba, k0 = ck.x - det * noba;
+    const int s0 = (int)bstart[k0];
+    const int n = (int)(bstart[k0 + ck.y] - s0);
+    const long long base = det * nsamp + s0;
+    // lane j < ck.y: scalars of baseline j, in flight with the samples
+    double detw = 0, pb = 0, apb = 0, npb = 0;
+    int a0 = 0, a1 = 0;
+    bool rm = false;
+    if (lane < ck.y) {
+      const long long b = ck.x + lane;
+      detw = bw[b];
+      pb = p[b];
+      apb = ap[b];
+      npb = nna[b] * pb;
+      rm = rmask[b] != 0;
+      a0 = (int)(bstart[k0 + lane] - s0);
+      a1 = (int)(bstart[k0 + lane + 1] - s0);
+    }
+    double v[U];
+    if (NMAP == 3) {
+      float4 q[U];
+#pragma unroll
+      for (int r = 0; r < U; ++r) {
+        const int i = r * 32 + lane;
+        q[r] = i < n ? __ldcs(p4 + base + i) : make_float4(0.f, 0.f, 0.f, __int_as_float(nloc));
+      }
+#pragma unroll
+      for (int r = 0; r < U; ++r) {
+        const int px = point_pix(q[r]);
+        v[r] = 0.0;
+        if (px < nloc) {
+          const double *mm = m + (long long)(px >> deg_shift) * 3;
+          v[r] = (double)q[r].x * mm[0] + (double)q[r].y * mm[1] + (double)q[r].z * mm[2];
+        }
+      }
+    } else {
+      int px[U];
+#pragma unroll
+      for (int r = 0; r < U; ++r) {
+        const int i = r * 32 + lane;
+        px[r] = i < n ? __ldcs(pc + base + i) : nloc;
+      }
+#pragma unroll
+      for (int r = 0; r < U; ++r) v[r] = px[r] < nloc ? m[px[r] >> deg_shift] : 0.0;
+    }
+#pragma unroll
+    for (int r = 0; r < U; ++r) vb[r * 32 + lane] = v[r];
+    __syncwarp();
+    if (lane < ck.y) {
+      const long long b = ck.x + lane;
+      if (detw == 0) {
+        if (rm) pap += pb * apb;
+      } else {
+        double apn = 0;
+        for (int i = a0; i < a1; ++i) apn += vb[i];
+        const double val = apb + (npb - apn * detw);
+        ap[b] = val;
+        if (rm) pap += pb * val;
+      }
+    }
+    __syncwarp();
+  }
+  double pv[1] = {pap};
+  block_sum<1>(pv);
+  if (threadIdx.x == 0) part[blockIdx.x] = pv[0];
+}
+
 // baseline_to_map (smadam_routines.f90:1074-1111) as a pixel-major gather:
 // the pointing is also stored sorted by cross pixel (time order inside a
 // pixel) as {w_I, w_Q, w_U, global baseline}.  Each pixel's entries are cut

@@ -164,6 +164,8 @@ class Engine {
   double dnshort_ = 0;
   FastDiv fdn_;
   int gather_kb_ = 0;
+  DevBuf<int2> gather_chunks_;  // {first global baseline, baselines} per warp chunk
+  long long ngather_chunks_ = 0;
   long long gather_tiles_det_ = 0;
   std::vector<long> intervals_, istart_iv_, noba_pp_, kstart_pp_;
   std::vector<uint32_t> bstart_;  // noba_short + 1

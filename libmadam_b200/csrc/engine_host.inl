@@ -250,6 +250,33 @@ void Engine::init_layout(long nperiod, const long *periods) {
       gather_tiles_det_ = (noba_short_ + gather_kb_ - 1) / gather_kb_;
     }
   }
+  // gather chunks: runs of consecutive baselines of one detector with at most
+  // kGatherChunk samples and 32 baselines (every baseline must fit one)
+  {
+    long maxlen = 0;
+    for (long k = 0; k < noba_short_; ++k)
+      maxlen = std::max<long>(maxlen, bstart_[k + 1] - bstart_[k]);
+    std::vector<int2> ck;
+    if (maxlen <= kGatherChunk && (long long)ndet_ * noba_short_ < (1LL << 31)) {
+      std::vector<int2> one;  // chunks of detector 0, repeated per detector
+      long k = 0;
+      while (k < noba_short_) {
+        long k1 = k + 1;
+        while (k1 < noba_short_ && k1 - k < 32 && bstart_[k1 + 1] - bstart_[k] <= kGatherChunk)
+          ++k1;
+        one.push_back(make_int2((int)k, (int)(k1 - k)));
+        k = k1;
+      }
+      ck.reserve(one.size() * ndet_);
+      for (long d = 0; d < ndet_; ++d)
+        for (const int2 &c : one) ck.push_back(make_int2((int)(d * noba_short_ + c.x), c.y));
+    }
+    ngather_chunks_ = (long long)ck.size();
+    gather_chunks_.alloc(std::max<size_t>(1, ck.size()));
+    if (!ck.empty())
+      MADAM_CUDA(cudaMemcpyAsync(gather_chunks_.get(), ck.data(), ck.size() * sizeof(int2),
+                                 cudaMemcpyHostToDevice, st_));
+  }
   // every baseline but the last of a period has length dnshort
   const double dnc = std::min(dnshort_, 4294967295.0);
   fdn_ = FastDiv((uint32_t)std::max(1.0, dnc));
@@ -1406,7 +1433,18 @@ void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) 
   }
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[3], st_));
   // 3) map -> baseline and p.ap (849-878)
-  if (gather_kb_ > 0) {
+  if (ngather_chunks_ > 0) {
+    if (nmap_ == 3)
+      MADAM_LAUNCH(k_gather_chunks<3>, kRedBlocks, 256, 0, st_, gather_chunks_.get(),
+                   ngather_chunks_, point4_.get(), pixc_.get(), bstart_d_.get(), noba_short_,
+                   nsamp_, bw_.get(), p, nna_.get(), lmap_.get(), (int)ndeg_shift_, (int)nloc_,
+                   rmask_.get(), ap, part_.get());
+    else
+      MADAM_LAUNCH(k_gather_chunks<1>, kRedBlocks, 256, 0, st_, gather_chunks_.get(),
+                   ngather_chunks_, point4_.get(), pixc_.get(), bstart_d_.get(), noba_short_,
+                   nsamp_, bw_.get(), p, nna_.get(), lmap_.get(), (int)ndeg_shift_, (int)nloc_,
+                   rmask_.get(), ap, part_.get());
+  } else if (gather_kb_ > 0) {
     if (nmap_ == 3)
       MADAM_LAUNCH(k_gather_tiled<3>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
                    bstart_d_.get(), noba_short_, nsamp_, gather_kb_, gather_tiles_det_,
