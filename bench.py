@@ -34,6 +34,18 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 
+def profiled_traffic(kernel, nsamp):
+    """DRAM bytes of one launch of `kernel` at `nsamp` samples, from the committed ncu
+    summary (bytes per sample of a smaller capture; traffic grows with the samples)."""
+    import re
+    try:
+        with open(os.path.join(ROOT, "profiles", kernel + "_mid.md")) as f:
+            m = re.search(r"dram_bytes_per_sample = ([0-9.]+) B", f.read())
+        return float(m.group(1)) * nsamp if m else None
+    except OSError:
+        return None
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -286,10 +298,16 @@ def main():
             "filter": None, "precond": None}
     dom = max(("scatter", "gather"), key=lambda k: phases[k])
     achieved = algo[dom] / (phases[dom] * 1e-3) / 1e9
-    b_iter = 32.0 * n + 8.0 * (16 + 20) * nb + (4 * 3 * 8 + 48) * npix_hit
-    roofline = {"bound": "hbm", "kernel": "k_" + dom, "achieved": achieved, "peak": hbm,
+    kname = {"scatter": "k_scatter_chunks", "gather": "k_gather_chunks"}[dom]
+    traffic = profiled_traffic(kname, n)
+    try:
+        w_p = float(np.mean(W.get_result("band_widths")))
+    except Exception:
+        w_p = 0.0
+    b_iter = 32.0 * n + 8.0 * (16 + w_p) * nb + (4 * 3 * 8 + 48) * npix_hit
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
                 "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
-                "traffic": None,
+                "algorithmic_bytes": algo[dom], "traffic": traffic,
                 "iteration": {"algorithmic_bytes": b_iter,
                               "achieved_gbs": b_iter / (ms_iter * 1e-3) / 1e9,
                               "frac": b_iter / (ms_iter * 1e-3) / 1e9 / hbm}}
