@@ -281,10 +281,14 @@ def main():
         t_e2e = time.perf_counter() - t1
         t_e2e = reduce_max(t_e2e, world)
         it_e2e = int(W.scalars()["noiter"])
+        te = W.timings()
         h2d = sum(v.numel() * v.element_size() for v in h.values())
         e2e = {"value": world * n * it_e2e / t_e2e, "unit": "samples/s per PCG iteration",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(m.nbytes),
-               "seconds": t_e2e, "iterations": it_e2e}
+               "seconds": t_e2e, "iterations": it_e2e,
+               "library_ms": {k: te[k] for k in ("setup_ms", "iterate_ms", "finalize_ms",
+                                                  "total_ms")},
+               "setup_marks_ms": W.setup_marks()}
         del h, hn
 
     # roofline of the dominant kernel (algorithmic bytes per launch / duration)

@@ -457,8 +457,9 @@ __global__ void k_band2_scan(const PSeg *segs, int nseg, const PChunk *ch, const
 // only when the matrix changes) and gathers the state by shuffles; the next
 // chunk's particular state and matrix offset are loaded one step ahead.
 template <int W>
-__global__ void k_band2_scan_reg(const PSeg *segs, int s0, int s1, const PChunk *ch,
+__global__ void k_band2_scan_reg(const PSeg *segs, int s0, int s1, const int *toff,
                                  const double *T, const double *p, double *s, int dir) {
+  constexpr int D = 8;  // chunks whose particular state and matrix offset are in flight
   const int seg = s0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (seg >= s1) return;
@@ -468,39 +469,53 @@ __global__ void k_band2_scan_reg(const PSeg *segs, int s0, int s1, const PChunk 
   const bool on = lane < w;
   const int c0 = g.ch_off, cl = g.ch_off + g.nch - 1;
   const int start = dir == 0 ? c0 : cl;
-  const int stop = dir == 0 ? cl : c0;  // exclusive
   const int step = dir == 0 ? 1 : -1;
-  double cur = on ? p[(long long)start * kBand2State + lane] : 0.0;
-  if (on) s[(long long)start * kBand2State + lane] = cur;
+  const int nsteps = g.nch - 2;  // chunks after start whose state is needed
+  const double *pp = p + (long long)start * kBand2State + lane;
+  double *sp = s + (long long)start * kBand2State + lane;
+  const long long stride = (long long)step * kBand2State;
+  const int *tp = toff + start;
+  double cur = on ? pp[0] : 0.0;
+  if (on) sp[0] = cur;
   double Tr[W];
   int tcur = -1;
-  int c = start + step;
-  if (c == stop) return;
-  double pn = on ? p[(long long)c * kBand2State + lane] : 0.0;
-  int tn = dir == 0 ? ch[c].tf : ch[c].tb;
-  for (; c != stop; c += step) {
-    const double pc = pn;
-    const int tc = tn;
-    const int cn = c + step;
-    if (cn != stop) {
-      pn = on ? p[(long long)cn * kBand2State + lane] : 0.0;
-      tn = dir == 0 ? ch[cn].tf : ch[cn].tb;
-    }
-    if (tc != tcur) {
+  double pq[D];
+  int tq[D];
 #pragma unroll
-      for (int qq = 0; qq < W; ++qq) Tr[qq] = (on && qq < w) ? T[tc + (long long)lane * w + qq] : 0.0;
-      tcur = tc;
-    }
-    double a0 = pc, a1 = 0, a2 = 0, a3 = 0;
+  for (int r = 0; r < D; ++r) {
+    pq[r] = (on && r < nsteps) ? pp[(r + 1) * stride] : 0.0;
+    tq[r] = r < nsteps ? tp[(r + 1) * step] : 0;
+  }
+  for (int u0 = 0; u0 < nsteps; u0 += D) {
 #pragma unroll
-    for (int qq = 0; qq < W; qq += 4) {
-      a0 += Tr[qq] * __shfl_sync(0xffffffffu, cur, qq);
-      if (qq + 1 < W) a1 += Tr[qq + 1] * __shfl_sync(0xffffffffu, cur, qq + 1);
-      if (qq + 2 < W) a2 += Tr[qq + 2] * __shfl_sync(0xffffffffu, cur, qq + 2);
-      if (qq + 3 < W) a3 += Tr[qq + 3] * __shfl_sync(0xffffffffu, cur, qq + 3);
+    for (int r = 0; r < D; ++r) {
+      const int u = u0 + r;
+      if (u < nsteps) {
+        const double pc = pq[r];
+        const int tc = tq[r];
+        const int un = u + D;
+        if (un < nsteps) {
+          pq[r] = on ? pp[(long long)(un + 1) * stride] : 0.0;
+          tq[r] = tp[(un + 1) * step];
+        }
+        if (tc != tcur) {
+#pragma unroll
+          for (int qq = 0; qq < W; ++qq)
+            Tr[qq] = (on && qq < w) ? T[tc + (long long)lane * w + qq] : 0.0;
+          tcur = tc;
+        }
+        double a0 = pc, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+        for (int qq = 0; qq < W; qq += 4) {
+          a0 += Tr[qq] * __shfl_sync(0xffffffffu, cur, qq);
+          if (qq + 1 < W) a1 += Tr[qq + 1] * __shfl_sync(0xffffffffu, cur, qq + 1);
+          if (qq + 2 < W) a2 += Tr[qq + 2] * __shfl_sync(0xffffffffu, cur, qq + 2);
+          if (qq + 3 < W) a3 += Tr[qq + 3] * __shfl_sync(0xffffffffu, cur, qq + 3);
+        }
+        cur = on ? (a0 + a1) + (a2 + a3) : 0.0;
+        if (on) sp[(long long)(u + 1) * stride] = cur;
+      }
     }
-    cur = on ? (a0 + a1) + (a2 + a3) : 0.0;
-    if (on) s[(long long)c * kBand2State + lane] = cur;
   }
 }
 
@@ -598,9 +613,10 @@ void band2_transfer(cudaStream_t st, const PSeg *segs, const PChunk *ch, const P
 }
 
 void band2_solve(cudaStream_t st, const PSeg *segs, int nseg, const PChunk *ch, int nch,
-                 const int *cls_w, const int *cls_begin, const int *cls_seg, int ncls,
-                 const PRun *runs, const PRun *cruns, const double *tab, const double *T,
-                 const double *r, double *z, double *work_p, double *work_s) {
+                 const int *toff_f, const int *toff_b, const int *cls_w, const int *cls_begin,
+                 const int *cls_seg, int ncls, const PRun *runs, const PRun *cruns,
+                 const double *tab, const double *T, const double *r, double *z, double *work_p,
+                 double *work_s) {
   if (nch == 0) return;
   auto passes = [&](int mode) {
     for (int i = 0; i < ncls; ++i)
@@ -616,8 +632,8 @@ void band2_solve(cudaStream_t st, const PSeg *segs, int nseg, const PChunk *ch, 
       switch (cls_w[i]) {
 #define MADAM_BAND2_CASE(X)                                                                   \
   case X:                                                                                     \
-    MADAM_LAUNCH(k_band2_scan_reg<X>, grid, 64, 0, st, segs, s0, s1, ch, T, work_p, work_s,    \
-                 dir);                                                                        \
+    MADAM_LAUNCH(k_band2_scan_reg<X>, grid, 64, 0, st, segs, s0, s1, dir == 0 ? toff_f : toff_b, \
+                 T, work_p, work_s, dir);                                                     \
     break;
         MADAM_BAND2_CASE(1)
         MADAM_BAND2_CASE(2)

@@ -60,10 +60,12 @@ void band2_transfer(cudaStream_t st, const PSeg *segs, const PChunk *ch, const P
 // Solve L L^T z = r on every factored segment.  Width class i: chunks
 // [cls_begin[i], cls_begin[i + 1]) of segments [cls_seg[i], cls_seg[i + 1])
 // with w <= cls_w[i] (host arrays).
+// toff_f / toff_b: the chunks' forward / backward transfer offsets (device).
 void band2_solve(cudaStream_t st, const PSeg *segs, int nseg, const PChunk *ch, int nch,
-                 const int *cls_w, const int *cls_begin, const int *cls_seg, int ncls,
-                 const PRun *runs, const PRun *cruns, const double *tab, const double *T,
-                 const double *r, double *z, double *work_p, double *work_s);
+                 const int *toff_f, const int *toff_b, const int *cls_w, const int *cls_begin,
+                 const int *cls_seg, int ncls, const PRun *runs, const PRun *cruns,
+                 const double *tab, const double *T, const double *r, double *z, double *work_p,
+                 double *work_s);
 // Smallest compiled register width >= w (0 when w needs the generic path).
 int band2_class_width(int w);
 

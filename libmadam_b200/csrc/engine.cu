@@ -872,6 +872,13 @@ __global__ void k_csr_fill(const int *keys, const uint32_t *idx, long long nvali
   }
 }
 
+// dst[i] = src[idx[i]]
+__global__ void k_take(const double *src, const uint32_t *idx, long long n, double *dst) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i] = src[idx[i]];
+}
+
 __global__ void k_fill_int(int *a, long long n, int v) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <future>
 #include <map>
 #include <memory>
 #include <string>
@@ -24,6 +25,14 @@ constexpr int kRedBlocks = 1184;      // 148 SMs x 8, fixed for determinism
 
 
 // Owning device allocation.
+// Device memory of the engine: stream-ordered allocations on the engine's
+// stream, served by the device's default memory pool, which keeps freed
+// blocks for reuse (one destripe call allocates and frees several GB of
+// temporaries; the pool turns the repeats into bookkeeping).
+extern cudaStream_t g_alloc_stream;
+void *dev_alloc(size_t bytes);
+void dev_free(void *p);
+
 template <typename T>
 struct DevBuf {
   T *p = nullptr;
@@ -33,7 +42,7 @@ struct DevBuf {
   DevBuf &operator=(const DevBuf &) = delete;
   ~DevBuf() { reset(); }
   void reset() {
-    if (p) cudaFree(p);
+    if (p) dev_free(p);
     p = nullptr;
     n = 0;
   }
@@ -41,7 +50,7 @@ struct DevBuf {
     if (count == n && p) return;
     reset();
     if (count == 0) return;
-    MADAM_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    p = (T *)dev_alloc(count * sizeof(T));
     n = count;
   }
   void zero(cudaStream_t s) {
@@ -112,7 +121,8 @@ class Engine {
   void bench_iterations(int warmup, int iters, std::vector<double> &out);
 
   Timings timings;
-  double setup_marks_[9] = {0};
+  static constexpr int kSetupMarks = 10;
+  double setup_marks_[kSetupMarks] = {0};
   long noiter = 0;
   double rrinit = 0, rr_final = 0;
   std::vector<double> rr_history;
@@ -131,6 +141,8 @@ class Engine {
   void initialize_a();
   void build_segments();
   void build_filter();
+  void filter_spectra(const std::vector<std::pair<long, int>> &tasks, long nh);
+  void build_filter_finish();
   void construct_preconditioner();
   void iterate();
   void finalize(bool first_call);
@@ -248,6 +260,7 @@ class Engine {
   DevBuf<PSeg> p2segs_;
   DevBuf<PRun> p2runs_, p2cruns_;
   DevBuf<PChunk> p2ch_;
+  DevBuf<int> p2tf_, p2tb_;  // per-chunk transfer offsets, forward / backward
   DevBuf<double> p2rows_, p2T_, p2wp_, p2ws_;
   int p2nseg_ = 0, p2nch_ = 0;
   long long band2_rows_ = 0;
@@ -256,6 +269,8 @@ class Engine {
   std::vector<int> band2_cls_w_, band2_cls_begin_, band2_cls_seg_;
   long n_band_fail_ = 0;
   std::unique_ptr<FFTPlan> fft_;
+  std::future<void> filter_job_;  // host spectra of build_filter
+  std::string filter_err_;
   std::unique_ptr<CgpWork> cgp_;
 
   // pixels flagged during the call (host write-back)

@@ -11,15 +11,39 @@ struct CgpWork {
   long nseg = 0;
 };
 
+cudaStream_t g_alloc_stream = nullptr;
+
+void *dev_alloc(size_t bytes) {
+  void *p = nullptr;
+  MADAM_CUDA(cudaMallocAsync(&p, bytes, g_alloc_stream));
+  return p;
+}
+
+void dev_free(void *p) { cudaFreeAsync(p, g_alloc_stream); }
+
 Engine::Engine() {
   MADAM_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+  {
+    int dev = 0;
+    MADAM_CUDA(cudaGetDevice(&dev));
+    cudaMemPool_t pool;
+    MADAM_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t keep = UINT64_MAX;
+    MADAM_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  }
+  g_alloc_stream = st_;
   for (auto &e : ev_) MADAM_CUDA(cudaEventCreate(&e));
 }
 
 Engine::~Engine() {
+  // members free their memory after this body: order those frees on the
+  // legacy stream once the engine's streams are idle
+  cudaStreamSynchronize(st_);
+  g_alloc_stream = nullptr;
   for (auto &e : ev_) cudaEventDestroy(e);
   if (st_) cudaStreamDestroy(st_);
 }
+
 
 static SampleMap sample_map(const long long *istart, const int *kstart, int niv,
                             long long nsamp, long noba, FastDiv fdn) {
@@ -851,7 +875,11 @@ void Engine::build_segments() {
 }
 
 void Engine::build_filter() {
-  // init_filter (noise_routines.f90:242-292) + build_filter (367-739)
+  // init_filter (noise_routines.f90:242-292) + build_filter (367-739).  The
+  // spectra are computed on the host (OpenMP over the PSDs) by a background
+  // job that overlaps the device-side setup; build_filter_finish() waits for
+  // it and uploads the result.
+  filter_err_.clear();
   if (!par_.kfilter) return;
   long nof_min = 2 * noba_pp_max_;
   if (par_.precond_width_max > nof_min - 1) nof_min = par_.precond_width_max + 1;
@@ -870,6 +898,17 @@ void Engine::build_filter() {
     if (!dets_[d].has_psd) fail("All detectors must have at least one PSD to build the filter");
     for (int ip = 0; ip < dets_[d].npsd; ++ip) tasks.push_back({d, ip});
   }
+  for (long it = 0; it < (long)tasks.size(); ++it) {
+    const long d = tasks[it].first;
+    const int ip = tasks[it].second;
+    psddet_[it] = (int)d;
+    psdstart_[it] = dets_[d].psdstarts[ip];
+    psdstop_[it] = (ip < dets_[d].npsd - 1) ? dets_[d].psdstarts[ip + 1] : fsp(1e30f);
+  }
+  filter_job_ = std::async(std::launch::async, [this, tasks, nh]() { filter_spectra(tasks, nh); });
+}
+
+void Engine::filter_spectra(const std::vector<std::pair<long, int>> &tasks, long nh) {
   const double fa = par_.fsample / (double)nshort_;
   const double kPi = 3.141592653589793238462643383279502884197;
   std::string err;
@@ -878,10 +917,7 @@ void Engine::build_filter() {
     try {
       const long d = tasks[it].first;
       const int ip = tasks[it].second;
-      Detector &det = dets_[d];
-      psddet_[it] = (int)d;
-      psdstart_[it] = det.psdstarts[ip];
-      psdstop_[it] = (ip < det.npsd - 1) ? det.psdstarts[ip + 1] : fsp(1e30f);
+      Detector &det = dets_[d];  // this task's entries only
       const double sigma = det.sigmas[ip];
       std::vector<double> aspec(nh, 0.0), f(nof_), g(nof_), spec(nof_);
       for (int k = 0; k <= 2; ++k) {
@@ -944,7 +980,13 @@ void Engine::build_filter() {
       err = e.what();
     }
   }
-  if (!err.empty()) fail(err);
+  filter_err_ = err;
+}
+
+void Engine::build_filter_finish() {
+  if (!par_.kfilter) return;
+  if (filter_job_.valid()) filter_job_.get();
+  if (!filter_err_.empty()) fail(filter_err_);
   fcov_.alloc(fcov_host_.size());
   MADAM_CUDA(cudaMemcpyAsync(fcov_.get(), fcov_host_.data(), fcov_host_.size() * sizeof(double),
                              cudaMemcpyHostToDevice, st_));
@@ -1315,6 +1357,17 @@ void Engine::construct_preconditioner() {
                                cudaMemcpyHostToDevice, st_));
     MADAM_CUDA(cudaMemcpyAsync(p2ch_.get(), chunks.data(), chunks.size() * sizeof(PChunk),
                                cudaMemcpyHostToDevice, st_));
+    std::vector<int> tf(chunks.size()), tb(chunks.size());
+    for (size_t c = 0; c < chunks.size(); ++c) {
+      tf[c] = chunks[c].tf;
+      tb[c] = chunks[c].tb;
+    }
+    p2tf_.alloc(tf.size());
+    p2tb_.alloc(tb.size());
+    MADAM_CUDA(cudaMemcpyAsync(p2tf_.get(), tf.data(), tf.size() * sizeof(int),
+                               cudaMemcpyHostToDevice, st_));
+    MADAM_CUDA(cudaMemcpyAsync(p2tb_.get(), tb.data(), tb.size() * sizeof(int),
+                               cudaMemcpyHostToDevice, st_));
     band2_columns(st_, p2segs_.get(), p2nseg_, max_ncrun, p2runs_.get(), p2cruns_.get(),
                   p2rows_.get());
     DevBuf<PTrans> dtr;
@@ -1535,7 +1588,8 @@ void Engine::apply_preconditioner(const double *r, double *z) {
       fft_->convolve(st_, filt_segs_d_.get(), (long)filt_segs_.size(), fprec_.get(), r, z);
     return;
   }
-  band2_solve(st_, p2segs_.get(), p2nseg_, p2ch_.get(), p2nch_, band2_cls_w_.data(),
+  band2_solve(st_, p2segs_.get(), p2nseg_, p2ch_.get(), p2nch_, p2tf_.get(), p2tb_.get(),
+              band2_cls_w_.data(),
               band2_cls_begin_.data(), band2_cls_seg_.data(), (int)band2_cls_w_.size(),
               p2runs_.get(), p2cruns_.get(), p2rows_.get(), p2T_.get(), r, z, p2wp_.get(),
               p2ws_.get());
@@ -1796,7 +1850,12 @@ void Engine::run(const Params &par, std::vector<Detector> dets, long ndet, long 
   cgp_.reset();
   d_pix_caller_ = is_device ? pix : nullptr;
   const long long n = (long long)ndet * nsamp;
+  auto mark = [&](int i) {
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    setup_marks_[i] = now_ms() - t0;
+  };
   bind_inputs(timestamps, pix, pixweights, signal, is_device, true);
+  mark(0);
   // pixel range check (smadam.F90:156-171)
   {
     DevBuf<int> mm;
@@ -1815,37 +1874,44 @@ void Engine::run(const Params &par, std::vector<Detector> dets, long ndet, long 
   // baseline start times (baseline_times, parameter_control.f90:956-977)
   btime_.assign(noba_short_, 0.0);
   if (is_device) {
-    std::vector<double> all(nsamp);
-    MADAM_CUDA(cudaMemcpyAsync(all.data(), timestamps, nsamp * sizeof(double),
-                               cudaMemcpyDeviceToHost, st_));
-    MADAM_CUDA(cudaStreamSynchronize(st_));
-    for (long k = 0; k < noba_short_; ++k) btime_[k] = all[bstart_[k]];
+    if (noba_short_ > 0) {
+      DevBuf<double> bt;
+      bt.alloc(noba_short_);
+      MADAM_LAUNCH(k_take, grid_for(noba_short_), 256, 0, st_, timestamps, bstart_d_.get(),
+                   (long long)noba_short_, bt.get());
+      MADAM_CUDA(cudaMemcpyAsync(btime_.data(), bt.get(), noba_short_ * sizeof(double),
+                                 cudaMemcpyDeviceToHost, st_));
+      MADAM_CUDA(cudaStreamSynchronize(st_));
+    }
   } else {
     for (long k = 0; k < noba_short_; ++k) btime_[k] = timestamps[bstart_[k]];
   }
-  auto mark = [&](int i) {
-    MADAM_CUDA(cudaStreamSynchronize(st_));
-    setup_marks_[i] = now_ms() - t0;
-  };
-  mark(0);
-  build_filter();
   mark(1);
-  flag_and_compact(true);
+  struct FilterJobGuard {
+    std::future<void> &f;
+    ~FilterJobGuard() {
+      if (f.valid()) f.wait();
+    }
+  } filter_guard{filter_job_};
+  build_filter();
   mark(2);
-  build_runs();
+  flag_and_compact(true);
   mark(3);
-  setup_scatter();
+  build_runs();
   mark(4);
-  if (par_.kfirst) build_csr();
+  setup_scatter();
   mark(5);
+  if (par_.kfirst) build_csr();
+  mark(6);
   if (par_.kfirst) {
     map_side_setup();
     initialize_a();
-    mark(6);
-    build_segments();
     mark(7);
-    construct_preconditioner();
+    build_segments();
+    build_filter_finish();
     mark(8);
+    construct_preconditioner();
+    mark(9);
     MADAM_CUDA(cudaStreamSynchronize(st_));
     timings.setup_ms = now_ms() - t0;
     iterate();
@@ -1918,7 +1984,7 @@ long Engine::result_size(const std::string &name) {
   if (name == "band_widths") return (long)band_widths_.size();
   if (name == "scalars") return 20;
   if (name == "timings") return 9;
-  if (name == "setup_marks") return 9;
+  if (name == "setup_marks") return kSetupMarks;
   return -1;
 }
 

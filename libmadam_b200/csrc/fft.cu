@@ -555,19 +555,19 @@ FFTPlan::FFTPlan(long nof_) : nof(nof_), N(nof_ / 2) {
 }
 
 FFTPlan::~FFTPlan() {
-  if (table) cudaFree(table);
-  if (work) cudaFree(work);
-  if (means) cudaFree(means);
+  if (table) dev_free(table);
+  if (work) dev_free(work);
+  if (means) dev_free(means);
 }
 
 void FFTPlan::reserve(long nseg) {
   if (nseg <= nseg_max) return;
-  if (work) cudaFree(work);
-  if (means) cudaFree(means);
+  if (work) dev_free(work);
+  if (means) dev_free(means);
   work = nullptr;
   means = nullptr;
-  if (R) MADAM_CUDA(cudaMalloc(&work, (size_t)nseg * N * sizeof(double2)));
-  MADAM_CUDA(cudaMalloc(&means, (size_t)nseg * kMeanBlocks * sizeof(double)));
+  if (R) work = (double *)dev_alloc((size_t)nseg * N * sizeof(double2));
+  means = (double *)dev_alloc((size_t)nseg * kMeanBlocks * sizeof(double));
   nseg_max = nseg;
 }
 
@@ -575,7 +575,7 @@ void FFTPlan::convolve(cudaStream_t st, const ConvSeg *segs, long nseg, const do
                        const double *x, double *y) {
   if (nseg == 0) return;
   if (!table) {
-    MADAM_CUDA(cudaMalloc(&table, (size_t)2 * N * sizeof(double2)));
+    table = (double *)dev_alloc((size_t)2 * N * sizeof(double2));
     MADAM_LAUNCH(k_fill_table, (unsigned)std::min<long long>(4096, (2 * N + 255) / 256), 256, 0,
                  st, (double2 *)table, 2LL * N);
   }

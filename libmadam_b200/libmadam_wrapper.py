@@ -213,9 +213,11 @@ def timings():
 
 def setup_marks():
     """Cumulative host time (ms) after each setup phase of the last destripe:
-    start, filter, flagging+compaction, runs, binning, pixel-sorted pointing,
+    input binding (host->device copies), layout (pixel check, periods, baseline
+    times), filter, flagging+compaction, runs, binning, pixel-sorted pointing,
     RHS, segments, preconditioner."""
-    keys = ["start", "filter", "compact", "runs", "bin", "csr", "rhs", "segments", "precond"]
+    keys = ["bind", "layout", "filter", "compact", "runs", "bin", "csr", "rhs", "segments",
+            "precond"]
     return dict(zip(keys, get_result("setup_marks").tolist()))
 
 
