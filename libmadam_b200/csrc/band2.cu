@@ -325,15 +325,217 @@ __device__ __forceinline__ void recur(int w, const Seq &q, int run, int p0, int 
   else recur_reg<(W > 0 ? W : 1), HAS_IN, HAS_OUT>(w, q, run, p0, p1, in, state, out, tail);
 }
 
+// ------------------------------------------------------ staged passes --
+// A warp takes 32 consecutive chunks, one per lane.  Each lane's positions are
+// read and written through shared-memory tiles: for every chunk of the warp
+// the lanes copy 32 consecutive values with 8-byte cp.async (one 256-byte
+// segment per copy round instead of 32 scattered lines), the next tile
+// streaming in while the current one is solved.  Tiles are TP positions, a
+// multiple of the window R = W + 1, so the register window keeps its slot
+// mapping across tiles.
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <int W>
+struct Stage {
+  static constexpr int R = W + 1;
+  static constexpr int TP = R * ((32 + R - 1) / R);  // tile positions
+  static constexpr int LD = TP + 1;                  // padded row
+  static constexpr int M = (TP + 31) / 32;           // copy rounds per row
+  static constexpr size_t kSmem = (size_t)3 * 32 * LD * sizeof(double);
+};
+
+// One lane's chunk in one direction: positions t in [0, len) are vector index
+// base + step * t and recurrence position p0 + t.
+struct Lane {
+  long long base;
+  int step, len, p0, run;
+  const PRun *runs;
+  int rend;
+};
+
+template <int W, bool HAS_OUT>
+__device__ void staged_recur(double *tin, double *tout, long long *sb, int *ss, int *sl,
+                             const double *tab, const Lane &L, int w, const double *in,
+                             const double *state, double *out, double *tail) {
+  using G = Stage<W>;
+  constexpr int R = G::R, TP = G::TP, LD = G::LD, M = G::M;
+  const int lane = threadIdx.x & 31;
+  __syncwarp();
+  sb[lane] = L.base;
+  ss[lane] = L.step;
+  sl[lane] = L.len;
+  int maxlen = L.len;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, o));
+  __syncwarp();
+  const int ntile = (maxlen + TP - 1) / TP;
+  auto stage = [&](int k, int b) {
+    double *dst = tin + (size_t)b * 32 * LD;
+    for (int j = 0; j < 32; ++j) {
+      const int len = sl[j];
+      const long long base = sb[j];
+      const int step = ss[j];
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        const int x = lane + 32 * m;
+        const int t = k * TP + x;
+        if (x < TP && t < len) cp_async8(dst + j * LD + x, in + base + (long long)step * t);
+      }
+    }
+  };
+  // register window: slot of position t is t mod R
+  double v[R];
+#pragma unroll
+  for (int s = 0; s < R; ++s) {
+    const int m = R - s;  // slot s >= 1 holds the value m positions before the start
+    v[s] = (s >= 1 && m <= w && state) ? state[w - m] : 0.0;
+  }
+  double K[W + 1];
+  double kinv = 0;
+  int run = L.run, next = INT_MAX;
+  auto load = [&](int rr) {
+    const double *E = tab + L.runs[rr].off;
+#pragma unroll
+    for (int d = 1; d <= W; ++d) K[d] = d <= w ? E[d] : 0.0;
+    kinv = E[w + 1];
+    next = (rr + 1 < L.rend) ? L.runs[rr + 1].start : INT_MAX;
+  };
+  if (L.len > 0) load(run);
+  if (ntile > 0) stage(0, 0);
+  cp_async_commit();
+  for (int k = 0; k < ntile; ++k) {
+    if (k + 1 < ntile) stage(k + 1, (k + 1) & 1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncwarp();
+    const double *row = tin + (size_t)(k & 1) * 32 * LD + lane * LD;
+    double *orow = tout + lane * LD;
+#pragma unroll 1
+    for (int b0 = 0; b0 < TP; b0 += R) {
+      const int t0 = k * TP + b0;
+      if (t0 >= L.len) break;
+      const int pb = L.p0 + t0;
+      if (t0 + R <= L.len && pb + R <= next) {
+#pragma unroll
+        for (int t = 0; t < R; ++t) {
+          double acc = row[b0 + t];
+#pragma unroll
+          for (int d = W; d >= 1; --d) acc -= K[d] * v[(t - d + 2 * R) % R];
+          v[t] = acc * kinv;
+          if (HAS_OUT) orow[b0 + t] = v[t];
+        }
+      } else {
+#pragma unroll
+        for (int t = 0; t < R; ++t) {
+          if (t0 + t < L.len) {
+            const int p = pb + t;
+            if (p >= next) {
+              while (p >= next) {
+                ++run;
+                next = (run + 1 < L.rend) ? L.runs[run + 1].start : INT_MAX;
+              }
+              load(run);
+            }
+            double acc = row[b0 + t];
+#pragma unroll
+            for (int d = W; d >= 1; --d) acc -= K[d] * v[(t - d + 2 * R) % R];
+            v[t] = acc * kinv;
+            if (HAS_OUT) orow[b0 + t] = v[t];
+          }
+        }
+      }
+    }
+    __syncwarp();
+    if (HAS_OUT) {
+      for (int j = 0; j < 32; ++j) {
+        const int len = sl[j];
+        const long long base = sb[j];
+        const int step = ss[j];
+#pragma unroll
+        for (int m = 0; m < M; ++m) {
+          const int x = lane + 32 * m;
+          const int t = k * TP + x;
+          if (x < TP && t < len) out[base + (long long)step * t] = tout[j * LD + x];
+        }
+      }
+      __syncwarp();
+    }
+  }
+  cp_async_wait<0>();
+  __syncwarp();
+  if (tail && L.len > 0) {
+    const int base = (((L.len - w) % R) + R) % R;  // slot of the value w before the end
+#pragma unroll
+    for (int s = 0; s < R; ++s) {
+      int i = s - base;
+      if (i < 0) i += R;
+      if (i < w) tail[i] = v[s];
+    }
+  }
+}
+
 // mode 0: forward pass 1 (tails -> wp)
 // mode 1: forward pass 2 (state ws[c-1], writes z), then backward pass 1 on
 //         the chunk's own rows of z (tails -> wp)
 // mode 2: backward pass 2 (state ws[c+1], z in place)
 template <int W>
-__global__ void __launch_bounds__(64) k_band2_pass(const PSeg *segs, const PChunk *ch, int c0,
-                                                   int c1, const PRun *runs, const PRun *cruns,
-                                                   const double *tab, int mode, const double *r,
-                                                   double *z, const double *ws, double *wp) {
+__global__ void __launch_bounds__(32) k_band2_pass_staged(
+    const PSeg *segs, const PChunk *ch, int c0, int c1, const PRun *runs, const PRun *cruns,
+    const double *tab, int mode, const double *r, double *z, const double *ws, double *wp) {
+  extern __shared__ double bsm[];
+  __shared__ long long sb[32];
+  __shared__ int ss[32], sl[32];
+  using G = Stage<W>;
+  double *tin = bsm, *tout = bsm + 2 * 32 * G::LD;
+  const int lane = threadIdx.x & 31;
+  const int c = c0 + blockIdx.x * 32 + lane;
+  const bool act = c < c1;
+  PChunk k{};
+  PSeg g{};
+  if (act) {
+    k = ch[c];
+    g = segs[k.seg];
+  }
+  const int w = g.nb - 1;
+  Lane f{}, b{};
+  if (act) {
+    f = Lane{g.k0 + k.a, 1, k.b - k.a, k.a, k.run_f, runs, g.run_off + g.nrun};
+    b = Lane{g.k0 + k.b - 1, -1, k.b - k.a, g.n - k.b, k.run_b, cruns, g.crun_off + g.ncrun};
+  }
+  if (mode == 0) {
+    staged_recur<W, false>(tin, tout, sb, ss, sl, tab, f, w, r, nullptr, nullptr,
+                           (act && !k.last) ? wp + (long long)c * kBand2State : nullptr);
+    return;
+  }
+  if (mode == 1) {
+    staged_recur<W, true>(tin, tout, sb, ss, sl, tab, f, w, r,
+                          (act && !k.first) ? ws + (long long)(c - 1) * kBand2State : nullptr,
+                          z, nullptr);
+    __threadfence_block();
+    __syncwarp();
+    staged_recur<W, false>(tin, tout, sb, ss, sl, tab, b, w, z, nullptr, nullptr,
+                           (act && !k.first) ? wp + (long long)c * kBand2State : nullptr);
+    return;
+  }
+  staged_recur<W, true>(tin, tout, sb, ss, sl, tab, b, w, z,
+                        (act && !k.last) ? ws + (long long)(c + 1) * kBand2State : nullptr, z,
+                        nullptr);
+}
+
+// Widths above 32: one thread per chunk, window in local memory.
+__global__ void __launch_bounds__(64) k_band2_pass_generic(
+    const PSeg *segs, const PChunk *ch, int c0, int c1, const PRun *runs, const PRun *cruns,
+    const double *tab, int mode, const double *r, double *z, const double *ws, double *wp) {
   const int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= c1) return;
   const PChunk k = ch[c];
@@ -342,20 +544,20 @@ __global__ void __launch_bounds__(64) k_band2_pass(const PSeg *segs, const PChun
   if (mode <= 1) {
     const Seq f = fwd_seq(g, runs, tab);
     if (mode == 0) {
-      recur<W, true, false>(w, f, k.run_f, k.a, k.b, r, nullptr, nullptr,
-                            k.last ? nullptr : wp + (long long)c * kBand2State);
+      recur_generic(w, f, k.run_f, k.a, k.b, r, nullptr, nullptr,
+                    k.last ? nullptr : wp + (long long)c * kBand2State);
       return;
     }
-    recur<W, true, true>(w, f, k.run_f, k.a, k.b, r,
-                         k.first ? nullptr : ws + (long long)(c - 1) * kBand2State, z, nullptr);
+    recur_generic(w, f, k.run_f, k.a, k.b, r,
+                  k.first ? nullptr : ws + (long long)(c - 1) * kBand2State, z, nullptr);
     const Seq b = bwd_seq(g, cruns, tab);
-    recur<W, true, false>(w, b, k.run_b, g.n - k.b, g.n - k.a, z, nullptr, nullptr,
-                          k.first ? nullptr : wp + (long long)c * kBand2State);
+    recur_generic(w, b, k.run_b, g.n - k.b, g.n - k.a, z, nullptr, nullptr,
+                  k.first ? nullptr : wp + (long long)c * kBand2State);
     return;
   }
   const Seq b = bwd_seq(g, cruns, tab);
-  recur<W, true, true>(w, b, k.run_b, g.n - k.b, g.n - k.a, z,
-                       k.last ? nullptr : ws + (long long)(c + 1) * kBand2State, z, nullptr);
+  recur_generic(w, b, k.run_b, g.n - k.b, g.n - k.a, z,
+                k.last ? nullptr : ws + (long long)(c + 1) * kBand2State, z, nullptr);
 }
 
 // Transfer matrices: column q of T = response of the tail to the unit state
@@ -456,76 +658,104 @@ __global__ void k_band2_scan(const PSeg *segs, int nseg, const PChunk *ch, const
 // w <= W <= 32): lane i keeps row i of the current T_c in registers (reloaded
 // only when the matrix changes) and gathers the state by shuffles; the next
 // chunk's particular state and matrix offset are loaded one step ahead.
+// The same propagation with the state in registers (lane i holds s_i,
+// w <= W <= 32): lane i keeps row i of the current T_c in registers (reloaded
+// only when the matrix changes) and gathers the state by shuffles.  The
+// particular states and matrix offsets of the next 32 chunks are copied into
+// shared memory (cp.async) while the current 32 steps run, so a step waits
+// only on its own arithmetic.  One warp per segment.
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
 template <int W>
-__global__ void k_band2_scan_reg(const PSeg *segs, int s0, int s1, const int *toff,
-                                 const double *T, const double *p, double *s, int dir) {
-  constexpr int D = 8;  // chunks whose particular state and matrix offset are in flight
-  const int seg = s0 + ((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+__global__ void __launch_bounds__(32) k_band2_scan_reg(const PSeg *segs, int s0, const int *toff,
+                                                       const double *T, const double *p,
+                                                       double *s, int dir) {
+  constexpr int B = 32;  // steps per staged block
+  __shared__ double pbuf[2][B][W];
+  __shared__ int tbuf[2][B];
+  const int seg = s0 + blockIdx.x;
   const int lane = threadIdx.x & 31;
-  if (seg >= s1) return;
   const PSeg g = segs[seg];
   const int w = g.nb - 1;
   if (g.nch <= 1 || w <= 0) return;
   const bool on = lane < w;
-  const int c0 = g.ch_off, cl = g.ch_off + g.nch - 1;
-  const int start = dir == 0 ? c0 : cl;
+  const int start = dir == 0 ? g.ch_off : g.ch_off + g.nch - 1;
   const int step = dir == 0 ? 1 : -1;
   const int nsteps = g.nch - 2;  // chunks after start whose state is needed
-  const double *pp = p + (long long)start * kBand2State + lane;
-  double *sp = s + (long long)start * kBand2State + lane;
-  const long long stride = (long long)step * kBand2State;
-  const int *tp = toff + start;
-  double cur = on ? pp[0] : 0.0;
-  if (on) sp[0] = cur;
+  double cur = on ? p[(long long)start * kBand2State + lane] : 0.0;
+  if (on) s[(long long)start * kBand2State + lane] = cur;
+  if (nsteps <= 0) return;
+  const int nblk = (nsteps + B - 1) / B;
+  auto stage = [&](int blk, int b) {
+    for (int r = 0; r < B; ++r) {
+      const int u = blk * B + r;
+      if (u >= nsteps) break;
+      const long long c = start + (long long)(u + 1) * step;
+      if (on) cp_async8(&pbuf[b][r][lane], p + c * kBand2State + lane);
+      if (lane == 0) cp_async4(&tbuf[b][r], toff + c);
+    }
+  };
   double Tr[W];
   int tcur = -1;
-  double pq[D];
-  int tq[D];
+  stage(0, 0);
+  cp_async_commit();
+  for (int blk = 0; blk < nblk; ++blk) {
+    if (blk + 1 < nblk) stage(blk + 1, (blk + 1) & 1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncwarp();
+    const int b = blk & 1;
+    const int nr = min(B, nsteps - blk * B);
+    for (int r = 0; r < nr; ++r) {
+      const double pc = on ? pbuf[b][r][lane] : 0.0;
+      const int tc = tbuf[b][r];
+      if (tc != tcur) {
 #pragma unroll
-  for (int r = 0; r < D; ++r) {
-    pq[r] = (on && r < nsteps) ? pp[(r + 1) * stride] : 0.0;
-    tq[r] = r < nsteps ? tp[(r + 1) * step] : 0;
-  }
-  for (int u0 = 0; u0 < nsteps; u0 += D) {
-#pragma unroll
-    for (int r = 0; r < D; ++r) {
-      const int u = u0 + r;
-      if (u < nsteps) {
-        const double pc = pq[r];
-        const int tc = tq[r];
-        const int un = u + D;
-        if (un < nsteps) {
-          pq[r] = on ? pp[(long long)(un + 1) * stride] : 0.0;
-          tq[r] = tp[(un + 1) * step];
-        }
-        if (tc != tcur) {
-#pragma unroll
-          for (int qq = 0; qq < W; ++qq)
-            Tr[qq] = (on && qq < w) ? T[tc + (long long)lane * w + qq] : 0.0;
-          tcur = tc;
-        }
-        double a0 = pc, a1 = 0, a2 = 0, a3 = 0;
-#pragma unroll
-        for (int qq = 0; qq < W; qq += 4) {
-          a0 += Tr[qq] * __shfl_sync(0xffffffffu, cur, qq);
-          if (qq + 1 < W) a1 += Tr[qq + 1] * __shfl_sync(0xffffffffu, cur, qq + 1);
-          if (qq + 2 < W) a2 += Tr[qq + 2] * __shfl_sync(0xffffffffu, cur, qq + 2);
-          if (qq + 3 < W) a3 += Tr[qq + 3] * __shfl_sync(0xffffffffu, cur, qq + 3);
-        }
-        cur = on ? (a0 + a1) + (a2 + a3) : 0.0;
-        if (on) sp[(long long)(u + 1) * stride] = cur;
+        for (int qq = 0; qq < W; ++qq)
+          Tr[qq] = (on && qq < w) ? T[tc + (long long)lane * w + qq] : 0.0;
+        tcur = tc;
       }
+      double a0 = pc, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+      for (int qq = 0; qq < W; qq += 4) {
+        a0 += Tr[qq] * __shfl_sync(0xffffffffu, cur, qq);
+        if (qq + 1 < W) a1 += Tr[qq + 1] * __shfl_sync(0xffffffffu, cur, qq + 1);
+        if (qq + 2 < W) a2 += Tr[qq + 2] * __shfl_sync(0xffffffffu, cur, qq + 2);
+        if (qq + 3 < W) a3 += Tr[qq + 3] * __shfl_sync(0xffffffffu, cur, qq + 3);
+      }
+      cur = on ? (a0 + a1) + (a2 + a3) : 0.0;
+      const long long c = start + (long long)(blk * B + r + 1) * step;
+      if (on) s[c * kBand2State + lane] = cur;
     }
+    __syncwarp();
   }
+  cp_async_wait<0>();
 }
 
 template <int W>
 void launch_pass(cudaStream_t st, const PSeg *segs, const PChunk *ch, int c0, int c1,
                  const PRun *runs, const PRun *cruns, const double *tab, int mode, const double *r,
                  double *z, const double *ws, double *wp) {
-  const unsigned grid = (unsigned)((c1 - c0 + 63) / 64);
-  MADAM_LAUNCH(k_band2_pass<W>, grid, 64, 0, st, segs, ch, c0, c1, runs, cruns, tab, mode, r, z,
-               ws, wp);
+  if (W == 0) {
+    const unsigned grid = (unsigned)((c1 - c0 + 63) / 64);
+    MADAM_LAUNCH(k_band2_pass_generic, grid, 64, 0, st, segs, ch, c0, c1, runs, cruns, tab, mode,
+                 r, z, ws, wp);
+    return;
+  }
+  constexpr int WW = W > 0 ? W : 1;
+  static bool attr = false;
+  if (!attr) {
+    MADAM_CUDA(cudaFuncSetAttribute(k_band2_pass_staged<WW>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)Stage<WW>::kSmem));
+    attr = true;
+  }
+  const unsigned grid = (unsigned)((c1 - c0 + 31) / 32);
+  MADAM_LAUNCH(k_band2_pass_staged<WW>, grid, 32, Stage<WW>::kSmem, st, segs, ch, c0, c1, runs,
+               cruns, tab, mode, r, z, ws, wp);
 }
 
 // Register widths compiled: the band widths precond_width_min = 10 gives
@@ -628,11 +858,11 @@ void band2_solve(cudaStream_t st, const PSeg *segs, int nseg, const PChunk *ch, 
     for (int i = 0; i < ncls; ++i) {
       const int s0 = cls_seg[i], s1 = cls_seg[i + 1];
       if (s1 <= s0) continue;
-      const unsigned grid = (unsigned)((s1 - s0 + 1) / 2);
+      const unsigned grid = (unsigned)(s1 - s0);
       switch (cls_w[i]) {
 #define MADAM_BAND2_CASE(X)                                                                   \
   case X:                                                                                     \
-    MADAM_LAUNCH(k_band2_scan_reg<X>, grid, 64, 0, st, segs, s0, s1, dir == 0 ? toff_f : toff_b, \
+    MADAM_LAUNCH(k_band2_scan_reg<X>, grid, 32, 0, st, segs, s0, dir == 0 ? toff_f : toff_b,   \
                  T, work_p, work_s, dir);                                                     \
     break;
         MADAM_BAND2_CASE(1)
