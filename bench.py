@@ -210,13 +210,68 @@ def reference_arm(args, world, rank):
     return 0
 
 
+def run_mc(args, world, rank, local):
+    """Batched Monte Carlo form (nside 512, 32 detectors x 2^22 samples, nrhs
+    noise-only realisations sharing one pointing): the multi-right-hand-side
+    solve against the same realisations one destripe_with_cache at a time."""
+    import torch
+    from libmadam_b200 import libmadam_wrapper as W
+    from libmadam_b200 import synthetic as syn
+    cfg = syn.config4()
+    cfg.seed += 1000 * rank
+    R = args.nrhs
+    d = syn.generate(cfg, device="cuda", with_signal=False)
+    sigs = syn.noise_realisations(cfg, R + 1, device="cuda")
+    torch.cuda.synchronize()
+    n = cfg.ndet * cfg.nsamp
+    pars = dict(d["pars"], mcmode=True)
+    pix = d["pixels"].reshape(-1)
+    wts = d["pixweights"].reshape(-1)
+    psd = (d["periods"], d["npsd"], d["psdstarts"], d["psdfreqs"], d["psdvals"])
+    W.destripe(None, pars, d["dets"], d["detweights"], d["timestamps"], pix.clone(), wts,
+               sigs[R].reshape(-1).clone(), *psd)
+    # one realisation at a time (the reference's way), then all at once
+    barrier(world)
+    clk = Clocks(local)
+    W.destripe_with_cache(None, d["timestamps"], pix.clone(), wts, sigs[0].reshape(-1).clone(), b"")
+    t1 = W.timings()
+    it1 = int(W.scalars()["noiter"])
+    single = n * it1 / (t1["iterate_ms"] * 1e-3)
+    W.destripe_with_cache_batch(None, d["timestamps"], pix.clone(), wts, sigs[:R])
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    tb = W.timings()
+    its = W.get_result("noiter_batch")
+    t_it = reduce_max(tb["iterate_ms"], world)
+    value = world * n * float(its.sum()) / (t_it * 1e-3)
+    if rank == 0:
+        line = {"metric": "TOD samples/s per PCG iteration (batched Monte Carlo)",
+                "value": value, "unit": "samples/s per PCG iteration", "n_gpus": world,
+                "steps": int(its.max()), "warmup": 0,
+                "ms_per_step": t_it / max(1, int(its.max())), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "batched MC nside512 32det x 2^22 @100Hz, %d noise "
+                                       "realisations, fknee 0.02-0.2 Hz" % R,
+                           "samples": n, "nrhs": R, "parallelism": "single GPU"},
+                "clocks": clocks,
+                "iterations": {"min": int(its.min()), "max": int(its.max()),
+                               "single_rhs": it1},
+                "batch_iterate_ms": t_it, "batch_setup_ms": tb["setup_ms"],
+                "batch_finalize_ms": tb["finalize_ms"],
+                "single_rhs": {"value": single, "iterate_ms": t1["iterate_ms"]},
+                "speedup_vs_one_at_a_time": value / single}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="2", choices=["2", "1", "prof", "mid", "small"])
+    ap.add_argument("--config", default="2", choices=["2", "1", "prof", "mid", "small", "mc"])
+    ap.add_argument("--nrhs", type=int, default=64)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
@@ -235,6 +290,8 @@ def main():
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device")
     torch.cuda.set_device(local)
+    if args.config == "mc":
+        return run_mc(args, world, rank, local)
     cfg, wname = config_for(args.config)
     cfg.seed += 1000 * rank
     t0 = time.time()

@@ -28,6 +28,19 @@ int madam_b200_destripe_with_cache(int comm, long ndet, long nsamp, long nnz, vo
 /* clear_caches() with a status (reference src/smadam.F90:921-951). */
 int madam_b200_clear_caches(void);
 
+/* Batched Monte Carlo: nrhs realisations of destripe_with_cache (reference
+ * src/smadam.F90:593-918, which takes one realisation per call) that share
+ * one pointing.  signals: float64 [nrhs][ndet][nsamp], host or device memory
+ * like pix.  Every realisation is solved as destripe_with_cache would solve
+ * it right after the caching destripe(..., mcmode=T) call; the cache is left
+ * unchanged.  Results: "map_batch", "binmap_batch" (float64
+ * [nrhs][npix][nmap]), "aa_batch" (float64 [nrhs][ndet][noba]),
+ * "noiter_batch", "rrinit_batch", "rr_final_batch" (float64 [nrhs]).  No
+ * files are written.  No reference counterpart as one call. */
+int madam_b200_destripe_with_cache_batch(int comm, long ndet, long nsamp, long nnz,
+                                         void *timestamps, void *pix, void *pixweights,
+                                         long nrhs, void *signals);
+
 /* Status of the last call (0 = success) and its error message; replaces the
  * reference's abort_mpi messages (src/mpi_wrappers.f90:120-137). */
 int madam_b200_last_error(char *buf, long buflen);

@@ -1142,6 +1142,8 @@ double now_ms() {
 
 }  // namespace
 
+#include "batch_kernels.inl"
 #include "engine_host.inl"
+#include "engine_batch.inl"
 
 }  // namespace madam

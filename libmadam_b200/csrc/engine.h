@@ -110,6 +110,14 @@ class Engine {
                   int32_t *pix, float *pixweights, double *signal,
                   bool is_device);
 
+  // Batched Monte Carlo: nrhs realisations of destripe_with_cache() sharing
+  // the pointing, solved as one multi-right-hand-side PCG.  signals:
+  // [nrhs][ndet][nsamp].  Each realisation is solved as destripe_with_cache
+  // would solve it right after the caching destripe(); the cache is left as
+  // it was.
+  void run_cached_batch(long ndet, long nsamp, long nnz, double *timestamps, int32_t *pix,
+                        float *pixweights, long nrhs, double *signals, bool is_device);
+
   bool cached() const { return cached_; }
   const Params &params() const { return par_; }
 
@@ -148,6 +156,32 @@ class Engine {
   void finalize(bool first_call);
   void writeback_host();
   void write_fits(bool first_call);
+
+  // --- batched Monte Carlo
+  void iterate_batch();
+  void apply_A_batch();
+  void apply_preconditioner_batch(const double *r, double *z);
+  void build_batch_tables();
+  long nrhs_ = 0;                        // right-hand sides of the last batch
+  DevBuf<double> yb_, aab_, rb_, pb_, zb_, apb_, rob_, pwb_;  // [R][nb]
+  DevBuf<double> lmapb_, scatpb_;        // [R][nloc_cross][nmap], scatter partials
+  DevBuf<double> binb_, mapb_, binmapb_; // [R][nloc][nmap]
+  DevBuf<double> partb_, scalb_;         // [R][3][kRedBlocks], [R][S_NSCAL]
+  DevBuf<int> actb_;
+  std::vector<int> act_host_;
+  std::vector<double> noiter_b_, rrinit_b_, rrfinal_b_;
+  // band factor tables replicated per right-hand side (offsets k0 + r nb)
+  std::vector<PSeg> band2_pseg_h_;
+  std::vector<PChunk> band2_ch_h_;
+  DevBuf<PSeg> p2segs_b_;
+  DevBuf<PChunk> p2ch_b_;
+  DevBuf<int> p2tf_b_, p2tb_b_;
+  DevBuf<double> p2wp_b_, p2ws_b_;
+  std::vector<int> band2_cls_begin_b_, band2_cls_seg_b_;
+  int p2nseg_b_ = 0, p2nch_b_ = 0;
+  DevBuf<ConvSeg> filt_segs_b_d_;
+  long batch_tables_r_ = 0;              // right-hand sides the tables were built for
+  bool suppress_fits_ = false;
 
   // --- iteration pieces
   void apply_A(const double *p, const double *pw, double *ap, bool timed);

@@ -1,0 +1,429 @@
+// Batched Monte Carlo: many destripe_with_cache() realisations (smadam.F90:
+// 593-918) that share one pointing, solved together.
+//
+// The reference solves Monte Carlo realisations one destripe_with_cache call
+// at a time.  Here the pointing-side setup (flagging, compaction, runs, the
+// pixel-sorted pointing) is done once, every realisation gets its own binned
+// map and right-hand side (bin_tod + initialize_a on top of the cached
+// state), and the R systems are solved as one multi-right-hand-side PCG:
+// each pass over the pointing serves a group of right-hand sides, the
+// filter and the band preconditioner run over R copies of their segment
+// tables, and every right-hand side keeps its own CG scalars, convergence
+// test and iteration count (iterate_a, smadam_routines.f90:677-983, per
+// realisation).  The per-realisation arithmetic is that of the single solve.
+
+namespace {
+constexpr int kScatterGroup = 8;  // right-hand sides per scatter pass
+constexpr int kGatherGroup = 4;   // right-hand sides per gather pass
+constexpr size_t kGatherGroupSmem = (size_t)8 * kGatherGroup * kGatherChunk * sizeof(double);
+}  // namespace
+
+void Engine::build_batch_tables() {
+  // band factor tables and filter segments replicated for nrhs_ right-hand
+  // sides (vector offsets r * nb), grouped by width class
+  const long long nb = (long long)ndet_ * noba_short_;
+  if (batch_tables_r_ == nrhs_) return;
+  std::vector<PSeg> ps;
+  std::vector<PChunk> ch;
+  std::vector<int> tf, tb;
+  band2_cls_begin_b_.clear();
+  band2_cls_seg_b_.clear();
+  for (size_t i = 0; i + 1 < band2_cls_seg_.size(); ++i) {
+    band2_cls_begin_b_.push_back((int)ch.size());
+    band2_cls_seg_b_.push_back((int)ps.size());
+    for (long r = 0; r < nrhs_; ++r)
+      for (int s = band2_cls_seg_[i]; s < band2_cls_seg_[i + 1]; ++s) {
+        PSeg q = band2_pseg_h_[s];
+        q.k0 += r * nb;
+        q.ch_off = (int)ch.size();
+        const int sn = (int)ps.size();
+        ps.push_back(q);
+        for (int c = band2_pseg_h_[s].ch_off; c < band2_pseg_h_[s].ch_off + q.nch; ++c) {
+          PChunk k = band2_ch_h_[c];
+          k.seg = sn;
+          ch.push_back(k);
+          tf.push_back(k.tf);
+          tb.push_back(k.tb);
+        }
+      }
+  }
+  band2_cls_begin_b_.push_back((int)ch.size());
+  band2_cls_seg_b_.push_back((int)ps.size());
+  p2nseg_b_ = (int)ps.size();
+  p2nch_b_ = (int)ch.size();
+  if (!ps.empty()) {
+    p2segs_b_.alloc(ps.size());
+    p2ch_b_.alloc(ch.size());
+    p2tf_b_.alloc(tf.size());
+    p2tb_b_.alloc(tb.size());
+    p2wp_b_.alloc((size_t)ch.size() * kBand2State);
+    p2ws_b_.alloc((size_t)ch.size() * kBand2State);
+    MADAM_CUDA(cudaMemcpyAsync(p2segs_b_.get(), ps.data(), ps.size() * sizeof(PSeg),
+                               cudaMemcpyHostToDevice, st_));
+    MADAM_CUDA(cudaMemcpyAsync(p2ch_b_.get(), ch.data(), ch.size() * sizeof(PChunk),
+                               cudaMemcpyHostToDevice, st_));
+    MADAM_CUDA(cudaMemcpyAsync(p2tf_b_.get(), tf.data(), tf.size() * sizeof(int),
+                               cudaMemcpyHostToDevice, st_));
+    MADAM_CUDA(cudaMemcpyAsync(p2tb_b_.get(), tb.data(), tb.size() * sizeof(int),
+                               cudaMemcpyHostToDevice, st_));
+  }
+  // the filter (or fprecond) segments
+  const std::vector<ConvSeg> &fs = par_.use_fprecond ? filt_segs_ : filt_segs_;
+  std::vector<ConvSeg> cs;
+  for (long r = 0; r < nrhs_; ++r)
+    for (ConvSeg c : fs) {
+      c.x_off += r * nb;
+      c.y_off += r * nb;
+      cs.push_back(c);
+    }
+  if ((long)cs.size() > 65535) fail("too many filter segments in one batch (reduce nrhs)");
+  filt_segs_b_d_.alloc(std::max<size_t>(1, cs.size()));
+  if (!cs.empty())
+    MADAM_CUDA(cudaMemcpyAsync(filt_segs_b_d_.get(), cs.data(), cs.size() * sizeof(ConvSeg),
+                               cudaMemcpyHostToDevice, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  batch_tables_r_ = nrhs_;
+}
+
+void Engine::apply_preconditioner_batch(const double *r, double *z) {
+  // preconditioning_band (noise_routines.f90:1159-1256) for every right-hand side
+  const long long nb = (long long)ndet_ * noba_short_;
+  const long long nt = nb * nrhs_;
+  if (par_.precond_width_max < 1) {
+    MADAM_CUDA(cudaMemcpyAsync(z, r, nt * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+    return;
+  }
+  if (use_diagonal_) {
+    for (long k = 0; k < nrhs_; ++k)
+      MADAM_LAUNCH(k_mul, grid_for(nb), 256, 0, st_, z + k * nb, r + k * nb, prec_diag_.get(), nb);
+    return;
+  }
+  MADAM_CUDA(cudaMemcpyAsync(z, r, nt * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+  const long nfs = (long)filt_segs_.size() * nrhs_;
+  if (par_.use_fprecond) {
+    if (nfs > 0) fft_->convolve(st_, filt_segs_b_d_.get(), nfs, fprec_.get(), r, z);
+    return;
+  }
+  band2_solve(st_, p2segs_b_.get(), p2nseg_b_, p2ch_b_.get(), p2nch_b_, p2tf_b_.get(),
+              p2tb_b_.get(), band2_cls_w_.data(), band2_cls_begin_b_.data(),
+              band2_cls_seg_b_.data(), (int)band2_cls_w_.size(), p2runs_.get(), p2cruns_.get(),
+              p2rows_.get(), p2T_.get(), r, z, p2wp_b_.get(), p2ws_b_.get());
+  for (long k = 0; k < nrhs_; ++k) {
+    band_solve(st_, band_segs_d_.get(), (int)band_segs_.size(), band_.get(), r + k * nb,
+               z + k * nb);
+    cg_preconditioner_segments(r + k * nb, z + k * nb);
+  }
+}
+
+void Engine::apply_A_batch() {
+  // A p for every right-hand side (iterate_a 798-878)
+  const long long nb = (long long)ndet_ * noba_short_;
+  const long long tstride = (long long)std::max<long>(1, nloc_cross_) * nmap_;
+  const long long pstride = (long long)scatter_partial_.n;
+  // 1) baseline -> map, combine, ccmultiply
+  if (nloc_cross_ > 0 && nscatter_chunks_ > 0) {
+    for (long r0 = 0; r0 < nrhs_; r0 += kScatterGroup) {
+      const int nr = (int)std::min<long>(kScatterGroup, nrhs_ - r0);
+      if (nmap_ == 3)
+        MADAM_LAUNCH((k_scatter_chunks_b<3, kScatterGroup>), kRedBlocks, 256, 0, st_,
+                     scatter_chunks_.get(), nscatter_chunks_, sp4_.get(), sp2_.get(), pwb_.get(),
+                     nb, (int)r0, nr, lmapb_.get(), tstride, scatpb_.get(), pstride);
+      else
+        MADAM_LAUNCH((k_scatter_chunks_b<1, kScatterGroup>), kRedBlocks, 256, 0, st_,
+                     scatter_chunks_.get(), nscatter_chunks_, sp4_.get(), sp2_.get(), pwb_.get(),
+                     nb, (int)r0, nr, lmapb_.get(), tstride, scatpb_.get(), pstride);
+    }
+    if (nscatter_multi_ > 0) {
+      const dim3 g((unsigned)std::min<long long>(1184, (nscatter_multi_ + 255) / 256),
+                   (unsigned)nrhs_);
+      if (nmap_ == 3)
+        MADAM_LAUNCH(k_scatter_combine_b<3>, g, 256, 0, st_, scatter_multi_.get(),
+                     nscatter_multi_, scatpb_.get(), pstride, lmapb_.get(), tstride);
+      else
+        MADAM_LAUNCH(k_scatter_combine_b<1>, g, 256, 0, st_, scatter_multi_.get(),
+                     nscatter_multi_, scatpb_.get(), pstride, lmapb_.get(), tstride);
+    }
+  }
+  if (nloc_cross_ > 0) {
+    const dim3 g((unsigned)std::min<long long>(1184, (nloc_cross_ + 255) / 256),
+                 (unsigned)nrhs_);
+    if (nmap_ == 3)
+      MADAM_LAUNCH(k_ccmult_b<3>, g, 256, 0, st_, cca_.get(), lmapb_.get(),
+                   (long long)nloc_cross_);
+    else
+      MADAM_LAUNCH(k_ccmult_b<1>, g, 256, 0, st_, cca_.get(), lmapb_.get(),
+                   (long long)nloc_cross_);
+  }
+  // 2) noise prior ap = C_a^-1 p (cinvmul, 829-845)
+  const long long nt = nb * nrhs_;
+  if (par_.kfilter) {
+    MADAM_CUDA(cudaMemcpyAsync(apb_.get(), pb_.get(), nt * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st_));
+    const long nfs = (long)filt_segs_.size() * nrhs_;
+    if (nfs > 0) fft_->convolve(st_, filt_segs_b_d_.get(), nfs, fcov_.get(), pb_.get(), apb_.get());
+  } else if (par_.diagfilter != 0) {
+    for (long k = 0; k < nrhs_; ++k)
+      MADAM_LAUNCH(k_diagfilter, grid_for(nb), 256, 0, st_, apb_.get() + k * nb, nna_.get(),
+                   pb_.get() + k * nb, par_.diagfilter, nb);
+  } else {
+    MADAM_CUDA(cudaMemsetAsync(apb_.get(), 0, nt * sizeof(double), st_));
+  }
+  // 3) map -> baseline and p.ap (849-878)
+  if (ngather_chunks_ > 0) {
+    static bool attr = false;
+    if (!attr) {
+      MADAM_CUDA(cudaFuncSetAttribute(k_gather_chunks_b<3, kGatherGroup>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kGatherGroupSmem));
+      MADAM_CUDA(cudaFuncSetAttribute(k_gather_chunks_b<1, kGatherGroup>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kGatherGroupSmem));
+      attr = true;
+    }
+    for (long r0 = 0; r0 < nrhs_; r0 += kGatherGroup) {
+      const int nr = (int)std::min<long>(kGatherGroup, nrhs_ - r0);
+      if (nmap_ == 3)
+        MADAM_LAUNCH((k_gather_chunks_b<3, kGatherGroup>), kRedBlocks, 256, kGatherGroupSmem, st_,
+                     gather_chunks_.get(), ngather_chunks_, point4_.get(), pixc_.get(),
+                     bstart_d_.get(), noba_short_, nsamp_, bw_.get(), pb_.get(), nb, nna_.get(),
+                     lmapb_.get(), tstride, (int)ndeg_shift_, (int)nloc_, rmask_.get(),
+                     apb_.get(), (int)r0, nr, partb_.get());
+      else
+        MADAM_LAUNCH((k_gather_chunks_b<1, kGatherGroup>), kRedBlocks, 256, kGatherGroupSmem, st_,
+                     gather_chunks_.get(), ngather_chunks_, point4_.get(), pixc_.get(),
+                     bstart_d_.get(), noba_short_, nsamp_, bw_.get(), pb_.get(), nb, nna_.get(),
+                     lmapb_.get(), tstride, (int)ndeg_shift_, (int)nloc_, rmask_.get(),
+                     apb_.get(), (int)r0, nr, partb_.get());
+    }
+  } else {
+    // long baselines: the single-RHS gathers, one right-hand side at a time
+    for (long k = 0; k < nrhs_; ++k) {
+      double *pk = pb_.get() + k * nb, *apk = apb_.get() + k * nb;
+      double *mk = lmapb_.get() + k * tstride, *partk = partb_.get() + k * 3 * kRedBlocks;
+      if (gather_kb_ > 0) {
+        if (nmap_ == 3)
+          MADAM_LAUNCH(k_gather_tiled<3>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
+                       bstart_d_.get(), noba_short_, nsamp_, gather_kb_, gather_tiles_det_,
+                       (int)ndet_, bw_.get(), pk, nna_.get(), mk, (int)ndeg_shift_, (int)nloc_,
+                       rmask_.get(), apk, partk);
+        else
+          MADAM_LAUNCH(k_gather_tiled<1>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
+                       bstart_d_.get(), noba_short_, nsamp_, gather_kb_, gather_tiles_det_,
+                       (int)ndet_, bw_.get(), pk, nna_.get(), mk, (int)ndeg_shift_, (int)nloc_,
+                       rmask_.get(), apk, partk);
+      } else if (nmap_ == 3) {
+        MADAM_LAUNCH(k_gather<3>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
+                     bstart_d_.get(), nb, noba_short_, nsamp_, bw_.get(), pk, nna_.get(), mk,
+                     (int)ndeg_shift_, (int)nloc_, rmask_.get(), apk, partk);
+      } else {
+        MADAM_LAUNCH(k_gather<1>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
+                     bstart_d_.get(), nb, noba_short_, nsamp_, bw_.get(), pk, nna_.get(), mk,
+                     (int)ndeg_shift_, (int)nloc_, rmask_.get(), apk, partk);
+      }
+    }
+  }
+  MADAM_LAUNCH(k_finish_b, (unsigned)nrhs_, 1024, 0, st_, partb_.get(), kRedBlocks, 1,
+               scalb_.get(), 1, 0, actb_.get());
+}
+
+void Engine::iterate_batch() {
+  // iterate_a (smadam_routines.f90:677-983) for every right-hand side
+  const double t0 = now_ms();
+  const long long nb = (long long)ndet_ * noba_short_;
+  const long long nt = nb * nrhs_;
+  const long R = nrhs_;
+  for (auto *b : {&rb_, &pb_, &zb_, &apb_, &rob_, &pwb_, &aab_}) b->alloc(nt);
+  partb_.alloc((size_t)R * 3 * kRedBlocks);
+  scalb_.alloc((size_t)R * S_NSCAL);
+  scalb_.zero(st_);
+  actb_.alloc(R);
+  lmapb_.alloc((size_t)R * std::max<long>(1, nloc_cross_) * nmap_);
+  scatpb_.alloc((size_t)R * std::max<size_t>(1, scatter_partial_.n));
+  build_batch_tables();
+  act_host_.assign(R, 1);
+  auto upload_act = [&]() {
+    MADAM_CUDA(cudaMemcpyAsync(actb_.get(), act_host_.data(), R * sizeof(int),
+                               cudaMemcpyHostToDevice, st_));
+  };
+  upload_act();
+  noiter_b_.assign(R, 0.0);
+  rrinit_b_.assign(R, 0.0);
+  rrfinal_b_.assign(R, 1.0);
+  MADAM_CUDA(cudaMemcpyAsync(rb_.get(), yb_.get(), nt * sizeof(double), cudaMemcpyDeviceToDevice,
+                             st_));
+  aab_.zero(st_);
+  apply_preconditioner_batch(rb_.get(), zb_.get());
+  const dim3 gv((unsigned)std::min<long long>(4736, (nb + 255) / 256), (unsigned)R);
+  const dim3 gd(kRedBlocks, (unsigned)R);
+  MADAM_LAUNCH(k_update_p_b, gv, 256, 0, st_, pb_.get(), zb_.get(), pwb_.get(), bw_.get(), nb,
+               scalb_.get(), 1, actb_.get());
+  MADAM_LAUNCH(k_dots_b, gd, 256, 0, st_, rb_.get(), zb_.get(), rb_.get(), rb_.get(), nullptr,
+               nullptr, 2, rmask_.get(), nb, actb_.get(), partb_.get());
+  MADAM_LAUNCH(k_finish_b, (unsigned)R, 1024, 0, st_, partb_.get(), kRedBlocks, 2, scalb_.get(),
+               0, S_RZ, actb_.get());
+  std::vector<double> sc((size_t)R * S_NSCAL);
+  auto fetch = [&]() {
+    MADAM_CUDA(cudaMemcpyAsync(sc.data(), scalb_.get(), sc.size() * sizeof(double),
+                               cudaMemcpyDeviceToHost, st_));
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+  };
+  fetch();
+  long nact = 0;
+  for (long k = 0; k < R; ++k) {
+    const double rzinit = sc[k * S_NSCAL + S_RZ];
+    rrinit_b_[k] = sc[k * S_NSCAL + S_RR];
+    if (rzinit < fsp(1e-30f) || std::isnan(rzinit)) act_host_[k] = 0;
+    nact += act_host_[k];
+  }
+  upload_act();
+  long istep = 0;
+  while (istep < par_.iter_max && nact > 0) {
+    ++istep;
+    apply_A_batch();
+    MADAM_LAUNCH(k_update_ar_b, gv, 256, 0, st_, aab_.get(), rb_.get(), rob_.get(), pb_.get(),
+                 apb_.get(), nb, scalb_.get(), actb_.get());
+    apply_preconditioner_batch(rb_.get(), zb_.get());
+    MADAM_LAUNCH(k_dots_b, gd, 256, 0, st_, rb_.get(), zb_.get(), rob_.get(), zb_.get(),
+                 rb_.get(), rb_.get(), 3, rmask_.get(), nb, actb_.get(), partb_.get());
+    MADAM_LAUNCH(k_finish_b, (unsigned)R, 1024, 0, st_, partb_.get(), kRedBlocks, 3,
+                 scalb_.get(), 2, 0, actb_.get());
+    fetch();
+    bool changed = false;
+    for (long k = 0; k < R; ++k) {
+      if (!act_host_[k]) continue;
+      const double rz = sc[k * S_NSCAL + S_RZ], rr = sc[k * S_NSCAL + S_RR];
+      rrfinal_b_[k] = rr / rrinit_b_[k];
+      noiter_b_[k] = (double)istep;
+      if (rr / rrinit_b_[k] > 1e3)
+        fail("CG is diverging (Monte Carlo realisation " + std::to_string(k) + ")");
+      if ((rr / rrinit_b_[k] < par_.cglimit && istep > par_.iter_min) || rz == 0) {
+        act_host_[k] = 0;
+        --nact;
+        changed = true;
+      }
+    }
+    if (changed) upload_act();
+    if (nact == 0) break;
+    MADAM_LAUNCH(k_update_p_b, gv, 256, 0, st_, pb_.get(), zb_.get(), pwb_.get(), bw_.get(), nb,
+                 scalb_.get(), 0, actb_.get());
+  }
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  timings.iterate_ms = now_ms() - t0;
+}
+
+void Engine::run_cached_batch(long ndet, long nsamp, long nnz, double *timestamps, int32_t *pix,
+                              float *pixweights, long nrhs, double *signals, bool is_device) {
+  if (!cached_) fail("destripe_with_cache called with empty caches.");
+  if (nrhs < 1) fail("nrhs must be at least 1");
+  if (par_.temperature_only && nnz != 1)
+    fail("temperature_only=T but pointing weights are polarized");
+  if (ndet != ndet_ || nsamp != nsamp_ || nnz != nnz_)
+    fail("destripe_with_cache: data shape differs from the cached call");
+  const double t0 = now_ms();
+  timings = Timings();
+  rr_history.clear();
+  noiter = 0;
+  const long long n = (long long)ndet * nsamp;
+  const long long nb = (long long)ndet_ * noba_short_;
+  nrhs_ = nrhs;
+  // pointing-side setup, once
+  d_pix_caller_ = is_device ? pix : nullptr;
+  bind_inputs(timestamps, pix, pixweights, signals, is_device, false);
+  flag_and_compact(false);
+  build_runs();
+  if (par_.kfirst) build_csr();
+  // the cached state every realisation starts from
+  DevBuf<double> wamap0;
+  wamap0.alloc(wamap_.n);
+  if (wamap_.n)
+    MADAM_CUDA(cudaMemcpyAsync(wamap0.get(), wamap_.get(), wamap_.n * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st_));
+  const long long nv = (long long)nloc_ * nmap_;
+  yb_.alloc((size_t)nrhs * nb);
+  binb_.alloc((size_t)nrhs * std::max<long long>(1, nv));
+  mapb_.alloc((size_t)nrhs * std::max<long long>(1, nv));
+  binmapb_.alloc((size_t)nrhs * std::max<long long>(1, nv));
+  auto select_tod = [&](long k) {
+    if (is_device) {
+      d_tod_ = signals + k * n;
+    } else {
+      MADAM_CUDA(cudaMemcpyAsync(tod_own_.get(), signals + k * n, n * sizeof(double),
+                                 cudaMemcpyHostToDevice, st_));
+      d_tod_ = tod_own_.get();
+      h_signal_ = signals + k * n;
+    }
+  };
+  // per realisation: binned map and right-hand side (bin_tod, initialize_a)
+  for (long k = 0; k < nrhs; ++k) {
+    select_tod(k);
+    if (wamap_.n)
+      MADAM_CUDA(cudaMemcpyAsync(wamap_.get(), wamap0.get(), wamap_.n * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, st_));
+    bin_tod(true);
+    if (nv)
+      MADAM_CUDA(cudaMemcpyAsync(binb_.get() + k * nv, map_.get(), nv * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, st_));
+    if (par_.kfirst) {
+      std::vector<Segment> old = segs_;
+      initialize_a();
+      if (k == 0) {
+        build_segments();
+        bool same = old.size() == segs_.size();
+        for (size_t i = 0; same && i < old.size(); ++i)
+          same = old[i].k0 == segs_[i].k0 && old[i].noba == segs_[i].noba;
+        if (!same) fail("destripe_with_cache: flagging differs from the cached call");
+      }
+      if (nb)
+        MADAM_CUDA(cudaMemcpyAsync(yb_.get() + k * nb, yba_.get(), nb * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, st_));
+    }
+  }
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  timings.setup_ms = now_ms() - t0;
+  if (par_.kfirst) iterate_batch();
+  else {
+    noiter_b_.assign(nrhs, 0.0);
+    rrinit_b_.assign(nrhs, 0.0);
+    rrfinal_b_.assign(nrhs, 0.0);
+    aab_.alloc((size_t)nrhs * nb);
+    aab_.zero(st_);
+  }
+  // per realisation: destriped and binned maps (subtract_baselines_a,
+  // makemaps), optional TOD cleaning; no files
+  const double tf = now_ms();
+  suppress_fits_ = true;
+  try {
+    for (long k = 0; k < nrhs; ++k) {
+      select_tod(k);
+      tod_cleaned_ = false;
+      if (nb)
+        MADAM_CUDA(cudaMemcpyAsync(aa_.get(), aab_.get() + k * nb, nb * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, st_));
+      if (nv) {
+        MADAM_CUDA(cudaMemcpyAsync(map_.get(), binb_.get() + k * nv, nv * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, st_));
+        MADAM_CUDA(cudaMemcpyAsync(binmap_.get(), binb_.get() + k * nv, nv * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, st_));
+      }
+      finalize(false);
+      if (nv) {
+        MADAM_CUDA(cudaMemcpyAsync(mapb_.get() + k * nv, map_.get(), nv * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, st_));
+        MADAM_CUDA(cudaMemcpyAsync(binmapb_.get() + k * nv, binmap_.get(), nv * sizeof(double),
+                                   cudaMemcpyDeviceToDevice, st_));
+      }
+    }
+  } catch (...) {
+    suppress_fits_ = false;
+    throw;
+  }
+  suppress_fits_ = false;
+  // leave the cache as it was
+  if (wamap_.n)
+    MADAM_CUDA(cudaMemcpyAsync(wamap_.get(), wamap0.get(), wamap_.n * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  noiter = (long)*std::max_element(noiter_b_.begin(), noiter_b_.end());
+  timings.finalize_ms = now_ms() - tf;
+  timings.total_ms = now_ms() - t0;
+}

@@ -1382,6 +1382,9 @@ void Engine::construct_preconditioner() {
     }
     MADAM_CUDA(cudaStreamSynchronize(st_));
   }
+  band2_pseg_h_ = pseg;
+  band2_ch_h_ = chunks;
+  batch_tables_r_ = 0;
   band2_rows_ = nunique;
   band2_ntrans_ = (long)trans.size();
   band2_chunk_ = C;
@@ -1742,6 +1745,7 @@ void Engine::finalize(bool first_call) {
 }
 
 void Engine::write_fits(bool first_call) {
+  if (suppress_fits_) return;
   // write_map / write_binmap / write_mask / write_hits / write_matrix
   // (smadam.F90:401-422, 756-764)
   const bool any = par_.do_map || par_.do_binmap ||
@@ -1986,6 +1990,10 @@ long Engine::result_size(const std::string &name) {
   if (name == "scalars") return 20;
   if (name == "timings") return 9;
   if (name == "setup_marks") return kSetupMarks;
+  if (name == "map_batch" || name == "binmap_batch") return nrhs_ * npm * nmap_;
+  if (name == "aa_batch") return nrhs_ * nb;
+  if (name == "noiter_batch" || name == "rrinit_batch" || name == "rr_final_batch")
+    return (long)noiter_b_.size();
   return -1;
 }
 
@@ -2025,7 +2033,22 @@ void Engine::result_copy(const std::string &name, void *dst, long nbytes) {
     }
   };
   const long ncc = nmap_ == 3 ? 6 : 1;
-  if (name == "map" || name == "binmap") {
+  if (name == "map_batch" || name == "binmap_batch") {
+    need(sizeof(double));
+    const long long nv = (long long)nloc_ * nmap_;
+    const long long npm = 12LL * par_.nside_map * par_.nside_map * nmap_;
+    const double *src = name == "map_batch" ? mapb_.get() : binmapb_.get();
+    for (long k = 0; k < nrhs_; ++k)
+      expand(src + k * nv, sizeof(double), nmap_, nosubpix_map_, (double *)dst + k * npm);
+  } else if (name == "aa_batch") {
+    need(sizeof(double));
+    if (sz) MADAM_CUDA(cudaMemcpy(dst, aab_.get(), sz * sizeof(double), cudaMemcpyDeviceToHost));
+  } else if (name == "noiter_batch" || name == "rrinit_batch" || name == "rr_final_batch") {
+    need(sizeof(double));
+    const std::vector<double> &v = name == "noiter_batch" ? noiter_b_
+                                   : name == "rrinit_batch" ? rrinit_b_ : rrfinal_b_;
+    std::memcpy(dst, v.data(), v.size() * sizeof(double));
+  } else if (name == "map" || name == "binmap") {
     need(sizeof(double));
     expand(name == "map" ? map_.get() : binmap_.get(), sizeof(double), nmap_, nosubpix_map_, dst);
   } else if (name == "hits") {

@@ -165,6 +165,34 @@ def destripe_with_cache(comm, timestamps, pixels, pixweights, signal, outpath):
     _check(status)
 
 
+def destripe_with_cache_batch(comm, timestamps, pixels, pixweights, signals):
+    """
+    Batched Monte Carlo: solve every realisation in `signals` ([nrhs, ndet,
+    nsamp] or [nrhs, ndet * nsamp]) as destripe_with_cache would right after
+    the caching destripe(..., mcmode=True) call, in one multi-right-hand-side
+    solve over the shared pointing.  The cache is left unchanged.  Results:
+    get_result("map_batch"), "binmap_batch", "aa_batch", "noiter_batch", ...
+    (no counterpart in the reference, whose destripe_with_cache takes one
+    realisation per call).
+    """
+    if not available:
+        raise RuntimeError("No libmadam available, cannot destripe")
+    fcomm = _fcomm(comm)
+    ts = _Buf(timestamps, TIMESTAMP_TYPE)
+    px = _Buf(pixels, PIXEL_TYPE)
+    pw = _Buf(pixweights, WEIGHT_TYPE)
+    sg = _Buf(signals, SIGNAL_TYPE)
+    nsamp = ts.size
+    ndet = px.size // nsamp
+    nnz = pw.size // nsamp // ndet
+    nrhs = sg.size // (ndet * nsamp)
+    status = _madam.madam_b200_destripe_with_cache_batch(fcomm, ndet, nsamp, nnz, ts.ptr, px.ptr,
+                                                         pw.ptr, nrhs, sg.ptr)
+    _writeback(pixels, px)
+    _writeback(signals, sg)
+    _check(status)
+
+
 def clear_caches():
     """
     Clear Monte Carlo caches after a destripe() call with mcmode=True
@@ -176,7 +204,9 @@ _RESULT_DTYPES = dict(map=np.float64, binmap=np.float64, hits=np.int32, mask=np.
                       crit=np.float32, cc=np.float64, cca=np.float64, aa=np.float64,
                       yba=np.float64, nna=np.float64, fcov=np.float64, invcov=np.float64,
                       rr_history=np.float64, band_widths=np.int64, scalars=np.float64,
-                      timings=np.float64, setup_marks=np.float64)
+                      timings=np.float64, setup_marks=np.float64, map_batch=np.float64,
+                      binmap_batch=np.float64, aa_batch=np.float64, noiter_batch=np.float64,
+                      rrinit_batch=np.float64, rr_final_batch=np.float64)
 
 
 def get_result(name):

@@ -126,6 +126,7 @@ class ScanConfig:
     npsdbin: int = 1000
     seed: int = 1001
     temperature_only: bool = False
+    fknee_range: tuple = ()      # (lo, hi): per-detector fknee drawn uniformly
     extra_pars: dict = field(default_factory=dict)
 
     @property
@@ -149,6 +150,16 @@ def config2() -> ScanConfig:
         nside=512, nside_submap=16, ndet=16, nobs=4, nsamp_obs=1 << 23,
         fsample=100.0, fknee=0.05, alpha=-1.5, base_first=0.5, seed=1002,
         extra_pars=dict(cglimit=1e-12),
+    )
+
+
+def config4() -> ScanConfig:
+    """Batched Monte Carlo form: nside 512, 32 dets x 2^22 @ 100 Hz sharing
+    one pointing, fknee per detector uniform in 0.02-0.2 Hz, alpha -1."""
+    return ScanConfig(
+        nside=512, nside_submap=16, ndet=32, nobs=1, nsamp_obs=1 << 22,
+        fsample=100.0, fknee=0.1, fknee_range=(0.02, 0.2), alpha=-1.0, base_first=1.0,
+        seed=1004, extra_pars=dict(cglimit=1e-12),
     )
 
 
@@ -219,12 +230,35 @@ def _boresight(cfg: ScanConfig, t: torch.Tensor, open_deg: float, psi_det: float
     return theta, phi, psi
 
 
-def psd_model(cfg: ScanConfig, f: np.ndarray) -> np.ndarray:
+def det_fknee(cfg: ScanConfig) -> np.ndarray:
+    """Knee frequency of every detector: cfg.fknee, or seeded draws from
+    cfg.fknee_range."""
+    if not cfg.fknee_range:
+        return np.full(cfg.ndet, cfg.fknee)
+    rng = np.random.default_rng(cfg.seed + 4242)
+    return rng.uniform(cfg.fknee_range[0], cfg.fknee_range[1], cfg.ndet)
+
+
+def psd_model(cfg: ScanConfig, f: np.ndarray, fknee=None) -> np.ndarray:
     """Noise PSD sigma^2/fs (1 + (f/fknee)^alpha) at frequencies f > 0."""
-    return cfg.sigma ** 2 / cfg.fsample * (1.0 + (f / cfg.fknee) ** cfg.alpha)
+    fk = cfg.fknee if fknee is None else fknee
+    return cfg.sigma ** 2 / cfg.fsample * (1.0 + (f / fk) ** cfg.alpha)
 
 
-def _noise(cfg: ScanConfig, nsamp: int, gen: torch.Generator, device) -> torch.Tensor:
+def noise_realisations(cfg: ScanConfig, nreal: int, device="cuda", seed0=0):
+    """nreal noise-only TODs [nreal, ndet, nsamp] (float64): white + 1/f with
+    each detector's knee frequency, seeded per (realisation, detector)."""
+    fk = det_fknee(cfg)
+    out = torch.empty((nreal, cfg.ndet, cfg.nsamp), dtype=torch.float64, device=device)
+    for r in range(nreal):
+        for d in range(cfg.ndet):
+            g = _generator(cfg.seed * 7 + 100003 * (seed0 + r) + d, torch.device(device))
+            out[r, d] = _noise(cfg, cfg.nsamp, g, device, fknee=fk[d])
+    return out
+
+
+def _noise(cfg: ScanConfig, nsamp: int, gen: torch.Generator, device,
+           fknee=None) -> torch.Tensor:
     """White + 1/f noise realisation of length nsamp (float64)."""
     n = 1
     while n < nsamp:
@@ -233,7 +267,7 @@ def _noise(cfg: ScanConfig, nsamp: int, gen: torch.Generator, device) -> torch.T
     spec = torch.fft.rfft(white)
     f = torch.fft.rfftfreq(n, d=1.0 / cfg.fsample, device=device).to(torch.float64)
     f[0] = f[1]
-    shape = torch.sqrt(1.0 + (f / cfg.fknee) ** cfg.alpha)
+    shape = torch.sqrt(1.0 + (f / (cfg.fknee if fknee is None else fknee)) ** cfg.alpha)
     shape[0] = 0.0
     out = torch.fft.irfft(spec * shape, n=n)[:nsamp]
     return out * cfg.sigma
@@ -286,11 +320,11 @@ def generate(cfg: ScanConfig, device="cpu", nnz=None, with_signal=True):
             del theta, phi, psi, pix
         if with_signal:
             gn = _generator(cfg.seed * 1000 + d, device)
-            signal[d] += _noise(cfg, nsamp, gn, device)
+            signal[d] += _noise(cfg, nsamp, gn, device, fknee=det_fknee(cfg)[d])
     periods = np.arange(cfg.nobs, dtype=np.int64) * cfg.nsamp_obs
     npsd = np.ones(cfg.ndet, dtype=np.int64)
     psdfreqs = np.logspace(-5, math.log10(cfg.fsample / 2), cfg.npsdbin)
-    psdvals = np.tile(psd_model(cfg, psdfreqs), cfg.ndet)
+    psdvals = np.concatenate([psd_model(cfg, psdfreqs, fk) for fk in det_fknee(cfg)])
     psdstarts = np.zeros(cfg.ndet, dtype=np.float64)
     detweights = np.full(cfg.ndet, 1.0 / cfg.sigma ** 2)
     dets = ["det{:03d}".format(d) for d in range(cfg.ndet)]

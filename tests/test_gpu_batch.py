@@ -1,0 +1,117 @@
+"""Batched Monte Carlo solve against one-at-a-time destripe_with_cache calls.
+
+madam_b200_destripe_with_cache_batch solves R noise realisations that share
+one pointing as a single multi-right-hand-side PCG.  Each realisation must
+come out as destripe_with_cache gives it when called right after the caching
+destripe(mcmode=True): same PCG iteration count, destriped and binned maps
+and baselines within BATCH_RTOL of their largest magnitude (the batched
+kernels repeat the single-solve arithmetic, so the difference is expected
+to be zero or a few ulp).
+"""
+import numpy as np
+import pytest
+
+from libmadam_b200 import synthetic as syn
+
+pytestmark = pytest.mark.gpu
+
+BATCH_RTOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def W():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from libmadam_b200 import libmadam_wrapper
+    assert libmadam_wrapper.available
+    return libmadam_wrapper
+
+
+def _close(a, b, rtol):
+    a = np.asarray(a, float)
+    b = np.asarray(b, float)
+    scale = np.abs(b).max() if b.size else 0.0
+    assert np.abs(a - b).max() <= rtol * max(scale, 1e-300)
+
+
+def _realisations(d, nrhs):
+    """Signal plus independent white and 1/f-like noise per realisation."""
+    out = []
+    for r in range(nrhs):
+        rng = np.random.default_rng(1000 + r)
+        noise = rng.standard_normal(d["signal"].shape) * 1e-3
+        drift = np.cumsum(rng.standard_normal(d["signal"].shape) * 1e-5, axis=-1)
+        out.append(d["signal"] + noise + drift)
+    return out
+
+
+def _cache(W, d, pars):
+    W.destripe(None, pars, d["dets"], d["detweights"], d["timestamps"], d["pixels"].copy(),
+               d["pixweights"], d["signal"].copy(), d["periods"], d["npsd"], d["psdstarts"],
+               d["psdfreqs"], d["psdvals"])
+
+
+def _sequential(W, d, pars, sigs):
+    res = []
+    for s in sigs:
+        W.clear_caches()
+        _cache(W, d, pars)
+        W.destripe_with_cache(None, d["timestamps"], d["pixels"].copy(), d["pixweights"],
+                              s.copy(), b"")
+        res.append({k: W.get_result(k) for k in ("map", "binmap", "aa")}
+                   | {"noiter": W.scalars()["noiter"]})
+    return res
+
+
+@pytest.mark.parametrize("extra", [dict(), dict(temperature_only=True),
+                                   dict(precond_width_min=3, precond_width_max=30)])
+def test_batch_matches_one_at_a_time(W, extra):
+    cfg = syn.small_config(seed=41)
+    d = syn.to_numpy(syn.generate(cfg, nnz=1 if extra.get("temperature_only") else None))
+    pars = dict(d["pars"], mcmode=True, **extra)
+    nrhs = 5
+    sigs = _realisations(d, nrhs)
+    ref = _sequential(W, d, pars, sigs)
+    W.clear_caches()
+    _cache(W, d, pars)
+    W.destripe_with_cache_batch(None, d["timestamps"], d["pixels"].copy(), d["pixweights"],
+                                np.stack(sigs))
+    nmap = 1 if extra.get("temperature_only") else 3
+    maps = W.get_result("map_batch").reshape(nrhs, -1, nmap)
+    bins = W.get_result("binmap_batch").reshape(nrhs, -1, nmap)
+    aas = W.get_result("aa_batch").reshape(nrhs, -1)
+    its = W.get_result("noiter_batch")
+    for r in range(nrhs):
+        assert its[r] == ref[r]["noiter"]
+        for c in range(nmap):
+            _close(maps[r][:, c], ref[r]["map"].reshape(-1, nmap)[:, c], BATCH_RTOL)
+            _close(bins[r][:, c], ref[r]["binmap"].reshape(-1, nmap)[:, c], BATCH_RTOL)
+        _close(aas[r], ref[r]["aa"], BATCH_RTOL)
+    # the cache is left as it was: a following single call gives the sequential answer
+    W.destripe_with_cache(None, d["timestamps"], d["pixels"].copy(), d["pixweights"],
+                          sigs[2].copy(), b"")
+    _close(W.get_result("map").reshape(-1, nmap)[:, 0], ref[2]["map"].reshape(-1, nmap)[:, 0],
+           BATCH_RTOL)
+    W.clear_caches()
+
+
+def test_batch_device_buffers(W):
+    import torch
+    cfg = syn.small_config(seed=43)
+    d = syn.to_numpy(syn.generate(cfg))
+    pars = dict(d["pars"], mcmode=True)
+    sigs = _realisations(d, 3)
+    W.clear_caches()
+    _cache(W, d, pars)
+    W.destripe_with_cache_batch(None, d["timestamps"], d["pixels"].copy(), d["pixweights"],
+                                np.stack(sigs))
+    mh = W.get_result("map_batch")
+    W.clear_caches()
+    _cache(W, d, pars)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    W.destripe_with_cache_batch(None, dev(d["timestamps"]), dev(d["pixels"]),
+                                dev(d["pixweights"]), dev(np.stack(sigs)))
+    torch.cuda.synchronize()
+    _close(W.get_result("map_batch"), mh, BATCH_RTOL)
+    W.clear_caches()
