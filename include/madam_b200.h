@@ -41,6 +41,41 @@ int madam_b200_destripe_with_cache_batch(int comm, long ndet, long nsamp, long n
                                          void *timestamps, void *pix, void *pixweights,
                                          long nrhs, void *signals);
 
+/* Serving: a job queue over one GPU.  No reference counterpart (the
+ * reference runs one destripe per call and per MPI job).
+ *
+ * serve_open starts nworkers worker threads, each with its own engine and
+ * CUDA stream, and a device-memory budget of mem_fraction of the free memory;
+ * NULL on error (message in err).  serve_submit queues one destripe() job
+ * with the reference's destripe arguments (src/smadam.F90:64-101; mcmode is
+ * refused) and returns its id, or -1 (message in err).  The caller's buffers
+ * must stay valid until the job is done.  Jobs start first come, first
+ * served, when their estimated footprint fits the budget beside the running
+ * jobs, and overlap on the device; their products do not depend on what else
+ * runs (beyond rounding).  serve_wait waits up to timeout_s seconds (< 0: no limit) and
+ * returns the job state: 0 queued, 1 running, 2 done, 3 failed, -1 unknown.
+ * serve_result_size / serve_result_copy give a done job's "map", "binmap"
+ * (float64 [npix][nmap]), "hits", "mask" (int32 [npix]), "aa" (float64
+ * [ndet][noba]), "scalars" (float64 [20]), "rr_history" (float64);
+ * serve_job_info gives out[0..5] = submit, start and end time (s), samples,
+ * PCG iterations, admitted bytes; serve_error the message of a failed job;
+ * serve_release frees a finished job; serve_close waits for the running
+ * jobs, drops the queued ones and frees the server. */
+void *madam_b200_serve_open(int nworkers, double mem_fraction, char *err, long errlen);
+long madam_b200_serve_submit(void *srv, char *parstring, long ndet, char *detstring,
+                             double *detweights, long nsamp, long nnz, void *timestamps, void *pix,
+                             void *pixweights, void *signal, long nperiod, long *periods,
+                             long *npsd, long npsdtot, double *psdstarts, long npsdbin,
+                             double *psdfreqs, long npsdval, double *psdvals, char *err,
+                             long errlen);
+int madam_b200_serve_wait(void *srv, long job, double timeout_s);
+long madam_b200_serve_result_size(void *srv, long job, const char *name);
+int madam_b200_serve_result_copy(void *srv, long job, const char *name, void *dst, long nbytes);
+int madam_b200_serve_job_info(void *srv, long job, double *out, long nout);
+int madam_b200_serve_error(void *srv, long job, char *buf, long buflen);
+int madam_b200_serve_release(void *srv, long job);
+int madam_b200_serve_close(void *srv);
+
 /* Status of the last call (0 = success) and its error message; replaces the
  * reference's abort_mpi messages (src/mpi_wrappers.f90:120-137). */
 int madam_b200_last_error(char *buf, long buflen);

@@ -179,7 +179,7 @@ int madam_b200_bench_iterations(int warmup, int iters, double *out, long nout) {
   });
 }
 
-unsigned long long madam_b200_kernel_launches(void) { return madam::g_kernel_launches; }
+unsigned long long madam_b200_kernel_launches(void) { return madam::g_kernel_launches.load(); }
 
 // Host-side check of the invariant-divisor division used by the kernels.
 int madam_b200_selftest_fastdiv(void) {

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <cstdint>
 #include <string>
 
@@ -20,7 +22,7 @@ namespace madam {
 
 // Every kernel launch of the library goes through this macro so the number
 // of launches inside a timed region can be reported.
-extern unsigned long long g_kernel_launches;
+extern std::atomic<unsigned long long> g_kernel_launches;
 #define MADAM_LAUNCH(kernel, grid, block, smem, stream, ...)                  \
   do {                                                                        \
     kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);               \

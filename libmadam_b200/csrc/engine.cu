@@ -31,7 +31,7 @@
 
 namespace madam {
 
-unsigned long long g_kernel_launches = 0;
+std::atomic<unsigned long long> g_kernel_launches{0};
 
 namespace {
 

@@ -25,11 +25,12 @@ constexpr int kRedBlocks = 1184;      // 148 SMs x 8, fixed for determinism
 
 
 // Owning device allocation.
-// Device memory of the engine: stream-ordered allocations on the engine's
-// stream, served by the device's default memory pool, which keeps freed
+// Device memory of the engine: stream-ordered allocations on the stream of
+// the engine the calling thread is working for (several engines may run in
+// parallel host threads), served by the device's default memory pool, which keeps freed
 // blocks for reuse (one destripe call allocates and frees several GB of
 // temporaries; the pool turns the repeats into bookkeeping).
-extern cudaStream_t g_alloc_stream;
+extern thread_local cudaStream_t g_alloc_stream;
 void *dev_alloc(size_t bytes);
 void dev_free(void *p);
 

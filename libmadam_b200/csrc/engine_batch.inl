@@ -67,8 +67,8 @@ void Engine::build_batch_tables() {
     MADAM_CUDA(cudaMemcpyAsync(p2tb_b_.get(), tb.data(), tb.size() * sizeof(int),
                                cudaMemcpyHostToDevice, st_));
   }
-  // the filter (or fprecond) segments
-  const std::vector<ConvSeg> &fs = par_.use_fprecond ? filt_segs_ : filt_segs_;
+  // the filter segments (also those of the fprecond preconditioner)
+  const std::vector<ConvSeg> &fs = filt_segs_;
   std::vector<ConvSeg> cs;
   for (long r = 0; r < nrhs_; ++r)
     for (ConvSeg c : fs) {
@@ -313,6 +313,7 @@ void Engine::iterate_batch() {
 
 void Engine::run_cached_batch(long ndet, long nsamp, long nnz, double *timestamps, int32_t *pix,
                               float *pixweights, long nrhs, double *signals, bool is_device) {
+  g_alloc_stream = st_;
   if (!cached_) fail("destripe_with_cache called with empty caches.");
   if (nrhs < 1) fail("nrhs must be at least 1");
   if (par_.temperature_only && nnz != 1)

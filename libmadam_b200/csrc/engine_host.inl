@@ -11,7 +11,7 @@ struct CgpWork {
   long nseg = 0;
 };
 
-cudaStream_t g_alloc_stream = nullptr;
+thread_local cudaStream_t g_alloc_stream = nullptr;
 
 void *dev_alloc(size_t bytes) {
   void *p = nullptr;
@@ -1838,6 +1838,7 @@ void Engine::writeback_host() {
 void Engine::run(const Params &par, std::vector<Detector> dets, long ndet, long nsamp, long nnz,
                  double *timestamps, int32_t *pix, float *pixweights, double *signal,
                  long nperiod, const long *periods, bool is_device) {
+  g_alloc_stream = st_;
   const double t0 = now_ms();
   timings = Timings();
   rr_history.clear();
@@ -1933,6 +1934,7 @@ void Engine::run(const Params &par, std::vector<Detector> dets, long ndet, long 
 
 void Engine::run_cached(long ndet, long nsamp, long nnz, double *timestamps, int32_t *pix,
                         float *pixweights, double *signal, bool is_device) {
+  g_alloc_stream = st_;
   // destripe_with_cache (smadam.F90:593-918)
   if (!cached_) fail("destripe_with_cache called with empty caches.");
   if (par_.temperature_only && nnz != 1)
@@ -1998,6 +2000,7 @@ long Engine::result_size(const std::string &name) {
 }
 
 void Engine::result_copy(const std::string &name, void *dst, long nbytes) {
+  g_alloc_stream = st_;
   const long sz = result_size(name);
   if (sz < 0) fail("unknown result: " + name);
   auto need = [&](size_t elem) {
@@ -2109,6 +2112,7 @@ void Engine::result_copy(const std::string &name, void *dst, long nbytes) {
 // solution of the last solve is kept.  out: [total_ms, ms_per_iter,
 // launches_per_iter, scatter_ms, filter_ms, gather_ms, precond_ms, update_ms]
 void Engine::bench_iterations(int warmup, int iters, std::vector<double> &out) {
+  g_alloc_stream = st_;
   if (!par_.kfirst || noba_short_ == 0) fail("no solve state to benchmark");
   const long long nb = (long long)ndet_ * noba_short_;
   DevBuf<double> aa_keep;

@@ -5,8 +5,8 @@ one pointing as a single multi-right-hand-side PCG.  Each realisation must
 come out as destripe_with_cache gives it when called right after the caching
 destripe(mcmode=True): same PCG iteration count, destriped and binned maps
 and baselines within BATCH_RTOL of their largest magnitude (the batched
-kernels repeat the single-solve arithmetic, so the difference is expected
-to be zero or a few ulp).
+kernels repeat the single-solve arithmetic; the setup's binning scatter sums
+with FP64 atomics, so separate runs agree to rounding, not to the bit).
 """
 import numpy as np
 import pytest
@@ -15,7 +15,7 @@ from libmadam_b200 import synthetic as syn
 
 pytestmark = pytest.mark.gpu
 
-BATCH_RTOL = 1e-12
+BATCH_RTOL = 1e-9
 
 
 @pytest.fixture(scope="module")

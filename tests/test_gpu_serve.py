@@ -1,0 +1,96 @@
+"""Serving: jobs of uneven sizes in flight together give the products each
+gives alone (same hits and PCG iteration count; maps and baselines within
+SERVE_RTOL of their largest magnitude: the setup's pixel-matrix and binning
+scatter sums with FP64 atomics, so two runs of one job agree to rounding,
+~1e-11 after the PCG, not to the bit), a failing job does not disturb the
+others, and device buffers are served like host buffers."""
+import numpy as np
+import pytest
+
+from libmadam_b200 import synthetic as syn
+
+pytestmark = pytest.mark.gpu
+
+SERVE_RTOL = 1e-9
+
+
+@pytest.fixture(scope="module")
+def W():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from libmadam_b200 import libmadam_wrapper
+    return libmadam_wrapper
+
+
+def _close(a, b, rtol):
+    a = np.asarray(a, float)
+    b = np.asarray(b, float)
+    scale = np.abs(b).max() if b.size else 0.0
+    assert np.abs(a - b).max() <= rtol * max(scale, 1e-300)
+
+
+def _jobs():
+    specs = [dict(nside=16, ndet=4, nsamp_obs=1 << 14, nobs=2, seed=51),
+             dict(nside=32, ndet=2, nsamp_obs=1 << 15, nobs=1, seed=52, base_first=0.5),
+             dict(nside=16, ndet=8, nsamp_obs=1 << 13, nobs=3, seed=53, base_first=2.0),
+             dict(nside=64, ndet=4, nsamp_obs=1 << 15, nobs=1, seed=54),
+             dict(nside=16, ndet=4, nsamp_obs=1 << 14, nobs=1, seed=55, temperature_only=True),
+             dict(nside=32, ndet=4, nsamp_obs=1 << 14, nobs=2, seed=56)]
+    out = []
+    for sp in specs:
+        cfg = syn.small_config(**sp)
+        out.append(syn.to_numpy(syn.generate(cfg, nnz=1 if sp.get("temperature_only") else None)))
+    return out
+
+
+def _args(d):
+    return (d["pars"], d["dets"], d["detweights"], d["timestamps"], d["pixels"].copy(),
+            d["pixweights"], d["signal"].copy(), d["periods"], d["npsd"], d["psdstarts"],
+            d["psdfreqs"], d["psdvals"])
+
+
+def test_jobs_in_flight_match_jobs_alone(W):
+    from libmadam_b200.serve import Server
+    jobs = _jobs()
+    alone = []
+    for d in jobs:
+        W.destripe(None, *_args(d))
+        alone.append(dict(map=W.get_result("map"), aa=W.get_result("aa"),
+                          hits=W.get_result("hits"), noiter=W.scalars()["noiter"]))
+    srv = Server(workers=3, mem_fraction=0.5)
+    tickets = [srv.submit(*_args(d)) for d in jobs]
+    bad = dict(jobs[0])
+    bad_pix = bad["pixels"].copy()
+    bad_pix.reshape(-1)[3] = 10 ** 8
+    tb = srv.submit(bad["pars"], bad["dets"], bad["detweights"], bad["timestamps"], bad_pix,
+                    bad["pixweights"], bad["signal"].copy(), bad["periods"], bad["npsd"],
+                    bad["psdstarts"], bad["psdfreqs"], bad["psdvals"])
+    for t, ref in zip(tickets, alone):
+        assert srv.wait(t) == 2
+        np.testing.assert_array_equal(srv.result(t, "hits"), ref["hits"])
+        _close(srv.result(t, "map"), ref["map"], SERVE_RTOL)
+        _close(srv.result(t, "aa"), ref["aa"], SERVE_RTOL)
+        assert srv.result(t, "scalars")[0] == ref["noiter"]
+        info = srv.info(t)
+        assert info["t_end"] >= info["t_start"] >= info["t_submit"]
+        srv.release(t)
+    with pytest.raises(RuntimeError, match="Too large pixel number"):
+        srv.wait(tb)
+    srv.close()
+
+
+def test_device_buffers_are_served(W):
+    import torch
+    from libmadam_b200.serve import Server
+    d = _jobs()[3]
+    W.destripe(None, *_args(d))
+    ref = W.get_result("map")
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    srv = Server(workers=2)
+    t = srv.submit(d["pars"], d["dets"], d["detweights"], dev(d["timestamps"]),
+                   dev(d["pixels"]), dev(d["pixweights"]), dev(d["signal"]), d["periods"],
+                   d["npsd"], d["psdstarts"], d["psdfreqs"], d["psdvals"])
+    assert srv.wait(t) == 2
+    _close(srv.result(t, "map"), ref, SERVE_RTOL)
+    srv.close()
