@@ -264,13 +264,84 @@ def run_mc(args, world, rank, local):
     return 0
 
 
+def run_serve(args, world, rank, local):
+    """Serving stream: requests of uneven size (nside 128-1024, 2-32 detectors,
+    2^18-2^22 samples per detector, base_first 0.25-2 s, cglimit 1e-10) arrive
+    as a Poisson process and are served by libmadam_b200.serve; reports p50 /
+    p99 latency (submit to done) and aggregate throughput."""
+    import torch
+    from libmadam_b200 import synthetic as syn
+    from libmadam_b200.serve import Server
+    rng = np.random.default_rng(5005 + rank)
+    reqs = []
+    for i in range(args.requests):
+        cfg = syn.ScanConfig(
+            nside=int(rng.choice([128, 256, 512, 1024])), nside_submap=16,
+            ndet=int(rng.integers(2, 33)), nobs=1,
+            nsamp_obs=int(2 ** rng.uniform(18, 22)), fsample=100.0,
+            fknee=float(rng.uniform(0.02, 0.2)), alpha=-1.0,
+            base_first=float(rng.choice([0.25, 0.5, 1.0, 2.0])), seed=7000 + i,
+            extra_pars=dict(cglimit=1e-10))
+        d = syn.generate(cfg, device="cuda")
+        d["pixels"] = d["pixels"].reshape(-1)
+        d["pixweights"] = d["pixweights"].reshape(-1)
+        d["signal"] = d["signal"].reshape(-1)
+        reqs.append(d)
+    torch.cuda.synchronize()
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, args.requests))
+    srv = Server(workers=args.workers, mem_fraction=0.8)
+    clk = Clocks(local)
+    t0 = time.perf_counter()
+    tickets = []
+    for d, ta in zip(reqs, arrivals):
+        dt = ta - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        tickets.append(srv.submit(d["pars"], d["dets"], d["detweights"], d["timestamps"],
+                                  d["pixels"], d["pixweights"], d["signal"], d["periods"],
+                                  d["npsd"], d["psdstarts"], d["psdfreqs"], d["psdvals"]))
+    infos = []
+    for t in tickets:
+        srv.wait(t)
+        infos.append(srv.info(t))
+    makespan = max(i["t_end"] for i in infos) - min(i["t_submit"] for i in infos)
+    clocks = clk.stop()
+    srv.close()
+    lat = np.array([i["t_end"] - i["t_submit"] for i in infos])
+    samples = np.array([i["samples"] for i in infos])
+    iters = np.array([i["iterations"] for i in infos])
+    line = {"metric": "serving latency p50 / p99 and TOD samples/s",
+            "value": float(np.percentile(lat, 50) * 1e3), "unit": "ms (p50 latency)",
+            "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "p50_ms": float(np.percentile(lat, 50) * 1e3),
+            "n_gpus": 1, "higher_is_better": False, "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "serving stream: %d requests, Poisson %.1f req/s, nside "
+                                   "128-1024, 2-32 detectors, 2^18-2^22 samples per detector, "
+                                   "base_first 0.25-2 s, cglimit 1e-10" % (args.requests,
+                                                                          args.rate),
+                       "workers": args.workers},
+            "clocks": clocks,
+            "makespan_s": makespan,
+            "samples_per_s": float(samples.sum() / makespan),
+            "samples_per_s_per_pcg_iteration": float((samples * iters).sum() / makespan),
+            "mean_iterations": float(iters.mean()),
+            "total_samples": float(samples.sum())}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="2", choices=["2", "1", "prof", "mid", "small", "mc"])
+    ap.add_argument("--config", default="2", choices=["2", "1", "prof", "mid", "small", "mc", "serve"])
+    ap.add_argument("--requests", type=int, default=60)
+    ap.add_argument("--rate", type=float, default=20.0)
+    ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--nrhs", type=int, default=64)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -292,6 +363,8 @@ def main():
     torch.cuda.set_device(local)
     if args.config == "mc":
         return run_mc(args, world, rank, local)
+    if args.config == "serve":
+        return run_serve(args, world, rank, local)
     cfg, wname = config_for(args.config)
     cfg.seed += 1000 * rank
     t0 = time.time()
