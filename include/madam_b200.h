@@ -21,6 +21,21 @@ int madam_b200_destripe(int comm, char *parstring, long ndet, char *detstring,
                         long npsdtot, double *psdstarts, long npsdbin, double *psdfreqs,
                         long npsdval, double *psdvals);
 
+/* FP32-TOD precision form of destripe() (reference src/smadam.F90:64-590,
+ * which takes float64 signals only): the same arguments with `signal` as
+ * float32 [ndet][nsamp] (host or device memory, like pix).  The PCG
+ * projections read float32 pointing (consecutive samples of one baseline in
+ * one pixel summed into pairs) and a float32 copy of the map; pixel
+ * matrices, binning, baselines and all PCG inner products stay float64.
+ * Maps and baselines agree with destripe() on the same samples to about
+ * 1e-6 relative (tested at 1e-4).  A cleaned TOD (write_tod) goes back into
+ * `signal` as float32.  No reference counterpart. */
+int madam_b200_destripe_fp32(int comm, char *parstring, long ndet, char *detstring,
+                             double *detweights, long nsamp, long nnz, void *timestamps, void *pix,
+                             void *pixweights, float *signal, long nperiod, long *periods,
+                             long *npsd, long npsdtot, double *psdstarts, long npsdbin,
+                             double *psdfreqs, long npsdval, double *psdvals);
+
 /* destripe_with_cache() with a status (reference src/smadam.F90:593-918). */
 int madam_b200_destripe_with_cache(int comm, long ndet, long nsamp, long nnz, void *timestamps,
                                    void *pix, void *pixweights, void *signal, char *outpath);
@@ -56,7 +71,7 @@ int madam_b200_destripe_with_cache_batch(int comm, long ndet, long nsamp, long n
  * returns the job state: 0 queued, 1 running, 2 done, 3 failed, -1 unknown.
  * serve_result_size / serve_result_copy give a done job's "map", "binmap"
  * (float64 [npix][nmap]), "hits", "mask" (int32 [npix]), "aa" (float64
- * [ndet][noba]), "scalars" (float64 [20]), "rr_history" (float64);
+ * [ndet][noba]), "scalars" (float64 [22]), "rr_history" (float64);
  * serve_job_info gives out[0..5] = submit, start and end time (s), samples,
  * PCG iterations, admitted bytes; serve_error the message of a failed job;
  * serve_release frees a finished job; serve_close waits for the running
@@ -87,7 +102,7 @@ int madam_b200_last_error(char *buf, long buflen);
  * matrices at nside_map / nside_cross), "aa", "yba", "nna" (float64
  * [ndet][noba]: baselines, RHS, F^T N^-1 F), "fcov" (float64
  * [npsdtot][nof/2+1]), "invcov" (float64 [npsdtot][nof]), "rr_history"
- * (float64 [niter]), "band_widths" (int64), "scalars" (float64 [16]),
+ * (float64 [niter]), "band_widths" (int64), "scalars" (float64 [22]),
  * "timings" (float64 [9], milliseconds).  result_size returns elements or
  * -1; result_copy fails when nbytes is too small. */
 long madam_b200_result_size(const char *name);

@@ -39,6 +39,8 @@ def load():
     L.madam_b200_destripe.argtypes = [ct.c_int, ct.c_char_p, ct.c_long, ct.c_char_p, P, ct.c_long,
                                       ct.c_long, P, P, P, P, ct.c_long, P, P, ct.c_long, P,
                                       ct.c_long, P, ct.c_long, P]
+    L.madam_b200_destripe_fp32.restype = ct.c_int
+    L.madam_b200_destripe_fp32.argtypes = L.madam_b200_destripe.argtypes
     L.madam_b200_destripe_with_cache.restype = ct.c_int
     L.madam_b200_destripe_with_cache.argtypes = [ct.c_int, ct.c_long, ct.c_long, ct.c_long, P, P,
                                                  P, P, ct.c_char_p]

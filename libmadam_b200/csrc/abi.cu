@@ -65,11 +65,37 @@ void report(const char *who) {
 
 extern "C" {
 
+static int destripe_impl(bool fp32, int comm, char *parstring, long ndet, char *detstring,
+                         double *detweights, long nsamp, long nnz, void *timestamps, void *pix,
+                         void *pixweights, void *signal, long nperiod, long *periods, long *npsd,
+                         long npsdtot, double *psdstarts, long npsdbin, double *psdfreqs,
+                         long npsdval, double *psdvals);
+
 int madam_b200_destripe(int comm, char *parstring, long ndet, char *detstring,
                         double *detweights, long nsamp, long nnz, void *timestamps, void *pix,
                         void *pixweights, void *signal, long nperiod, long *periods, long *npsd,
                         long npsdtot, double *psdstarts, long npsdbin, double *psdfreqs,
                         long npsdval, double *psdvals) {
+  return destripe_impl(false, comm, parstring, ndet, detstring, detweights, nsamp, nnz,
+                       timestamps, pix, pixweights, signal, nperiod, periods, npsd, npsdtot,
+                       psdstarts, npsdbin, psdfreqs, npsdval, psdvals);
+}
+
+int madam_b200_destripe_fp32(int comm, char *parstring, long ndet, char *detstring,
+                             double *detweights, long nsamp, long nnz, void *timestamps, void *pix,
+                             void *pixweights, float *signal, long nperiod, long *periods,
+                             long *npsd, long npsdtot, double *psdstarts, long npsdbin,
+                             double *psdfreqs, long npsdval, double *psdvals) {
+  return destripe_impl(true, comm, parstring, ndet, detstring, detweights, nsamp, nnz,
+                       timestamps, pix, pixweights, signal, nperiod, periods, npsd, npsdtot,
+                       psdstarts, npsdbin, psdfreqs, npsdval, psdvals);
+}
+
+static int destripe_impl(bool fp32, int comm, char *parstring, long ndet, char *detstring,
+                         double *detweights, long nsamp, long nnz, void *timestamps, void *pix,
+                         void *pixweights, void *signal, long nperiod, long *periods, long *npsd,
+                         long npsdtot, double *psdstarts, long npsdbin, double *psdfreqs,
+                         long npsdval, double *psdvals) {
   (void)comm;  // single rank: the communicator handle is accepted and ignored
   std::lock_guard<std::mutex> lock(g_mutex);
   return guarded([&] {
@@ -84,6 +110,9 @@ int madam_b200_destripe(int comm, char *parstring, long ndet, char *detstring,
     auto dets = madam::read_detectors(par, detstring, ndet, detweights, npsd, npsdtot, psdstarts,
                                       npsdbin, psdfreqs, npsdval, psdvals);
     const bool dev = is_device_pointer(pix);
+    if (fp32 && dev != is_device_pointer(signal))
+      madam::fail("destripe_fp32: pixels and signal must both be host or both device memory");
+    engine().set_fp32(fp32);
     engine().run(par, std::move(dets), ndet, nsamp, nnz, (double *)timestamps, (int32_t *)pix,
                  (float *)pixweights, (double *)signal, nperiod, periods, dev);
   });

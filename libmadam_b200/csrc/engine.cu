@@ -442,6 +442,36 @@ __global__ void k_ccmult(const double *cc, double *m, long long n) {
   }
 }
 
+// ccmultiply of the PCG (iterate_a, smadam_routines.f90:809-812) that also
+// writes the copy of the map the gather reads: FP64 padded to 32 bytes a
+// pixel ({I, Q}, {U, 0}: one aligned sector per lookup) or, in the FP32-TOD
+// form, float32 {I, Q, U, 0} (one 16-byte load)
+template <bool F32>
+__global__ void k_ccmult_copy(const double *cc, double *m, long long n, double2 *mg,
+                              float4 *mf) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x) {
+    const double *c = cc + p * 6;
+    double *v = m + p * 3;
+    double tm = 0, qm = 0, um = 0;
+    if (c[0] != 0) {
+      const double a = v[0], b = v[1], d = v[2];
+      tm = c[0] * a + c[1] * b + c[2] * d;
+      qm = c[1] * a + c[3] * b + c[4] * d;
+      um = c[2] * a + c[4] * b + c[5] * d;
+    }
+    v[0] = tm;
+    v[1] = qm;
+    v[2] = um;
+    if (F32) {
+      mf[p] = make_float4((float)tm, (float)qm, (float)um, 0.f);
+    } else {
+      mg[2 * p] = make_double2(tm, qm);
+      mg[2 * p + 1] = make_double2(um, 0.0);
+    }
+  }
+}
+
 // initialize_a (smadam_routines.f90:508-653): one warp per baseline
 template <int NMAP>
 __global__ void k_init_a(const float4 *p4, const int32_t *pc, const double *tod,
@@ -658,6 +688,17 @@ __global__ void __launch_bounds__(256) k_gather_tiled(
   if (threadIdx.x == 0) part[blockIdx.x] = v[0];
 }
 
+__device__ __forceinline__ double map_dot(const double2 *__restrict__ mg, long long cp,
+                                          const float4 &q) {
+  const double2 a = __ldg(mg + 2 * cp), b = __ldg(mg + 2 * cp + 1);
+  return (double)q.x * a.x + (double)q.y * a.y + (double)q.z * b.x;
+}
+__device__ __forceinline__ double map_dot(const float4 *__restrict__ mf, long long cp,
+                                          const float4 &q) {
+  const float4 a = __ldg(mf + cp);
+  return (double)q.x * a.x + (double)q.y * a.y + (double)q.z * a.z;
+}
+
 // map_to_baseline, warp chunks: a warp takes a chunk of consecutive
 // baselines of one detector (at most kGatherChunk samples, at most 32
 // baselines), loads all of its samples (8 per lane, coalesced) with their map
@@ -667,13 +708,16 @@ __global__ void __launch_bounds__(256) k_gather_tiled(
 // at most kGatherChunk samples long.
 constexpr int kGatherChunk = 256;
 
-template <int NMAP>
+// MAPT (NMAP = 3): the map copy it reads, double2 (padded FP64, two 16-byte
+// loads in one sector) or float4 (FP32-TOD form, one load).
+template <int NMAP, class MAPT>
 __global__ void __launch_bounds__(256) k_gather_chunks(
     const int2 *__restrict__ chunks, long long nchunks, const float4 *__restrict__ p4,
     const int32_t *__restrict__ pc, const uint32_t *__restrict__ bstart, long noba,
     long long nsamp, const double *__restrict__ bw, const double *__restrict__ p,
-    const double *__restrict__ nna, const double *__restrict__ m, int deg_shift, int nloc,
-    const uint8_t *__restrict__ rmask, double *__restrict__ ap, double *__restrict__ part) {
+    const double *__restrict__ nna, const double *__restrict__ m, const MAPT *__restrict__ mx,
+    int deg_shift, int nloc, const uint8_t *__restrict__ rmask, double *__restrict__ ap,
+    double *__restrict__ part) {
   __shared__ double vbuf[8][kGatherChunk];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   double *vb = vbuf[wid];
@@ -713,10 +757,7 @@ __global__ void __launch_bounds__(256) k_gather_chunks(
       for (int r = 0; r < U; ++r) {
         const int px = point_pix(q[r]);
         v[r] = 0.0;
-        if (px < nloc) {
-          const double *mm = m + (long long)(px >> deg_shift) * 3;
-          v[r] = (double)q[r].x * mm[0] + (double)q[r].y * mm[1] + (double)q[r].z * mm[2];
-        }
+        if (px < nloc) v[r] = map_dot(mx, px >> deg_shift, q[r]);
       }
     } else {
       int px[U];
@@ -1143,6 +1184,7 @@ double now_ms() {
 }  // namespace
 
 #include "batch_kernels.inl"
+#include "pair_kernels.inl"
 #include "engine_host.inl"
 #include "engine_batch.inl"
 

@@ -119,6 +119,14 @@ class Engine {
   void run_cached_batch(long ndet, long nsamp, long nnz, double *timestamps, int32_t *pix,
                         float *pixweights, long nrhs, double *signals, bool is_device);
 
+  // Precision of the next run(): false = FP64 TOD (destripe), true = the
+  // FP32-TOD form (madam_b200_destripe_fp32): `signal` holds float32
+  // samples, the PCG projections read float32 pointing sums and a float32
+  // copy of the map; pixel matrices, baselines and reductions stay FP64.
+  void set_fp32(bool v) { fp32_next_ = v; }
+  bool fp32() const { return fp32_; }
+  long long pairs() const { return use_pairs_ ? npairs_ : 0; }
+
   bool cached() const { return cached_; }
   const Params &params() const { return par_; }
 
@@ -313,6 +321,20 @@ class Engine {
   DevBuf<int32_t> flagged_val_;
   std::vector<int32_t> orig_pix_values_;
   bool tod_cleaned_ = false;
+
+  // FP32-TOD form
+  bool fp32_next_ = false, fp32_ = false;
+  float *sig32_caller_ = nullptr;  // caller's float32 signal (host or device)
+  bool build_pairs();
+  void build_scatter_chunks();
+  bool use_pairs_ = false;        // PCG projections over pointing pairs
+  long long npairs_ = 0;
+  DevBuf<float4> gp4_;            // time-ordered pairs {sum w, cross pixel}
+  DevBuf<int> poff_;              // first pair of each baseline [nb + 1]
+  DevBuf<int2> pair_chunks_;      // gather chunks over pairs
+  long long npair_chunks_ = 0;
+  DevBuf<float4> lmapf_;          // float32 map copy read by the FP32 gather
+  DevBuf<double2> lmapg_;         // padded FP64 map copy {I, Q}, {U, 0}
 };
 
 }  // namespace madam

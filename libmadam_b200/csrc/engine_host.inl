@@ -71,6 +71,32 @@ void Engine::bind_inputs(double *timestamps, int32_t *pix, float *pixweights, do
   MADAM_CUDA(cudaMemcpyAsync(pix_orig_.get(), pix, n * sizeof(int32_t), kind, st_));
   MADAM_CUDA(cudaMemcpyAsync(pix_.get(), pix_orig_.get(), n * sizeof(int32_t),
                              cudaMemcpyDeviceToDevice, st_));
+  if (fp32_) {
+    // FP32-TOD form: float32 samples, widened once into the engine's copy
+    sig32_caller_ = (float *)signal;
+    h_signal_ = nullptr;
+    if (is_device) {
+      d_w_ = pixweights;
+    } else {
+      wraw_.alloc(n * nnz_);
+      MADAM_CUDA(cudaMemcpyAsync(wraw_.get(), pixweights, n * nnz_ * sizeof(float),
+                                 cudaMemcpyHostToDevice, st_));
+      d_w_ = wraw_.get();
+    }
+    tod_own_.alloc(n);
+    const float *src = (const float *)signal;
+    DevBuf<float> t32;
+    if (!is_device) {
+      t32.alloc(n);
+      MADAM_CUDA(cudaMemcpyAsync(t32.get(), signal, n * sizeof(float), cudaMemcpyHostToDevice,
+                                 st_));
+      src = t32.get();
+    }
+    if (n > 0) MADAM_LAUNCH(k_f32_to_f64, grid_for(n), 256, 0, st_, src, tod_own_.get(), n);
+    d_tod_ = tod_own_.get();
+    return;
+  }
+  sig32_caller_ = nullptr;
   if (is_device) {
     d_w_ = pixweights;
     d_tod_ = signal;
@@ -581,6 +607,16 @@ void Engine::build_csr() {
     return;
   }
   if (n >= (1LL << 31)) fail("too many samples for the pixel-sorted pointing");
+  use_pairs_ = false;
+  npairs_ = 0;
+  gp4_.reset();
+  poff_.reset();
+  pair_chunks_.reset();
+  npair_chunks_ = 0;
+  if (fp32_ && nmap_ == 3 && build_pairs()) {
+    build_scatter_chunks();
+    return;
+  }
   const SampleMap sm = sample_map(istart_d_.get(), kstart_d_.get(), (int)ninterval_, nsamp_,
                                   noba_short_, fdn_);
   DevBuf<int> keys, keys_s;
@@ -631,6 +667,10 @@ void Engine::build_csr() {
                    csr_nvalid_, point4_.get(), sm, (float4 *)nullptr, sp2_.get(), csr_off_.get());
   }
   MADAM_CUDA(cudaStreamSynchronize(st_));
+  build_scatter_chunks();
+}
+
+void Engine::build_scatter_chunks() {
   // scatter chunks: every pixel's entries cut into chunks of at most
   // kScatterChunk; pixels of several chunks combine their partial sums
   {
@@ -664,6 +704,100 @@ void Engine::build_csr() {
                                  cudaMemcpyHostToDevice, st_));
   }
   MADAM_CUDA(cudaStreamSynchronize(st_));
+}
+
+// Pointing pairs of the FP32-TOD form (pair_kernels.inl): time-ordered pairs
+// with per-baseline offsets and gather chunks, and the pixel-sorted pairs in
+// sp4_ / csr_off_ for the scatter.  false (nothing built) when a baseline
+// holds more than kGatherChunk pairs.
+bool Engine::build_pairs() {
+  const long long n = (long long)ndet_ * nsamp_;
+  const long long nb = (long long)ndet_ * noba_short_;
+  const SampleMap sm = sample_map(istart_d_.get(), kstart_d_.get(), (int)ninterval_, nsamp_,
+                                  noba_short_, fdn_);
+  DevBuf<int> head, pidx;
+  head.alloc(n);
+  pidx.alloc(n);
+  MADAM_LAUNCH(k_pair_heads, grid_for(n), 256, 0, st_, point4_.get(), n, sm, bw_.get(),
+               (int)nloc_, (int)ndeg_shift_, head.get());
+  {
+    size_t tmpb = 0;
+    MADAM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmpb, head.get(), pidx.get(), (int)n, st_));
+    DevBuf<uint8_t> tmp;
+    tmp.alloc(tmpb);
+    MADAM_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tmpb, head.get(), pidx.get(), (int)n, st_));
+  }
+  int last[2] = {0, 0};
+  MADAM_CUDA(cudaMemcpyAsync(&last[0], pidx.get() + (n - 1), sizeof(int), cudaMemcpyDeviceToHost,
+                             st_));
+  MADAM_CUDA(cudaMemcpyAsync(&last[1], head.get() + (n - 1), sizeof(int), cudaMemcpyDeviceToHost,
+                             st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  const int np = last[0] + last[1];
+  // per-baseline pair offsets, checked on the host before anything else
+  poff_.alloc(nb + 1);
+  MADAM_LAUNCH(k_pair_offsets, grid_for(nb + 1), 256, 0, st_, pidx.get(), bstart_d_.get(),
+               (long long)nsamp_, noba_short_, nb, n, np, poff_.get());
+  std::vector<int> offh((size_t)nb + 1);
+  MADAM_CUDA(cudaMemcpyAsync(offh.data(), poff_.get(), offh.size() * sizeof(int),
+                             cudaMemcpyDeviceToHost, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  std::vector<int2> ck;
+  for (long long d = 0; d < ndet_; ++d) {
+    long long b = d * noba_short_;
+    const long long b1 = b + noba_short_;
+    while (b < b1) {
+      if (offh[b + 1] - offh[b] > kGatherChunk) {
+        poff_.reset();
+        return false;
+      }
+      long long e = b + 1;
+      while (e < b1 && e - b < 32 && offh[e + 1] - offh[b] <= kGatherChunk) ++e;
+      ck.push_back(make_int2((int)b, (int)(e - b)));
+      b = e;
+    }
+  }
+  npairs_ = np;
+  gp4_.alloc(std::max(1, np));
+  DevBuf<int> pbase;
+  pbase.alloc(std::max(1, np));
+  MADAM_LAUNCH(k_pair_fill, grid_for(n), 256, 0, st_, point4_.get(), n, sm, bstart_d_.get(),
+               (int)nloc_, (int)ndeg_shift_, head.get(), pidx.get(), gp4_.get(), pbase.get());
+  head.reset();
+  pidx.reset();
+  npair_chunks_ = (long long)ck.size();
+  pair_chunks_.alloc(std::max<size_t>(1, ck.size()));
+  if (!ck.empty())
+    MADAM_CUDA(cudaMemcpyAsync(pair_chunks_.get(), ck.data(), ck.size() * sizeof(int2),
+                               cudaMemcpyHostToDevice, st_));
+  // pixel-sorted pairs (stable radix sort: time order inside a pixel)
+  csr_nvalid_ = np;
+  MADAM_LAUNCH(k_fill_int, grid_for(nloc_cross_ + 1), 256, 0, st_, csr_off_.get(),
+               (long long)nloc_cross_ + 1, np);
+  sp4_.alloc(std::max(1, np));
+  if (np > 0) {
+    DevBuf<int> keys, keys_s;
+    DevBuf<uint32_t> vals, vals_s;
+    keys.alloc(np);
+    vals.alloc(np);
+    keys_s.alloc(np);
+    vals_s.alloc(np);
+    MADAM_LAUNCH(k_pair_keys, grid_for(np), 256, 0, st_, gp4_.get(), np, keys.get(), vals.get());
+    int endbit = 1;
+    while ((1L << endbit) <= nloc_cross_) ++endbit;
+    size_t tmpb = 0;
+    MADAM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmpb, keys.get(), keys_s.get(),
+                                               vals.get(), vals_s.get(), np, 0, endbit, st_));
+    DevBuf<uint8_t> tmp;
+    tmp.alloc(tmpb);
+    MADAM_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tmpb, keys.get(), keys_s.get(),
+                                               vals.get(), vals_s.get(), np, 0, endbit, st_));
+    MADAM_LAUNCH(k_pair_csr_fill, grid_for(np), 256, 0, st_, keys_s.get(), vals_s.get(), np,
+                 gp4_.get(), pbase.get(), sp4_.get(), csr_off_.get());
+  }
+  use_pairs_ = true;
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  return true;
 }
 
 void Engine::bin_tod(bool accumulate_wamap) {
@@ -1470,9 +1604,12 @@ void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) 
   }
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[1], st_));
   if (nloc_cross_ > 0) {
-    if (nmap_ == 3)
-      MADAM_LAUNCH(k_ccmult<3>, grid_for(nloc_cross_), 256, 0, st_, cca_.get(), lmap_.get(),
-                   (long long)nloc_cross_);
+    if (nmap_ == 3 && fp32_)
+      MADAM_LAUNCH(k_ccmult_copy<true>, grid_for(nloc_cross_), 256, 0, st_, cca_.get(),
+                   lmap_.get(), (long long)nloc_cross_, (double2 *)nullptr, lmapf_.get());
+    else if (nmap_ == 3)
+      MADAM_LAUNCH(k_ccmult_copy<false>, grid_for(nloc_cross_), 256, 0, st_, cca_.get(),
+                   lmap_.get(), (long long)nloc_cross_, lmapg_.get(), (float4 *)nullptr);
     else
       MADAM_LAUNCH(k_ccmult<1>, grid_for(nloc_cross_), 256, 0, st_, cca_.get(), lmap_.get(),
                    (long long)nloc_cross_);
@@ -1490,17 +1627,26 @@ void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) 
   }
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[3], st_));
   // 3) map -> baseline and p.ap (849-878)
-  if (ngather_chunks_ > 0) {
-    if (nmap_ == 3)
-      MADAM_LAUNCH(k_gather_chunks<3>, kRedBlocks, 256, 0, st_, gather_chunks_.get(),
+  if (use_pairs_) {
+    MADAM_LAUNCH(k_gather_pairs, kRedBlocks, 256, 0, st_, pair_chunks_.get(), npair_chunks_,
+                 gp4_.get(), poff_.get(), bw_.get(), p, nna_.get(), lmapf_.get(), rmask_.get(),
+                 ap, part_.get());
+  } else if (ngather_chunks_ > 0) {
+    if (nmap_ == 3 && fp32_)
+      MADAM_LAUNCH((k_gather_chunks<3, float4>), kRedBlocks, 256, 0, st_, gather_chunks_.get(),
                    ngather_chunks_, point4_.get(), pixc_.get(), bstart_d_.get(), noba_short_,
-                   nsamp_, bw_.get(), p, nna_.get(), lmap_.get(), (int)ndeg_shift_, (int)nloc_,
-                   rmask_.get(), ap, part_.get());
+                   nsamp_, bw_.get(), p, nna_.get(), lmap_.get(), lmapf_.get(),
+                   (int)ndeg_shift_, (int)nloc_, rmask_.get(), ap, part_.get());
+    else if (nmap_ == 3)
+      MADAM_LAUNCH((k_gather_chunks<3, double2>), kRedBlocks, 256, 0, st_, gather_chunks_.get(),
+                   ngather_chunks_, point4_.get(), pixc_.get(), bstart_d_.get(), noba_short_,
+                   nsamp_, bw_.get(), p, nna_.get(), lmap_.get(), lmapg_.get(),
+                   (int)ndeg_shift_, (int)nloc_, rmask_.get(), ap, part_.get());
     else
-      MADAM_LAUNCH(k_gather_chunks<1>, kRedBlocks, 256, 0, st_, gather_chunks_.get(),
+      MADAM_LAUNCH((k_gather_chunks<1, double2>), kRedBlocks, 256, 0, st_, gather_chunks_.get(),
                    ngather_chunks_, point4_.get(), pixc_.get(), bstart_d_.get(), noba_short_,
-                   nsamp_, bw_.get(), p, nna_.get(), lmap_.get(), (int)ndeg_shift_, (int)nloc_,
-                   rmask_.get(), ap, part_.get());
+                   nsamp_, bw_.get(), p, nna_.get(), lmap_.get(), (const double2 *)nullptr,
+                   (int)ndeg_shift_, (int)nloc_, rmask_.get(), ap, part_.get());
   } else if (gather_kb_ > 0) {
     if (nmap_ == 3)
       MADAM_LAUNCH(k_gather_tiled<3>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
@@ -1610,6 +1756,10 @@ void Engine::iterate() {
   scal_.alloc(S_NSCAL);
   scal_.zero(st_);
   lmap_.alloc((size_t)std::max<long>(1, nloc_cross_) * nmap_);
+  if (nmap_ == 3) {
+    if (fp32_) lmapf_.alloc((size_t)std::max<long>(1, nloc_cross_));
+    else lmapg_.alloc((size_t)std::max<long>(1, nloc_cross_) * 2);
+  }
   MADAM_CUDA(cudaMemcpyAsync(r_.get(), yba_.get(), nb * sizeof(double), cudaMemcpyDeviceToDevice,
                              st_));
   aa_.zero(st_);
@@ -1828,9 +1978,22 @@ void Engine::writeback_host() {
       MADAM_CUDA(cudaMemcpyAsync(h_pix_, fin.get(), n * sizeof(int32_t), cudaMemcpyDeviceToHost,
                                  st_));
     }
-    if (tod_cleaned_)
+    if (tod_cleaned_ && !fp32_)
       MADAM_CUDA(cudaMemcpyAsync(h_signal_, d_tod_, n * sizeof(double), cudaMemcpyDeviceToHost,
                                  st_));
+  }
+  if (tod_cleaned_ && fp32_) {
+    // the cleaned float32 TOD goes back into the caller's signal buffer
+    if (in_device_) {
+      MADAM_LAUNCH(k_f64_to_f32, grid_for(n), 256, 0, st_, d_tod_, sig32_caller_, n);
+    } else {
+      DevBuf<float> t32;
+      t32.alloc(n);
+      MADAM_LAUNCH(k_f64_to_f32, grid_for(n), 256, 0, st_, d_tod_, t32.get(), n);
+      MADAM_CUDA(cudaMemcpyAsync(sig32_caller_, t32.get(), n * sizeof(float),
+                                 cudaMemcpyDeviceToHost, st_));
+      MADAM_CUDA(cudaStreamSynchronize(st_));
+    }
   }
   MADAM_CUDA(cudaStreamSynchronize(st_));
 }
@@ -1846,6 +2009,8 @@ void Engine::run(const Params &par, std::vector<Detector> dets, long ndet, long 
   rrinit = 0;
   rr_final = 0;
   par_ = par;
+  fp32_ = fp32_next_;
+  fp32_next_ = false;
   dets_ = std::move(dets);
   ndet_ = ndet;
   nsamp_ = nsamp;
@@ -1948,6 +2113,8 @@ void Engine::run_cached(long ndet, long nsamp, long nnz, double *timestamps, int
   tod_cleaned_ = false;
   d_pix_caller_ = is_device ? pix : nullptr;
   (void)timestamps;
+  fp32_ = false;  // destripe_with_cache takes float64 signals
+  fp32_next_ = false;
   bind_inputs(timestamps, pix, pixweights, signal, is_device, false);
   flag_and_compact(false);
   build_runs();
@@ -1989,7 +2156,7 @@ long Engine::result_size(const std::string &name) {
   if (name == "invcov") return (long)invcov_host_.size();
   if (name == "rr_history") return (long)rr_history.size();
   if (name == "band_widths") return (long)band_widths_.size();
-  if (name == "scalars") return 20;
+  if (name == "scalars") return 22;
   if (name == "timings") return 9;
   if (name == "setup_marks") return kSetupMarks;
   if (name == "map_batch" || name == "binmap_batch") return nrhs_ * npm * nmap_;
@@ -2088,13 +2255,14 @@ void Engine::result_copy(const std::string &name, void *dst, long nbytes) {
     std::memcpy(dst, band_widths_.data(), sz * sizeof(long));
   } else if (name == "scalars") {
     need(sizeof(double));
-    const double v[20] = {(double)noiter, rrinit, rr_final, (double)nof_,
+    const double v[22] = {(double)noiter, rrinit, rr_final, (double)nof_,
                           (double)band_widths_.size(), (double)n_band_fail_, timings.iterate_ms,
                           timings.total_ms, (double)nmap_, (double)noba_short_,
                           (double)(12 * par_.nside_map * par_.nside_map), (double)nruns_,
                           (double)nwork_, (double)nloc_, (double)segs_.size(),
                           (double)cg_prec_segs_.size(), (double)band2_rows_,
-                          (double)band2_ntrans_, (double)p2nch_, (double)csr_nvalid_};
+                          (double)band2_ntrans_, (double)p2nch_, (double)csr_nvalid_,
+                          (double)(use_pairs_ ? npairs_ : 0), fp32_ ? 1.0 : 0.0};
     std::memcpy(dst, v, sizeof v);
   } else if (name == "setup_marks") {
     need(sizeof(double));

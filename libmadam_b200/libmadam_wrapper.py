@@ -100,6 +100,26 @@ def destripe(comm, pars, dets, weights, timestamps, pixels, pixweights, signal, 
     """
     Solve and subtract baseline offsets from signal
     """
+    _destripe(False, comm, pars, dets, weights, timestamps, pixels, pixweights, signal, periods,
+              npsd, psdstarts, psdfreqs, psdvals)
+
+
+def destripe_fp32(comm, pars, dets, weights, timestamps, pixels, pixweights, signal, periods,
+                  npsd, psdstarts, psdfreqs, psdvals):
+    """
+    destripe() on a float32 signal (the FP32-TOD precision form; no
+    counterpart in the reference, whose signal is float64): the PCG
+    projections read float32 pointing sums and a float32 copy of the map,
+    while pixel matrices, baselines and inner products stay float64.  Maps
+    and baselines agree with destripe() on the same samples to about 1e-6
+    relative.
+    """
+    _destripe(True, comm, pars, dets, weights, timestamps, pixels, pixweights, signal, periods,
+              npsd, psdstarts, psdfreqs, psdvals)
+
+
+def _destripe(fp32, comm, pars, dets, weights, timestamps, pixels, pixweights, signal, periods,
+              npsd, psdstarts, psdfreqs, psdvals):
     if not available:
         raise RuntimeError("No libmadam available, cannot destripe")
     fcomm = _fcomm(comm)
@@ -109,7 +129,7 @@ def destripe(comm, pars, dets, weights, timestamps, pixels, pixweights, signal, 
     ts = _Buf(timestamps, TIMESTAMP_TYPE)
     px = _Buf(pixels, PIXEL_TYPE)
     pw = _Buf(pixweights, WEIGHT_TYPE)
-    sg = _Buf(signal, SIGNAL_TYPE)
+    sg = _Buf(signal, np.float32 if fp32 else SIGNAL_TYPE)
     nsamp = ts.size
     nnz = pw.size // nsamp // ndet
     w = np.ascontiguousarray(weights, dtype=np.float64)
@@ -122,7 +142,8 @@ def destripe(comm, pars, dets, weights, timestamps, pixels, pixweights, signal, 
     npsdval = psdvals.size
     npsdtot = npsdval // npsdbin
     p = lambda a: a.ctypes.data_as(ct.c_void_p)
-    status = _madam.madam_b200_destripe(
+    entry = _madam.madam_b200_destripe_fp32 if fp32 else _madam.madam_b200_destripe
+    status = entry(
         fcomm, parstring, ndet, detstring, p(w), nsamp, nnz, ts.ptr, px.ptr, pw.ptr, sg.ptr,
         periods.size, p(periods), p(npsd), npsdtot, p(psdstarts), npsdbin, p(psdfreqs),
         npsdval, p(psdvals))
@@ -231,7 +252,8 @@ def get_result(name):
 def scalars():
     keys = ["noiter", "rrinit", "rr_final", "nof", "n_band", "n_band_fail", "iterate_ms",
             "total_ms", "nmap", "noba_short", "npix_map", "nruns", "nwork", "nloc", "nseg",
-            "n_cg_prec", "band_rows", "band_transfers", "band_chunks", "scatter_samples"]
+            "n_cg_prec", "band_rows", "band_transfers", "band_chunks", "scatter_samples",
+            "pairs", "fp32"]
     return dict(zip(keys, get_result("scalars").tolist()))
 
 
