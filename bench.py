@@ -102,6 +102,14 @@ def config_for(name):
         return syn.config2(), "plain destripe nside512 16det x 4obs x 2^23 @100Hz IQU"
     if name == "1":
         return syn.config1(), "plain destripe nside64 4det x 2^20 @10Hz IQU"
+    if name == "3":
+        return syn.config3(), ("precision form (float32 TOD, destripe_fp32) nside1024 "
+                               "64det x 2^24 @100Hz IQU")
+    if name == "mid3":
+        cfg = syn.config3()
+        cfg.ndet = 16
+        cfg.nsamp_obs = 1 << 21
+        return cfg, "precision form nside1024 16det x 2^21 @100Hz IQU (profiling size)"
     if name == "prof":
         cfg = syn.config2()
         cfg.nobs = 1
@@ -338,7 +346,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="2", choices=["2", "1", "prof", "mid", "small", "mc", "serve"])
+    ap.add_argument("--config", default="2", choices=["2", "1", "3", "prof", "mid", "mid3", "small", "mc",
+                                                   "serve"])
     ap.add_argument("--requests", type=int, default=60)
     ap.add_argument("--rate", type=float, default=20.0)
     ap.add_argument("--workers", type=int, default=4)
@@ -372,18 +381,26 @@ def main():
     torch.cuda.synchronize()
     t_gen = time.time() - t0
     n = cfg.ndet * cfg.nsamp
+    fp32 = args.config in ("3", "mid3")
+    destripe = W.destripe_fp32 if fp32 else W.destripe
     pix = d["pixels"].reshape(-1)
     wts = d["pixweights"].reshape(-1)
     sig = d["signal"].reshape(-1)
+    if fp32:
+        sig64 = sig
+        sig = sig.float()
+        d["signal"] = d["signal"].float()
     common = (d["pars"], d["dets"], d["detweights"])
     psd = (d["periods"], d["npsd"], d["psdstarts"], d["psdfreqs"], d["psdvals"])
 
     # full solve with inputs resident in HBM: time to cglimit
-    W.destripe(None, *common, d["timestamps"], pix, wts, sig, *psd)
+    destripe(None, *common, d["timestamps"], pix, wts, sig, *psd)
     tim = W.timings()
     sca = W.scalars()
     marks = W.setup_marks()
     noiter = int(sca["noiter"])
+    if fp32:
+        map32, aa32 = W.get_result("map"), W.get_result("aa")
 
     # timed PCG iterations (the step)
     barrier(world)
@@ -405,8 +422,8 @@ def main():
         hn = {k: v.numpy().reshape(-1) for k, v in h.items()}
         barrier(world)
         t1 = time.perf_counter()
-        W.destripe(None, *common, hn["timestamps"], hn["pixels"], hn["pixweights"], hn["signal"],
-                   *psd)
+        destripe(None, *common, hn["timestamps"], hn["pixels"], hn["pixweights"], hn["signal"],
+                 *psd)
         m = W.get_result("map")
         t_e2e = time.perf_counter() - t1
         t_e2e = reduce_max(t_e2e, world)
@@ -421,24 +438,48 @@ def main():
                "setup_marks_ms": W.setup_marks()}
         del h, hn
 
+    # the precision form against a float64-TOD solve of the same samples
+    fp64_cmp = None
+    if fp32:
+        del d["signal"], sig
+        torch.cuda.empty_cache()
+        W.destripe(None, *common, d["timestamps"], pix, wts, sig64, *psd)
+        m64 = W.get_result("map").reshape(-1, 3)
+        a64 = W.get_result("aa")
+        it64 = int(W.scalars()["noiter"])
+        t64 = W.timings()["iterate_ms"]
+        b64 = W.bench_iterations(args.warmup, args.steps)
+        m32 = map32.reshape(-1, 3)
+        rel = lambda a, b: float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+        fp64_cmp = {"map_rel_err_iqu": [rel(m32[:, c], m64[:, c]) for c in range(3)],
+                    "baseline_rel_err": rel(aa32, a64),
+                    "tolerance": 1e-4, "fp64_ms_per_iteration": b64["ms_per_iter"],
+                    "fp64_iterations_to_cglimit": it64, "fp64_time_to_cglimit_ms": t64,
+                    "speedup_per_iteration": b64["ms_per_iter"] / b["ms_per_iter"],
+                    "pointing_pairs": sca["pairs"], "samples_per_pair": n / max(1.0, sca["pairs"])}
+        del sig64
+
     # roofline of the dominant kernel (algorithmic bytes per launch / duration)
     hbm, peak_kind = peaks()
     nb = cfg.ndet * int(sca["noba_short"])
     npix_hit = int(sca["nloc"])
     phases = {"scatter": b["scatter_ms"], "gather": b["gather_ms"], "filter": b["filter_ms"],
               "precond": b["precond_ms"]}
-    algo = {"scatter": 16.0 * n + 8.0 * n / max(1, cfg.base_first * cfg.fsample),
-            "gather": 16.0 * n + 5 * 8.0 * nb + 24.0 * npix_hit,
+    # pointing entries streamed per iteration: samples, or pairs in the FP32 form
+    nent = int(sca["pairs"]) if fp32 and sca["pairs"] > 0 else n
+    algo = {"scatter": 16.0 * nent + 8.0 * nent / max(1, cfg.base_first * cfg.fsample),
+            "gather": 16.0 * nent + 5 * 8.0 * nb + (16.0 if fp32 else 32.0) * npix_hit,
             "filter": None, "precond": None}
     dom = max(("scatter", "gather"), key=lambda k: phases[k])
     achieved = algo[dom] / (phases[dom] * 1e-3) / 1e9
-    kname = {"scatter": "k_scatter_chunks", "gather": "k_gather_chunks"}[dom]
-    traffic = profiled_traffic(kname, n)
+    kname = {"scatter": "k_scatter_chunks",
+             "gather": "k_gather_pairs" if nent != n else "k_gather_chunks"}[dom]
+    traffic = profiled_traffic(kname, nent)
     try:
         w_p = float(np.mean(W.get_result("band_widths")))
     except Exception:
         w_p = 0.0
-    b_iter = 32.0 * n + 8.0 * (16 + w_p) * nb + (4 * 3 * 8 + 48) * npix_hit
+    b_iter = 32.0 * nent + 8.0 * (16 + w_p) * nb + (4 * 3 * 8 + 48) * npix_hit
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": hbm,
                 "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,
                 "algorithmic_bytes": algo[dom], "traffic": traffic,
@@ -460,7 +501,8 @@ def main():
             "metric": "TOD samples/s per PCG iteration", "value": value,
             "unit": "samples/s per PCG iteration", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_iter, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if fp32 else "f64",
+            "data": "synthetic",
             "config": {"workload": wname, "samples": n, "baselines": nb,
                        "hit_pixels": npix_hit, "nside": cfg.nside,
                        "l2": "inputs larger than L2 (pointing {:.1f} GB)".format(16e-9 * n),
@@ -476,6 +518,10 @@ def main():
             "setup_marks_ms": marks,
             "band": {k: sca[k] for k in ("band_rows", "band_transfers", "band_chunks", "nseg")},
         }
+        if fp32:
+            line["precision"] = ("float32 TOD, pointing pairs and map copy in the projections; "
+                                 "float64 pixel matrices, baselines and reductions")
+            line["fp64_comparison"] = fp64_cmp
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

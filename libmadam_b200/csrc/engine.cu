@@ -699,6 +699,83 @@ __device__ __forceinline__ double map_dot(const float4 *__restrict__ mf, long lo
   return (double)q.x * a.x + (double)q.y * a.y + (double)q.z * a.z;
 }
 
+// Per-baseline sums of a warp chunk of at most kGatherChunk staged values
+// (map_to_baseline's inner sum, smadam_routines.f90:1018-1032, for up to 32
+// consecutive baselines at once), for chunks of few long baselines.  vb
+// holds the chunk's values in time order with entry i at vb[i + i / 8]
+// (entries n..255 are zero); baseline j < nbl owns entries [a0, a1) (lane
+// j's arguments).  Lane L adds entries 8L..8L+7 in order; a segmented warp
+// scan joins the parts of a baseline that spans lanes.  bsum[j] receives
+// baseline j's sum (0 when empty).  The padding keeps both the strided
+// staging writes and these lane-contiguous reads free of bank conflicts.
+// Where a chunk holds a few long baselines this replaces up to 256 serial
+// shared-memory reads by one or two lanes with 8 reads by every lane.
+struct ChunkSmem {
+  double bsum[32];
+  unsigned heads[8];        // bit e: entry e starts a nonempty baseline
+  unsigned char ord2b[32];  // k-th nonempty baseline -> its lane
+};
+
+__device__ __forceinline__ void chunk_baseline_sums(const double *vb, int nbl, int a0, int a1,
+                                                    ChunkSmem &cs, int lane) {
+  const unsigned full = 0xffffffffu;
+  cs.bsum[lane] = 0.0;
+  if (lane < 8) cs.heads[lane] = 0u;
+  __syncwarp();
+  const bool ne = lane < nbl && a1 > a0;
+  const unsigned nem = __ballot_sync(full, ne);
+  if (ne) {
+    cs.ord2b[__popc(nem & ((1u << lane) - 1u))] = (unsigned char)lane;
+    atomicOr(&cs.heads[a0 >> 5], 1u << (a0 & 31));
+  }
+  __syncwarp();
+  const int wl = lane >> 2, sh = (lane & 3) * 8;
+  int cnt = 0;  // heads before entry 8L
+#pragma unroll
+  for (int w = 0; w < 8; ++w) {
+    const unsigned x = cs.heads[w];
+    if (w < wl) cnt += __popc(x);
+    else if (w == wl) cnt += __popc(x & ((1u << sh) - 1u));
+  }
+  const unsigned bits = (cs.heads[wl] >> sh) & 0xffu;
+  const int nh0 = cnt;
+  double w[8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) w[r] = vb[9 * lane + r];
+  double run = 0.0, first = 0.0;
+  bool seen = false;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    if ((bits >> r) & 1u) {
+      if (!seen) {
+        first = run;
+        seen = true;
+      } else {
+        cs.bsum[cs.ord2b[cnt - 1]] = run;
+      }
+      run = 0.0;
+      ++cnt;
+    }
+    run += w[r];
+  }
+  // segmented inclusive scan of (run, seen) over the lanes, left to right
+  double sc = run;
+  int fl = seen ? 1 : 0;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const double so = __shfl_up_sync(full, sc, d);
+    const int fo = __shfl_up_sync(full, fl, d);
+    if (lane >= d) {
+      if (!fl) sc = so + sc;
+      fl |= fo;
+    }
+  }
+  const double carry = __shfl_up_sync(full, sc, 1);
+  if (seen && nh0 > 0) cs.bsum[cs.ord2b[nh0 - 1]] = carry + first;
+  if (lane == 31 && cnt > 0) cs.bsum[cs.ord2b[cnt - 1]] = sc;
+  __syncwarp();
+}
+
 // map_to_baseline, warp chunks: a warp takes a chunk of consecutive
 // baselines of one detector (at most kGatherChunk samples, at most 32
 // baselines), loads all of its samples (8 per lane, coalesced) with their map
@@ -707,6 +784,7 @@ __device__ __forceinline__ double map_dot(const float4 *__restrict__ mf, long lo
 // No block barriers: warps run independently.  Used when every baseline is
 // at most kGatherChunk samples long.
 constexpr int kGatherChunk = 256;
+static_assert(kGatherChunk == 256, "chunk_baseline_sums takes 8 entries a lane");
 
 // MAPT (NMAP = 3): the map copy it reads, double2 (padded FP64, two 16-byte
 // loads in one sector) or float4 (FP32-TOD form, one load).

@@ -331,7 +331,7 @@ class Engine {
   long long npairs_ = 0;
   DevBuf<float4> gp4_;            // time-ordered pairs {sum w, cross pixel}
   DevBuf<int> poff_;              // first pair of each baseline [nb + 1]
-  DevBuf<int2> pair_chunks_;      // gather chunks over pairs
+  DevBuf<int4> pair_chunks_;      // gather chunks over pairs {b0, nbl, first pair, pairs}
   long long npair_chunks_ = 0;
   DevBuf<float4> lmapf_;          // float32 map copy read by the FP32 gather
   DevBuf<double2> lmapg_;         // padded FP64 map copy {I, Q}, {U, 0}

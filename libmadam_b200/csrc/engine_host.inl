@@ -742,7 +742,7 @@ bool Engine::build_pairs() {
   MADAM_CUDA(cudaMemcpyAsync(offh.data(), poff_.get(), offh.size() * sizeof(int),
                              cudaMemcpyDeviceToHost, st_));
   MADAM_CUDA(cudaStreamSynchronize(st_));
-  std::vector<int2> ck;
+  std::vector<int4> ck;
   for (long long d = 0; d < ndet_; ++d) {
     long long b = d * noba_short_;
     const long long b1 = b + noba_short_;
@@ -753,7 +753,7 @@ bool Engine::build_pairs() {
       }
       long long e = b + 1;
       while (e < b1 && e - b < 32 && offh[e + 1] - offh[b] <= kGatherChunk) ++e;
-      ck.push_back(make_int2((int)b, (int)(e - b)));
+      ck.push_back(make_int4((int)b, (int)(e - b), offh[b], offh[e] - offh[b]));
       b = e;
     }
   }
@@ -768,7 +768,7 @@ bool Engine::build_pairs() {
   npair_chunks_ = (long long)ck.size();
   pair_chunks_.alloc(std::max<size_t>(1, ck.size()));
   if (!ck.empty())
-    MADAM_CUDA(cudaMemcpyAsync(pair_chunks_.get(), ck.data(), ck.size() * sizeof(int2),
+    MADAM_CUDA(cudaMemcpyAsync(pair_chunks_.get(), ck.data(), ck.size() * sizeof(int4),
                                cudaMemcpyHostToDevice, st_));
   // pixel-sorted pairs (stable radix sort: time order inside a pixel)
   csr_nvalid_ = np;

@@ -104,25 +104,28 @@ __global__ void k_pair_csr_fill(const int *keys, const uint32_t *idx, int npair,
   }
 }
 
-// map_to_baseline over pairs, warp chunks of <= kGatherChunk pairs and <= 32
-// baselines (the single-RHS k_gather_chunks with pair offsets); fused with
-// the p.ap partial sums
+// map_to_baseline over pairs: warp chunks {first baseline, baselines, first
+// pair, pairs} of <= kGatherChunk pairs and <= 32 baselines.  A lane loads
+// its 8 pairs (coalesced) with their float32 map values in flight, stages
+// w.m in the warp's shared-memory slice, and chunk_baseline_sums adds every
+// baseline of the chunk at once (a pair chunk holds few long baselines);
+// fused with the p.ap partial sums.
 __global__ void __launch_bounds__(256) k_gather_pairs(
-    const int2 *__restrict__ chunks, long long nchunks, const float4 *__restrict__ gp4,
+    const int4 *__restrict__ chunks, long long nchunks, const float4 *__restrict__ gp4,
     const int *__restrict__ poff, const double *__restrict__ bw, const double *__restrict__ p,
     const double *__restrict__ nna, const float4 *__restrict__ mf,
     const uint8_t *__restrict__ rmask, double *__restrict__ ap, double *__restrict__ part) {
-  __shared__ double vbuf[8][kGatherChunk];
+  __shared__ double vbuf[8][kGatherChunk + kGatherChunk / 8];
+  __shared__ ChunkSmem csm[8];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   double *vb = vbuf[wid];
+  ChunkSmem &cs = csm[wid];
   const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
   constexpr int U = kGatherChunk / 32;
   double pap = 0;
   for (long long c = w0; c < nchunks; c += nwarps) {
-    const int2 ck = chunks[c];
-    const int q0 = poff[ck.x];
-    const int n = poff[ck.x + ck.y] - q0;
+    const int4 ck = chunks[c];
     double detw = 0, pb = 0, apb = 0, npb = 0;
     int a0 = 0, a1 = 0;
     bool rm = false;
@@ -133,29 +136,29 @@ __global__ void __launch_bounds__(256) k_gather_pairs(
       apb = ap[b];
       npb = nna[b] * pb;
       rm = rmask[b] != 0;
-      a0 = poff[b] - q0;
-      a1 = poff[b + 1] - q0;
+      a0 = poff[b] - ck.z;
+      a1 = poff[b + 1] - ck.z;
     }
     float4 q[U];
 #pragma unroll
     for (int r = 0; r < U; ++r) {
       const int i = r * 32 + lane;
-      q[r] = i < n ? __ldcs(gp4 + q0 + i) : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+      q[r] = i < ck.w ? __ldcs(gp4 + (long long)ck.z + i)
+                      : make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
     }
 #pragma unroll
     for (int r = 0; r < U; ++r) {
       const int px = __float_as_int(q[r].w);
-      vb[r * 32 + lane] = px >= 0 ? map_dot(mf, px, q[r]) : 0.0;
+      vb[r * 36 + lane + (lane >> 3)] = px >= 0 ? map_dot(mf, px, q[r]) : 0.0;
     }
     __syncwarp();
+    chunk_baseline_sums(vb, ck.y, a0, a1, cs, lane);
     if (lane < ck.y) {
       const long long b = ck.x + lane;
       if (detw == 0) {
         if (rm) pap += pb * apb;
       } else {
-        double apn = 0;
-        for (int i = a0; i < a1; ++i) apn += vb[i];
-        const double val = apb + (npb - apn * detw);
+        const double val = apb + (npb - cs.bsum[lane] * detw);
         ap[b] = val;
         if (rm) pap += pb * val;
       }

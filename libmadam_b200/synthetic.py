@@ -153,6 +153,16 @@ def config2() -> ScanConfig:
     )
 
 
+def config3() -> ScanConfig:
+    """Precision form: nside 1024, 64 dets x 2^24 @ 100 Hz (1.07e9 samples),
+    fknee 0.1 Hz, alpha -1, base_first 1 s; float32 TOD in destripe_fp32."""
+    return ScanConfig(
+        nside=1024, nside_submap=16, ndet=64, nobs=1, nsamp_obs=1 << 24,
+        fsample=100.0, fknee=0.1, alpha=-1.0, base_first=1.0, seed=1003,
+        extra_pars=dict(cglimit=1e-12),
+    )
+
+
 def config4() -> ScanConfig:
     """Batched Monte Carlo form: nside 512, 32 dets x 2^22 @ 100 Hz sharing
     one pointing, fknee per detector uniform in 0.02-0.2 Hz, alpha -1."""
