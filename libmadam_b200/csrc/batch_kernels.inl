@@ -1,12 +1,11 @@
 // Multi-right-hand-side kernels of the batched Monte-Carlo solve
 // (madam_b200_destripe_with_cache_batch).  The R realisations share the
 // pointing, the pixel matrices, the filter and the preconditioner, so one
-// pass over the pointing serves a group of RB right-hand sides.  Vectors are
-// stored right-hand-side major ([R][nb] baseline vectors, [R][npix][nmap]
-// maps).  For every right-hand side the arithmetic and its order are those
-// of the single-RHS kernels (same chunking, same per-lane sums, same warp
-// trees), so a batched solve repeats the single solves to the last bit.
-// `act[r]` is 0 for right-hand sides whose PCG has stopped.
+// pass over the pointing serves a group of right-hand sides.  Baseline
+// vectors are stored right-hand-side major ([R][nb]); the projections work
+// on right-hand-side-minor copies (below).  For every right-hand side the
+// arithmetic of the projections and its order are those of the single-RHS
+// kernels.  `act[r]` is 0 for right-hand sides whose PCG has stopped.
 
 // baseline_to_map for right-hand sides [r0, r0 + nr), nr <= RB
 template <int NMAP, int RB>
@@ -112,113 +111,6 @@ __global__ void k_ccmult_b(const double *cc, double *m, long long n) {
   }
 }
 
-// map_to_baseline for right-hand sides [r0, r0 + nr), nr <= RB; the warps'
-// staging slices are [RB][kGatherChunk] doubles of dynamic shared memory
-template <int NMAP, int RB>
-__global__ void __launch_bounds__(256) k_gather_chunks_b(
-    const int2 *__restrict__ chunks, long long nchunks, const float4 *__restrict__ p4,
-    const int32_t *__restrict__ pc, const uint32_t *__restrict__ bstart, long noba,
-    long long nsamp, const double *__restrict__ bw, const double *__restrict__ p, long long nb,
-    const double *__restrict__ nna, const double *__restrict__ m, long long mstride,
-    int deg_shift, int nloc, const uint8_t *__restrict__ rmask, double *__restrict__ ap,
-    int r0, int nr, double *__restrict__ part) {
-  extern __shared__ double gvb[];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  double *vb = gvb + (size_t)wid * RB * kGatherChunk;
-  const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  constexpr int U = kGatherChunk / 32;
-  double pap[RB];
-#pragma unroll
-  for (int j = 0; j < RB; ++j) pap[j] = 0.0;
-  for (long long c = w0; c < nchunks; c += nwarps) {
-    const int2 ck = chunks[c];
-    const long long det = ck.x / noba, k0 = ck.x - det * noba;
-    const int s0 = (int)bstart[k0];
-    const int n = (int)(bstart[k0 + ck.y] - s0);
-    const long long base = det * nsamp + s0;
-    double detw = 0;
-    double pb[RB], apb[RB], npb[RB];
-    int a0 = 0, a1 = 0;
-    bool rm = false;
-    if (lane < ck.y) {
-      const long long b = ck.x + lane;
-      detw = bw[b];
-      const double nn = nna[b];
-#pragma unroll
-      for (int j = 0; j < RB; ++j) {
-        if (j < nr) {
-          pb[j] = p[(long long)(r0 + j) * nb + b];
-          apb[j] = ap[(long long)(r0 + j) * nb + b];
-          npb[j] = nn * pb[j];
-        }
-      }
-      rm = rmask[b] != 0;
-      a0 = (int)(bstart[k0 + lane] - s0);
-      a1 = (int)(bstart[k0 + lane + 1] - s0);
-    }
-    if (NMAP == 3) {
-      float4 q[U];
-#pragma unroll
-      for (int r = 0; r < U; ++r) {
-        const int i = r * 32 + lane;
-        q[r] = i < n ? __ldcs(p4 + base + i) : make_float4(0.f, 0.f, 0.f, __int_as_float(nloc));
-      }
-#pragma unroll
-      for (int j = 0; j < RB; ++j) {
-        if (j >= nr) break;
-        const double *mj = m + (long long)(r0 + j) * mstride;
-#pragma unroll
-        for (int r = 0; r < U; ++r) {
-          const int px = point_pix(q[r]);
-          double v = 0.0;
-          if (px < nloc) {
-            const double *mm = mj + (long long)(px >> deg_shift) * 3;
-            v = (double)q[r].x * mm[0] + (double)q[r].y * mm[1] + (double)q[r].z * mm[2];
-          }
-          vb[j * kGatherChunk + r * 32 + lane] = v;
-        }
-      }
-    } else {
-      int px[U];
-#pragma unroll
-      for (int r = 0; r < U; ++r) {
-        const int i = r * 32 + lane;
-        px[r] = i < n ? __ldcs(pc + base + i) : nloc;
-      }
-#pragma unroll
-      for (int j = 0; j < RB; ++j) {
-        if (j >= nr) break;
-        const double *mj = m + (long long)(r0 + j) * mstride;
-#pragma unroll
-        for (int r = 0; r < U; ++r)
-          vb[j * kGatherChunk + r * 32 + lane] = px[r] < nloc ? mj[px[r] >> deg_shift] : 0.0;
-      }
-    }
-    __syncwarp();
-    if (lane < ck.y) {
-      const long long b = ck.x + lane;
-#pragma unroll
-      for (int j = 0; j < RB; ++j) {
-        if (j >= nr) break;
-        if (detw == 0) {
-          if (rm) pap[j] += pb[j] * apb[j];
-        } else {
-          double apn = 0;
-          for (int i = a0; i < a1; ++i) apn += vb[j * kGatherChunk + i];
-          const double val = apb[j] + (npb[j] - apn * detw);
-          ap[(long long)(r0 + j) * nb + b] = val;
-          if (rm) pap[j] += pb[j] * val;
-        }
-      }
-    }
-    __syncwarp();
-  }
-  block_sum<RB>(pap);
-  if (threadIdx.x == 0)
-    for (int j = 0; j < nr; ++j) part[(long long)(r0 + j) * 3 * kRedBlocks + blockIdx.x] = pap[j];
-}
-
 // masked dots for every active right-hand side: blockIdx.y = r, part
 // [R][3][kRedBlocks]
 __global__ void k_dots_b(const double *a0, const double *b0, const double *a1, const double *b1,
@@ -293,5 +185,290 @@ __global__ void k_update_p_b(double *p, const double *z, double *pw, const doubl
     const double v = first ? z[o + i] : z[o + i] + beta * p[o + i];
     p[o + i] = v;
     pw[o + i] = v * bw[i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Right-hand-side-minor projections.  For a group of up to 32 G right-hand
+// sides, p.detw and the map are stored transposed, [baseline][32 G] and
+// [pixel][nmap][32 G], so that the lanes of a warp hold 32 G right-hand
+// sides of ONE sample: a pointing record is read once (a shared-memory
+// broadcast) and its lookups are coalesced 256-byte rows instead of one
+// scattered 8-byte load per sample and right-hand side.  Each right-hand
+// side sees the arithmetic of k_scatter_chunks / k_gather_chunks in the same
+// order, so its map and baseline sums equal theirs to the bit.
+
+// [R][nb] (right-hand sides r0 .. r0 + nr) -> [nb][32 G], zero padded
+template <int G>
+__global__ void k_transpose_rhs(const double *__restrict__ src, long long nb, int r0, int nr,
+                                double *__restrict__ dst) {
+  constexpr int GW = 32 * G;
+  __shared__ double t[32][33];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+  const int g = blockIdx.y;
+  for (long long b0 = (long long)blockIdx.x * 32; b0 < nb; b0 += (long long)gridDim.x * 32) {
+    for (int rr = ty; rr < 32; rr += 8) {
+      const int r = g * 32 + rr;
+      const long long b = b0 + tx;
+      t[rr][tx] = (r < nr && b < nb) ? src[(long long)(r0 + r) * nb + b] : 0.0;
+    }
+    __syncthreads();
+    for (int bb = ty; bb < 32; bb += 8) {
+      const long long b = b0 + bb;
+      if (b < nb) dst[b * GW + g * 32 + tx] = t[tx][bb];
+    }
+    __syncthreads();
+  }
+}
+
+__host__ __device__ constexpr int cpopc5(int x) {
+  return (x & 1) + ((x >> 1) & 1) + ((x >> 2) & 1) + ((x >> 3) & 1) + ((x >> 4) & 1);
+}
+__host__ __device__ constexpr int ctrail1(int x) { return (x & 1) ? 1 + ctrail1(x >> 1) : 0; }
+__host__ __device__ constexpr int cbrev5(int x) {
+  return ((x & 1) << 4) | ((x & 2) << 2) | (x & 4) | ((x & 8) >> 2) | ((x & 16) >> 4);
+}
+
+// baseline_to_map over the pixel-sorted chunks of k_scatter_chunks.  There,
+// lane L adds entries L, L + 32, ... and a xor butterfly adds the 32 lane
+// sums; the butterfly's association (as lane 0 holds it) is a balanced
+// binary tree over the lane sums in bit-reversed lane order.  Here lane r
+// forms right-hand side r's lane sums one column at a time in that order and
+// combines them on a binary-counter stack, which rebuilds the same tree.
+template <int NMAP, int G>
+__global__ void __launch_bounds__(256) k_scatter_T(
+    const int4 *__restrict__ chunks, long long nchunks, const float4 *__restrict__ sp4,
+    const int2 *__restrict__ sp2, const double *__restrict__ pwT, double *__restrict__ target,
+    double *__restrict__ partial) {
+  constexpr int GW = 32 * G;
+  constexpr int U = kScatterChunk / 32;
+  __shared__ float4 rec[8][kScatterChunk];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  float4 *rw = rec[wid];
+  for (long long c = w0; c < nchunks; c += nwarps) {
+    const int4 ck = chunks[c];  // {pixel, first entry, entries, partial slot or -1}
+#pragma unroll
+    for (int r = 0; r < U; ++r) {
+      const int i = r * 32 + lane;
+      if (i < ck.z)
+        rw[i] = NMAP == 3 ? __ldcs(sp4 + ck.y + i)
+                          : make_float4(1.f, 0.f, 0.f, __int_as_float(__ldcs(&sp2[ck.y + i].x)));
+    }
+    __syncwarp();
+    double S[6][G][NMAP];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      const int L = cbrev5(i);
+      double P[G][NMAP];
+#pragma unroll
+      for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int e = 0; e < NMAP; ++e) P[g][e] = 0.0;
+#pragma unroll
+      for (int r = 0; r < U; ++r) {
+        const int e0 = r * 32 + L;
+        if (e0 < ck.z) {
+          const float4 q = rw[e0];
+          const double *pk = pwT + (long long)__float_as_int(q.w) * GW + lane;
+#pragma unroll
+          for (int g = 0; g < G; ++g) {
+            const double wv = __ldg(pk + g * 32);
+            if (NMAP == 3) {
+              P[g][0] = fma((double)q.x, wv, P[g][0]);
+              P[g][1] = fma((double)q.y, wv, P[g][1]);
+              P[g][2] = fma((double)q.z, wv, P[g][2]);
+            } else {
+              P[g][0] += wv;
+            }
+          }
+        }
+      }
+      // push column i's sum, then carry as a binary counter does
+      const int pos = cpopc5(i);
+#pragma unroll
+      for (int g = 0; g < G; ++g)
+#pragma unroll
+        for (int e = 0; e < NMAP; ++e) S[pos][g][e] = P[g][e];
+      const int t = ctrail1(i);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        if (k < t) {
+          const int lo = pos - 1 - k;
+#pragma unroll
+          for (int g = 0; g < G; ++g)
+#pragma unroll
+            for (int e = 0; e < NMAP; ++e) S[lo][g][e] = S[lo][g][e] + S[lo + 1][g][e];
+        }
+      }
+    }
+    double *o = ck.w < 0 ? target + (long long)ck.x * NMAP * GW
+                         : partial + (long long)ck.w * NMAP * GW;
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int e = 0; e < NMAP; ++e) o[e * GW + g * 32 + lane] = S[0][g][e];
+    __syncwarp();
+  }
+}
+
+// multi-chunk pixels {pixel, first partial slot, chunks}: partial sums added
+// in chunk order; thread per (pixel, component, right-hand side)
+template <int NMAP, int G>
+__global__ void k_scatter_combine_T(const int4 *__restrict__ multi, int nmulti,
+                                    const double *__restrict__ partial,
+                                    double *__restrict__ target) {
+  constexpr int GW = 32 * G;
+  const long long total = (long long)nmulti * NMAP * GW;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t / (NMAP * GW));
+    const int ce = (int)(t - (long long)i * NMAP * GW);
+    const int4 mp = multi[i];
+    double a = 0.0;
+    for (int c = 0; c < mp.z; ++c) a += partial[(long long)(mp.y + c) * NMAP * GW + ce];
+    target[(long long)mp.x * NMAP * GW + ce] = a;
+  }
+}
+
+// ccmultiply on the transposed map; thread per (pixel, right-hand side)
+template <int NMAP, int G>
+__global__ void k_ccmult_T(const double *__restrict__ cc, double *__restrict__ m, long long n) {
+  constexpr int GW = 32 * G;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n * GW;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long p = t / GW;
+    const int r = (int)(t - p * GW);
+    double *v = m + p * NMAP * GW + r;
+    if (NMAP == 1) {
+      const double c = cc[p];
+      v[0] = (c == 0) ? 0.0 : c * v[0];
+    } else {
+      const double *c = cc + p * 6;
+      if (c[0] == 0) {
+        v[0] = v[GW] = v[2 * GW] = 0;
+      } else {
+        const double a = v[0], b = v[GW], d = v[2 * GW];
+        v[0] = fma(c[2], d, fma(c[1], b, c[0] * a));
+        v[GW] = fma(c[4], d, fma(c[3], b, c[1] * a));
+        v[2 * GW] = fma(c[5], d, fma(c[4], b, c[2] * a));
+      }
+    }
+  }
+}
+
+// map_to_baseline sums per baseline and right-hand side, in time order as
+// lane j of k_gather_chunks adds baseline j: apnT[b][r] = sum_s w_s . m_r[p_s]
+template <int NMAP, int G>
+__global__ void __launch_bounds__(256) k_gather_T(
+    const int2 *__restrict__ chunks, long long nchunks, const float4 *__restrict__ p4,
+    const int32_t *__restrict__ pc, const uint32_t *__restrict__ bstart, long noba,
+    long long nsamp, const double *__restrict__ mT, int deg_shift, int nloc,
+    double *__restrict__ apnT) {
+  constexpr int GW = 32 * G;
+  constexpr int U = kGatherChunk / 32;
+  __shared__ float4 rec[8][kGatherChunk];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  float4 *rw = rec[wid];
+  for (long long c = w0; c < nchunks; c += nwarps) {
+    const int2 ck = chunks[c];
+    const long long det = ck.x / noba, k0 = ck.x - det * noba;
+    const int s0 = (int)bstart[k0];
+    const int n = (int)(bstart[k0 + ck.y] - s0);
+    const long long base = det * nsamp + s0;
+#pragma unroll
+    for (int r = 0; r < U; ++r) {
+      const int i = r * 32 + lane;
+      if (i < n)
+        rw[i] = NMAP == 3 ? __ldcs(p4 + base + i)
+                          : make_float4(0.f, 0.f, 0.f, __int_as_float(__ldcs(pc + base + i)));
+    }
+    __syncwarp();
+    int a1 = 0;
+    for (int j = 0; j < ck.y; ++j) {
+      const int a0 = a1;
+      a1 = (int)(bstart[k0 + j + 1] - s0);
+      double apn[G];
+#pragma unroll
+      for (int g = 0; g < G; ++g) apn[g] = 0.0;
+#pragma unroll 4
+      for (int s = a0; s < a1; ++s) {
+        const float4 q = rw[s];
+        const int px = __float_as_int(q.w);
+        if (px < nloc) {
+          const double *mm = mT + (long long)(px >> deg_shift) * NMAP * GW + lane;
+#pragma unroll
+          for (int g = 0; g < G; ++g) {
+            if (NMAP == 3) {
+              const double m0 = __ldg(mm + g * 32), m1 = __ldg(mm + GW + g * 32),
+                           m2 = __ldg(mm + 2 * GW + g * 32);
+              apn[g] += fma((double)q.z, m2, fma((double)q.y, m1, (double)q.x * m0));
+            } else {
+              apn[g] += __ldg(mm + g * 32);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int g = 0; g < G; ++g) apn[g] += 0.0;
+        }
+      }
+#pragma unroll
+      for (int g = 0; g < G; ++g) apnT[(long long)(ck.x + j) * GW + g * 32 + lane] = apn[g];
+    }
+    __syncwarp();
+  }
+}
+
+// ap[r][b] = ap + (nna p - apn detw) for the group's right-hand sides and the
+// p.ap partial sums per block; a block transposes tiles of 32 baselines
+template <int G>
+__global__ void __launch_bounds__(256) k_gather_finish_T(
+    const double *__restrict__ apnT, long long nb, const double *__restrict__ bw,
+    const double *__restrict__ nna, const uint8_t *__restrict__ rmask,
+    const double *__restrict__ p, double *__restrict__ ap, int r0, int nr,
+    double *__restrict__ part) {
+  constexpr int GW = 32 * G;
+  constexpr int RPW = GW / 8;  // right-hand sides per warp
+  __shared__ double t[32][GW + 1];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double pap[RPW];
+#pragma unroll
+  for (int k = 0; k < RPW; ++k) pap[k] = 0.0;
+  for (long long b0 = (long long)blockIdx.x * 32; b0 < nb; b0 += (long long)gridDim.x * 32) {
+    for (int idx = threadIdx.x; idx < 32 * GW; idx += blockDim.x) {
+      const int bl = idx / GW, r = idx - bl * GW;
+      t[bl][r] = b0 + bl < nb ? apnT[(b0 + bl) * GW + r] : 0.0;
+    }
+    __syncthreads();
+    const long long b = b0 + lane;
+    if (b < nb) {
+      const double detw = bw[b], nn = nna[b];
+      const bool rm = rmask[b] != 0;
+#pragma unroll
+      for (int k = 0; k < RPW; ++k) {
+        const int r = wid + 8 * k;
+        if (r < nr) {
+          const long long o = (long long)(r0 + r) * nb + b;
+          const double pb = p[o], apb = ap[o];
+          if (detw == 0) {
+            if (rm) pap[k] += pb * apb;
+          } else {
+            const double val = apb + fma(-t[lane][r], detw, nn * pb);
+            ap[o] = val;
+            if (rm) pap[k] += pb * val;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int k = 0; k < RPW; ++k) {
+    const int r = wid + 8 * k;
+    const double s = warp_sum(pap[k]);
+    if (lane == 0 && r < nr) part[(long long)(r0 + r) * 3 * kRedBlocks + blockIdx.x] = s;
   }
 }

@@ -456,9 +456,9 @@ __global__ void k_ccmult_copy(const double *cc, double *m, long long n, double2 
     double tm = 0, qm = 0, um = 0;
     if (c[0] != 0) {
       const double a = v[0], b = v[1], d = v[2];
-      tm = c[0] * a + c[1] * b + c[2] * d;
-      qm = c[1] * a + c[3] * b + c[4] * d;
-      um = c[2] * a + c[4] * b + c[5] * d;
+      tm = fma(c[2], d, fma(c[1], b, c[0] * a));
+      qm = fma(c[4], d, fma(c[3], b, c[1] * a));
+      um = fma(c[5], d, fma(c[4], b, c[2] * a));
     }
     v[0] = tm;
     v[1] = qm;
@@ -691,12 +691,12 @@ __global__ void __launch_bounds__(256) k_gather_tiled(
 __device__ __forceinline__ double map_dot(const double2 *__restrict__ mg, long long cp,
                                           const float4 &q) {
   const double2 a = __ldg(mg + 2 * cp), b = __ldg(mg + 2 * cp + 1);
-  return (double)q.x * a.x + (double)q.y * a.y + (double)q.z * b.x;
+  return fma((double)q.z, b.x, fma((double)q.y, a.y, (double)q.x * a.x));
 }
 __device__ __forceinline__ double map_dot(const float4 *__restrict__ mf, long long cp,
                                           const float4 &q) {
   const float4 a = __ldg(mf + cp);
-  return (double)q.x * a.x + (double)q.y * a.y + (double)q.z * a.z;
+  return fma((double)q.z, (double)a.z, fma((double)q.y, (double)a.y, (double)q.x * a.x));
 }
 
 // Per-baseline sums of a warp chunk of at most kGatherChunk staged values
@@ -857,7 +857,7 @@ __global__ void __launch_bounds__(256) k_gather_chunks(
       } else {
         double apn = 0;
         for (int i = a0; i < a1; ++i) apn += vb[i];
-        const double val = apb + (npb - apn * detw);
+        const double val = apb + fma(-apn, detw, npb);
         ap[b] = val;
         if (rm) pap += pb * val;
       }
@@ -905,9 +905,9 @@ __global__ void __launch_bounds__(256) k_scatter_chunks(
       }
 #pragma unroll
       for (int r = 0; r < U; ++r) {
-        a0 += (double)q[r].x * wv[r];
-        a1 += (double)q[r].y * wv[r];
-        a2 += (double)q[r].z * wv[r];
+        a0 = fma((double)q[r].x, wv[r], a0);
+        a1 = fma((double)q[r].y, wv[r], a1);
+        a2 = fma((double)q[r].z, wv[r], a2);
       }
     } else {
       int k[U];

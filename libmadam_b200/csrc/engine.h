@@ -171,6 +171,9 @@ class Engine {
   void apply_A_batch();
   void apply_preconditioner_batch(const double *r, double *z);
   void build_batch_tables();
+  template <int G>
+  void project_group_T(long r0, int nr);
+  DevBuf<double> pwT_, lmapT_, scatpT_, apnT_;  // right-hand-side-minor copies
   long nrhs_ = 0;                        // right-hand sides of the last batch
   DevBuf<double> yb_, aab_, rb_, pb_, zb_, apb_, rob_, pwb_;  // [R][nb]
   DevBuf<double> lmapb_, scatpb_;        // [R][nloc_cross][nmap], scatter partials

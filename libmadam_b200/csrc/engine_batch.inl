@@ -13,9 +13,7 @@
 // realisation).  The per-realisation arithmetic is that of the single solve.
 
 namespace {
-constexpr int kScatterGroup = 8;  // right-hand sides per scatter pass
-constexpr int kGatherGroup = 4;   // right-hand sides per gather pass
-constexpr size_t kGatherGroupSmem = (size_t)8 * kGatherGroup * kGatherChunk * sizeof(double);
+constexpr int kScatterGroup = 8;  // right-hand sides per scatter pass (long baselines)
 }  // namespace
 
 void Engine::build_batch_tables() {
@@ -115,12 +113,93 @@ void Engine::apply_preconditioner_batch(const double *r, double *z) {
   }
 }
 
+template <int G>
+void Engine::project_group_T(long r0, int nr) {
+  // A p's projections for right-hand sides [r0, r0 + nr), nr <= 32 G, on
+  // right-hand-side-minor copies (batch_kernels.inl)
+  constexpr int GW = 32 * G;
+  const long long nb = (long long)ndet_ * noba_short_;
+  const long long ncross = std::max<long>(1, nloc_cross_);
+  pwT_.alloc((size_t)nb * GW);
+  lmapT_.alloc((size_t)ncross * nmap_ * GW);
+  scatpT_.alloc((size_t)std::max<size_t>(1, scatter_partial_.n / nmap_) * nmap_ * GW);
+  apnT_.alloc((size_t)nb * GW);
+  const unsigned tb = (unsigned)std::min<long long>(4736, (nb + 31) / 32);
+  MADAM_LAUNCH(k_transpose_rhs<G>, dim3(tb, G), 256, 0, st_, pwb_.get(), nb, (int)r0, nr,
+               pwT_.get());
+  // 1) baseline -> map, combine, ccmultiply
+  if (nloc_cross_ > 0 && nscatter_chunks_ > 0) {
+    if (nmap_ == 3)
+      MADAM_LAUNCH((k_scatter_T<3, G>), kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
+                   nscatter_chunks_, sp4_.get(), sp2_.get(), pwT_.get(), lmapT_.get(),
+                   scatpT_.get());
+    else
+      MADAM_LAUNCH((k_scatter_T<1, G>), kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
+                   nscatter_chunks_, sp4_.get(), sp2_.get(), pwT_.get(), lmapT_.get(),
+                   scatpT_.get());
+    if (nscatter_multi_ > 0) {
+      const long long tot = (long long)nscatter_multi_ * nmap_ * GW;
+      if (nmap_ == 3)
+        MADAM_LAUNCH((k_scatter_combine_T<3, G>), grid_for(tot), 256, 0, st_,
+                     scatter_multi_.get(), nscatter_multi_, scatpT_.get(), lmapT_.get());
+      else
+        MADAM_LAUNCH((k_scatter_combine_T<1, G>), grid_for(tot), 256, 0, st_,
+                     scatter_multi_.get(), nscatter_multi_, scatpT_.get(), lmapT_.get());
+    }
+  }
+  if (nloc_cross_ > 0) {
+    if (nmap_ == 3)
+      MADAM_LAUNCH((k_ccmult_T<3, G>), grid_for((long long)nloc_cross_ * GW), 256, 0, st_,
+                   cca_.get(), lmapT_.get(), (long long)nloc_cross_);
+    else
+      MADAM_LAUNCH((k_ccmult_T<1, G>), grid_for((long long)nloc_cross_ * GW), 256, 0, st_,
+                   cca_.get(), lmapT_.get(), (long long)nloc_cross_);
+  }
+  // 3) map -> baseline sums, then ap and p.ap per right-hand side
+  if (nmap_ == 3)
+    MADAM_LAUNCH((k_gather_T<3, G>), kRedBlocks, 256, 0, st_, gather_chunks_.get(),
+                 ngather_chunks_, point4_.get(), pixc_.get(), bstart_d_.get(), noba_short_,
+                 nsamp_, lmapT_.get(), (int)ndeg_shift_, (int)nloc_, apnT_.get());
+  else
+    MADAM_LAUNCH((k_gather_T<1, G>), kRedBlocks, 256, 0, st_, gather_chunks_.get(),
+                 ngather_chunks_, point4_.get(), pixc_.get(), bstart_d_.get(), noba_short_,
+                 nsamp_, lmapT_.get(), (int)ndeg_shift_, (int)nloc_, apnT_.get());
+  MADAM_LAUNCH(k_gather_finish_T<G>, kRedBlocks, 256, 0, st_, apnT_.get(), nb, bw_.get(),
+               nna_.get(), rmask_.get(), pb_.get(), apb_.get(), (int)r0, nr, partb_.get());
+}
+
 void Engine::apply_A_batch() {
   // A p for every right-hand side (iterate_a 798-878)
   const long long nb = (long long)ndet_ * noba_short_;
   const long long tstride = (long long)std::max<long>(1, nloc_cross_) * nmap_;
   const long long pstride = (long long)scatter_partial_.n;
-  // 1) baseline -> map, combine, ccmultiply
+  // noise prior ap = C_a^-1 p (cinvmul, 829-845); the projections add to it
+  const long long nt = nb * nrhs_;
+  if (par_.kfilter) {
+    MADAM_CUDA(cudaMemcpyAsync(apb_.get(), pb_.get(), nt * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st_));
+    const long nfs = (long)filt_segs_.size() * nrhs_;
+    if (nfs > 0) fft_->convolve(st_, filt_segs_b_d_.get(), nfs, fcov_.get(), pb_.get(), apb_.get());
+  } else if (par_.diagfilter != 0) {
+    for (long k = 0; k < nrhs_; ++k)
+      MADAM_LAUNCH(k_diagfilter, grid_for(nb), 256, 0, st_, apb_.get() + k * nb, nna_.get(),
+                   pb_.get() + k * nb, par_.diagfilter, nb);
+  } else {
+    MADAM_CUDA(cudaMemsetAsync(apb_.get(), 0, nt * sizeof(double), st_));
+  }
+  if (ngather_chunks_ > 0) {
+    // right-hand-side-minor projections, 64 right-hand sides a pass
+    for (long r0 = 0; r0 < nrhs_; r0 += 64) {
+      const int nr = (int)std::min<long>(64, nrhs_ - r0);
+      if (nr > 32) project_group_T<2>(r0, nr);
+      else project_group_T<1>(r0, nr);
+    }
+    MADAM_LAUNCH(k_finish_b, (unsigned)nrhs_, 1024, 0, st_, partb_.get(), kRedBlocks, 1,
+                 scalb_.get(), 1, 0, actb_.get());
+    return;
+  }
+  // baselines longer than a gather chunk: right-hand-side-major scatter,
+  // single-RHS gathers
   if (nloc_cross_ > 0 && nscatter_chunks_ > 0) {
     for (long r0 = 0; r0 < nrhs_; r0 += kScatterGroup) {
       const int nr = (int)std::min<long>(kScatterGroup, nrhs_ - r0);
@@ -154,72 +233,28 @@ void Engine::apply_A_batch() {
       MADAM_LAUNCH(k_ccmult_b<1>, g, 256, 0, st_, cca_.get(), lmapb_.get(),
                    (long long)nloc_cross_);
   }
-  // 2) noise prior ap = C_a^-1 p (cinvmul, 829-845)
-  const long long nt = nb * nrhs_;
-  if (par_.kfilter) {
-    MADAM_CUDA(cudaMemcpyAsync(apb_.get(), pb_.get(), nt * sizeof(double),
-                               cudaMemcpyDeviceToDevice, st_));
-    const long nfs = (long)filt_segs_.size() * nrhs_;
-    if (nfs > 0) fft_->convolve(st_, filt_segs_b_d_.get(), nfs, fcov_.get(), pb_.get(), apb_.get());
-  } else if (par_.diagfilter != 0) {
-    for (long k = 0; k < nrhs_; ++k)
-      MADAM_LAUNCH(k_diagfilter, grid_for(nb), 256, 0, st_, apb_.get() + k * nb, nna_.get(),
-                   pb_.get() + k * nb, par_.diagfilter, nb);
-  } else {
-    MADAM_CUDA(cudaMemsetAsync(apb_.get(), 0, nt * sizeof(double), st_));
-  }
-  // 3) map -> baseline and p.ap (849-878)
-  if (ngather_chunks_ > 0) {
-    static bool attr = false;
-    if (!attr) {
-      MADAM_CUDA(cudaFuncSetAttribute(k_gather_chunks_b<3, kGatherGroup>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kGatherGroupSmem));
-      MADAM_CUDA(cudaFuncSetAttribute(k_gather_chunks_b<1, kGatherGroup>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kGatherGroupSmem));
-      attr = true;
-    }
-    for (long r0 = 0; r0 < nrhs_; r0 += kGatherGroup) {
-      const int nr = (int)std::min<long>(kGatherGroup, nrhs_ - r0);
+  for (long k = 0; k < nrhs_; ++k) {
+    double *pk = pb_.get() + k * nb, *apk = apb_.get() + k * nb;
+    double *mk = lmapb_.get() + k * tstride, *partk = partb_.get() + k * 3 * kRedBlocks;
+    if (gather_kb_ > 0) {
       if (nmap_ == 3)
-        MADAM_LAUNCH((k_gather_chunks_b<3, kGatherGroup>), kRedBlocks, 256, kGatherGroupSmem, st_,
-                     gather_chunks_.get(), ngather_chunks_, point4_.get(), pixc_.get(),
-                     bstart_d_.get(), noba_short_, nsamp_, bw_.get(), pb_.get(), nb, nna_.get(),
-                     lmapb_.get(), tstride, (int)ndeg_shift_, (int)nloc_, rmask_.get(),
-                     apb_.get(), (int)r0, nr, partb_.get());
+        MADAM_LAUNCH(k_gather_tiled<3>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
+                     bstart_d_.get(), noba_short_, nsamp_, gather_kb_, gather_tiles_det_,
+                     (int)ndet_, bw_.get(), pk, nna_.get(), mk, (int)ndeg_shift_, (int)nloc_,
+                     rmask_.get(), apk, partk);
       else
-        MADAM_LAUNCH((k_gather_chunks_b<1, kGatherGroup>), kRedBlocks, 256, kGatherGroupSmem, st_,
-                     gather_chunks_.get(), ngather_chunks_, point4_.get(), pixc_.get(),
-                     bstart_d_.get(), noba_short_, nsamp_, bw_.get(), pb_.get(), nb, nna_.get(),
-                     lmapb_.get(), tstride, (int)ndeg_shift_, (int)nloc_, rmask_.get(),
-                     apb_.get(), (int)r0, nr, partb_.get());
-    }
-  } else {
-    // long baselines: the single-RHS gathers, one right-hand side at a time
-    for (long k = 0; k < nrhs_; ++k) {
-      double *pk = pb_.get() + k * nb, *apk = apb_.get() + k * nb;
-      double *mk = lmapb_.get() + k * tstride, *partk = partb_.get() + k * 3 * kRedBlocks;
-      if (gather_kb_ > 0) {
-        if (nmap_ == 3)
-          MADAM_LAUNCH(k_gather_tiled<3>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
-                       bstart_d_.get(), noba_short_, nsamp_, gather_kb_, gather_tiles_det_,
-                       (int)ndet_, bw_.get(), pk, nna_.get(), mk, (int)ndeg_shift_, (int)nloc_,
-                       rmask_.get(), apk, partk);
-        else
-          MADAM_LAUNCH(k_gather_tiled<1>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
-                       bstart_d_.get(), noba_short_, nsamp_, gather_kb_, gather_tiles_det_,
-                       (int)ndet_, bw_.get(), pk, nna_.get(), mk, (int)ndeg_shift_, (int)nloc_,
-                       rmask_.get(), apk, partk);
-      } else if (nmap_ == 3) {
-        MADAM_LAUNCH(k_gather<3>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
-                     bstart_d_.get(), nb, noba_short_, nsamp_, bw_.get(), pk, nna_.get(), mk,
-                     (int)ndeg_shift_, (int)nloc_, rmask_.get(), apk, partk);
-      } else {
-        MADAM_LAUNCH(k_gather<1>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
-                     bstart_d_.get(), nb, noba_short_, nsamp_, bw_.get(), pk, nna_.get(), mk,
-                     (int)ndeg_shift_, (int)nloc_, rmask_.get(), apk, partk);
-      }
+        MADAM_LAUNCH(k_gather_tiled<1>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
+                     bstart_d_.get(), noba_short_, nsamp_, gather_kb_, gather_tiles_det_,
+                     (int)ndet_, bw_.get(), pk, nna_.get(), mk, (int)ndeg_shift_, (int)nloc_,
+                     rmask_.get(), apk, partk);
+    } else if (nmap_ == 3) {
+      MADAM_LAUNCH(k_gather<3>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
+                   bstart_d_.get(), nb, noba_short_, nsamp_, bw_.get(), pk, nna_.get(), mk,
+                   (int)ndeg_shift_, (int)nloc_, rmask_.get(), apk, partk);
+    } else {
+      MADAM_LAUNCH(k_gather<1>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
+                   bstart_d_.get(), nb, noba_short_, nsamp_, bw_.get(), pk, nna_.get(), mk,
+                   (int)ndeg_shift_, (int)nloc_, rmask_.get(), apk, partk);
     }
   }
   MADAM_LAUNCH(k_finish_b, (unsigned)nrhs_, 1024, 0, st_, partb_.get(), kRedBlocks, 1,

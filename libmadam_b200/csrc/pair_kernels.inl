@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(256) k_gather_pairs(
       if (detw == 0) {
         if (rm) pap += pb * apb;
       } else {
-        const double val = apb + (npb - cs.bsum[lane] * detw);
+        const double val = apb + fma(-cs.bsum[lane], detw, npb);
         ap[b] = val;
         if (rm) pap += pb * val;
       }
