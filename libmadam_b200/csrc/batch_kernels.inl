@@ -233,14 +233,18 @@ __host__ __device__ constexpr int cbrev5(int x) {
 // lane L adds entries L, L + 32, ... and a xor butterfly adds the 32 lane
 // sums; the butterfly's association (as lane 0 holds it) is a balanced
 // binary tree over the lane sums in bit-reversed lane order.  Here lane r
-// forms right-hand side r's lane sums one column at a time in that order and
-// combines them on a binary-counter stack, which rebuilds the same tree.
-template <int NMAP, int G>
+// forms right-hand side r's lane sums one column at a time in that order:
+// four subtrees of 8 columns each (unrolled, on a binary-counter stack),
+// then ((X0 + X1) + (X2 + X3)) - the same tree.  Keeping the unrolled part
+// to 8 columns keeps the kernel's code small enough for the instruction
+// cache.  One launch covers the 32 right-hand sides g0 .. g0 + 31 of rows
+// of GW.
+template <int NMAP, int GW>
 __global__ void __launch_bounds__(256) k_scatter_T(
     const int4 *__restrict__ chunks, long long nchunks, const float4 *__restrict__ sp4,
-    const int2 *__restrict__ sp2, const double *__restrict__ pwT, double *__restrict__ target,
-    double *__restrict__ partial) {
-  constexpr int GW = 32 * G;
+    const int2 *__restrict__ sp2, const double *__restrict__ pwT, int g0,
+    double *__restrict__ target, double *__restrict__ partial) {
+  constexpr int G = 1;
   constexpr int U = kScatterChunk / 32;
   __shared__ float4 rec[8][kScatterChunk];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -257,58 +261,74 @@ __global__ void __launch_bounds__(256) k_scatter_T(
                           : make_float4(1.f, 0.f, 0.f, __int_as_float(__ldcs(&sp2[ck.y + i].x)));
     }
     __syncwarp();
-    double S[6][G][NMAP];
+    double B0[G][NMAP], B1[G][NMAP];
+#pragma unroll 1
+    for (int o = 0; o < 4; ++o) {
+      // columns i = 8 o + j, lanes L = bitrev5(i) = 4 bitrev3(j) + bitrev2(o)
+      const int lo2 = ((o & 1) << 1) | (o >> 1);
+      double S[4][G][NMAP];
 #pragma unroll
-    for (int i = 0; i < 32; ++i) {
-      const int L = cbrev5(i);
-      double P[G][NMAP];
+      for (int jj = 0; jj < 8; ++jj) {
+        const int L = (cbrev5(jj) >> 0) + lo2;  // cbrev5(jj) = 4 bitrev3(jj) for jj < 8
+        double P[G][NMAP];
 #pragma unroll
-      for (int g = 0; g < G; ++g)
+        for (int g = 0; g < G; ++g)
 #pragma unroll
-        for (int e = 0; e < NMAP; ++e) P[g][e] = 0.0;
+          for (int e = 0; e < NMAP; ++e) P[g][e] = 0.0;
 #pragma unroll
-      for (int r = 0; r < U; ++r) {
-        const int e0 = r * 32 + L;
-        if (e0 < ck.z) {
-          const float4 q = rw[e0];
-          const double *pk = pwT + (long long)__float_as_int(q.w) * GW + lane;
+        for (int r = 0; r < U; ++r) {
+          const int e0 = r * 32 + L;
+          if (e0 < ck.z) {
+            const float4 q = rw[e0];
+            const double *pk = pwT + (long long)__float_as_int(q.w) * GW + g0 + lane;
 #pragma unroll
-          for (int g = 0; g < G; ++g) {
-            const double wv = __ldg(pk + g * 32);
-            if (NMAP == 3) {
-              P[g][0] = fma((double)q.x, wv, P[g][0]);
-              P[g][1] = fma((double)q.y, wv, P[g][1]);
-              P[g][2] = fma((double)q.z, wv, P[g][2]);
-            } else {
-              P[g][0] += wv;
+            for (int g = 0; g < G; ++g) {
+              const double wv = __ldg(pk + g * 32);
+              if (NMAP == 3) {
+                P[g][0] = fma((double)q.x, wv, P[g][0]);
+                P[g][1] = fma((double)q.y, wv, P[g][1]);
+                P[g][2] = fma((double)q.z, wv, P[g][2]);
+              } else {
+                P[g][0] += wv;
+              }
             }
           }
         }
+        // push column jj's sum, then carry as a binary counter does
+        const int pos = cpopc5(jj);
+#pragma unroll
+        for (int g = 0; g < G; ++g)
+#pragma unroll
+          for (int e = 0; e < NMAP; ++e) S[pos][g][e] = P[g][e];
+        const int t = ctrail1(jj);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          if (k < t) {
+            const int lv = pos - 1 - k;
+#pragma unroll
+            for (int g = 0; g < G; ++g)
+#pragma unroll
+              for (int e = 0; e < NMAP; ++e) S[lv][g][e] = S[lv][g][e] + S[lv + 1][g][e];
+          }
+        }
       }
-      // push column i's sum, then carry as a binary counter does
-      const int pos = cpopc5(i);
 #pragma unroll
       for (int g = 0; g < G; ++g)
 #pragma unroll
-        for (int e = 0; e < NMAP; ++e) S[pos][g][e] = P[g][e];
-      const int t = ctrail1(i);
-#pragma unroll
-      for (int k = 0; k < 5; ++k) {
-        if (k < t) {
-          const int lo = pos - 1 - k;
-#pragma unroll
-          for (int g = 0; g < G; ++g)
-#pragma unroll
-            for (int e = 0; e < NMAP; ++e) S[lo][g][e] = S[lo][g][e] + S[lo + 1][g][e];
+        for (int e = 0; e < NMAP; ++e) {
+          const double x = S[0][g][e];
+          if (o == 0) B0[g][e] = x;
+          else if (o == 1) B0[g][e] = B0[g][e] + x;
+          else if (o == 2) B1[g][e] = x;
+          else B1[g][e] = B1[g][e] + x;
         }
-      }
     }
-    double *o = ck.w < 0 ? target + (long long)ck.x * NMAP * GW
-                         : partial + (long long)ck.w * NMAP * GW;
+    double *out = ck.w < 0 ? target + (long long)ck.x * NMAP * GW
+                           : partial + (long long)ck.w * NMAP * GW;
 #pragma unroll
     for (int g = 0; g < G; ++g)
 #pragma unroll
-      for (int e = 0; e < NMAP; ++e) o[e * GW + g * 32 + lane] = S[0][g][e];
+      for (int e = 0; e < NMAP; ++e) out[e * GW + g0 + g * 32 + lane] = B0[g][e] + B1[g][e];
     __syncwarp();
   }
 }

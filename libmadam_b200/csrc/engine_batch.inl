@@ -129,14 +129,17 @@ void Engine::project_group_T(long r0, int nr) {
                pwT_.get());
   // 1) baseline -> map, combine, ccmultiply
   if (nloc_cross_ > 0 && nscatter_chunks_ > 0) {
-    if (nmap_ == 3)
-      MADAM_LAUNCH((k_scatter_T<3, G>), kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
-                   nscatter_chunks_, sp4_.get(), sp2_.get(), pwT_.get(), lmapT_.get(),
-                   scatpT_.get());
-    else
-      MADAM_LAUNCH((k_scatter_T<1, G>), kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
-                   nscatter_chunks_, sp4_.get(), sp2_.get(), pwT_.get(), lmapT_.get(),
-                   scatpT_.get());
+    // one launch per 32 right-hand sides (fewer registers, more warps)
+    for (int g0 = 0; g0 < GW; g0 += 32) {
+      if (nmap_ == 3)
+        MADAM_LAUNCH((k_scatter_T<3, GW>), kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
+                     nscatter_chunks_, sp4_.get(), sp2_.get(), pwT_.get(), g0, lmapT_.get(),
+                     scatpT_.get());
+      else
+        MADAM_LAUNCH((k_scatter_T<1, GW>), kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
+                     nscatter_chunks_, sp4_.get(), sp2_.get(), pwT_.get(), g0, lmapT_.get(),
+                     scatpT_.get());
+    }
     if (nscatter_multi_ > 0) {
       const long long tot = (long long)nscatter_multi_ * nmap_ * GW;
       if (nmap_ == 3)
