@@ -220,8 +220,11 @@ def reference_arm(args, world, rank):
 
 def run_mc(args, world, rank, local):
     """Batched Monte Carlo form (nside 512, 32 detectors x 2^22 samples, nrhs
-    noise-only realisations sharing one pointing): the multi-right-hand-side
-    solve against the same realisations one destripe_with_cache at a time."""
+    noise-only realisations sharing one pointing).  The headline is the
+    FP32-TOD multi-right-hand-side solve (float32 realisations, float64
+    pixel matrices and reductions); beside it the float64 batched solve of the
+    same realisations, the error between the two, and the plain float64
+    destripe_with_cache of one realisation at a time."""
     import torch
     from libmadam_b200 import libmadam_wrapper as W
     from libmadam_b200 import synthetic as syn
@@ -238,35 +241,59 @@ def run_mc(args, world, rank, local):
     psd = (d["periods"], d["npsd"], d["psdstarts"], d["psdfreqs"], d["psdvals"])
     W.destripe(None, pars, d["dets"], d["detweights"], d["timestamps"], pix.clone(), wts,
                sigs[R].reshape(-1).clone(), *psd)
-    # one realisation at a time (the reference's way), then all at once
+    # one realisation at a time (the reference's way), float64
     barrier(world)
-    clk = Clocks(local)
     W.destripe_with_cache(None, d["timestamps"], pix.clone(), wts, sigs[0].reshape(-1).clone(), b"")
     t1 = W.timings()
     it1 = int(W.scalars()["noiter"])
     single = n * it1 / (t1["iterate_ms"] * 1e-3)
+    # all at once, float64
     W.destripe_with_cache_batch(None, d["timestamps"], pix.clone(), wts, sigs[:R])
+    torch.cuda.synchronize()
+    t64 = W.timings()
+    its64 = W.get_result("noiter_batch")
+    aa64 = W.get_result("aa_batch")
+    map64 = W.get_result("map_batch")
+    value64 = world * n * float(its64.sum()) / (reduce_max(t64["iterate_ms"], world) * 1e-3)
+    # all at once, FP32-TOD form (the headline)
+    s32 = sigs[:R].float()
+    del sigs
+    torch.cuda.empty_cache()
+    barrier(world)
+    clk = Clocks(local)
+    W.destripe_with_cache_batch_fp32(None, d["timestamps"], pix.clone(), wts, s32)
     torch.cuda.synchronize()
     clocks = clk.stop()
     tb = W.timings()
     its = W.get_result("noiter_batch")
     t_it = reduce_max(tb["iterate_ms"], world)
     value = world * n * float(its.sum()) / (t_it * 1e-3)
+    rel = lambda a, b: float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+    err_aa = rel(W.get_result("aa_batch"), aa64)
+    m32 = W.get_result("map_batch").reshape(R, -1, 3)
+    m64 = map64.reshape(R, -1, 3)
+    err_map = [max(rel(m32[r][:, c], m64[r][:, c]) for r in range(R)) for c in range(3)]
     if rank == 0:
         line = {"metric": "TOD samples/s per PCG iteration (batched Monte Carlo)",
                 "value": value, "unit": "samples/s per PCG iteration", "n_gpus": world,
                 "steps": int(its.max()), "warmup": 0,
                 "ms_per_step": t_it / max(1, int(its.max())), "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": "batched MC nside512 32det x 2^22 @100Hz, %d noise "
-                                       "realisations, fknee 0.02-0.2 Hz" % R,
+                                       "realisations, fknee 0.02-0.2 Hz, float32 TOD" % R,
                            "samples": n, "nrhs": R, "parallelism": "single GPU"},
                 "clocks": clocks,
                 "iterations": {"min": int(its.min()), "max": int(its.max()),
                                "single_rhs": it1},
                 "batch_iterate_ms": t_it, "batch_setup_ms": tb["setup_ms"],
                 "batch_finalize_ms": tb["finalize_ms"],
-                "single_rhs": {"value": single, "iterate_ms": t1["iterate_ms"]},
+                "fp64_batch": {"value": value64, "iterate_ms": t64["iterate_ms"],
+                               "iterations_max": int(its64.max()),
+                               "speedup_vs_one_at_a_time": value64 / single},
+                "fp32_vs_fp64": {"map_rel_err_iqu": err_map, "baseline_rel_err": err_aa,
+                                 "tolerance": 1e-4},
+                "single_rhs": {"value": single, "iterate_ms": t1["iterate_ms"],
+                               "dtype": "f64"},
                 "speedup_vs_one_at_a_time": value / single}
         print(json.dumps(line), flush=True)
     return 0

@@ -56,6 +56,18 @@ int madam_b200_destripe_with_cache_batch(int comm, long ndet, long nsamp, long n
                                          void *timestamps, void *pix, void *pixweights,
                                          long nrhs, void *signals);
 
+/* The batched Monte Carlo solve in the FP32-TOD precision form: signals are
+ * float32 [nrhs][ndet][nsamp] (host or device memory, like pix); the
+ * projections read float32 copies of p.detw and of the map (and the
+ * scatter's pointing as pairs), while pixel matrices, baselines and all
+ * inner products stay float64.  Results as for
+ * madam_b200_destripe_with_cache_batch; they agree with the float64 solve of
+ * the same samples to about 1e-6 relative (tested at 1e-4).  No reference
+ * counterpart. */
+int madam_b200_destripe_with_cache_batch_fp32(int comm, long ndet, long nsamp, long nnz,
+                                              void *timestamps, void *pix, void *pixweights,
+                                              long nrhs, float *signals);
+
 /* Serving: a job queue over one GPU.  No reference counterpart (the
  * reference runs one destripe per call and per MPI job).
  *

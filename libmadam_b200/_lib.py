@@ -47,6 +47,9 @@ def load():
     L.madam_b200_destripe_with_cache_batch.restype = ct.c_int
     L.madam_b200_destripe_with_cache_batch.argtypes = [ct.c_int, ct.c_long, ct.c_long, ct.c_long,
                                                        P, P, P, ct.c_long, P]
+    L.madam_b200_destripe_with_cache_batch_fp32.restype = ct.c_int
+    L.madam_b200_destripe_with_cache_batch_fp32.argtypes = \
+        L.madam_b200_destripe_with_cache_batch.argtypes
     L.madam_b200_clear_caches.restype = ct.c_int
     L.madam_b200_last_error.restype = ct.c_int
     L.madam_b200_last_error.argtypes = [ct.c_char_p, ct.c_long]

@@ -148,6 +148,22 @@ int madam_b200_destripe_with_cache_batch(int comm, long ndet, long nsamp, long n
   });
 }
 
+int madam_b200_destripe_with_cache_batch_fp32(int comm, long ndet, long nsamp, long nnz,
+                                              void *timestamps, void *pix, void *pixweights,
+                                              long nrhs, float *signals) {
+  (void)comm;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  return guarded([&] {
+    if (!g_engine || !g_engine->cached())
+      madam::fail("destripe_with_cache called with empty caches.");
+    const bool dev = is_device_pointer(pix);
+    if (dev != is_device_pointer(signals))
+      madam::fail("pointing and signals must both be host or both be device memory");
+    g_engine->run_cached_batch(ndet, nsamp, nnz, (double *)timestamps, (int32_t *)pix,
+                               (float *)pixweights, nrhs, (double *)signals, dev, true);
+  });
+}
+
 int madam_b200_clear_caches(void) {
   std::lock_guard<std::mutex> lock(g_mutex);
   return guarded([&] { g_engine.reset(); });

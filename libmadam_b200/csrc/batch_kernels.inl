@@ -198,10 +198,11 @@ __global__ void k_update_p_b(double *p, const double *z, double *pw, const doubl
 // side sees the arithmetic of k_scatter_chunks / k_gather_chunks in the same
 // order, so its map and baseline sums equal theirs to the bit.
 
-// [R][nb] (right-hand sides r0 .. r0 + nr) -> [nb][32 G], zero padded
-template <int G>
+// [R][nb] (right-hand sides r0 .. r0 + nr) -> [nb][32 G], zero padded; T =
+// float in the FP32-TOD form
+template <int G, class T>
 __global__ void k_transpose_rhs(const double *__restrict__ src, long long nb, int r0, int nr,
-                                double *__restrict__ dst) {
+                                T *__restrict__ dst) {
   constexpr int GW = 32 * G;
   __shared__ double t[32][33];
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
@@ -215,7 +216,7 @@ __global__ void k_transpose_rhs(const double *__restrict__ src, long long nb, in
     __syncthreads();
     for (int bb = ty; bb < 32; bb += 8) {
       const long long b = b0 + bb;
-      if (b < nb) dst[b * GW + g * 32 + tx] = t[tx][bb];
+      if (b < nb) dst[b * GW + g * 32 + tx] = (T)t[tx][bb];
     }
     __syncthreads();
   }
@@ -239,10 +240,10 @@ __host__ __device__ constexpr int cbrev5(int x) {
 // to 8 columns keeps the kernel's code small enough for the instruction
 // cache.  One launch covers the 32 right-hand sides g0 .. g0 + 31 of rows
 // of GW.
-template <int NMAP, int GW>
+template <int NMAP, int GW, class TW>
 __global__ void __launch_bounds__(256) k_scatter_T(
     const int4 *__restrict__ chunks, long long nchunks, const float4 *__restrict__ sp4,
-    const int2 *__restrict__ sp2, const double *__restrict__ pwT, int g0,
+    const int2 *__restrict__ sp2, const TW *__restrict__ pwT, int g0,
     double *__restrict__ target, double *__restrict__ partial) {
   constexpr int G = 1;
   constexpr int U = kScatterChunk / 32;
@@ -280,10 +281,10 @@ __global__ void __launch_bounds__(256) k_scatter_T(
           const int e0 = r * 32 + L;
           if (e0 < ck.z) {
             const float4 q = rw[e0];
-            const double *pk = pwT + (long long)__float_as_int(q.w) * GW + g0 + lane;
+            const TW *pk = pwT + (long long)__float_as_int(q.w) * GW + g0 + lane;
 #pragma unroll
             for (int g = 0; g < G; ++g) {
-              const double wv = __ldg(pk + g * 32);
+              const double wv = (double)__ldg(pk + g * 32);
               if (NMAP == 3) {
                 P[g][0] = fma((double)q.x, wv, P[g][0]);
                 P[g][1] = fma((double)q.y, wv, P[g][1]);
@@ -353,8 +354,10 @@ __global__ void k_scatter_combine_T(const int4 *__restrict__ multi, int nmulti,
 }
 
 // ccmultiply on the transposed map; thread per (pixel, right-hand side)
+// (and, in the FP32-TOD form, a float32 copy mf for the gather)
 template <int NMAP, int G>
-__global__ void k_ccmult_T(const double *__restrict__ cc, double *__restrict__ m, long long n) {
+__global__ void k_ccmult_T(const double *__restrict__ cc, double *__restrict__ m, long long n,
+                           float *__restrict__ mf) {
   constexpr int GW = 32 * G;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n * GW;
        t += (long long)gridDim.x * blockDim.x) {
@@ -375,16 +378,21 @@ __global__ void k_ccmult_T(const double *__restrict__ cc, double *__restrict__ m
         v[2 * GW] = fma(c[5], d, fma(c[4], b, c[2] * a));
       }
     }
+    if (mf) {
+      float *f = mf + p * NMAP * GW + r;
+#pragma unroll
+      for (int e = 0; e < NMAP; ++e) f[e * GW] = (float)v[e * GW];
+    }
   }
 }
 
 // map_to_baseline sums per baseline and right-hand side, in time order as
 // lane j of k_gather_chunks adds baseline j: apnT[b][r] = sum_s w_s . m_r[p_s]
-template <int NMAP, int G>
+template <int NMAP, int G, class TM>
 __global__ void __launch_bounds__(256) k_gather_T(
     const int2 *__restrict__ chunks, long long nchunks, const float4 *__restrict__ p4,
     const int32_t *__restrict__ pc, const uint32_t *__restrict__ bstart, long noba,
-    long long nsamp, const double *__restrict__ mT, int deg_shift, int nloc,
+    long long nsamp, const TM *__restrict__ mT, int deg_shift, int nloc,
     double *__restrict__ apnT) {
   constexpr int GW = 32 * G;
   constexpr int U = kGatherChunk / 32;
@@ -419,15 +427,15 @@ __global__ void __launch_bounds__(256) k_gather_T(
         const float4 q = rw[s];
         const int px = __float_as_int(q.w);
         if (px < nloc) {
-          const double *mm = mT + (long long)(px >> deg_shift) * NMAP * GW + lane;
+          const TM *mm = mT + (long long)(px >> deg_shift) * NMAP * GW + lane;
 #pragma unroll
           for (int g = 0; g < G; ++g) {
             if (NMAP == 3) {
-              const double m0 = __ldg(mm + g * 32), m1 = __ldg(mm + GW + g * 32),
-                           m2 = __ldg(mm + 2 * GW + g * 32);
+              const double m0 = (double)__ldg(mm + g * 32), m1 = (double)__ldg(mm + GW + g * 32),
+                           m2 = (double)__ldg(mm + 2 * GW + g * 32);
               apn[g] += fma((double)q.z, m2, fma((double)q.y, m1, (double)q.x * m0));
             } else {
-              apn[g] += __ldg(mm + g * 32);
+              apn[g] += (double)__ldg(mm + g * 32);
             }
           }
         } else {

@@ -13,6 +13,7 @@
 // it with one global atomic per touched pixel value.  Gather passes
 // (baselines <- samples) use one warp per baseline in time order.
 #include <cub/cub.cuh>
+#include <type_traits>
 
 #include <algorithm>
 #include <chrono>

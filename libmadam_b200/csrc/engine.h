@@ -117,7 +117,8 @@ class Engine {
   // would solve it right after the caching destripe(); the cache is left as
   // it was.
   void run_cached_batch(long ndet, long nsamp, long nnz, double *timestamps, int32_t *pix,
-                        float *pixweights, long nrhs, double *signals, bool is_device);
+                        float *pixweights, long nrhs, double *signals, bool is_device,
+                        bool fp32 = false);
 
   // Precision of the next run(): false = FP64 TOD (destripe), true = the
   // FP32-TOD form (madam_b200_destripe_fp32): `signal` holds float32
@@ -173,7 +174,10 @@ class Engine {
   void build_batch_tables();
   template <int G>
   void project_group_T(long r0, int nr);
+  template <int G, class T>
+  void project_group_T2(long r0, int nr);
   DevBuf<double> pwT_, lmapT_, scatpT_, apnT_;  // right-hand-side-minor copies
+  DevBuf<float> pwTf_, lmapTf_;                 // their float32 forms (FP32-TOD batch)
   long nrhs_ = 0;                        // right-hand sides of the last batch
   DevBuf<double> yb_, aab_, rb_, pb_, zb_, apb_, rob_, pwb_;  // [R][nb]
   DevBuf<double> lmapb_, scatpb_;        // [R][nloc_cross][nmap], scatter partials

@@ -115,30 +115,46 @@ void Engine::apply_preconditioner_batch(const double *r, double *z) {
 
 template <int G>
 void Engine::project_group_T(long r0, int nr) {
+  if (fp32_) project_group_T2<G, float>(r0, nr);
+  else project_group_T2<G, double>(r0, nr);
+}
+
+template <int G, class T>
+void Engine::project_group_T2(long r0, int nr) {
   // A p's projections for right-hand sides [r0, r0 + nr), nr <= 32 G, on
-  // right-hand-side-minor copies (batch_kernels.inl)
+  // right-hand-side-minor copies (batch_kernels.inl).  T = float in the
+  // FP32-TOD form: p.detw and the map the gather reads are float32.
   constexpr int GW = 32 * G;
   const long long nb = (long long)ndet_ * noba_short_;
   const long long ncross = std::max<long>(1, nloc_cross_);
-  pwT_.alloc((size_t)nb * GW);
+  const bool f32 = std::is_same<T, float>::value;
+  T *pwT;
+  if (f32) {
+    pwTf_.alloc((size_t)nb * GW);
+    pwT = (T *)pwTf_.get();
+    lmapTf_.alloc((size_t)ncross * nmap_ * GW);
+  } else {
+    pwT_.alloc((size_t)nb * GW);
+    pwT = (T *)pwT_.get();
+  }
   lmapT_.alloc((size_t)ncross * nmap_ * GW);
   scatpT_.alloc((size_t)std::max<size_t>(1, scatter_partial_.n / nmap_) * nmap_ * GW);
   apnT_.alloc((size_t)nb * GW);
   const unsigned tb = (unsigned)std::min<long long>(4736, (nb + 31) / 32);
-  MADAM_LAUNCH(k_transpose_rhs<G>, dim3(tb, G), 256, 0, st_, pwb_.get(), nb, (int)r0, nr,
-               pwT_.get());
+  MADAM_LAUNCH((k_transpose_rhs<G, T>), dim3(tb, G), 256, 0, st_, pwb_.get(), nb, (int)r0, nr,
+               pwT);
   // 1) baseline -> map, combine, ccmultiply
   if (nloc_cross_ > 0 && nscatter_chunks_ > 0) {
     // one launch per 32 right-hand sides (fewer registers, more warps)
     for (int g0 = 0; g0 < GW; g0 += 32) {
       if (nmap_ == 3)
-        MADAM_LAUNCH((k_scatter_T<3, GW>), kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
-                     nscatter_chunks_, sp4_.get(), sp2_.get(), pwT_.get(), g0, lmapT_.get(),
-                     scatpT_.get());
+        MADAM_LAUNCH((k_scatter_T<3, GW, T>), kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
+                     nscatter_chunks_, sp4_.get(), sp2_.get(), (const T *)pwT, g0,
+                     lmapT_.get(), scatpT_.get());
       else
-        MADAM_LAUNCH((k_scatter_T<1, GW>), kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
-                     nscatter_chunks_, sp4_.get(), sp2_.get(), pwT_.get(), g0, lmapT_.get(),
-                     scatpT_.get());
+        MADAM_LAUNCH((k_scatter_T<1, GW, T>), kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
+                     nscatter_chunks_, sp4_.get(), sp2_.get(), (const T *)pwT, g0,
+                     lmapT_.get(), scatpT_.get());
     }
     if (nscatter_multi_ > 0) {
       const long long tot = (long long)nscatter_multi_ * nmap_ * GW;
@@ -150,23 +166,25 @@ void Engine::project_group_T(long r0, int nr) {
                      scatter_multi_.get(), nscatter_multi_, scatpT_.get(), lmapT_.get());
     }
   }
+  float *mf = f32 ? lmapTf_.get() : nullptr;
   if (nloc_cross_ > 0) {
     if (nmap_ == 3)
       MADAM_LAUNCH((k_ccmult_T<3, G>), grid_for((long long)nloc_cross_ * GW), 256, 0, st_,
-                   cca_.get(), lmapT_.get(), (long long)nloc_cross_);
+                   cca_.get(), lmapT_.get(), (long long)nloc_cross_, mf);
     else
       MADAM_LAUNCH((k_ccmult_T<1, G>), grid_for((long long)nloc_cross_ * GW), 256, 0, st_,
-                   cca_.get(), lmapT_.get(), (long long)nloc_cross_);
+                   cca_.get(), lmapT_.get(), (long long)nloc_cross_, mf);
   }
   // 3) map -> baseline sums, then ap and p.ap per right-hand side
+  const T *mT = f32 ? (const T *)lmapTf_.get() : (const T *)lmapT_.get();
   if (nmap_ == 3)
-    MADAM_LAUNCH((k_gather_T<3, G>), kRedBlocks, 256, 0, st_, gather_chunks_.get(),
+    MADAM_LAUNCH((k_gather_T<3, G, T>), kRedBlocks, 256, 0, st_, gather_chunks_.get(),
                  ngather_chunks_, point4_.get(), pixc_.get(), bstart_d_.get(), noba_short_,
-                 nsamp_, lmapT_.get(), (int)ndeg_shift_, (int)nloc_, apnT_.get());
+                 nsamp_, mT, (int)ndeg_shift_, (int)nloc_, apnT_.get());
   else
-    MADAM_LAUNCH((k_gather_T<1, G>), kRedBlocks, 256, 0, st_, gather_chunks_.get(),
+    MADAM_LAUNCH((k_gather_T<1, G, T>), kRedBlocks, 256, 0, st_, gather_chunks_.get(),
                  ngather_chunks_, point4_.get(), pixc_.get(), bstart_d_.get(), noba_short_,
-                 nsamp_, lmapT_.get(), (int)ndeg_shift_, (int)nloc_, apnT_.get());
+                 nsamp_, mT, (int)ndeg_shift_, (int)nloc_, apnT_.get());
   MADAM_LAUNCH(k_gather_finish_T<G>, kRedBlocks, 256, 0, st_, apnT_.get(), nb, bw_.get(),
                nna_.get(), rmask_.get(), pb_.get(), apb_.get(), (int)r0, nr, partb_.get());
 }
@@ -350,7 +368,8 @@ void Engine::iterate_batch() {
 }
 
 void Engine::run_cached_batch(long ndet, long nsamp, long nnz, double *timestamps, int32_t *pix,
-                              float *pixweights, long nrhs, double *signals, bool is_device) {
+                              float *pixweights, long nrhs, double *signals, bool is_device,
+                              bool fp32) {
   g_alloc_stream = st_;
   if (!cached_) fail("destripe_with_cache called with empty caches.");
   if (nrhs < 1) fail("nrhs must be at least 1");
@@ -365,7 +384,10 @@ void Engine::run_cached_batch(long ndet, long nsamp, long nnz, double *timestamp
   const long long n = (long long)ndet * nsamp;
   const long long nb = (long long)ndet_ * noba_short_;
   nrhs_ = nrhs;
-  // pointing-side setup, once
+  // pointing-side setup, once; fp32: float32 signals and projections (the
+  // FP32-TOD form), which also compresses the scatter's pointing into pairs
+  fp32_ = fp32;
+  fp32_next_ = false;
   d_pix_caller_ = is_device ? pix : nullptr;
   bind_inputs(timestamps, pix, pixweights, signals, is_device, false);
   flag_and_compact(false);
@@ -382,7 +404,22 @@ void Engine::run_cached_batch(long ndet, long nsamp, long nnz, double *timestamp
   binb_.alloc((size_t)nrhs * std::max<long long>(1, nv));
   mapb_.alloc((size_t)nrhs * std::max<long long>(1, nv));
   binmapb_.alloc((size_t)nrhs * std::max<long long>(1, nv));
+  DevBuf<float> t32;
   auto select_tod = [&](long k) {
+    if (fp32) {
+      float *src = (float *)signals + k * n;
+      sig32_caller_ = src;
+      const float *dsrc = src;
+      if (!is_device) {
+        t32.alloc(n);
+        MADAM_CUDA(cudaMemcpyAsync(t32.get(), src, n * sizeof(float), cudaMemcpyHostToDevice,
+                                   st_));
+        dsrc = t32.get();
+      }
+      if (n > 0) MADAM_LAUNCH(k_f32_to_f64, grid_for(n), 256, 0, st_, dsrc, tod_own_.get(), n);
+      d_tod_ = tod_own_.get();
+      return;
+    }
     if (is_device) {
       d_tod_ = signals + k * n;
     } else {

@@ -115,3 +115,37 @@ def test_batch_device_buffers(W):
     torch.cuda.synchronize()
     _close(W.get_result("map_batch"), mh, BATCH_RTOL)
     W.clear_caches()
+
+
+FP32_RTOL = 1e-4
+
+
+@pytest.mark.parametrize("extra", [dict(), dict(temperature_only=True)])
+def test_batch_fp32_matches_fp64(W, extra):
+    """The FP32-TOD batched form against one-at-a-time float64 solves: maps
+    and baselines within FP32_RTOL of their largest magnitude."""
+    cfg = syn.small_config(seed=45)
+    d = syn.to_numpy(syn.generate(cfg, nnz=1 if extra.get("temperature_only") else None))
+    pars = dict(d["pars"], mcmode=True, **extra)
+    nrhs = 4
+    sigs = _realisations(d, nrhs)
+    ref = _sequential(W, d, pars, sigs)
+    W.clear_caches()
+    _cache(W, d, pars)
+    W.destripe_with_cache_batch_fp32(None, d["timestamps"], d["pixels"].copy(), d["pixweights"],
+                                     np.stack(sigs).astype(np.float32))
+    nmap = 1 if extra.get("temperature_only") else 3
+    maps = W.get_result("map_batch").reshape(nrhs, -1, nmap)
+    aas = W.get_result("aa_batch").reshape(nrhs, -1)
+    its = W.get_result("noiter_batch")
+    for r in range(nrhs):
+        assert abs(its[r] - ref[r]["noiter"]) <= 3
+        for c in range(nmap):
+            _close(maps[r][:, c], ref[r]["map"].reshape(-1, nmap)[:, c], FP32_RTOL)
+        _close(aas[r], ref[r]["aa"], FP32_RTOL)
+    # the cache still gives the float64 answer afterwards
+    W.destripe_with_cache(None, d["timestamps"], d["pixels"].copy(), d["pixweights"],
+                          sigs[1].copy(), b"")
+    _close(W.get_result("map").reshape(-1, nmap)[:, 0], ref[1]["map"].reshape(-1, nmap)[:, 0],
+           BATCH_RTOL)
+    W.clear_caches()
