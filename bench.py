@@ -301,7 +301,8 @@ def run_mc(args, world, rank, local):
 
 def run_serve(args, world, rank, local):
     """Serving stream: requests of uneven size (nside 128-1024, 2-32 detectors,
-    2^18-2^22 samples per detector, base_first 0.25-2 s, cglimit 1e-10) arrive
+    2^18-2^22 samples per detector, base_first 0.25-2 s, cglimit 1e-10, half
+    of them with float32 TOD served in the FP32-TOD form) arrive
     as a Poisson process and are served by libmadam_b200.serve; reports p50 /
     p99 latency (submit to done) and aggregate throughput."""
     import torch
@@ -321,6 +322,8 @@ def run_serve(args, world, rank, local):
         d["pixels"] = d["pixels"].reshape(-1)
         d["pixweights"] = d["pixweights"].reshape(-1)
         d["signal"] = d["signal"].reshape(-1)
+        if rng.random() < 0.5:  # mixed float32 / float64 TOD
+            d["signal"] = d["signal"].float()
         reqs.append(d)
     torch.cuda.synchronize()
     arrivals = np.cumsum(rng.exponential(1.0 / args.rate, args.requests))
@@ -349,12 +352,14 @@ def run_serve(args, world, rank, local):
             "value": float(np.percentile(lat, 50) * 1e3), "unit": "ms (p50 latency)",
             "p99_ms": float(np.percentile(lat, 99) * 1e3),
             "p50_ms": float(np.percentile(lat, 50) * 1e3),
-            "n_gpus": 1, "higher_is_better": False, "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
+            "n_gpus": 1, "higher_is_better": False, "vs_baseline": None,
+            "dtype": "f64 and f32 (mixed TOD)", "data": "synthetic",
             "config": {"workload": "serving stream: %d requests, Poisson %.1f req/s, nside "
                                    "128-1024, 2-32 detectors, 2^18-2^22 samples per detector, "
-                                   "base_first 0.25-2 s, cglimit 1e-10" % (args.requests,
-                                                                          args.rate),
+                                   "base_first 0.25-2 s, cglimit 1e-10, half the requests "
+                                   "float32 TOD" % (args.requests, args.rate),
+                       "float32_requests": int(sum(1 for d in reqs
+                                                   if d["signal"].dtype == torch.float32)),
                        "workers": args.workers},
             "clocks": clocks,
             "makespan_s": makespan,

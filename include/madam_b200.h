@@ -95,6 +95,14 @@ long madam_b200_serve_submit(void *srv, char *parstring, long ndet, char *detstr
                              long *npsd, long npsdtot, double *psdstarts, long npsdbin,
                              double *psdfreqs, long npsdval, double *psdvals, char *err,
                              long errlen);
+/* serve_submit for a float32 signal: the job runs in the FP32-TOD form of
+ * madam_b200_destripe_fp32. */
+long madam_b200_serve_submit_fp32(void *srv, char *parstring, long ndet, char *detstring,
+                                  double *detweights, long nsamp, long nnz, void *timestamps,
+                                  void *pix, void *pixweights, float *signal, long nperiod,
+                                  long *periods, long *npsd, long npsdtot, double *psdstarts,
+                                  long npsdbin, double *psdfreqs, long npsdval, double *psdvals,
+                                  char *err, long errlen);
 int madam_b200_serve_wait(void *srv, long job, double timeout_s);
 long madam_b200_serve_result_size(void *srv, long job, const char *name);
 int madam_b200_serve_result_copy(void *srv, long job, const char *name, void *dst, long nbytes);

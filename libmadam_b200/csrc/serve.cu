@@ -1,7 +1,8 @@
 // Serving: a queue of destriping jobs of uneven sizes on one GPU.
 //
 // Callers submit complete destripe() jobs (the arguments of the reference
-// C-ABI, smadam.F90:64-101) and collect their products later.  A fixed set
+// C-ABI, smadam.F90:64-101; float64 signals, or float32 signals for the
+// FP32-TOD form of destripe_fp32) and collect their products later.  A fixed set
 // of worker threads each owns an engine with its own CUDA stream, so jobs in
 // flight overlap on the device.  A job is admitted when its estimated device
 // footprint fits the memory budget next to the jobs already running (the
@@ -62,6 +63,7 @@ struct Job {
   double *sig = nullptr;
   std::vector<long> periods;
   bool dev = false;
+  bool fp32 = false;  // float32 signal: the FP32-TOD form (destripe_fp32)
   size_t bytes = 0;
   int state = 0;  // 0 queued, 1 running, 2 done, 3 failed
   std::string error;
@@ -77,6 +79,7 @@ size_t job_bytes(const Job &j) {
   const double nb = n / dn + j.ndet;
   const double npix = 12.0 * j.par.nside_map * j.par.nside_map;
   double b = n * (j.dev ? 64.0 : 84.0) + nb * 8.0 * 24 + npix * 8.0 * 24 + (256 << 20);
+  if (j.fp32) b += n * (j.dev ? 40.0 : 44.0);  // pairs, their sort and the float32 staging
   return (size_t)b;
 }
 
@@ -159,6 +162,7 @@ class Server {
       double noiter = 0;
       try {
         if (!eng) eng.reset(new Engine());
+        eng->set_fp32(j->fp32);
         eng->run(j->par, j->dets, j->ndet, j->nsamp, j->nnz, j->ts, j->pix, j->w, j->sig,
                  (long)j->periods.size(), j->periods.data(), j->dev);
         for (const char *nm : {"map", "binmap", "hits", "mask", "aa", "scalars", "rr_history"}) {
@@ -226,12 +230,39 @@ void *madam_b200_serve_open(int nworkers, double mem_fraction, char *err, long e
   }
 }
 
+static long serve_submit(bool fp32, void *srv, char *parstring, long ndet, char *detstring,
+                         double *detweights, long nsamp, long nnz, void *timestamps, void *pix,
+                         void *pixweights, void *signal, long nperiod, long *periods, long *npsd,
+                         long npsdtot, double *psdstarts, long npsdbin, double *psdfreqs,
+                         long npsdval, double *psdvals, char *err, long errlen);
+
 long madam_b200_serve_submit(void *srv, char *parstring, long ndet, char *detstring,
                              double *detweights, long nsamp, long nnz, void *timestamps, void *pix,
                              void *pixweights, void *signal, long nperiod, long *periods,
                              long *npsd, long npsdtot, double *psdstarts, long npsdbin,
                              double *psdfreqs, long npsdval, double *psdvals, char *err,
                              long errlen) {
+  return serve_submit(false, srv, parstring, ndet, detstring, detweights, nsamp, nnz, timestamps,
+                      pix, pixweights, signal, nperiod, periods, npsd, npsdtot, psdstarts,
+                      npsdbin, psdfreqs, npsdval, psdvals, err, errlen);
+}
+
+long madam_b200_serve_submit_fp32(void *srv, char *parstring, long ndet, char *detstring,
+                                  double *detweights, long nsamp, long nnz, void *timestamps,
+                                  void *pix, void *pixweights, float *signal, long nperiod,
+                                  long *periods, long *npsd, long npsdtot, double *psdstarts,
+                                  long npsdbin, double *psdfreqs, long npsdval, double *psdvals,
+                                  char *err, long errlen) {
+  return serve_submit(true, srv, parstring, ndet, detstring, detweights, nsamp, nnz, timestamps,
+                      pix, pixweights, signal, nperiod, periods, npsd, npsdtot, psdstarts,
+                      npsdbin, psdfreqs, npsdval, psdvals, err, errlen);
+}
+
+static long serve_submit(bool fp32, void *srv, char *parstring, long ndet, char *detstring,
+                         double *detweights, long nsamp, long nnz, void *timestamps, void *pix,
+                         void *pixweights, void *signal, long nperiod, long *periods, long *npsd,
+                         long npsdtot, double *psdstarts, long npsdbin, double *psdfreqs,
+                         long npsdval, double *psdvals, char *err, long errlen) {
   Server *s = (Server *)srv;
   if (!s) return -1;
   try {
@@ -252,6 +283,9 @@ long madam_b200_serve_submit(void *srv, char *parstring, long ndet, char *detstr
     j->sig = (double *)signal;
     j->periods.assign(periods, periods + nperiod);
     j->dev = madam::device_ptr(pix);
+    if (j->dev != madam::device_ptr(signal))
+      madam::fail("pixels and signal must both be host or both device memory");
+    j->fp32 = fp32;
     j->bytes = madam::job_bytes(*j);
     return s->submit(std::move(j));
   } catch (const std::exception &e) {

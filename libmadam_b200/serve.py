@@ -8,7 +8,8 @@
     srv.close()
 
 `submit` takes the arguments of libmadam_wrapper.destripe (the reference's
-destripe call without `comm`) and returns at once.  Worker threads, each with
+destripe call without `comm`) and returns at once; a float32 signal runs the
+job in the FP32-TOD form of destripe_fp32, any other dtype as float64.  Worker threads, each with
 its own engine and CUDA stream, run the jobs; a job starts when its estimated
 device footprint fits the memory budget beside the running jobs (first come,
 first served), so jobs in flight overlap on the GPU.  The products of a job
@@ -37,6 +38,8 @@ def _lib_serve():
     L.madam_b200_serve_submit.argtypes = [P, ct.c_char_p, ct.c_long, ct.c_char_p, P, ct.c_long,
                                           ct.c_long, P, P, P, P, ct.c_long, P, P, ct.c_long, P,
                                           ct.c_long, P, ct.c_long, P, ct.c_char_p, ct.c_long]
+    L.madam_b200_serve_submit_fp32.restype = ct.c_long
+    L.madam_b200_serve_submit_fp32.argtypes = L.madam_b200_serve_submit.argtypes
     L.madam_b200_serve_wait.restype = ct.c_int
     L.madam_b200_serve_wait.argtypes = [P, ct.c_long, ct.c_double]
     L.madam_b200_serve_result_size.restype = ct.c_long
@@ -53,6 +56,13 @@ def _lib_serve():
     L.madam_b200_serve_close.argtypes = [P]
     L._serve_ready = True
     return L
+
+
+def _is_float32(a):
+    cai = getattr(a, "__cuda_array_interface__", None)
+    if cai is not None:
+        return np.dtype(cai["typestr"]) == np.float32
+    return np.asarray(a).dtype == np.float32
 
 
 class Ticket:
@@ -79,7 +89,8 @@ class Server:
         ts = _Buf(timestamps, TIMESTAMP_TYPE)
         px = _Buf(pixels, PIXEL_TYPE)
         pw = _Buf(pixweights, WEIGHT_TYPE)
-        sg = _Buf(signal, SIGNAL_TYPE)
+        fp32 = _is_float32(signal)
+        sg = _Buf(signal, np.float32 if fp32 else SIGNAL_TYPE)
         nsamp = ts.size
         nnz = pw.size // nsamp // ndet
         w = np.ascontiguousarray(weights, dtype=np.float64)
@@ -92,7 +103,8 @@ class Server:
         npsdval = psdvals.size
         p = lambda a: a.ctypes.data_as(ct.c_void_p)
         err = ct.create_string_buffer(512)
-        job = self._L.madam_b200_serve_submit(
+        entry = self._L.madam_b200_serve_submit_fp32 if fp32 else self._L.madam_b200_serve_submit
+        job = entry(
             self._h, parstring, ndet, detstring, p(w), nsamp, nnz, ts.ptr, px.ptr, pw.ptr, sg.ptr,
             periods.size, p(periods), p(npsd), npsdval // npsdbin, p(psdstarts), npsdbin,
             p(psdfreqs), npsdval, p(psdvals), err, 512)

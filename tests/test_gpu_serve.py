@@ -94,3 +94,42 @@ def test_device_buffers_are_served(W):
     assert srv.wait(t) == 2
     _close(srv.result(t, "map"), ref, SERVE_RTOL)
     srv.close()
+
+
+FP32_RTOL = 1e-4
+
+
+def test_mixed_float32_and_float64_jobs(W):
+    """float32 signals run in the FP32-TOD form (destripe_fp32) and float64
+    signals in the float64 form, side by side; each gives its lone result
+    (float32 jobs within FP32_RTOL: their float32 projections round the
+    setup's rounding-level differences, so two runs agree to ~1e-6)."""
+    from libmadam_b200.serve import Server
+    jobs = _jobs()
+    f32 = [True, False, True, False, True, True]
+    alone = []
+    for d, f in zip(jobs, f32):
+        a = list(_args(d))
+        if f:
+            a[6] = a[6].astype(np.float32)
+            W.destripe_fp32(None, *a)
+        else:
+            W.destripe(None, *a)
+        alone.append(dict(map=W.get_result("map"), aa=W.get_result("aa"),
+                          hits=W.get_result("hits"), fp32=W.scalars()["fp32"]))
+        assert alone[-1]["fp32"] == (1.0 if f else 0.0)
+    srv = Server(workers=3, mem_fraction=0.5)
+    tickets = []
+    for d, f in zip(jobs, f32):
+        a = list(_args(d))
+        if f:
+            a[6] = a[6].astype(np.float32)
+        tickets.append(srv.submit(*a))
+    for t, ref, f in zip(tickets, alone, f32):
+        assert srv.wait(t) == 2
+        np.testing.assert_array_equal(srv.result(t, "hits"), ref["hits"])
+        tol = FP32_RTOL if f else SERVE_RTOL
+        _close(srv.result(t, "map"), ref["map"], tol)
+        _close(srv.result(t, "aa"), ref["aa"], tol)
+        assert srv.result(t, "scalars")[21] == (1.0 if f else 0.0)
+    srv.close()
