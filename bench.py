@@ -229,6 +229,9 @@ def run_mc(args, world, rank, local):
     from libmadam_b200 import libmadam_wrapper as W
     from libmadam_b200 import synthetic as syn
     cfg = syn.config4()
+    if args.config == "mc-prof":  # 4 detectors x 2^20 samples: small enough for ncu captures
+        cfg.ndet = 4
+        cfg.nsamp_obs = 1 << 20
     cfg.seed += 1000 * rank
     R = args.nrhs
     d = syn.generate(cfg, device="cuda", with_signal=False)
@@ -279,8 +282,9 @@ def run_mc(args, world, rank, local):
                 "steps": int(its.max()), "warmup": 0,
                 "ms_per_step": t_it / max(1, int(its.max())), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "batched MC nside512 32det x 2^22 @100Hz, %d noise "
-                                       "realisations, fknee 0.02-0.2 Hz, float32 TOD" % R,
+                "config": {"workload": "batched MC nside512 %ddet x 2^%d @100Hz, %d noise "
+                                       "realisations, fknee 0.02-0.2 Hz, float32 TOD"
+                                       % (cfg.ndet, cfg.nsamp_obs.bit_length() - 1, R),
                            "samples": n, "nrhs": R, "parallelism": "single GPU"},
                 "clocks": clocks,
                 "iterations": {"min": int(its.min()), "max": int(its.max()),
@@ -378,8 +382,8 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="2", choices=["2", "1", "3", "prof", "mid", "mid3", "small", "mc",
-                                                   "serve"])
+    ap.add_argument("--config", default="2", choices=["2", "1", "3", "prof", "mid", "mid3", "small",
+                                                   "mc", "mc-prof", "serve"])
     ap.add_argument("--requests", type=int, default=60)
     ap.add_argument("--rate", type=float, default=20.0)
     ap.add_argument("--workers", type=int, default=4)
@@ -402,7 +406,7 @@ def main():
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device")
     torch.cuda.set_device(local)
-    if args.config == "mc":
+    if args.config in ("mc", "mc-prof"):
         return run_mc(args, world, rank, local)
     if args.config == "serve":
         return run_serve(args, world, rank, local)
