@@ -537,22 +537,44 @@ struct Params {
        do_leakmatrix = false;
   long nthreads = 1;
   int ndetset = 0, nsurvey = 0;
+  // detector sets and surveys (inputparam.f90:375-492); entry 0 is the full
+  // set / span, whose name an "all" definition sets
+  struct DetSet {
+    std::string name;
+    std::vector<std::string> dets;
+    bool nopol = false;
+  };
+  struct Survey {
+    std::string name;
+    std::vector<double> starts, stops;
+  };
+  std::vector<DetSet> detsets = std::vector<DetSet>(1);
+  std::vector<Survey> surveys = std::vector<Survey>(1);
 };
 
-void parse_detset(Params &p, const std::string &value) {
+// parse_detset (inputparam.f90:375-434)
+void parse_detset(Params &p, const std::string &value, bool nopol) {
   size_t i = value.find(':');
   if (i == std::string::npos)
     fail("Failed to parse: " + trim(value) + " for valid detector set name");
   std::string name = trim(value.substr(0, i));
   if (name.empty()) fail("Empty detset name");
   std::string line = trim(value.substr(i + 1));
+  Params::DetSet ds;
+  ds.name = name;
+  ds.nopol = nopol;
   while (true) {
     size_t c = line.find(',');
     std::string det = trim(c == std::string::npos ? line : line.substr(0, c));
-    if (det.empty() || det == "all" || det == "All" || det == "ALL") return;
+    if (det.empty() || det == "all" || det == "All" || det == "ALL") {
+      p.detsets[0].name = name;  // names the full detector set
+      return;
+    }
+    ds.dets.push_back(det);
     if (c == std::string::npos) break;
     line = trim(line.substr(c + 1));
   }
+  p.detsets.push_back(ds);
   p.ndetset += 1;
 }
 
@@ -563,11 +585,15 @@ void parse_survey(Params &p, const std::string &value) {
   std::string name = trim(value.substr(0, i));
   if (name.empty()) fail("Empty survey name");
   std::string line = trim(value.substr(i + 1));
+  Params::Survey sv;
+  sv.name = name;
   while (true) {
     size_t d = line.find('-');
     if (d == std::string::npos) {
-      if (line.empty() || line == "all" || line == "All" || line == "ALL")
+      if (line.empty() || line == "all" || line == "All" || line == "ALL") {
+        p.surveys[0].name = name;  // names the full data span
         return;
+      }
       fail("Failed to parse: " + line + " for valid survey span marker (-)");
     }
     double a, b;
@@ -576,10 +602,13 @@ void parse_survey(Params &p, const std::string &value) {
     line = trim(line.substr(d + 1));
     if (!read_real(line, b))
       fail("Failed to parse: " + line + " for valid survey stop");
+    sv.starts.push_back(a);
+    sv.stops.push_back(b);
     size_t c = line.find(',');
     if (c == std::string::npos) break;
     line = trim(line.substr(c + 1));
   }
+  p.surveys.push_back(sv);
   p.nsurvey += 1;
 }
 
@@ -683,8 +712,8 @@ void read_line(Params &p, const std::string &line_in) {
   else if (key == "binary_output") L(p.binary_output);
   else if (key == "nwrite_binary") I(p.nwrite_binary);
   else if (key == "file_covmat") p.file_covmat = tv;
-  else if (key == "detset") parse_detset(p, value);
-  else if (key == "detset_nopol") parse_detset(p, value);
+  else if (key == "detset") parse_detset(p, value, false);
+  else if (key == "detset_nopol") parse_detset(p, value, true);
   else if (key == "survey") parse_survey(p, value);
   else if (key == "bin_subsets") L(p.bin_subsets);
   else if (key == "mcmode") L(p.mcmode);
@@ -775,8 +804,17 @@ struct State {
   double t_iterate = 0, t_total = 0;
   bool tod_cleaned = false;
 
+  // subsets (run_subsets): empty = every detector / sample
+  std::vector<char> detflags, surveyflags;
+  // subset and leakage products, by result name
+  std::map<std::string, std::vector<double>> extra_d;
+  std::map<std::string, std::vector<int>> extra_i;
+
   ~State() { delete fft; }
 };
+
+inline bool det_on(const State &S, long d) { return S.detflags.empty() || S.detflags[d]; }
+inline bool samp_on(const State &S, long i) { return S.surveyflags.empty() || S.surveyflags[i]; }
 
 State *g_state = nullptr;
 std::string g_error;
@@ -1340,6 +1378,7 @@ void pixel_matrix(State &S) {
     long first, last;
     pix_range(S, tid, nth, first, last);
     for (long d = 0; d < S.ndet; ++d) {
+      if (!det_on(S, d)) continue;  // not included in this subset
       for (long iv = 0; iv < S.ninterval; ++iv) {
         long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
         int ipsd = psd_index_det(S, d, S.btime[ks]);
@@ -1349,6 +1388,7 @@ void pixel_matrix(State &S) {
         double sqw = std::sqrt(detw);
         for (long k = ks; k < ks + noba; ++k)
           for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+            if (!samp_on(S, i)) continue;
             long ip = S.pixels[(size_t)d * S.nsamp + i];
             if (ip < first || ip > last) continue;
             double *c = &S.loccc[(size_t)ip * nn];
@@ -1377,6 +1417,7 @@ void pixel_matrix(State &S) {
 void count_hits(State &S) {
   std::fill(S.lochits.begin(), S.lochits.end(), 0);
   for (long d = 0; d < S.ndet; ++d) {
+    if (!det_on(S, d)) continue;  // not included in this subset
 #pragma omp parallel num_threads(S.nthreads)
     {
       int tid = omp_get_thread_num(), nth = omp_get_num_threads();
@@ -1389,6 +1430,7 @@ void count_hits(State &S) {
         if (S.dets[d].weights[ipsd] == 0) continue;
         for (long k = ks; k < ks + noba; ++k)
           for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+            if (!samp_on(S, i)) continue;
             long ip = S.pixels[(size_t)d * S.nsamp + i];
             if (ip < first || ip > last) continue;
             S.lochits[ip] += 1;
@@ -1408,7 +1450,8 @@ void bin_tod(State &S) {
     int tid = omp_get_thread_num(), nth = omp_get_num_threads();
     long first, last;
     pix_range(S, tid, nth, first, last);
-    for (long d = 0; d < S.ndet; ++d)
+    for (long d = 0; d < S.ndet; ++d) {
+      if (!det_on(S, d)) continue;  // not included in this subset
       for (long iv = 0; iv < S.ninterval; ++iv) {
         long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
         int ipsd = psd_index_det(S, d, S.btime[ks]);
@@ -1417,6 +1460,7 @@ void bin_tod(State &S) {
         if (detw == 0) continue;
         for (long k = ks; k < ks + noba; ++k)
           for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+            if (!samp_on(S, i)) continue;
             size_t s = (size_t)d * S.nsamp + i;
             long ip = S.pixels[s];
             if (ip < first || ip > last) continue;
@@ -1430,6 +1474,7 @@ void bin_tod(State &S) {
             }
           }
       }
+    }
   }
   if (S.par.kfirst) collect_map(S, S.map, S.nosubpix_map);
   collect_map(S, S.binmap, S.nosubpix_map);  // binned map always kept
@@ -2087,6 +2132,132 @@ void makemaps(State &S, std::vector<double> &map) {
     if (S.outmask[ip] > 0) map[(size_t)ip * S.nmap] -= mono;
 }
 
+// leakmatrix (smadam_routines.f90:38-105): the pixel matrix of detector
+// idet alone, times the inverted matrix of the (sub)set, per pixel.  Both
+// matrices are symmetrised from their upper triangles first (the set's in
+// place, as the reference does).  out: [npix][nmap][nmap], row i column j =
+// gamma(i, j).
+void leakmatrix(State &S, long idet, std::vector<double> &out) {
+  const int nmap = S.nmap, nn = nmap * nmap;
+  std::vector<char> flags_save = S.detflags;
+  const bool kfirst_save = S.par.kfirst;
+  S.detflags.assign(S.ndet, 0);
+  S.detflags[idet] = 1;
+  S.par.kfirst = false;
+  std::vector<double> cc_set = S.cc;
+  std::fill(S.cc.begin(), S.cc.end(), 0.0);
+  pixel_matrix(S);
+  std::vector<double> cc_det = S.cc;
+  S.cc = cc_set;
+  out.assign((size_t)S.nopix_map * nn, 0.0);
+  for (long ip = 0; ip < S.nopix_map; ++ip) {
+    for (int i = 0; i < nmap; ++i)
+      for (int j = 0; j < i; ++j) {
+        CC(cc_det, nmap, ip, i, j) = CC(cc_det, nmap, ip, j, i);
+        CC(S.cc, nmap, ip, i, j) = CC(S.cc, nmap, ip, j, i);
+      }
+    for (int i = 0; i < nmap; ++i)
+      for (int j = 0; j < nmap; ++j) {
+        double g = 0;
+        for (int k = 0; k < nmap; ++k) g += CC(S.cc, nmap, ip, i, k) * CC(cc_det, nmap, ip, k, j);
+        out[(size_t)ip * nn + i * nmap + j] = g;
+      }
+  }
+  S.detflags = flags_save;
+  S.par.kfirst = kfirst_save;
+}
+
+// run_subsets (smadam.F90:954-1257).  Every (survey, detector set) pair but
+// the full one is binned again from the TOD as it stands: the reference sets
+// kfirst = F before its passes, so their clean_tod returns at once and the
+// "destriped" subset maps of the last pass equal the binned ones.  A nopol
+// set of polarised data is binned with nmap = 1 (weights ignored, as
+// pixel_matrix / bin_tod do for nmap = 1).  The pass-1 products (hits, mask,
+// inverted matrices, leakage matrices) and each pass's map are kept as
+// results; the full-data products stay as they were.
+void run_subsets(State &S) {
+  const Params &p = S.par;
+  if (!p.bin_subsets) return;
+  const int nmap_save = S.nmap;
+  const bool kfirst_save = S.par.kfirst, binmap_save = S.par.do_binmap;
+  std::vector<double> cc0 = S.cc, bin0 = S.binmap;
+  std::vector<int> hits0 = S.nohits, mask0 = S.outmask;
+  std::vector<float> crit0 = S.crit;
+  int npass = (p.do_binmap && p.do_map) ? 2 : 1;
+  S.par.kfirst = false;
+  if (p.do_map) S.par.do_binmap = true;
+  std::vector<double> table;
+  long k = 0;
+  for (int pass = 1; pass <= npass; ++pass) {
+    for (int isv = 0; isv <= p.nsurvey; ++isv) {
+      if (isv != 0) {
+        const Params::Survey &sv = p.surveys[isv];
+        S.surveyflags.assign(S.nsamp, 0);
+        for (long i = 0; i < S.nsamp; ++i)
+          for (size_t j = 0; j < sv.starts.size(); ++j)
+            if (sv.starts[j] <= S.times[i] && S.times[i] <= sv.stops[j]) S.surveyflags[i] = 1;
+      } else {
+        S.surveyflags.clear();
+      }
+      long nhs = 0;
+      for (long i = 0; i < S.nsamp; ++i) nhs += samp_on(S, i) ? 1 : 0;
+      if (nhs == 0) continue;
+      for (int ids = 0; ids <= p.ndetset; ++ids) {
+        if (ids == 0 && isv == 0) continue;
+        bool tonly = p.temperature_only;
+        if (ids != 0) {
+          const Params::DetSet &ds = p.detsets[ids];
+          S.detflags.assign(S.ndet, 0);
+          for (long d = 0; d < S.ndet; ++d)
+            for (const std::string &n : ds.dets)
+              if (S.dets[d].name == n) S.detflags[d] = 1;
+          tonly = ds.nopol && !p.force_pol;
+        } else {
+          S.detflags.clear();
+        }
+        long nhd = 0;
+        for (long d = 0; d < S.ndet; ++d) nhd += det_on(S, d) ? 1 : 0;
+        if (nhd == 0) continue;
+        S.nmap = tonly ? 1 : nmap_save;
+        const int nn = S.nmap * S.nmap;
+        std::fill(S.cc.begin(), S.cc.end(), 0.0);
+        std::fill(S.binmap.begin(), S.binmap.end(), 0.0);
+        std::fill(S.nohits.begin(), S.nohits.end(), 0);
+        pixel_matrix(S);
+        if (pass == 1) count_hits(S);
+        bin_tod(S);
+        invert_pixelmatrix_map(S);
+        const std::string key = std::to_string(k);
+        if (pass == 1 && p.do_leakmatrix)
+          for (long d = 0; d < S.ndet; ++d)
+            if (det_on(S, d)) leakmatrix(S, d, S.extra_d["subset_leak:" + key + ":" + std::to_string(d)]);
+        makemaps(S, S.binmap);
+        S.extra_d["subset_binmap:" + key].assign(S.binmap.begin(),
+                                                 S.binmap.begin() + (size_t)S.nopix_map * S.nmap);
+        if (pass == 1) {
+          S.extra_i["subset_hits:" + key] = S.nohits;
+          S.extra_i["subset_mask:" + key] = S.outmask;
+          S.extra_d["subset_cc:" + key].assign(S.cc.begin(),
+                                               S.cc.begin() + (size_t)S.nopix_map * nn);
+        }
+        table.insert(table.end(), {(double)pass, (double)isv, (double)ids, (double)S.nmap});
+        ++k;
+      }
+    }
+  }
+  S.extra_d["subsets"] = table;
+  S.nmap = nmap_save;
+  S.par.kfirst = kfirst_save;
+  S.par.do_binmap = binmap_save;
+  S.detflags.clear();
+  S.surveyflags.clear();
+  S.cc = cc0;
+  S.binmap = bin0;
+  S.nohits = hits0;
+  S.outmask = mask0;
+  S.crit = crit0;
+}
+
 // clean_tod (smadam_routines.f90:1545-1585)
 void clean_tod(State &S) {
   const Params &p = S.par;
@@ -2231,6 +2402,11 @@ void run_destripe(State &S, long nperiod, const long *periods) {
   invert_pixelmatrix_map(S);
   makemaps(S, S.binmap);
   makemaps(S, S.map);
+  S.extra_d.clear();
+  S.extra_i.clear();
+  if (p.do_leakmatrix)
+    for (long d = 0; d < S.ndet; ++d) leakmatrix(S, d, S.extra_d["leakmatrix:" + std::to_string(d)]);
+  run_subsets(S);
   S.tod_cleaned = false;
   clean_tod(S);
   S.t_total = omp_get_wtime() - t0;
@@ -2264,6 +2440,9 @@ void run_cached(State &S) {
   }
   makemaps(S, S.binmap);
   makemaps(S, S.map);
+  S.extra_d.clear();
+  S.extra_i.clear();
+  run_subsets(S);
   S.tod_cleaned = false;
   clean_tod(S);
   S.t_total = omp_get_wtime() - t0;
@@ -2366,6 +2545,10 @@ long oracle_result_size(const char *name) {
   if (n == "rr_history") return (long)S.rr_history.size();
   if (n == "band_widths") return (long)S.band_widths.size();
   if (n == "scalars") return 12;
+  auto id = S.extra_d.find(n);
+  if (id != S.extra_d.end()) return (long)id->second.size();
+  auto ii = S.extra_i.find(n);
+  if (ii != S.extra_i.end()) return (long)ii->second.size();
   return -1;
 }
 
@@ -2398,6 +2581,10 @@ int oracle_result_copy(const char *name, void *dst) {
     std::memcpy(dst, v, sizeof v);
     return 0;
   }
+  auto id = S.extra_d.find(n);
+  if (id != S.extra_d.end()) return cp(id->second);
+  auto ii = S.extra_i.find(n);
+  if (ii != S.extra_i.end()) return cp(ii->second);
   return 1;
 }
 

@@ -118,12 +118,18 @@ _DT = dict(map=np.float64, binmap=np.float64, hits=np.int32, mask=np.int32, cc=n
            invcov=np.float64, rr_history=np.float64, band_widths=np.int64, scalars=np.float64)
 
 
+def _dtype(name):
+    if name in _DT:
+        return _DT[name]
+    return np.int32 if name.startswith(("subset_hits:", "subset_mask:")) else np.float64
+
+
 def result(name):
     L = lib()
     n = L.oracle_result_size(name.encode())
     if n < 0:
         raise KeyError(name)
-    out = np.empty(n, dtype=_DT[name])
+    out = np.empty(n, dtype=_dtype(name))
     if n:
         L.oracle_result_copy(name.encode(), _p(out))
     return out
