@@ -123,6 +123,11 @@ int madam_b200_last_error(char *buf, long buflen);
  * [ndet][noba]: baselines, RHS, F^T N^-1 F), "fcov" (float64
  * [npsdtot][nof/2+1]), "invcov" (float64 [npsdtot][nof]), "rr_history"
  * (float64 [niter]), "band_widths" (int64), "scalars" (float64 [22]),
+ * "leakmatrix:<d>" (float64 [npix][nmap][nmap], row i column j: the leakage
+ * matrix of detector d, write_leakmatrix), the subsets of bin_subsets
+ * (smadam.F90:954-1257) as "subsets" (float64 [nsub][4]: pass, survey, detector
+ * set, nmap) with "subset_binmap:<k>", "subset_hits:<k>", "subset_mask:<k>"
+ * (int32), "subset_cc:<k>", "subset_leak:<k>:<d>",
  * "timings" (float64 [9], milliseconds).  result_size returns elements or
  * -1; result_copy fails when nbytes is too small. */
 long madam_b200_result_size(const char *name);

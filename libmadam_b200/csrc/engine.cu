@@ -1266,5 +1266,6 @@ double now_ms() {
 #include "pair_kernels.inl"
 #include "engine_host.inl"
 #include "engine_batch.inl"
+#include "subsets.inl"
 
 }  // namespace madam

@@ -329,6 +329,26 @@ class Engine {
   std::vector<int32_t> orig_pix_values_;
   bool tod_cleaned_ = false;
 
+  // subsets and leakage matrices (subsets.inl)
+  void run_subsets();
+  void leak_matrices();
+  void subset_accumulate(const std::vector<uint8_t> &detflags, const std::vector<double2> &spans,
+                         int nmaps, double *cc, double *bin, int *hits);
+  std::vector<double> leak_product(const std::vector<double> &cinv,
+                                   const std::vector<double> &cdet, int nmaps);
+  std::vector<double> detector_matrix(long det, int nmaps);
+  static std::vector<double> full_sym(const std::vector<double> &packed, int nmaps);
+  // compacted per-pixel arrays (device or host) -> full sky, zeros elsewhere
+  void expand_to_sky(const void *dev, size_t elem, long per_pix, long nosubpix, void *out);
+  void expand_host(const void *host, size_t elem, long per_pix, long nosubpix, void *out);
+  const double *times_in_ = nullptr;  // the caller's timestamps
+  bool times_dev_ = false;
+  DevBuf<double> times_own_;
+  const double *subset_times_ = nullptr;
+  std::vector<double2> subset_spans_;
+  std::map<std::string, std::vector<double>> extra_d_;  // subset / leakage results
+  std::map<std::string, std::vector<int>> extra_i_;
+
   // FP32-TOD form
   bool fp32_next_ = false, fp32_ = false;
   float *sig32_caller_ = nullptr;  // caller's float32 signal (host or device)

@@ -1888,6 +1888,14 @@ void Engine::finalize(bool first_call) {
       }
     }
   }
+  // leakage matrices and subsets (smadam.F90:405-408, 430), binned from the
+  // TOD before clean_tod
+  extra_d_.clear();
+  extra_i_.clear();
+  if (!suppress_fits_) {
+    if (first_call && par_.do_leakmatrix) leak_matrices();
+    run_subsets();
+  }
   clean_tod();
   writeback_host();
   MADAM_CUDA(cudaStreamSynchronize(st_));
@@ -1899,7 +1907,8 @@ void Engine::write_fits(bool first_call) {
   // write_map / write_binmap / write_mask / write_hits / write_matrix
   // (smadam.F90:401-422, 756-764)
   const bool any = par_.do_map || par_.do_binmap ||
-                   (first_call && (par_.do_hits || par_.do_mask || par_.do_matrix || par_.do_wcov));
+                   (first_call && (par_.do_hits || par_.do_mask || par_.do_matrix || par_.do_wcov ||
+                                   par_.do_leakmatrix));
   if (!any) return;
   const long npix = 12 * par_.nside_map * par_.nside_map;
   std::vector<double> map((size_t)npix * nmap_), bin((size_t)npix * nmap_), ccinv;
@@ -1930,6 +1939,10 @@ void Engine::write_fits(bool first_call) {
   in.crit = crit.data();
   in.cc_raw = cc_raw_host_.empty() ? nullptr : cc_raw_host_.data();
   in.cc_inv = ccinv.empty() ? nullptr : ccinv.data();
+  for (long d = 0; d < ndet_; ++d) {
+    auto it = extra_d_.find("leakmatrix:" + std::to_string(d));
+    if (it != extra_d_.end()) in.leak.push_back({dets_[d].name, it->second.data()});
+  }
   write_products(in);
   cc_raw_host_.clear();
 }
@@ -2020,6 +2033,8 @@ void Engine::run(const Params &par, std::vector<Detector> dets, long ndet, long 
   tod_cleaned_ = false;
   cgp_.reset();
   d_pix_caller_ = is_device ? pix : nullptr;
+  times_in_ = timestamps;
+  times_dev_ = is_device;
   const long long n = (long long)ndet * nsamp;
   auto mark = [&](int i) {
     MADAM_CUDA(cudaStreamSynchronize(st_));
@@ -2112,7 +2127,8 @@ void Engine::run_cached(long ndet, long nsamp, long nnz, double *timestamps, int
   noiter = 0;
   tod_cleaned_ = false;
   d_pix_caller_ = is_device ? pix : nullptr;
-  (void)timestamps;
+  times_in_ = timestamps;
+  times_dev_ = is_device;
   fp32_ = false;  // destripe_with_cache takes float64 signals
   fp32_next_ = false;
   bind_inputs(timestamps, pix, pixweights, signal, is_device, false);
@@ -2143,6 +2159,27 @@ namespace {
 enum RKind { RK_DOUBLE, RK_INT, RK_FLOAT, RK_LONG };
 }
 
+// compacted per-pixel arrays (hit submaps only) -> the full sky
+void Engine::expand_host(const void *host, size_t elem, long per_pix, long nosubpix, void *out) {
+  const long total = nosubmaps_tot_ * nosubpix;
+  std::memset(out, 0, (size_t)total * per_pix * elem);
+  for (long j = 0; j < nolocmaps_; ++j) {
+    const long g = j + subtable2_[j];
+    std::memcpy((char *)out + (size_t)g * nosubpix * per_pix * elem,
+                (const char *)host + (size_t)j * nosubpix * per_pix * elem,
+                (size_t)nosubpix * per_pix * elem);
+  }
+}
+
+void Engine::expand_to_sky(const void *dev, size_t elem, long per_pix, long nosubpix,
+                           void *out) {
+  const long nloc_pix = nolocmaps_ * nosubpix;
+  std::vector<char> h((size_t)nloc_pix * per_pix * elem);
+  MADAM_CUDA(cudaStreamSynchronize(st_));  // the engine's stream does not order cudaMemcpy
+  if (nloc_pix) MADAM_CUDA(cudaMemcpy(h.data(), dev, h.size(), cudaMemcpyDeviceToHost));
+  expand_host(h.data(), elem, per_pix, nosubpix, out);
+}
+
 long Engine::result_size(const std::string &name) {
   const long npm = 12 * par_.nside_map * par_.nside_map;
   const long npc = 12 * par_.nside_cross * par_.nside_cross;
@@ -2163,6 +2200,10 @@ long Engine::result_size(const std::string &name) {
   if (name == "aa_batch") return nrhs_ * nb;
   if (name == "noiter_batch" || name == "rrinit_batch" || name == "rr_final_batch")
     return (long)noiter_b_.size();
+  auto ed = extra_d_.find(name);
+  if (ed != extra_d_.end()) return (long)ed->second.size();
+  auto ei = extra_i_.find(name);
+  if (ei != extra_i_.end()) return (long)ei->second.size();
   return -1;
 }
 
@@ -2174,20 +2215,8 @@ void Engine::result_copy(const std::string &name, void *dst, long nbytes) {
     if ((size_t)nbytes < (size_t)sz * elem) fail("result buffer too small for " + name);
   };
   MADAM_CUDA(cudaStreamSynchronize(st_));
-  // expand compacted per-pixel arrays to the full sky
   auto expand = [&](const void *dev, size_t elem, long per_pix, long nosubpix, void *out) {
-    const long nloc_pix = nolocmaps_ * nosubpix;
-    std::vector<char> h((size_t)nloc_pix * per_pix * elem);
-    if (nloc_pix)
-      MADAM_CUDA(cudaMemcpy(h.data(), dev, h.size(), cudaMemcpyDeviceToHost));
-    const long total = nosubmaps_tot_ * nosubpix;
-    std::memset(out, 0, (size_t)total * per_pix * elem);
-    for (long j = 0; j < nolocmaps_; ++j) {
-      const long g = j + subtable2_[j];
-      std::memcpy((char *)out + (size_t)g * nosubpix * per_pix * elem,
-                  h.data() + (size_t)j * nosubpix * per_pix * elem,
-                  (size_t)nosubpix * per_pix * elem);
-    }
+    expand_to_sky(dev, elem, per_pix, nosubpix, out);
   };
   auto sym = [&](const std::vector<double> &s6, long npix, double *out) {
     for (long p = 0; p < npix; ++p) {
@@ -2203,6 +2232,20 @@ void Engine::result_copy(const std::string &name, void *dst, long nbytes) {
     }
   };
   const long ncc = nmap_ == 3 ? 6 : 1;
+  {
+    auto ed = extra_d_.find(name);
+    if (ed != extra_d_.end()) {
+      need(sizeof(double));
+      std::memcpy(dst, ed->second.data(), ed->second.size() * sizeof(double));
+      return;
+    }
+    auto ei = extra_i_.find(name);
+    if (ei != extra_i_.end()) {
+      need(sizeof(int));
+      std::memcpy(dst, ei->second.data(), ei->second.size() * sizeof(int));
+      return;
+    }
+  }
   if (name == "map_batch" || name == "binmap_batch") {
     need(sizeof(double));
     const long long nv = (long long)nloc_ * nmap_;

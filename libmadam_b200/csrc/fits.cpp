@@ -6,7 +6,9 @@
 // component with nosubpix values per row ('E' float32 maps, 'J' hits and
 // mask, 'D' pixel matrices); unobserved map pixels hold the HEALPix
 // undefined value -1.6375e30.  Files are named <path_output><file_root>
-// _map.fits, _bmap.fits, _hmap.fits, _mask.fits, _wcov_inv.fits, _wcov.fits;
+// _map.fits, _bmap.fits, _hmap.fits, _mask.fits, _wcov_inv.fits, _wcov.fits,
+// _leakmatrix_<detector>.fits (write_leakmatrix 1181-1323), and the subset
+// products of run_subsets (smadam.F90:954-1257);
 // an existing file gets a _001, _002, ... suffix unless the name starts with
 // '!' (check_outfile, output.f90:1329-1366).
 #include "fits.h"
@@ -150,121 +152,188 @@ void write_table(const std::string &fname, const std::vector<Col> &cols, long lo
   std::fclose(f);
 }
 
-}  // namespace
+// HEALPix tables of one run (or one subset of it): full-sky host arrays at
+// nside_map with nmap components.
+class Tables {
+ public:
+  Tables(const Params &p, long nsub, long nsm, long ndet, int nmap)
+      : p_(p), nsub_(nsub), nsm_(nsm), ndet_(ndet), nmap_(nmap) {}
 
-void write_products(const FitsInput &in) {
-  const Params &p = *in.par;
-  std::string root = p.file_root;
-  std::string path = p.path_output;
-  if (!path.empty() && path.back() != '/') path += '/';
-  auto name = [&](const std::string &suffix) {
-    std::string f = root + suffix;
-    if (!f.empty() && f[0] == '!') return "!" + path + f.substr(1);
-    return path + f;
-  };
-  const long nsub = in.nosubpix_map, nsm = in.nosubmaps_tot, npix = nsub * nsm;
-  const int nmap = in.nmap;
-  const char *mapnames[3] = {"TEMPERATURE", "Q-POLARISATION", "U-POLARISATION"};
-  auto healpix = [&](Header &h) {
-    h.str("PIXTYPE", "HEALPIX", "HEALPIX Pixelisation");
-    h.str("ORDERING", "NESTED", "Pixel ordering scheme");
-    h.integer("NSIDE", p.nside_map, "Resolution parameter for HEALPIX");
-    h.integer("FIRSTPIX", 0, "First pixel # (0 based)");
-    h.integer("LASTPIX", 12LL * p.nside_map * p.nside_map - 1, "Last pixel # (0 based)");
-    h.logical("POLAR", nmap != 1, "Polarisation included (True/False)");
-    h.str("POLCCONV", "COSMO", "Coord. convention for polarisation (COSMO/IAU)");
-    h.str("EXTNAME", "FULL SKY MAP");
-    h.str("OBJECT", "FULLSKY");
-    h.str("INDXSCHM", "IMPLICIT", "Indexing : IMPLICIT or EXPLICIT");
-    h.integer("GRAIN", 0, "Grain of pixel indexing");
-    h.str("CREATOR", "Madam", "Software creating FITS file");
-    h.integer("NODET", in.ndet, "Number of detectors");
-    h.real("FSAMPLE", p.fsample, "Sampling frequency (Hz)");
-    h.integer("NSIDESUB", p.nside_submap, "Submap resolution");
-    h.integer("NSIDECR", p.nside_cross, "Crossing point resolution");
-  };
-  auto map_file = [&](const std::string &suffix, const double *m, const char *objtype) {
-    const std::string f = resolve(name(suffix));
+  void map(const std::string &f, const double *m, const int *mask, const char *objtype) {
     if (f.empty()) return;
+    const char *mapnames[3] = {"TEMPERATURE", "Q-POLARISATION", "U-POLARISATION"};
     std::vector<Col> cols;
-    for (int j = 0; j < nmap; ++j)
-      cols.push_back({nmap == 3 ? mapnames[j] : "TEMPERATURE", std::to_string(nsub) + "E",
-                      p.unit_tod, (int)(4 * nsub)});
+    for (int j = 0; j < nmap_; ++j)
+      cols.push_back({nmap_ == 3 ? mapnames[j] : "TEMPERATURE", std::to_string(nsub_) + "E",
+                      p_.unit_tod, (int)(4 * nsub_)});
     auto keys = [&](Header &h) {
       h.str("OBJTYPE", objtype, "Object type");
       healpix(h);
-      h.logical("MONOPOLE", p.rm_monopole, "Monopole removed (T map)");
+      h.logical("MONOPOLE", p_.rm_monopole, "Monopole removed (T map)");
     };
-    write_table(f, cols, nsm, keys, [&](long long r, std::vector<unsigned char> &b) {
-      for (int j = 0; j < nmap; ++j)
-        for (long i = 0; i < nsub; ++i) {
-          const long px = r * nsub + i;
-          const float v = in.mask[px] > 0 ? (float)m[px * nmap + j] : kUndef;
+    write_table(f, cols, nsm_, keys, [&](long long r, std::vector<unsigned char> &b) {
+      for (int j = 0; j < nmap_; ++j)
+        for (long i = 0; i < nsub_; ++i) {
+          const long px = r * nsub_ + i;
+          const float v = mask[px] > 0 ? (float)m[px * nmap_ + j] : kUndef;
           put_be(b, v);
         }
     });
-  };
-  if (p.do_map && in.map) map_file("_map.fits", in.map, "madam.map");
-  if (p.do_binmap && in.binmap) map_file("_bmap.fits", in.binmap, "madam.binmap");
-  if (in.first_call && p.do_hits && in.hits) {
-    const std::string f = resolve(name("_hmap.fits"));
-    if (!f.empty()) {
-      long rep = std::max<long>(12 * 1024, nsub);
-      rep = std::min<long>(rep, npix);
-      const long nrows = (npix + rep - 1) / rep;
-      std::vector<Col> cols = {{"Total hits", std::to_string(rep) + "J", "", (int)(4 * rep)}};
-      auto keys = [&](Header &h) {
-        h.str("OBJTYPE", "madam.hits", "Object type");
-        healpix(h);
-      };
-      write_table(f, cols, nrows, keys, [&](long long r, std::vector<unsigned char> &b) {
-        for (long i = 0; i < rep; ++i) {
-          const long px = r * rep + i;
-          put_be(b, (int32_t)(px < npix ? in.hits[px] : 0));
-        }
-      });
-    }
   }
-  if (in.first_call && p.do_mask && in.mask) {
-    const std::string f = resolve(name("_mask.fits"));
-    if (!f.empty()) {
-      std::vector<Col> cols = {{"Mask", std::to_string(nsub) + "J", "", (int)(4 * nsub)},
-                               {"criterion", std::to_string(nsub) + "E", "", (int)(4 * nsub)}};
-      auto keys = [&](Header &h) {
-        h.str("OBJTYPE", "madam.mask", "Object type");
-        healpix(h);
-      };
-      write_table(f, cols, nsm, keys, [&](long long r, std::vector<unsigned char> &b) {
-        for (long i = 0; i < nsub; ++i) put_be(b, (int32_t)in.mask[r * nsub + i]);
-        for (long i = 0; i < nsub; ++i) put_be(b, in.crit ? in.crit[r * nsub + i] : 0.0f);
-      });
-    }
+
+  void hits(const std::string &f, const int *hits) {
+    if (f.empty()) return;
+    const long npix = nsub_ * nsm_;
+    long rep = std::max<long>(12 * 1024, nsub_);
+    rep = std::min<long>(rep, npix);
+    const long nrows = (npix + rep - 1) / rep;
+    std::vector<Col> cols = {{"Total hits", std::to_string(rep) + "J", "", (int)(4 * rep)}};
+    auto keys = [&](Header &h) {
+      h.str("OBJTYPE", "madam.hits", "Object type");
+      healpix(h);
+    };
+    write_table(f, cols, nrows, keys, [&](long long r, std::vector<unsigned char> &b) {
+      for (long i = 0; i < rep; ++i) {
+        const long px = r * rep + i;
+        put_be(b, (int32_t)(px < npix ? hits[px] : 0));
+      }
+    });
   }
-  auto matrix_file = [&](const std::string &suffix, const double *cc) {
-    const std::string f = resolve(name(suffix));
+
+  void mask(const std::string &f, const int *mask, const float *crit) {
+    if (f.empty()) return;
+    std::vector<Col> cols = {{"Mask", std::to_string(nsub_) + "J", "", (int)(4 * nsub_)},
+                             {"criterion", std::to_string(nsub_) + "E", "", (int)(4 * nsub_)}};
+    auto keys = [&](Header &h) {
+      h.str("OBJTYPE", "madam.mask", "Object type");
+      healpix(h);
+    };
+    write_table(f, cols, nsm_, keys, [&](long long r, std::vector<unsigned char> &b) {
+      for (long i = 0; i < nsub_; ++i) put_be(b, (int32_t)mask[r * nsub_ + i]);
+      for (long i = 0; i < nsub_; ++i) put_be(b, crit ? crit[r * nsub_ + i] : 0.0f);
+    });
+  }
+
+  // upper triangle of [npix][nmap][nmap] (write_matrix, output.f90:1031-1175)
+  void matrix(const std::string &f, const double *cc) {
     if (f.empty()) return;
     std::vector<Col> cols;
     std::vector<std::pair<int, int>> ij;
-    for (int i = 0; i < nmap; ++i)
-      for (int j = i; j < nmap; ++j) {
+    for (int i = 0; i < nmap_; ++i)
+      for (int j = i; j < nmap_; ++j) {
         cols.push_back({"cc(" + std::to_string(i + 1) + "," + std::to_string(j + 1) + ")",
-                        std::to_string(nsub) + "D", "", (int)(8 * nsub)});
+                        std::to_string(nsub_) + "D", "", (int)(8 * nsub_)});
         ij.push_back({i, j});
       }
     auto keys = [&](Header &h) {
       h.str("OBJTYPE", "madam.matrix", "Object type");
       healpix(h);
     };
-    write_table(f, cols, nsm, keys, [&](long long r, std::vector<unsigned char> &b) {
+    write_table(f, cols, nsm_, keys, [&](long long r, std::vector<unsigned char> &b) {
       for (auto e : ij)
-        for (long q = 0; q < nsub; ++q) {
-          const long px = r * nsub + q;
-          put_be(b, cc[(size_t)px * nmap * nmap + e.second * nmap + e.first]);
+        for (long q = 0; q < nsub_; ++q) {
+          const long px = r * nsub_ + q;
+          put_be(b, cc[(size_t)px * nmap_ * nmap_ + e.second * nmap_ + e.first]);
         }
     });
+  }
+
+  // every element gamma(i, j) of [npix][nmap][nmap], row i column j
+  // (write_leakmatrix, output.f90:1181-1323)
+  void leak(const std::string &f, const double *g) {
+    if (f.empty()) return;
+    std::vector<Col> cols;
+    for (int i = 0; i < nmap_; ++i)
+      for (int j = 0; j < nmap_; ++j)
+        cols.push_back({"gamma(" + std::to_string(i + 1) + "," + std::to_string(j + 1) + ")",
+                        std::to_string(nsub_) + "D", "", (int)(8 * nsub_)});
+    auto keys = [&](Header &h) {
+      h.str("OBJTYPE", "madam.leakmatrix", "Object type");
+      healpix(h);
+    };
+    write_table(f, cols, nsm_, keys, [&](long long r, std::vector<unsigned char> &b) {
+      for (int e = 0; e < nmap_ * nmap_; ++e)
+        for (long q = 0; q < nsub_; ++q) put_be(b, g[(size_t)(r * nsub_ + q) * nmap_ * nmap_ + e]);
+    });
+  }
+
+ private:
+  void healpix(Header &h) {
+    h.str("PIXTYPE", "HEALPIX", "HEALPIX Pixelisation");
+    h.str("ORDERING", "NESTED", "Pixel ordering scheme");
+    h.integer("NSIDE", p_.nside_map, "Resolution parameter for HEALPIX");
+    h.integer("FIRSTPIX", 0, "First pixel # (0 based)");
+    h.integer("LASTPIX", 12LL * p_.nside_map * p_.nside_map - 1, "Last pixel # (0 based)");
+    h.logical("POLAR", nmap_ != 1, "Polarisation included (True/False)");
+    h.str("POLCCONV", "COSMO", "Coord. convention for polarisation (COSMO/IAU)");
+    h.str("EXTNAME", "FULL SKY MAP");
+    h.str("OBJECT", "FULLSKY");
+    h.str("INDXSCHM", "IMPLICIT", "Indexing : IMPLICIT or EXPLICIT");
+    h.integer("GRAIN", 0, "Grain of pixel indexing");
+    h.str("CREATOR", "Madam", "Software creating FITS file");
+    h.integer("NODET", ndet_, "Number of detectors");
+    h.real("FSAMPLE", p_.fsample, "Sampling frequency (Hz)");
+    h.integer("NSIDESUB", p_.nside_submap, "Submap resolution");
+    h.integer("NSIDECR", p_.nside_cross, "Crossing point resolution");
+  }
+  const Params &p_;
+  long nsub_, nsm_, ndet_;
+  int nmap_;
+};
+
+// <path_output><file_root>[_<set>][_<survey>] (parameter_control.f90:48-63,
+// smadam.F90:1112-1116); a leading '!' of the root is kept in front
+std::string stem(const Params &p, const std::string &set, const std::string &survey) {
+  std::string path = p.path_output;
+  if (!path.empty() && path.back() != '/') path += '/';
+  std::string f = p.file_root;
+  if (!set.empty()) f += "_" + set;
+  if (!survey.empty()) f += "_" + survey;
+  if (!f.empty() && f[0] == '!') return "!" + path + f.substr(1);
+  return path + f;
+}
+
+}  // namespace
+
+void write_products(const FitsInput &in) {
+  const Params &p = *in.par;
+  const std::string root = stem(p, p.detsets[0].name, p.surveys[0].name);
+  Tables t(p, in.nosubpix_map, in.nosubmaps_tot, in.ndet, in.nmap);
+  if (p.do_map && in.map) t.map(resolve(root + "_map.fits"), in.map, in.mask, "madam.map");
+  if (p.do_binmap && in.binmap)
+    t.map(resolve(root + "_bmap.fits"), in.binmap, in.mask, "madam.binmap");
+  if (in.first_call && p.do_hits && in.hits) t.hits(resolve(root + "_hmap.fits"), in.hits);
+  if (in.first_call && p.do_mask && in.mask)
+    t.mask(resolve(root + "_mask.fits"), in.mask, in.crit);
+  if (in.first_call && p.do_matrix && in.cc_raw)
+    t.matrix(resolve(root + "_wcov_inv.fits"), in.cc_raw);
+  if (in.first_call && p.do_wcov && in.cc_inv) t.matrix(resolve(root + "_wcov.fits"), in.cc_inv);
+  if (in.first_call && p.do_leakmatrix)
+    for (const auto &lk : in.leak)
+      t.leak(resolve(root + "_leakmatrix_" + lk.first + ".fits"), lk.second);
+}
+
+void write_subset_products(const SubsetFits &in) {
+  // run_subsets (smadam.F90:1112-1224): names from the set and survey; a
+  // file that exists already is not written (skip_existing there)
+  const Params &p = *in.par;
+  const std::string sub = stem(p, in.set, in.survey);
+  auto fresh = [](const std::string &f) {
+    if (!f.empty() && f[0] == '!') return f.substr(1);  // overwrite, as cfitsio does
+    return exists(f) ? std::string() : f;
   };
-  if (in.first_call && p.do_matrix && in.cc_raw) matrix_file("_wcov_inv.fits", in.cc_raw);
-  if (in.first_call && p.do_wcov && in.cc_inv) matrix_file("_wcov.fits", in.cc_inv);
+  Tables t(p, in.nosubpix_map, in.nosubmaps_tot, in.ndet, in.nmap);
+  const bool last_map = in.pass == in.npass && p.do_map;
+  if (last_map) t.map(fresh(sub + "_map.fits"), in.binmap, in.mask, "madam.binmap");
+  else if (p.do_binmap || p.do_map) t.map(fresh(sub + "_bmap.fits"), in.binmap, in.mask, "madam.binmap");
+  if (in.pass != 1) return;
+  if (p.do_hits) t.hits(fresh(sub + "_hmap.fits"), in.hits);
+  if (p.do_matrix) t.matrix(fresh(sub + "_wcov_inv.fits"), in.cc_raw);
+  if (p.do_leakmatrix && !exists(sub + "_leakmatrix.fits"))
+    for (const auto &lk : in.leak)
+      t.leak(resolve(sub + "_leakmatrix.fits_" + lk.first + ".fits"), lk.second);
+  if (p.do_wcov) t.matrix(fresh(sub + "_wcov.fits"), in.cc_inv);
+  if (p.do_mask) t.mask(fresh(sub + "_mask.fits"), in.mask, in.crit);
 }
 
 }  // namespace madam

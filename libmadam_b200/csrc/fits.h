@@ -1,6 +1,10 @@
 // FITS products of destripe() (fits.cpp).
 #pragma once
 
+#include <string>
+#include <utility>
+#include <vector>
+
 #include "params.h"
 
 namespace madam {
@@ -18,8 +22,25 @@ struct FitsInput {
   const float *crit = nullptr;     // [npix]
   const double *cc_raw = nullptr;  // [npix][nmap][nmap] before inversion
   const double *cc_inv = nullptr;  // [npix][nmap][nmap] after inversion
+  // leakage matrices [npix][nmap][nmap] (row i, column j) by detector name
+  std::vector<std::pair<std::string, const double *>> leak;
 };
 
 void write_products(const FitsInput &in);
+
+// One subset of run_subsets: the products of one (pass, detector set, survey).
+struct SubsetFits {
+  const Params *par = nullptr;
+  long nosubpix_map = 0, nosubmaps_tot = 0, ndet = 0;
+  int nmap = 0, pass = 1, npass = 1;
+  std::string set, survey;
+  const double *binmap = nullptr;
+  const int *hits = nullptr, *mask = nullptr;
+  const float *crit = nullptr;
+  const double *cc_raw = nullptr, *cc_inv = nullptr;
+  std::vector<std::pair<std::string, const double *>> leak;
+};
+
+void write_subset_products(const SubsetFits &in);
 
 }  // namespace madam

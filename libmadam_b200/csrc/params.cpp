@@ -56,34 +56,51 @@ bool as_logical(const std::string &v, bool &out) {
   return true;
 }
 
-// parse_detset (inputparam.f90:375-434): only the count matters here
-void count_detset(Params &p, const std::string &value) {
+// parse_detset (inputparam.f90:375-434): "name : det, det, ..."; a name
+// with an empty or "all" member names the full detector set instead
+void count_detset(Params &p, const std::string &value, bool nopol) {
   size_t c = value.find(':');
   if (c == std::string::npos)
     fail("Failed to parse: " + strip(value) + " for valid detector set name");
-  if (strip(value.substr(0, c)).empty()) fail("Empty detset name");
+  const std::string name = strip(value.substr(0, c));
+  if (name.empty()) fail("Empty detset name");
+  Params::DetSet ds;
+  ds.name = name;
+  ds.nopol = nopol;
   std::string rest = strip(value.substr(c + 1));
   for (;;) {
     size_t k = rest.find(',');
     std::string det = strip(k == std::string::npos ? rest : rest.substr(0, k));
-    if (det.empty() || det == "all" || det == "All" || det == "ALL") return;
+    if (det.empty() || det == "all" || det == "All" || det == "ALL") {
+      p.detsets[0].name = name;
+      return;
+    }
+    ds.dets.push_back(det);
     if (k == std::string::npos) break;
     rest = strip(rest.substr(k + 1));
   }
+  p.detsets.push_back(ds);
   ++p.ndetset;
 }
 
-// parse_survey (inputparam.f90:438-492): only the count matters here
+// parse_survey (inputparam.f90:438-492): "name : start - stop, start - stop";
+// a name with no span or "all" names the full data span instead
 void count_survey(Params &p, const std::string &value) {
   size_t c = value.find(':');
   if (c == std::string::npos)
     fail("Failed to parse: " + strip(value) + " for valid survey name");
-  if (strip(value.substr(0, c)).empty()) fail("Empty survey name");
+  const std::string name = strip(value.substr(0, c));
+  if (name.empty()) fail("Empty survey name");
+  Params::Survey sv;
+  sv.name = name;
   std::string rest = strip(value.substr(c + 1));
   for (;;) {
     size_t dash = rest.find('-');
     if (dash == std::string::npos) {
-      if (rest.empty() || rest == "all" || rest == "All" || rest == "ALL") return;
+      if (rest.empty() || rest == "all" || rest == "All" || rest == "ALL") {
+        p.surveys[0].name = name;
+        return;
+      }
       fail("Failed to parse: " + rest + " for valid survey span marker (-)");
     }
     double a, b;
@@ -91,10 +108,13 @@ void count_survey(Params &p, const std::string &value) {
       fail("Failed to parse: " + rest + " for valid survey start");
     rest = strip(rest.substr(dash + 1));
     if (!as_real(rest, b)) fail("Failed to parse: " + rest + " for valid survey stop");
+    sv.starts.push_back(a);
+    sv.stops.push_back(b);
     size_t k = rest.find(',');
     if (k == std::string::npos) break;
     rest = strip(rest.substr(k + 1));
   }
+  p.surveys.push_back(sv);
   ++p.nsurvey;
 }
 
@@ -202,8 +222,9 @@ const std::unordered_map<std::string, Setter> &keytable() {
       {"binary_output", L(&Params::binary_output)},
       {"nwrite_binary", I(&Params::nwrite_binary)},
       {"file_covmat", S(&Params::file_covmat)},
-      {"detset", [](Params &p, const std::string &v) { count_detset(p, v); return true; }},
-      {"detset_nopol", [](Params &p, const std::string &v) { count_detset(p, v); return true; }},
+      {"detset", [](Params &p, const std::string &v) { count_detset(p, v, false); return true; }},
+      {"detset_nopol",
+       [](Params &p, const std::string &v) { count_detset(p, v, true); return true; }},
       {"survey", [](Params &p, const std::string &v) { count_survey(p, v); return true; }},
       {"bin_subsets", L(&Params::bin_subsets)},
       {"mcmode", L(&Params::mcmode)},

@@ -72,6 +72,19 @@ struct Params {
        do_leakmatrix = false;
   long nthreads = 1;
   int ndetset = 0, nsurvey = 0;
+  // detector sets and surveys (inputparam.f90:375-492); entry 0 is the full
+  // set / span, whose name an "all" definition sets
+  struct DetSet {
+    std::string name;
+    std::vector<std::string> dets;
+    bool nopol = false;
+  };
+  struct Survey {
+    std::string name;
+    std::vector<double> starts, stops;
+  };
+  std::vector<DetSet> detsets = std::vector<DetSet>(1);
+  std::vector<Survey> surveys = std::vector<Survey>(1);
 };
 
 // Parse "key = value;key = value;..." exactly as read_parameters does,

@@ -245,6 +245,32 @@ _RESULT_DTYPES = dict(map=np.float64, binmap=np.float64, hits=np.int32, mask=np.
                       rrinit_batch=np.float64, rr_final_batch=np.float64)
 
 
+def _result_dtype(name):
+    if name in _RESULT_DTYPES:
+        return _RESULT_DTYPES[name]
+    return np.int32 if name.startswith(("subset_hits:", "subset_mask:")) else np.float64
+
+
+def subsets():
+    """The subsets binned by the last call (bin_subsets with detset /
+    detset_nopol / survey parameters; smadam.F90:954-1257), in processing
+    order: a list of dicts with pass, survey and detset indices (0 = the full
+    set), nmap and the result names of its products ("subset_binmap:k" for
+    every pass; "subset_hits:k", "subset_mask:k", "subset_cc:k" and, with
+    write_leakmatrix, "subset_leak:k:<detector index>" for the first).  The
+    full-data leakage matrices are "leakmatrix:<detector index>".  Maps are
+    [npix, nmap], matrices [npix, nmap, nmap] (leakage: row i column j)."""
+    try:
+        tab = get_result("subsets").reshape(-1, 4)
+    except KeyError:
+        return []
+    out = []
+    for k, (ps, sv, ds, nm) in enumerate(tab):
+        out.append(dict(index=k, pass_=int(ps), survey=int(sv), detset=int(ds), nmap=int(nm),
+                        binmap="subset_binmap:%d" % k))
+    return out
+
+
 def get_result(name):
     """Host copy of a result of the last destripe call.
 
@@ -257,7 +283,7 @@ def get_result(name):
     n = L.madam_b200_result_size(name.encode())
     if n < 0:
         raise KeyError(name)
-    out = np.empty(n, dtype=_RESULT_DTYPES[name])
+    out = np.empty(n, dtype=_result_dtype(name))
     if n:
         _check(L.madam_b200_result_copy(name.encode(), out.ctypes.data_as(ct.c_void_p),
                                         out.nbytes))
