@@ -112,9 +112,27 @@ static int destripe_impl(bool fp32, int comm, char *parstring, long ndet, char *
     const bool dev = is_device_pointer(pix);
     if (fp32 && dev != is_device_pointer(signal))
       madam::fail("destripe_fp32: pixels and signal must both be host or both device memory");
-    engine().set_fp32(fp32);
-    engine().run(par, std::move(dets), ndet, nsamp, nnz, (double *)timestamps, (int32_t *)pix,
-                 (float *)pixweights, (double *)signal, nperiod, periods, dev);
+    Engine &e = engine();
+    e.clear_subchunk_results();
+    // subchunk passes (smadam.F90:192-196): isubchunk = 1 .. nsubchunk, then
+    // 0 (the full data) last, starting from the isubchunk parameter
+    const int nsub = par.nsubchunk >= 2 ? (int)par.nsubchunk : 0;
+    if (nsub && (par.isubchunk < 0 || par.isubchunk > nsub))
+      madam::fail("ERROR: isubchunk > nsubchunk");
+    // the reference's flag_bad_baselines flags whole baselines from a
+    // subchunk's sample count and those flags stay for the later passes;
+    // the passes here start from the caller's pointing each time
+    if (nsub && par.good_baseline_fraction != 0 && !par.kfilter)
+      madam::fail("good_baseline_fraction with nsubchunk > 1 is not supported");
+    for (int counter = nsub ? (int)par.isubchunk : 0; counter <= nsub; ++counter) {
+      const int isub = nsub ? (counter + 1) % (nsub + 1) : 0;
+      e.set_subchunk(isub, nsub);
+      e.set_fp32(fp32);
+      e.run(par, dets, ndet, nsamp, nnz, (double *)timestamps, (int32_t *)pix,
+            (float *)pixweights, (double *)signal, nperiod, periods, dev);
+      if (isub > 0) e.keep_subchunk_results(isub);
+    }
+    e.set_subchunk(0, 0);
   });
 }
 

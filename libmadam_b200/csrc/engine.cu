@@ -66,6 +66,19 @@ __device__ __forceinline__ int sample_pix(const float4 *p4, const int32_t *pc, l
 }
 
 // ---------------------------------------------------------------- setup --
+// samples outside [rg[2i], rg[2i+1]) of every interval i take the dummy pixel
+__global__ void k_subchunk_mask(int32_t *pix, long long n, long long nsamp, const long long *rg,
+                                int nrange, int dummy) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long s = i % nsamp;
+    bool in = false;
+    for (int r = 0; r < nrange; ++r)
+      if (rg[2 * r] <= s && s < rg[2 * r + 1]) in = true;
+    if (!in) pix[i] = dummy;
+  }
+}
+
 __global__ void k_minmax(const int32_t *pix, long long n, int *out) {
   int mn = INT_MAX, mx = INT_MIN;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;

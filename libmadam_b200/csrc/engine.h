@@ -128,6 +128,18 @@ class Engine {
   bool fp32() const { return fp32_; }
   long long pairs() const { return use_pairs_ ? npairs_ : 0; }
 
+  // Subchunk pass of the next run() (nsubchunk > 1): isub 1..nsub bins and
+  // solves only that subchunk of every interval; 0 is the full-data pass.
+  void set_subchunk(int isub, int nsub) {
+    isubchunk_ = isub;
+    nsubchunk_ = nsub;
+  }
+  void keep_subchunk_results(int isub);
+  void clear_subchunk_results() {
+    subchunk_d_.clear();
+    subchunk_i_.clear();
+  }
+
   bool cached() const { return cached_; }
   const Params &params() const { return par_; }
 
@@ -348,6 +360,9 @@ class Engine {
   std::vector<double2> subset_spans_;
   std::map<std::string, std::vector<double>> extra_d_;  // subset / leakage results
   std::map<std::string, std::vector<int>> extra_i_;
+  int isubchunk_ = 0, nsubchunk_ = 0;
+  std::map<std::string, std::vector<double>> subchunk_d_;  // products of subchunk passes
+  std::map<std::string, std::vector<int>> subchunk_i_;
 
   // FP32-TOD form
   bool fp32_next_ = false, fp32_ = false;

@@ -171,7 +171,7 @@ void Engine::init_layout(long nperiod, const long *periods) {
     p.nsubchunk = 0;
     p.isubchunk = 0;
   }
-  if (p.nsubchunk > 1) fail("nsubchunk > 1 is not supported");
+  if (p.isubchunk > p.nsubchunk) fail("ERROR: isubchunk > nsubchunk");
   if (p.good_baseline_fraction < 0 || p.good_baseline_fraction > 1)
     fail("ERROR: good_baseline_fraction must be in 0..1");
   if (p.nside_cross < 0) p.nside_cross = p.nside_map;
@@ -374,6 +374,30 @@ void Engine::flag_and_compact(bool first_call) {
   if (n > 0)
     MADAM_LAUNCH(k_dummy_ksub, grid_for(n), 256, 0, st_, pix_.get(), n, (int)dummy_global_,
                  (int)nosubpix_max_, ksub.get());
+  if (isubchunk_ > 0 && n > 0) {
+    // a subchunk pass (smadam.F90:194-196; parameter_control.f90:820-835):
+    // interval i contributes its samples [sublen (isub - 1), sublen isub) with
+    // sublen = len / nsubchunk (the last subchunk takes the rest); the other
+    // samples take the dummy pixel, which excludes them from every sum as the
+    // reference's subchunk test does.  The hit submaps stay those of the
+    // full data, as the reference compacts once before its passes.
+    std::vector<long long> rg;
+    long long off = 0;
+    for (long iv = 0; iv < ninterval_; ++iv) {
+      const long long len = intervals_[iv], sublen = len / nsubchunk_;
+      const long long a = off + sublen * (isubchunk_ - 1);
+      const long long b = isubchunk_ == nsubchunk_ ? off + len : a + sublen;
+      rg.push_back(a);
+      rg.push_back(b);
+      off += len;
+    }
+    DevBuf<long long> drg;
+    drg.alloc(rg.size());
+    MADAM_CUDA(cudaMemcpyAsync(drg.get(), rg.data(), rg.size() * sizeof(long long),
+                               cudaMemcpyHostToDevice, st_));
+    MADAM_LAUNCH(k_subchunk_mask, grid_for(n), 256, 0, st_, pix_.get(), n, (long long)nsamp_,
+                 drg.get(), (int)ninterval_, (int)dummy_global_);
+  }
   std::vector<int> ks(nosubmaps_tot_ + 1);
   MADAM_CUDA(cudaMemcpyAsync(ks.data(), ksub.get(), ks.size() * sizeof(int),
                              cudaMemcpyDeviceToHost, st_));
@@ -1841,6 +1865,7 @@ void Engine::clean_tod() {
   // clean_tod (smadam_routines.f90:1545-1585)
   if (!par_.write_tod && par_.ndetset == 0 && par_.nsurvey == 0) return;
   if (!par_.kfirst || tod_cleaned_) return;
+  if (isubchunk_ > 0) return;  // only the full-data pass cleans (smadam.F90:432)
   const long long n = (long long)ndet_ * nsamp_;
   const SampleMap sm = sample_map(istart_d_.get(), kstart_d_.get(), (int)ninterval_, nsamp_,
                                   noba_short_, fdn_);
@@ -1932,6 +1957,8 @@ void Engine::write_fits(bool first_call) {
   in.ndet = ndet_;
   in.nmap = nmap_;
   in.first_call = first_call;
+  in.isubchunk = isubchunk_;
+  in.nsubchunk = nsubchunk_;
   in.map = par_.do_map ? map.data() : nullptr;
   in.binmap = par_.do_binmap ? bin.data() : nullptr;
   in.hits = hits.data();
@@ -1949,9 +1976,10 @@ void Engine::write_fits(bool first_call) {
 
 void Engine::writeback_host() {
   // restore_pixels (pointing.f90:168-191): the caller's pixel buffer shows the
-  // reference's edits (flagged samples become 12 nside_max^2)
+  // reference's edits (flagged samples become 12 nside_max^2); a subchunk pass
+  // leaves the caller's buffers to the full-data pass that follows it
   const long long n = (long long)ndet_ * nsamp_;
-  if (n == 0) return;
+  if (n == 0 || isubchunk_ > 0) return;
   DevBuf<int> sub2;
   sub2.alloc(nosubmaps_tot_ + 1);
   std::vector<int> s2(subtable2_.begin(), subtable2_.end());
@@ -2204,7 +2232,28 @@ long Engine::result_size(const std::string &name) {
   if (ed != extra_d_.end()) return (long)ed->second.size();
   auto ei = extra_i_.find(name);
   if (ei != extra_i_.end()) return (long)ei->second.size();
+  auto sd = subchunk_d_.find(name);
+  if (sd != subchunk_d_.end()) return (long)sd->second.size();
+  auto si = subchunk_i_.find(name);
+  if (si != subchunk_i_.end()) return (long)si->second.size();
   return -1;
+}
+
+void Engine::keep_subchunk_results(int isub) {
+  // the products of subchunk pass isub, kept beside the full-data pass's
+  const std::string k = ":" + std::to_string(isub);
+  for (const char *nm : {"map", "binmap"}) {
+    std::vector<double> &v = subchunk_d_[std::string("subchunk_") + nm + k];
+    v.resize(result_size(nm));
+    result_copy(nm, v.data(), (long)(v.size() * sizeof(double)));
+  }
+  for (const char *nm : {"hits", "mask"}) {
+    std::vector<int> &v = subchunk_i_[std::string("subchunk_") + nm + k];
+    v.resize(result_size(nm));
+    result_copy(nm, v.data(), (long)(v.size() * sizeof(int)));
+  }
+  for (auto &e : extra_d_) subchunk_d_["subchunk" + k + "/" + e.first] = e.second;
+  for (auto &e : extra_i_) subchunk_i_["subchunk" + k + "/" + e.first] = e.second;
 }
 
 void Engine::result_copy(const std::string &name, void *dst, long nbytes) {
@@ -2233,6 +2282,18 @@ void Engine::result_copy(const std::string &name, void *dst, long nbytes) {
   };
   const long ncc = nmap_ == 3 ? 6 : 1;
   {
+    auto sd = subchunk_d_.find(name);
+    if (sd != subchunk_d_.end()) {
+      need(sizeof(double));
+      std::memcpy(dst, sd->second.data(), sd->second.size() * sizeof(double));
+      return;
+    }
+    auto si = subchunk_i_.find(name);
+    if (si != subchunk_i_.end()) {
+      need(sizeof(int));
+      std::memcpy(dst, si->second.data(), si->second.size() * sizeof(int));
+      return;
+    }
     auto ed = extra_d_.find(name);
     if (ed != extra_d_.end()) {
       need(sizeof(double));

@@ -293,24 +293,40 @@ std::string stem(const Params &p, const std::string &set, const std::string &sur
   return path + f;
 }
 
+// add_subchunk_id (smadam.F90:1285-1314): "_sub<i>of<n>" before the last
+// '.' (at the end when there is none); one digit each below 10 subchunks,
+// two from 10
+std::string subchunk_id(const std::string &f, int isub, int nsub) {
+  if (f.empty() || isub == 0) return f;
+  char tag[32];
+  if (nsub < 10) std::snprintf(tag, sizeof tag, "_sub%1dof%1d", isub, nsub);
+  else std::snprintf(tag, sizeof tag, "_sub%02dof%02d", isub, nsub);
+  const size_t dot = f.rfind('.');
+  if (dot == std::string::npos) return f + tag;
+  return f.substr(0, dot) + tag + f.substr(dot);
+}
+
 }  // namespace
 
 void write_products(const FitsInput &in) {
   const Params &p = *in.par;
   const std::string root = stem(p, p.detsets[0].name, p.surveys[0].name);
+  auto nm = [&](const std::string &suffix) {
+    return resolve(subchunk_id(root + suffix, in.isubchunk, in.nsubchunk));
+  };
   Tables t(p, in.nosubpix_map, in.nosubmaps_tot, in.ndet, in.nmap);
-  if (p.do_map && in.map) t.map(resolve(root + "_map.fits"), in.map, in.mask, "madam.map");
-  if (p.do_binmap && in.binmap)
-    t.map(resolve(root + "_bmap.fits"), in.binmap, in.mask, "madam.binmap");
-  if (in.first_call && p.do_hits && in.hits) t.hits(resolve(root + "_hmap.fits"), in.hits);
-  if (in.first_call && p.do_mask && in.mask)
-    t.mask(resolve(root + "_mask.fits"), in.mask, in.crit);
-  if (in.first_call && p.do_matrix && in.cc_raw)
-    t.matrix(resolve(root + "_wcov_inv.fits"), in.cc_raw);
-  if (in.first_call && p.do_wcov && in.cc_inv) t.matrix(resolve(root + "_wcov.fits"), in.cc_inv);
-  if (in.first_call && p.do_leakmatrix)
-    for (const auto &lk : in.leak)
-      t.leak(resolve(root + "_leakmatrix_" + lk.first + ".fits"), lk.second);
+  if (p.do_map && in.map) t.map(nm("_map.fits"), in.map, in.mask, "madam.map");
+  if (p.do_binmap && in.binmap) t.map(nm("_bmap.fits"), in.binmap, in.mask, "madam.binmap");
+  if (in.first_call && p.do_hits && in.hits) t.hits(nm("_hmap.fits"), in.hits);
+  if (in.first_call && p.do_mask && in.mask) t.mask(nm("_mask.fits"), in.mask, in.crit);
+  if (in.first_call && p.do_matrix && in.cc_raw) t.matrix(nm("_wcov_inv.fits"), in.cc_raw);
+  if (in.first_call && p.do_wcov && in.cc_inv) t.matrix(nm("_wcov.fits"), in.cc_inv);
+  if (in.first_call && p.do_leakmatrix) {
+    // file_leakmatrix = <stem>_leakmatrix (parameter_control.f90:61), then
+    // write_leakmatrix appends _<detector>.fits (output.f90:1199)
+    const std::string base = subchunk_id(root + "_leakmatrix", in.isubchunk, in.nsubchunk);
+    for (const auto &lk : in.leak) t.leak(resolve(base + "_" + lk.first + ".fits"), lk.second);
+  }
 }
 
 void write_subset_products(const SubsetFits &in) {
@@ -318,7 +334,8 @@ void write_subset_products(const SubsetFits &in) {
   // file that exists already is not written (skip_existing there)
   const Params &p = *in.par;
   const std::string sub = stem(p, in.set, in.survey);
-  auto fresh = [](const std::string &f) {
+  auto fresh = [&](const std::string &f0) {
+    const std::string f = subchunk_id(f0, in.isubchunk, in.nsubchunk);
     if (!f.empty() && f[0] == '!') return f.substr(1);  // overwrite, as cfitsio does
     return exists(f) ? std::string() : f;
   };
@@ -329,9 +346,9 @@ void write_subset_products(const SubsetFits &in) {
   if (in.pass != 1) return;
   if (p.do_hits) t.hits(fresh(sub + "_hmap.fits"), in.hits);
   if (p.do_matrix) t.matrix(fresh(sub + "_wcov_inv.fits"), in.cc_raw);
-  if (p.do_leakmatrix && !exists(sub + "_leakmatrix.fits"))
-    for (const auto &lk : in.leak)
-      t.leak(resolve(sub + "_leakmatrix.fits_" + lk.first + ".fits"), lk.second);
+  const std::string lbase = subchunk_id(sub + "_leakmatrix.fits", in.isubchunk, in.nsubchunk);
+  if (p.do_leakmatrix && !exists(lbase))
+    for (const auto &lk : in.leak) t.leak(resolve(lbase + "_" + lk.first + ".fits"), lk.second);
   if (p.do_wcov) t.matrix(fresh(sub + "_wcov.fits"), in.cc_inv);
   if (p.do_mask) t.mask(fresh(sub + "_mask.fits"), in.mask, in.crit);
 }

@@ -15,6 +15,7 @@ struct FitsInput {
   long nosubpix_map = 0, nosubmaps_tot = 0, ndet = 0;
   int nmap = 0;
   bool first_call = true;          // destripe (all products) or destripe_with_cache (maps)
+  int isubchunk = 0, nsubchunk = 0;  // subchunk pass: names get _sub<i>of<n>
   const double *map = nullptr;     // [npix][nmap]
   const double *binmap = nullptr;  // [npix][nmap]
   const int *hits = nullptr;       // [npix]
@@ -33,6 +34,7 @@ struct SubsetFits {
   const Params *par = nullptr;
   long nosubpix_map = 0, nosubmaps_tot = 0, ndet = 0;
   int nmap = 0, pass = 1, npass = 1;
+  int isubchunk = 0, nsubchunk = 0;
   std::string set, survey;
   const double *binmap = nullptr;
   const int *hits = nullptr, *mask = nullptr;

@@ -269,6 +269,7 @@ static long serve_submit(bool fp32, void *srv, char *parstring, long ndet, char 
     std::unique_ptr<Job> j(new Job());
     j->par = madam::parse_parstring(parstring);
     if (j->par.mcmode) madam::fail("mcmode jobs are not served");
+    if (j->par.nsubchunk > 1) madam::fail("nsubchunk > 1 jobs are not served");
     if (j->par.temperature_only && nnz != 1)
       madam::fail("temperature_only=T but pointing weights are polarized");
     if (ndet <= 0 || nsamp <= 0 || nnz <= 0) madam::fail("empty data");

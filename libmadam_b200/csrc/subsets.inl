@@ -339,6 +339,8 @@ void Engine::run_subsets() {
           sf.nmap = nms;
           sf.pass = pass;
           sf.npass = npass;
+          sf.isubchunk = isubchunk_;
+          sf.nsubchunk = nsubchunk_;
           sf.set = p.detsets[ids].name;
           sf.survey = p.surveys[isv].name;
           sf.binmap = bm.data();

@@ -806,6 +806,9 @@ struct State {
 
   // subsets (run_subsets): empty = every detector / sample
   std::vector<char> detflags, surveyflags;
+  // subchunks (nsubchunk > 1): subchunk of every sample index, the pass's one
+  int isubchunk = 0, nsubchunk = 0;
+  std::vector<int> subchunk;
   // subset and leakage products, by result name
   std::map<std::string, std::vector<double>> extra_d;
   std::map<std::string, std::vector<int>> extra_i;
@@ -814,7 +817,13 @@ struct State {
 };
 
 inline bool det_on(const State &S, long d) { return S.detflags.empty() || S.detflags[d]; }
-inline bool samp_on(const State &S, long i) { return S.surveyflags.empty() || S.surveyflags[i]; }
+// `if (isubchunk /= 0 .and. subchunk(i) /= isubchunk) cycle` of every sample loop
+inline bool sub_on(const State &S, long i) {
+  return S.isubchunk == 0 || S.subchunk[i] == S.isubchunk;
+}
+inline bool samp_on(const State &S, long i) {
+  return (S.surveyflags.empty() || S.surveyflags[i]) && sub_on(S, i);
+}
 
 State *g_state = nullptr;
 std::string g_error;
@@ -1015,7 +1024,8 @@ void init_parameters(State &S) {
     p.nsubchunk = 0;
     p.isubchunk = 0;
   }
-  if (p.nsubchunk > 1) fail("nsubchunk > 1 is not supported");
+  if (p.isubchunk > p.nsubchunk) fail("ERROR: isubchunk > nsubchunk");
+  S.nsubchunk = (int)p.nsubchunk;
   if (p.good_baseline_fraction < 0 || p.good_baseline_fraction > 1)
     fail("ERROR: good_baseline_fraction must be in 0..1");
   if (p.nside_cross < 0) p.nside_cross = p.nside_map;
@@ -1134,6 +1144,20 @@ void start_timeloop(State &S) {
   }
   S.btime.assign(S.noba_short, 0);
   for (long k = 0; k < S.noba_short; ++k) S.btime[k] = S.times[S.bstart[k]];
+  // split every interval into subchunks (parameter_control.f90:820-835)
+  if (S.nsubchunk > 0) {
+    S.subchunk.assign(S.nsamp, 0);
+    long off = 0;
+    for (long i = 0; i < S.ninterval; ++i) {
+      const long n = S.intervals[i], sublen = n / S.nsubchunk;
+      for (int isub = 1; isub <= S.nsubchunk; ++isub) {
+        const long a = off + sublen * (isub - 1);
+        const long b = isub == S.nsubchunk ? off + n : a + sublen;
+        for (long j = a; j < b; ++j) S.subchunk[j] = isub;
+      }
+      off += n;
+    }
+  }
 }
 
 // init_filter (noise_routines.f90:242-292)
@@ -1635,6 +1659,7 @@ void initialize_a(State &S) {
       for (long k = ks; k < ks + noba; ++k) {
         double y = 0, n = 0;
         for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+          if (!sub_on(S, i)) continue;
           size_t s = (size_t)d * S.nsamp + i;
           long ip = S.pixels[s];
           if (ip == S.dummy_pixel) continue;
@@ -2013,6 +2038,7 @@ void iterate_a(State &S) {
           for (long k = ks; k < ks + noba; ++k) {
             double pw = pv[d * S.noba_short + k] * detw;
             for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+              if (!sub_on(S, i)) continue;
               size_t s = (size_t)d * S.nsamp + i;
               long ip = S.pixels[s];
               if (ip < first || ip > last) continue;
@@ -2049,6 +2075,7 @@ void iterate_a(State &S) {
       for (long k = ks; k < ks + noba; ++k) {
         double apn = 0;
         for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+          if (!sub_on(S, i)) continue;
           size_t s = (size_t)d * S.nsamp + i;
           long ip = S.pixels[s];
           if (ip == S.dummy_pixel) continue;
@@ -2101,6 +2128,7 @@ void subtract_baselines_a(State &S) {
       if (detw == 0) continue;
       for (long k = ks; k < ks + noba; ++k)
         for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+          if (!sub_on(S, i)) continue;
           size_t s = (size_t)d * S.nsamp + i;
           long ip = S.pixels[s];
           if (ip == S.dummy_pixel) continue;
@@ -2267,8 +2295,9 @@ void clean_tod(State &S) {
   for (long d = 0; d < S.ndet; ++d)
     for (long k = 0; k < S.noba_short; ++k)
       for (long i = S.bstart[k]; i <= S.bstop[k]; ++i)
-        S.tod[(size_t)d * S.nsamp + i] =
-            S.tod[(size_t)d * S.nsamp + i] - 1.0 * S.aa[d * S.noba_short + k];
+        if (sub_on(S, i))
+          S.tod[(size_t)d * S.nsamp + i] =
+              S.tod[(size_t)d * S.nsamp + i] - 1.0 * S.aa[d * S.noba_short + k];
   S.tod_cleaned = true;
 }
 
@@ -2293,7 +2322,7 @@ void flag_bad_baselines(State &S) {
     for (long k = 0; k < S.noba_short; ++k) {
       long ngood = 0;
       for (long i = S.bstart[k]; i <= S.bstop[k]; ++i)
-        if (S.pixels[(size_t)d * S.nsamp + i] != S.dummy_pixel) ++ngood;
+        if (sub_on(S, i) && S.pixels[(size_t)d * S.nsamp + i] != S.dummy_pixel) ++ngood;
       long len = S.bstop[k] - S.bstart[k] + 1;
       if (ngood > 0 && ngood < S.par.good_baseline_fraction * len)
         for (long i = S.bstart[k]; i <= S.bstop[k]; ++i)
@@ -2383,32 +2412,60 @@ void run_destripe(State &S, long nperiod, const long *periods) {
   reduce_pixels(S);
   update_maptod_transfer(S);
   S.dummy_pixel = 12 * S.nside_max * S.nside_max;
-  S.aa.assign((size_t)S.noba_short * S.ndet, 0.0);
-  S.yba.assign((size_t)S.noba_short * S.ndet, 0.0);
-  S.nna.assign((size_t)S.noba_short * S.ndet, 0.0);
-  S.nna_inv.assign((size_t)S.noba_short * S.ndet, 0.0);
-  allocate_maps(S);
-  if (p.kfirst) flag_bad_baselines(S);
-  pixel_matrix(S);
-  count_hits(S);
-  bin_tod(S);
-  if (p.kfirst) {
-    invert_pixelmatrix_cross(S);
-    initialize_a(S);
-    construct_preconditioner(S);
-    iterate_a(S);
-    subtract_baselines_a(S);
-  }
-  invert_pixelmatrix_map(S);
-  makemaps(S, S.binmap);
-  makemaps(S, S.map);
   S.extra_d.clear();
   S.extra_i.clear();
-  if (p.do_leakmatrix)
-    for (long d = 0; d < S.ndet; ++d) leakmatrix(S, d, S.extra_d["leakmatrix:" + std::to_string(d)]);
-  run_subsets(S);
-  S.tod_cleaned = false;
-  clean_tod(S);
+  // the subchunk passes (smadam.F90:192-196): isubchunk = 1 .. nsubchunk,
+  // then 0 (the full data), starting from the isubchunk parameter; a pass
+  // keeps the samples of its subchunk only (sub_on in every sample loop)
+  const int nsub = S.nsubchunk;
+  for (int counter = nsub ? (int)p.isubchunk : 0; counter <= nsub; ++counter) {
+    S.isubchunk = nsub ? (counter + 1) % (nsub + 1) : 0;
+    S.aa.assign((size_t)S.noba_short * S.ndet, 0.0);
+    S.yba.assign((size_t)S.noba_short * S.ndet, 0.0);
+    S.nna.assign((size_t)S.noba_short * S.ndet, 0.0);
+    S.nna_inv.assign((size_t)S.noba_short * S.ndet, 0.0);
+    allocate_maps(S);
+    if (p.kfirst) flag_bad_baselines(S);
+    pixel_matrix(S);
+    count_hits(S);
+    bin_tod(S);
+    if (p.kfirst) {
+      invert_pixelmatrix_cross(S);
+      initialize_a(S);
+      construct_preconditioner(S);
+      iterate_a(S);
+      subtract_baselines_a(S);
+    }
+    invert_pixelmatrix_map(S);
+    makemaps(S, S.binmap);
+    makemaps(S, S.map);
+    std::map<std::string, std::vector<double>> keep_d;
+    std::map<std::string, std::vector<int>> keep_i;
+    keep_d.swap(S.extra_d);
+    keep_i.swap(S.extra_i);
+    if (p.do_leakmatrix)
+      for (long d = 0; d < S.ndet; ++d)
+        leakmatrix(S, d, S.extra_d["leakmatrix:" + std::to_string(d)]);
+    run_subsets(S);
+    S.tod_cleaned = false;
+    if (S.isubchunk == 0) {
+      clean_tod(S);  // the full-data baselines only (smadam.F90:432-437)
+      for (auto &e : keep_d) S.extra_d[e.first] = e.second;
+      for (auto &e : keep_i) S.extra_i[e.first] = e.second;
+    } else {
+      // the pass's products, kept beside the full-data pass's
+      const std::string k = ":" + std::to_string(S.isubchunk);
+      for (auto &e : S.extra_d) keep_d["subchunk" + k + "/" + e.first] = e.second;
+      for (auto &e : S.extra_i) keep_i["subchunk" + k + "/" + e.first] = e.second;
+      keep_d["subchunk_map" + k] = S.map;
+      keep_d["subchunk_binmap" + k] = S.binmap;
+      keep_i["subchunk_hits" + k] = S.nohits;
+      keep_i["subchunk_mask" + k] = S.outmask;
+      S.extra_d.swap(keep_d);
+      S.extra_i.swap(keep_i);
+    }
+  }
+  S.isubchunk = 0;
   S.t_total = omp_get_wtime() - t0;
 }
 
@@ -2471,6 +2528,7 @@ int oracle_destripe(int comm, const char *parstring, long ndet,
     Params p = read_parameters(parstring);
     if (g_state && p.mcmode && g_state->cached)
       fail("Destripe called while caches are not empty.");
+    if (p.mcmode && p.nsubchunk > 1) fail("MCMode is not compatible with nsubchunk > 1.");
     if (p.temperature_only && nnz != 1)
       fail("temperature_only=T but pointing weights are polarized");
     if (ndet > 10000) fail("ndet > NDETMAX");

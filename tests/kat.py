@@ -22,7 +22,7 @@ def load(name):
 
 
 def libmadam_pars(nside, nside_cross, nside_submap):
-    # test_libmadam.py:47-76 minus the subset / subchunk / FITS-only keys
+    # test_libmadam.py:47-76 (the subset / subchunk keys are added by the caller)
     return {
         "base_first": 1.0, "fsample": 32.5, "nside_map": nside, "nside_cross": nside_cross,
         "nside_submap": nside_submap, "write_map": True, "write_binmap": True,
@@ -39,8 +39,12 @@ def run_libmadam_kat(backend, check_files=False):
     g = load("kat_libmadam.npz")
     nside = 8
     out = []
+    nsamp = g["timestamps"].size
     for i in range(2):
         pars = libmadam_pars(nside, 4, 2)
+        # the reference test's remaining keys (test_libmadam.py:58-77)
+        pars.update(write_leakmatrix=True, nsubchunk=2, bin_subsets=True,
+                    survey=["hm1 : {} - {}".format(0, nsamp / 2)])
         pixels = g["pixels"].copy()
         signal = g["signal"].copy()
         backend.destripe(pars, DETS, np.ones(4), g["timestamps"].copy(), pixels,
@@ -78,6 +82,14 @@ def run_libmadam_kat(backend, check_files=False):
                                        backend.result("map")[good].astype(np.float32), rtol=1e-6)
             for suffix in ("_wcov_inv.fits", "_wcov.fits"):
                 assert os.path.exists(os.path.join(pars["path_output"], "madam_pytest" + suffix))
+            # the subchunk hit maps add up to the full one (test_libmadam.py:171-174)
+            h1 = read_table(os.path.join(pars["path_output"], "madam_pytest_hmap_sub1of2.fits"))
+            h2 = read_table(os.path.join(pars["path_output"], "madam_pytest_hmap_sub2of2.fits"))
+            np.testing.assert_array_equal(h1[1]["Total hits"] + h2[1]["Total hits"], expect_h)
+            assert os.path.exists(os.path.join(pars["path_output"],
+                                               "madam_pytest_hm1_hmap_sub1of2.fits"))
+        np.testing.assert_array_equal(backend.result("subchunk_hits:1")
+                                      + backend.result("subchunk_hits:2"), expect_h)
         out.append((hits, binmap, backend.result("map"), backend.result("aa")))
         nside *= 2
     return out

@@ -121,7 +121,11 @@ _DT = dict(map=np.float64, binmap=np.float64, hits=np.int32, mask=np.int32, cc=n
 def _dtype(name):
     if name in _DT:
         return _DT[name]
-    return np.int32 if name.startswith(("subset_hits:", "subset_mask:")) else np.float64
+    base = name.split("/")[-1]
+    ints = ("subset_hits:", "subset_mask:", "subchunk_hits:", "subchunk_mask:")
+    if base in ("hits", "mask") or base.startswith(ints):
+        return np.int32
+    return np.float64
 
 
 def result(name):
