@@ -1270,10 +1270,33 @@ void build_filter(State &S) {
 }
 
 // reduce_pixels (pointing.f90:115-163)
+// ---- a run over several ranks (the reference's MPI layer,
+// mpi_wrappers.f90 / maptod_transfer.f90).  Every rank holds its own
+// detectors and the whole map: the reference's reductions (collect_map,
+// collect_cc, collect_hits, sum_mpi of inner products and counts) become sum
+// all-reduces of the replicated arrays and reduce_pixels' submap table a max
+// all-reduce.  The all-reduce is the caller's function (op 0 sum, 1 max).
+typedef void (*AllreduceFn)(double *buf, long n, int op);
+AllreduceFn g_allreduce = nullptr;
+int g_rank = 0, g_nranks = 1;
+
+void allreduce(double *buf, long n, int op) {
+  if (g_allreduce && g_nranks > 1 && n > 0) g_allreduce(buf, n, op);
+}
+double allreduce_sum(double v) {
+  allreduce(&v, 1, 0);
+  return v;
+}
+
 void reduce_pixels(State &S) {
   S.ksubmap.assign(S.nosubmaps_tot + 1, 0);
   size_t ntot = (size_t)S.ndet * S.nsamp;
   for (size_t i = 0; i < ntot; ++i) S.ksubmap[S.pixels[i] / S.nosubpix_max] = 1;
+  if (g_nranks > 1) {
+    std::vector<double> k(S.ksubmap.begin(), S.ksubmap.end());
+    allreduce(k.data(), (long)k.size(), 1);
+    for (size_t i = 0; i < k.size(); ++i) S.ksubmap[i] = k[i] > 0 ? 1 : 0;
+  }
   S.ksubmap[S.nosubmaps_tot] = 1;
   S.subtable1.assign(S.nosubmaps_tot + 1, -1);
   S.subtable2.assign(S.nosubmaps_tot + 1, -1);
@@ -1314,7 +1337,16 @@ void update_maptod_transfer(State &S) {
 }
 
 // collect_map (maptod_transfer.f90:461-625), single rank: map += locmap
+void collect_map_local(State &S, std::vector<double> &map, long nosubpix);
 void collect_map(State &S, std::vector<double> &map, long nosubpix) {
+  if (g_nranks == 1) return collect_map_local(S, map, nosubpix);
+  std::vector<double> part(map.size(), 0.0);
+  collect_map_local(S, part, nosubpix);
+  allreduce(part.data(), (long)part.size(), 0);
+  for (size_t i = 0; i < map.size(); ++i) map[i] += part[i];
+}
+
+void collect_map_local(State &S, std::vector<double> &map, long nosubpix) {
   long ndegrade = S.nosubpix_max / nosubpix;
   int nmap = S.nmap;
   long k = 0;
@@ -1333,7 +1365,16 @@ void collect_map(State &S, std::vector<double> &map, long nosubpix) {
   }
 }
 
+void collect_cc_local(State &S, std::vector<double> &cc, long nosubpix);
 void collect_cc(State &S, std::vector<double> &cc, long nosubpix) {
+  if (g_nranks == 1) return collect_cc_local(S, cc, nosubpix);
+  std::vector<double> part(cc.size(), 0.0);
+  collect_cc_local(S, part, nosubpix);
+  allreduce(part.data(), (long)part.size(), 0);
+  for (size_t i = 0; i < cc.size(); ++i) cc[i] += part[i];
+}
+
+void collect_cc_local(State &S, std::vector<double> &cc, long nosubpix) {
   long ndegrade = S.nosubpix_max / nosubpix;
   int nmap = S.nmap, nn = nmap * nmap;
   long k = 0;
@@ -1352,7 +1393,17 @@ void collect_cc(State &S, std::vector<double> &cc, long nosubpix) {
   }
 }
 
+void collect_hits_local(State &S, std::vector<int> &hits, long nosubpix);
 void collect_hits(State &S, std::vector<int> &hits, long nosubpix) {
+  if (g_nranks == 1) return collect_hits_local(S, hits, nosubpix);
+  std::vector<int> part(hits.size(), 0);
+  collect_hits_local(S, part, nosubpix);
+  std::vector<double> d(part.begin(), part.end());
+  allreduce(d.data(), (long)d.size(), 0);
+  for (size_t i = 0; i < hits.size(); ++i) hits[i] += (int)d[i];
+}
+
+void collect_hits_local(State &S, std::vector<int> &hits, long nosubpix) {
   long ndegrade = S.nosubpix_max / nosubpix;
   long k = 0;
   for (long i = 0; i < S.nosubmaps_tot; ++i) {
@@ -1997,7 +2048,7 @@ void iterate_a(State &S) {
     double s = 0;
     for (long i = 0; i < nb; ++i)
       if (rmask[i]) s += a[i] * b[i];
-    return s;
+    return allreduce_sum(s);
   };
   double rz = mdot(r, z), rr = mdot(r, r);
   double rzinit = rz, rrinit = rr;
@@ -2229,6 +2280,7 @@ void run_subsets(State &S) {
       }
       long nhs = 0;
       for (long i = 0; i < S.nsamp; ++i) nhs += samp_on(S, i) ? 1 : 0;
+      nhs = (long)allreduce_sum((double)nhs);
       if (nhs == 0) continue;
       for (int ids = 0; ids <= p.ndetset; ++ids) {
         if (ids == 0 && isv == 0) continue;
@@ -2245,6 +2297,7 @@ void run_subsets(State &S) {
         }
         long nhd = 0;
         for (long d = 0; d < S.ndet; ++d) nhd += det_on(S, d) ? 1 : 0;
+        nhd = (long)allreduce_sum((double)nhd);
         if (nhd == 0) continue;
         S.nmap = tonly ? 1 : nmap_save;
         const int nn = S.nmap * S.nmap;
@@ -2394,8 +2447,12 @@ void run_destripe(State &S, long nperiod, const long *periods) {
     }
   }
   long nside_max = std::max(p.nside_map, p.nside_cross);
-  if (pmin < -1) fail("Too small pixel number");
-  if (pmax > 12 * nside_max * nside_max - 1) fail("Too large pixel number");
+  std::string err;
+  if (pmin < -1) err = "Too small pixel number";
+  if (pmax > 12 * nside_max * nside_max - 1) err = "Too large pixel number";
+  // every rank learns of a failed check before the first reduction
+  if (allreduce_sum(err.empty() ? 0.0 : 1.0) > 0)
+    fail(err.empty() ? "another rank failed its input checks" : err);
   check_files(S, nperiod, periods);
   init_parameters(S);
   // init_pointing + where (pixels < 0) pixels = dummy_pixel
@@ -2511,6 +2568,15 @@ void run_cached(State &S) {
 extern "C" {
 
 const char *oracle_last_error(void) { return g_error.c_str(); }
+
+// Ranks of a sharded run: rank r of nranks holds its own detectors; fn
+// all-reduces a double buffer across the ranks (op 0 sum, 1 max).
+// nranks = 1 (or fn = NULL) returns to single-rank runs.
+void oracle_set_comm(int rank, int nranks, AllreduceFn fn) {
+  g_rank = rank;
+  g_nranks = (fn && nranks > 1) ? nranks : 1;
+  g_allreduce = fn;
+}
 
 // Same arguments as destripe() (madam.h:1-2).  Returns 0 on success, nonzero
 // on any condition where the reference would call abort_mpi / stop.

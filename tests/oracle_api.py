@@ -51,8 +51,33 @@ def lib():
         L.oracle_invert_pixel.restype = ct.c_int
         L.oracle_interpolate_psd.argtypes = [ct.c_long, P, P, ct.c_long, P, P]
         L.oracle_max_threads.restype = ct.c_int
+        L.oracle_set_comm.restype = None
+        L.oracle_set_comm.argtypes = [ct.c_int, ct.c_int, ALLREDUCE]
         _lib = L
     return _lib
+
+
+ALLREDUCE = ct.CFUNCTYPE(None, ct.POINTER(ct.c_double), ct.c_long, ct.c_int)
+_comm_keep = []
+
+
+def set_comm(rank, nranks, allreduce=None):
+    """Make the following oracle calls one rank of a sharded run.
+    allreduce(array, op) reduces a float64 numpy array in place across the
+    ranks (op 0 sum, 1 max); None returns to single-rank runs."""
+    L = lib()
+    if allreduce is None:
+        L.oracle_set_comm(0, 1, ALLREDUCE())
+        _comm_keep.clear()
+        return
+
+    def cb(ptr, n, op):
+        a = np.ctypeslib.as_array(ptr, shape=(n,))
+        allreduce(a, op)
+
+    fn = ALLREDUCE(cb)
+    _comm_keep[:] = [fn]
+    L.oracle_set_comm(rank, nranks, fn)
 
 
 def _p(a):
