@@ -16,8 +16,10 @@ Synthetic inputs of that shape are generated on the GPU with a fixed seed.
              the Fortran reference cannot be built here) on a bounded sample
 
 --impl reference times that CPU restatement alone (the reference arm).
-Multi-GPU: every rank solves its own replica (the north-star path does not
-shard); value is the sum over ranks divided by the slowest rank's time.
+Multi-GPU: by default every rank solves its own replica; with --sharded the
+ranks run one solve sharded by detector (maps and inner products summed over
+NCCL every iteration).  value is the sum over ranks divided by the slowest
+rank's time.
 """
 import argparse
 import json
@@ -390,6 +392,9 @@ def main():
     ap.add_argument("--nrhs", type=int, default=64)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--sharded", action="store_true",
+                    help="N > 1: one sharded solve over NCCL (each rank its own detectors) "
+                         "instead of N independent replicas")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     world, rank, local = dist_setup(args)
@@ -430,7 +435,11 @@ def main():
     psd = (d["periods"], d["npsd"], d["psdstarts"], d["psdfreqs"], d["psdvals"])
 
     # full solve with inputs resident in HBM: time to cglimit
-    destripe(None, *common, d["timestamps"], pix, wts, sig, *psd)
+    comm = None
+    if args.sharded and world > 1:
+        from libmadam_b200.comm import NcclComm
+        comm = NcclComm()
+    destripe(comm, *common, d["timestamps"], pix, wts, sig, *psd)
     tim = W.timings()
     sca = W.scalars()
     marks = W.setup_marks()
@@ -458,7 +467,7 @@ def main():
         hn = {k: v.numpy().reshape(-1) for k, v in h.items()}
         barrier(world)
         t1 = time.perf_counter()
-        destripe(None, *common, hn["timestamps"], hn["pixels"], hn["pixweights"], hn["signal"],
+        destripe(comm, *common, hn["timestamps"], hn["pixels"], hn["pixweights"], hn["signal"],
                  *psd)
         m = W.get_result("map")
         t_e2e = time.perf_counter() - t1
@@ -479,7 +488,7 @@ def main():
     if fp32:
         del d["signal"], sig
         torch.cuda.empty_cache()
-        W.destripe(None, *common, d["timestamps"], pix, wts, sig64, *psd)
+        W.destripe(comm, *common, d["timestamps"], pix, wts, sig64, *psd)
         m64 = W.get_result("map").reshape(-1, 3)
         a64 = W.get_result("aa")
         it64 = int(W.scalars()["noiter"])
@@ -542,7 +551,8 @@ def main():
             "config": {"workload": wname, "samples": n, "baselines": nb,
                        "hit_pixels": npix_hit, "nside": cfg.nside,
                        "l2": "inputs larger than L2 (pointing {:.1f} GB)".format(16e-9 * n),
-                       "parallelism": "replicas" if world > 1 else "single GPU"},
+                       "parallelism": ("sharded by detector over NCCL" if comm is not None
+                                       else "replicas" if world > 1 else "single GPU")},
             "gpu_launches": int(launches),
             "clocks": clocks,
             "e2e": e2e,
@@ -559,6 +569,8 @@ def main():
                                  "float64 pixel matrices, baselines and reductions")
             line["fp64_comparison"] = fp64_cmp
         print(json.dumps(line), flush=True)
+    if comm is not None:
+        comm.free()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

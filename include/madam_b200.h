@@ -111,6 +111,29 @@ int madam_b200_serve_error(void *srv, long job, char *buf, long buflen);
 int madam_b200_serve_release(void *srv, long job);
 int madam_b200_serve_close(void *srv);
 
+/* Sharded runs: communicators standing in for the reference's MPI
+ * communicator (mpi_wrappers.f90).  Each rank (one process per GPU) passes
+ * its own TOD (detectors and/or time spans) to destripe / destripe_with_cache
+ * with `comm` = the handle returned here; the pixel matrices, hits, maps and
+ * the PCG inner products are summed across the ranks (the reference's
+ * collect_map / collect_cc / collect_hits / sum_mpi), so every rank ends with
+ * the whole maps and its own baselines; rank 0 writes the FITS files.
+ * Leakage matrices need every rank to hold the same detectors, as in the
+ * reference.  comm_nccl_id fills 128 bytes of NCCL unique id (rank 0, to be
+ * sent to the other ranks); comm_init_nccl makes an NCCL communicator (NVLink
+ * / NVSwitch, libnccl.so.2 loaded on first use); comm_init_host one whose
+ * reductions call fn(host buffer, n, op) (op 0 sum, 1 max), e.g. over a CPU
+ * process group.  Both return a handle > 0, or -1 (message from
+ * comm_error); comm 0 or an unknown handle means a single rank.  The batched
+ * solve and the job server run on one rank.  No reference counterpart beyond
+ * the MPI communicator. */
+int madam_b200_comm_nccl_id(char *id);
+int madam_b200_comm_init_nccl(int rank, int nranks, const char *id);
+typedef void (*madam_b200_allreduce_fn)(double *buf, long n, int op);
+int madam_b200_comm_init_host(int rank, int nranks, madam_b200_allreduce_fn fn);
+int madam_b200_comm_free(int handle);
+int madam_b200_comm_error(char *buf, long buflen);
+
 /* Status of the last call (0 = success) and its error message; replaces the
  * reference's abort_mpi messages (src/mpi_wrappers.f90:120-137). */
 int madam_b200_last_error(char *buf, long buflen);

@@ -18,6 +18,7 @@
 #include <string>
 
 #include "engine.h"
+#include "comm.h"
 #include "params.h"
 
 using madam::Engine;
@@ -96,7 +97,6 @@ static int destripe_impl(bool fp32, int comm, char *parstring, long ndet, char *
                          void *pixweights, void *signal, long nperiod, long *periods, long *npsd,
                          long npsdtot, double *psdstarts, long npsdbin, double *psdfreqs,
                          long npsdval, double *psdvals) {
-  (void)comm;  // single rank: the communicator handle is accepted and ignored
   std::lock_guard<std::mutex> lock(g_mutex);
   return guarded([&] {
     madam::Params par = madam::parse_parstring(parstring);
@@ -114,6 +114,9 @@ static int destripe_impl(bool fp32, int comm, char *parstring, long ndet, char *
       madam::fail("destripe_fp32: pixels and signal must both be host or both device memory");
     Engine &e = engine();
     e.clear_subchunk_results();
+    // comm: a communicator of madam_b200_comm_init_* (a sharded run), else a
+    // single rank (the reference's MPI handle has no meaning here)
+    e.set_comm(madam::comm_lookup(comm));
     // subchunk passes (smadam.F90:192-196): isubchunk = 1 .. nsubchunk, then
     // 0 (the full data) last, starting from the isubchunk parameter
     const int nsub = par.nsubchunk >= 2 ? (int)par.nsubchunk : 0;
@@ -138,12 +141,12 @@ static int destripe_impl(bool fp32, int comm, char *parstring, long ndet, char *
 
 int madam_b200_destripe_with_cache(int comm, long ndet, long nsamp, long nnz, void *timestamps,
                                    void *pix, void *pixweights, void *signal, char *outpath) {
-  (void)comm;
   (void)outpath;  // output files are not written by this library
   std::lock_guard<std::mutex> lock(g_mutex);
   return guarded([&] {
     if (!g_engine || !g_engine->cached())
       madam::fail("destripe_with_cache called with empty caches.");
+    g_engine->set_comm(madam::comm_lookup(comm));
     const bool dev = is_device_pointer(pix);
     g_engine->run_cached(ndet, nsamp, nnz, (double *)timestamps, (int32_t *)pix,
                          (float *)pixweights, (double *)signal, dev);

@@ -40,7 +40,7 @@ constexpr int kTileMax = 1024;        // pixels per scatter tile (fine res)
 constexpr uint32_t kRunMax = 1024;    // samples per run
 constexpr long long kItemSamples = 1 << 16;  // samples per scatter work item
 
-enum Scal { S_RZ = 0, S_RR, S_PAP, S_RZ2, S_RZO, S_ALPHA, S_BETA, S_NSCAL = 16 };
+enum Scal { S_RZ = 0, S_RR, S_PAP, S_RZ2, S_RZO, S_ALPHA, S_BETA, S_SHARD = 12, S_NSCAL = 16 };
 
 __device__ __forceinline__ int find_iv(const long long *istart, int niv, long long s) {
   int lo = 0, hi = niv - 1;
@@ -1056,6 +1056,23 @@ __global__ void k_finish(const double *part, int nblk, int nd, double *scal, int
     scal[S_RZ2] = v[1];
     scal[S_RR] = v[2];
     scal[S_BETA] = (v[0] - v[1]) / scal[S_RZO];
+  }
+}
+
+// k_finish's CG scalars from inner products already summed over the ranks
+// of a sharded run (scal[src .. src + 2])
+__global__ void k_finish_apply(double *scal, int mode, int src) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double v0 = scal[src], v1 = scal[src + 1], v2 = scal[src + 2];
+  if (mode == 1) {
+    scal[S_PAP] = v0;
+    scal[S_ALPHA] = scal[S_RZ] / v0;
+  } else {
+    scal[S_RZO] = scal[S_RZ];
+    scal[S_RZ] = v0;
+    scal[S_RZ2] = v1;
+    scal[S_RR] = v2;
+    scal[S_BETA] = (v0 - v1) / scal[S_RZO];
   }
 }
 

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "band2.cuh"
+#include "comm.h"
 #include "common.cuh"
 #include "params.h"
 
@@ -128,6 +129,10 @@ class Engine {
   bool fp32() const { return fp32_; }
   long long pairs() const { return use_pairs_ ? npairs_ : 0; }
 
+  // Rank of a sharded run (comm.h), or nullptr for a single rank.
+  void set_comm(Comm *c) { comm_ = c; }
+  bool sharded() const { return comm_ && comm_->nranks > 1; }
+
   // Subchunk pass of the next run() (nsubchunk > 1): isub 1..nsub bins and
   // solves only that subchunk of every interval; 0 is the full-data pass.
   void set_subchunk(int isub, int nsub) {
@@ -221,7 +226,8 @@ class Engine {
   void convolve(const double *x, double *y, const std::vector<ConvSeg> &segs,
                 const double *spectra, DevBuf<ConvSeg> &dsegs);
   void cg_preconditioner_segments(const double *r, double *z);
-  void finish_dots(int nd, int mode, int slot0, int nblk = kRedBlocks);
+  // global: the inner product spans the ranks of a sharded run
+  void finish_dots(int nd, int mode, int slot0, int nblk = kRedBlocks, bool global = false);
 
   Params par_;
   std::vector<Detector> dets_;
@@ -344,6 +350,7 @@ class Engine {
   // subsets and leakage matrices (subsets.inl)
   void run_subsets();
   void leak_matrices();
+  void check_same_detectors();
   void subset_accumulate(const std::vector<uint8_t> &detflags, const std::vector<double2> &spans,
                          int nmaps, double *cc, double *bin, int *hits);
   std::vector<double> leak_product(const std::vector<double> &cinv,
@@ -361,6 +368,19 @@ class Engine {
   std::map<std::string, std::vector<double>> extra_d_;  // subset / leakage results
   std::map<std::string, std::vector<int>> extra_i_;
   int isubchunk_ = 0, nsubchunk_ = 0;
+  // sharded runs: in-place reductions across the ranks (no-ops on one rank)
+  Comm *comm_ = nullptr;
+  void ar_sum(double *dev, size_t n) {
+    if (sharded()) comm_->allreduce(dev, n, 0, st_);
+  }
+  void ar_sum(int *dev, size_t n) {
+    if (sharded()) comm_->allreduce(dev, n, 0, st_);
+  }
+  void ar_max(int *dev, size_t n) {
+    if (sharded()) comm_->allreduce(dev, n, 1, st_);
+  }
+  double ar_sum_host(double v);
+  bool writes_files() const { return !comm_ || comm_->rank == 0; }
   std::map<std::string, std::vector<double>> subchunk_d_;  // products of subchunk passes
   std::map<std::string, std::vector<int>> subchunk_i_;
 

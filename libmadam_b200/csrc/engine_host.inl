@@ -398,6 +398,7 @@ void Engine::flag_and_compact(bool first_call) {
     MADAM_LAUNCH(k_subchunk_mask, grid_for(n), 256, 0, st_, pix_.get(), n, (long long)nsamp_,
                  drg.get(), (int)ninterval_, (int)dummy_global_);
   }
+  ar_max(ksub.get(), nosubmaps_tot_ + 1);  // the hit submaps of every rank
   std::vector<int> ks(nosubmaps_tot_ + 1);
   MADAM_CUDA(cudaMemcpyAsync(ks.data(), ksub.get(), ks.size() * sizeof(int),
                              cudaMemcpyDeviceToHost, st_));
@@ -855,6 +856,10 @@ void Engine::bin_tod(bool accumulate_wamap) {
                    item_tile_.get(), runs_.get(), point4_.get(), pixc_.get(), d_tod_, bw_.get(),
                    fdn_, tile_shift_, ccacc.get(), bin.get(), hits.get());
   }
+  // collect_cc / collect_hits / collect_map across the ranks
+  ar_sum(ccacc.get(), ccacc.n);
+  ar_sum(bin.get(), bin.n);
+  ar_sum(hits.get(), hits.n);
   const long long nv = (long long)nloc_ * nmap_;
   if (!accumulate_wamap) {
     // first call: cc, cca, hits, map, binmap, wamap from scratch
@@ -1576,8 +1581,28 @@ void Engine::construct_preconditioner() {
   cg_prec_segs_ = cgk;
 }
 
-void Engine::finish_dots(int nd, int mode, int slot0, int nblk) {
-  MADAM_LAUNCH(k_finish, 1, 1024, 0, st_, part_.get(), nblk, nd, scal_.get(), mode, slot0);
+void Engine::finish_dots(int nd, int mode, int slot0, int nblk, bool global) {
+  if (!global || !sharded()) {
+    MADAM_LAUNCH(k_finish, 1, 1024, 0, st_, part_.get(), nblk, nd, scal_.get(), mode, slot0);
+    return;
+  }
+  // the rank's partial sums, summed over the ranks, then the CG scalars
+  // (sum_mpi of the inner products, smadam_routines.f90:865-901)
+  const int dst = mode == 0 ? slot0 : S_SHARD;
+  MADAM_LAUNCH(k_finish, 1, 1024, 0, st_, part_.get(), nblk, nd, scal_.get(), 0, dst);
+  ar_sum(scal_.get() + dst, nd);
+  if (mode != 0) MADAM_LAUNCH(k_finish_apply, 1, 32, 0, st_, scal_.get(), mode, S_SHARD);
+}
+
+double Engine::ar_sum_host(double v) {
+  if (!sharded()) return v;
+  DevBuf<double> t;
+  t.alloc(1);
+  MADAM_CUDA(cudaMemcpyAsync(t.get(), &v, sizeof v, cudaMemcpyHostToDevice, st_));
+  ar_sum(t.get(), 1);
+  MADAM_CUDA(cudaMemcpyAsync(&v, t.get(), sizeof v, cudaMemcpyDeviceToHost, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  return v;
 }
 
 void Engine::scatter_baselines(const double *pw, double *target, bool fine) {
@@ -1609,6 +1634,7 @@ void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) 
   const long long nb = (long long)ndet_ * noba_short_;
   // 1) baseline -> map, collect, ccmultiply, scatter back (iterate_a 798-827)
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[0], st_));
+  if (nscatter_chunks_ == 0 && nloc_cross_ > 0) lmap_.zero(st_);  // a rank with no samples
   if (nloc_cross_ > 0 && nscatter_chunks_ > 0) {
     if (nmap_ == 3) {
       MADAM_LAUNCH(k_scatter_chunks<3>, kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
@@ -1626,6 +1652,7 @@ void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) 
                      scatter_multi_.get(), nscatter_multi_, scatter_partial_.get(), lmap_.get());
     }
   }
+  ar_sum(lmap_.get(), (size_t)nloc_cross_ * nmap_);  // collect_map across the ranks
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[1], st_));
   if (nloc_cross_ > 0) {
     if (nmap_ == 3 && fp32_)
@@ -1691,7 +1718,7 @@ void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) 
                  bstart_d_.get(), nb, noba_short_, nsamp_, bw_.get(), p, nna_.get(), lmap_.get(),
                  (int)ndeg_shift_, (int)nloc_, rmask_.get(), ap, part_.get());
   }
-  finish_dots(1, 1, 0);
+  finish_dots(1, 1, 0, kRedBlocks, true);
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[4], st_));
 }
 
@@ -1792,7 +1819,7 @@ void Engine::iterate() {
                nb, scal_.get(), 1);
   MADAM_LAUNCH(k_dots, kRedBlocks, 256, 0, st_, r_.get(), z_.get(), r_.get(), r_.get(), nullptr,
                nullptr, 2, rmask_.get(), nb, part_.get());
-  finish_dots(2, 0, S_RZ);
+  finish_dots(2, 0, S_RZ, kRedBlocks, true);
   scal_host_.assign(S_NSCAL, 0.0);
   MADAM_CUDA(cudaMemcpyAsync(scal_host_.data(), scal_.get(), S_NSCAL * sizeof(double),
                              cudaMemcpyDeviceToHost, st_));
@@ -1817,7 +1844,7 @@ void Engine::iterate() {
     MADAM_CUDA(cudaEventRecord(ev_[6], st_));
     MADAM_LAUNCH(k_dots, kRedBlocks, 256, 0, st_, r_.get(), z_.get(), ro_.get(), z_.get(),
                  r_.get(), r_.get(), 3, rmask_.get(), nb, part_.get());
-    finish_dots(3, 2, 0);
+    finish_dots(3, 2, 0, kRedBlocks, true);
     MADAM_CUDA(cudaMemcpyAsync(scal_host_.data(), scal_.get(), S_NSCAL * sizeof(double),
                                cudaMemcpyDeviceToHost, st_));
     MADAM_CUDA(cudaStreamSynchronize(st_));
@@ -1858,6 +1885,7 @@ void Engine::subtract_baselines() {
   lmap_fine_.zero(st_);
   scatter_baselines(tmpv_.get(), lmap_fine_.get(), true);
   const long long nv = (long long)nloc_ * nmap_;
+  ar_sum(lmap_fine_.get(), (size_t)nv);
   if (nv > 0) MADAM_LAUNCH(k_add, grid_for(nv), 256, 0, st_, map_.get(), lmap_fine_.get(), nv);
 }
 
@@ -1928,7 +1956,7 @@ void Engine::finalize(bool first_call) {
 }
 
 void Engine::write_fits(bool first_call) {
-  if (suppress_fits_) return;
+  if (suppress_fits_ || !writes_files()) return;
   // write_map / write_binmap / write_mask / write_hits / write_matrix
   // (smadam.F90:401-422, 756-764)
   const bool any = par_.do_map || par_.do_binmap ||
@@ -2081,8 +2109,13 @@ void Engine::run(const Params &par, std::vector<Detector> dets, long ndet, long 
     MADAM_CUDA(cudaMemcpyAsync(out, mm.get(), sizeof out, cudaMemcpyDeviceToHost, st_));
     MADAM_CUDA(cudaStreamSynchronize(st_));
     const long nside_max = std::max(par_.nside_map, par_.nside_cross);
-    if (n > 0 && out[0] < -1) fail("Too small pixel number");
-    if (n > 0 && (long)out[1] > 12 * nside_max * nside_max - 1) fail("Too large pixel number");
+    std::string err;
+    if (n > 0 && out[0] < -1) err = "Too small pixel number";
+    if (n > 0 && (long)out[1] > 12 * nside_max * nside_max - 1) err = "Too large pixel number";
+    // every rank of a sharded run learns of a failed check before the first
+    // reduction that would otherwise wait for it
+    if (ar_sum_host(err.empty() ? 0.0 : 1.0) > 0)
+      fail(err.empty() ? "another rank failed its input checks" : err);
   }
   init_layout(nperiod, periods);
   // baseline start times (baseline_times, parameter_control.f90:956-977)
@@ -2400,7 +2433,7 @@ void Engine::bench_iterations(int warmup, int iters, std::vector<double> &out) {
                  nb, scal_.get(), 1);
     MADAM_LAUNCH(k_dots, kRedBlocks, 256, 0, st_, r_.get(), z_.get(), r_.get(), r_.get(), nullptr,
                  nullptr, 2, rmask_.get(), nb, part_.get());
-    finish_dots(2, 0, S_RZ);
+    finish_dots(2, 0, S_RZ, kRedBlocks, true);
   };
   auto one = [&](bool timed) {
     apply_A(p_.get(), pw_.get(), ap_.get(), timed);
@@ -2411,7 +2444,7 @@ void Engine::bench_iterations(int warmup, int iters, std::vector<double> &out) {
     if (timed) MADAM_CUDA(cudaEventRecord(ev_[6], st_));
     MADAM_LAUNCH(k_dots, kRedBlocks, 256, 0, st_, r_.get(), z_.get(), ro_.get(), z_.get(),
                  r_.get(), r_.get(), 3, rmask_.get(), nb, part_.get());
-    finish_dots(3, 2, 0);
+    finish_dots(3, 2, 0, kRedBlocks, true);
     MADAM_LAUNCH(k_update_p, grid_for(nb), 256, 0, st_, p_.get(), z_.get(), pw_.get(), bw_.get(),
                  nb, scal_.get(), 0);
     if (timed) MADAM_CUDA(cudaEventRecord(ev_[7], st_));

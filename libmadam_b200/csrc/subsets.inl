@@ -98,6 +98,7 @@ void Engine::subset_accumulate(const std::vector<uint8_t> &detflags,
   if (!spans.empty())
     MADAM_CUDA(cudaMemcpyAsync(sp.get(), spans.data(), spans.size() * sizeof(double2),
                                cudaMemcpyHostToDevice, st_));
+
   const SampleMap sm = sample_map(istart_d_.get(), kstart_d_.get(), (int)ninterval_, nsamp_,
                                   noba_short_, fdn_);
   const double *times = spans.empty() ? nullptr : subset_times_;
@@ -113,6 +114,10 @@ void Engine::subset_accumulate(const std::vector<uint8_t> &detflags,
     MADAM_LAUNCH((k_subset_accum<1, 1>), grid_for(n), 256, 0, st_, point4_.get(), pixc_.get(),
                  d_tod_, n, sm, bw_.get(), (int)nloc_, df.get(), times, sp.get(),
                  (int)spans.size(), cc, bin, hits);
+  // collect_cc / collect_hits / collect_map across the ranks of a sharded run
+  if (cc) ar_sum(cc, (size_t)nloc_ * (nmaps == 3 ? 6 : 1));
+  if (bin) ar_sum(bin, (size_t)nloc_ * nmaps);
+  if (hits) ar_sum(hits, (size_t)nloc_);
   MADAM_CUDA(cudaStreamSynchronize(st_));
 }
 
@@ -154,9 +159,31 @@ std::vector<double> Engine::detector_matrix(long det, int nmaps) {
   return h;
 }
 
+// In a sharded run the leakage matrices take one reduction per detector, so,
+// as in the reference, every rank must hold the same detectors: compared
+// through a hash of their names, on every rank alike.
+void Engine::check_same_detectors() {
+  if (!sharded()) return;
+  uint64_t h = 1469598103934665603ull;
+  for (const auto &d : dets_)
+    for (char c : d.name + ";") h = (h ^ (unsigned char)c) * 1099511628211ull;
+  DevBuf<int> v;
+  v.alloc(4);
+  const int hv[4] = {(int)(h & 0x3fffffff), (int)((h >> 30) & 0x3fffffff),
+                     -(int)(h & 0x3fffffff), -(int)((h >> 30) & 0x3fffffff)};
+  MADAM_CUDA(cudaMemcpyAsync(v.get(), hv, sizeof hv, cudaMemcpyHostToDevice, st_));
+  ar_max(v.get(), 4);
+  int r[4];
+  MADAM_CUDA(cudaMemcpyAsync(r, v.get(), sizeof r, cudaMemcpyDeviceToHost, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  if (r[0] != -r[2] || r[1] != -r[3])
+    fail("leakage matrices of a sharded run need the same detectors on every rank");
+}
+
 void Engine::leak_matrices() {
   // leakmatrix (smadam_routines.f90:38-105) for every detector of the
   // full-data run, from the inverted full-data matrices
+  check_same_detectors();
   const int ncc = nmap_ == 3 ? 6 : 1;
   MADAM_CUDA(cudaStreamSynchronize(st_));
   std::vector<double> cinv((size_t)nloc_ * ncc);
@@ -191,6 +218,7 @@ void Engine::run_subsets() {
     }
   }
   const int npass = (p.do_binmap && p.do_map) ? 2 : 1;
+  if (p.do_leakmatrix) check_same_detectors();
   std::vector<double> table;
   long k = 0;
   for (int pass = 1; pass <= npass; ++pass) {
@@ -209,6 +237,7 @@ void Engine::run_subsets() {
               break;
             }
       }
+      nhs = (long)ar_sum_host((double)nhs);  // sum_mpi(nhit_survey)
       if (nhs == 0) continue;
       for (int ids = 0; ids <= p.ndetset; ++ids) {
         if (ids == 0 && isv == 0) continue;
@@ -225,6 +254,7 @@ void Engine::run_subsets() {
         }
         long nhd = 0;
         for (long d = 0; d < ndet_; ++d) nhd += df[d];
+        nhd = (long)ar_sum_host((double)nhd);  // sum_mpi(nhit_det)
         if (nhd == 0) continue;
         const int nms = tonly ? 1 : nmap_;
         const int ncc = nms == 3 ? 6 : 1;
@@ -330,7 +360,7 @@ void Engine::run_subsets() {
             expand_host(craw.data(), sizeof(double), nms * nms, nosubpix_map_, crawfull.data());
           }
         }
-        if (!suppress_fits_) {
+        if (!suppress_fits_ && writes_files()) {
           SubsetFits sf;
           sf.par = &par_;
           sf.nosubpix_map = nosubpix_map_;

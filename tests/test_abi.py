@@ -18,7 +18,9 @@ def _declared():
         src = open(os.path.join(ROOT, "include", h)).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         names += re.findall(r"\b([a-z_0-9]+)\s*\(", src)
-    return sorted(set(n for n in names if n not in ("if", "sizeof")))
+    # (a function-pointer parameter's return type is not a symbol)
+    skip = ("if", "sizeof", "void", "int", "long", "double", "char", "float")
+    return sorted(set(n for n in names if n not in skip))
 
 
 def test_library_builds_and_loads():
