@@ -1059,6 +1059,14 @@ __global__ void k_finish(const double *part, int nblk, int nd, double *scal, int
   }
 }
 
+// zero the cross-resolution pixel matrices of the pixels the input mask drops
+__global__ void k_apply_inmask(double *cca, long long n, int ncc, const uint8_t *mask) {
+  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+       p += (long long)gridDim.x * blockDim.x)
+    if (!mask[p])
+      for (int j = 0; j < ncc; ++j) cca[p * ncc + j] = 0.0;
+}
+
 // k_finish's CG scalars from inner products already summed over the ranks
 // of a sharded run (scal[src .. src + 2])
 __global__ void k_finish_apply(double *scal, int mode, int src) {

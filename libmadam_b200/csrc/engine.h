@@ -173,6 +173,7 @@ class Engine {
   void build_csr();
   void setup_scatter();
   void map_side_setup();
+  void apply_inmask();
   void initialize_a();
   void build_segments();
   void build_filter();

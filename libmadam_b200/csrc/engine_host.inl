@@ -183,7 +183,6 @@ void Engine::init_layout(long nperiod, const long *periods) {
   if (p.pixlim_cross < 0) p.pixlim_cross = p.pixlim_map;
   if (p.pixmode_map < 0 || p.pixmode_map > 2) fail("Pixmode_map must be in range [0-2]");
   if (p.pixmode_cross < 0 || p.pixmode_cross > 4) fail("Pixmode_cross must be in range [0-4]");
-  if (!p.file_inmask.empty()) fail("file_inmask is not supported");
   if (!p.file_spectrum.empty()) fail("file_spectrum is not supported");
   if (!p.file_covmat.empty()) fail("file_covmat is not supported");
   if (nmap_ == 1) p.temperature_only = true;
@@ -469,7 +468,11 @@ void Engine::flag_and_compact(bool first_call) {
     MADAM_CUDA(cudaStreamSynchronize(st_));
   }
   // flag_bad_baselines (read_data.f90:30-74)
-  if (par_.kfirst && par_.good_baseline_fraction != 0 && !par_.kfilter) {
+  // flag_bad_baselines counts only samples whose pixel the input mask keeps,
+  // but it runs before the mask is read (smadam.F90:309, 337-345), when the
+  // mask table is still zero: with file_inmask it flags nothing
+  if (par_.kfirst && par_.good_baseline_fraction != 0 && !par_.kfilter &&
+      par_.file_inmask.empty()) {
     const long long nb = (long long)ndet_ * noba_short_;
     const unsigned grid = (unsigned)((nb * 32 + 255) / 256);
     if (nmap_ == 3)
@@ -908,6 +911,45 @@ void Engine::bin_tod(bool accumulate_wamap) {
 
 void Engine::setup_scatter() { bin_tod(false); }
 
+void Engine::apply_inmask() {
+  // read_inmask (read_data.f90:90-190) up- or downgraded to nside_cross, and
+  // the zeroing of the masked pixel matrices in invert_pixelmatrix_cross
+  // (map_routines.f90:100-104); zeroing after the inversion gives the same
+  // zero matrix, which the inversion leaves alone
+  long ns = 0;
+  std::string ord;
+  const std::vector<float> col = read_mask_column(par_.file_inmask, ns, ord);
+  if (ord == "RING") fail("Error in subroutine Read_inmask. Input mask should be in NESTED ordering.");
+  if (ord != "NESTED")
+    fail("Error in subroutine Read_inmask. Cannot determine the ordering (nested or ring).");
+  const long nsc = par_.nside_cross;
+  if (ns < par_.nside_submap || (ns & (ns - 1))) fail("file_inmask: invalid NSIDE");
+  const long nin = (ns / par_.nside_submap) * (ns / par_.nside_submap);
+  const long n = nsc >= ns ? (nsc / ns) * (nsc / ns) : (ns / nsc) * (ns / nsc);
+  if ((long)col.size() < nosubmaps_tot_ * nin) fail("file_inmask: too few pixels");
+  std::vector<uint8_t> m((size_t)nloc_cross_, 1);
+  for (long j = 0; j < nolocmaps_; ++j) {
+    const float *fb = col.data() + (size_t)(j + subtable2_[j]) * nin;
+    uint8_t *mj = m.data() + (size_t)j * nosubpix_cross_;
+    if (nsc >= ns) {
+      for (long i = 0; i < nin; ++i)
+        for (long q = 0; q < n; ++q) mj[i * n + q] = fb[i] < 0.5f ? 0 : 1;
+    } else {
+      for (long i = 0; i < nosubpix_cross_; ++i) {
+        bool any = false;
+        for (long q = 0; q < n; ++q) any = any || fb[i * n + q] < 0.5f;
+        mj[i] = any ? 0 : 1;
+      }
+    }
+  }
+  DevBuf<uint8_t> dm;
+  dm.alloc(m.size());
+  MADAM_CUDA(cudaMemcpyAsync(dm.get(), m.data(), m.size(), cudaMemcpyHostToDevice, st_));
+  MADAM_LAUNCH(k_apply_inmask, grid_for(nloc_cross_), 256, 0, st_, cca_.get(),
+               (long long)nloc_cross_, nmap_ == 3 ? 6 : 1, dm.get());
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+}
+
 void Engine::map_side_setup() {
   // invert_pixelmatrix_cross (map_routines.f90:83-212)
   MatrixRules mr{(int)par_.pixmode_cross, par_.pixlim_cross, par_.allow_decoupling ? 1 : 0,
@@ -919,6 +961,7 @@ void Engine::map_side_setup() {
   else
     MADAM_LAUNCH(k_invert_cross<1>, grid_for(nloc_cross_), 128, 0, st_, cca_.get(),
                  (long long)nloc_cross_, mr);
+  if (!par_.file_inmask.empty()) apply_inmask();
 }
 
 void Engine::initialize_a() {

@@ -15,7 +15,10 @@
 
 #include <sys/stat.h>
 
+#include <cctype>
 #include <cmath>
+#include <cstdint>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -327,6 +330,109 @@ void write_products(const FitsInput &in) {
     const std::string base = subchunk_id(root + "_leakmatrix", in.isubchunk, in.nsubchunk);
     for (const auto &lk : in.leak) t.leak(resolve(base + "_" + lk.first + ".fits"), lk.second);
   }
+}
+
+// ---- reading: the input mask (read_inmask, read_data.f90:90-190)
+namespace {
+std::string card_value(const std::string &card) {
+  std::string v = card.size() > 10 ? card.substr(10) : "";
+  const size_t q = v.find('\'');
+  if (q != std::string::npos) {
+    const size_t e = v.find('\'', q + 1);
+    std::string t = v.substr(q + 1, e == std::string::npos ? std::string::npos : e - q - 1);
+    while (!t.empty() && t.back() == ' ') t.pop_back();
+    return t;
+  }
+  const size_t sl = v.find('/');
+  if (sl != std::string::npos) v = v.substr(0, sl);
+  size_t a = v.find_first_not_of(' '), b = v.find_last_not_of(' ');
+  return a == std::string::npos ? "" : v.substr(a, b - a + 1);
+}
+
+// one header: keyword -> value; the stream is left after its END block
+std::vector<std::pair<std::string, std::string>> read_header(FILE *f) {
+  std::vector<std::pair<std::string, std::string>> kv;
+  char block[2880];
+  for (;;) {
+    if (std::fread(block, 1, 2880, f) != 2880) fail("truncated FITS header");
+    for (int c = 0; c < 36; ++c) {
+      const std::string card(block + 80 * c, 80);
+      std::string key = card.substr(0, 8);
+      while (!key.empty() && key.back() == ' ') key.pop_back();
+      if (key == "END") return kv;
+      if (card.size() > 9 && card[8] == '=') kv.push_back({key, card_value(card)});
+    }
+  }
+}
+
+std::string get(const std::vector<std::pair<std::string, std::string>> &kv, const std::string &k,
+                const std::string &dflt = "") {
+  for (auto &e : kv)
+    if (e.first == k) return e.second;
+  return dflt;
+}
+}  // namespace
+
+std::vector<float> read_mask_column(const std::string &file, long &nside, std::string &ordering) {
+  FILE *f = std::fopen(file.c_str(), "rb");
+  if (!f) fail("cannot open " + file);
+  std::vector<float> out;
+  try {
+    auto prim = read_header(f);
+    long long psize = 0;
+    const long naxis = std::stol(get(prim, "NAXIS", "0"));
+    if (naxis > 0) {
+      psize = std::llabs(std::stoll(get(prim, "BITPIX", "8"))) / 8;
+      for (long i = 1; i <= naxis; ++i) psize *= std::stoll(get(prim, "NAXIS" + std::to_string(i)));
+    }
+    std::fseek(f, (long)((psize + 2879) / 2880 * 2880), SEEK_CUR);
+    auto ext = read_header(f);
+    if (get(ext, "XTENSION") != "BINTABLE") fail(file + ": no binary table");
+    const long long rowb = std::stoll(get(ext, "NAXIS1")), nrow = std::stoll(get(ext, "NAXIS2"));
+    const std::string tf = get(ext, "TFORM1");
+    size_t i = 0;
+    while (i < tf.size() && isdigit((unsigned char)tf[i])) ++i;
+    const long rep = i ? std::stol(tf.substr(0, i)) : 1;
+    const char t = i < tf.size() ? tf[i] : 'E';
+    const int w = t == 'E' || t == 'J' ? 4 : t == 'D' || t == 'K' ? 8 : t == 'I' ? 2 : 1;
+    ordering = get(ext, "ORDERING");
+    nside = std::stol(get(ext, "NSIDE", "0"));
+    std::vector<unsigned char> row((size_t)rowb);
+    out.reserve((size_t)(nrow * rep));
+    for (long long r = 0; r < nrow; ++r) {
+      if (std::fread(row.data(), 1, row.size(), f) != row.size()) fail(file + ": truncated table");
+      for (long k = 0; k < rep; ++k) {
+        const unsigned char *p = row.data() + k * w;
+        uint64_t u = 0;
+        for (int b = 0; b < w; ++b) u = (u << 8) | p[b];
+        double v;
+        if (t == 'E') {
+          uint32_t u32 = (uint32_t)u;
+          float x;
+          std::memcpy(&x, &u32, 4);
+          v = x;
+        } else if (t == 'D') {
+          std::memcpy(&v, &u, 8);
+        } else if (t == 'J') {
+          v = (double)(int32_t)(uint32_t)u;
+        } else if (t == 'K') {
+          v = (double)(int64_t)u;
+        } else if (t == 'I') {
+          v = (double)(int16_t)(uint16_t)u;
+        } else if (t == 'L') {
+          v = p[0] == 'T' ? 1.0 : 0.0;
+        } else {
+          v = (double)p[0];
+        }
+        out.push_back((float)v);
+      }
+    }
+  } catch (...) {
+    std::fclose(f);
+    throw;
+  }
+  std::fclose(f);
+  return out;
 }
 
 void write_subset_products(const SubsetFits &in) {

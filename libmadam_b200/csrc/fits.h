@@ -45,4 +45,8 @@ struct SubsetFits {
 
 void write_subset_products(const SubsetFits &in);
 
+// The first column of the first binary table of a FITS file (the input mask
+// of read_inmask, read_data.f90:90-190) with its NSIDE and ORDERING keys.
+std::vector<float> read_mask_column(const std::string &file, long &nside, std::string &ordering);
+
 }  // namespace madam

@@ -64,6 +64,7 @@
 //     product U^-1 U^-T.
 
 #include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -1039,7 +1040,6 @@ void init_parameters(State &S) {
     fail("Pixmode_map must be in range [0-2]");
   if (p.pixmode_cross < 0 || p.pixmode_cross > 4)
     fail("Pixmode_cross must be in range [0-4]");
-  if (!p.file_inmask.empty()) fail("file_inmask is not supported");
   if (!p.file_spectrum.empty()) fail("file_spectrum is not supported");
   if (!p.file_covmat.empty()) fail("file_covmat is not supported");
   if (S.nmap == 1) p.temperature_only = true;
@@ -1579,10 +1579,109 @@ void ccmultiply(const State &S, const std::vector<double> &cc,
   }
 }
 
+// read_inmask (read_data.f90:90-190): column 1 of the first binary table,
+// its NSIDE and ORDERING, as the reference reads it through cfitsio
+std::vector<double> read_fits_column(const std::string &file, long &nside, std::string &ord) {
+  FILE *f = std::fopen(file.c_str(), "rb");
+  if (!f) fail("cannot open " + file);
+  std::map<std::string, std::string> hdr;
+  auto header = [&]() {
+    hdr.clear();
+    char card[81];
+    card[80] = 0;
+    long ncard = 0;
+    for (;;) {
+      if (std::fread(card, 1, 80, f) != 80) fail("truncated FITS header");
+      ++ncard;
+      std::string c(card), key = trim(c.substr(0, 8));
+      if (key == "END") break;
+      if (c[8] != '=') continue;
+      std::string v = c.substr(10);
+      size_t q = v.find('\'');
+      if (q != std::string::npos) v = v.substr(q + 1, v.find('\'', q + 1) - q - 1);
+      else v = v.substr(0, v.find('/'));
+      hdr[key] = trim(v);
+    }
+    std::fseek(f, (long)(((ncard + 35) / 36 * 36 - ncard) * 80), SEEK_CUR);
+  };
+  header();
+  long long psize = 0;
+  if (hdr.count("NAXIS") && std::stol(hdr["NAXIS"]) > 0) {
+    psize = std::llabs(std::stoll(hdr["BITPIX"])) / 8;
+    for (long i = 1; i <= std::stol(hdr["NAXIS"]); ++i) psize *= std::stoll(hdr["NAXIS" + std::to_string(i)]);
+  }
+  std::fseek(f, (long)((psize + 2879) / 2880 * 2880), SEEK_CUR);
+  header();
+  const long long rowb = std::stoll(hdr["NAXIS1"]), nrow = std::stoll(hdr["NAXIS2"]);
+  std::string tf = hdr["TFORM1"];
+  size_t i = 0;
+  while (i < tf.size() && std::isdigit((unsigned char)tf[i])) ++i;
+  long rep = i ? std::stol(tf.substr(0, i)) : 1;
+  char t = i < tf.size() ? tf[i] : 'E';
+  int w = (t == 'E' || t == 'J') ? 4 : (t == 'D' || t == 'K') ? 8 : t == 'I' ? 2 : 1;
+  ord = hdr["ORDERING"];
+  nside = hdr.count("NSIDE") ? std::stol(hdr["NSIDE"]) : 0;
+  std::vector<double> out;
+  std::vector<unsigned char> row(rowb);
+  for (long long r = 0; r < nrow; ++r) {
+    if (std::fread(row.data(), 1, rowb, f) != (size_t)rowb) fail("truncated FITS table");
+    for (long k = 0; k < rep; ++k) {
+      unsigned char b[8] = {0};
+      for (int j = 0; j < w; ++j) b[j] = row[k * w + w - 1 - j];  // big-endian -> host
+      double v;
+      if (t == 'E') { float x; std::memcpy(&x, b, 4); v = x; }
+      else if (t == 'D') std::memcpy(&v, b, 8);
+      else if (t == 'J') { int32_t x; std::memcpy(&x, b, 4); v = x; }
+      else if (t == 'K') { int64_t x; std::memcpy(&x, b, 8); v = (double)x; }
+      else if (t == 'I') { int16_t x; std::memcpy(&x, b, 2); v = x; }
+      else if (t == 'L') v = row[k] == 'T' ? 1 : 0;
+      else v = row[k];
+      out.push_back(v);
+    }
+  }
+  std::fclose(f);
+  return out;
+}
+
+// inmask at nside_cross over the full sky (read_inmask's up/downgrade)
+std::vector<int> read_inmask(const State &S) {
+  long ns = 0;
+  std::string ord;
+  std::vector<double> col = read_fits_column(S.par.file_inmask, ns, ord);
+  if (ord == "RING") fail("Error in subroutine Read_inmask. Input mask should be in NESTED ordering.");
+  if (ord != "NESTED")
+    fail("Error in subroutine Read_inmask. Cannot determine the ordering (nested or ring).");
+  const long nsc = S.par.nside_cross, nss = S.par.nside_submap;
+  const long nin = (ns / nss) * (ns / nss), ncr = (nsc / nss) * (nsc / nss);
+  const long n = nsc >= ns ? (nsc / ns) * (nsc / ns) : (ns / nsc) * (ns / nsc);
+  std::vector<int> mask((size_t)S.nosubmaps_tot * ncr, 0);
+  for (long sm = 0; sm < S.nosubmaps_tot; ++sm) {
+    const double *fb = col.data() + (size_t)sm * nin;
+    int *m = mask.data() + (size_t)sm * ncr;
+    if (nsc >= ns) {
+      for (long i = 0; i < nin; ++i)
+        for (long q = 0; q < n; ++q) m[i * n + q] = fb[i] < 0.5 ? 0 : 1;
+    } else {
+      for (long i = 0; i < ncr; ++i) {
+        bool any = false;
+        for (long q = 0; q < n; ++q) any = any || fb[i * n + q] < 0.5;
+        m[i] = any ? 0 : 1;
+      }
+    }
+  }
+  return mask;
+}
+
 // invert_pixelmatrix_cross (map_routines.f90:83-212)
 void invert_pixelmatrix_cross(State &S) {
   int nmap = S.nmap, nn = nmap * nmap;
   Params &p = S.par;
+  if (!p.file_inmask.empty()) {
+    const std::vector<int> inmask = read_inmask(S);
+    for (long ip = 0; ip < S.nopix_cross; ++ip)
+      if (inmask[ip] == 0)
+        for (int e = 0; e < nn; ++e) S.cca[(size_t)ip * nn + e] = 0.0;
+  }
   if (nmap == 1) {
     for (long ip = 0; ip < S.nopix_cross; ++ip) {
       double &c = S.cca[ip];
@@ -2371,6 +2470,9 @@ void allocate_maps(State &S) {
 // flag_bad_baselines (read_data.f90:30-74)
 void flag_bad_baselines(State &S) {
   if (S.par.good_baseline_fraction == 0 || S.par.kfilter) return;
+  // with an input mask every sample is skipped here: locmask is still zero
+  // when this runs (smadam.F90:309 before the mask is read at 337-345)
+  if (!S.par.file_inmask.empty()) return;
   for (long d = 0; d < S.ndet; ++d)
     for (long k = 0; k < S.noba_short; ++k) {
       long ngood = 0;
