@@ -1305,5 +1305,6 @@ double now_ms() {
 #include "engine_host.inl"
 #include "engine_batch.inl"
 #include "subsets.inl"
+#include "basis.inl"
 
 }  // namespace madam

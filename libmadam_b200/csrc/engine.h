@@ -23,6 +23,7 @@
 namespace madam {
 
 constexpr int kRedBlocks = 1184;      // 148 SMs x 8, fixed for determinism
+constexpr int kMaxBasis = 8;          // basis_order + 1 at most
 
 
 // Owning device allocation.
@@ -223,6 +224,13 @@ class Engine {
   void subtract_baselines();
   void clean_tod();
   void apply_preconditioner(const double *r, double *z);
+  // higher-order baselines (basis_order > 0)
+  void initialize_a_basis();
+  void basis_vectors();
+  void scatter_basis(const double *amp, double sign, double *target, bool fine);
+  void apply_A_basis(const double *p, double *ap, bool timed);
+  void precondition_basis(const double *r, double *z);
+  void clean_tod_basis();
   void scatter_baselines(const double *pw, double *target, bool fine);
   void convolve(const double *x, double *y, const std::vector<ConvSeg> &segs,
                 const double *spectra, DevBuf<ConvSeg> &dsegs);
@@ -277,6 +285,11 @@ class Engine {
   DevBuf<uint32_t> bstart_d_;
   DevBuf<double> bw_;         // per-baseline detector weight
   DevBuf<uint8_t> rmask_;
+  // basis_order + 1 amplitudes per baseline: the F^T F inverses and the
+  // per-amplitude detector weights / residual mask
+  int nbasis_ = 1;  // at most kMaxBasis
+  DevBuf<double> nna_inv_, bwn_;
+  DevBuf<uint8_t> rmaskn_;
   DevBuf<double> times_d_;
 
   // runs for the privatised scatters

@@ -374,6 +374,7 @@ void Engine::run_cached_batch(long ndet, long nsamp, long nnz, double *timestamp
   if (!cached_) fail("destripe_with_cache called with empty caches.");
   if (nrhs < 1) fail("nrhs must be at least 1");
   if (sharded()) fail("the batched solve runs on one rank");
+  if (nbasis_ > 1) fail("the batched solve takes basis_order 0");
   if (par_.temperature_only && nnz != 1)
     fail("temperature_only=T but pointing weights are polarized");
   if (ndet != ndet_ || nsamp != nsamp_ || nnz != nnz_)

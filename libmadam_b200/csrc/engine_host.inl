@@ -237,7 +237,10 @@ void Engine::init_layout(long nperiod, const long *periods) {
     p.precond_width_max = std::max(p.precond_width_min, p.precond_width_max);
   }
   if (p.basis_order > 0 && p.kfilter) fail("Filter only implemented for basis_order==0");
-  if (p.basis_order > 0) fail("basis_order > 0 is not supported");
+  nbasis_ = (int)p.basis_order + 1;
+  if (nbasis_ > kMaxBasis)
+    fail("basis_order above " + std::to_string(kMaxBasis - 1) + " is not supported");
+  if (nbasis_ > 1 && fp32_) fail("the float32 TOD form takes basis_order 0");
   dnshort_ = p.dnshort;
   noba_pp_.assign(ninterval_, 0);
   kstart_pp_.assign(ninterval_ + 1, 0);
@@ -975,6 +978,7 @@ void Engine::initialize_a() {
       MADAM_LAUNCH(k_ccmult<1>, grid_for(nloc_cross_), 256, 0, st_, cca_.get(), wamap_.get(),
                    (long long)nloc_cross_);
   }
+  if (nbasis_ > 1) return initialize_a_basis();
   yba_.alloc(nb);
   nna_.alloc(nb);
   aa_.alloc(nb);
@@ -1207,6 +1211,7 @@ void Engine::construct_preconditioner() {
   band_widths_.clear();
   n_band_fail_ = 0;
   use_diagonal_ = false;
+  if (nbasis_ > 1) return;  // the F^T F inverses precondition (initialize_a_basis)
   const long long nb = (long long)ndet_ * noba_short_;
   if (par_.precond_width_max < 1) return;
   if (!par_.kfilter || par_.precond_width_max == 1) {
@@ -1674,6 +1679,7 @@ void Engine::convolve(const double *x, double *y, const std::vector<ConvSeg> &se
 }
 
 void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) {
+  if (nbasis_ > 1) return apply_A_basis(p, ap, timed);
   const long long nb = (long long)ndet_ * noba_short_;
   // 1) baseline -> map, collect, ccmultiply, scatter back (iterate_a 798-827)
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[0], st_));
@@ -1817,6 +1823,7 @@ void Engine::cg_preconditioner_segments(const double *r, double *z) {
 
 void Engine::apply_preconditioner(const double *r, double *z) {
   // preconditioning_band (noise_routines.f90:1159-1256)
+  if (nbasis_ > 1) return precondition_basis(r, z);
   const long long nb = (long long)ndet_ * noba_short_;
   if (par_.precond_width_max < 1) {
     MADAM_CUDA(cudaMemcpyAsync(z, r, nb * sizeof(double), cudaMemcpyDeviceToDevice, st_));
@@ -1842,10 +1849,18 @@ void Engine::apply_preconditioner(const double *r, double *z) {
 }
 
 void Engine::iterate() {
-  // iterate_a (smadam_routines.f90:677-983)
+  // iterate_a (smadam_routines.f90:677-983); nb counts the CG vectors'
+  // amplitudes (basis_order + 1 per baseline)
   const double t0 = now_ms();
-  const long long nb = (long long)ndet_ * noba_short_;
-  for (auto *b : {&r_, &p_, &z_, &ap_, &ro_, &pw_}) b->alloc(nb);
+  const long long nb = (long long)ndet_ * noba_short_ * nbasis_;
+  const double *bwv = bw_.get();
+  const uint8_t *rmv = rmask_.get();
+  if (nbasis_ > 1) {
+    basis_vectors();
+    bwv = bwn_.get();
+    rmv = rmaskn_.get();
+  }
+  for (auto *b : {&r_, &p_, &z_, &ap_, &ro_, &pw_}) b->alloc(std::max<long long>(1, nb));
   part_.alloc(3 * kRedBlocks);
   scal_.alloc(S_NSCAL);
   scal_.zero(st_);
@@ -1858,10 +1873,10 @@ void Engine::iterate() {
                              st_));
   aa_.zero(st_);
   apply_preconditioner(r_.get(), z_.get());
-  MADAM_LAUNCH(k_update_p, grid_for(nb), 256, 0, st_, p_.get(), z_.get(), pw_.get(), bw_.get(),
+  MADAM_LAUNCH(k_update_p, grid_for(nb), 256, 0, st_, p_.get(), z_.get(), pw_.get(), bwv,
                nb, scal_.get(), 1);
   MADAM_LAUNCH(k_dots, kRedBlocks, 256, 0, st_, r_.get(), z_.get(), r_.get(), r_.get(), nullptr,
-               nullptr, 2, rmask_.get(), nb, part_.get());
+               nullptr, 2, rmv, nb, part_.get());
   finish_dots(2, 0, S_RZ, kRedBlocks, true);
   scal_host_.assign(S_NSCAL, 0.0);
   MADAM_CUDA(cudaMemcpyAsync(scal_host_.data(), scal_.get(), S_NSCAL * sizeof(double),
@@ -1886,7 +1901,7 @@ void Engine::iterate() {
     apply_preconditioner(r_.get(), z_.get());
     MADAM_CUDA(cudaEventRecord(ev_[6], st_));
     MADAM_LAUNCH(k_dots, kRedBlocks, 256, 0, st_, r_.get(), z_.get(), ro_.get(), z_.get(),
-                 r_.get(), r_.get(), 3, rmask_.get(), nb, part_.get());
+                 r_.get(), r_.get(), 3, rmv, nb, part_.get());
     finish_dots(3, 2, 0, kRedBlocks, true);
     MADAM_CUDA(cudaMemcpyAsync(scal_host_.data(), scal_.get(), S_NSCAL * sizeof(double),
                                cudaMemcpyDeviceToHost, st_));
@@ -1906,7 +1921,7 @@ void Engine::iterate() {
     if (rr / rrinit > 1e3) fail("CG is diverging");
     if (rr / rrinit < par_.cglimit && istep > par_.iter_min) break;
     if (rz == 0) break;
-    MADAM_LAUNCH(k_update_p, grid_for(nb), 256, 0, st_, p_.get(), z_.get(), pw_.get(), bw_.get(),
+    MADAM_LAUNCH(k_update_p, grid_for(nb), 256, 0, st_, p_.get(), z_.get(), pw_.get(), bwv,
                  nb, scal_.get(), 0);
   }
   // iterate_a leaves wamap holding the last A.p map (collect_map + ccmultiply
@@ -1922,11 +1937,15 @@ void Engine::iterate() {
 void Engine::subtract_baselines() {
   // subtract_baselines_a (smadam_routines.f90:1489-1539)
   const long long nb = (long long)ndet_ * noba_short_;
-  tmpv_.alloc(nb);
-  MADAM_LAUNCH(k_scale_neg, grid_for(nb), 256, 0, st_, aa_.get(), bw_.get(), tmpv_.get(), nb);
   lmap_fine_.alloc((size_t)std::max<long>(1, nloc_) * nmap_);
   lmap_fine_.zero(st_);
-  scatter_baselines(tmpv_.get(), lmap_fine_.get(), true);
+  if (nbasis_ > 1) {
+    scatter_basis(aa_.get(), -1.0, lmap_fine_.get(), true);
+  } else {
+    tmpv_.alloc(nb);
+    MADAM_LAUNCH(k_scale_neg, grid_for(nb), 256, 0, st_, aa_.get(), bw_.get(), tmpv_.get(), nb);
+    scatter_baselines(tmpv_.get(), lmap_fine_.get(), true);
+  }
   const long long nv = (long long)nloc_ * nmap_;
   ar_sum(lmap_fine_.get(), (size_t)nv);
   if (nv > 0) MADAM_LAUNCH(k_add, grid_for(nv), 256, 0, st_, map_.get(), lmap_fine_.get(), nv);
@@ -1937,11 +1956,12 @@ void Engine::clean_tod() {
   if (!par_.write_tod && par_.ndetset == 0 && par_.nsurvey == 0) return;
   if (!par_.kfirst || tod_cleaned_) return;
   if (isubchunk_ > 0) return;  // only the full-data pass cleans (smadam.F90:432)
+  tod_cleaned_ = true;
+  if (nbasis_ > 1) return clean_tod_basis();
   const long long n = (long long)ndet_ * nsamp_;
   const SampleMap sm = sample_map(istart_d_.get(), kstart_d_.get(), (int)ninterval_, nsamp_,
                                   noba_short_, fdn_);
   if (n > 0) MADAM_LAUNCH(k_clean_tod, grid_for(n), 256, 0, st_, d_tod_, n, sm, aa_.get());
-  tod_cleaned_ = true;
 }
 
 void Engine::finalize(bool first_call) {
@@ -2292,7 +2312,8 @@ long Engine::result_size(const std::string &name) {
   if (name == "hits" || name == "mask" || name == "crit") return npm;
   if (name == "cc") return npm * nmap_ * nmap_;
   if (name == "cca") return npc * nmap_ * nmap_;
-  if (name == "aa" || name == "yba" || name == "nna") return nb;
+  if (name == "aa" || name == "yba") return nb * nbasis_;
+  if (name == "nna") return nb * nbasis_ * nbasis_;
   if (name == "fcov") return (long)fcov_host_.size();
   if (name == "invcov") return (long)invcov_host_.size();
   if (name == "rr_history") return (long)rr_history.size();
@@ -2462,6 +2483,7 @@ void Engine::result_copy(const std::string &name, void *dst, long nbytes) {
 void Engine::bench_iterations(int warmup, int iters, std::vector<double> &out) {
   g_alloc_stream = st_;
   if (!par_.kfirst || noba_short_ == 0) fail("no solve state to benchmark");
+  if (nbasis_ > 1) fail("the iteration benchmark takes basis_order 0");
   const long long nb = (long long)ndet_ * noba_short_;
   DevBuf<double> aa_keep;
   aa_keep.alloc(nb);

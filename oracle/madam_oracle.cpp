@@ -781,8 +781,12 @@ struct State {
   std::vector<int> nohits, outmask;
   std::vector<float> crit;
 
-  // baselines
-  std::vector<double> aa, yba, nna, nna_inv;
+  // baselines; with basis_order > 0 aa / yba hold nbasis amplitudes per
+  // baseline, nnab and nna_inv the nbasis x nbasis blocks (column-major) and
+  // nna their (0, 0) elements
+  std::vector<double> aa, yba, nna, nna_inv, nnab;
+  long nbasis = 1;
+  std::map<long, std::vector<double>> basis_tab;  // baseline length -> table
 
   // filter
   long nof = -1;
@@ -1095,7 +1099,7 @@ void init_parameters(State &S) {
   }
   if (p.basis_order > 0 && p.kfilter)
     fail("Filter only implemented for basis_order==0");
-  if (p.basis_order > 0) fail("basis_order > 0 is not supported");
+  S.nbasis = p.basis_order + 1;
   S.dnshort = p.dnshort;
   if (S.ninterval <= 0) fail("ERROR: intervals not known.");
   S.noba_short_pp.assign(S.ninterval, 0);
@@ -1118,6 +1122,62 @@ void init_parameters(State &S) {
 }
 
 // start_timeloop (parameter_control.f90:752-950) + baseline_times (956-977)
+// r**n for an integer n >= 0 by binary powering
+double ipow(double r, long n) {
+  double out = 1, x = r;
+  while (n > 0) {
+    if (n & 1) out *= x;
+    n >>= 1;
+    if (n) x *= x;
+  }
+  return out;
+}
+
+// the destriping basis functions of one baseline length (start_timeloop,
+// parameter_control.f90:853-933), table[o + nbasis * i] for sample i of
+// the baseline and order o.  `dr = 2. / nsamp` divides in default real.
+const std::vector<double> &basis_table(State &S, long len) {
+  auto it = S.basis_tab.find(len);
+  if (it != S.basis_tab.end()) return it->second;
+  const long nf = S.nbasis;
+  std::vector<double> t((size_t)nf * std::max(len, 0L), 0.0);
+  const double dr = (double)(2.0f / (float)len);
+  const double rstart = 0.5 * dr - 1;
+  for (long i = 0; i < len; ++i) {
+    double *f = &t[(size_t)nf * i];
+    const double r = rstart + (double)i * dr;
+    switch (S.par.basis_func) {
+      case 1:  // polynomial
+        for (long o = 0; o < nf; ++o) f[o] = ipow(r, o);
+        break;
+      case 2: {  // real Fourier
+        const double x = (double)i * (kPi / (double)len);
+        for (long o = 0; o < nf; ++o)
+          f[o] = (o % 2 == 0) ? std::cos((double)o * x) : std::sin((double)(o + 1) * x);
+        break;
+      }
+      case 3: {  // Chebyshev, second kind, times (1 - r^2)^(1/4)
+        for (long o = 0; o < nf; ++o)
+          f[o] = o == 0 ? 1.0 : o == 1 ? 2 * r : 2 * r * f[o - 1] - f[o - 2];
+        const double g = std::pow(1 - r * r, 0.25);
+        for (long o = 0; o < nf; ++o) f[o] = f[o] * g;
+        break;
+      }
+      default:  // Legendre
+        for (long o = 0; o < nf; ++o)
+          f[o] = o == 0 ? 1.0
+                 : o == 1 ? r
+                          : ((double)(2 * o - 1) * r * f[o - 1] - (double)(o - 1) * f[o - 2]) /
+                                (double)o;
+    }
+  }
+  return S.basis_tab[len] = std::move(t);
+}
+
+const double *basis_of(const State &S, long k) {
+  return S.basis_tab.at(S.bstop[k] - S.bstart[k] + 1).data();
+}
+
 void start_timeloop(State &S) {
   std::vector<long> len(S.noba_short);
   long m = 0;
@@ -1144,6 +1204,9 @@ void start_timeloop(State &S) {
   }
   S.btime.assign(S.noba_short, 0);
   for (long k = 0; k < S.noba_short; ++k) S.btime[k] = S.times[S.bstart[k]];
+  S.basis_tab.clear();
+  if (S.par.kfirst && S.nbasis > 1)
+    for (long k = 0; k < S.noba_short; ++k) basis_table(S, len[k]);
   // split every interval into subchunks (parameter_control.f90:820-835)
   if (S.nsubchunk > 0) {
     S.subchunk.assign(S.nsamp, 0);
@@ -1794,7 +1857,10 @@ void invert_pixelmatrix_map(State &S) {
 }
 
 // initialize_a (smadam_routines.f90:428-671), basis_order = 0
+void initialize_a_basis(State &S);
+
 void initialize_a(State &S) {
+  if (S.nbasis > 1) return initialize_a_basis(S);
   ccmultiply(S, S.cca, S.wamap, S.nopix_cross);
   scatter_map(S, S.wamap, S.nosubpix_cross);
   int nmap = S.nmap;
@@ -1852,6 +1918,101 @@ void initialize_a(State &S) {
         S.nna_inv[o] = 1.0 / ev;
       }
     }
+}
+
+// initialize_a (smadam_routines.f90:505-671) for basis_order > 0: the
+// right-hand side yba(0:order) and the F^T F blocks nna of every baseline,
+// then their inverses for the block-diagonal preconditioner from the
+// eigen-decomposition (dsyev), with the reference's rules for empty and
+// degenerate blocks
+void initialize_a_basis(State &S) {
+  ccmultiply(S, S.cca, S.wamap, S.nopix_cross);
+  scatter_map(S, S.wamap, S.nosubpix_cross);
+  const int nmap = S.nmap;
+  const long nf = S.nbasis, nn = nf * nf;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(S.nthreads)
+  for (long d = 0; d < S.ndet; ++d) {
+    for (long iv = 0; iv < S.ninterval; ++iv) {
+      long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
+      int ipsd = psd_index_det(S, d, S.btime[ks]);
+      if (ipsd < 0) continue;
+      double detw = S.dets[d].weights[ipsd];
+      if (detw == 0) continue;
+      for (long k = ks; k < ks + noba; ++k) {
+        const size_t b = d * S.noba_short + k;
+        double *y = &S.yba[b * nf], *n = &S.nnab[b * nn];
+        for (long o = 0; o < nf; ++o) y[o] = 0;
+        for (long e = 0; e < nn; ++e) n[e] = 0;
+        const double *bf = basis_of(S, k);
+        for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+          if (!sub_on(S, i)) continue;
+          size_t s = (size_t)d * S.nsamp + i;
+          long ip = S.pixels[s];
+          if (ip == S.dummy_pixel) continue;
+          const double *lm = &S.locmap[(size_t)ip * nmap];
+          bool allz = true;
+          for (int c = 0; c < nmap; ++c)
+            if (lm[c] != 0) allz = false;
+          if (allz) continue;
+          const double *f = bf + nf * (i - S.bstart[k]);
+          for (long o = 0; o < nf; ++o) {
+            y[o] = y[o] + f[o] * S.tod[s];
+            for (long o2 = 0; o2 < nf; ++o2) n[o2 + nf * o] = n[o2 + nf * o] + f[o] * f[o2];
+          }
+          double mw;
+          if (nmap == 1) {
+            mw = lm[0];
+          } else {
+            const float *wf = S.weights + s * S.nnz;
+            mw = lm[0] * (double)wf[0] + lm[1] * (double)wf[1] + lm[2] * (double)wf[2];
+          }
+          for (long o = 0; o < nf; ++o) y[o] = y[o] - f[o] * mw;
+        }
+        for (long o = 0; o < nf; ++o) y[o] = y[o] * detw;
+        for (long e = 0; e < nn; ++e) n[e] = n[e] * detw;
+      }
+    }
+  }
+  std::vector<double> w(nf), v(nn);
+  for (long d = 0; d < S.ndet; ++d)
+    for (long iv = 0; iv < S.ninterval; ++iv) {
+      long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
+      int ipsd = psd_index_det(S, d, S.btime[ks]);
+      if (ipsd < 0) continue;
+      if (S.dets[d].weights[ipsd] == 0) continue;
+      for (long k = ks; k < ks + noba; ++k) {
+        const size_t b = d * S.noba_short + k;
+        double *n = &S.nnab[b * nn], *inv = &S.nna_inv[b * nn], *y = &S.yba[b * nf];
+        for (long e = 0; e < nn; ++e) inv[e] = 0;
+        int ierr = 0;
+        if (std::fabs(n[0]) < kTiny30) {
+          std::fill(w.begin(), w.end(), 0.0);
+        } else {
+          ierr = sym_eig((int)nf, n, w.data(), v.data());
+        }
+        const double wmin = *std::min_element(w.begin(), w.end());
+        const double wmax = *std::max_element(w.begin(), w.end());
+        if (ierr != 0) {
+          for (long e = 0; e < nn; ++e) n[e] = 0;
+          for (long o = 0; o < nf; ++o) y[o] = 0;
+        } else if (wmin == 0 && wmax == 0) {
+          for (long e = 0; e < nn; ++e) n[e] = 0;
+          for (long o = 0; o < nf; ++o) y[o] = 0;
+          continue;
+        } else if (wmin / wmax < kRcondSing) {
+          for (long j = 0; j < nf; ++j) inv[j + nf * j] = 1 / n[j + nf * j];
+          continue;
+        }
+        // V diag(1/w) V^T
+        for (long a = 0; a < nf; ++a)
+          for (long c = 0; c < nf; ++c) {
+            double t = 0;
+            for (long i = 0; i < nf; ++i) t += (v[a + nf * i] / w[i]) * v[c + nf * i];
+            inv[a + nf * c] = t;
+          }
+      }
+    }
+  for (size_t b = 0; b < S.nna.size(); ++b) S.nna[b] = S.nnab[b * nn];
 }
 
 // ----------------------------------------------------- FFT convolution ---
@@ -2121,8 +2282,11 @@ void apply_preconditioner(State &S, std::vector<double> &z,
   }
 }
 
+void iterate_a_basis(State &S);
+
 // iterate_a (smadam_routines.f90:677-983), basis_order = 0
 void iterate_a(State &S) {
+  if (S.nbasis > 1) return iterate_a_basis(S);
   Params &p = S.par;
   long nb = S.noba_short * S.ndet;
   int nmap = S.nmap;
@@ -2265,10 +2429,173 @@ void iterate_a(State &S) {
   S.rr_final = rr / rrinit;
 }
 
+// iterate_a (smadam_routines.f90:677-983) for basis_order > 0: the
+// baseline_to_map_{nopol,general} (1140-1226) and map_to_baseline_{nopol,
+// general} (1379-1480) projections with the basis functions, no noise
+// filter (only diagfilter), and the block-diagonal preconditioner nna_inv
+// (apply_preconditioner, 943-957)
+void iterate_a_basis(State &S) {
+  Params &p = S.par;
+  const long nf = S.nbasis, nn = nf * nf;
+  const long nbl = S.noba_short * S.ndet, nv = nbl * nf;
+  const int nmap = S.nmap;
+  std::vector<double> r(nv, 0), pv(nv, 0), z(nv, 0), ap(nv, 0), ro(nv, 0);
+  std::vector<char> rmask(nv, 0);
+  for (long d = 0; d < S.ndet; ++d)
+    for (long iv = 0; iv < S.ninterval; ++iv) {
+      long ks = S.kstart_pp[iv], kstop = ks + S.noba_short_pp[iv];
+      while (true) {
+        long noba;
+        trim_interval(S, ks, kstop, noba, d);
+        if (noba == 0) break;
+        for (long k = ks; k < ks + noba; ++k)
+          for (long o = 0; o < nf; ++o) rmask[(d * S.noba_short + k) * nf + o] = 1;
+        ks += noba;
+      }
+    }
+  auto precondition = [&](std::vector<double> &zz, const std::vector<double> &rr) {
+    for (long b = 0; b < nbl; ++b)
+      for (long a = 0; a < nf; ++a) {
+        double t = 0;
+        for (long c = 0; c < nf; ++c) t += S.nna_inv[b * nn + a + nf * c] * rr[b * nf + c];
+        zz[b * nf + a] = t;
+      }
+  };
+  std::fill(S.aa.begin(), S.aa.end(), 0.0);
+  r = S.yba;
+  precondition(z, r);
+  pv = z;
+  auto mdot = [&](const std::vector<double> &a, const std::vector<double> &b) {
+    double s = 0;
+    for (long i = 0; i < nv; ++i)
+      if (rmask[i]) s += a[i] * b[i];
+    return allreduce_sum(s);
+  };
+  double rz = mdot(r, z), rr = mdot(r, r);
+  double rzinit = rz, rrinit = rr;
+  S.rrinit = rrinit;
+  S.rr_history.clear();
+  S.noiter = 0;
+  if (rzinit < kTiny30) return;
+  if (std::isnan(rz)) return;
+  std::vector<double> bw(nbl, 0.0);
+  for (long d = 0; d < S.ndet; ++d)
+    for (long iv = 0; iv < S.ninterval; ++iv) {
+      long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
+      int ipsd = psd_index_det(S, d, S.btime[ks]);
+      if (ipsd < 0) continue;
+      double detw = S.dets[d].weights[ipsd];
+      for (long k = ks; k < ks + noba; ++k) bw[d * S.noba_short + k] = detw;
+    }
+  double t0 = omp_get_wtime();
+  long istep = 0;
+  while (true) {
+    if (istep >= p.iter_max) break;
+    ++istep;
+    std::fill(S.locmap.begin(), S.locmap.end(), 0.0);
+#pragma omp parallel num_threads(S.nthreads)
+    {
+      int tid = omp_get_thread_num(), nth = omp_get_num_threads();
+      long npix_thread = (S.nsize_locmap + nth - 1) / nth;
+      long first = tid * npix_thread;
+      long last = std::min(first + npix_thread - 1, S.dummy_pixel - 1);
+      for (long d = 0; d < S.ndet; ++d)
+        for (long iv = 0; iv < S.ninterval; ++iv) {
+          long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
+          double detw = bw[d * S.noba_short + ks];
+          if (detw == 0) continue;
+          for (long k = ks; k < ks + noba; ++k) {
+            const double *bf = basis_of(S, k), *pk = &pv[(d * S.noba_short + k) * nf];
+            for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+              if (!sub_on(S, i)) continue;
+              size_t s = (size_t)d * S.nsamp + i;
+              long ip = S.pixels[s];
+              if (ip < first || ip > last) continue;
+              const double *f = bf + nf * (i - S.bstart[k]);
+              double dp = 0;
+              for (long o = 0; o < nf; ++o) dp += f[o] * pk[o];
+              if (nmap == 1) {
+                S.locmap[ip] = S.locmap[ip] + detw * dp;
+              } else {
+                const double pw = dp * detw;
+                const float *wf = S.weights + s * S.nnz;
+                for (int c = 0; c < 3; ++c)
+                  S.locmap[(size_t)ip * 3 + c] = S.locmap[(size_t)ip * 3 + c] + (double)wf[c] * pw;
+              }
+            }
+          }
+        }
+    }
+    std::fill(S.wamap.begin(), S.wamap.end(), 0.0);
+    collect_map(S, S.wamap, S.nosubpix_cross);
+    ccmultiply(S, S.cca, S.wamap, S.nopix_cross);
+    scatter_map(S, S.wamap, S.nosubpix_cross);
+    std::fill(ap.begin(), ap.end(), 0.0);
+    if (p.diagfilter != 0)
+      for (long b = 0; b < nbl; ++b)
+        for (long o = 0; o < nf; ++o)
+          ap[b * nf + o] = S.nnab[b * nn + o + nf * o] * pv[b * nf + o] * p.diagfilter;
+#pragma omp parallel for schedule(static, 1) num_threads(S.nthreads)
+    for (long t = 0; t < S.ndet * S.ninterval; ++t) {
+      long d = t / S.ninterval, iv = t % S.ninterval;
+      long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
+      double detw = bw[d * S.noba_short + ks];
+      if (detw == 0) continue;
+      std::vector<double> apnv(nf);
+      for (long k = ks; k < ks + noba; ++k) {
+        const double *bf = basis_of(S, k);
+        std::fill(apnv.begin(), apnv.end(), 0.0);
+        for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+          if (!sub_on(S, i)) continue;
+          size_t s = (size_t)d * S.nsamp + i;
+          long ip = S.pixels[s];
+          if (ip == S.dummy_pixel) continue;
+          double mw;
+          if (nmap == 1) {
+            mw = S.locmap[ip];
+          } else {
+            const float *wf = S.weights + s * S.nnz;
+            const double *lm = &S.locmap[(size_t)ip * 3];
+            mw = (double)wf[0] * lm[0] + (double)wf[1] * lm[1] + (double)wf[2] * lm[2];
+          }
+          const double *f = bf + nf * (i - S.bstart[k]);
+          for (long o = 0; o < nf; ++o) apnv[o] = apnv[o] + mw * f[o];
+        }
+        const size_t b = d * S.noba_short + k;
+        for (long a = 0; a < nf; ++a) {
+          double t2 = 0;
+          for (long c = 0; c < nf; ++c) t2 += S.nnab[b * nn + a + nf * c] * pv[b * nf + c];
+          ap[b * nf + a] = ap[b * nf + a] + (t2 - apnv[a] * detw);
+        }
+      }
+    }
+    double pap = mdot(pv, ap);
+    double alpha = rz / pap;
+    ro = r;
+    for (long i = 0; i < nv; ++i) S.aa[i] = S.aa[i] + alpha * pv[i];
+    for (long i = 0; i < nv; ++i) r[i] = r[i] - alpha * ap[i];
+    precondition(z, r);
+    double rzo = rz;
+    rz = mdot(r, z);
+    double rz2 = mdot(ro, z);
+    rr = mdot(r, r);
+    double beta = (rz - rz2) / rzo;
+    S.rr_history.push_back(rr / rrinit);
+    S.noiter = istep;
+    if (rr / rrinit > 1e3) fail("CG is diverging");
+    if (rr / rrinit < p.cglimit && istep > p.iter_min) break;
+    if (rz == 0) break;
+    for (long i = 0; i < nv; ++i) pv[i] = z[i] + beta * pv[i];
+  }
+  S.t_iterate = omp_get_wtime() - t0;
+  S.rr_final = rr / rrinit;
+}
+
 // subtract_baselines_a (smadam_routines.f90:1489-1539)
 void subtract_baselines_a(State &S) {
   std::fill(S.locmap.begin(), S.locmap.end(), 0.0);
   int nmap = S.nmap;
+  const long nf = S.nbasis;
   for (long d = 0; d < S.ndet; ++d)
     for (long iv = 0; iv < S.ninterval; ++iv) {
       long ks = S.kstart_pp[iv], noba = S.noba_short_pp[iv];
@@ -2282,7 +2609,16 @@ void subtract_baselines_a(State &S) {
           size_t s = (size_t)d * S.nsamp + i;
           long ip = S.pixels[s];
           if (ip == S.dummy_pixel) continue;
-          double aw = (1.0 * S.aa[d * S.noba_short + k]) * detw;
+          double aw;
+          if (nf == 1) {
+            aw = (1.0 * S.aa[d * S.noba_short + k]) * detw;
+          } else {
+            const double *f = basis_of(S, k) + nf * (i - S.bstart[k]);
+            const double *a = &S.aa[(d * S.noba_short + k) * nf];
+            double dp = 0;
+            for (long o = 0; o < nf; ++o) dp += f[o] * a[o];
+            aw = dp * detw;
+          }
           if (nmap == 1) {
             S.locmap[ip] = S.locmap[ip] - aw;
           } else {
@@ -2444,12 +2780,19 @@ void clean_tod(State &S) {
   if (!p.write_tod && p.ndetset == 0 && p.nsurvey == 0) return;
   if (!p.kfirst) return;
   if (S.tod_cleaned) return;
+  const long nf = S.nbasis;
   for (long d = 0; d < S.ndet; ++d)
     for (long k = 0; k < S.noba_short; ++k)
-      for (long i = S.bstart[k]; i <= S.bstop[k]; ++i)
-        if (sub_on(S, i))
-          S.tod[(size_t)d * S.nsamp + i] =
-              S.tod[(size_t)d * S.nsamp + i] - 1.0 * S.aa[d * S.noba_short + k];
+      for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+        if (!sub_on(S, i)) continue;
+        double &t = S.tod[(size_t)d * S.nsamp + i];
+        if (nf == 1) {
+          t = t - 1.0 * S.aa[d * S.noba_short + k];
+        } else {
+          const double *f = basis_of(S, k) + nf * (i - S.bstart[k]);
+          for (long o = 0; o < nf; ++o) t = t - f[o] * S.aa[(d * S.noba_short + k) * nf + o];
+        }
+      }
   S.tod_cleaned = true;
 }
 
@@ -2579,10 +2922,12 @@ void run_destripe(State &S, long nperiod, const long *periods) {
   const int nsub = S.nsubchunk;
   for (int counter = nsub ? (int)p.isubchunk : 0; counter <= nsub; ++counter) {
     S.isubchunk = nsub ? (counter + 1) % (nsub + 1) : 0;
-    S.aa.assign((size_t)S.noba_short * S.ndet, 0.0);
-    S.yba.assign((size_t)S.noba_short * S.ndet, 0.0);
-    S.nna.assign((size_t)S.noba_short * S.ndet, 0.0);
-    S.nna_inv.assign((size_t)S.noba_short * S.ndet, 0.0);
+    const size_t nbl = (size_t)S.noba_short * S.ndet, nf = S.nbasis;
+    S.aa.assign(nbl * nf, 0.0);
+    S.yba.assign(nbl * nf, 0.0);
+    S.nna.assign(nbl, 0.0);
+    S.nna_inv.assign(nbl * nf * nf, 0.0);
+    S.nnab.assign(nf > 1 ? nbl * nf * nf : 0, 0.0);
     allocate_maps(S);
     if (p.kfirst) flag_bad_baselines(S);
     pixel_matrix(S);
@@ -2642,6 +2987,7 @@ void run_cached(State &S) {
   std::fill(S.yba.begin(), S.yba.end(), 0.0);
   std::fill(S.nna.begin(), S.nna.end(), 0.0);
   std::fill(S.nna_inv.begin(), S.nna_inv.end(), 0.0);
+  std::fill(S.nnab.begin(), S.nnab.end(), 0.0);
   reduce_pixels(S);
   update_maptod_transfer(S);
   std::fill(S.map.begin(), S.map.end(), 0.0);
@@ -2765,7 +3111,7 @@ long oracle_result_size(const char *name) {
   if (n == "cca") return (long)S.cca.size();
   if (n == "aa") return (long)S.aa.size();
   if (n == "yba") return (long)S.yba.size();
-  if (n == "nna") return (long)S.nna.size();
+  if (n == "nna") return (long)(S.nbasis > 1 ? S.nnab.size() : S.nna.size());
   if (n == "fcov") return (long)S.fcov.size();
   if (n == "invcov") return (long)S.invcov.size();
   if (n == "rr_history") return (long)S.rr_history.size();
@@ -2794,7 +3140,7 @@ int oracle_result_copy(const char *name, void *dst) {
   if (n == "cca") return cp(S.cca);
   if (n == "aa") return cp(S.aa);
   if (n == "yba") return cp(S.yba);
-  if (n == "nna") return cp(S.nna);
+  if (n == "nna") return S.nbasis > 1 ? cp(S.nnab) : cp(S.nna);
   if (n == "fcov") return cp(S.fcov);
   if (n == "invcov") return cp(S.invcov);
   if (n == "rr_history") return cp(S.rr_history);
