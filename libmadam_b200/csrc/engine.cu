@@ -1306,5 +1306,6 @@ double now_ms() {
 #include "engine_batch.inl"
 #include "subsets.inl"
 #include "basis.inl"
+#include "covmat.inl"
 
 }  // namespace madam

@@ -231,6 +231,8 @@ class Engine {
   void apply_A_basis(const double *p, double *ap, bool timed);
   void precondition_basis(const double *r, double *z);
   void clean_tod_basis();
+  // the inverse noise covariance files (file_covmat) in place of the solve
+  void write_covmat();
   void scatter_baselines(const double *pw, double *target, bool fine);
   void convolve(const double *x, double *y, const std::vector<ConvSeg> &segs,
                 const double *spectra, DevBuf<ConvSeg> &dsegs);

@@ -172,6 +172,12 @@ void Engine::init_layout(long nperiod, const long *periods) {
     p.isubchunk = 0;
   }
   if (p.isubchunk > p.nsubchunk) fail("ERROR: isubchunk > nsubchunk");
+  // parameter_control.f90:128-131
+  if (!p.file_covmat.empty()) {
+    p.kfilter = true;
+    p.kfirst = true;
+    if (p.nsubchunk > 0) fail("file_covmat with nsubchunk > 1 is not supported");
+  }
   if (p.good_baseline_fraction < 0 || p.good_baseline_fraction > 1)
     fail("ERROR: good_baseline_fraction must be in 0..1");
   if (p.nside_cross < 0) p.nside_cross = p.nside_map;
@@ -184,7 +190,6 @@ void Engine::init_layout(long nperiod, const long *periods) {
   if (p.pixmode_map < 0 || p.pixmode_map > 2) fail("Pixmode_map must be in range [0-2]");
   if (p.pixmode_cross < 0 || p.pixmode_cross > 4) fail("Pixmode_cross must be in range [0-4]");
   if (!p.file_spectrum.empty()) fail("file_spectrum is not supported");
-  if (!p.file_covmat.empty()) fail("file_covmat is not supported");
   if (nmap_ == 1) p.temperature_only = true;
   else if (p.temperature_only) nmap_ = 1;
   if (nmap_ != 1 && nmap_ != 3) fail("only nnz = 1 or nnz = 3 is supported");
@@ -450,7 +455,9 @@ void Engine::flag_and_compact(bool first_call) {
                    (int)nosubpix_max_, nullptr, pixc_.get());
   }
   MADAM_CUDA(cudaStreamSynchronize(st_));
-  if (!in_device_) wraw_.reset();
+  // the staging copy of host weights is done with, unless the covariance
+  // files read the raw weights later
+  if (!in_device_ && par_.file_covmat.empty()) wraw_.reset();
   // detector weights per (det, period) and per baseline
   if (first_call) {
     detw_iv_.assign((size_t)ndet_ * ninterval_, 0.0);
@@ -2224,7 +2231,9 @@ void Engine::run(const Params &par, std::vector<Detector> dets, long ndet, long 
     mark(9);
     MADAM_CUDA(cudaStreamSynchronize(st_));
     timings.setup_ms = now_ms() - t0;
-    iterate();
+    // write_covmat in place of the solve (smadam.F90:364-377)
+    if (par_.file_covmat.empty()) iterate();
+    else write_covmat();
   } else {
     MADAM_CUDA(cudaStreamSynchronize(st_));
     timings.setup_ms = now_ms() - t0;

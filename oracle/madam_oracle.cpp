@@ -1031,6 +1031,12 @@ void init_parameters(State &S) {
   }
   if (p.isubchunk > p.nsubchunk) fail("ERROR: isubchunk > nsubchunk");
   S.nsubchunk = (int)p.nsubchunk;
+  // parameter_control.f90:128-131
+  if (!p.file_covmat.empty()) {
+    p.kfilter = true;
+    p.kfirst = true;
+    if (S.nsubchunk > 0) fail("file_covmat with nsubchunk > 1 is not supported");
+  }
   if (p.good_baseline_fraction < 0 || p.good_baseline_fraction > 1)
     fail("ERROR: good_baseline_fraction must be in 0..1");
   if (p.nside_cross < 0) p.nside_cross = p.nside_map;
@@ -1045,7 +1051,6 @@ void init_parameters(State &S) {
   if (p.pixmode_cross < 0 || p.pixmode_cross > 4)
     fail("Pixmode_cross must be in range [0-4]");
   if (!p.file_spectrum.empty()) fail("file_spectrum is not supported");
-  if (!p.file_covmat.empty()) fail("file_covmat is not supported");
   if (S.nmap == 1) p.temperature_only = true;
   else if (p.temperature_only) S.nmap = 1;
   if (S.nmap != 1 && S.nmap != 3) fail("only nnz = 1 or nnz = 3 is supported");
@@ -2631,6 +2636,142 @@ void subtract_baselines_a(State &S) {
   collect_map(S, S.map, S.nosubpix_map);
 }
 
+// write_covmat (covmat.F90:48-186) with get_ptf (434-470), get_hitmap
+// (358-431), get_middlematrix (474-530), add_white (190-222), symmetrize
+// (226-244) and save_matrix (248-354): for every detector the dense inverse
+// noise covariance of the map per pointing period,
+//   P^T C_w^-1 P - P^T C_w^-1 F M F^T C_w^-1 P,  M = (C_a^-1 + F^T C_w^-1 F)^-1,
+// with M the Toeplitz matrix of irfft(1 / (fcov + nshort / sigma^2)),
+// written as N x N native doubles (N = 12 nside_map^2 nmap), column-major,
+// to <file_covmat>_<detector>_inv_bin.dat; an existing file is skipped.
+// Ranks add their matrices (the reference's ring pass) and rank 0 writes.
+void write_covmat(State &S) {
+  const Params &p = S.par;
+  const int nmap = S.nmap;
+  const long npix = 12 * p.nside_map * p.nside_map, N = npix * nmap;
+  // nolocpix local pixels; the flagged samples carry the local dummy pixel
+  // nolocpix, which the reference accumulates into an extra slot of its
+  // local matrices and never saves (dummy_pixel itself is 12 nside_max^2
+  // here, smadam.F90:293)
+  const long nloc = S.nolocmaps * S.nosubpix_max, nof = S.nof, nh = nof / 2 + 1;
+  auto gpix = [&](long ip) { return ip + S.subtable2[ip / S.nosubpix_max] * S.nosubpix_max; };
+  double detweight = 0;
+  std::vector<double> mm, xx(nof);
+  std::vector<std::complex<double>> fx(nh), work;
+  for (long d = 0; d < S.ndet; ++d) {
+    const std::string out = p.file_covmat + "_" + S.dets[d].name + "_inv_bin.dat";
+    int there = 0;
+    if (g_rank == 0) {
+      FILE *f = std::fopen(out.c_str(), "rb");
+      there = f != nullptr;
+      if (f) std::fclose(f);
+    }
+    if (allreduce_sum(there) > 0) continue;
+    // local_covmat(a, b, jpix, ipix) at ((ipix * nloc + jpix) * nmap + b) * nmap + a
+    std::vector<double> lc((size_t)nmap * nmap * nloc * nloc, 0.0);
+    auto L = [&](int a, int b, long j, long i) -> double & {
+      return lc[(((size_t)i * nloc + j) * nmap + b) * nmap + a];
+    };
+    long last_ipsd = -1, last_noba = -1;
+    for (long iv = 0; iv < S.ninterval; ++iv) {
+      long ks = S.kstart_pp[iv], kstop = ks + S.noba_short_pp[iv];
+      while (true) {
+        long noba;
+        trim_interval(S, ks, kstop, noba, d);
+        if (noba == 0) break;
+        const int ipsd = psd_index(S, d, S.btime[ks]);
+        const int ipsd_det = psd_index_det(S, d, S.btime[ks]);
+        if (ipsd_det < 0) break;
+        detweight = 1 / (S.dets[d].sigmas[ipsd_det] * S.dets[d].sigmas[ipsd_det]);
+        if (detweight == 0) break;
+        // get_ptf: P^T F of the segment, ptf[(ip * noba + k) * nmap + c]
+        std::vector<double> ptf((size_t)nloc * noba * nmap, 0.0);
+        std::vector<std::vector<long>> hits(nloc);
+        for (long k = 0; k < noba; ++k)
+          for (long i = S.bstart[ks + k]; i <= S.bstop[ks + k]; ++i) {
+            const size_t s = (size_t)d * S.nsamp + i;
+            const long ip = S.pixels[s];
+            if (ip == S.dummy_pixel || ip >= nloc) continue;
+            const float *wf = S.weights + s * S.nnz;
+            for (int c = 0; c < nmap; ++c) ptf[((size_t)ip * noba + k) * nmap + c] += (double)wf[c];
+            if (hits[ip].empty() || hits[ip].back() != k) hits[ip].push_back(k);
+          }
+        for (double &v : ptf)
+          if (v != 0) v = v * detweight;
+        // get_middlematrix
+        if (ipsd != last_ipsd || noba != last_noba) {
+          if (nof < 2 * noba)
+            fail("ERROR: filter is too short to reliably estimate the middle matrix");
+          for (long k = 0; k < nh; ++k)
+            fx[k] = 1.0 / std::complex<double>(S.fcov[(size_t)ipsd * nh + k] +
+                                                   (double)S.nshort * detweight, 0.0);
+          S.fft->irfft(fx.data(), xx.data(), work);
+          mm.assign(xx.begin(), xx.begin() + noba);
+          last_ipsd = ipsd;
+          last_noba = noba;
+        }
+        // the double loop over the non-zeros of P^T F
+        for (long ip = 0; ip < nloc; ++ip) {
+          if (hits[ip].empty()) continue;
+          for (long jp = ip; jp < nloc; ++jp) {
+            if (hits[jp].empty()) continue;
+            for (long ib : hits[ip])
+              for (long jb : hits[jp]) {
+                const double m = -mm[std::labs(jb - ib)];
+                const double *pi = &ptf[((size_t)ip * noba + ib) * nmap];
+                const double *pj = &ptf[((size_t)jp * noba + jb) * nmap];
+                for (int b = 0; b < nmap; ++b) {
+                  const double ptf1 = m * pi[b];
+                  for (int a = 0; a < nmap; ++a) L(a, b, jp, ip) = L(a, b, jp, ip) + pj[a] * ptf1;
+                }
+              }
+          }
+        }
+        ks += noba;
+      }
+    }
+    // add_white: detweight w w^T on the diagonal blocks, every sample
+    for (long k = 0; k < S.noba_short; ++k)
+      for (long i = S.bstart[k]; i <= S.bstop[k]; ++i) {
+        const size_t s = (size_t)d * S.nsamp + i;
+        const long ip = S.pixels[s];
+        if (ip == S.dummy_pixel || ip >= nloc) continue;
+        const float *wf = S.weights + s * S.nnz;
+        for (int b = 0; b < nmap; ++b) {
+          const double t = detweight * (double)wf[b];
+          for (int a = 0; a < nmap; ++a) L(a, b, ip, ip) = L(a, b, ip, ip) + (double)wf[a] * t;
+        }
+      }
+    // symmetrize
+    for (long ip = 0; ip < nloc; ++ip)
+      for (long jp = ip + 1; jp < nloc; ++jp)
+        if (L(0, 0, jp, ip) != 0)
+          for (int a = 0; a < nmap; ++a)
+            for (int b = 0; b < nmap; ++b) L(a, b, ip, jp) = L(b, a, jp, ip);
+    // save_matrix
+    std::vector<double> G((size_t)N * N, 0.0);
+    for (long i1 = 0; i1 < nloc; ++i1)
+      for (long i2 = 0; i2 < nloc; ++i2) {
+        if (L(0, 0, i2, i1) == 0) continue;
+        const long p1 = gpix(i1), p2 = gpix(i2);
+        for (int b = 0; b < nmap; ++b)
+          for (int a = 0; a < nmap; ++a)
+            G[(size_t)(p1 * nmap + b) * N + p2 * nmap + a] += L(a, b, i2, i1);
+      }
+    if (g_nranks > 1) allreduce(G.data(), (long)G.size(), 0);
+    for (long p1 = 0; p1 < npix; ++p1)
+      if (G[(size_t)(p1 * nmap) * N + p1 * nmap] == 0)
+        for (int a = 0; a < nmap; ++a) G[(size_t)(p1 * nmap + a) * N + p1 * nmap + a] = -1;
+    if (g_rank == 0) {
+      FILE *f = std::fopen(out.c_str(), "wb");
+      if (!f) fail("Unable to open covmat file");
+      const bool ok = std::fwrite(G.data(), sizeof(double), G.size(), f) == G.size();
+      std::fclose(f);
+      if (!ok) fail("Failed to write covmat file");
+    }
+  }
+}
+
 // makemaps (map_routines.f90:327-357)
 void makemaps(State &S, std::vector<double> &map) {
   ccmultiply(S, S.cc, map, S.nopix_map);
@@ -2937,8 +3078,12 @@ void run_destripe(State &S, long nperiod, const long *periods) {
       invert_pixelmatrix_cross(S);
       initialize_a(S);
       construct_preconditioner(S);
-      iterate_a(S);
-      subtract_baselines_a(S);
+      if (!p.file_covmat.empty()) {
+        write_covmat(S);  // in place of the solve (smadam.F90:364-377)
+      } else {
+        iterate_a(S);
+        subtract_baselines_a(S);
+      }
     }
     invert_pixelmatrix_map(S);
     makemaps(S, S.binmap);
@@ -3113,6 +3258,11 @@ long oracle_result_size(const char *name) {
   if (n == "yba") return (long)S.yba.size();
   if (n == "nna") return (long)(S.nbasis > 1 ? S.nnab.size() : S.nna.size());
   if (n == "fcov") return (long)S.fcov.size();
+  if (n == "sigmas") {
+    long m = 0;
+    for (const auto &d : S.dets) m += (long)d.sigmas.size();
+    return m;
+  }
   if (n == "invcov") return (long)S.invcov.size();
   if (n == "rr_history") return (long)S.rr_history.size();
   if (n == "band_widths") return (long)S.band_widths.size();
@@ -3142,6 +3292,11 @@ int oracle_result_copy(const char *name, void *dst) {
   if (n == "yba") return cp(S.yba);
   if (n == "nna") return S.nbasis > 1 ? cp(S.nnab) : cp(S.nna);
   if (n == "fcov") return cp(S.fcov);
+  if (n == "sigmas") {
+    std::vector<double> v;
+    for (const auto &d : S.dets) v.insert(v.end(), d.sigmas.begin(), d.sigmas.end());
+    return cp(v);
+  }
   if (n == "invcov") return cp(S.invcov);
   if (n == "rr_history") return cp(S.rr_history);
   if (n == "band_widths") return cp(S.band_widths);
