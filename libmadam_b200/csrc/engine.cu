@@ -1059,6 +1059,27 @@ __global__ void k_finish(const double *part, int nblk, int nd, double *scal, int
   }
 }
 
+// device copy of a pinned (page-locked, device-mapped) host buffer read
+// over the bus by the SMs, so that the copy engine stays free for the
+// setup's small transfers; 16-byte loads, four in flight per thread
+__global__ void __launch_bounds__(256) k_fetch_host(const double *src, double *dst,
+                                                    long long n) {
+  const long long n2 = n / 2;
+  const double2 *s2 = (const double2 *)src;
+  double2 *d2 = (double2 *)dst;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  for (; i + 3 * stride < n2; i += 4 * stride) {
+    const double2 a = s2[i], b = s2[i + stride], c = s2[i + 2 * stride], d = s2[i + 3 * stride];
+    d2[i] = a;
+    d2[i + stride] = b;
+    d2[i + 2 * stride] = c;
+    d2[i + 3 * stride] = d;
+  }
+  for (; i < n2; i += stride) d2[i] = s2[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0 && (n & 1)) dst[n - 1] = src[n - 1];
+}
+
 // zero the cross-resolution pixel matrices of the pixels the input mask drops
 __global__ void k_apply_inmask(double *cca, long long n, int ncc, const uint8_t *mask) {
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;

@@ -245,6 +245,13 @@ class Engine {
   bool cached_ = false;
   cudaStream_t st_ = nullptr;
   cudaEvent_t ev_[8];
+  // host-signal upload on a copy stream, overlapped with the pointing setup
+  // (bind_inputs); wait_tod() orders the engine stream after it
+  cudaStream_t cst_ = nullptr;
+  cudaEvent_t ev_ptr_ = nullptr, ev_tod_ = nullptr;
+  bool tod_pending_ = false;
+  void wait_tod();
+  void sync_tod();
 
   // sizes
   long ndet_ = 0, nsamp_ = 0, nnz_ = 0;

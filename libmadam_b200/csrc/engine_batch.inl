@@ -392,6 +392,7 @@ void Engine::run_cached_batch(long ndet, long nsamp, long nnz, double *timestamp
   fp32_next_ = false;
   d_pix_caller_ = is_device ? pix : nullptr;
   bind_inputs(timestamps, pix, pixweights, signals, is_device, false);
+  wait_tod();  // the realisations are copied on the engine stream below
   flag_and_compact(false);
   build_runs();
   if (par_.kfirst) build_csr();

@@ -33,14 +33,36 @@ Engine::Engine() {
   }
   g_alloc_stream = st_;
   for (auto &e : ev_) MADAM_CUDA(cudaEventCreate(&e));
+  MADAM_CUDA(cudaStreamCreateWithFlags(&cst_, cudaStreamNonBlocking));
+  MADAM_CUDA(cudaEventCreateWithFlags(&ev_ptr_, cudaEventDisableTiming));
+  MADAM_CUDA(cudaEventCreateWithFlags(&ev_tod_, cudaEventDisableTiming));
+}
+
+void Engine::wait_tod() {
+  if (!tod_pending_) return;
+  MADAM_CUDA(cudaStreamWaitEvent(st_, ev_tod_, 0));
+  tod_pending_ = false;
+}
+
+void Engine::sync_tod() {
+  // a call that fails before it reads the signal still waits for the copy
+  // from the caller's buffer
+  if (!tod_pending_) return;
+  cudaStreamSynchronize(cst_);
+  cudaStreamWaitEvent(st_, ev_tod_, 0);
+  tod_pending_ = false;
 }
 
 Engine::~Engine() {
   // members free their memory after this body: order those frees on the
   // legacy stream once the engine's streams are idle
+  if (cst_) cudaStreamSynchronize(cst_);
   cudaStreamSynchronize(st_);
   g_alloc_stream = nullptr;
   for (auto &e : ev_) cudaEventDestroy(e);
+  if (ev_ptr_) cudaEventDestroy(ev_ptr_);
+  if (ev_tod_) cudaEventDestroy(ev_tod_);
+  if (cst_) cudaStreamDestroy(cst_);
   if (st_) cudaStreamDestroy(st_);
 }
 
@@ -62,6 +84,7 @@ void Engine::bind_inputs(double *timestamps, int32_t *pix, float *pixweights, do
   (void)first_call;
   (void)timestamps;
   const long long n = (long long)ndet_ * nsamp_;
+  sync_tod();
   in_device_ = is_device;
   h_pix_ = is_device ? nullptr : pix;
   h_signal_ = is_device ? nullptr : signal;
@@ -106,9 +129,30 @@ void Engine::bind_inputs(double *timestamps, int32_t *pix, float *pixweights, do
                                cudaMemcpyHostToDevice, st_));
     d_w_ = wraw_.get();
     tod_own_.alloc(n);
-    MADAM_CUDA(cudaMemcpyAsync(tod_own_.get(), signal, n * sizeof(double),
-                               cudaMemcpyHostToDevice, st_));
     d_tod_ = tod_own_.get();
+    // the signal is first read by the binning: its upload follows the
+    // pointing's on the copy stream while the engine stream flags, compacts
+    // and sorts the pointing
+    if (n > 0) {
+      MADAM_CUDA(cudaEventRecord(ev_ptr_, st_));
+      MADAM_CUDA(cudaStreamWaitEvent(cst_, ev_ptr_, 0));
+      // a page-locked buffer is read by a kernel (the copy engine would
+      // queue the setup's small transfers behind this one), a pageable one
+      // goes through the copy engine
+      cudaPointerAttributes pa{};
+      const bool mapped = cudaPointerGetAttributes(&pa, signal) == cudaSuccess &&
+                          pa.type == cudaMemoryTypeHost && pa.devicePointer != nullptr &&
+                          ((uintptr_t)pa.devicePointer % 16) == 0;
+      cudaGetLastError();
+      if (mapped)
+        MADAM_LAUNCH(k_fetch_host, 148 * 2, 256, 0, cst_, (const double *)pa.devicePointer,
+                     tod_own_.get(), n);
+      else
+        MADAM_CUDA(cudaMemcpyAsync(tod_own_.get(), signal, n * sizeof(double),
+                                   cudaMemcpyHostToDevice, cst_));
+      MADAM_CUDA(cudaEventRecord(ev_tod_, cst_));
+      tod_pending_ = true;
+    }
   }
 }
 
@@ -839,6 +883,7 @@ bool Engine::build_pairs() {
 }
 
 void Engine::bin_tod(bool accumulate_wamap) {
+  wait_tod();
   // pixel_matrix + count_hits + bin_tod (smadam_routines.f90:111-422)
   const int ncc = nmap_ == 3 ? 6 : 1;
   const int T = 1 << tile_shift_;
@@ -2167,6 +2212,10 @@ void Engine::run(const Params &par, std::vector<Detector> dets, long ndet, long 
     setup_marks_[i] = now_ms() - t0;
   };
   bind_inputs(timestamps, pix, pixweights, signal, is_device, true);
+  struct TodGuard {
+    Engine &e;
+    ~TodGuard() { e.sync_tod(); }
+  } tod_guard{*this};
   mark(0);
   // pixel range check (smadam.F90:156-171)
   {
@@ -2265,6 +2314,10 @@ void Engine::run_cached(long ndet, long nsamp, long nnz, double *timestamps, int
   fp32_ = false;  // destripe_with_cache takes float64 signals
   fp32_next_ = false;
   bind_inputs(timestamps, pix, pixweights, signal, is_device, false);
+  struct TodGuard {
+    Engine &e;
+    ~TodGuard() { e.sync_tod(); }
+  } tod_guard{*this};
   flag_and_compact(false);
   build_runs();
   bin_tod(true);

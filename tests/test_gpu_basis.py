@@ -67,7 +67,7 @@ def run_both(W, d, pars):
     return ro, rp, do, dp
 
 
-def compare(ro, rp, nmap, nbasis):
+def compare(ro, rp, nmap, nbasis, iters=True):
     np.testing.assert_array_equal(rp["hits"], ro["hits"])
     np.testing.assert_array_equal(rp["mask"], ro["mask"])
     for name in ("binmap", "map"):
@@ -79,7 +79,8 @@ def compare(ro, rp, nmap, nbasis):
     assert rp["nna"].size == rp["aa"].size * nbasis
     _close(rp["nna"], ro["nna"], 1e-12)
     _close(rp["aa"], ro["aa"], MAP_RTOL)
-    assert abs(rp["noiter"] - ro["noiter"]) <= 1
+    if iters:
+        assert abs(rp["noiter"] - ro["noiter"]) <= 1
 
 
 @pytest.mark.parametrize("func,order", [("legendre", 1), ("legendre", 3), ("poly", 2),
@@ -92,7 +93,9 @@ def test_bases(W, func, order):
 def test_ring_scan_converged(W):
     d = syn.to_numpy(syn.generate(syn.small_config(seed=159)))
     ro, rp, _, _ = run_both(W, d, dict(basis_order=1, iter_max=3000, cglimit=1e-24))
-    compare(ro, rp, 3, 2)
+    # at this cglimit both solves run into the rounding floor, where the
+    # iteration count depends on the summation order
+    compare(ro, rp, 3, 2, iters=False)
 
 
 def test_drifts_on_random_pointing(W):
