@@ -702,10 +702,17 @@ __global__ void __launch_bounds__(256) k_gather_tiled(
   if (threadIdx.x == 0) part[blockIdx.x] = v[0];
 }
 
+// w . m with the pixel's (T, Q, U, pad) fetched by one 256-bit load (sm_100):
+// one L1 wavefront per lane instead of two for the random map lookups; the
+// padded copy is 32-byte aligned (k_ccmult_copy) and read-only here
 __device__ __forceinline__ double map_dot(const double2 *__restrict__ mg, long long cp,
                                           const float4 &q) {
-  const double2 a = __ldg(mg + 2 * cp), b = __ldg(mg + 2 * cp + 1);
-  return fma((double)q.z, b.x, fma((double)q.y, a.y, (double)q.x * a.x));
+  double t, qq, u, pad;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(t), "=d"(qq), "=d"(u), "=d"(pad)
+      : "l"(mg + 2 * cp));
+  (void)pad;
+  return fma((double)q.z, u, fma((double)q.y, qq, (double)q.x * t));
 }
 __device__ __forceinline__ double map_dot(const float4 *__restrict__ mf, long long cp,
                                           const float4 &q) {
