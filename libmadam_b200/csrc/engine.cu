@@ -625,6 +625,10 @@ __global__ void k_gather(const float4 *p4, const int32_t *pc, const uint32_t *bs
 // sample in shared memory and sums each baseline with one warp.  Used when
 // every baseline is at most kGatherTile / 2 samples long.
 constexpr int kGatherTile = 2048;
+// k_gather_chunks: resident CTAs per SM (its register budget) and a grid of
+// exactly one wave of them
+constexpr int kGatherChunkBlocksPerSM = 4;
+constexpr int kGatherChunkBlocks = 148 * kGatherChunkBlocksPerSM;
 constexpr int kGatherUnroll = 4;
 constexpr int kScatterUnroll = 8;
 
@@ -810,7 +814,7 @@ static_assert(kGatherChunk == 256, "chunk_baseline_sums takes 8 entries a lane")
 // MAPT (NMAP = 3): the map copy it reads, double2 (padded FP64, two 16-byte
 // loads in one sector) or float4 (FP32-TOD form, one load).
 template <int NMAP, class MAPT>
-__global__ void __launch_bounds__(256) k_gather_chunks(
+__global__ void __launch_bounds__(256, kGatherChunkBlocksPerSM) k_gather_chunks(
     const int2 *__restrict__ chunks, long long nchunks, const float4 *__restrict__ p4,
     const int32_t *__restrict__ pc, const uint32_t *__restrict__ bstart, long noba,
     long long nsamp, const double *__restrict__ bw, const double *__restrict__ p,

@@ -1785,17 +1785,17 @@ void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) 
                  ap, part_.get());
   } else if (ngather_chunks_ > 0) {
     if (nmap_ == 3 && fp32_)
-      MADAM_LAUNCH((k_gather_chunks<3, float4>), kRedBlocks, 256, 0, st_, gather_chunks_.get(),
+      MADAM_LAUNCH((k_gather_chunks<3, float4>), kGatherChunkBlocks, 256, 0, st_, gather_chunks_.get(),
                    ngather_chunks_, point4_.get(), pixc_.get(), bstart_d_.get(), noba_short_,
                    nsamp_, bw_.get(), p, nna_.get(), lmap_.get(), lmapf_.get(),
                    (int)ndeg_shift_, (int)nloc_, rmask_.get(), ap, part_.get());
     else if (nmap_ == 3)
-      MADAM_LAUNCH((k_gather_chunks<3, double2>), kRedBlocks, 256, 0, st_, gather_chunks_.get(),
+      MADAM_LAUNCH((k_gather_chunks<3, double2>), kGatherChunkBlocks, 256, 0, st_, gather_chunks_.get(),
                    ngather_chunks_, point4_.get(), pixc_.get(), bstart_d_.get(), noba_short_,
                    nsamp_, bw_.get(), p, nna_.get(), lmap_.get(), lmapg_.get(),
                    (int)ndeg_shift_, (int)nloc_, rmask_.get(), ap, part_.get());
     else
-      MADAM_LAUNCH((k_gather_chunks<1, double2>), kRedBlocks, 256, 0, st_, gather_chunks_.get(),
+      MADAM_LAUNCH((k_gather_chunks<1, double2>), kGatherChunkBlocks, 256, 0, st_, gather_chunks_.get(),
                    ngather_chunks_, point4_.get(), pixc_.get(), bstart_d_.get(), noba_short_,
                    nsamp_, bw_.get(), p, nna_.get(), lmap_.get(), (const double2 *)nullptr,
                    (int)ndeg_shift_, (int)nloc_, rmask_.get(), ap, part_.get());
@@ -1819,7 +1819,8 @@ void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) 
                  bstart_d_.get(), nb, noba_short_, nsamp_, bw_.get(), p, nna_.get(), lmap_.get(),
                  (int)ndeg_shift_, (int)nloc_, rmask_.get(), ap, part_.get());
   }
-  finish_dots(1, 1, 0, kRedBlocks, true);
+  finish_dots(1, 1, 0, (!use_pairs_ && ngather_chunks_ > 0) ? kGatherChunkBlocks : kRedBlocks,
+              true);
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[4], st_));
 }
 
