@@ -145,7 +145,9 @@ void Engine::bind_inputs(double *timestamps, int32_t *pix, float *pixweights, do
                           ((uintptr_t)pa.devicePointer % 16) == 0;
       cudaGetLastError();
       if (mapped)
-        MADAM_LAUNCH(k_fetch_host, 148 * 2, 256, 0, cst_, (const double *)pa.devicePointer,
+        // one small CTA per SM: the bus, not the SMs, limits it, and the
+        // setup kernels beside it keep their warp slots
+        MADAM_LAUNCH(k_fetch_host, 148, 128, 0, cst_, (const double *)pa.devicePointer,
                      tod_own_.get(), n);
       else
         MADAM_CUDA(cudaMemcpyAsync(tod_own_.get(), signal, n * sizeof(double),
