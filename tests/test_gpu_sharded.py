@@ -90,3 +90,29 @@ def test_two_ranks_by_detector_on_one_gpu(W):
 
 def test_two_ranks_by_time_with_subsets_on_one_gpu(W):
     SU.run_ranks(_rank, 2, (True,))
+
+
+def _covmat_rank(rank, world, root):
+    import torch
+    from libmadam_b200 import libmadam_wrapper as W
+    from libmadam_b200.comm import HostComm
+    from test_oracle_covmat import _data, read_covmat
+    torch.cuda.set_device(0)
+    d = _data(174)
+    N = 12 * d["pars"]["nside_map"] ** 2 * 3
+    full = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
+    W.destripe(None, *_args(dict(d["pars"], file_covmat="{}_full{}".format(root, rank)), full))
+    mine = SU.shard_time(d, rank, world)
+    comm = HostComm()
+    W.destripe(comm, *_args(dict(d["pars"], file_covmat=root + "_shard"), mine))
+    if rank == 0:
+        for det in d["dets"]:
+            a = read_covmat(root + "_shard", det, N)
+            b = read_covmat("{}_full{}".format(root, rank), det, N)
+            _close(a, b, 1e-11)
+
+
+def test_two_host_ranks_covmat(W, tmp_path):
+    # the ranks' covariance matrices are summed on the device arrays and
+    # rank 0 writes the files
+    SU.run_ranks(_covmat_rank, 2, (str(tmp_path / "ncm"),))

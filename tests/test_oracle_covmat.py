@@ -165,3 +165,28 @@ def test_existing_file_is_skipped_and_map_is_binned(tmp_path):
     # write_covmat replaces the solve: no baselines, the map is the binned map
     assert np.all(O.result("aa") == 0)
     np.testing.assert_array_equal(O.result("map"), O.result("binmap"))
+
+
+def _covmat_rank(rank, world, root):
+    import oracle_api as O
+    import shard_util as SU
+    d = _data(163)
+    N = 12 * d["pars"]["nside_map"] ** 2 * 3
+    O.set_comm(0, 1, None)
+    run_oracle_covmat(d, "{}_full{}".format(root, rank))
+    mine = SU.shard_time(d, rank, world)
+    O.set_comm(rank, world, SU.gloo_allreduce)
+    run_oracle_covmat(mine, root + "_shard")
+    O.set_comm(0, 1, None)
+    if rank == 0:
+        for det in d["dets"]:
+            a = read_covmat(root + "_shard", det, N)
+            b = read_covmat("{}_full{}".format(root, rank), det, N)
+            assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+
+
+def test_ranks_sum_their_matrices(tmp_path):
+    # each rank holds one pointing period of every detector; save_matrix
+    # adds the ranks' matrices (covmat.F90:282-318) and rank 0 writes
+    import shard_util as SU
+    SU.run_ranks(_covmat_rank, 2, (str(tmp_path / "ncm"),))
