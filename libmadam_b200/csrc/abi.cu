@@ -141,11 +141,17 @@ static int destripe_impl(bool fp32, int comm, char *parstring, long ndet, char *
 
 int madam_b200_destripe_with_cache(int comm, long ndet, long nsamp, long nnz, void *timestamps,
                                    void *pix, void *pixweights, void *signal, char *outpath) {
-  (void)outpath;  // output files are not written by this library
   std::lock_guard<std::mutex> lock(g_mutex);
   return guarded([&] {
     if (!g_engine || !g_engine->cached())
       madam::fail("destripe_with_cache called with empty caches.");
+    // a non-empty outpath replaces path_output for this and later calls
+    // (smadam.F90:644-656)
+    if (outpath && outpath[0]) {
+      std::string s(outpath);
+      const size_t a = s.find_first_not_of(' '), b = s.find_last_not_of(' ');
+      g_engine->set_output_path(a == std::string::npos ? std::string() : s.substr(a, b - a + 1));
+    }
     g_engine->set_comm(madam::comm_lookup(comm));
     const bool dev = is_device_pointer(pix);
     g_engine->run_cached(ndet, nsamp, nnz, (double *)timestamps, (int32_t *)pix,

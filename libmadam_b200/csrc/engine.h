@@ -109,6 +109,8 @@ class Engine {
            long nnz, double *timestamps, int32_t *pix, float *pixweights,
            double *signal, long nperiod, const long *periods, bool is_device);
   // destripe_with_cache(): new TOD, cached pixel matrices / filter / preconditioner
+  // path_output of the cached parameters (destripe_with_cache's outpath)
+  void set_output_path(const std::string &path) { par_.path_output = path; }
   void run_cached(long ndet, long nsamp, long nnz, double *timestamps,
                   int32_t *pix, float *pixweights, double *signal,
                   bool is_device);

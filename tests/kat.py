@@ -95,8 +95,11 @@ def run_libmadam_kat(backend, check_files=False):
     return out
 
 
-def run_mc_kat(backend):
-    """mcmode cache sequence of test_libmadam_mc.py:133-208."""
+def run_mc_kat(backend, check_files=False):
+    """mcmode cache sequence of test_libmadam_mc.py:133-208; the cached call
+    gets an output path as the reference test gives it one
+    (test_libmadam_mc.py:173-185), and with check_files its map file is read
+    back from there."""
     g = load("kat_libmadam_mc.npz")
     pars = libmadam_pars(8, 8, 8)
     pars["nsubchunk"] = 1
@@ -115,9 +118,18 @@ def run_mc_kat(backend):
     pars["mcmode"] = True
     backend.destripe(*args(g["signal2"].copy()))
     map2 = backend.result("map")
+    outpath = tempfile.mkdtemp(prefix="madam_kat_mc_") + "/"
     backend.destripe_with_cache(g["timestamps"].copy(), g["pixels"].copy(),
-                                g["pixweights"].copy(), g["signal"].copy(), 4)
+                                g["pixweights"].copy(), g["signal"].copy(), 4,
+                                outpath.encode("ascii"))
     map3 = backend.result("map")
+    if check_files:
+        from fits_reader import read_table
+        mh, mc = read_table(os.path.join(outpath, "madam_pytest_map.fits"))
+        assert mh["OBJTYPE"] == "madam.map"
+        good = g["hmap"] > 0
+        np.testing.assert_allclose(mc["TEMPERATURE"][good], map3[good].astype(np.float32),
+                                   rtol=1e-6)
     backend.clear_caches()
     backend.clear_caches()
     return map1, map2, map3

@@ -12,8 +12,8 @@ class ProductBackend:
                    npsd, psdstarts, psdfreqs, psdvals)
 
     @staticmethod
-    def destripe_with_cache(timestamps, pixels, pixweights, signal, ndet):
-        W.destripe_with_cache(None, timestamps, pixels, pixweights, signal, b"")
+    def destripe_with_cache(timestamps, pixels, pixweights, signal, ndet, outpath=b""):
+        W.destripe_with_cache(None, timestamps, pixels, pixweights, signal, outpath)
 
     @staticmethod
     def clear_caches():

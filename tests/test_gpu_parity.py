@@ -87,7 +87,7 @@ def test_reference_kat_hits_and_binned_map(W):
 def test_reference_kat_mc_sequence(W):
     from product_api import ProductBackend
     from test_oracle_kat import OracleBackend
-    mp = kat.run_mc_kat(ProductBackend())
+    mp = kat.run_mc_kat(ProductBackend(), check_files=True)
     mo = kat.run_mc_kat(OracleBackend())
     for a, b in zip(mp, mo):
         _close(a, b, MAP_RTOL)

@@ -10,7 +10,7 @@ class OracleBackend:
     clear_caches = staticmethod(O.clear_caches)
 
     @staticmethod
-    def destripe_with_cache(timestamps, pixels, pixweights, signal, ndet):
+    def destripe_with_cache(timestamps, pixels, pixweights, signal, ndet, outpath=b""):
         O.destripe_with_cache(timestamps, pixels, pixweights, signal, ndet)
 
     @staticmethod
