@@ -5,6 +5,7 @@ changes nothing, a mask that drops pixels zeroes their matrices and changes
 the destriped map, and a mask at another resolution is up- or downgraded
 to nside_cross."""
 import numpy as np
+import pytest
 
 import oracle_api as O
 from fits_reader import write_mask
@@ -56,3 +57,12 @@ def test_mask_zeroes_cross_matrices_and_up_downgrades(tmp_path):
     down = _run(d, dict(pars, file_inmask=f32))
     keep16 = m32.reshape(-1, 4).min(axis=1)
     np.testing.assert_array_equal(down["cca"].reshape(-1, 9)[keep16 == 0], 0)
+
+
+def test_ring_ordering_is_refused(tmp_path):
+    # read_inmask accepts NESTED masks only (read_data.f90:90-190)
+    d = syn.to_numpy(syn.generate(syn.small_config(seed=123)))
+    f = str(tmp_path / "ring.fits")
+    write_mask(f, np.ones(12 * 16 ** 2), 16, ordering="RING")
+    with pytest.raises(O.OracleError, match="NESTED"):
+        _run(d, dict(d["pars"], file_inmask=f))
