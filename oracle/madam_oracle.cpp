@@ -3258,6 +3258,10 @@ long oracle_result_size(const char *name) {
   if (n == "yba") return (long)S.yba.size();
   if (n == "nna") return (long)(S.nbasis > 1 ? S.nnab.size() : S.nna.size());
   if (n == "fcov") return (long)S.fcov.size();
+  if (n.rfind("basis_table:", 0) == 0) {
+    // the basis functions of one baseline length (a test hook)
+    return S.nbasis * std::stol(n.substr(12));
+  }
   if (n == "sigmas") {
     long m = 0;
     for (const auto &d : S.dets) m += (long)d.sigmas.size();
@@ -3292,6 +3296,7 @@ int oracle_result_copy(const char *name, void *dst) {
   if (n == "yba") return cp(S.yba);
   if (n == "nna") return S.nbasis > 1 ? cp(S.nnab) : cp(S.nna);
   if (n == "fcov") return cp(S.fcov);
+  if (n.rfind("basis_table:", 0) == 0) return cp(basis_table(S, std::stol(n.substr(12))));
   if (n == "sigmas") {
     std::vector<double> v;
     for (const auto &d : S.dets) v.insert(v.end(), d.sigmas.begin(), d.sigmas.end());

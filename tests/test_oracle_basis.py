@@ -142,3 +142,37 @@ def test_filter_refused_with_higher_orders():
     d = syn.to_numpy(syn.generate(syn.small_config(seed=145)))
     with pytest.raises(O.OracleError, match="Filter only implemented"):
         _run(d, dict(d["pars"], kfilter=True, basis_order=1))
+
+
+def _numpy_basis(func, order, n):
+    """start_timeloop's tables (parameter_control.f90:865-933) from numpy's
+    own polynomials: r at sample centres, dr = 2. / nsamp in single
+    precision as the reference divides"""
+    dr = float(np.float32(2.0) / np.float32(n))
+    r = (0.5 * dr - 1) + np.arange(n) * dr
+    out = np.zeros((n, order + 1))
+    for o in range(order + 1):
+        e = np.zeros(o + 1)
+        e[o] = 1
+        if func == "poly":
+            out[:, o] = r ** o
+        elif func == "legendre":
+            out[:, o] = np.polynomial.legendre.legval(r, e)
+        elif func == "chebyshev":
+            # second kind, normalised by (1 - r^2)^(1/4)
+            th = np.arccos(r)
+            out[:, o] = np.sin((o + 1) * th) / np.sin(th) * (1 - r * r) ** 0.25
+        else:
+            x = np.arange(n) * np.pi / n
+            out[:, o] = np.cos(o * x) if o % 2 == 0 else np.sin((o + 1) * x)
+    return out
+
+
+@pytest.mark.parametrize("func", ["legendre", "poly", "chebyshev", "fourier"])
+def test_basis_tables_match_numpy(func):
+    d = syn.to_numpy(syn.generate(syn.small_config(seed=146)))
+    order = 5
+    _run(d, dict(d["pars"], kfilter=False, basis_order=order, basis_func=func))
+    for n in (10, 7, 50, 4096):
+        t = O.result("basis_table:%d" % n).reshape(n, order + 1)
+        np.testing.assert_allclose(t, _numpy_basis(func, order, n), rtol=1e-12, atol=1e-12)
