@@ -14,8 +14,13 @@
  * psdvals float64[npsdval].  Host or CUDA device pointers are accepted.
  * pix is rewritten in place (flagged samples become 12*nside_max^2) and
  * signal is destriped in place when write_tod or subsets are set, as in the
- * reference.  `comm` is a Fortran MPI handle in the reference; this library
- * runs one rank and ignores it.  On an error the reference aborts the MPI job;
+ * reference.  `comm` is a Fortran MPI handle in the reference; here it is 0
+ * (one rank) or a handle of madam_b200_comm_init_nccl / _host (madam_b200.h),
+ * whose ranks each pass their own share of the data and get the whole maps,
+ * as the reference's MPI ranks do.  Any other value runs one rank: an MPI
+ * handle has no meaning to this library (library handles start at
+ * 0x2D420001, away from Open MPI's and MPICH's Fortran handle values), so a
+ * job of several MPI ranks must pass library communicators.  On an error the reference aborts the MPI job;
  * these void entry points print the message and return; the status is
  * available from madam_b200_last_error (madam_b200.h).
  */

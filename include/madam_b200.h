@@ -179,14 +179,22 @@ int madam_b200_selftest_fastdiv(void);
  * All arrays are device memory owned by the caller: detweights [ndet],
  * pix int64 [ndet][nsamp] (NESTED at nside; negative = flagged, skipped),
  * pixweights float64 [ndet][nsamp][nnz], hits int32 [12 nside^2], cc
- * float64 [12 nside^2][nnz][nnz] (zero where the rcond cut of pixmode /
- * pixlim rejects the pixel).  Work is queued on `stream` (NULL = legacy
+ * float64 [12 nside^2][nnz][nnz].  Every array must be device memory of the
+ * current device (or managed memory).  A pixel matrix is rejected, and its
+ * cc entries zeroed, by the reference's invert_pixelmatrix_map test with
+ * allow_decoupling = F and incomplete_matrices = F (fixed; the reference
+ * defaults): pixmode 0 rejects det(C) < pixlim, pixmode 1 rejects
+ * det(C) (3 / trace C)^3 < pixlim, pixmode 2 rejects rcond (smallest over
+ * largest eigenvalue) < pixlim.  Work is queued on `stream` (NULL = legacy
  * default stream) and is complete once that stream is synchronised.
  * Limits: nside <= 64 (the accumulators are a fixed 2.75 MB device array of
  * 49152 pixels; larger maps return status 1 and say so); nnz 1 or 3.  The
- * first call on a device looks up that array's address (make it before
- * any stream capture).  Calls that overlap on one device share the array
- * and race.  Returns 0, 1 (invalid argument) or 2 (CUDA error); the message
+ * first call on a device looks up that array's address and loads the code of
+ * all this entry point's kernels (for every nnz), so make it before any
+ * stream capture; later calls load and allocate nothing.  Calls that overlap
+ * on one device share the array and race.  A CUDA error already pending when
+ * the call starts is reported as status 2 and left pending; no work is
+ * queued.  Returns 0, 1 (invalid argument) or 2 (CUDA error); the message
  * goes to err (errlen bytes, may be NULL). */
 int madam_b200_pixel_matrices_noalloc(long nside, long nnz, long ndet, long nsamp,
                                       const double *detweights, const long long *pix,

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <initializer_list>
 #include <mutex>
 #include <string>
 
@@ -23,6 +24,43 @@
 
 using madam::Engine;
 
+namespace madam {
+
+// Where the caller's buffers live: true for device memory that the kernels of
+// device `dev` (< 0: the current device) read directly (its own memory, or
+// managed memory), false for host memory (pageable or page-locked), which is copied in.  Device
+// memory of another GPU, or a mix of host and device buffers, is refused:
+// the kernels would read a device buffer in place, and a host buffer taken
+// for a device one would be read through an address the GPU cannot use.
+bool inputs_on_device(int dev, std::initializer_list<const void *> ptrs) {
+  if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    fail("no CUDA device");
+  }
+  int kind = -1;
+  for (const void *p : ptrs) {
+    if (!p) continue;
+    int k = 0;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+      cudaGetLastError();
+    } else if (a.type == cudaMemoryTypeManaged) {
+      k = 1;
+    } else if (a.type == cudaMemoryTypeDevice) {
+      if (a.device != dev)
+        fail("device buffers must be memory of the CUDA device that runs the solve");
+      k = 1;
+    }
+    if (kind >= 0 && k != kind)
+      fail("timestamps, pixels, weights and signal must all be host memory or all "
+           "device memory");
+    kind = k;
+  }
+  return kind == 1;
+}
+
+}  // namespace madam
+
 namespace {
 
 std::mutex g_mutex;
@@ -30,15 +68,6 @@ std::unique_ptr<Engine> g_engine;
 std::string g_last_error;
 int g_last_status = 0;
 
-bool is_device_pointer(const void *p) {
-  if (!p) return false;
-  cudaPointerAttributes a;
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
 
 template <typename F>
 int guarded(F &&f) {
@@ -109,9 +138,7 @@ static int destripe_impl(bool fp32, int comm, char *parstring, long ndet, char *
     if (ndet <= 0 || nsamp <= 0 || nnz <= 0) madam::fail("empty data");
     auto dets = madam::read_detectors(par, detstring, ndet, detweights, npsd, npsdtot, psdstarts,
                                       npsdbin, psdfreqs, npsdval, psdvals);
-    const bool dev = is_device_pointer(pix);
-    if (fp32 && dev != is_device_pointer(signal))
-      madam::fail("destripe_fp32: pixels and signal must both be host or both device memory");
+    const bool dev = madam::inputs_on_device(-1, {timestamps, pix, pixweights, signal});
     Engine &e = engine();
     e.clear_subchunk_results();
     // comm: a communicator of madam_b200_comm_init_* (a sharded run), else a
@@ -153,7 +180,7 @@ int madam_b200_destripe_with_cache(int comm, long ndet, long nsamp, long nnz, vo
       g_engine->set_output_path(a == std::string::npos ? std::string() : s.substr(a, b - a + 1));
     }
     g_engine->set_comm(madam::comm_lookup(comm));
-    const bool dev = is_device_pointer(pix);
+    const bool dev = madam::inputs_on_device(-1, {timestamps, pix, pixweights, signal});
     g_engine->run_cached(ndet, nsamp, nnz, (double *)timestamps, (int32_t *)pix,
                          (float *)pixweights, (double *)signal, dev);
   });
@@ -167,9 +194,7 @@ int madam_b200_destripe_with_cache_batch(int comm, long ndet, long nsamp, long n
   return guarded([&] {
     if (!g_engine || !g_engine->cached())
       madam::fail("destripe_with_cache called with empty caches.");
-    const bool dev = is_device_pointer(pix);
-    if (dev != is_device_pointer(signals))
-      madam::fail("pointing and signals must both be host or both be device memory");
+    const bool dev = madam::inputs_on_device(-1, {timestamps, pix, pixweights, signals});
     g_engine->run_cached_batch(ndet, nsamp, nnz, (double *)timestamps, (int32_t *)pix,
                                (float *)pixweights, nrhs, (double *)signals, dev);
   });
@@ -183,9 +208,7 @@ int madam_b200_destripe_with_cache_batch_fp32(int comm, long ndet, long nsamp, l
   return guarded([&] {
     if (!g_engine || !g_engine->cached())
       madam::fail("destripe_with_cache called with empty caches.");
-    const bool dev = is_device_pointer(pix);
-    if (dev != is_device_pointer(signals))
-      madam::fail("pointing and signals must both be host or both be device memory");
+    const bool dev = madam::inputs_on_device(-1, {timestamps, pix, pixweights, signals});
     g_engine->run_cached_batch(ndet, nsamp, nnz, (double *)timestamps, (int32_t *)pix,
                                (float *)pixweights, nrhs, (double *)signals, dev, true);
   });

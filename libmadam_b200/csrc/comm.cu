@@ -116,7 +116,13 @@ class HostComm : public Comm {
 
 std::mutex g_comm_mu;
 std::map<int, std::unique_ptr<Comm>> g_comms;
-int g_next_handle = 1;
+// Library handles start far from the values MPI libraries give Fortran
+// communicator handles (Open MPI: small table indices, MPI_COMM_WORLD = 0,
+// MPI_COMM_SELF = 1; MPICH: bit patterns 0x44000000 and up for the built-in
+// communicators, negative as int for created ones), so an MPI handle passed
+// as `comm` is never taken for one of this library's communicators.
+constexpr int kFirstHandle = 0x2D420001;
+int g_next_handle = kFirstHandle;
 std::string g_comm_err;
 
 int add(Comm *c) {

@@ -10,6 +10,7 @@
 
 #include <cstdint>
 #include <future>
+#include <initializer_list>
 #include <map>
 #include <memory>
 #include <string>
@@ -33,6 +34,11 @@ constexpr int kMaxBasis = 8;          // basis_order + 1 at most
 // blocks for reuse (one destripe call allocates and frees several GB of
 // temporaries; the pool turns the repeats into bookkeeping).
 extern thread_local cudaStream_t g_alloc_stream;
+
+// True when every non-null buffer is device memory of device `dev` (< 0: the
+// current one) or managed memory, false when all are host memory; throws on a
+// mix, or on device memory of another GPU.
+bool inputs_on_device(int dev, std::initializer_list<const void *> ptrs);
 void *dev_alloc(size_t bytes);
 void dev_free(void *p);
 

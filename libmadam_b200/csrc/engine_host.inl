@@ -139,11 +139,22 @@ void Engine::bind_inputs(double *timestamps, int32_t *pix, float *pixweights, do
       // a page-locked buffer is read by a kernel (the copy engine would
       // queue the setup's small transfers behind this one), a pageable one
       // goes through the copy engine
-      cudaPointerAttributes pa{};
-      const bool mapped = cudaPointerGetAttributes(&pa, signal) == cudaSuccess &&
-                          pa.type == cudaMemoryTypeHost && pa.devicePointer != nullptr &&
-                          ((uintptr_t)pa.devicePointer % 16) == 0;
+      // the kernel reads all n values through the device alias, so the
+      // last one must lie in the same page-locked, mapped range (a buffer
+      // registered only in part goes through the copy engine instead)
+      cudaPointerAttributes pa{}, pz{};
+      bool mapped = cudaPointerGetAttributes(&pa, signal) == cudaSuccess &&
+                    pa.type == cudaMemoryTypeHost && pa.devicePointer != nullptr &&
+                    ((uintptr_t)pa.devicePointer % 16) == 0;
       cudaGetLastError();
+      if (mapped) {
+        const double *last = (const double *)signal + (n - 1);
+        mapped = cudaPointerGetAttributes(&pz, last) == cudaSuccess &&
+                 pz.type == cudaMemoryTypeHost && pz.devicePointer != nullptr &&
+                 (const char *)pz.devicePointer ==
+                     (const char *)pa.devicePointer + (n - 1) * sizeof(double);
+        cudaGetLastError();
+      }
       if (mapped)
         // one small CTA per SM: the bus, not the SMs, limits it, and the
         // setup kernels beside it keep their warp slots

@@ -1,4 +1,5 @@
-// Device kernels of the destriping engine (definitions in kernels.cu).
+// Types shared by the device code of the engine (engine.cu and the .inl
+// files it includes) and the no-allocation entry point (noalloc.cu).
 #pragma once
 
 #include <cuda_runtime.h>

@@ -15,8 +15,9 @@
 // six upper-triangle entries of the 3 x 3 matrix, or one entry for
 // nnz = 1, and the hit count): 2.75 MB.  Its address is looked up once per
 // device, with that device current, by cudaGetSymbolAddress on the first
-// call made on that device (which is why the first call should come before
-// any stream capture).  Every call clears the npix x 7 entries it uses
+// call made on that device, which also loads the code of all the kernels
+// below (cudaFuncGetAttributes); that first call should therefore come
+// before any stream capture.  Later calls load and allocate nothing.  Every call clears the npix x 7 entries it uses
 // before accumulating, so nothing needs to be zero beforehand.  There is one
 // scratch array per device: calls that overlap on one device (two streams,
 // two threads) race on it and give wrong results.
@@ -79,7 +80,12 @@ __global__ void k_na_accum(const long long *pix, const double *pw, const double 
   }
 }
 
-// Inversion with the rcond cut and expansion to full nnz x nnz matrices.
+// Inversion and expansion to full nnz x nnz matrices.  Rejection as in
+// invert_pixelmatrix_map with allow_decoupling = F and incomplete_matrices = F
+// (the reference defaults): pixmode 0 rejects det(C) < pixlim, pixmode 1
+// det(C) (3 / trace C)^3 < pixlim, pixmode 2 rcond (smallest over largest
+// eigenvalue) < pixlim; a rejected or empty pixel gets a zero matrix.
+// nnz = 1: 1 / sum(detw), zero for an empty pixel.
 template <int NNZ>
 __global__ void k_na_invert(const double *s, long long npix, int pixmode, double pixlim,
                             int *hits, double *cc) {
@@ -107,13 +113,33 @@ int set_err(char *err, long errlen, int status, const char *msg) {
   return status;
 }
 
-bool on_device(const void *p) {
+// True when the kernels of this call, running on device `dev`, can read `p`:
+// managed memory, or device memory of `dev` itself.  Device memory of another
+// GPU is refused even when peer access happens to be enabled, so a call never
+// depends on a peer mapping it did not set up.
+bool on_device(const void *p, int dev) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
+}
+
+// Loads the code of every kernel this file launches (lazy module loading
+// would otherwise do it at the first launch of each), so that after the
+// first call on a device no later call loads anything.
+cudaError_t resolve_kernels() {
+  cudaFuncAttributes fa;
+  const void *fns[] = {(const void *)k_na_clear, (const void *)k_na_accum<1>,
+                       (const void *)k_na_accum<3>, (const void *)k_na_invert<1>,
+                       (const void *)k_na_invert<3>};
+  for (const void *f : fns) {
+    cudaError_t e = cudaFuncGetAttributes(&fa, f);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace
@@ -139,20 +165,31 @@ extern "C" int madam_b200_pixel_matrices_noalloc(long nside, long nnz, long ndet
   if (nnz != 1 && nnz != 3) return set_err(err, errlen, 1, "nnz must be 1 or 3");
   if (ndet < 1 || nsamp < 0) return set_err(err, errlen, 1, "ndet must be >= 1 and nsamp >= 0");
   if (pixmode < 0 || pixmode > 2) return set_err(err, errlen, 1, "pixmode must be 0, 1 or 2");
-  const long long ntot = (long long)ndet * nsamp;
-  if (!on_device(detweights) || !on_device(hits) || !on_device(cc) ||
-      (ntot > 0 && (!on_device(pix) || !on_device(pixweights))))
-    return set_err(err, errlen, 1, "all arrays must be in device memory");
+  // an error left pending by earlier work is the caller's, not this call's:
+  // report it without clearing it and launch nothing
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess) {
+    char m[200];
+    std::snprintf(m, sizeof m, "a CUDA error was pending before the call: %s",
+                  cudaGetErrorString(e));
+    return set_err(err, errlen, 2, m);
+  }
   int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return set_err(err, errlen, 2, cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return set_err(err, errlen, 1, "device index out of range");
+  const long long ntot = (long long)ndet * nsamp;
+  if (!on_device(detweights, dev) || !on_device(hits, dev) || !on_device(cc, dev) ||
+      (ntot > 0 && (!on_device(pix, dev) || !on_device(pixweights, dev))))
+    return set_err(err, errlen, 1,
+                   "all arrays must be in device memory of the current device");
   double *s = g_scratch_ptr[dev].load(std::memory_order_acquire);
   if (!s) {
     std::lock_guard<std::mutex> lk(g_setup_mutex);
     s = g_scratch_ptr[dev].load(std::memory_order_acquire);
     if (!s) {
       e = cudaGetSymbolAddress((void **)&s, g_pixmat_scratch);
+      if (e == cudaSuccess && s) e = resolve_kernels();
       if (e != cudaSuccess || !s) {
         cudaGetLastError();
         return set_err(err, errlen, 2, e != cudaSuccess ? cudaGetErrorString(e)
@@ -163,18 +200,23 @@ extern "C" int madam_b200_pixel_matrices_noalloc(long nside, long nnz, long ndet
   }
   cudaStream_t st = (cudaStream_t)stream;
   const unsigned grid = 148 * 8;
+  // each launch is checked on its own, so a status belongs to this call
   k_na_clear<<<grid, 256, 0, st>>>(s, npix * kScratchStride);
+  if ((e = cudaGetLastError()) != cudaSuccess)
+    return set_err(err, errlen, 2, cudaGetErrorString(e));
   if (ntot > 0) {
     if (nnz == 3)
       k_na_accum<3><<<grid, 256, 0, st>>>(pix, pixweights, detweights, nsamp, ntot, npix, s);
     else
       k_na_accum<1><<<grid, 256, 0, st>>>(pix, pixweights, detweights, nsamp, ntot, npix, s);
+    if ((e = cudaGetLastError()) != cudaSuccess)
+      return set_err(err, errlen, 2, cudaGetErrorString(e));
   }
   if (nnz == 3)
     k_na_invert<3><<<grid, 128, 0, st>>>(s, npix, (int)pixmode, pixlim, hits, cc);
   else
     k_na_invert<1><<<grid, 128, 0, st>>>(s, npix, (int)pixmode, pixlim, hits, cc);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return set_err(err, errlen, 2, cudaGetErrorString(e));
+  if ((e = cudaGetLastError()) != cudaSuccess)
+    return set_err(err, errlen, 2, cudaGetErrorString(e));
   return 0;
 }

@@ -42,16 +42,6 @@ double wall_s() {
   return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
-bool device_ptr(const void *p) {
-  if (!p) return false;
-  cudaPointerAttributes a;
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
-
 struct Job {
   long id = 0;
   Params par;
@@ -85,6 +75,7 @@ size_t job_bytes(const Job &j) {
 
 class Server {
  public:
+  int device() const { return device_; }
   Server(int nworkers, double frac) {
     MADAM_CUDA(cudaGetDevice(&device_));
     size_t fr = 0, tot = 0;
@@ -283,9 +274,7 @@ static long serve_submit(bool fp32, void *srv, char *parstring, long ndet, char 
     j->w = (float *)pixweights;
     j->sig = (double *)signal;
     j->periods.assign(periods, periods + nperiod);
-    j->dev = madam::device_ptr(pix);
-    if (j->dev != madam::device_ptr(signal))
-      madam::fail("pixels and signal must both be host or both device memory");
+    j->dev = madam::inputs_on_device(s->device(), {timestamps, pix, pixweights, signal});
     j->fp32 = fp32;
     j->bytes = madam::job_bytes(*j);
     return s->submit(std::move(j));

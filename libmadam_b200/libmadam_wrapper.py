@@ -55,9 +55,31 @@ def dets2detstring(dets):
 
 
 def _fcomm(comm):
+    """The C-ABI `comm` handle.  None, and any communicator of one rank, run
+    one rank (0); a libmadam_b200.comm communicator passes its handle, and an
+    int is taken as such a handle.  Any other communicator of several ranks
+    (an mpi4py communicator, as the reference wrapper takes) is refused: its
+    ranks' reductions would not happen here, so each rank would solve its own
+    share of the data alone and write the same file names."""
     if comm is None:
         return 0
-    return int(comm.py2f()) if hasattr(comm, "py2f") else int(comm)
+    from .comm import _Comm
+    if isinstance(comm, _Comm):
+        return int(comm.py2f())
+    if isinstance(comm, (int, np.integer)):
+        return int(comm)
+    size = None
+    get_size = getattr(comm, "Get_size", None)
+    if callable(get_size):
+        size = int(get_size())
+    elif hasattr(comm, "size"):
+        size = int(comm.size)
+    if size is not None and size > 1:
+        raise ValueError(
+            "libmadam_b200: a communicator of {} ranks was passed; sharded runs take a "
+            "libmadam_b200.comm.NcclComm or HostComm (this library does not reduce over "
+            "MPI)".format(size))
+    return 0
 
 
 class _Buf:

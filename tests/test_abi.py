@@ -102,3 +102,39 @@ def test_no_cpu_fallback_without_gpu():
         W.destripe(None, d["pars"], d["dets"], d["detweights"], d["timestamps"], d["pixels"],
                    d["pixweights"], d["signal"], d["periods"], d["npsd"], d["psdstarts"],
                    d["psdfreqs"], d["psdvals"])
+
+
+class _FakeMpiComm:
+    """Stands in for an mpi4py communicator (Get_size, py2f)."""
+
+    def __init__(self, size, handle):
+        self._size, self._handle = size, handle
+
+    def Get_size(self):
+        return self._size
+
+    def py2f(self):
+        return self._handle
+
+
+def test_multi_rank_mpi_communicator_is_refused():
+    # the reference reduces over its MPI communicator (smadam.F90:115-117);
+    # this library does not, so N MPI ranks must not become N one-rank solves
+    from libmadam_b200 import libmadam_wrapper as W
+    with pytest.raises(ValueError, match="communicator of 2 ranks"):
+        W._fcomm(_FakeMpiComm(2, 0))
+    with pytest.raises(ValueError, match="communicator of 2 ranks"):
+        W.destripe(_FakeMpiComm(2, 0), {}, ["a"], np.ones(1), np.zeros(4),
+                   np.zeros(4, np.int32), np.ones(4, np.float32), np.zeros(4), np.array([0]),
+                   np.ones(1, np.int64), np.zeros(1), np.array([1.0, 2.0]), np.ones(2))
+    # one rank (MPI_COMM_SELF is Fortran handle 1 in Open MPI) runs one rank,
+    # whatever its handle
+    assert W._fcomm(_FakeMpiComm(1, 1)) == 0
+    assert W._fcomm(None) == 0
+
+
+def test_library_handles_avoid_mpi_fortran_handles():
+    src = open(os.path.join(ROOT, "libmadam_b200", "csrc", "comm.cu")).read()
+    first = int(re.search(r"kFirstHandle = (0x[0-9A-Fa-f]+)", src).group(1), 16)
+    # Open MPI: small indices; MPICH built-ins 0x44000000.., created ones negative
+    assert 1 << 16 < first < 0x44000000 - (1 << 20)
