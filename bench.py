@@ -138,14 +138,23 @@ def cpu_sample_config(cfg):
     return s
 
 
-def run_cpu(cfg):
-    """Time the CPU restatement on the bounded sample: samples/s per PCG iteration."""
+def run_cpu(cfg, full=False, parity_fp32=None):
+    """Time the CPU restatement: samples/s per PCG iteration, on the bounded
+    sample (cpu_sample_config) or, with full=True, on the whole workload.
+    With parity_fp32 set (False: destripe, True: destripe_fp32 on the float32
+    signal), the GPU library then solves the same inputs and the result
+    carries a "parity" block: hits and masks equal, per-pixel errors of the
+    destriped map and baselines against the oracle (tests/parity.py), PCG
+    iteration counts."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_api as O
     from libmadam_b200 import synthetic as syn
-    s = cpu_sample_config(cfg)
+    s = cfg if full else cpu_sample_config(cfg)
     dev = "cuda" if _has_cuda() else "cpu"
     d = syn.to_numpy(syn.generate(s, device=dev))
+    keep = None
+    if parity_fp32 is not None:
+        keep = {k: d[k].copy() for k in ("pixels", "signal")}
     O.destripe(d["pars"], d["dets"], d["detweights"], d["timestamps"], d["pixels"],
                d["pixweights"], d["signal"], d["periods"], d["npsd"], d["psdstarts"],
                d["psdfreqs"], d["psdvals"])
@@ -153,12 +162,49 @@ def run_cpu(cfg):
     n = s.ndet * s.nsamp
     it = max(1, int(sc["noiter"]))
     t_iter = sc["t_iterate"] / it
-    return {"value": n / t_iter, "unit": "samples/s per PCG iteration",
-            "cores": int(sc["nthreads"]), "kind": "port",
-            "sample": "{} detectors x {} samples of the workload ({} PCG iterations, "
-                      "{:.1f} ms/iteration, setup+solve {:.1f} s)".format(
-                          s.ndet, s.nsamp, it, 1e3 * t_iter, sc["t_total"]),
-            "iterations": it, "ms_per_iteration": 1e3 * t_iter}
+    what = "the whole workload" if full else "{} detectors x {} samples of the workload".format(
+        s.ndet, s.nsamp)
+    out = {"value": n / t_iter, "unit": "samples/s per PCG iteration",
+           "cores": int(sc["nthreads"]), "kind": "port",
+           "sample": "{} ({} PCG iterations, {:.1f} ms/iteration, setup+solve {:.1f} s)".format(
+               what, it, 1e3 * t_iter, sc["t_total"]),
+           "iterations": it, "ms_per_iteration": 1e3 * t_iter,
+           "time_to_cglimit_ms": 1e3 * sc["t_iterate"], "destripe_s": sc["t_total"]}
+    if parity_fp32 is not None:
+        out["parity"] = gpu_parity(O, d, keep, it, parity_fp32, what)
+    return out
+
+
+def gpu_parity(O, d, keep, oracle_iters, fp32, what):
+    """GPU destripe (or destripe_fp32) of the inputs the oracle just solved,
+    compared with the oracle's products."""
+    import parity
+    from libmadam_b200 import libmadam_wrapper as W
+    ro = {k: O.result(k) for k in ("map", "hits", "mask", "aa")}
+    sig = keep["signal"].astype(np.float32) if fp32 else keep["signal"]
+    (W.destripe_fp32 if fp32 else W.destripe)(
+        None, d["pars"], d["dets"], d["detweights"], d["timestamps"], keep["pixels"],
+        d["pixweights"], sig, d["periods"], d["npsd"], d["psdstarts"], d["psdfreqs"],
+        d["psdvals"])
+    mp = W.get_result("map").reshape(-1, 3)
+    mo = ro["map"].reshape(-1, 3)
+    err = lambda a, b: parity.per_pixel_error(a, b)[0]
+    it = int(W.scalars()["noiter"])
+    tol = 1e-4 if fp32 else 1e-6
+    out = {"sample": what + (", float32 TOD against the float64 oracle" if fp32 else ""),
+           "hits_equal": bool(np.array_equal(W.get_result("hits"), ro["hits"])),
+           "mask_equal": bool(np.array_equal(W.get_result("mask"), ro["mask"])),
+           "pixels_equal": bool(np.array_equal(keep["pixels"], d["pixels"])),
+           "map_max_rel_err_iqu": [err(mp[:, c], mo[:, c]) for c in range(3)],
+           "baseline_max_rel_err": err(W.get_result("aa"), ro["aa"]),
+           "iters": [it, oracle_iters], "iters_equal": it == oracle_iters,
+           "tolerance": tol,
+           "error_definition": "max |gpu - oracle| / max(|oracle|, 1e-3 max|oracle|) per "
+                               "pixel (per baseline)"}
+    out["pass"] = bool(out["hits_equal"] and out["mask_equal"] and out["pixels_equal"]
+                       and max(out["map_max_rel_err_iqu"]) <= tol
+                       and out["baseline_max_rel_err"] <= tol)
+    return out
 
 
 def _has_cuda():
@@ -201,16 +247,22 @@ def barrier(world):
 
 
 def reference_arm(args, world, rank):
+    """The CPU restatement on the whole workload (all host threads): one
+    destripe to cglimit, its PCG iterations are the steps."""
     if rank != 0:
         return 0
     cfg, wname = config_for(args.config)
-    res = run_cpu(cfg)
+    res = run_cpu(cfg, full=not args.ref_sample)
     line = {"impl": "reference", "metric": "TOD samples/s per PCG iteration",
             "value": res["value"], "unit": "samples/s per PCG iteration", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup,
+            "steps": res["iterations"], "warmup": 0,
             "ms_per_step": res["ms_per_iteration"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": wname, "sample": res["sample"]},
+            "config": {"workload": wname, "samples": cfg.ndet * cfg.nsamp, "nside": cfg.nside,
+                       "sample": res["sample"],
+                       "parallelism": "CPU, {} threads".format(res["cores"])},
+            "time_to_cglimit_ms": res["time_to_cglimit_ms"],
+            "iterations_to_cglimit": res["iterations"], "destripe_s": res["destripe_s"],
             "cpu_baseline": {"value": res["value"], "unit": res["unit"], "cores": res["cores"],
                              "kind": res["kind"], "sample": res["sample"]},
             "e2e": {"value": res["value"], "unit": res["unit"], "h2d_bytes_per_step": 0,
@@ -280,6 +332,7 @@ def run_mc(args, world, rank, local):
     m32 = W.get_result("map_batch").reshape(R, -1, 3)
     m64 = map64.reshape(R, -1, 3)
     err_map = [max(rel(m32[r][:, c], m64[r][:, c]) for r in range(R)) for c in range(3)]
+    line = None
     if rank == 0:
         line = {"metric": "TOD samples/s per PCG iteration (batched Monte Carlo)",
                 "value": value, "unit": "samples/s per PCG iteration", "n_gpus": world,
@@ -303,8 +356,10 @@ def run_mc(args, world, rank, local):
                 "single_rhs": {"value": single, "iterate_ms": t1["iterate_ms"],
                                "dtype": "f64"},
                 "speedup_vs_one_at_a_time": value / single}
-        print(json.dumps(line), flush=True)
-    return 0
+    del s32, d
+    W.clear_caches()
+    torch.cuda.empty_cache()
+    return line
 
 
 def run_serve(args, world, rank, local):
@@ -375,56 +430,25 @@ def run_serve(args, world, rank, local):
             "samples_per_s_per_pcg_iteration": float((samples * iters).sum() / makespan),
             "mean_iterations": float(iters.mean()),
             "total_samples": float(samples.sum())}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    return 0
+    return line if rank == 0 else None
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="2", choices=["2", "1", "3", "prof", "mid", "mid3", "small",
-                                                   "mc", "mc-prof", "serve"])
-    ap.add_argument("--requests", type=int, default=60)
-    ap.add_argument("--rate", type=float, default=20.0)
-    ap.add_argument("--workers", type=int, default=4)
-    ap.add_argument("--nrhs", type=int, default=64)
-    ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--sharded", action="store_true",
-                    help="N > 1: one sharded solve over NCCL (each rank its own detectors) "
-                         "instead of N independent replicas")
-    args = ap.parse_args()
-    args.warmup = max(3, args.warmup)
-    world, rank, local = dist_setup(args)
-    if args.impl == "reference":
-        rc = reference_arm(args, world, rank)
-        if world > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
-        return rc
-
+def run_destripe(args, world, rank, local, config, with_e2e=True, with_cpu=True):
+    """One destripe() workload: the full solve with inputs resident in HBM
+    (time to cglimit), the timed PCG iterations (the step), optionally the
+    end-to-end calls from pinned host buffers and the CPU leg, and the
+    roofline.  Returns rank 0's JSON line (None on other ranks)."""
     import torch
     from libmadam_b200 import libmadam_wrapper as W
     from libmadam_b200 import synthetic as syn
-    if not torch.cuda.is_available():
-        raise SystemExit("bench.py needs a CUDA device")
-    torch.cuda.set_device(local)
-    if args.config in ("mc", "mc-prof"):
-        return run_mc(args, world, rank, local)
-    if args.config == "serve":
-        return run_serve(args, world, rank, local)
-    cfg, wname = config_for(args.config)
+    cfg, wname = config_for(config)
     cfg.seed += 1000 * rank
     t0 = time.time()
     d = syn.generate(cfg, device="cuda")
     torch.cuda.synchronize()
     t_gen = time.time() - t0
     n = cfg.ndet * cfg.nsamp
-    fp32 = args.config in ("3", "mid3")
+    fp32 = config in ("3", "mid3")
     destripe = W.destripe_fp32 if fp32 else W.destripe
     pix = d["pixels"].reshape(-1)
     wts = d["pixweights"].reshape(-1)
@@ -464,7 +488,7 @@ def main():
 
     # end to end through the C-ABI with pinned host buffers
     e2e = None
-    if not args.no_e2e:
+    if with_e2e:
         h = {k: d[k].cpu().pin_memory() for k in ("timestamps", "pixels", "pixweights", "signal")}
         hn = {k: v.numpy().reshape(-1) for k, v in h.items()}
         # one untimed call from host buffers (the library's memory pool grows
@@ -543,14 +567,17 @@ def main():
                               "frac": b_iter / (ms_iter * 1e-3) / 1e9 / hbm}}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    par = None
+    if rank == 0 and world == 1 and with_cpu:
         try:
-            cpu = run_cpu(cfg)
+            cpu = run_cpu(cfg, parity_fp32=fp32)
+            par = cpu.get("parity")
             cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         except Exception as e:  # the CPU leg never blocks the GPU line
             cpu = {"value": None, "unit": "samples/s per PCG iteration", "cores": None,
                    "kind": "port", "sample": "failed: {}".format(e)}
 
+    line = None
     if rank == 0:
         line = {
             "metric": "TOD samples/s per PCG iteration", "value": value,
@@ -568,6 +595,7 @@ def main():
             "e2e": e2e,
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "parity": par,
             "time_to_cglimit_ms": tim["iterate_ms"], "iterations_to_cglimit": noiter,
             "destripe_device_ms": tim["total_ms"], "setup_ms": tim["setup_ms"],
             "phases_ms_per_iteration": phases, "generate_s": t_gen,
@@ -578,9 +606,113 @@ def main():
             line["precision"] = ("float32 TOD, pointing pairs and map copy in the projections; "
                                  "float64 pixel matrices, baselines and reductions")
             line["fp64_comparison"] = fp64_cmp
-        print(json.dumps(line), flush=True)
     if comm is not None:
         comm.free()
+    d = pix = wts = sig = None
+    W.clear_caches()
+    torch.cuda.empty_cache()
+    return line
+
+
+def extra_precision(args, world, rank, local):
+    """The precision form on its workload (nside 1024, 64 detectors x 2^24
+    samples, float32 TOD through destripe_fp32) and the float64 destripe()
+    of the same samples, for the line's "precision_form" key."""
+    r = run_destripe(args, world, rank, local, "3", with_e2e=False, with_cpu=False)
+    if r is None:
+        return None
+    cmp = r["fp64_comparison"]
+    return {"workload": r["config"]["workload"], "value": r["value"], "unit": r["unit"],
+            "ms_per_step": r["ms_per_step"], "clocks": r["clocks"], "dtype": r["dtype"],
+            "iterations_to_cglimit": r["iterations_to_cglimit"],
+            "time_to_cglimit_ms": r["time_to_cglimit_ms"],
+            "phases_ms_per_iteration": r["phases_ms_per_iteration"],
+            "roofline": r["roofline"],
+            "fp64_destripe_ms_per_iteration": cmp["fp64_ms_per_iteration"],
+            "fp64_destripe_time_to_cglimit_ms": cmp["fp64_time_to_cglimit_ms"],
+            "fp64_destripe_iterations": cmp["fp64_iterations_to_cglimit"],
+            "speedup_vs_fp64_destripe_per_iteration": cmp["speedup_per_iteration"],
+            "speedup_vs_fp64_destripe_to_cglimit": cmp["fp64_time_to_cglimit_ms"]
+            / r["time_to_cglimit_ms"],
+            "error_vs_fp64": {"map_rel_err_iqu": cmp["map_rel_err_iqu"],
+                              "baseline_rel_err": cmp["baseline_rel_err"],
+                              "tolerance": cmp["tolerance"]},
+            "pointing_pairs": cmp["pointing_pairs"], "samples_per_pair": cmp["samples_per_pair"],
+            "target_3x": "not met by this form alone (see batched_mc)"
+            if cmp["speedup_per_iteration"] < 3 else "met"}
+
+
+def extra_mc(args, world, rank, local):
+    """The batched Monte Carlo form (nside 512, 32 detectors x 2^22 samples,
+    64 noise realisations as one float32-TOD multi-right-hand-side PCG) for
+    the line's "batched_mc" key."""
+    r = run_mc(args, world, rank, local)
+    if r is None:
+        return None
+    keep = ("metric", "value", "unit", "ms_per_step", "clocks", "dtype", "iterations",
+            "batch_iterate_ms", "batch_setup_ms", "fp64_batch", "fp32_vs_fp64", "single_rhs",
+            "speedup_vs_one_at_a_time")
+    out = {k: r[k] for k in keep}
+    out["workload"] = r["config"]["workload"]
+    out["target_3x"] = ("met: {:.2f}x the float64 destripe_with_cache one realisation at a "
+                        "time".format(r["speedup_vs_one_at_a_time"])
+                        if r["speedup_vs_one_at_a_time"] >= 3 else
+                        "not met: {:.2f}x".format(r["speedup_vs_one_at_a_time"]))
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="2", choices=["2", "1", "3", "prof", "mid", "mid3", "small",
+                                                   "mc", "mc-prof", "serve"])
+    ap.add_argument("--requests", type=int, default=60)
+    ap.add_argument("--rate", type=float, default=20.0)
+    ap.add_argument("--workers", type=int, default=4)
+    ap.add_argument("--nrhs", type=int, default=64)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--only", action="store_true",
+                    help="config 2: the headline workload alone, without the precision-form "
+                         "and batched Monte Carlo keys")
+    ap.add_argument("--ref-sample", action="store_true",
+                    help="--impl reference: time the bounded sample instead of the whole "
+                         "workload")
+    ap.add_argument("--sharded", action="store_true",
+                    help="N > 1: one sharded solve over NCCL (each rank its own detectors) "
+                         "instead of N independent replicas")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        rc = reference_arm(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return rc
+
+    import torch
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    if args.config in ("mc", "mc-prof"):
+        line = run_mc(args, world, rank, local)
+    elif args.config == "serve":
+        line = run_serve(args, world, rank, local)
+    else:
+        line = run_destripe(args, world, rank, local, args.config,
+                            with_e2e=not args.no_e2e, with_cpu=not args.no_cpu)
+        if args.config == "2" and world == 1 and not args.only:
+            # the headline line carries the precision form (float32 TOD at
+            # nside 1024) and the batched Monte Carlo form (64 realisations),
+            # each measured in the same run with its own clocks record
+            line["precision_form"] = extra_precision(args, world, rank, local)
+            line["batched_mc"] = extra_mc(args, world, rank, local)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

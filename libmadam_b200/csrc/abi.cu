@@ -216,7 +216,22 @@ int madam_b200_destripe_with_cache_batch_fp32(int comm, long ndet, long nsamp, l
 
 int madam_b200_clear_caches(void) {
   std::lock_guard<std::mutex> lock(g_mutex);
-  return guarded([&] { g_engine.reset(); });
+  return guarded([&] {
+    const bool had = (bool)g_engine;
+    g_engine.reset();
+    // the engine's buffers went back to the device's memory pool, which
+    // keeps freed memory for the next call; clearing the caches hands it
+    // back to the device once those frees (ordered on the legacy stream by
+    // the engine's destructor) have run
+    if (had) {
+      int dev = 0;
+      cudaMemPool_t pool;
+      if (cudaStreamSynchronize(nullptr) == cudaSuccess && cudaGetDevice(&dev) == cudaSuccess &&
+          cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess)
+        cudaMemPoolTrimTo(pool, 0);
+      cudaGetLastError();
+    }
+  });
 }
 
 void destripe(int comm, char *parstring, long ndet, char *detstring, double *detweights,

@@ -151,7 +151,7 @@ __global__ void k_finish_b(const double *part, int nblk, int nd, double *scal, i
     sc[S_PAP] = v[0];
     sc[S_ALPHA] = sc[S_RZ] / v[0];
   } else {
-    sc[S_RZO] = sc[S_RZ];
+    if (mode == 2) sc[S_RZO] = sc[S_RZ];  // mode 3: a reliable update's redo
     sc[S_RZ] = v[0];
     sc[S_RZ2] = v[1];
     sc[S_RR] = v[2];

@@ -1062,7 +1062,9 @@ __global__ void k_finish(const double *part, int nblk, int nd, double *scal, int
     scal[S_PAP] = v[0];
     scal[S_ALPHA] = scal[S_RZ] / v[0];
   } else {
-    scal[S_RZO] = scal[S_RZ];
+    // mode 2: a new residual; mode 3: the same step's residual replaced (a
+    // reliable update), so rz of the previous step stays where it is
+    if (mode == 2) scal[S_RZO] = scal[S_RZ];
     scal[S_RZ] = v[0];
     scal[S_RZ2] = v[1];
     scal[S_RR] = v[2];
@@ -1108,7 +1110,7 @@ __global__ void k_finish_apply(double *scal, int mode, int src) {
     scal[S_PAP] = v0;
     scal[S_ALPHA] = scal[S_RZ] / v0;
   } else {
-    scal[S_RZO] = scal[S_RZ];
+    if (mode == 2) scal[S_RZO] = scal[S_RZ];
     scal[S_RZ] = v0;
     scal[S_RZ2] = v1;
     scal[S_RR] = v2;
@@ -1145,6 +1147,13 @@ __global__ void k_scale_neg(const double *a, const double *bw, double *out, long
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     out[i] = -(a[i] * bw[i]);
+}
+
+// r = b - ax (the true residual of a reliable update)
+__global__ void k_residual(double *r, const double *b, const double *ax, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    r[i] = b[i] - ax[i];
 }
 
 __global__ void k_mul(double *z, const double *r, const double *d, long long n) {

@@ -25,6 +25,10 @@ namespace madam {
 
 constexpr int kRedBlocks = 1184;      // 148 SMs x 8, fixed for determinism
 constexpr int kMaxBasis = 8;          // basis_order + 1 at most
+// FP32-TOD forms: a reliable update (true float64 residual) each time the
+// squared residual norm the float32 projections carried has dropped by this
+// factor since the last one
+constexpr double kReliableDrop = 1e-6;
 
 
 // Owning device allocation.
@@ -428,6 +432,15 @@ class Engine {
   long long npair_chunks_ = 0;
   DevBuf<float4> lmapf_;          // float32 map copy read by the FP32 gather
   DevBuf<double2> lmapg_;         // padded FP64 map copy {I, Q}, {U, 0}
+  // reliable updates of the FP32-TOD forms: the true residual b - A x with
+  // float64 projections over the exact sample pointing
+  // (the single FP32-TOD solve projects through float32 only with nmap 3)
+  bool refine() const { return fp32_ && nmap_ == 3; }
+  void apply_A_exact(const double *x, double *ax);
+  void true_residual(const double *x, const double *b, double *r);
+  DevBuf<double> pwx_, lmapx_, apx_, partx_;
+  DevBuf<double2> lmapgx_;
+  long n_reliable_ = 0;           // reliable updates of the last solve
 };
 
 }  // namespace madam

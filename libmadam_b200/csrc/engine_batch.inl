@@ -332,6 +332,10 @@ void Engine::iterate_batch() {
     nact += act_host_[k];
   }
   upload_act();
+  // FP32-TOD batch: reliable updates per right-hand side (see iterate())
+  const bool refine_b = fp32_;
+  std::vector<double> rr_true(rrinit_b_);
+  n_reliable_ = 0;
   long istep = 0;
   while (istep < par_.iter_max && nact > 0) {
     ++istep;
@@ -344,6 +348,28 @@ void Engine::iterate_batch() {
     MADAM_LAUNCH(k_finish_b, (unsigned)R, 1024, 0, st_, partb_.get(), kRedBlocks, 3,
                  scalb_.get(), 2, 0, actb_.get());
     fetch();
+    if (refine_b) {
+      std::vector<long> upd;
+      for (long k = 0; k < R; ++k) {
+        if (!act_host_[k]) continue;
+        const double rr = sc[k * S_NSCAL + S_RR];
+        if ((rr / rrinit_b_[k] < par_.cglimit && istep > par_.iter_min) ||
+            rr < kReliableDrop * rr_true[k])
+          upd.push_back(k);
+      }
+      if (!upd.empty()) {
+        // the true residuals of those right-hand sides, then z, rz, rz2 and rr
+        // again for all (unchanged for the others; mode 3 keeps rz_old)
+        for (long k : upd) true_residual(aab_.get() + k * nb, yb_.get() + k * nb, rb_.get() + k * nb);
+        apply_preconditioner_batch(rb_.get(), zb_.get());
+        MADAM_LAUNCH(k_dots_b, gd, 256, 0, st_, rb_.get(), zb_.get(), rob_.get(), zb_.get(),
+                     rb_.get(), rb_.get(), 3, rmask_.get(), nb, actb_.get(), partb_.get());
+        MADAM_LAUNCH(k_finish_b, (unsigned)R, 1024, 0, st_, partb_.get(), kRedBlocks, 3,
+                     scalb_.get(), 3, 0, actb_.get());
+        fetch();
+        for (long k : upd) rr_true[k] = sc[k * S_NSCAL + S_RR];
+      }
+    }
     bool changed = false;
     for (long k = 0; k < R; ++k) {
       if (!act_host_[k]) continue;

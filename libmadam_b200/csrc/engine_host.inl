@@ -1837,6 +1837,108 @@ void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) 
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[4], st_));
 }
 
+// A x with float64 projections over the exact sample pointing (the caller's
+// float32 weights, float64 map and baseline values): the operator of the
+// float64 path, for the true residual of the FP32-TOD forms' reliable
+// updates.  Works in its own buffers, so the PCG's vectors and its last
+// A p map (wamap) are left alone.
+void Engine::apply_A_exact(const double *x, double *ax) {
+  const long long nb = (long long)ndet_ * noba_short_;
+  const long ncross = std::max<long>(1, nloc_cross_);
+  pwx_.alloc(std::max<long long>(1, nb));
+  lmapx_.alloc((size_t)ncross * nmap_);
+  partx_.alloc(3 * kRedBlocks);
+  if (nmap_ == 3) lmapgx_.alloc((size_t)ncross * 2);
+  MADAM_LAUNCH(k_mul, grid_for(nb), 256, 0, st_, pwx_.get(), x, bw_.get(), nb);
+  // 1) baseline -> map over the samples: the pixel-sorted samples when the
+  // scatter has them, else the time-ordered runs (pairs round the weights)
+  if (nloc_cross_ > 0) {
+    if (!use_pairs_ && nscatter_chunks_ > 0) {
+      if (nmap_ == 3) {
+        MADAM_LAUNCH(k_scatter_chunks<3>, kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
+                     nscatter_chunks_, sp4_.get(), sp2_.get(), pwx_.get(), lmapx_.get(),
+                     scatter_partial_.get());
+        if (nscatter_multi_ > 0)
+          MADAM_LAUNCH(k_scatter_combine<3>, grid_for(nscatter_multi_), 256, 0, st_,
+                       scatter_multi_.get(), nscatter_multi_, scatter_partial_.get(),
+                       lmapx_.get());
+      } else {
+        MADAM_LAUNCH(k_scatter_chunks<1>, kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
+                     nscatter_chunks_, sp4_.get(), sp2_.get(), pwx_.get(), lmapx_.get(),
+                     scatter_partial_.get());
+        if (nscatter_multi_ > 0)
+          MADAM_LAUNCH(k_scatter_combine<1>, grid_for(nscatter_multi_), 256, 0, st_,
+                       scatter_multi_.get(), nscatter_multi_, scatter_partial_.get(),
+                       lmapx_.get());
+      }
+    } else {
+      lmapx_.zero(st_);
+      scatter_baselines(pwx_.get(), lmapx_.get(), false);
+    }
+  }
+  ar_sum(lmapx_.get(), (size_t)nloc_cross_ * nmap_);
+  if (nloc_cross_ > 0) {
+    if (nmap_ == 3)
+      MADAM_LAUNCH(k_ccmult_copy<false>, grid_for(nloc_cross_), 256, 0, st_, cca_.get(),
+                   lmapx_.get(), (long long)nloc_cross_, lmapgx_.get(), (float4 *)nullptr);
+    else
+      MADAM_LAUNCH(k_ccmult<1>, grid_for(nloc_cross_), 256, 0, st_, cca_.get(), lmapx_.get(),
+                   (long long)nloc_cross_);
+  }
+  // 2) noise prior
+  if (par_.kfilter) {
+    MADAM_CUDA(cudaMemcpyAsync(ax, x, nb * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+    if (!filt_segs_.empty())
+      fft_->convolve(st_, filt_segs_d_.get(), (long)filt_segs_.size(), fcov_.get(), x, ax);
+  } else if (par_.diagfilter != 0) {
+    MADAM_LAUNCH(k_diagfilter, grid_for(nb), 256, 0, st_, ax, nna_.get(), x, par_.diagfilter, nb);
+  } else {
+    MADAM_CUDA(cudaMemsetAsync(ax, 0, nb * sizeof(double), st_));
+  }
+  // 3) map -> baseline over the samples (the partial x.Ax sums are not used)
+  if (ngather_chunks_ > 0) {
+    if (nmap_ == 3)
+      MADAM_LAUNCH((k_gather_chunks<3, double2>), kGatherChunkBlocks, 256, 0, st_,
+                   gather_chunks_.get(), ngather_chunks_, point4_.get(), pixc_.get(),
+                   bstart_d_.get(), noba_short_, nsamp_, bw_.get(), x, nna_.get(), lmapx_.get(),
+                   lmapgx_.get(), (int)ndeg_shift_, (int)nloc_, rmask_.get(), ax, partx_.get());
+    else
+      MADAM_LAUNCH((k_gather_chunks<1, double2>), kGatherChunkBlocks, 256, 0, st_,
+                   gather_chunks_.get(), ngather_chunks_, point4_.get(), pixc_.get(),
+                   bstart_d_.get(), noba_short_, nsamp_, bw_.get(), x, nna_.get(), lmapx_.get(),
+                   (const double2 *)nullptr, (int)ndeg_shift_, (int)nloc_, rmask_.get(), ax,
+                   partx_.get());
+  } else if (gather_kb_ > 0) {
+    if (nmap_ == 3)
+      MADAM_LAUNCH(k_gather_tiled<3>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
+                   bstart_d_.get(), noba_short_, nsamp_, gather_kb_, gather_tiles_det_,
+                   (int)ndet_, bw_.get(), x, nna_.get(), lmapx_.get(), (int)ndeg_shift_,
+                   (int)nloc_, rmask_.get(), ax, partx_.get());
+    else
+      MADAM_LAUNCH(k_gather_tiled<1>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
+                   bstart_d_.get(), noba_short_, nsamp_, gather_kb_, gather_tiles_det_,
+                   (int)ndet_, bw_.get(), x, nna_.get(), lmapx_.get(), (int)ndeg_shift_,
+                   (int)nloc_, rmask_.get(), ax, partx_.get());
+  } else if (nmap_ == 3) {
+    MADAM_LAUNCH(k_gather<3>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
+                 bstart_d_.get(), nb, noba_short_, nsamp_, bw_.get(), x, nna_.get(),
+                 lmapx_.get(), (int)ndeg_shift_, (int)nloc_, rmask_.get(), ax, partx_.get());
+  } else {
+    MADAM_LAUNCH(k_gather<1>, kRedBlocks, 256, 0, st_, point4_.get(), pixc_.get(),
+                 bstart_d_.get(), nb, noba_short_, nsamp_, bw_.get(), x, nna_.get(),
+                 lmapx_.get(), (int)ndeg_shift_, (int)nloc_, rmask_.get(), ax, partx_.get());
+  }
+}
+
+// r = b - A x with the float64 operator (apply_A_exact)
+void Engine::true_residual(const double *x, const double *b, double *r) {
+  const long long nb = (long long)ndet_ * noba_short_;
+  apx_.alloc(std::max<long long>(1, nb));
+  apply_A_exact(x, apx_.get());
+  MADAM_LAUNCH(k_residual, grid_for(nb), 256, 0, st_, r, b, apx_.get(), nb);
+  ++n_reliable_;
+}
+
 void Engine::cg_preconditioner_segments(const double *r, double *z) {
   if (cg_prec_segs_.empty()) return;
   const long long nb = (long long)ndet_ * noba_short_;
@@ -1958,6 +2060,12 @@ void Engine::iterate() {
   }
   long istep = 0;
   float tm[4];
+  // FP32-TOD form: reliable updates each time the carried residual norm has
+  // dropped by kReliableDrop (squared) since the last true one, and before
+  // convergence is accepted
+  const bool reliable = refine() && nbasis_ == 1;
+  double rr_true = rrinit;
+  n_reliable_ = 0;
   while (istep < par_.iter_max) {
     ++istep;
     apply_A(p_.get(), pw_.get(), ap_.get(), true);
@@ -1980,7 +2088,24 @@ void Engine::iterate() {
     timings.filter_ms += tm[1];
     timings.gather_ms += tm[2];
     timings.precond_ms += tm[3];
-    const double rz = scal_host_[S_RZ], rr = scal_host_[S_RR];
+    double rz = scal_host_[S_RZ], rr = scal_host_[S_RR];
+    if (reliable && ((rr / rrinit < par_.cglimit && istep > par_.iter_min) ||
+                     rr < kReliableDrop * rr_true)) {
+      // reliable update: the residual the float32 projections carried is
+      // replaced by the true one, so that convergence is judged, and the
+      // iteration continues, on the float64 system
+      true_residual(aa_.get(), yba_.get(), r_.get());
+      apply_preconditioner(r_.get(), z_.get());
+      MADAM_LAUNCH(k_dots, kRedBlocks, 256, 0, st_, r_.get(), z_.get(), ro_.get(), z_.get(),
+                   r_.get(), r_.get(), 3, rmv, nb, part_.get());
+      finish_dots(3, 3, 0, kRedBlocks, true);
+      MADAM_CUDA(cudaMemcpyAsync(scal_host_.data(), scal_.get(), S_NSCAL * sizeof(double),
+                                 cudaMemcpyDeviceToHost, st_));
+      MADAM_CUDA(cudaStreamSynchronize(st_));
+      rz = scal_host_[S_RZ];
+      rr = scal_host_[S_RR];
+      rr_true = rr;
+    }
     rr_history.push_back(rr / rrinit);
     rr_final = rr / rrinit;
     noiter = istep;
@@ -2394,7 +2519,7 @@ long Engine::result_size(const std::string &name) {
   if (name == "invcov") return (long)invcov_host_.size();
   if (name == "rr_history") return (long)rr_history.size();
   if (name == "band_widths") return (long)band_widths_.size();
-  if (name == "scalars") return 22;
+  if (name == "scalars") return 23;
   if (name == "timings") return 9;
   if (name == "setup_marks") return kSetupMarks;
   if (name == "map_batch" || name == "binmap_batch") return nrhs_ * npm * nmap_;
@@ -2532,14 +2657,15 @@ void Engine::result_copy(const std::string &name, void *dst, long nbytes) {
     std::memcpy(dst, band_widths_.data(), sz * sizeof(long));
   } else if (name == "scalars") {
     need(sizeof(double));
-    const double v[22] = {(double)noiter, rrinit, rr_final, (double)nof_,
+    const double v[23] = {(double)noiter, rrinit, rr_final, (double)nof_,
                           (double)band_widths_.size(), (double)n_band_fail_, timings.iterate_ms,
                           timings.total_ms, (double)nmap_, (double)noba_short_,
                           (double)(12 * par_.nside_map * par_.nside_map), (double)nruns_,
                           (double)nwork_, (double)nloc_, (double)segs_.size(),
                           (double)cg_prec_segs_.size(), (double)band2_rows_,
                           (double)band2_ntrans_, (double)p2nch_, (double)csr_nvalid_,
-                          (double)(use_pairs_ ? npairs_ : 0), fp32_ ? 1.0 : 0.0};
+                          (double)(use_pairs_ ? npairs_ : 0), fp32_ ? 1.0 : 0.0,
+                          (double)n_reliable_};
     std::memcpy(dst, v, sizeof v);
   } else if (name == "setup_marks") {
     need(sizeof(double));

@@ -1,0 +1,59 @@
+"""Per-pixel tolerance shared by the GPU tests.
+
+A map, baseline vector or TOD `a` matches its reference `b` within `rtol`
+when every element satisfies
+
+    |a_i - b_i| <= rtol * max(|b_i|, FLOOR * max_j |b_j|)
+
+that is, a relative error of at most `rtol` per pixel (per baseline, per
+sample) for every element whose magnitude is at least FLOOR = 1e-3 of the
+largest, and an absolute error of at most rtol * FLOOR * max|b| for the
+elements closer to zero, whose relative error has no meaning (a Q or U pixel
+that happens to cross zero).  The bar is 1e-6 for the float64 path and 1e-4
+for the float32-TOD form.
+
+With MADAM_PARITY_REPORT=<file> every check appends one JSON line (test,
+quantity, error, tolerance, the largest per-element error among the elements
+at or above the floor and the absolute error of those below it relative to
+max|b|), so a run records the margins as well as the verdicts.
+"""
+import json
+import os
+
+import numpy as np
+
+FLOOR = 1e-3
+
+
+def per_pixel_error(a, b, floor=FLOOR):
+    """max_i |a_i - b_i| / max(|b_i|, floor * max|b|), with the two parts."""
+    a = np.asarray(a, dtype=float).reshape(-1)
+    b = np.asarray(b, dtype=float).reshape(-1)
+    assert a.shape == b.shape, (a.shape, b.shape)
+    if b.size == 0:
+        return 0.0, 0.0, 0.0
+    mag = np.abs(b)
+    scale = float(mag.max())
+    diff = np.abs(a - b)
+    if scale == 0.0:
+        e = float(diff.max()) * 1e300 if diff.max() > 0 else 0.0
+        return e, e, 0.0
+    cut = floor * scale
+    big = mag >= cut
+    rel_big = float((diff[big] / mag[big]).max()) if big.any() else 0.0
+    abs_small = float(diff[~big].max() / scale) if (~big).any() else 0.0
+    return max(rel_big, abs_small / floor), rel_big, abs_small
+
+
+def close(a, b, rtol, what=""):
+    """Assert the per-pixel tolerance; returns the error."""
+    e, rel_big, abs_small = per_pixel_error(a, b)
+    path = os.environ.get("MADAM_PARITY_REPORT")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps({"test": os.environ.get("PYTEST_CURRENT_TEST", "").split(" ")[0],
+                                "what": what, "err": e, "rtol": rtol,
+                                "max_rel_above_floor": rel_big,
+                                "max_abs_below_floor_over_max": abs_small}) + "\n")
+    assert e <= rtol, (what, "per-pixel error", e, "rtol", rtol, rel_big, abs_small)
+    return e

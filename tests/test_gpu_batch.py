@@ -4,18 +4,22 @@ madam_b200_destripe_with_cache_batch solves R noise realisations that share
 one pointing as a single multi-right-hand-side PCG.  Each realisation must
 come out as destripe_with_cache gives it when called right after the caching
 destripe(mcmode=True): same PCG iteration count, destriped and binned maps
-and baselines within BATCH_RTOL of their largest magnitude (the batched
+and baselines within BATCH_RTOL per pixel (parity.close; the batched
 kernels repeat the single-solve arithmetic; the setup's binning scatter sums
-with FP64 atomics, so separate runs agree to rounding, not to the bit).
+with FP64 atomics, so separate runs agree to rounding, not to the bit), and
+within MAP_RTOL of the CPU oracle's cached solve of each realisation.
 """
 import numpy as np
 import pytest
 
+import oracle_api as O
+import parity
 from libmadam_b200 import synthetic as syn
 
 pytestmark = pytest.mark.gpu
 
 BATCH_RTOL = 1e-9
+MAP_RTOL = 1e-6  # against the CPU oracle
 
 
 @pytest.fixture(scope="module")
@@ -28,11 +32,8 @@ def W():
     return libmadam_wrapper
 
 
-def _close(a, b, rtol):
-    a = np.asarray(a, float)
-    b = np.asarray(b, float)
-    scale = np.abs(b).max() if b.size else 0.0
-    assert np.abs(a - b).max() <= rtol * max(scale, 1e-300)
+def _close(a, b, rtol, what=""):
+    return parity.close(a, b, rtol, what)
 
 
 def _realisations(d, nrhs):
@@ -50,6 +51,22 @@ def _cache(W, d, pars):
     W.destripe(None, pars, d["dets"], d["detweights"], d["timestamps"], d["pixels"].copy(),
                d["pixweights"], d["signal"].copy(), d["periods"], d["npsd"], d["psdstarts"],
                d["psdfreqs"], d["psdvals"])
+
+
+def _oracle_sequential(d, pars, sigs):
+    """The CPU oracle's cached solve of every realisation, each right after
+    the caching call (what the batch reproduces)."""
+    res = []
+    for s in sigs:
+        O.clear_caches()
+        O.destripe(pars, d["dets"], d["detweights"], d["timestamps"], d["pixels"].copy(),
+                   d["pixweights"], d["signal"].copy(), d["periods"], d["npsd"],
+                   d["psdstarts"], d["psdfreqs"], d["psdvals"])
+        O.destripe_with_cache(d["timestamps"], d["pixels"].copy(), d["pixweights"], s.copy(),
+                              len(d["dets"]))
+        res.append({k: O.result(k) for k in ("map", "aa")} | {"noiter": O.scalars()["noiter"]})
+    O.clear_caches()
+    return res
 
 
 def _sequential(W, d, pars, sigs):
@@ -73,6 +90,7 @@ def test_batch_matches_one_at_a_time(W, extra):
     nrhs = 5
     sigs = _realisations(d, nrhs)
     ref = _sequential(W, d, pars, sigs)
+    oref = _oracle_sequential(d, pars, sigs)
     W.clear_caches()
     _cache(W, d, pars)
     W.destripe_with_cache_batch(None, d["timestamps"], d["pixels"].copy(), d["pixweights"],
@@ -83,11 +101,14 @@ def test_batch_matches_one_at_a_time(W, extra):
     aas = W.get_result("aa_batch").reshape(nrhs, -1)
     its = W.get_result("noiter_batch")
     for r in range(nrhs):
-        assert its[r] == ref[r]["noiter"]
+        assert its[r] == ref[r]["noiter"] == oref[r]["noiter"]
         for c in range(nmap):
             _close(maps[r][:, c], ref[r]["map"].reshape(-1, nmap)[:, c], BATCH_RTOL)
             _close(bins[r][:, c], ref[r]["binmap"].reshape(-1, nmap)[:, c], BATCH_RTOL)
+            _close(maps[r][:, c], oref[r]["map"].reshape(-1, nmap)[:, c], MAP_RTOL,
+                   "map_batch vs oracle")
         _close(aas[r], ref[r]["aa"], BATCH_RTOL)
+        _close(aas[r], oref[r]["aa"], MAP_RTOL, "aa_batch vs oracle")
     # the cache is left as it was: a following single call gives the sequential answer
     W.destripe_with_cache(None, d["timestamps"], d["pixels"].copy(), d["pixweights"],
                           sigs[2].copy(), b"")

@@ -6,6 +6,7 @@ call that fails after the upload started leaves the engine usable."""
 import numpy as np
 import pytest
 
+import parity
 from libmadam_b200 import synthetic as syn
 
 pytestmark = pytest.mark.gpu
@@ -21,10 +22,8 @@ def W():
     return libmadam_wrapper
 
 
-def _close(a, b, rtol):
-    a = np.asarray(a, float)
-    b = np.asarray(b, float)
-    assert np.abs(a - b).max() <= rtol * max(np.abs(b).max(), 1e-300)
+def _close(a, b, rtol, what=""):
+    return parity.close(a, b, rtol, what)
 
 
 def _pinned(a):

@@ -7,11 +7,14 @@ others, and device buffers are served like host buffers."""
 import numpy as np
 import pytest
 
+import oracle_api as O
+import parity
 from libmadam_b200 import synthetic as syn
 
 pytestmark = pytest.mark.gpu
 
 SERVE_RTOL = 1e-9
+MAP_RTOL = 1e-6
 
 
 @pytest.fixture(scope="module")
@@ -23,11 +26,8 @@ def W():
     return libmadam_wrapper
 
 
-def _close(a, b, rtol):
-    a = np.asarray(a, float)
-    b = np.asarray(b, float)
-    scale = np.abs(b).max() if b.size else 0.0
-    assert np.abs(a - b).max() <= rtol * max(scale, 1e-300)
+def _close(a, b, rtol, what=""):
+    return parity.close(a, b, rtol, what)
 
 
 def _jobs():
@@ -66,15 +66,26 @@ def test_jobs_in_flight_match_jobs_alone(W):
     tb = srv.submit(bad["pars"], bad["dets"], bad["detweights"], bad["timestamps"], bad_pix,
                     bad["pixweights"], bad["signal"].copy(), bad["periods"], bad["npsd"],
                     bad["psdstarts"], bad["psdfreqs"], bad["psdvals"])
+    served = []
     for t, ref in zip(tickets, alone):
         assert srv.wait(t) == 2
         np.testing.assert_array_equal(srv.result(t, "hits"), ref["hits"])
         _close(srv.result(t, "map"), ref["map"], SERVE_RTOL)
         _close(srv.result(t, "aa"), ref["aa"], SERVE_RTOL)
         assert srv.result(t, "scalars")[0] == ref["noiter"]
+        served.append({k: srv.result(t, k) for k in ("map", "aa", "hits")})
         info = srv.info(t)
         assert info["t_end"] >= info["t_start"] >= info["t_submit"]
         srv.release(t)
+    # jobs served in the mix against the CPU oracle (the largest, polarised,
+    # and the temperature-only job)
+    for i, nmap in ((3, 3), (4, 1)):
+        O.destripe(*_args(jobs[i]))
+        np.testing.assert_array_equal(served[i]["hits"], O.result("hits"))
+        mo = O.result("map").reshape(-1, nmap)
+        for c in range(nmap):
+            _close(served[i]["map"].reshape(-1, nmap)[:, c], mo[:, c], MAP_RTOL, "map[%d]" % c)
+        _close(served[i]["aa"], O.result("aa"), MAP_RTOL, "aa")
     with pytest.raises(RuntimeError, match="Too large pixel number"):
         srv.wait(tb)
     srv.close()

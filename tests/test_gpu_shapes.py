@@ -1,0 +1,167 @@
+"""GPU against the CPU oracle at the shapes the benchmarks run.
+
+The other parity tests use small scans (nside <= 64, 10 Hz, baselines of at
+most 20 samples).  These cases take the benchmarked workloads' per-segment
+shapes at sizes the oracle solves in seconds:
+
+* the plain float64 workload (nside 512, nside_submap 16, 100 Hz,
+  base_first 0.5 s, fknee 0.05 Hz, alpha -1.5): 4 detectors x 2^23 samples,
+  the full length of one of its observations, so the filter runs at its
+  nof = 2^19 and the band preconditioner over its 167,773-baseline segments;
+* the precision form (nside 1024, base_first 1 s, float32 TOD):
+  4 detectors x 2^22 samples against the float64 oracle;
+* the batched Monte Carlo form (nside 512, base_first 1 s, per-detector fknee
+  in 0.02-0.2 Hz): 8 noise realisations of 4 detectors x 2^20 samples, float64
+  and float32 batches, each realisation against the oracle's cached solve;
+* baselines longer than the warp-chunk gather takes: base_first 5 s and 20 s
+  at 100 Hz (500- and 2000-sample baselines, the tiled and the per-baseline
+  map-to-baseline kernels).
+
+Tolerances as in the other parity tests, per pixel (parity.close): float64
+maps and baselines 1e-6, float32-TOD 1e-4; hits and masks bit-exact.
+"""
+import numpy as np
+import pytest
+
+import oracle_api as O
+import parity
+from libmadam_b200 import synthetic as syn
+
+pytestmark = pytest.mark.gpu
+
+MAP_RTOL = 1e-6
+BIN_RTOL = 1e-10
+FP32_RTOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def W():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from libmadam_b200 import libmadam_wrapper
+    assert libmadam_wrapper.available
+    return libmadam_wrapper
+
+
+def _args(pars, x, signal=None):
+    return (pars, x["dets"], x["detweights"], x["timestamps"], x["pixels"], x["pixweights"],
+            x["signal"] if signal is None else signal, x["periods"], x["npsd"], x["psdstarts"],
+            x["psdfreqs"], x["psdvals"])
+
+
+def _copy(d):
+    return {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
+
+
+def _data(cfg):
+    return syn.to_numpy(syn.generate(cfg, device="cuda"))
+
+
+def _oracle(d, pars):
+    do = _copy(d)
+    O.destripe(*_args(pars, do))
+    r = {k: O.result(k) for k in ("map", "binmap", "hits", "mask", "aa")}
+    r["scalars"] = O.scalars()
+    r["pixels"] = do["pixels"]
+    return r
+
+
+def _check(rp, ro, nmap, rtol, bin_rtol):
+    np.testing.assert_array_equal(rp["hits"], ro["hits"])
+    np.testing.assert_array_equal(rp["mask"], ro["mask"])
+    for c in range(nmap):
+        parity.close(rp["binmap"].reshape(-1, nmap)[:, c], ro["binmap"].reshape(-1, nmap)[:, c],
+                     bin_rtol, "binmap[%d]" % c)
+        parity.close(rp["map"].reshape(-1, nmap)[:, c], ro["map"].reshape(-1, nmap)[:, c],
+                     rtol, "map[%d]" % c)
+    parity.close(rp["aa"], ro["aa"], rtol, "aa")
+
+
+def test_plain_float64_workload_shape(W):
+    cfg = syn.config2()
+    cfg.ndet, cfg.nobs = 4, 1
+    d = _data(cfg)
+    ro = _oracle(d, d["pars"])
+    dp = _copy(d)
+    W.destripe(None, *_args(d["pars"], dp))
+    rp = {k: W.get_result(k) for k in ("map", "binmap", "hits", "mask", "aa")}
+    sc = W.scalars()
+    assert sc["nof"] == ro["scalars"]["nof"] == 1 << 19
+    np.testing.assert_array_equal(dp["pixels"], ro["pixels"])
+    _check(rp, ro, 3, MAP_RTOL, BIN_RTOL)
+    assert sc["noiter"] == ro["scalars"]["noiter"]
+
+
+def test_precision_form_workload_shape(W):
+    cfg = syn.config3()
+    cfg.ndet, cfg.nsamp_obs = 4, 1 << 22
+    d = _data(cfg)
+    ro = _oracle(d, d["pars"])
+    dp = _copy(d)
+    W.destripe_fp32(None, *_args(d["pars"], dp, d["signal"].astype(np.float32)))
+    rp = {k: W.get_result(k) for k in ("map", "binmap", "hits", "mask", "aa")}
+    sc = W.scalars()
+    assert sc["fp32"] == 1.0 and sc["pairs"] > 0
+    np.testing.assert_array_equal(dp["pixels"], ro["pixels"])
+    # the binned map of a float32 signal: float32 rounding of every sample
+    _check(rp, ro, 3, FP32_RTOL, FP32_RTOL)
+    assert abs(sc["noiter"] - ro["scalars"]["noiter"]) <= 2
+
+
+def test_batched_monte_carlo_workload_shape(W):
+    cfg = syn.config4()
+    cfg.ndet, cfg.nsamp_obs = 4, 1 << 20
+    nrhs = 8
+    d = syn.to_numpy(syn.generate(cfg, device="cuda", with_signal=False))
+    sigs = syn.noise_realisations(cfg, nrhs + 1, device="cuda").cpu().numpy()
+    pars = dict(d["pars"], mcmode=True)
+    cache_sig = sigs[nrhs].reshape(-1)
+    # the oracle: each realisation's cached call right after the caching call
+    ref = []
+    for r in range(nrhs):
+        O.clear_caches()
+        do = _copy(d)
+        O.destripe(*_args(pars, do, cache_sig.copy()))
+        O.destripe_with_cache(d["timestamps"], d["pixels"].copy(), d["pixweights"],
+                              sigs[r].reshape(-1).copy(), cfg.ndet)
+        ref.append(dict(map=O.result("map"), aa=O.result("aa"),
+                        noiter=O.scalars()["noiter"]))
+    O.clear_caches()
+    for fp32, rtol in ((False, MAP_RTOL), (True, FP32_RTOL)):
+        W.clear_caches()
+        W.destripe(None, *_args(pars, _copy(d), cache_sig.copy()))
+        if fp32:
+            W.destripe_with_cache_batch_fp32(None, d["timestamps"], d["pixels"].copy(),
+                                             d["pixweights"], sigs[:nrhs].astype(np.float32))
+        else:
+            W.destripe_with_cache_batch(None, d["timestamps"], d["pixels"].copy(),
+                                        d["pixweights"], sigs[:nrhs])
+        maps = W.get_result("map_batch").reshape(nrhs, -1, 3)
+        aas = W.get_result("aa_batch").reshape(nrhs, -1)
+        its = W.get_result("noiter_batch")
+        for r in range(nrhs):
+            if fp32:
+                assert abs(its[r] - ref[r]["noiter"]) <= 3
+            else:
+                assert its[r] == ref[r]["noiter"]
+            for c in range(3):
+                parity.close(maps[r][:, c], ref[r]["map"].reshape(-1, 3)[:, c], rtol,
+                             "map_batch[%d][%d]" % (r, c))
+            parity.close(aas[r], ref[r]["aa"], rtol, "aa_batch[%d]" % r)
+    W.clear_caches()
+
+
+@pytest.mark.parametrize("base_first", [5.0, 20.0])
+def test_long_baselines(W, base_first):
+    cfg = syn.ScanConfig(nside=128, nside_submap=16, ndet=4, nobs=2, nsamp_obs=1 << 19,
+                         fsample=100.0, fknee=0.05, alpha=-1.5, base_first=base_first,
+                         seed=1200 + int(base_first), extra_pars=dict(cglimit=1e-12))
+    d = _data(cfg)
+    ro = _oracle(d, d["pars"])
+    dp = _copy(d)
+    W.destripe(None, *_args(d["pars"], dp))
+    rp = {k: W.get_result(k) for k in ("map", "binmap", "hits", "mask", "aa")}
+    np.testing.assert_array_equal(dp["pixels"], ro["pixels"])
+    _check(rp, ro, 3, MAP_RTOL, BIN_RTOL)
+    assert W.scalars()["noiter"] == ro["scalars"]["noiter"]

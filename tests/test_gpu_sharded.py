@@ -8,6 +8,7 @@ largest magnitude (the ranks' partial sums add in another order)."""
 import numpy as np
 import pytest
 
+import parity
 import shard_util as SU
 from libmadam_b200 import synthetic as syn
 
@@ -29,11 +30,8 @@ def _args(pars, x):
             x["signal"], x["periods"], x["npsd"], x["psdstarts"], x["psdfreqs"], x["psdvals"])
 
 
-def _close(a, b, rtol):
-    a = np.asarray(a, float)
-    b = np.asarray(b, float)
-    scale = np.abs(b).max() if b.size else 0.0
-    assert np.abs(a - b).max() <= rtol * max(scale, 1e-300)
+def _close(a, b, rtol, what=""):
+    return parity.close(a, b, rtol, what)
 
 
 def test_nccl_single_rank_matches_plain(W):
