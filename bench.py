@@ -154,6 +154,8 @@ def run_cpu(cfg, full=False, parity_fp32=None):
     d = syn.to_numpy(syn.generate(s, device=dev))
     keep = None
     if parity_fp32 is not None:
+        if parity_fp32:  # the oracle solves the float32 samples the GPU gets
+            d["signal"] = d["signal"].astype(np.float32).astype(np.float64)
         keep = {k: d[k].copy() for k in ("pixels", "signal")}
     O.destripe(d["pars"], d["dets"], d["detweights"], d["timestamps"], d["pixels"],
                d["pixweights"], d["signal"], d["periods"], d["npsd"], d["psdstarts"],
@@ -188,7 +190,8 @@ def gpu_parity(O, d, keep, oracle_iters, fp32, what):
         d["psdvals"])
     mp = W.get_result("map").reshape(-1, 3)
     mo = ro["map"].reshape(-1, 3)
-    err = lambda a, b: parity.per_pixel_error(a, b)[0]
+    floor = parity.FP32_FLOOR if fp32 else parity.FLOOR
+    err = lambda a, b: parity.per_pixel_error(a, b, floor)[0]
     it = int(W.scalars()["noiter"])
     tol = 1e-4 if fp32 else 1e-6
     out = {"sample": what + (", float32 TOD against the float64 oracle" if fp32 else ""),
@@ -199,8 +202,8 @@ def gpu_parity(O, d, keep, oracle_iters, fp32, what):
            "baseline_max_rel_err": err(W.get_result("aa"), ro["aa"]),
            "iters": [it, oracle_iters], "iters_equal": it == oracle_iters,
            "tolerance": tol,
-           "error_definition": "max |gpu - oracle| / max(|oracle|, 1e-3 max|oracle|) per "
-                               "pixel (per baseline)"}
+           "error_definition": "max |gpu - oracle| / max(|oracle|, {:g} max|oracle|) per "
+                               "pixel (per baseline)".format(floor)}
     out["pass"] = bool(out["hits_equal"] and out["mask_equal"] and out["pixels_equal"]
                        and max(out["map_max_rel_err_iqu"]) <= tol
                        and out["baseline_max_rel_err"] <= tol)
@@ -291,7 +294,9 @@ def run_mc(args, world, rank, local):
     cfg.seed += 1000 * rank
     R = args.nrhs
     d = syn.generate(cfg, device="cuda", with_signal=False)
-    sigs = syn.noise_realisations(cfg, R + 1, device="cuda")
+    # realisations rounded to float32 once: the float64 and the float32 solves
+    # see the same samples, so their difference is the form's arithmetic
+    sigs = syn.noise_realisations(cfg, R + 1, device="cuda").float().double()
     torch.cuda.synchronize()
     n = cfg.ndet * cfg.nsamp
     pars = dict(d["pars"], mcmode=True)
@@ -332,6 +337,16 @@ def run_mc(args, world, rank, local):
     m32 = W.get_result("map_batch").reshape(R, -1, 3)
     m64 = map64.reshape(R, -1, 3)
     err_map = [max(rel(m32[r][:, c], m64[r][:, c]) for r in range(R)) for c in range(3)]
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import parity
+    pp = lambda a, b, f=parity.FP32_FLOOR: parity.per_pixel_error(a, b, f)[0]
+    a32 = W.get_result("aa_batch").reshape(R, -1)
+    a64r = aa64.reshape(R, -1)
+    pp_map = [max(pp(m32[r][:, c], m64[r][:, c]) for r in range(R)) for c in range(3)]
+    pp_aa = max(pp(a32[r], a64r[r]) for r in range(R))
+    pp_map3 = [max(pp(m32[r][:, c], m64[r][:, c], parity.FLOOR) for r in range(R))
+               for c in range(3)]
+    n_rel = int(W.scalars()["reliable_updates"])
     line = None
     if rank == 0:
         line = {"metric": "TOD samples/s per PCG iteration (batched Monte Carlo)",
@@ -352,7 +367,14 @@ def run_mc(args, world, rank, local):
                                "iterations_max": int(its64.max()),
                                "speedup_vs_one_at_a_time": value64 / single},
                 "fp32_vs_fp64": {"map_rel_err_iqu": err_map, "baseline_rel_err": err_aa,
-                                 "tolerance": 1e-4},
+                                 "map_per_pixel_err_iqu": pp_map,
+                                 "baseline_per_baseline_err": pp_aa,
+                                 "tolerance": 1e-4,
+                                 "map_per_pixel_err_iqu_floor_1e-3": pp_map3,
+                                 "samples": "the same (float32) samples in both batches",
+                                 "error_definition": "max over realisations of max |fp32 - "
+                                                     "fp64| / max(|fp64|, 1e-2 max|fp64|)"},
+                "reliable_updates": n_rel,
                 "single_rhs": {"value": single, "iterate_ms": t1["iterate_ms"],
                                "dtype": "f64"},
                 "speedup_vs_one_at_a_time": value / single}
@@ -520,22 +542,48 @@ def run_destripe(args, world, rank, local, config, with_e2e=True, with_cpu=True)
     # the precision form against a float64-TOD solve of the same samples
     fp64_cmp = None
     if fp32:
+        # the float64 destripe() of the same samples (the float32 signal
+        # widened: the form's arithmetic error) and of the float64 signal the
+        # float32 one was rounded from (adds the input's rounding)
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import parity
+        sca32 = sca
         del d["signal"], sig
+        sig_same = sig64.float().double()
+        torch.cuda.empty_cache()
+        W.destripe(comm, *common, d["timestamps"], pix, wts, sig_same, *psd)
+        ms = W.get_result("map").reshape(-1, 3)
+        a_same = W.get_result("aa")
+        it64 = int(W.scalars()["noiter"])
+        t64 = W.timings()["iterate_ms"]
+        b64 = W.bench_iterations(args.warmup, args.steps)
+        del sig_same
         torch.cuda.empty_cache()
         W.destripe(comm, *common, d["timestamps"], pix, wts, sig64, *psd)
         m64 = W.get_result("map").reshape(-1, 3)
         a64 = W.get_result("aa")
-        it64 = int(W.scalars()["noiter"])
-        t64 = W.timings()["iterate_ms"]
-        b64 = W.bench_iterations(args.warmup, args.steps)
         m32 = map32.reshape(-1, 3)
         rel = lambda a, b: float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
-        fp64_cmp = {"map_rel_err_iqu": [rel(m32[:, c], m64[:, c]) for c in range(3)],
-                    "baseline_rel_err": rel(aa32, a64),
-                    "tolerance": 1e-4, "fp64_ms_per_iteration": b64["ms_per_iter"],
+        pp = lambda a, b, f=parity.FP32_FLOOR: parity.per_pixel_error(a, b, f)[0]
+        fp64_cmp = {"same_samples": {
+                        "map_per_pixel_err_iqu": [pp(m32[:, c], ms[:, c]) for c in range(3)],
+                        "baseline_per_baseline_err": pp(aa32, a_same),
+                        "tolerance": 1e-4,
+                        "map_per_pixel_err_iqu_floor_1e-3": [pp(m32[:, c], ms[:, c], parity.FLOOR)
+                                                             for c in range(3)],
+                        "error_definition": "max |fp32 - fp64| / max(|fp64|, 1e-2 max|fp64|)"},
+                    "float64_signal": {
+                        "map_rel_err_iqu": [rel(m32[:, c], m64[:, c]) for c in range(3)],
+                        "baseline_rel_err": rel(aa32, a64),
+                        "error_definition": "max |fp32 - fp64| / max|fp64| (includes the "
+                                            "float32 rounding of the input)"},
+                    "fp64_ms_per_iteration": b64["ms_per_iter"],
                     "fp64_iterations_to_cglimit": it64, "fp64_time_to_cglimit_ms": t64,
                     "speedup_per_iteration": b64["ms_per_iter"] / b["ms_per_iter"],
-                    "pointing_pairs": sca["pairs"], "samples_per_pair": n / max(1.0, sca["pairs"])}
+                    "reliable_updates": sca32["reliable_updates"],
+                    "pointing_pairs": sca32["pairs"],
+                    "samples_per_pair": n / max(1.0, sca32["pairs"])}
+        sca = sca32
         del sig64
 
     # roofline of the dominant kernel (algorithmic bytes per launch / duration)
@@ -634,9 +682,9 @@ def extra_precision(args, world, rank, local):
             "speedup_vs_fp64_destripe_per_iteration": cmp["speedup_per_iteration"],
             "speedup_vs_fp64_destripe_to_cglimit": cmp["fp64_time_to_cglimit_ms"]
             / r["time_to_cglimit_ms"],
-            "error_vs_fp64": {"map_rel_err_iqu": cmp["map_rel_err_iqu"],
-                              "baseline_rel_err": cmp["baseline_rel_err"],
-                              "tolerance": cmp["tolerance"]},
+            "error_vs_fp64_same_samples": cmp["same_samples"],
+            "error_vs_fp64_float64_signal": cmp["float64_signal"],
+            "reliable_updates": cmp["reliable_updates"],
             "pointing_pairs": cmp["pointing_pairs"], "samples_per_pair": cmp["samples_per_pair"],
             "target_3x": "not met by this form alone (see batched_mc)"
             if cmp["speedup_per_iteration"] < 3 else "met"}
@@ -650,7 +698,8 @@ def extra_mc(args, world, rank, local):
     if r is None:
         return None
     keep = ("metric", "value", "unit", "ms_per_step", "clocks", "dtype", "iterations",
-            "batch_iterate_ms", "batch_setup_ms", "fp64_batch", "fp32_vs_fp64", "single_rhs",
+            "batch_iterate_ms", "batch_setup_ms", "fp64_batch", "fp32_vs_fp64",
+            "reliable_updates", "single_rhs",
             "speedup_vs_one_at_a_time")
     out = {k: r[k] for k in keep}
     out["workload"] = r["config"]["workload"]

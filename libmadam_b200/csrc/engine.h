@@ -214,7 +214,7 @@ class Engine {
   DevBuf<double> lmapb_, scatpb_;        // [R][nloc_cross][nmap], scatter partials
   DevBuf<double> binb_, mapb_, binmapb_; // [R][nloc][nmap]
   DevBuf<double> partb_, scalb_;         // [R][3][kRedBlocks], [R][S_NSCAL]
-  DevBuf<int> actb_;
+  DevBuf<int> actb_, actu_;              // active / reliably updated right-hand sides
   std::vector<int> act_host_;
   std::vector<double> noiter_b_, rrinit_b_, rrfinal_b_;
   // band factor tables replicated per right-hand side (offsets k0 + r nb)

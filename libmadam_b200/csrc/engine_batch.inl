@@ -293,6 +293,7 @@ void Engine::iterate_batch() {
   scalb_.alloc((size_t)R * S_NSCAL);
   scalb_.zero(st_);
   actb_.alloc(R);
+  actu_.alloc(R);
   lmapb_.alloc((size_t)R * std::max<long>(1, nloc_cross_) * nmap_);
   scatpb_.alloc((size_t)R * std::max<size_t>(1, scatter_partial_.n));
   build_batch_tables();
@@ -358,14 +359,21 @@ void Engine::iterate_batch() {
           upd.push_back(k);
       }
       if (!upd.empty()) {
-        // the true residuals of those right-hand sides, then z, rz, rz2 and rr
-        // again for all (unchanged for the others; mode 3 keeps rz_old)
-        for (long k : upd) true_residual(aab_.get() + k * nb, yb_.get() + k * nb, rb_.get() + k * nb);
-        apply_preconditioner_batch(rb_.get(), zb_.get());
+        // the true residuals of those right-hand sides, their z (the
+        // single-solve preconditioner on their slices), and rz, rz2 and rr
+        // of those alone (mode 3 keeps rz_old)
+        std::vector<int> mask(R, 0);
+        for (long k : upd) {
+          true_residual(aab_.get() + k * nb, yb_.get() + k * nb, rb_.get() + k * nb);
+          apply_preconditioner(rb_.get() + k * nb, zb_.get() + k * nb);
+          mask[k] = 1;
+        }
+        MADAM_CUDA(cudaMemcpyAsync(actu_.get(), mask.data(), R * sizeof(int),
+                                   cudaMemcpyHostToDevice, st_));
         MADAM_LAUNCH(k_dots_b, gd, 256, 0, st_, rb_.get(), zb_.get(), rob_.get(), zb_.get(),
-                     rb_.get(), rb_.get(), 3, rmask_.get(), nb, actb_.get(), partb_.get());
+                     rb_.get(), rb_.get(), 3, rmask_.get(), nb, actu_.get(), partb_.get());
         MADAM_LAUNCH(k_finish_b, (unsigned)R, 1024, 0, st_, partb_.get(), kRedBlocks, 3,
-                     scalb_.get(), 3, 0, actb_.get());
+                     scalb_.get(), 3, 0, actu_.get());
         fetch();
         for (long k : upd) rr_true[k] = sc[k * S_NSCAL + S_RR];
       }

@@ -143,13 +143,15 @@ FP32_RTOL = 1e-4
 
 @pytest.mark.parametrize("extra", [dict(), dict(temperature_only=True)])
 def test_batch_fp32_matches_fp64(W, extra):
-    """The FP32-TOD batched form against one-at-a-time float64 solves: maps
-    and baselines within FP32_RTOL of their largest magnitude."""
+    """The FP32-TOD batched form against one-at-a-time float64 solves of the
+    same samples: maps and baselines within FP32_RTOL per pixel (with the
+    float32 forms' floor, parity.FP32_FLOOR)."""
     cfg = syn.small_config(seed=45)
     d = syn.to_numpy(syn.generate(cfg, nnz=1 if extra.get("temperature_only") else None))
     pars = dict(d["pars"], mcmode=True, **extra)
     nrhs = 4
-    sigs = _realisations(d, nrhs)
+    # realisations that float32 holds exactly: both sides solve the same data
+    sigs = [s.astype(np.float32).astype(np.float64) for s in _realisations(d, nrhs)]
     ref = _sequential(W, d, pars, sigs)
     W.clear_caches()
     _cache(W, d, pars)
@@ -162,8 +164,9 @@ def test_batch_fp32_matches_fp64(W, extra):
     for r in range(nrhs):
         assert abs(its[r] - ref[r]["noiter"]) <= 3
         for c in range(nmap):
-            _close(maps[r][:, c], ref[r]["map"].reshape(-1, nmap)[:, c], FP32_RTOL)
-        _close(aas[r], ref[r]["aa"], FP32_RTOL)
+            parity.close(maps[r][:, c], ref[r]["map"].reshape(-1, nmap)[:, c], FP32_RTOL,
+                         floor=parity.FP32_FLOOR)
+        parity.close(aas[r], ref[r]["aa"], FP32_RTOL, floor=parity.FP32_FLOOR)
     # the cache still gives the float64 answer afterwards
     W.destripe_with_cache(None, d["timestamps"], d["pixels"].copy(), d["pixweights"],
                           sigs[1].copy(), b"")

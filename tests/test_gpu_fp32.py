@@ -2,10 +2,13 @@
 
 The form takes float32 samples and runs the PCG projections on float32
 pointing-pair sums and a float32 copy of the map, with pixel matrices,
-binning, baselines and inner products in float64.  Tolerances: hit counts
-and masks bit-exact (they do not depend on the signal); binned maps,
-destriped maps and baselines within FP32_RTOL of the component's largest
-magnitude of the oracle's solution on the float64 signal.
+binning, baselines, inner products and the reliable updates' true residuals
+in float64.  The oracle solves the same samples in float64 (the float32
+signal widened: identical inputs), so the comparison measures the form's
+arithmetic, not the rounding of the input.  Tolerances: hit counts and
+masks bit-exact (they do not depend on the signal); binned maps, destriped
+maps and baselines within FP32_RTOL per pixel (parity.close with the
+float32 forms' floor, parity.FP32_FLOOR).
 """
 import numpy as np
 import pytest
@@ -30,7 +33,8 @@ def W():
 
 
 def _close(a, b, rtol, what=""):
-    return parity.close(a, b, rtol, what)
+    # float32-TOD form: per pixel above 1e-2 of the largest magnitude
+    return parity.close(a, b, rtol, what, floor=parity.FP32_FLOOR)
 
 
 def _args(pars, x, signal):
@@ -42,9 +46,11 @@ def run_fp32_vs_oracle(W, d, pars=None):
     pars = dict(d["pars"], **(pars or {}))
     do = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
     dp = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
+    sig32 = d["signal"].astype(np.float32)
+    do["signal"] = sig32.astype(np.float64)
     O.destripe(*_args(pars, do, do["signal"]))
     ro = {k: O.result(k) for k in ("map", "binmap", "hits", "mask", "aa")}
-    sig32 = d["signal"].astype(np.float32)
+    ro["scalars"] = O.scalars()
     W.destripe_fp32(None, *_args(pars, dp, sig32))
     rp = {k: W.get_result(k) for k in ("map", "binmap", "hits", "mask", "aa")}
     rp["scalars"] = W.scalars()
@@ -73,8 +79,11 @@ def test_fp32_iqu_matches_fp64_oracle(W, seed):
     # the projections ran over pointing pairs, fewer than the samples
     sc = rp["scalars"]
     assert 0 < sc["pairs"] < d["pixels"].size
-    # float32 projections: the error is far below the tolerance
+    # float32 projections with reliable updates: the error is far below the
+    # tolerance, and the PCG takes about the oracle's iterations
     assert errs["map"] < 1e-5, errs
+    assert abs(sc["noiter"] - ro["scalars"]["noiter"]) <= 3
+    assert sc["reliable_updates"] >= 1
 
 
 def test_fp32_temperature_only(W):
@@ -128,8 +137,10 @@ def test_fp32_device_buffers_match_host(W):
                     dg["signal"].reshape(-1).float(), dg["periods"], dg["npsd"],
                     dg["psdstarts"], dg["psdfreqs"], dg["psdvals"])
     torch.cuda.synchronize()
-    # the binning's float64 atomic sums make any two runs differ by rounding
-    _close(W.get_result("map"), mh, 1e-8)
+    # the binning's float64 atomic sums make any two runs differ by rounding,
+    # which the float32 projections do not damp: the two solves agree to the
+    # accuracy the cglimit gives each (measured 7.5e-7 per pixel)
+    _close(W.get_result("map"), mh, 1e-5)
 
 
 def test_fp32_then_fp64_call_uses_fp64_path(W):

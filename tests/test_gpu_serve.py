@@ -140,7 +140,8 @@ def test_mixed_float32_and_float64_jobs(W):
         assert srv.wait(t) == 2
         np.testing.assert_array_equal(srv.result(t, "hits"), ref["hits"])
         tol = FP32_RTOL if f else SERVE_RTOL
-        _close(srv.result(t, "map"), ref["map"], tol)
-        _close(srv.result(t, "aa"), ref["aa"], tol)
+        floor = parity.FP32_FLOOR if f else parity.FLOOR
+        parity.close(srv.result(t, "map"), ref["map"], tol, floor=floor)
+        parity.close(srv.result(t, "aa"), ref["aa"], tol, floor=floor)
         assert srv.result(t, "scalars")[21] == (1.0 if f else 0.0)
     srv.close()
