@@ -648,7 +648,7 @@ def run_destripe(args, world, rank, local, config, with_e2e=True, with_cpu=True)
             "destripe_device_ms": tim["total_ms"], "setup_ms": tim["setup_ms"],
             "phases_ms_per_iteration": phases, "generate_s": t_gen,
             "setup_marks_ms": marks,
-            "band": {k: sca[k] for k in ("band_rows", "band_transfers", "band_chunks", "nseg")},
+            "band": {k: sca[k] for k in ("band_rows", "band_transfers", "band_chunks", "nseg", "band_guard")},
         }
         if fp32:
             line["precision"] = ("float32 TOD, pointing pairs and map copy in the projections; "

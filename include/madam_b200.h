@@ -84,7 +84,7 @@ int madam_b200_destripe_with_cache_batch_fp32(int comm, long ndet, long nsamp, l
  * returns the job state: 0 queued, 1 running, 2 done, 3 failed, -1 unknown.
  * serve_result_size / serve_result_copy give a done job's "map", "binmap"
  * (float64 [npix][nmap]), "hits", "mask" (int32 [npix]), "aa" (float64
- * [ndet][noba]), "scalars" (float64 [23]), "rr_history" (float64);
+ * [ndet][noba]), "scalars" (float64 [24]), "rr_history" (float64);
  * serve_job_info gives out[0..5] = submit, start and end time (s), samples,
  * PCG iterations, admitted bytes; serve_error the message of a failed job;
  * serve_release frees a finished job; serve_close waits for the running
@@ -146,7 +146,7 @@ int madam_b200_last_error(char *buf, long buflen);
  * matrices at nside_map / nside_cross), "aa", "yba", "nna" (float64
  * [ndet][noba]: baselines, RHS, F^T N^-1 F), "fcov" (float64
  * [npsdtot][nof/2+1]), "invcov" (float64 [npsdtot][nof]), "rr_history"
- * (float64 [niter]), "band_widths" (int64), "scalars" (float64 [23]),
+ * (float64 [niter]), "band_widths" (int64), "scalars" (float64 [24]),
  * "leakmatrix:<d>" (float64 [npix][nmap][nmap], row i column j: the leakage
  * matrix of detector d, write_leakmatrix), the subsets of bin_subsets
  * (smadam.F90:954-1257) as "subsets" (float64 [nsub][4]: pass, survey, detector

@@ -560,6 +560,306 @@ __global__ void __launch_bounds__(64) k_band2_pass_generic(
                 k.last ? nullptr : ws + (long long)(c + 1) * kBand2State, z, nullptr);
 }
 
+// ------------------------------------------------------- guarded solve --
+// One warp (one block) takes 32 guarded chunks, one per lane, and walks them
+// in tiles of TP positions (a multiple of the window R = W + 1, so the
+// register window keeps its slot mapping across tiles).  A lane's positions
+// of one tile are contiguous in memory (ascending forward, descending
+// backward), so the lane stages them with one 1-D bulk copy
+// (cp.async.bulk, completion on an mbarrier, no cluster multicast) into its
+// shared-memory row, the next tile streaming in while the current one is
+// solved; the outputs go to a second row and back with one bulk store per
+// lane (the 16-byte-aligned interior) plus plain stores of at most two edge
+// values.  Bulk copies move whole aligned 16-byte blocks, so a row holds
+// the tile from the 16-byte boundary at or below its lowest address; reading
+// the whole blocks never leaves the pages the tile lies in.  Waits on the
+// mbarrier are bounded: a wait that runs out sets *err and the warp returns.
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes,
+                                          unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void bulk_store(void *dst, const void *src, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst),
+               "r"(smem_u32(src)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read0() {
+  asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait0() {
+  asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+
+// Tiles of about 32 positions, 3 in flight per lane (measured on B200: 2
+// and 4 run alike, tiles of 16 or 64 positions slower).
+template <int W>
+struct GStage {
+  static constexpr int R = W + 1;
+  static constexpr int TP = R * (R > 32 ? 1 : 32 / R);  // tile positions
+  // row length: the tile plus one double of alignment slack on either side,
+  // even (16-byte rows) and 2 mod 16 (consecutive rows start 2 banks apart)
+  static constexpr int L0 = TP + 2;
+  static constexpr int LD = L0 + (((2 - L0) % 16) + 16) % 16;
+  static constexpr int NS = 3;  // tiles in flight (ring of row buffers)
+  static constexpr size_t kSmem = (size_t)NS * 32 * LD * sizeof(double);
+};
+constexpr long kGuardWaitLimit = 1L << 22;
+
+// One step of the recurrence at window slot t (positions ahead of the
+// previous are v[(t - d) mod R]): the older taps d = W..2 summed in two
+// interleaved partial sums, then the tap d = 1.  (DTBSV sums d = w..1 in one
+// sequence; this order differs by rounding only.)
+template <int W>
+__device__ __forceinline__ double guard_step(const double (&K)[W + 1], const double (&v)[W + 1],
+                                             int t, double x, double kinv) {
+  constexpr int R = W + 1;
+  double a0 = x, a1 = 0.0;
+#pragma unroll
+  for (int d = W; d >= 2; --d) {
+    if ((d & 1) == (W & 1)) a0 -= K[d] * v[(t - d + 2 * R) % R];
+    else a1 -= K[d] * v[(t - d + 2 * R) % R];
+  }
+  return ((a0 + a1) - K[1] * v[(t - 1 + 2 * R) % R]) * kinv;
+}
+
+// DIR 0: forward (ascending indices), 1: backward (descending).  Tiles
+// stream through a ring of NS row buffers; each value's output overwrites
+// its input slot (it is not read again), and the row goes back with the bulk
+// store when `in` and `out` share their 16-byte phase at the tile (else with
+// plain stores).
+template <int W, int DIR>
+__global__ void __launch_bounds__(32) k_band2_guard_pass(
+    const PSeg *segs, const GChunk *gc, int c0, int c1, const PRun *runs, const PRun *cruns,
+    const double *tab, const double *in, double *out, int *err) {
+  using G = GStage<W>;
+  constexpr int R = G::R, TP = G::TP, LD = G::LD, NS = G::NS;
+  constexpr int S = DIR == 0 ? 1 : -1;  // index step per position
+  extern __shared__ __align__(16) double gsm[];
+  __shared__ __align__(8) unsigned long long bar[NS];
+  const int lane = threadIdx.x & 31;
+  const int c = c0 + blockIdx.x * 32 + lane;
+  // this lane's chunk: positions t in [0, len) at vector index base + S t,
+  // recurrence position p0 + t; positions below skip are the guard
+  long long base = 0;
+  int len = 0, p0 = 0, skip = 0, run = 0, rend = 0, w = 0;
+  const PRun *rl = DIR == 0 ? runs : cruns;
+  if (c < c1) {
+    const GChunk k = gc[c];
+    const PSeg g = segs[k.seg];
+    w = g.nb - 1;
+    if (DIR == 0) {
+      base = g.k0 + k.ga;
+      len = k.b - k.ga;
+      p0 = k.ga;
+      skip = k.a - k.ga;
+      run = k.run_fg;
+      rend = g.run_off + g.nrun;
+    } else {
+      base = g.k0 + g.n - 1 - k.gp;
+      len = g.n - k.a - k.gp;
+      p0 = k.gp;
+      skip = g.n - k.b - k.gp;
+      run = k.run_bg;
+      rend = g.crun_off + g.ncrun;
+    }
+  }
+  int maxlen = len;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, o));
+  const int ntile = (maxlen + TP - 1) / TP;
+  if (lane == 0) {
+#pragma unroll
+    for (int b = 0; b < NS; ++b) mbar_init(&bar[b], 32);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncwarp();
+  // lowest vector index of tile k's positions [t0, t1) (nt = t1 - t0 > 0)
+  auto tile_lo = [&](int k, int &nt) -> long long {
+    const int t0 = k * TP, t1 = min(len, t0 + TP);
+    nt = t1 - t0;
+    return DIR == 0 ? base + t0 : base - (t1 - 1);
+  };
+  auto issue = [&](int k) {
+    const int b = k % NS;
+    int nt = 0;
+    const long long lo = tile_lo(k, nt);
+    unsigned bytes = 0;
+    const char *src = nullptr;
+    if (nt > 0) {
+      const uintptr_t a0 = (uintptr_t)(in + lo) & ~(uintptr_t)15;
+      const uintptr_t a1 = ((uintptr_t)(in + lo + nt - 1) + 8 + 15) & ~(uintptr_t)15;
+      src = (const char *)a0;
+      bytes = (unsigned)(a1 - a0);
+    }
+    mbar_arrive_tx(&bar[b], bytes);
+    if (bytes) bulk_load(gsm + (b * 32 + lane) * LD, src, bytes, &bar[b]);
+  };
+  double v[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) v[q] = 0.0;
+  double K[W + 1];
+  K[0] = 0.0;
+  double kinv = 0;
+  int next = INT_MAX;
+  auto load = [&](int rr) {
+    const double *E = tab + rl[rr].off;
+#pragma unroll
+    for (int d = 1; d <= W; ++d) K[d] = d <= w ? E[d] : 0.0;
+    kinv = E[w + 1];
+    next = (rr + 1 < rend) ? rl[rr + 1].start : INT_MAX;
+  };
+  if (len > 0) load(run);
+  for (int k = 0; k < NS - 1 && k < ntile; ++k) issue(k);
+  for (int k = 0; k < ntile; ++k) {
+    if (k + NS - 1 < ntile) {
+      // the ring slot of tile k - 1: its bulk store has read it
+      bulk_wait_read0();
+      fence_proxy_async();
+      issue(k + NS - 1);
+    }
+    {
+      const unsigned parity = (unsigned)(k / NS) & 1u;
+      long it = 0;
+      while (!mbar_try_wait(&bar[k % NS], parity)) {
+        if (++it > kGuardWaitLimit) {
+          if (lane == 0) atomicOr(err, 1);
+          bulk_wait0();
+          return;
+        }
+      }
+    }
+    int nt = 0;
+    const long long lo = tile_lo(k, nt);
+    // index i sits at slot lead + (i - lo) of the row (lead: 8-byte offset of
+    // in + lo in its 16-byte block); position t0 + x is index lo + x
+    // forward, lo + nt - 1 - x backward
+    double *row = gsm + ((k % NS) * 32 + lane) * LD;
+    const int lead = nt > 0 ? (int)(((uintptr_t)(in + lo) >> 3) & 1) : 0;
+    double *ip = row + lead + (DIR == 0 ? 0 : nt - 1);
+#pragma unroll 1
+    for (int b0 = 0; b0 < TP; b0 += R) {
+      const int t0 = k * TP + b0;
+      if (t0 >= len) break;
+      const int pb = p0 + t0;
+      if (t0 + R <= len && pb + R <= next) {
+#pragma unroll
+        for (int t = 0; t < R; ++t) {
+          v[t] = guard_step<W>(K, v, t, ip[S * (b0 + t)], kinv);
+          ip[S * (b0 + t)] = v[t];
+        }
+      } else {
+#pragma unroll
+        for (int t = 0; t < R; ++t) {
+          if (t0 + t < len) {
+            const int p = pb + t;
+            if (p >= next) {
+              while (p >= next) {
+                ++run;
+                next = (run + 1 < rend) ? rl[run + 1].start : INT_MAX;
+              }
+              load(run);
+            }
+            v[t] = guard_step<W>(K, v, t, ip[S * (b0 + t)], kinv);
+            ip[S * (b0 + t)] = v[t];
+          }
+        }
+      }
+    }
+    // write the tile's outputs past the guard: positions [max(t0, skip), t1)
+    const int tw0 = max(k * TP, skip), tw1 = min(len, (k + 1) * TP);
+    if (tw1 > tw0) {
+      const long long wlo = DIR == 0 ? base + tw0 : base - (tw1 - 1);
+      const long long whi = DIR == 0 ? base + (tw1 - 1) : base - tw0;
+      const int olead = (int)(((uintptr_t)(out + lo) >> 3) & 1);
+      if (olead != lead) {
+        for (long long i = wlo; i <= whi; ++i) out[i] = row[lead + (i - lo)];
+      } else {
+        // [alo, aend): the written bytes; [ilo, iend): their whole 16-byte
+        // blocks (bulk store); a value in a partly written block is stored
+        // alone (at most one at either end)
+        const uintptr_t alo = (uintptr_t)(out + wlo), aend = (uintptr_t)(out + whi) + 8;
+        const uintptr_t ilo = (alo + 15) & ~(uintptr_t)15, iend = aend & ~(uintptr_t)15;
+        if (alo < ilo) out[wlo] = row[lead + (wlo - lo)];
+        if (aend > iend) out[whi] = row[lead + (whi - lo)];
+        if (iend > ilo) {
+          const long long i0 = (long long)((const double *)ilo - out);
+          fence_proxy_async();
+          bulk_store((void *)ilo, row + lead + (i0 - lo), (unsigned)(iend - ilo));
+        }
+      }
+    }
+    bulk_commit();
+    __syncwarp();
+  }
+  bulk_wait0();
+}
+
+// Guard check: thread (chunk, direction, q) runs the recurrence over the
+// guard from the unit state e_q with zero input and records the largest
+// entry of the state it reaches (a max over non-negative doubles, as bits).
+template <int W>
+__global__ void k_band2_guard_check(const PSeg *segs, const GChunk *gc, int c0, int c1,
+                                    const PRun *runs, const PRun *cruns, const double *tab,
+                                    unsigned long long *worst) {
+  constexpr int WS = W > 0 ? W : kRing - 1;
+  const long long gid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long c = c0 + gid / (2 * WS);
+  const int rem = (int)(gid % (2 * WS));
+  const int dir = rem / WS, qq = rem % WS;
+  if (c >= c1) return;
+  const GChunk k = gc[c];
+  const PSeg g = segs[k.seg];
+  const int w = g.nb - 1;
+  if (qq >= w) return;
+  const int p0 = dir == 0 ? k.ga : k.gp;
+  const int p1 = dir == 0 ? k.a : g.n - k.b;
+  if (p1 <= p0) return;
+  double unit[WS], res[WS];
+  for (int i = 0; i < w; ++i) unit[i] = (i == qq) ? 1.0 : 0.0;
+  if (dir == 0)
+    recur<W, false, false>(w, fwd_seq(g, runs, tab), k.run_fg, p0, p1, nullptr, unit, nullptr,
+                           res);
+  else
+    recur<W, false, false>(w, bwd_seq(g, cruns, tab), k.run_bg, p0, p1, nullptr, unit, nullptr,
+                           res);
+  double m = 0;
+  for (int i = 0; i < w; ++i) m = fmax(m, fabs(res[i]));
+  if (!(m <= 1e300)) m = 1e300;  // a NaN or an overflow fails the check
+  atomicMax(worst + c, (unsigned long long)__double_as_longlong(m));
+}
+
 // Transfer matrices: column q of T = response of the tail to the unit state
 // e_q with zero input; one thread per (matrix, q).
 template <int W>
@@ -889,6 +1189,100 @@ void band2_solve(cudaStream_t st, const PSeg *segs, int nseg, const PChunk *ch, 
   passes(1);
   scans(1);
   passes(2);
+}
+
+void band2_guard_check(cudaStream_t st, const PSeg *segs, const GChunk *gc, const int *cls_w,
+                       const int *gcls_begin, int ncls, const PRun *runs, const PRun *cruns,
+                       const double *tab, double *worst) {
+  const int n = gcls_begin[ncls];
+  if (n == 0) return;
+  MADAM_CUDA(cudaMemsetAsync(worst, 0, (size_t)n * sizeof(double), st));
+  for (int i = 0; i < ncls; ++i) {
+    const int c0 = gcls_begin[i], c1 = gcls_begin[i + 1];
+    if (c1 <= c0) continue;
+    const int W = cls_w[i];
+    const long long nthr = (long long)(c1 - c0) * 2 * (W > 0 ? W : kRing - 1);
+    const unsigned grid = (unsigned)((nthr + 63) / 64);
+    unsigned long long *wb = (unsigned long long *)worst;
+    switch (W) {
+#define MADAM_BAND2_CASE(X)                                                                  \
+  case X:                                                                                    \
+    MADAM_LAUNCH(k_band2_guard_check<X>, grid, 64, 0, st, segs, gc, c0, c1, runs, cruns, tab, \
+                 wb);                                                                        \
+    break;
+      MADAM_BAND2_CASE(1)
+      MADAM_BAND2_CASE(2)
+      MADAM_BAND2_CASE(4)
+      MADAM_BAND2_CASE(8)
+      MADAM_BAND2_CASE(9)
+      MADAM_BAND2_CASE(12)
+      MADAM_BAND2_CASE(16)
+      MADAM_BAND2_CASE(19)
+      MADAM_BAND2_CASE(24)
+      MADAM_BAND2_CASE(29)
+      MADAM_BAND2_CASE(32)
+#undef MADAM_BAND2_CASE
+      default:
+        MADAM_LAUNCH(k_band2_guard_check<0>, grid, 64, 0, st, segs, gc, c0, c1, runs, cruns,
+                     tab, wb);
+        break;
+    }
+  }
+}
+
+namespace {
+template <int W>
+void launch_guard(cudaStream_t st, const PSeg *segs, const GChunk *gc, int c0, int c1,
+                  const PRun *runs, const PRun *cruns, const double *tab, int dir,
+                  const double *in, double *out, int *err) {
+  static bool attr = false;
+  if (!attr) {
+    MADAM_CUDA(cudaFuncSetAttribute(k_band2_guard_pass<W, 0>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)GStage<W>::kSmem));
+    MADAM_CUDA(cudaFuncSetAttribute(k_band2_guard_pass<W, 1>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)GStage<W>::kSmem));
+    attr = true;
+  }
+  const unsigned grid = (unsigned)((c1 - c0 + 31) / 32);
+  if (dir == 0)
+    MADAM_LAUNCH((k_band2_guard_pass<W, 0>), grid, 32, GStage<W>::kSmem, st, segs, gc, c0, c1,
+                 runs, cruns, tab, in, out, err);
+  else
+    MADAM_LAUNCH((k_band2_guard_pass<W, 1>), grid, 32, GStage<W>::kSmem, st, segs, gc, c0, c1,
+                 runs, cruns, tab, in, out, err);
+}
+}  // namespace
+
+void band2_solve_guarded(cudaStream_t st, const PSeg *segs, const GChunk *gc, const int *cls_w,
+                         const int *gcls_begin, int ncls, const PRun *runs, const PRun *cruns,
+                         const double *tab, const double *r, double *y, double *z, int *err) {
+  for (int dir = 0; dir < 2; ++dir)
+    for (int i = 0; i < ncls; ++i) {
+      const int c0 = gcls_begin[i], c1 = gcls_begin[i + 1];
+      if (c1 <= c0) continue;
+      const double *in = dir == 0 ? r : y;
+      double *out = dir == 0 ? y : z;
+      switch (cls_w[i]) {
+#define MADAM_BAND2_CASE(X) \
+  case X: launch_guard<X>(st, segs, gc, c0, c1, runs, cruns, tab, dir, in, out, err); break;
+        MADAM_BAND2_CASE(1)
+        MADAM_BAND2_CASE(2)
+        MADAM_BAND2_CASE(4)
+        MADAM_BAND2_CASE(8)
+        MADAM_BAND2_CASE(9)
+        MADAM_BAND2_CASE(12)
+        MADAM_BAND2_CASE(16)
+        MADAM_BAND2_CASE(19)
+        MADAM_BAND2_CASE(24)
+        MADAM_BAND2_CASE(29)
+        MADAM_BAND2_CASE(32)
+#undef MADAM_BAND2_CASE
+        default:
+          fail("band2_solve_guarded: band width class without registers");
+      }
+    }
 }
 
 }  // namespace madam

@@ -42,6 +42,21 @@ struct PTrans {
   long long off;  // offset of the w x w matrix
 };
 
+// A chunk of the guarded solve: rows [a, b) of segment seg.  The forward
+// recurrence starts from a zero state at row ga <= a (in forward run run_fg)
+// and writes rows a .. b-1; the backward one starts at backward position
+// gp <= n - b (in backward run run_bg) and writes positions n-b .. n-a-1
+// (rows b-1 .. a).  The guard (a - ga, n - b - gp positions) is checked at
+// set-up: the response of the first written position's state to a unit
+// state at the guard start is below kBand2GuardTol in every entry, so the
+// zero start differs from the true state by less than that relative amount.
+struct GChunk {
+  int seg, a, b;
+  int ga, run_fg, run_fa;  // forward guard start, runs containing ga and a
+  int gp, run_bg, run_bb;  // backward guard start, runs containing gp and n - b
+};
+constexpr double kBand2GuardTol = 1e-20;
+
 constexpr int kBand2MaxWidth = 128;
 constexpr int kBand2State = 128;  // doubles per chunk state slot (>= w)
 
@@ -68,5 +83,20 @@ void band2_solve(cudaStream_t st, const PSeg *segs, int nseg, const PChunk *ch, 
                  double *work_s);
 // Smallest compiled register width >= w (0 when w needs the generic path).
 int band2_class_width(int w);
+
+// Guard check: worst[c] = the largest entry, over both directions, of the
+// response at guarded chunk c's first written position to a unit state at its
+// guard start (0 for chunks without a guard).  Width class i: guarded chunks
+// [gcls_begin[i], gcls_begin[i + 1]) with w <= cls_w[i] (host arrays).
+void band2_guard_check(cudaStream_t st, const PSeg *segs, const GChunk *gc, const int *cls_w,
+                       const int *gcls_begin, int ncls, const PRun *runs, const PRun *cruns,
+                       const double *tab, double *worst);
+// Solve L L^T z = r on every factored segment with the guarded chunks: one
+// forward launch (r -> y) and one backward launch (y -> z) per width class;
+// no state propagation.  Register widths only (cls_w[i] > 0).  *err (device)
+// becomes nonzero if a staging wait ran out (the result is then invalid).
+void band2_solve_guarded(cudaStream_t st, const PSeg *segs, const GChunk *gc, const int *cls_w,
+                         const int *gcls_begin, int ncls, const PRun *runs, const PRun *cruns,
+                         const double *tab, const double *r, double *y, double *z, int *err);
 
 }  // namespace madam

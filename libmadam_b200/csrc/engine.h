@@ -193,6 +193,10 @@ class Engine {
   void filter_spectra(const std::vector<std::pair<long, int>> &tasks, long nh);
   void build_filter_finish();
   void construct_preconditioner();
+  void build_guarded_chunks(const std::vector<PRun> &pruns, const std::vector<PRun> &cruns);
+  std::vector<GChunk> make_gchunks(int Cg, int G, std::vector<int> &cls_begin,
+                                   std::vector<int> &seg_off) const;
+  int guard_chunk_len(long long npos) const;
   void iterate();
   void finalize(bool first_call);
   void writeback_host();
@@ -222,6 +226,9 @@ class Engine {
   std::vector<PChunk> band2_ch_h_;
   DevBuf<PSeg> p2segs_b_;
   DevBuf<PChunk> p2ch_b_;
+  DevBuf<GChunk> p2gc_b_;
+  std::vector<int> band2_gcls_begin_b_;
+  DevBuf<double> p2y_b_;
   DevBuf<int> p2tf_b_, p2tb_b_;
   DevBuf<double> p2wp_b_, p2ws_b_;
   std::vector<int> band2_cls_begin_b_, band2_cls_seg_b_;
@@ -370,6 +377,17 @@ class Engine {
   long band2_ntrans_ = 0;
   int band2_chunk_ = 0;
   std::vector<int> band2_cls_w_, band2_cls_begin_, band2_cls_seg_;
+  // guarded solve (band2_solve_guarded): chunks of band2_gchunk_ rows with
+  // guards of band2_guard_ positions, when every chunk's guard checks out
+  bool band2_guarded_ = false;
+  int band2_guard_ = 0, band2_gchunk_ = 0;
+  std::vector<GChunk> band2_gch_h_;
+  std::vector<PRun> band2_pruns_h_, band2_cruns_h_;
+  std::vector<int> band2_gcls_begin_, band2_gseg_off_;
+  DevBuf<GChunk> p2gc_;
+  DevBuf<double> p2y_;  // forward solution L^-1 r, full baseline vector
+  DevBuf<int> band2_err_;  // a staging wait of the guarded solve ran out
+  void check_band_err();
   long n_band_fail_ = 0;
   std::unique_ptr<FFTPlan> fft_;
   std::future<void> filter_job_;  // host spectra of build_filter

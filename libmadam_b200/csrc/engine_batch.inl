@@ -47,6 +47,34 @@ void Engine::build_batch_tables() {
   }
   band2_cls_begin_b_.push_back((int)ch.size());
   band2_cls_seg_b_.push_back((int)ps.size());
+  // the guarded chunks, replicated the same way (segment r * nseg_class + s),
+  // at the chunk length of the whole batch's positions
+  if (band2_guarded_) {
+    long long npos = 0;
+    for (const PSeg &q : band2_pseg_h_) npos += q.n;
+    std::vector<int> gb1, soff;
+    const std::vector<GChunk> one =
+        make_gchunks(guard_chunk_len(npos * nrhs_), band2_guard_, gb1, soff);
+    std::vector<GChunk> gcs;
+    band2_gcls_begin_b_.clear();
+    for (size_t i = 0; i + 1 < band2_cls_seg_.size(); ++i) {
+      band2_gcls_begin_b_.push_back((int)gcs.size());
+      const int sbase = band2_cls_seg_b_[i];
+      const int ns = band2_cls_seg_[i + 1] - band2_cls_seg_[i];
+      for (long r = 0; r < nrhs_; ++r)
+        for (int s = band2_cls_seg_[i]; s < band2_cls_seg_[i + 1]; ++s)
+          for (int c = soff[s]; c < soff[s + 1]; ++c) {
+            GChunk k = one[c];
+            k.seg = sbase + (int)r * ns + (s - band2_cls_seg_[i]);
+            gcs.push_back(k);
+          }
+    }
+    band2_gcls_begin_b_.push_back((int)gcs.size());
+    p2gc_b_.alloc(std::max<size_t>(1, gcs.size()));
+    if (!gcs.empty())
+      MADAM_CUDA(cudaMemcpyAsync(p2gc_b_.get(), gcs.data(), gcs.size() * sizeof(GChunk),
+                                 cudaMemcpyHostToDevice, st_));
+  }
   p2nseg_b_ = (int)ps.size();
   p2nch_b_ = (int)ch.size();
   if (!ps.empty()) {
@@ -102,10 +130,17 @@ void Engine::apply_preconditioner_batch(const double *r, double *z) {
     if (nfs > 0) fft_->convolve(st_, filt_segs_b_d_.get(), nfs, fprec_.get(), r, z);
     return;
   }
-  band2_solve(st_, p2segs_b_.get(), p2nseg_b_, p2ch_b_.get(), p2nch_b_, p2tf_b_.get(),
-              p2tb_b_.get(), band2_cls_w_.data(), band2_cls_begin_b_.data(),
-              band2_cls_seg_b_.data(), (int)band2_cls_w_.size(), p2runs_.get(), p2cruns_.get(),
-              p2rows_.get(), p2T_.get(), r, z, p2wp_b_.get(), p2ws_b_.get());
+  if (band2_guarded_) {
+    p2y_b_.alloc(std::max<long long>(1, nt));
+    band2_solve_guarded(st_, p2segs_b_.get(), p2gc_b_.get(), band2_cls_w_.data(),
+                        band2_gcls_begin_b_.data(), (int)band2_cls_w_.size(), p2runs_.get(),
+                        p2cruns_.get(), p2rows_.get(), r, p2y_b_.get(), z, band2_err_.get());
+  } else {
+    band2_solve(st_, p2segs_b_.get(), p2nseg_b_, p2ch_b_.get(), p2nch_b_, p2tf_b_.get(),
+                p2tb_b_.get(), band2_cls_w_.data(), band2_cls_begin_b_.data(),
+                band2_cls_seg_b_.data(), (int)band2_cls_w_.size(), p2runs_.get(),
+                p2cruns_.get(), p2rows_.get(), p2T_.get(), r, z, p2wp_b_.get(), p2ws_b_.get());
+  }
   for (long k = 0; k < nrhs_; ++k) {
     band_solve(st_, band_segs_d_.get(), (int)band_segs_.size(), band_.get(), r + k * nb,
                z + k * nb);
@@ -398,6 +433,7 @@ void Engine::iterate_batch() {
                  scalb_.get(), 0, actb_.get());
   }
   MADAM_CUDA(cudaStreamSynchronize(st_));
+  check_band_err();
   timings.iterate_ms = now_ms() - t0;
 }
 

@@ -1664,6 +1664,7 @@ void Engine::construct_preconditioner() {
   band2_rows_ = nunique;
   band2_ntrans_ = (long)trans.size();
   band2_chunk_ = C;
+  build_guarded_chunks(pruns, cruns);
   // plain column store for the wide bands
   long long total = 0;
   band_segs_.clear();
@@ -1939,6 +1940,140 @@ void Engine::true_residual(const double *x, const double *b, double *r) {
   ++n_reliable_;
 }
 
+// Chunks of the guarded band solve.  The factor's rows settle to a fixed
+// point whose recurrence forgets its state geometrically (at the 1/f priors
+// of the benchmarked workloads by 1e-17 within about 200 positions), so a
+// chunk can start its recurrence a guard of G positions early from a zero
+// state instead of waiting for the true state: every chunk is independent
+// and the solve is two launches, forward and backward, without transfer
+// matrices or state scans.  The guard is checked at set-up for every chunk
+// start a multiple of kGuardGrain rows (and every backward end the same
+// distance from the segment end), so that chunks of any multiple of
+// kGuardGrain rows are covered: the state a unit state at the guard start
+// leaves at the chunk's first written position stays below kBand2GuardTol.
+// G = 256, 512, 1024 are tried; if none passes everywhere (or a band is
+// wider than the register classes) the state-scan solve stays in use.
+// MADAM_B200_BAND_SOLVE=scan selects the state-scan solve.
+namespace {
+constexpr int kGuardGrain = 128;
+}  // namespace
+
+std::vector<GChunk> Engine::make_gchunks(int Cg, int G, std::vector<int> &cls_begin,
+                                         std::vector<int> &seg_off) const {
+  auto find = [](const std::vector<PRun> &v, int lo, int hi, int pos) {
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      if (v[mid].start <= pos) lo = mid;
+      else hi = mid - 1;
+    }
+    return lo;
+  };
+  const std::vector<PSeg> &pseg = band2_pseg_h_;
+  const std::vector<PRun> &pr = band2_pruns_h_, &cr = band2_cruns_h_;
+  std::vector<GChunk> gcs;
+  cls_begin.clear();
+  seg_off.clear();
+  for (size_t ci = 0; ci + 1 < band2_cls_seg_.size(); ++ci) {
+    cls_begin.push_back((int)gcs.size());
+    for (int si = band2_cls_seg_[ci]; si < band2_cls_seg_[ci + 1]; ++si) {
+      const PSeg &q = pseg[si];
+      const int n = q.n;
+      seg_off.push_back((int)gcs.size());
+      for (int a = 0; a < n; a += Cg) {
+        GChunk k;
+        k.seg = si;
+        k.a = a;
+        k.b = std::min(n, a + Cg);
+        k.ga = std::max(0, a - G);
+        k.run_fg = find(pr, q.run_off, q.run_off + q.nrun - 1, k.ga);
+        k.run_fa = find(pr, q.run_off, q.run_off + q.nrun - 1, k.a);
+        k.gp = std::max(0, n - k.b - G);
+        k.run_bg = find(cr, q.crun_off, q.crun_off + q.ncrun - 1, k.gp);
+        k.run_bb = find(cr, q.crun_off, q.crun_off + q.ncrun - 1, n - k.b);
+        gcs.push_back(k);
+      }
+    }
+  }
+  cls_begin.push_back((int)gcs.size());
+  seg_off.push_back((int)gcs.size());
+  return gcs;
+}
+
+// chunk length for npos positions in all: a multiple of kGuardGrain rows
+// giving at most one resident wave of the guarded kernel (a warp of 32
+// chunks per block, about 8 blocks per SM at its shared-memory size), so
+// that no second wave's tail idles the SMs; up to 4096 rows
+int Engine::guard_chunk_len(long long npos) const {
+  const long long maxchains = 148LL * 8 * 32;
+  const long long units = (npos + kGuardGrain * maxchains - 1) / (kGuardGrain * maxchains);
+  return (int)std::min<long long>(4096, kGuardGrain * std::max<long long>(1, units));
+}
+
+void Engine::build_guarded_chunks(const std::vector<PRun> &pruns,
+                                  const std::vector<PRun> &cruns) {
+  band2_guarded_ = false;
+  band2_gch_h_.clear();
+  band2_gcls_begin_.clear();
+  band2_gseg_off_.clear();
+  p2gc_.reset();
+  const std::vector<PSeg> &pseg = band2_pseg_h_;
+  if (pseg.empty()) return;
+  const char *mode = std::getenv("MADAM_B200_BAND_SOLVE");
+  if (mode && std::string(mode) == "scan") return;
+  for (int W : band2_cls_w_)
+    if (W == 0) return;
+  band2_pruns_h_ = pruns;
+  band2_cruns_h_ = cruns;
+  DevBuf<double> worst;
+  DevBuf<GChunk> dgc;
+  for (int G = 256; G <= 1024; G *= 2) {
+    std::vector<int> gb, soff;
+    std::vector<GChunk> gcs = make_gchunks(kGuardGrain, G, gb, soff);
+    if (gcs.empty()) return;
+    dgc.alloc(gcs.size());
+    MADAM_CUDA(cudaMemcpyAsync(dgc.get(), gcs.data(), gcs.size() * sizeof(GChunk),
+                               cudaMemcpyHostToDevice, st_));
+    worst.alloc(gcs.size());
+    band2_guard_check(st_, p2segs_.get(), dgc.get(), band2_cls_w_.data(), gb.data(),
+                      (int)band2_cls_w_.size(), p2runs_.get(), p2cruns_.get(), p2rows_.get(),
+                      worst.get());
+    std::vector<double> wh(gcs.size());
+    MADAM_CUDA(cudaMemcpyAsync(wh.data(), worst.get(), wh.size() * sizeof(double),
+                               cudaMemcpyDeviceToHost, st_));
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    bool ok = true;
+    for (double v : wh) ok = ok && v < kBand2GuardTol;
+    if (!ok) continue;
+    long long npos = 0;
+    for (const PSeg &q : pseg) npos += q.n;
+    band2_guarded_ = true;
+    band2_guard_ = G;
+    band2_err_.alloc(1);
+    band2_err_.zero(st_);
+    band2_gchunk_ = guard_chunk_len(npos);
+    band2_gch_h_ = make_gchunks(band2_gchunk_, G, band2_gcls_begin_, band2_gseg_off_);
+    p2gc_.alloc(band2_gch_h_.size());
+    MADAM_CUDA(cudaMemcpyAsync(p2gc_.get(), band2_gch_h_.data(),
+                               band2_gch_h_.size() * sizeof(GChunk), cudaMemcpyHostToDevice,
+                               st_));
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    return;
+  }
+}
+
+// The guarded band solve's staging waits are bounded; one that ran out
+// leaves a flag (never seen in practice), checked once per solve.
+void Engine::check_band_err() {
+  if (!band2_guarded_ || !band2_err_.get()) return;
+  int e = 0;
+  MADAM_CUDA(cudaMemcpyAsync(&e, band2_err_.get(), sizeof e, cudaMemcpyDeviceToHost, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  if (e) {
+    band2_err_.zero(st_);
+    fail("band preconditioner: a staging wait of the guarded solve ran out");
+  }
+}
+
 void Engine::cg_preconditioner_segments(const double *r, double *z) {
   if (cg_prec_segs_.empty()) return;
   const long long nb = (long long)ndet_ * noba_short_;
@@ -2007,11 +2142,18 @@ void Engine::apply_preconditioner(const double *r, double *z) {
       fft_->convolve(st_, filt_segs_d_.get(), (long)filt_segs_.size(), fprec_.get(), r, z);
     return;
   }
-  band2_solve(st_, p2segs_.get(), p2nseg_, p2ch_.get(), p2nch_, p2tf_.get(), p2tb_.get(),
-              band2_cls_w_.data(),
-              band2_cls_begin_.data(), band2_cls_seg_.data(), (int)band2_cls_w_.size(),
-              p2runs_.get(), p2cruns_.get(), p2rows_.get(), p2T_.get(), r, z, p2wp_.get(),
-              p2ws_.get());
+  if (band2_guarded_) {
+    p2y_.alloc(std::max<long long>(1, nb));
+    band2_solve_guarded(st_, p2segs_.get(), p2gc_.get(), band2_cls_w_.data(),
+                        band2_gcls_begin_.data(), (int)band2_cls_w_.size(), p2runs_.get(),
+                        p2cruns_.get(), p2rows_.get(), r, p2y_.get(), z, band2_err_.get());
+  } else {
+    band2_solve(st_, p2segs_.get(), p2nseg_, p2ch_.get(), p2nch_, p2tf_.get(), p2tb_.get(),
+                band2_cls_w_.data(),
+                band2_cls_begin_.data(), band2_cls_seg_.data(), (int)band2_cls_w_.size(),
+                p2runs_.get(), p2cruns_.get(), p2rows_.get(), p2T_.get(), r, z, p2wp_.get(),
+                p2ws_.get());
+  }
   band_solve(st_, band_segs_d_.get(), (int)band_segs_.size(), band_.get(), r, z);
   cg_preconditioner_segments(r, z);
 }
@@ -2115,6 +2257,7 @@ void Engine::iterate() {
     MADAM_LAUNCH(k_update_p, grid_for(nb), 256, 0, st_, p_.get(), z_.get(), pw_.get(), bwv,
                  nb, scal_.get(), 0);
   }
+  check_band_err();
   // iterate_a leaves wamap holding the last A.p map (collect_map + ccmultiply
   // on wamap, smadam_routines.f90:818-822); destripe_with_cache adds the new
   // binned map onto it (smadam.F90:719-732)
@@ -2519,7 +2662,7 @@ long Engine::result_size(const std::string &name) {
   if (name == "invcov") return (long)invcov_host_.size();
   if (name == "rr_history") return (long)rr_history.size();
   if (name == "band_widths") return (long)band_widths_.size();
-  if (name == "scalars") return 23;
+  if (name == "scalars") return 24;
   if (name == "timings") return 9;
   if (name == "setup_marks") return kSetupMarks;
   if (name == "map_batch" || name == "binmap_batch") return nrhs_ * npm * nmap_;
@@ -2657,7 +2800,7 @@ void Engine::result_copy(const std::string &name, void *dst, long nbytes) {
     std::memcpy(dst, band_widths_.data(), sz * sizeof(long));
   } else if (name == "scalars") {
     need(sizeof(double));
-    const double v[23] = {(double)noiter, rrinit, rr_final, (double)nof_,
+    const double v[24] = {(double)noiter, rrinit, rr_final, (double)nof_,
                           (double)band_widths_.size(), (double)n_band_fail_, timings.iterate_ms,
                           timings.total_ms, (double)nmap_, (double)noba_short_,
                           (double)(12 * par_.nside_map * par_.nside_map), (double)nruns_,
@@ -2665,7 +2808,7 @@ void Engine::result_copy(const std::string &name, void *dst, long nbytes) {
                           (double)cg_prec_segs_.size(), (double)band2_rows_,
                           (double)band2_ntrans_, (double)p2nch_, (double)csr_nvalid_,
                           (double)(use_pairs_ ? npairs_ : 0), fp32_ ? 1.0 : 0.0,
-                          (double)n_reliable_};
+                          (double)n_reliable_, band2_guarded_ ? (double)band2_guard_ : 0.0};
     std::memcpy(dst, v, sizeof v);
   } else if (name == "setup_marks") {
     need(sizeof(double));
@@ -2732,6 +2875,7 @@ void Engine::bench_iterations(int warmup, int iters, std::vector<double> &out) {
   MADAM_CUDA(cudaEventElapsedTime(&total, a, b));
   cudaEventDestroy(a);
   cudaEventDestroy(b);
+  check_band_err();
   // per-phase breakdown on separate iterations
   double sc = 0, fi = 0, ga = 0, pr = 0, up = 0;
   const int nbrk = std::max(1, std::min(iters, 5));

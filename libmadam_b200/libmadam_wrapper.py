@@ -320,7 +320,7 @@ def scalars():
     keys = ["noiter", "rrinit", "rr_final", "nof", "n_band", "n_band_fail", "iterate_ms",
             "total_ms", "nmap", "noba_short", "npix_map", "nruns", "nwork", "nloc", "nseg",
             "n_cg_prec", "band_rows", "band_transfers", "band_chunks", "scatter_samples",
-            "pairs", "fp32", "reliable_updates"]
+            "pairs", "fp32", "reliable_updates", "band_guard"]
     return dict(zip(keys, get_result("scalars").tolist()))
 
 

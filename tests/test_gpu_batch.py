@@ -144,11 +144,12 @@ FP32_RTOL = 1e-4
 @pytest.mark.parametrize("extra", [dict(), dict(temperature_only=True)])
 def test_batch_fp32_matches_fp64(W, extra):
     """The FP32-TOD batched form against one-at-a-time float64 solves of the
-    same samples: maps and baselines within FP32_RTOL per pixel (with the
-    float32 forms' floor, parity.FP32_FLOOR)."""
+    same samples, both to parity.CONVERGED_CGLIMIT: maps and baselines within
+    FP32_RTOL per pixel."""
     cfg = syn.small_config(seed=45)
     d = syn.to_numpy(syn.generate(cfg, nnz=1 if extra.get("temperature_only") else None))
-    pars = dict(d["pars"], mcmode=True, **extra)
+    # both solved to the converged cglimit: the difference is the arithmetic's
+    pars = dict(d["pars"], mcmode=True, cglimit=parity.CONVERGED_CGLIMIT, iter_max=2000, **extra)
     nrhs = 4
     # realisations that float32 holds exactly: both sides solve the same data
     sigs = [s.astype(np.float32).astype(np.float64) for s in _realisations(d, nrhs)]
@@ -162,11 +163,10 @@ def test_batch_fp32_matches_fp64(W, extra):
     aas = W.get_result("aa_batch").reshape(nrhs, -1)
     its = W.get_result("noiter_batch")
     for r in range(nrhs):
-        assert abs(its[r] - ref[r]["noiter"]) <= 3
+        assert its[r] <= 2.5 * ref[r]["noiter"] + 3  # converges, in more steps
         for c in range(nmap):
-            parity.close(maps[r][:, c], ref[r]["map"].reshape(-1, nmap)[:, c], FP32_RTOL,
-                         floor=parity.FP32_FLOOR)
-        parity.close(aas[r], ref[r]["aa"], FP32_RTOL, floor=parity.FP32_FLOOR)
+            _close(maps[r][:, c], ref[r]["map"].reshape(-1, nmap)[:, c], FP32_RTOL)
+        _close(aas[r], ref[r]["aa"], FP32_RTOL)
     # the cache still gives the float64 answer afterwards
     W.destripe_with_cache(None, d["timestamps"], d["pixels"].copy(), d["pixweights"],
                           sigs[1].copy(), b"")

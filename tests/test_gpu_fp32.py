@@ -4,11 +4,12 @@ The form takes float32 samples and runs the PCG projections on float32
 pointing-pair sums and a float32 copy of the map, with pixel matrices,
 binning, baselines, inner products and the reliable updates' true residuals
 in float64.  The oracle solves the same samples in float64 (the float32
-signal widened: identical inputs), so the comparison measures the form's
-arithmetic, not the rounding of the input.  Tolerances: hit counts and
-masks bit-exact (they do not depend on the signal); binned maps, destriped
-maps and baselines within FP32_RTOL per pixel (parity.close with the
-float32 forms' floor, parity.FP32_FLOOR).
+signal widened: identical inputs), and both solve to
+parity.CONVERGED_CGLIMIT, so the comparison measures the form's arithmetic,
+not the rounding of the input or the truncation of the solve.  Tolerances:
+hit counts and masks bit-exact (they do not depend on the signal); binned
+maps, destriped maps and baselines within FP32_RTOL per pixel
+(parity.close).
 """
 import numpy as np
 import pytest
@@ -33,8 +34,7 @@ def W():
 
 
 def _close(a, b, rtol, what=""):
-    # float32-TOD form: per pixel above 1e-2 of the largest magnitude
-    return parity.close(a, b, rtol, what, floor=parity.FP32_FLOOR)
+    return parity.close(a, b, rtol, what)
 
 
 def _args(pars, x, signal):
@@ -43,7 +43,7 @@ def _args(pars, x, signal):
 
 
 def run_fp32_vs_oracle(W, d, pars=None):
-    pars = dict(d["pars"], **(pars or {}))
+    pars = dict(d["pars"], cglimit=parity.CONVERGED_CGLIMIT, iter_max=2000, **(pars or {}))
     do = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
     dp = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in d.items()}
     sig32 = d["signal"].astype(np.float32)
@@ -79,10 +79,10 @@ def test_fp32_iqu_matches_fp64_oracle(W, seed):
     # the projections ran over pointing pairs, fewer than the samples
     sc = rp["scalars"]
     assert 0 < sc["pairs"] < d["pixels"].size
-    # float32 projections with reliable updates: the error is far below the
-    # tolerance, and the PCG takes about the oracle's iterations
+    # float32 projections with reliable updates, both solves converged: the
+    # error is far below the tolerance
     assert errs["map"] < 1e-5, errs
-    assert abs(sc["noiter"] - ro["scalars"]["noiter"]) <= 3
+    assert sc["noiter"] <= 2.5 * ro["scalars"]["noiter"] + 3  # converges, in more steps
     assert sc["reliable_updates"] >= 1
 
 
@@ -140,7 +140,7 @@ def test_fp32_device_buffers_match_host(W):
     # the binning's float64 atomic sums make any two runs differ by rounding,
     # which the float32 projections do not damp: the two solves agree to the
     # accuracy the cglimit gives each (measured 7.5e-7 per pixel)
-    _close(W.get_result("map"), mh, 1e-5)
+    parity.close(W.get_result("map"), mh, 1e-5, floor=parity.FP32_FLOOR)
 
 
 def test_fp32_then_fp64_call_uses_fp64_path(W):

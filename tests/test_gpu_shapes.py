@@ -12,15 +12,16 @@ shapes at sizes the oracle solves in seconds:
   4 detectors x 2^22 samples against the float64 oracle on the same
   (float32) samples;
 * the batched Monte Carlo form (nside 512, base_first 1 s, per-detector fknee
-  in 0.02-0.2 Hz): 8 noise realisations of 4 detectors x 2^20 samples, float64
-  and float32 batches, each realisation against the oracle's cached solve;
+  in 0.02-0.2 Hz): noise realisations of 4 detectors x 2^20 samples, a
+  float64 batch of 8 and a float32 batch of 4, each realisation against the
+  oracle's cached solve;
 * baselines longer than the warp-chunk gather takes: base_first 5 s and 20 s
   at 100 Hz (500- and 2000-sample baselines, the tiled and the per-baseline
   map-to-baseline kernels).
 
 Tolerances as in the other parity tests, per pixel (parity.close): float64
-maps and baselines 1e-6, float32-TOD 1e-4 (with the float32 forms' floor);
-hits and masks bit-exact.
+maps and baselines 1e-6, float32-TOD 1e-4 (both sides solved to
+parity.CONVERGED_CGLIMIT); hits and masks bit-exact.
 """
 import numpy as np
 import pytest
@@ -101,15 +102,31 @@ def test_precision_form_workload_shape(W):
     d = _data(cfg)
     sig32 = d["signal"].astype(np.float32)
     d["signal"] = sig32.astype(np.float64)  # the oracle solves the same samples
-    ro = _oracle(d, d["pars"])
+    pars = dict(d["pars"], cglimit=parity.CONVERGED_CGLIMIT)  # both converged
+    ro = _oracle(d, pars)
     dp = _copy(d)
-    W.destripe_fp32(None, *_args(d["pars"], dp, sig32))
+    W.destripe_fp32(None, *_args(pars, dp, sig32))
     rp = {k: W.get_result(k) for k in ("map", "binmap", "hits", "mask", "aa")}
     sc = W.scalars()
     assert sc["fp32"] == 1.0 and sc["pairs"] > 0
     np.testing.assert_array_equal(dp["pixels"], ro["pixels"])
-    _check(rp, ro, 3, FP32_RTOL, BIN_RTOL, parity.FP32_FLOOR)
-    assert abs(sc["noiter"] - ro["scalars"]["noiter"]) <= 3
+    _check(rp, ro, 3, FP32_RTOL, BIN_RTOL)
+    assert sc["noiter"] <= 2.5 * ro["scalars"]["noiter"] + 3  # converges, in more steps
+
+
+def _oracle_cached(d, pars, cache_sig, sigs, ndet):
+    """The oracle's cached solve of every realisation, each right after the
+    caching call (what the batch reproduces)."""
+    ref = []
+    for s in sigs:
+        O.clear_caches()
+        do = _copy(d)
+        O.destripe(*_args(pars, do, cache_sig.copy()))
+        O.destripe_with_cache(d["timestamps"], d["pixels"].copy(), d["pixweights"],
+                              s.reshape(-1).copy(), ndet)
+        ref.append(dict(map=O.result("map"), aa=O.result("aa"), noiter=O.scalars()["noiter"]))
+    O.clear_caches()
+    return ref
 
 
 def test_batched_monte_carlo_workload_shape(W):
@@ -120,41 +137,34 @@ def test_batched_monte_carlo_workload_shape(W):
     # realisations that float32 holds exactly, so that the float64 and the
     # float32 batch and the oracle all solve the same samples
     sigs = syn.noise_realisations(cfg, nrhs + 1, device="cuda").float().double().cpu().numpy()
-    pars = dict(d["pars"], mcmode=True)
     cache_sig = sigs[nrhs].reshape(-1)
-    # the oracle: each realisation's cached call right after the caching call
-    ref = []
-    for r in range(nrhs):
-        O.clear_caches()
-        do = _copy(d)
-        O.destripe(*_args(pars, do, cache_sig.copy()))
-        O.destripe_with_cache(d["timestamps"], d["pixels"].copy(), d["pixweights"],
-                              sigs[r].reshape(-1).copy(), cfg.ndet)
-        ref.append(dict(map=O.result("map"), aa=O.result("aa"),
-                        noiter=O.scalars()["noiter"]))
-    O.clear_caches()
-    for fp32, rtol, floor in ((False, MAP_RTOL, parity.FLOOR),
-                              (True, FP32_RTOL, parity.FP32_FLOOR)):
+    # float64 batch at the workload's cglimit (it follows the oracle's
+    # iterates); float32 batch with both converged (parity.CONVERGED_CGLIMIT)
+    cases = ((False, dict(d["pars"], mcmode=True), nrhs),
+             (True, dict(d["pars"], mcmode=True, cglimit=parity.CONVERGED_CGLIMIT), 4))
+    for fp32, pars, nr in cases:
+        ref = _oracle_cached(d, pars, cache_sig, sigs[:nr], cfg.ndet)
+        rtol = FP32_RTOL if fp32 else MAP_RTOL
         W.clear_caches()
         W.destripe(None, *_args(pars, _copy(d), cache_sig.copy()))
         if fp32:
             W.destripe_with_cache_batch_fp32(None, d["timestamps"], d["pixels"].copy(),
-                                             d["pixweights"], sigs[:nrhs].astype(np.float32))
+                                             d["pixweights"], sigs[:nr].astype(np.float32))
         else:
             W.destripe_with_cache_batch(None, d["timestamps"], d["pixels"].copy(),
-                                        d["pixweights"], sigs[:nrhs])
-        maps = W.get_result("map_batch").reshape(nrhs, -1, 3)
-        aas = W.get_result("aa_batch").reshape(nrhs, -1)
+                                        d["pixweights"], sigs[:nr])
+        maps = W.get_result("map_batch").reshape(nr, -1, 3)
+        aas = W.get_result("aa_batch").reshape(nr, -1)
         its = W.get_result("noiter_batch")
-        for r in range(nrhs):
+        for r in range(nr):
             if fp32:
-                assert abs(its[r] - ref[r]["noiter"]) <= 3
+                assert its[r] <= 2.5 * ref[r]["noiter"] + 3  # converges, in more steps
             else:
                 assert its[r] == ref[r]["noiter"]
             for c in range(3):
                 parity.close(maps[r][:, c], ref[r]["map"].reshape(-1, 3)[:, c], rtol,
-                             "map_batch[%d][%d]" % (r, c), floor)
-            parity.close(aas[r], ref[r]["aa"], rtol, "aa_batch[%d]" % r, floor)
+                             "map_batch[%d][%d]" % (r, c))
+            parity.close(aas[r], ref[r]["aa"], rtol, "aa_batch[%d]" % r)
     W.clear_caches()
 
 
