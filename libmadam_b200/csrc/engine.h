@@ -458,6 +458,18 @@ class Engine {
   void true_residual(const double *x, const double *b, double *r);
   DevBuf<double> pwx_, lmapx_, apx_, partx_;
   DevBuf<double2> lmapgx_;
+  // FP32-TOD form: the pixel-sorted samples and their scatter chunks, kept
+  // beside the pairs for the exact scatter
+  void build_sample_csr();
+  void swap_csr();
+  bool have_xcsr_ = false;
+  DevBuf<float4> xsp4_;
+  DevBuf<int2> xsp2_;
+  DevBuf<int> xcsr_off_;
+  DevBuf<int4> xscatter_chunks_, xscatter_multi_;
+  DevBuf<double> xscatter_partial_;
+  long long xnscatter_chunks_ = 0, xcsr_nvalid_ = 0;
+  int xnscatter_multi_ = 0;
   long n_reliable_ = 0;           // reliable updates of the last solve
 };
 

@@ -708,10 +708,42 @@ void Engine::build_csr() {
   poff_.reset();
   pair_chunks_.reset();
   npair_chunks_ = 0;
-  if (fp32_ && nmap_ == 3 && build_pairs()) {
-    build_scatter_chunks();
-    return;
+  have_xcsr_ = false;
+  build_sample_csr();
+  if (fp32_ && nmap_ == 3) {
+    // FP32-TOD form: the scatter runs over pointing pairs; the sample CSR
+    // stays for the reliable updates' exact scatter (apply_A_exact)
+    swap_csr();
+    csr_off_.alloc((size_t)nloc_cross_ + 1);
+    if (build_pairs()) {
+      build_scatter_chunks();
+      have_xcsr_ = true;
+      return;
+    }
+    swap_csr();  // no pairs: the samples serve both
   }
+}
+
+// The pixel-sorted samples and their scatter chunks trade places with the
+// exact-scatter copy (x*).
+void Engine::swap_csr() {
+  auto sw = [](auto &a, auto &b) {
+    std::swap(a.p, b.p);
+    std::swap(a.n, b.n);
+  };
+  sw(sp4_, xsp4_);
+  sw(sp2_, xsp2_);
+  sw(csr_off_, xcsr_off_);
+  sw(scatter_chunks_, xscatter_chunks_);
+  sw(scatter_multi_, xscatter_multi_);
+  sw(scatter_partial_, xscatter_partial_);
+  std::swap(nscatter_chunks_, xnscatter_chunks_);
+  std::swap(nscatter_multi_, xnscatter_multi_);
+  std::swap(csr_nvalid_, xcsr_nvalid_);
+}
+
+void Engine::build_sample_csr() {
+  const long long n = (long long)ndet_ * nsamp_;
   const SampleMap sm = sample_map(istart_d_.get(), kstart_d_.get(), (int)ninterval_, nsamp_,
                                   noba_short_, fdn_);
   DevBuf<int> keys, keys_s;
@@ -1854,23 +1886,29 @@ void Engine::apply_A_exact(const double *x, double *ax) {
   // 1) baseline -> map over the samples: the pixel-sorted samples when the
   // scatter has them, else the time-ordered runs (pairs round the weights)
   if (nloc_cross_ > 0) {
-    if (!use_pairs_ && nscatter_chunks_ > 0) {
+    if (have_xcsr_ || (!use_pairs_ && nscatter_chunks_ > 0)) {
+      // the pixel-sorted samples (kept beside the pairs in the FP32-TOD form)
+      DevBuf<int4> &ck = have_xcsr_ ? xscatter_chunks_ : scatter_chunks_;
+      DevBuf<int4> &mu = have_xcsr_ ? xscatter_multi_ : scatter_multi_;
+      DevBuf<double> &pa = have_xcsr_ ? xscatter_partial_ : scatter_partial_;
+      const float4 *q4 = have_xcsr_ ? xsp4_.get() : sp4_.get();
+      const int2 *q2 = have_xcsr_ ? xsp2_.get() : sp2_.get();
+      const long long nck = have_xcsr_ ? xnscatter_chunks_ : nscatter_chunks_;
+      const int nmu = have_xcsr_ ? xnscatter_multi_ : nscatter_multi_;
       if (nmap_ == 3) {
-        MADAM_LAUNCH(k_scatter_chunks<3>, kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
-                     nscatter_chunks_, sp4_.get(), sp2_.get(), pwx_.get(), lmapx_.get(),
-                     scatter_partial_.get());
-        if (nscatter_multi_ > 0)
-          MADAM_LAUNCH(k_scatter_combine<3>, grid_for(nscatter_multi_), 256, 0, st_,
-                       scatter_multi_.get(), nscatter_multi_, scatter_partial_.get(),
-                       lmapx_.get());
+        if (nck > 0)
+          MADAM_LAUNCH(k_scatter_chunks<3>, kRedBlocks, 256, 0, st_, ck.get(), nck, q4, q2,
+                       pwx_.get(), lmapx_.get(), pa.get());
+        if (nmu > 0)
+          MADAM_LAUNCH(k_scatter_combine<3>, grid_for(nmu), 256, 0, st_, mu.get(), nmu,
+                       pa.get(), lmapx_.get());
       } else {
-        MADAM_LAUNCH(k_scatter_chunks<1>, kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
-                     nscatter_chunks_, sp4_.get(), sp2_.get(), pwx_.get(), lmapx_.get(),
-                     scatter_partial_.get());
-        if (nscatter_multi_ > 0)
-          MADAM_LAUNCH(k_scatter_combine<1>, grid_for(nscatter_multi_), 256, 0, st_,
-                       scatter_multi_.get(), nscatter_multi_, scatter_partial_.get(),
-                       lmapx_.get());
+        if (nck > 0)
+          MADAM_LAUNCH(k_scatter_chunks<1>, kRedBlocks, 256, 0, st_, ck.get(), nck, q4, q2,
+                       pwx_.get(), lmapx_.get(), pa.get());
+        if (nmu > 0)
+          MADAM_LAUNCH(k_scatter_combine<1>, grid_for(nmu), 256, 0, st_, mu.get(), nmu,
+                       pa.get(), lmapx_.get());
       }
     } else {
       lmapx_.zero(st_);

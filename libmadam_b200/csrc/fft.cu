@@ -35,9 +35,10 @@ __device__ __forceinline__ cplx twiddle(long long num, long long den) {
   return make_double2(c, s);
 }
 
-// T2[m] = exp(-2 pi i m / (2N)), m < 2N, precomputed once per plan
+// T2[m] = exp(-2 pi i m / (2N)), m < 2N, precomputed once per plan; N is a
+// power of two
 __device__ __forceinline__ cplx tw_n(const cplx *T2, long long num, long long N) {
-  return T2[2 * (num % N)];
+  return T2[2 * (num & (N - 1))];
 }
 
 __global__ void k_fill_table(cplx *T2, long long n2) {
@@ -286,10 +287,17 @@ __global__ void k_conv_small(const ConvSeg *segs, const double *spectra, long lo
 // pass write to it through the load / store functors.
 __device__ __forceinline__ int pad8(int i) { return i + (i >> 3); }
 
+// twL[q] = exp(-2 pi i q / L), q < L: the sub-transform's twiddles, copied
+// into shared memory by the kernel (load_twl) before its first transform
 template <bool INV>
-__device__ __forceinline__ cplx tw_l(const cplx *T2, long long q, long long step) {
-  const cplx w = T2[q * step];  // exp(-2 pi i q / L), step = 2N / L
+__device__ __forceinline__ cplx tw_l(const cplx *twL, int q) {
+  const cplx w = twL[q];
   return INV ? cconj(w) : w;
+}
+
+__device__ __forceinline__ void load_twl(cplx *twL, int L, const cplx *T2, long long N) {
+  const long long step = 2 * N / L;
+  for (int q = threadIdx.x; q < L; q += blockDim.x) twL[q] = T2[q * step];
 }
 
 template <bool INV>
@@ -345,8 +353,8 @@ __device__ __forceinline__ void dft4(cplx *v) {
 // Last radix-R pass (R = 2 or 4, Ns = L / R): butterflies j < L / R over the
 // elements j + k L / R; each thread takes 8 / R butterflies.
 template <int R, bool INV, bool FFAST, typename Store>
-__device__ __forceinline__ void last_pass(cplx *s, int S, int L, int nfft, const cplx *T2,
-                                          long long step, int nb8, Store store) {
+__device__ __forceinline__ void last_pass(cplx *s, int S, int L, int nfft, const cplx *twL,
+                                          int nb8, Store store) {
   constexpr int PER = 8 / R;
   const int Lr = L / R, t = threadIdx.x;
   cplx v[PER][R];
@@ -368,7 +376,7 @@ __device__ __forceinline__ void last_pass(cplx *s, int S, int L, int nfft, const
   for (int u = 0; u < PER; ++u) {
     if (ff[u] < 0) continue;
 #pragma unroll
-    for (int k = 1; k < R; ++k) v[u][k] = cmul(v[u][k], tw_l<INV>(T2, (long long)jj[u] * k, step));
+    for (int k = 1; k < R; ++k) v[u][k] = cmul(v[u][k], tw_l<INV>(twL, jj[u] * k));
     if (R == 4) {
       dft4<INV>(v[u]);
     } else {
@@ -388,9 +396,8 @@ __device__ __forceinline__ void last_pass(cplx *s, int S, int L, int nfft, const
 // store(f, i, v) takes output element i of the last pass.
 template <bool INV, bool FFAST, typename Load, typename Store>
 __device__ __forceinline__ void fft_block(cplx *s, int S, int L, int logL, int nfft,
-                                          const cplx *T2, long long N, Load load, Store store) {
+                                          const cplx *twL, Load load, Store store) {
   const int L8 = L >> 3, n8 = logL / 3, rem = logL - 3 * n8;
-  const long long step = 2 * N / L;
   const int nb8 = nfft * L8;
   const int t = threadIdx.x;
   int Ns = 1;
@@ -408,10 +415,10 @@ __device__ __forceinline__ void fft_block(cplx *s, int S, int L, int logL, int n
     __syncthreads();
     if (act) {
       if (!first) {
-        const long long r = j & (Ns - 1);
-        const long long qs = r * (L / (8 * Ns));
+        const int r = j & (Ns - 1);
+        const int qs = r * (L / (8 * Ns));
 #pragma unroll
-        for (int k = 1; k < 8; ++k) v[k] = cmul(v[k], tw_l<INV>(T2, qs * k, step));
+        for (int k = 1; k < 8; ++k) v[k] = cmul(v[k], tw_l<INV>(twL, qs * k));
       }
       dft8<INV>(v);
       if (last) {
@@ -426,8 +433,8 @@ __device__ __forceinline__ void fft_block(cplx *s, int S, int L, int logL, int n
     __syncthreads();
     Ns *= 8;
   }
-  if (rem == 1) last_pass<2, INV, FFAST>(s, S, L, nfft, T2, step, nb8, store);
-  else if (rem == 2) last_pass<4, INV, FFAST>(s, S, L, nfft, T2, step, nb8, store);
+  if (rem == 1) last_pass<2, INV, FFAST>(s, S, L, nfft, twL, nb8, store);
+  else if (rem == 2) last_pass<4, INV, FFAST>(s, S, L, nfft, twL, nb8, store);
 }
 
 // ------------------------------------------------------- four-step path --
@@ -437,6 +444,8 @@ __global__ void __launch_bounds__(512, 2) k_conv_cols_fwd(const ConvSeg *segs, c
                                                        int logR, int C, int G, const cplx *T2) {
   extern __shared__ double2 sm[];
   const int S = pad8(R) + 1;
+  cplx *twL = sm + G * S;
+  load_twl(twL, R, T2, (long long)R * C);
   const int seg = blockIdx.y;
   const ConvSeg sg = segs[seg];
   const double mean = seg_mean(part, seg, sg.n_in, sg.flags & 1);
@@ -451,7 +460,7 @@ __global__ void __launch_bounds__(512, 2) k_conv_cols_fwd(const ConvSeg *segs, c
     const int n2 = c0 + f;
     W[(long long)k1 * C + n2] = cmul(v, tw_n(T2, (long long)n2 * k1, N));
   };
-  fft_block<false, true>(sm, S, R, logR, G, T2, N, load, store);
+  fft_block<false, true>(sm, S, R, logR, G, twL, load, store);
 }
 
 // Pass 2: forward row FFTs of rows k1 and R-k1, spectral product, inverse
@@ -462,6 +471,8 @@ __global__ void __launch_bounds__(1024) k_conv_rows(const ConvSeg *segs, const d
   extern __shared__ double2 sm[];
   const int S = pad8(C) + 1;
   cplx *s = sm;  // 2 rows
+  cplx *twL = sm + 2 * S;
+  load_twl(twL, C, T2, (long long)R * C);
   const int seg = blockIdx.y;
   const ConvSeg sg = segs[seg];
   const long long N = (long long)R * C;
@@ -472,7 +483,7 @@ __global__ void __launch_bounds__(1024) k_conv_rows(const ConvSeg *segs, const d
   auto gload = [&](int f, int n2) { return W[(long long)(f ? kb : ka) * C + n2]; };
   auto sload = [&](int f, int n2) { return s[f * S + pad8(n2)]; };
   auto sstore = [&](int f, int n2, cplx v) { s[f * S + pad8(n2)] = v; };
-  fft_block<false, false>(s, S, C, logC, nrows, T2, N, gload, sstore);
+  fft_block<false, false>(s, S, C, logC, nrows, twL, gload, sstore);
   const double *H = spectra + (long long)sg.spec * spec_len;
   auto at = [&](int f, int n2) -> cplx & { return s[f * S + pad8(n2)]; };
   if (ka == 0) {
@@ -508,7 +519,7 @@ __global__ void __launch_bounds__(1024) k_conv_rows(const ConvSeg *segs, const d
     const int k1 = f ? kb : ka;
     W[(long long)k1 * C + n2] = cmul(v, cconj(tw_n(T2, (long long)n2 * k1, N)));
   };
-  fft_block<true, false>(s, S, C, logC, nrows, T2, N, sload, gstore);
+  fft_block<true, false>(s, S, C, logC, nrows, twL, sload, gstore);
 }
 
 // Pass 3: inverse column FFTs and real output.
@@ -517,6 +528,8 @@ __global__ void __launch_bounds__(512, 2) k_conv_cols_inv(const ConvSeg *segs, c
                                                        const cplx *T2) {
   extern __shared__ double2 sm[];
   const int S = pad8(R) + 1;
+  cplx *twL = sm + G * S;
+  load_twl(twL, R, T2, (long long)R * C);
   const int seg = blockIdx.y;
   const ConvSeg sg = segs[seg];
   const int c0 = blockIdx.x * G;
@@ -529,7 +542,7 @@ __global__ void __launch_bounds__(512, 2) k_conv_cols_inv(const ConvSeg *segs, c
     if (2 * m < sg.n_out) y[sg.y_off + 2 * m] = v.x * scale;
     if (2 * m + 1 < sg.n_out) y[sg.y_off + 2 * m + 1] = v.y * scale;
   };
-  fft_block<true, true>(sm, S, R, logR, G, T2, N, load, store);
+  fft_block<true, true>(sm, S, R, logR, G, twL, load, store);
 }
 
 int ilog2(long v) {
@@ -599,8 +612,9 @@ void FFTPlan::convolve(cudaStream_t st, const ConvSeg *segs, long nseg, const do
   } else {
     const int logR = ilog2(R), logC = ilog2(C);
     auto padded = [](long L) { return L + L / 8 + 1; };
-    size_t smem_cols = (size_t)(G * padded(R)) * sizeof(double2);
-    size_t smem_rows = (size_t)(2 * padded(C)) * sizeof(double2);
+    // rows padded one slot in nine, then the sub-transform twiddle table
+    size_t smem_cols = (size_t)(G * padded(R) + R) * sizeof(double2);
+    size_t smem_rows = (size_t)(2 * padded(C) + C) * sizeof(double2);
     const unsigned tcols = (unsigned)std::max(32, G * R / 8);
     const unsigned trows = (unsigned)std::max(32, C / 4);
     static bool attr = false;
