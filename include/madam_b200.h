@@ -152,7 +152,11 @@ int madam_b200_last_error(char *buf, long buflen);
  * (smadam.F90:954-1257) as "subsets" (float64 [nsub][4]: pass, survey, detector
  * set, nmap) with "subset_binmap:<k>", "subset_hits:<k>", "subset_mask:<k>"
  * (int32), "subset_cc:<k>", "subset_leak:<k>:<d>",
- * "timings" (float64 [9], milliseconds).  result_size returns elements or
+ * "timings" (float64 [9], milliseconds), "nan_checks" (float64 [7], with
+ * checknan: detectors with NaN parameters, NaN counts of yba, the binned
+ * cross map, the pointing weights, and r, z, p at the first CG step; the
+ * reference prints these checks, smadam_routines.f90:456-502, 978-1033).
+ * result_size returns elements or
  * -1; result_copy fails when nbytes is too small. */
 long madam_b200_result_size(const char *name);
 int madam_b200_result_copy(const char *name, void *dst, long nbytes);

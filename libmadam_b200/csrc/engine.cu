@@ -1150,6 +1150,17 @@ __global__ void k_scale_neg(const double *a, const double *bw, double *out, long
     out[i] = -(a[i] * bw[i]);
 }
 
+// NaN count of n values (checknan diagnostics)
+template <typename T>
+__global__ void k_count_nan(const T *v, long long n, unsigned long long *out) {
+  unsigned long long c = 0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    c += isnan(v[i]) ? 1 : 0;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
 // r = b - ax (the true residual of a reliable update)
 __global__ void k_residual(double *r, const double *b, const double *ax, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;

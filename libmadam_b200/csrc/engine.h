@@ -194,6 +194,15 @@ class Engine {
   void build_filter_finish();
   void construct_preconditioner();
   void build_guarded_chunks(const std::vector<PRun> &pruns, const std::vector<PRun> &cruns);
+  // checknan diagnostics: [0] detectors with NaN parameters, NaN counts of
+  // [1] yba, [2] the binned cross map, [3] the pointing weights, [4] r, [5] z,
+  // [6] p at the first CG step
+  static constexpr int kNanChecks = 7;
+  std::vector<double> nan_checks_;
+  unsigned long long count_nan(const double *v, long long n);
+  unsigned long long count_nan(const float *v, long long n);
+  void check_nan_setup();
+  void check_nan_iterate(double rz, long long nb);
   std::vector<GChunk> make_gchunks(int Cg, int G, std::vector<int> &cls_begin,
                                    std::vector<int> &seg_off) const;
   int guard_chunk_len(long long npos) const;
@@ -434,6 +443,7 @@ class Engine {
   }
   double ar_sum_host(double v);
   bool writes_files() const { return !comm_ || comm_->rank == 0; }
+  int rank() const { return comm_ ? comm_->rank : 0; }
   std::map<std::string, std::vector<double>> subchunk_d_;  // products of subchunk passes
   std::map<std::string, std::vector<int>> subchunk_i_;
 

@@ -2112,6 +2112,71 @@ void Engine::check_band_err() {
   }
 }
 
+// checknan (parameter_control.f90:321-330, smadam_routines.f90:456-502,
+// 740 / 978-1033): NaN counts of the detector parameters, of the right-hand
+// side, the binned map and the pointing weights after initialize_a, and of
+// the first CG vectors, reported as the reference reports them (a message
+// per kind on standard output; the solve goes on) and kept as "nan_checks".
+unsigned long long Engine::count_nan(const double *v, long long n) {
+  if (n <= 0 || !v) return 0;
+  DevBuf<unsigned long long> c;
+  c.alloc(1);
+  c.zero(st_);
+  MADAM_LAUNCH(k_count_nan<double>, grid_for(n), 256, 0, st_, v, n, c.get());
+  unsigned long long h = 0;
+  MADAM_CUDA(cudaMemcpyAsync(&h, c.get(), sizeof h, cudaMemcpyDeviceToHost, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  return h;
+}
+
+unsigned long long Engine::count_nan(const float *v, long long n) {
+  if (n <= 0 || !v) return 0;
+  DevBuf<unsigned long long> c;
+  c.alloc(1);
+  c.zero(st_);
+  MADAM_LAUNCH(k_count_nan<float>, grid_for(n), 256, 0, st_, v, n, c.get());
+  unsigned long long h = 0;
+  MADAM_CUDA(cudaMemcpyAsync(&h, c.get(), sizeof h, cudaMemcpyDeviceToHost, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  return h;
+}
+
+void Engine::check_nan_setup() {
+  nan_checks_.assign(kNanChecks, 0.0);
+  if (!par_.checknan) return;
+  for (const Detector &d : dets_) {
+    bool bad = false;
+    for (double w : d.weights) bad = bad || std::isnan(w);
+    for (double s : d.sigmas) bad = bad || std::isnan(s);
+    if (bad) {
+      std::printf("%d : Bad detector params (NaN in sigmas or weights) : %s\n", rank(),
+                  d.name.c_str());
+      nan_checks_[0] += 1;
+    }
+  }
+  const long long nb = (long long)ndet_ * noba_short_ * nbasis_;
+  nan_checks_[1] = (double)count_nan(yba_.get(), nb);
+  nan_checks_[2] = (double)count_nan(wamap_.get(), (long long)wamap_.n);
+  if (nmap_ != 1) nan_checks_[3] = (double)count_nan(d_w_, (long long)ndet_ * nsamp_ * nnz_);
+  if (nan_checks_[1] > 0) std::printf("%d : NaN in uninitialized yba\n", rank());
+  if (nan_checks_[2] > 0) std::printf("%d : NaN in locmap\n", rank());
+  if (nan_checks_[3] > 0) std::printf("%d : NaN in weights\n", rank());
+  std::fflush(stdout);
+}
+
+void Engine::check_nan_iterate(double rz, long long nb) {
+  if (!par_.checknan) return;
+  if (std::isnan(rz)) std::printf("%d : ERROR: rz is nan\n", rank());
+  nan_checks_[4] = (double)count_nan(r_.get(), nb);
+  nan_checks_[5] = (double)count_nan(z_.get(), nb);
+  nan_checks_[6] = (double)count_nan(p_.get(), nb);
+  if (nan_checks_[1] > 0) std::printf("%d : yba has NaN(s)\n", rank());
+  if (nan_checks_[4] > 0) std::printf("%d : r has NaN(s)\n", rank());
+  if (nan_checks_[5] > 0) std::printf("%d : z has NaN(s)\n", rank());
+  if (nan_checks_[6] > 0) std::printf("%d : p has NaN(s)\n", rank());
+  std::fflush(stdout);
+}
+
 void Engine::cg_preconditioner_segments(const double *r, double *z) {
   if (cg_prec_segs_.empty()) return;
   const long long nb = (long long)ndet_ * noba_short_;
@@ -2234,6 +2299,7 @@ void Engine::iterate() {
   rrinit = scal_host_[S_RR];
   rr_final = 1.0;
   noiter = 0;
+  check_nan_iterate(rzinit, nb);
   if (rzinit < fsp(1e-30f) || std::isnan(rzinit)) {
     timings.iterate_ms = now_ms() - t0;
     return;
@@ -2592,6 +2658,7 @@ void Engine::run(const Params &par, std::vector<Detector> dets, long ndet, long 
   if (par_.kfirst) {
     map_side_setup();
     initialize_a();
+    check_nan_setup();
     mark(7);
     build_segments();
     build_filter_finish();
@@ -2702,6 +2769,7 @@ long Engine::result_size(const std::string &name) {
   if (name == "band_widths") return (long)band_widths_.size();
   if (name == "scalars") return 24;
   if (name == "timings") return 9;
+  if (name == "nan_checks") return (long)nan_checks_.size();
   if (name == "setup_marks") return kSetupMarks;
   if (name == "map_batch" || name == "binmap_batch") return nrhs_ * npm * nmap_;
   if (name == "aa_batch") return nrhs_ * nb;
@@ -2851,6 +2919,9 @@ void Engine::result_copy(const std::string &name, void *dst, long nbytes) {
   } else if (name == "setup_marks") {
     need(sizeof(double));
     std::memcpy(dst, setup_marks_, sizeof setup_marks_);
+  } else if (name == "nan_checks") {
+    need(sizeof(double));
+    std::memcpy(dst, nan_checks_.data(), nan_checks_.size() * sizeof(double));
   } else if (name == "timings") {
     need(sizeof(double));
     const double v[9] = {timings.setup_ms, timings.iterate_ms, timings.finalize_ms,

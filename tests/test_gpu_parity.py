@@ -208,3 +208,62 @@ def test_config1_full_size(W):
     d = syn.to_numpy(syn.generate(syn.config1()))
     ro, rp, _, _ = run_both(W, d)
     compare(ro, rp, 3)
+
+
+@pytest.mark.parametrize("pars", [
+    # invert_pixelmatrix_cross / _map criteria (map_routines.f90:126-182, 255-302):
+    # determinant, scaled determinant, rcond, and the cross-only modes 3 / 4
+    dict(pixmode_cross=0, pixlim_cross=1e-12, pixmode_map=0, pixlim_map=1e-12),
+    dict(pixmode_cross=1, pixlim_cross=1e-3, pixmode_map=1, pixlim_map=1e-3),
+    dict(pixmode_cross=3, pixlim_cross=1e-3),
+    dict(pixmode_cross=4, pixlim_cross=1e-3),
+    dict(pixmode_cross=2, pixlim_cross=0.2, pixmode_map=2, pixlim_map=0.2),
+])
+def test_pixel_matrix_modes(W, pars):
+    d = syn.to_numpy(syn.generate(syn.small_config(seed=27)))
+    ro, rp, _, _ = run_both(W, d, pars)
+    compare(ro, rp, 3)
+
+
+def test_good_baseline_fraction(W):
+    # flag_bad_baselines (read_data.f90:30-74): without the filter, a baseline
+    # with fewer good samples than the fraction loses all of them
+    d = syn.to_numpy(syn.generate(syn.small_config(seed=28)))
+    rng = np.random.default_rng(8)
+    n = d["pixels"].size
+    d["pixweights"].reshape(-1, 3)[rng.choice(n, n // 3, replace=False)] = 0.0
+    ro, rp, do, dp = run_both(W, d, dict(kfilter=False, good_baseline_fraction=0.7))
+    compare(ro, rp, 3)
+    # some samples were flagged by the rule beyond the zero-weight ones (the
+    # rule's come back past the dummy pixel, read_data.f90:51 and
+    # pointing.f90:178-186)
+    assert (dp["pixels"] >= 12 * d["pars"]["nside_map"] ** 2).sum() > n // 3
+
+
+@pytest.mark.parametrize("radiometers", [True, False])
+def test_noise_weights_from_psd(W, radiometers):
+    # measure_noise_weights (noise_routines.f90:65-127): detector weights from
+    # the PSD plateau instead of the caller's detweights
+    d = syn.to_numpy(syn.generate(syn.small_config(seed=29)))
+    d["detweights"] = d["detweights"] * np.array([0.5, 1.0, 2.0, 4.0])
+    ro, rp, _, _ = run_both(W, d, dict(noise_weights_from_psd=True, radiometers=radiometers))
+    compare(ro, rp, 3)
+
+
+def test_checknan_reports_nan_inputs(W, capfd):
+    # checknan (smadam_routines.f90:456-502, 978-1033) reports NaNs in the
+    # right-hand side and the CG vectors and lets the call go on
+    d = syn.to_numpy(syn.generate(syn.small_config(seed=30)))
+    pars = dict(d["pars"], checknan=True)
+    args = lambda x, s: (pars, x["dets"], x["detweights"], x["timestamps"], x["pixels"].copy(),
+                         x["pixweights"], s, x["periods"], x["npsd"], x["psdstarts"],
+                         x["psdfreqs"], x["psdvals"])
+    W.destripe(None, *args(d, d["signal"].copy()))
+    assert not W.get_result("nan_checks").any()
+    sig = d["signal"].copy()
+    sig.reshape(-1)[1234] = np.nan
+    W.destripe(None, *args(d, sig))
+    nc = W.get_result("nan_checks")
+    assert nc[1] >= 1 and nc[4] >= 1  # yba and r
+    out = capfd.readouterr().out
+    assert "NaN in uninitialized yba" in out and "r has NaN(s)" in out
