@@ -80,15 +80,23 @@ int madam_b200_destripe_with_cache_batch_fp32(int comm, long ndet, long nsamp, l
  * must stay valid until the job is done.  Jobs start first come, first
  * served, when their estimated footprint fits the budget beside the running
  * jobs, and overlap on the device; their products do not depend on what else
- * runs (beyond rounding).  serve_wait waits up to timeout_s seconds (< 0: no limit) and
+ * runs (beyond rounding).  A job's setup runs on its worker; its PCG then
+ * iterates in shared rounds with the other jobs past their setup, driven by
+ * one stepper thread: per round each job's A p and preconditioner, the CG
+ * vector algebra and inner products of all jobs in shared launches, and one
+ * host synchronisation for every job's convergence test (a job with a
+ * covariance-matrix output, or kfirst off, runs on its worker alone).
+ * serve_wait waits up to timeout_s seconds (< 0: no limit) and
  * returns the job state: 0 queued, 1 running, 2 done, 3 failed, -1 unknown.
  * serve_result_size / serve_result_copy give a done job's "map", "binmap"
  * (float64 [npix][nmap]), "hits", "mask" (int32 [npix]), "aa" (float64
  * [ndet][noba]), "scalars" (float64 [24]), "rr_history" (float64);
  * serve_job_info gives out[0..5] = submit, start and end time (s), samples,
  * PCG iterations, admitted bytes; serve_error the message of a failed job;
- * serve_release frees a finished job; serve_close waits for the running
- * jobs, drops the queued ones and frees the server. */
+ * serve_release frees a finished job; serve_stats gives out[0..2] = PCG
+ * rounds run, job-rounds (jobs summed over the rounds) and the most jobs in
+ * one round; serve_close waits for the running jobs, drops the queued ones
+ * and frees the server. */
 void *madam_b200_serve_open(int nworkers, double mem_fraction, char *err, long errlen);
 long madam_b200_serve_submit(void *srv, char *parstring, long ndet, char *detstring,
                              double *detweights, long nsamp, long nnz, void *timestamps, void *pix,
@@ -110,6 +118,7 @@ int madam_b200_serve_result_copy(void *srv, long job, const char *name, void *ds
 int madam_b200_serve_job_info(void *srv, long job, double *out, long nout);
 int madam_b200_serve_error(void *srv, long job, char *buf, long buflen);
 int madam_b200_serve_release(void *srv, long job);
+int madam_b200_serve_stats(void *srv, double *out, long nout);
 int madam_b200_serve_close(void *srv);
 
 /* Sharded runs: communicators standing in for the reference's MPI

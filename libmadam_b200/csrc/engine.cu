@@ -1150,6 +1150,69 @@ __global__ void k_scale_neg(const double *a, const double *bw, double *out, long
     out[i] = -(a[i] * bw[i]);
 }
 
+// ---------------------------------------------------- serving stepper --
+// The vector algebra of several PCG jobs in one launch each (grid.y: job);
+// per job the arithmetic of k_update_ar, k_dots + k_finish (mode 2) and
+// k_update_p.
+__global__ void k_pcg_update_ar_j(const PcgJob *tab) {
+  const PcgJob j = tab[blockIdx.y];
+  if (!j.active) return;
+  const double alpha = j.scal[S_ALPHA];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < j.nb;
+       i += (long long)gridDim.x * blockDim.x) {
+    j.aa[i] = j.aa[i] + alpha * j.p[i];
+    const double ri = j.r[i];
+    j.ro[i] = ri;
+    j.r[i] = ri - alpha * j.ap[i];
+  }
+}
+
+__global__ void k_pcg_dots_j(const PcgJob *tab) {
+  const PcgJob j = tab[blockIdx.y];
+  if (!j.active) return;
+  double v[3] = {0, 0, 0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < j.nb;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (!j.rmask[i]) continue;
+    v[0] += j.r[i] * j.z[i];
+    v[1] += j.ro[i] * j.z[i];
+    v[2] += j.r[i] * j.r[i];
+  }
+  block_sum<3>(v);
+  if (threadIdx.x == 0)
+    for (int q = 0; q < 3; ++q) j.part[q * gridDim.x + blockIdx.x] = v[q];
+}
+
+__global__ void k_pcg_finish_j(const PcgJob *tab, int nblk, double *out) {
+  const PcgJob j = tab[blockIdx.x];
+  if (!j.active) return;
+  double v[3] = {0, 0, 0};
+  for (int q = 0; q < 3; ++q)
+    for (int i = threadIdx.x; i < nblk; i += blockDim.x) v[q] += j.part[q * nblk + i];
+  block_sum<3>(v);
+  if (threadIdx.x != 0) return;
+  double *sc = j.scal;
+  sc[S_RZO] = sc[S_RZ];
+  sc[S_RZ] = v[0];
+  sc[S_RZ2] = v[1];
+  sc[S_RR] = v[2];
+  sc[S_BETA] = (v[0] - v[1]) / sc[S_RZO];
+  out[2 * blockIdx.x] = v[0];
+  out[2 * blockIdx.x + 1] = v[2];
+}
+
+__global__ void k_pcg_update_p_j(const PcgJob *tab) {
+  const PcgJob j = tab[blockIdx.y];
+  if (!j.active) return;
+  const double beta = j.scal[S_BETA];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < j.nb;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double v = j.z[i] + beta * j.p[i];
+    j.p[i] = v;
+    j.pw[i] = v * j.bw[i];
+  }
+}
+
 // NaN count of n values (checknan diagnostics)
 template <typename T>
 __global__ void k_count_nan(const T *v, long long n, unsigned long long *out) {

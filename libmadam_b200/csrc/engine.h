@@ -31,6 +31,25 @@ constexpr int kMaxBasis = 8;          // basis_order + 1 at most
 constexpr double kReliableDrop = 1e-6;
 
 
+// A job's CG vectors for the serving stepper's shared launches (pcg_shared).
+struct PcgJob {
+  double *aa, *r, *ro, *p, *ap, *z, *pw;
+  const double *bw;
+  const uint8_t *rmask;
+  double *part, *scal;
+  long long nb;
+  int active;
+};
+
+// Shared launches over the PCG jobs of a device table of n entries, on st:
+// step 0: aa += alpha p, ro = r, r -= alpha ap (k_update_ar of each job);
+// step 1: r.z, ro.z, r.r and the CG scalars of each job, its rz and rr also
+// to out[2 j], out[2 j + 1] (k_dots + k_finish mode 2); step 2: p = z + beta
+// p, pw = p bw (k_update_p).  Same grids and reduction order as the
+// single-job kernels; nbmax: the largest job's vector length.
+void pcg_shared(cudaStream_t st, const PcgJob *tab, int n, long long nbmax, int step,
+                double *out);
+
 // Owning device allocation.
 // Device memory of the engine: stream-ordered allocations on the stream of
 // the engine the calling thread is working for (several engines may run in
@@ -165,6 +184,22 @@ class Engine {
   long result_size(const std::string &name);
   void result_copy(const std::string &name, void *dst, long nbytes);
 
+  // destripe() in parts, for the serving stepper: run_setup (everything
+  // before the PCG), the stepwise PCG (pcg_*), run_finish (maps, files)
+  void run_setup(const Params &par, std::vector<Detector> dets, long ndet, long nsamp, long nnz,
+                 double *timestamps, int32_t *pix, float *pixweights, double *signal,
+                 long nperiod, const long *periods, bool is_device);
+  void run_finish();
+  void run_solve();                // the PCG (or write_covmat) as destripe() runs it
+  bool stepwise_ok() const;        // the PCG can be stepped (kfirst, no covmat, one rank)
+  bool pcg_begin();                // first residual; false: no iteration to do
+  void pcg_use_stream(cudaStream_t s);  // launch the steps on s (nullptr: own stream)
+  void pcg_apply();                // A p and alpha
+  void pcg_precond();              // z = M r
+  PcgJob pcg_job();
+  bool pcg_after(double rz, double rr);  // after a round: true when the PCG stops
+  void pcg_end();
+
   // Times `iters` PCG iterations on the state of the last solve (bench).
   void bench_iterations(int warmup, int iters, std::vector<double> &out);
 
@@ -207,6 +242,14 @@ class Engine {
                                    std::vector<int> &seg_off) const;
   int guard_chunk_len(long long npos) const;
   void iterate();
+  void pcg_reset();
+  bool pcg_judge(long istep, double rz, double rr);
+  long pcg_istep_ = 0;
+  double pcg_t0_ = 0, run_t0_ = 0, pcg_rr_true_ = 0;
+  bool pcg_reliable_ = false;
+  const double *pcg_bw_ = nullptr;
+  const uint8_t *pcg_rmask_ = nullptr;
+  cudaStream_t pcg_own_st_ = nullptr;
   void finalize(bool first_call);
   void writeback_host();
   void write_fits(bool first_call);

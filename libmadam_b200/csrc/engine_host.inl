@@ -2306,12 +2306,7 @@ void Engine::iterate() {
   }
   long istep = 0;
   float tm[4];
-  // FP32-TOD form: reliable updates each time the carried residual norm has
-  // dropped by kReliableDrop (squared) since the last true one, and before
-  // convergence is accepted
-  const bool reliable = refine() && nbasis_ == 1;
-  double rr_true = rrinit;
-  n_reliable_ = 0;
+  pcg_reset();
   while (istep < par_.iter_max) {
     ++istep;
     apply_A(p_.get(), pw_.get(), ap_.get(), true);
@@ -2334,30 +2329,7 @@ void Engine::iterate() {
     timings.filter_ms += tm[1];
     timings.gather_ms += tm[2];
     timings.precond_ms += tm[3];
-    double rz = scal_host_[S_RZ], rr = scal_host_[S_RR];
-    if (reliable && ((rr / rrinit < par_.cglimit && istep > par_.iter_min) ||
-                     rr < kReliableDrop * rr_true)) {
-      // reliable update: the residual the float32 projections carried is
-      // replaced by the true one, so that convergence is judged, and the
-      // iteration continues, on the float64 system
-      true_residual(aa_.get(), yba_.get(), r_.get());
-      apply_preconditioner(r_.get(), z_.get());
-      MADAM_LAUNCH(k_dots, kRedBlocks, 256, 0, st_, r_.get(), z_.get(), ro_.get(), z_.get(),
-                   r_.get(), r_.get(), 3, rmv, nb, part_.get());
-      finish_dots(3, 3, 0, kRedBlocks, true);
-      MADAM_CUDA(cudaMemcpyAsync(scal_host_.data(), scal_.get(), S_NSCAL * sizeof(double),
-                                 cudaMemcpyDeviceToHost, st_));
-      MADAM_CUDA(cudaStreamSynchronize(st_));
-      rz = scal_host_[S_RZ];
-      rr = scal_host_[S_RR];
-      rr_true = rr;
-    }
-    rr_history.push_back(rr / rrinit);
-    rr_final = rr / rrinit;
-    noiter = istep;
-    if (rr / rrinit > 1e3) fail("CG is diverging");
-    if (rr / rrinit < par_.cglimit && istep > par_.iter_min) break;
-    if (rz == 0) break;
+    if (pcg_judge(istep, scal_host_[S_RZ], scal_host_[S_RR])) break;
     MADAM_LAUNCH(k_update_p, grid_for(nb), 256, 0, st_, p_.get(), z_.get(), pw_.get(), bwv,
                  nb, scal_.get(), 0);
   }
@@ -2370,6 +2342,159 @@ void Engine::iterate() {
                                cudaMemcpyDeviceToDevice, st_));
   MADAM_CUDA(cudaStreamSynchronize(st_));
   timings.iterate_ms = now_ms() - t0;
+}
+
+// The step after a PCG iteration's inner products (iterate_a 890-924):
+// reliable update of the FP32-TOD form, history, divergence and convergence
+// tests.  Returns true when the iteration stops.
+void Engine::pcg_reset() {
+  // FP32-TOD form: reliable updates each time the carried residual norm has
+  // dropped by kReliableDrop (squared) since the last true one, and before
+  // convergence is accepted
+  pcg_reliable_ = refine() && nbasis_ == 1;
+  pcg_rr_true_ = rrinit;
+  n_reliable_ = 0;
+}
+
+bool Engine::pcg_judge(long istep, double rz, double rr) {
+  if (pcg_reliable_ && ((rr / rrinit < par_.cglimit && istep > par_.iter_min) ||
+                        rr < kReliableDrop * pcg_rr_true_)) {
+    // reliable update: the residual the float32 projections carried is
+    // replaced by the true one, so that convergence is judged, and the
+    // iteration continues, on the float64 system
+    const long long nb = (long long)ndet_ * noba_short_ * nbasis_;
+    true_residual(aa_.get(), yba_.get(), r_.get());
+    apply_preconditioner(r_.get(), z_.get());
+    MADAM_LAUNCH(k_dots, kRedBlocks, 256, 0, st_, r_.get(), z_.get(), ro_.get(), z_.get(),
+                 r_.get(), r_.get(), 3, rmask_.get(), nb, part_.get());
+    finish_dots(3, 3, 0, kRedBlocks, true);
+    MADAM_CUDA(cudaMemcpyAsync(scal_host_.data(), scal_.get(), S_NSCAL * sizeof(double),
+                               cudaMemcpyDeviceToHost, st_));
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    rz = scal_host_[S_RZ];
+    rr = scal_host_[S_RR];
+    pcg_rr_true_ = rr;
+  }
+  rr_history.push_back(rr / rrinit);
+  rr_final = rr / rrinit;
+  noiter = istep;
+  if (rr / rrinit > 1e3) fail("CG is diverging");
+  if (rr / rrinit < par_.cglimit && istep > par_.iter_min) return true;
+  return rz == 0;
+}
+
+// ---------------------------------------------------------- stepwise PCG --
+// The serving stepper advances the PCG of several engines in rounds: per
+// round every engine's A p (pcg_apply) and preconditioner (pcg_precond) on a
+// stream the stepper picks, the vector algebra of all of them in shared
+// launches (pcg_shared), one host synchronisation, then pcg_after for each.
+// The arithmetic is that of iterate(): the same kernels, grids and reduction
+// order, so a job's products do not depend on the others in its rounds.
+bool Engine::stepwise_ok() const {
+  return par_.kfirst && par_.file_covmat.empty() && !sharded();
+}
+
+bool Engine::pcg_begin() {
+  const double t0 = now_ms();
+  pcg_t0_ = t0;
+  const long long nb = (long long)ndet_ * noba_short_ * nbasis_;
+  pcg_bw_ = bw_.get();
+  pcg_rmask_ = rmask_.get();
+  if (nbasis_ > 1) {
+    basis_vectors();
+    pcg_bw_ = bwn_.get();
+    pcg_rmask_ = rmaskn_.get();
+  }
+  for (auto *b : {&r_, &p_, &z_, &ap_, &ro_, &pw_}) b->alloc(std::max<long long>(1, nb));
+  part_.alloc(3 * kRedBlocks);
+  scal_.alloc(S_NSCAL);
+  scal_.zero(st_);
+  lmap_.alloc((size_t)std::max<long>(1, nloc_cross_) * nmap_);
+  if (nmap_ == 3) {
+    if (fp32_) lmapf_.alloc((size_t)std::max<long>(1, nloc_cross_));
+    else lmapg_.alloc((size_t)std::max<long>(1, nloc_cross_) * 2);
+  }
+  MADAM_CUDA(cudaMemcpyAsync(r_.get(), yba_.get(), nb * sizeof(double), cudaMemcpyDeviceToDevice,
+                             st_));
+  aa_.zero(st_);
+  apply_preconditioner(r_.get(), z_.get());
+  MADAM_LAUNCH(k_update_p, grid_for(nb), 256, 0, st_, p_.get(), z_.get(), pw_.get(), pcg_bw_,
+               nb, scal_.get(), 1);
+  MADAM_LAUNCH(k_dots, kRedBlocks, 256, 0, st_, r_.get(), z_.get(), r_.get(), r_.get(), nullptr,
+               nullptr, 2, pcg_rmask_, nb, part_.get());
+  finish_dots(2, 0, S_RZ, kRedBlocks, true);
+  scal_host_.assign(S_NSCAL, 0.0);
+  MADAM_CUDA(cudaMemcpyAsync(scal_host_.data(), scal_.get(), S_NSCAL * sizeof(double),
+                             cudaMemcpyDeviceToHost, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  const double rzinit = scal_host_[S_RZ];
+  rrinit = scal_host_[S_RR];
+  rr_final = 1.0;
+  noiter = 0;
+  pcg_istep_ = 0;
+  check_nan_iterate(rzinit, nb);
+  pcg_reset();
+  return !(rzinit < fsp(1e-30f) || std::isnan(rzinit)) && par_.iter_max > 0;
+}
+
+void Engine::pcg_use_stream(cudaStream_t s) {
+  if (!pcg_own_st_) pcg_own_st_ = st_;
+  st_ = s ? s : pcg_own_st_;
+  g_alloc_stream = st_;
+}
+
+void Engine::pcg_apply() {
+  ++pcg_istep_;
+  apply_A(p_.get(), pw_.get(), ap_.get(), false);
+}
+
+void Engine::pcg_precond() { apply_preconditioner(r_.get(), z_.get()); }
+
+PcgJob Engine::pcg_job() {
+  PcgJob j{};
+  j.aa = aa_.get();
+  j.r = r_.get();
+  j.ro = ro_.get();
+  j.p = p_.get();
+  j.ap = ap_.get();
+  j.z = z_.get();
+  j.pw = pw_.get();
+  j.bw = pcg_bw_;
+  j.rmask = pcg_rmask_;
+  j.part = part_.get();
+  j.scal = scal_.get();
+  j.nb = (long long)ndet_ * noba_short_ * nbasis_;
+  j.active = 1;
+  return j;
+}
+
+bool Engine::pcg_after(double rz, double rr) {
+  return pcg_judge(pcg_istep_, rz, rr) || pcg_istep_ >= par_.iter_max;
+}
+
+void Engine::pcg_end() {
+  check_band_err();
+  if (pcg_istep_ > 0)
+    MADAM_CUDA(cudaMemcpyAsync(wamap_.get(), lmap_.get(), wamap_.n * sizeof(double),
+                               cudaMemcpyDeviceToDevice, st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  pcg_use_stream(nullptr);
+  pcg_own_st_ = nullptr;
+  timings.iterate_ms = now_ms() - pcg_t0_;
+}
+
+void pcg_shared(cudaStream_t st, const PcgJob *tab, int n, long long nbmax, int step,
+                double *out) {
+  if (n <= 0) return;
+  if (n > 65535) fail("too many jobs in one stepper round");
+  if (step == 0) {
+    MADAM_LAUNCH(k_pcg_update_ar_j, dim3(grid_for(nbmax), (unsigned)n), 256, 0, st, tab);
+  } else if (step == 1) {
+    MADAM_LAUNCH(k_pcg_dots_j, dim3(kRedBlocks, (unsigned)n), 256, 0, st, tab);
+    MADAM_LAUNCH(k_pcg_finish_j, (unsigned)n, 1024, 0, st, tab, kRedBlocks, out);
+  } else {
+    MADAM_LAUNCH(k_pcg_update_p_j, dim3(grid_for(nbmax), (unsigned)n), 256, 0, st, tab);
+  }
 }
 
 void Engine::subtract_baselines() {
@@ -2568,9 +2693,11 @@ void Engine::writeback_host() {
   MADAM_CUDA(cudaStreamSynchronize(st_));
 }
 
-void Engine::run(const Params &par, std::vector<Detector> dets, long ndet, long nsamp, long nnz,
-                 double *timestamps, int32_t *pix, float *pixweights, double *signal,
-                 long nperiod, const long *periods, bool is_device) {
+// destripe() up to the PCG: inputs, layout, filter, flagging, pointing
+// tables, binning, right-hand side, preconditioner (smadam.F90:64-362)
+void Engine::run_setup(const Params &par, std::vector<Detector> dets, long ndet, long nsamp,
+                       long nnz, double *timestamps, int32_t *pix, float *pixweights,
+                       double *signal, long nperiod, const long *periods, bool is_device) {
   g_alloc_stream = st_;
   const double t0 = now_ms();
   timings = Timings();
@@ -2665,20 +2792,34 @@ void Engine::run(const Params &par, std::vector<Detector> dets, long ndet, long 
     mark(8);
     construct_preconditioner();
     mark(9);
-    MADAM_CUDA(cudaStreamSynchronize(st_));
-    timings.setup_ms = now_ms() - t0;
-    // write_covmat in place of the solve (smadam.F90:364-377)
-    if (par_.file_covmat.empty()) iterate();
-    else write_covmat();
-  } else {
-    MADAM_CUDA(cudaStreamSynchronize(st_));
-    timings.setup_ms = now_ms() - t0;
   }
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  timings.setup_ms = now_ms() - t0;
+  run_t0_ = t0;
+}
+
+void Engine::run(const Params &par, std::vector<Detector> dets, long ndet, long nsamp, long nnz,
+                 double *timestamps, int32_t *pix, float *pixweights, double *signal,
+                 long nperiod, const long *periods, bool is_device) {
+  run_setup(par, std::move(dets), ndet, nsamp, nnz, timestamps, pix, pixweights, signal, nperiod,
+            periods, is_device);
+  run_solve();
+  run_finish();
+}
+
+void Engine::run_solve() {
+  if (!par_.kfirst) return;
+  // write_covmat in place of the solve (smadam.F90:364-377)
+  if (par_.file_covmat.empty()) iterate();
+  else write_covmat();
+}
+
+void Engine::run_finish() {
   const double tf = now_ms();
   finalize(true);
   timings.finalize_ms = now_ms() - tf;
   if (par_.mcmode) cached_ = true;
-  timings.total_ms = now_ms() - t0;
+  timings.total_ms = now_ms() - run_t0_;
 }
 
 void Engine::run_cached(long ndet, long nsamp, long nnz, double *timestamps, int32_t *pix,

@@ -2,19 +2,32 @@
 //
 // Callers submit complete destripe() jobs (the arguments of the reference
 // C-ABI, smadam.F90:64-101; float64 signals, or float32 signals for the
-// FP32-TOD form of destripe_fp32) and collect their products later.  A fixed set
-// of worker threads each owns an engine with its own CUDA stream, so jobs in
-// flight overlap on the device.  A job is admitted when its estimated device
-// footprint fits the memory budget next to the jobs already running (the
-// first job in flight is always admitted); admission is first come, first
-// served, so a large job at the head of the queue holds back smaller ones
-// behind it until memory frees up.  Every job runs the kernels of a lone
-// destripe() on its own engine, so its products do not depend on what else
-// is in flight (up to the rounding-level order effects of the setup's
-// atomic sums, which differ between any two runs).  Each job's products (maps, hits, baselines, scalars) are
-// copied to host memory when it finishes, and the worker's engine moves on.
-// The caller's buffers must stay valid until its job is done; host pixel
-// buffers are written back like destripe() does.
+// FP32-TOD form of destripe_fp32) and collect their products later.  A fixed
+// set of worker threads, the job slots, each owns an engine with its own CUDA
+// stream.  A job is admitted when its estimated device footprint fits the
+// memory budget next to the jobs already running (the first job in flight is
+// always admitted); admission is first come, first served, so a large job at
+// the head of the queue holds back smaller ones behind it until memory frees
+// up.  A worker runs its job's setup (everything before the PCG) on its
+// engine, so the setups of jobs in flight overlap on the device.
+//
+// Continuous batching of the PCG: the jobs whose setup is done iterate in
+// shared rounds driven by one stepper thread.  Per round every job in flight
+// takes one PCG iteration: the stepper queues each job's A p (projections,
+// filter) and preconditioner on one of a few streams, so the jobs' kernels
+// overlap, and runs the CG vector algebra of all jobs in shared launches (one
+// kernel each for aa/r/ro, for the inner products, for the CG scalars and for
+// p; pcg_shared), then one host synchronisation serves every job's
+// convergence test.  Jobs join the rounds when their setup finishes and leave
+// when they converge, each with its own CG scalars, iteration count and
+// stopping rule.  A job's arithmetic is that of a lone destripe() (same
+// kernels, grids and reduction order), so its products do not depend on what
+// else is in flight (up to the rounding-level order effects of the setup's
+// atomic sums, which differ between any two runs).  Each job's products
+// (maps, hits, baselines, scalars) are copied to host memory when it
+// finishes, and the worker's engine moves on.  The caller's buffers must stay
+// valid until its job is done; host pixel buffers are written back like
+// destripe() does.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -73,6 +86,13 @@ size_t job_bytes(const Job &j) {
   return (size_t)b;
 }
 
+// A job handed from its worker to the stepper for the PCG rounds.
+struct Stepping {
+  Engine *eng = nullptr;
+  bool done = false, failed = false;
+  std::string err;
+};
+
 class Server {
  public:
   int device() const { return device_; }
@@ -81,15 +101,43 @@ class Server {
     size_t fr = 0, tot = 0;
     MADAM_CUDA(cudaMemGetInfo(&fr, &tot));
     budget_ = (size_t)(frac * (double)fr);
+    MADAM_CUDA(cudaStreamCreateWithFlags(&ssm_, cudaStreamNonBlocking));
+    MADAM_CUDA(cudaEventCreateWithFlags(&se0_, cudaEventDisableTiming));
+    for (int k = 0; k < kStepStreams; ++k) {
+      MADAM_CUDA(cudaStreamCreateWithFlags(&ssa_[k], cudaStreamNonBlocking));
+      MADAM_CUDA(cudaEventCreateWithFlags(&sek_[k], cudaEventDisableTiming));
+    }
+    stepper_ = std::thread([this] { stepper(); });
     for (int i = 0; i < nworkers; ++i) threads_.emplace_back([this] { worker(); });
   }
+  // rounds, job-rounds (jobs summed over rounds), most jobs in one round
+  void stats(double *out) {
+    std::lock_guard<std::mutex> lk(smu_);
+    out[0] = (double)rounds_;
+    out[1] = (double)job_rounds_;
+    out[2] = (double)max_round_;
+  }
   ~Server() {
+    // the workers finish their jobs (whose PCG needs the stepper), then the
+    // stepper stops
     {
       std::lock_guard<std::mutex> lk(mu_);
       stop_ = true;
     }
     cv_work_.notify_all();
     for (auto &t : threads_) t.join();
+    {
+      std::lock_guard<std::mutex> lk(smu_);
+      sstop_ = true;
+    }
+    scv_in_.notify_all();
+    stepper_.join();
+    for (int k = 0; k < kStepStreams; ++k) {
+      cudaEventDestroy(sek_[k]);
+      cudaStreamDestroy(ssa_[k]);
+    }
+    cudaEventDestroy(se0_);
+    cudaStreamDestroy(ssm_);
   }
   long submit(std::unique_ptr<Job> j) {
     std::lock_guard<std::mutex> lk(mu_);
@@ -154,8 +202,29 @@ class Server {
       try {
         if (!eng) eng.reset(new Engine());
         eng->set_fp32(j->fp32);
-        eng->run(j->par, j->dets, j->ndet, j->nsamp, j->nnz, j->ts, j->pix, j->w, j->sig,
-                 (long)j->periods.size(), j->periods.data(), j->dev);
+        eng->run_setup(j->par, j->dets, j->ndet, j->nsamp, j->nnz, j->ts, j->pix, j->w, j->sig,
+                       (long)j->periods.size(), j->periods.data(), j->dev);
+        if (eng->stepwise_ok() && !stepper_dead_) {
+          // the PCG in the stepper's shared rounds
+          if (eng->pcg_begin()) {
+            Stepping sp;
+            sp.eng = eng.get();
+            {
+              std::lock_guard<std::mutex> lk(smu_);
+              incoming_.push_back(&sp);
+            }
+            scv_in_.notify_all();
+            {
+              std::unique_lock<std::mutex> lk(smu_);
+              scv_done_.wait(lk, [&] { return sp.done; });
+            }
+            if (sp.failed) throw Error(sp.err);
+          }
+          eng->pcg_end();
+        } else {
+          eng->run_solve();
+        }
+        eng->run_finish();
         for (const char *nm : {"map", "binmap", "hits", "mask", "aa", "scalars", "rr_history"}) {
           const long sz = eng->result_size(nm);
           const size_t el = (std::strcmp(nm, "hits") == 0 || std::strcmp(nm, "mask") == 0)
@@ -185,6 +254,183 @@ class Server {
       cv_work_.notify_all();
     }
   }
+
+  // The PCG rounds of the jobs in flight (see the file comment).
+  void stepper() {
+    constexpr int K = kStepStreams;
+    cudaStream_t sm = ssm_, (&sa)[K] = ssa_;
+    cudaEvent_t e0 = se0_, (&ek)[K] = sek_;
+    if (cudaSetDevice(device_) != cudaSuccess) {
+      // the jobs then run their PCG on their own workers; any handed over
+      // before this was seen fail
+      stepper_dead_ = true;
+      for (;;) {
+        std::unique_lock<std::mutex> lk(smu_);
+        scv_in_.wait(lk, [&] { return sstop_ || !incoming_.empty(); });
+        for (Stepping *sp : incoming_) {
+          sp->failed = true;
+          sp->err = "the PCG stepper could not select the device";
+          sp->done = true;
+        }
+        incoming_.clear();
+        scv_done_.notify_all();
+        if (sstop_) return;
+      }
+    }
+    g_alloc_stream = sm;
+    DevBuf<PcgJob> tab_d;
+    DevBuf<double> out_d;
+    double *out_h = nullptr;
+    size_t cap = 0;
+    std::vector<Stepping *> active;
+    std::vector<PcgJob> tab;
+    auto finish = [&](Stepping *sp, const char *err) {
+      std::lock_guard<std::mutex> lk(smu_);
+      if (err) {
+        sp->failed = true;
+        sp->err = err;
+      }
+      sp->done = true;
+    };
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(smu_);
+        scv_in_.wait(lk, [&] { return sstop_ || !incoming_.empty() || !active.empty(); });
+        for (Stepping *sp : incoming_) active.push_back(sp);
+        incoming_.clear();
+        if (active.empty() && sstop_) break;
+      }
+      if (active.empty()) continue;
+      const int n = (int)active.size();
+      tab.resize(n);
+      std::vector<char> stop(n, 0);
+      std::vector<std::string> msgs(n);
+      std::vector<char> failed(n, 0);
+      try {
+        if ((size_t)n > cap) {
+          if (out_h) cudaFreeHost(out_h);
+          out_h = nullptr;
+          cap = 0;
+          const size_t c = std::max<size_t>(16, 2 * (size_t)n);
+          tab_d.alloc(c);
+          out_d.alloc(2 * c);
+          MADAM_CUDA(cudaMallocHost((void **)&out_h, 2 * c * sizeof(double)));
+          cap = c;
+        }
+        round(active, tab, stop, failed, msgs, sm, sa, e0, ek, tab_d.get(), out_d.get(), out_h);
+      } catch (const std::exception &e) {
+        // a failure of the shared launches: every job of the round fails
+        for (int i = 0; i < n; ++i)
+          if (!failed[i]) {
+            failed[i] = 1;
+            msgs[i] = e.what();
+          }
+        cudaStreamSynchronize(sm);
+        for (int k = 0; k < K; ++k) cudaStreamSynchronize(sa[k]);
+      }
+      g_alloc_stream = sm;
+      {
+        std::lock_guard<std::mutex> lk(smu_);
+        ++rounds_;
+        job_rounds_ += n;
+        max_round_ = std::max(max_round_, (long)n);
+      }
+      std::vector<Stepping *> keep;
+      bool any = false;
+      for (int i = 0; i < n; ++i) {
+        if (failed[i] || stop[i]) {
+          active[i]->eng->pcg_use_stream(nullptr);  // back to the job's own stream
+          g_alloc_stream = sm;
+          finish(active[i], failed[i] ? msgs[i].c_str() : nullptr);
+          any = true;
+        } else {
+          keep.push_back(active[i]);
+        }
+      }
+      active.swap(keep);
+      if (any) scv_done_.notify_all();
+    }
+    if (out_h) cudaFreeHost(out_h);
+    tab_d.reset();
+    out_d.reset();
+    cudaStreamSynchronize(sm);
+  }
+
+  // One PCG round of the jobs in `act`: A p of each job on the K job streams,
+  // aa, r and ro of all in one launch, z = M r of each, the inner products
+  // and CG scalars of all in two launches, one synchronisation, each job's
+  // convergence test, then p of those that go on in one launch.  A job whose
+  // own step throws is marked in `failed` and left out of the rest.
+  template <int K>
+  void round(const std::vector<Stepping *> &act, std::vector<PcgJob> &tab,
+             std::vector<char> &stop, std::vector<char> &failed, std::vector<std::string> &msgs,
+             cudaStream_t sm, cudaStream_t (&sa)[K], cudaEvent_t e0, cudaEvent_t (&ek)[K],
+             PcgJob *tab_d, double *out_d, double *out_h) {
+    const int n = (int)act.size();
+    long long nbmax = 1;
+    for (int i = 0; i < n; ++i) {
+      act[i]->eng->pcg_use_stream(sa[i % K]);
+      tab[i] = act[i]->eng->pcg_job();
+      nbmax = std::max(nbmax, tab[i].nb);
+    }
+    auto fork = [&]() {  // the job streams wait for the main stream
+      MADAM_CUDA(cudaEventRecord(e0, sm));
+      for (int k = 0; k < K; ++k) MADAM_CUDA(cudaStreamWaitEvent(sa[k], e0, 0));
+    };
+    auto join = [&]() {  // and the main stream for them
+      for (int k = 0; k < K; ++k) {
+        MADAM_CUDA(cudaEventRecord(ek[k], sa[k]));
+        MADAM_CUDA(cudaStreamWaitEvent(sm, ek[k], 0));
+      }
+    };
+    auto each = [&](auto &&f) {  // a job's own step; a failure drops the job
+      for (int i = 0; i < n; ++i) {
+        if (failed[i] || stop[i]) continue;
+        try {
+          f(i);
+        } catch (const std::exception &e) {
+          msgs[i] = e.what();
+          failed[i] = 1;
+          tab[i].active = 0;
+        }
+      }
+    };
+    auto upload = [&]() {
+      MADAM_CUDA(cudaMemcpyAsync(tab_d, tab.data(), n * sizeof(PcgJob), cudaMemcpyHostToDevice,
+                                 sm));
+    };
+    fork();
+    each([&](int i) { act[i]->eng->pcg_apply(); });
+    join();
+    upload();
+    pcg_shared(sm, tab_d, n, nbmax, 0, nullptr);
+    fork();
+    each([&](int i) { act[i]->eng->pcg_precond(); });
+    join();
+    upload();
+    pcg_shared(sm, tab_d, n, nbmax, 1, out_d);
+    MADAM_CUDA(cudaMemcpyAsync(out_h, out_d, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, sm));
+    MADAM_CUDA(cudaStreamSynchronize(sm));
+    each([&](int i) {
+      stop[i] = act[i]->eng->pcg_after(out_h[2 * i], out_h[2 * i + 1]) ? 1 : 0;
+      if (stop[i]) tab[i].active = 0;
+    });
+    join();  // the reliable updates a convergence test may run
+    upload();
+    pcg_shared(sm, tab_d, n, nbmax, 2, nullptr);
+    MADAM_CUDA(cudaStreamSynchronize(sm));
+  }
+
+  static constexpr int kStepStreams = 4;  // streams the jobs' own kernels spread over
+  cudaStream_t ssm_ = nullptr, ssa_[kStepStreams] = {};
+  cudaEvent_t se0_ = nullptr, sek_[kStepStreams] = {};
+  std::atomic<bool> stepper_dead_{false};
+  std::thread stepper_;
+  std::mutex smu_;
+  std::condition_variable scv_in_, scv_done_;
+  std::vector<Stepping *> incoming_;
+  bool sstop_ = false;
+  long rounds_ = 0, job_rounds_ = 0, max_round_ = 0;
 
   int device_ = 0;
   size_t budget_ = 0, in_flight_ = 0;
@@ -333,6 +579,13 @@ int madam_b200_serve_error(void *srv, long job, char *buf, long buflen) {
 int madam_b200_serve_release(void *srv, long job) {
   Server *s = (Server *)srv;
   return s ? s->release(job) : 1;
+}
+
+int madam_b200_serve_stats(void *srv, double *out, long nout) {
+  Server *s = (Server *)srv;
+  if (!s || nout < 3) return 1;
+  s->stats(out);
+  return 0;
 }
 
 int madam_b200_serve_close(void *srv) {

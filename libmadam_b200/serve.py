@@ -52,6 +52,8 @@ def _lib_serve():
     L.madam_b200_serve_error.argtypes = [P, ct.c_long, ct.c_char_p, ct.c_long]
     L.madam_b200_serve_release.restype = ct.c_int
     L.madam_b200_serve_release.argtypes = [P, ct.c_long]
+    L.madam_b200_serve_stats.restype = ct.c_int
+    L.madam_b200_serve_stats.argtypes = [P, P, ct.c_long]
     L.madam_b200_serve_close.restype = ct.c_int
     L.madam_b200_serve_close.argtypes = [P]
     L._serve_ready = True
@@ -143,6 +145,13 @@ class Server:
             raise RuntimeError("job {} is not finished".format(ticket.job))
         keys = ("t_submit", "t_start", "t_end", "samples", "iterations", "bytes")
         return dict(zip(keys, out.tolist()))
+
+    def stats(self):
+        """PCG rounds run by the stepper, job-rounds (jobs summed over the
+        rounds) and the most jobs in one round."""
+        out = np.zeros(3)
+        self._L.madam_b200_serve_stats(self._h, out.ctypes.data_as(ct.c_void_p), 3)
+        return dict(rounds=int(out[0]), job_rounds=int(out[1]), max_jobs=int(out[2]))
 
     def release(self, ticket):
         self._L.madam_b200_serve_release(self._h, ticket.job)

@@ -1,9 +1,12 @@
 """Serving: jobs of uneven sizes in flight together give the products each
 gives alone (same hits and PCG iteration count; maps and baselines within
-SERVE_RTOL of their largest magnitude: the setup's pixel-matrix and binning
-scatter sums with FP64 atomics, so two runs of one job agree to rounding,
-~1e-11 after the PCG, not to the bit), a failing job does not disturb the
-others, and device buffers are served like host buffers."""
+SERVE_RTOL per pixel: the setup's pixel-matrix and binning scatter sums with
+FP64 atomics, so two runs of one job agree to rounding, ~1e-11 after the
+PCG, not to the bit), a failing job does not disturb the others, and device
+buffers are served like host buffers.  The jobs' PCG iterations run in the
+stepper's shared rounds: the job-rounds it counts are the served jobs'
+iterations summed, and with several jobs past their setup at once a round
+carries more than one job."""
 import numpy as np
 import pytest
 
@@ -88,7 +91,35 @@ def test_jobs_in_flight_match_jobs_alone(W):
         _close(served[i]["aa"], O.result("aa"), MAP_RTOL, "aa")
     with pytest.raises(RuntimeError, match="Too large pixel number"):
         srv.wait(tb)
+    st = srv.stats()
+    assert st["job_rounds"] == sum(int(a["noiter"]) for a in alone)
+    assert st["rounds"] <= st["job_rounds"]
     srv.close()
+
+
+def test_pcg_rounds_are_shared(W):
+    """Four jobs started together: their PCGs share rounds, and each gives
+    its lone result."""
+    from libmadam_b200.serve import Server
+    jobs = [syn.to_numpy(syn.generate(syn.small_config(nside=32, ndet=4, nsamp_obs=1 << 15,
+                                                       nobs=2, seed=60 + k)))
+            for k in range(4)]
+    alone = []
+    for d in jobs:
+        W.destripe(None, *_args(d))
+        alone.append(dict(map=W.get_result("map"), aa=W.get_result("aa"),
+                          noiter=W.scalars()["noiter"]))
+    srv = Server(workers=4, mem_fraction=0.5)
+    tickets = [srv.submit(*_args(d)) for d in jobs]
+    for t, ref in zip(tickets, alone):
+        assert srv.wait(t) == 2
+        assert srv.result(t, "scalars")[0] == ref["noiter"]
+        _close(srv.result(t, "map"), ref["map"], SERVE_RTOL)
+        _close(srv.result(t, "aa"), ref["aa"], SERVE_RTOL)
+    st = srv.stats()
+    srv.close()
+    assert st["job_rounds"] == sum(int(a["noiter"]) for a in alone)
+    assert st["max_jobs"] >= 2 and st["rounds"] < st["job_rounds"], st
 
 
 def test_device_buffers_are_served(W):
