@@ -385,74 +385,210 @@ def run_mc(args, world, rank, local):
 
 
 def run_serve(args, world, rank, local):
-    """Serving stream: requests of uneven size (nside 128-1024, 2-32 detectors,
-    2^18-2^22 samples per detector, base_first 0.25-2 s, cglimit 1e-10, half
-    of them with float32 TOD served in the FP32-TOD form) arrive
-    as a Poisson process and are served by libmadam_b200.serve; reports p50 /
-    p99 latency (submit to done) and aggregate throughput."""
+    """Serving stream with the request mix of the serving workload: requests
+    draw nside in {128, 256, 512, 1024}, 2-32 detectors, log-uniform 2^18-2^24
+    samples per detector, base_first in {0.25, 0.5, 1, 2} s and their own
+    seeded scan, sky and 1/f noise (fknee 0.02-0.2 Hz), cglimit 1e-10, half of
+    them float32 TOD (served in the FP32-TOD form); they arrive as a Poisson
+    process at args.rate and are served by libmadam_b200.serve.
+
+    A client thread generates the requests' inputs on the device (on its own
+    stream) ahead of their arrival, with at most 45% of the free HBM
+    outstanding, and a reaper frees them once the job is done, so that a
+    stream of any length fits the device.  The clock starts when the client
+    has filled that share (or generated every request), so a stream that fits
+    it runs with no generation beside the server; a longer one has the
+    client generating on the same GPU while it runs (client_generation_s
+    counts that time).  Latency is measured from the scheduled arrival to
+    the job's end (it includes any wait for the client) and from the
+    submission; throughput is samples over the makespan."""
+    import threading
     import torch
     from libmadam_b200 import synthetic as syn
     from libmadam_b200.serve import Server
     rng = np.random.default_rng(5005 + rank)
-    reqs = []
+    specs = []
     for i in range(args.requests):
-        cfg = syn.ScanConfig(
-            nside=int(rng.choice([128, 256, 512, 1024])), nside_submap=16,
-            ndet=int(rng.integers(2, 33)), nobs=1,
-            nsamp_obs=int(2 ** rng.uniform(18, 22)), fsample=100.0,
-            fknee=float(rng.uniform(0.02, 0.2)), alpha=-1.0,
-            base_first=float(rng.choice([0.25, 0.5, 1.0, 2.0])), seed=7000 + i,
-            extra_pars=dict(cglimit=1e-10))
-        d = syn.generate(cfg, device="cuda")
-        d["pixels"] = d["pixels"].reshape(-1)
-        d["pixweights"] = d["pixweights"].reshape(-1)
-        d["signal"] = d["signal"].reshape(-1)
-        if rng.random() < 0.5:  # mixed float32 / float64 TOD
-            d["signal"] = d["signal"].float()
-        reqs.append(d)
-    torch.cuda.synchronize()
+        specs.append(dict(
+            nside=int(rng.choice([128, 256, 512, 1024])), ndet=int(rng.integers(2, 33)),
+            nsamp=int(2 ** rng.uniform(18, 24)), fknee=float(rng.uniform(0.02, 0.2)),
+            base_first=float(rng.choice([0.25, 0.5, 1.0, 2.0])), f32=bool(rng.random() < 0.5),
+            seed=7000 + i))
     arrivals = np.cumsum(rng.exponential(1.0 / args.rate, args.requests))
+    free, _ = torch.cuda.mem_get_info()
+    gen_cap = 0.45 * free
+    cond = threading.Condition()
+    ready = [None] * len(specs)
+    state = dict(outstanding=0.0, gen_s=0.0, err=None, primed=False, gen_run_s=0.0,
+                 pregenerated=0)
+
+    def in_bytes(sp):
+        return sp["ndet"] * sp["nsamp"] * (4 + 12 + (4 if sp["f32"] else 8)) + 8 * sp["nsamp"]
+
+    def client():
+        try:
+            torch.cuda.set_device(local)
+            st = torch.cuda.Stream()
+            with torch.cuda.stream(st):
+                for i, sp in enumerate(specs):
+                    b = in_bytes(sp)
+                    with cond:
+                        if state["outstanding"] > 0 and state["outstanding"] + b > gen_cap:
+                            state["primed"] = True
+                            cond.notify_all()
+                        cond.wait_for(lambda: state["outstanding"] == 0
+                                      or state["outstanding"] + b <= gen_cap)
+                        state["outstanding"] += b
+                    tg = time.perf_counter()
+                    cfg = syn.ScanConfig(nside=sp["nside"], nside_submap=16, ndet=sp["ndet"],
+                                         nobs=1, nsamp_obs=sp["nsamp"], fsample=100.0,
+                                         fknee=sp["fknee"], alpha=-1.0,
+                                         base_first=sp["base_first"], seed=sp["seed"],
+                                         extra_pars=dict(cglimit=1e-10))
+                    d = syn.generate(cfg, device="cuda")
+                    d.pop("sky")
+                    d["pixels"] = d["pixels"].reshape(-1)
+                    d["pixweights"] = d["pixweights"].reshape(-1)
+                    d["signal"] = d["signal"].reshape(-1)
+                    if sp["f32"]:
+                        d["signal"] = d["signal"].float()
+                    st.synchronize()
+                    with cond:
+                        state["gen_s"] += time.perf_counter() - tg
+                        if state["primed"]:
+                            state["gen_run_s"] += time.perf_counter() - tg
+                        else:
+                            state["pregenerated"] += 1
+                        ready[i] = (d, b)
+                        cond.notify_all()
+            with cond:
+                state["primed"] = True
+                cond.notify_all()
+        except Exception as e:  # reported by the submitting loop
+            with cond:
+                state["err"] = e
+                state["primed"] = True
+                cond.notify_all()
+
+    tickets = [None] * len(specs)
+    t_sub = np.zeros(len(specs))
+    done = np.zeros(len(specs), dtype=bool)
+    infos = [None] * len(specs)
+    failures = []
+
+    def reaper():
+        left = set()
+        nsub = 0
+        while not done.all():
+            with cond:
+                while nsub < len(specs) and tickets[nsub] is not None:
+                    left.add(nsub)
+                    nsub += 1
+            fin = []
+            for i in left:
+                try:
+                    if srv.wait(tickets[i], 0.0) == 2:
+                        fin.append(i)
+                except RuntimeError as e:  # a failed job
+                    failures.append(str(e))
+                    fin.append(i)
+            for i in fin:
+                try:
+                    infos[i] = srv.info(tickets[i])
+                except RuntimeError:
+                    infos[i] = None
+                srv.release(tickets[i])
+                left.discard(i)
+                with cond:
+                    state["outstanding"] -= ready[i][1]
+                    ready[i] = None
+                    tickets[i] = 0
+                    done[i] = True
+                    cond.notify_all()
+            if not fin:
+                time.sleep(0.001)
+
+    th_c = threading.Thread(target=client, daemon=True)
+    th_c.start()
+    with cond:
+        cond.wait_for(lambda: state["primed"])
+        if state["err"] is not None:
+            raise state["err"]
     srv = Server(workers=args.workers, mem_fraction=0.8)
     clk = Clocks(local)
     t0 = time.perf_counter()
-    tickets = []
-    for d, ta in zip(reqs, arrivals):
+    th_r = threading.Thread(target=reaper, daemon=True)
+    th_r.start()
+    for i, ta in enumerate(arrivals):
         dt = ta - (time.perf_counter() - t0)
         if dt > 0:
             time.sleep(dt)
-        tickets.append(srv.submit(d["pars"], d["dets"], d["detweights"], d["timestamps"],
-                                  d["pixels"], d["pixweights"], d["signal"], d["periods"],
-                                  d["npsd"], d["psdstarts"], d["psdfreqs"], d["psdvals"]))
-    infos = []
-    for t in tickets:
-        srv.wait(t)
-        infos.append(srv.info(t))
-    makespan = max(i["t_end"] for i in infos) - min(i["t_submit"] for i in infos)
+        with cond:
+            cond.wait_for(lambda: ready[i] is not None or state["err"] is not None)
+            if state["err"] is not None:
+                raise state["err"]
+            d = ready[i][0]
+        t_sub[i] = time.perf_counter() - t0
+        tk = srv.submit(d["pars"], d["dets"], d["detweights"], d["timestamps"], d["pixels"],
+                        d["pixweights"], d["signal"], d["periods"], d["npsd"], d["psdstarts"],
+                        d["psdfreqs"], d["psdvals"])
+        with cond:
+            tickets[i] = tk
+    th_r.join()
     clocks = clk.stop()
+    stats = srv.stats()
     srv.close()
-    lat = np.array([i["t_end"] - i["t_submit"] for i in infos])
-    samples = np.array([i["samples"] for i in infos])
-    iters = np.array([i["iterations"] for i in infos])
+    if failures:
+        raise RuntimeError("%d serving jobs failed, the first: %s" % (len(failures), failures[0]))
+    lat_sub = np.array([inf["t_end"] - inf["t_submit"] for inf in infos])
+    lat = lat_sub + (t_sub - arrivals)
+    makespan = max(inf["t_end"] for inf in infos) - min(inf["t_submit"] for inf in infos)
+    samples = np.array([inf["samples"] for inf in infos])
+    iters = np.array([inf["iterations"] for inf in infos])
     line = {"metric": "serving latency p50 / p99 and TOD samples/s",
             "value": float(np.percentile(lat, 50) * 1e3), "unit": "ms (p50 latency)",
-            "p99_ms": float(np.percentile(lat, 99) * 1e3),
             "p50_ms": float(np.percentile(lat, 50) * 1e3),
+            "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "p50_ms_from_submit": float(np.percentile(lat_sub, 50) * 1e3),
+            "p99_ms_from_submit": float(np.percentile(lat_sub, 99) * 1e3),
             "n_gpus": 1, "higher_is_better": False, "vs_baseline": None,
             "dtype": "f64 and f32 (mixed TOD)", "data": "synthetic",
             "config": {"workload": "serving stream: %d requests, Poisson %.1f req/s, nside "
-                                   "128-1024, 2-32 detectors, 2^18-2^22 samples per detector, "
+                                   "128-1024, 2-32 detectors, 2^18-2^24 samples per detector, "
                                    "base_first 0.25-2 s, cglimit 1e-10, half the requests "
                                    "float32 TOD" % (args.requests, args.rate),
-                       "float32_requests": int(sum(1 for d in reqs
-                                                   if d["signal"].dtype == torch.float32)),
+                       "float32_requests": int(sum(sp["f32"] for sp in specs)),
                        "workers": args.workers},
             "clocks": clocks,
             "makespan_s": makespan,
+            "arrival_span_s": float(arrivals[-1]),
+            "requests_generated_before_the_clock": state["pregenerated"],
+            "client_generation_s_while_serving": state["gen_run_s"],
             "samples_per_s": float(samples.sum() / makespan),
             "samples_per_s_per_pcg_iteration": float((samples * iters).sum() / makespan),
             "mean_iterations": float(iters.mean()),
-            "total_samples": float(samples.sum())}
+            "total_samples": float(samples.sum()),
+            "job_phase_seconds_summed": {
+                k: float(sum(inf[k + "_ms"] for inf in infos) / 1e3)
+                for k in ("setup", "iterate", "finalize")},
+            "queue_seconds_summed": float(sum(inf["t_start"] - inf["t_submit"] for inf in infos)),
+            "pcg_rounds": stats["rounds"], "pcg_job_rounds": stats["job_rounds"],
+            "most_jobs_in_one_round": stats["max_jobs"],
+            "mean_jobs_per_round": stats["job_rounds"] / max(1, stats["rounds"])}
     return line if rank == 0 else None
+
+
+def extra_serve(args, world, rank, local):
+    """The serving stream for the headline line's "serving" key."""
+    r = run_serve(args, world, rank, local)
+    if r is None:
+        return None
+    out = {k: v for k, v in r.items() if k not in ("n_gpus", "higher_is_better", "vs_baseline",
+                                                   "data", "config")}
+    out["workload"] = r["config"]["workload"]
+    out["float32_requests"] = r["config"]["float32_requests"]
+    out["workers"] = r["config"]["workers"]
+    return out
 
 
 def run_destripe(args, world, rank, local, config, with_e2e=True, with_cpu=True):
@@ -718,7 +854,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default="2", choices=["2", "1", "3", "prof", "mid", "mid3", "small",
                                                    "mc", "mc-prof", "serve"])
-    ap.add_argument("--requests", type=int, default=60)
+    ap.add_argument("--requests", type=int, default=200,
+                    help="serving: requests in the stream (the serving workload names 2000; "
+                         "the headline line runs this many)")
     ap.add_argument("--rate", type=float, default=20.0)
     ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--nrhs", type=int, default=64)
@@ -756,10 +894,12 @@ def main():
                             with_e2e=not args.no_e2e, with_cpu=not args.no_cpu)
         if args.config == "2" and world == 1 and not args.only:
             # the headline line carries the precision form (float32 TOD at
-            # nside 1024) and the batched Monte Carlo form (64 realisations),
-            # each measured in the same run with its own clocks record
+            # nside 1024), the batched Monte Carlo form (64 realisations) and
+            # the serving stream, each measured in the same run with its own
+            # clocks record
             line["precision_form"] = extra_precision(args, world, rank, local)
             line["batched_mc"] = extra_mc(args, world, rank, local)
+            line["serving"] = extra_serve(args, world, rank, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -92,7 +92,9 @@ int madam_b200_destripe_with_cache_batch_fp32(int comm, long ndet, long nsamp, l
  * (float64 [npix][nmap]), "hits", "mask" (int32 [npix]), "aa" (float64
  * [ndet][noba]), "scalars" (float64 [24]), "rr_history" (float64);
  * serve_job_info gives out[0..5] = submit, start and end time (s), samples,
- * PCG iterations, admitted bytes; serve_error the message of a failed job;
+ * PCG iterations, admitted bytes, and with nout >= 9 out[6..8] = the job's
+ * setup, PCG and finalisation wall times (ms; the PCG's includes the shared
+ * rounds it waited in); serve_error the message of a failed job;
  * serve_release frees a finished job; serve_stats gives out[0..2] = PCG
  * rounds run, job-rounds (jobs summed over the rounds) and the most jobs in
  * one round; serve_close waits for the running jobs, drops the queued ones

@@ -238,7 +238,7 @@ void Engine::write_covmat() {
       for (int i = 0; i < nseg; ++i)
         for (long k = 0; k < nh; ++k)
           spec[(size_t)i * nh + k] =
-              1.0 / (fcov_host_[(size_t)seg_psd[i] * nh + k] + (double)nshort_ * seg_w[i]);
+              1.0 / (fcov_host()[(size_t)seg_psd[i] * nh + k] + (double)nshort_ * seg_w[i]);
       std::vector<double> imp(mtot, 0.0);
       std::vector<ConvSeg> cs(nseg);
       for (int i = 0; i < nseg; ++i) {

@@ -1030,6 +1030,174 @@ __global__ void k_fill_int(int *a, long long n, int v) {
     a[i] = v;
 }
 
+// ------------------------------------------------------- filter spectra --
+// The noise filter's spectra (build_filter, noise_routines.f90:367-739) on
+// the device: one thread per (PSD, frequency bin i < nof/2 + 1).  A PSD's
+// table is its frequencies and values with their logarithms (taken on the
+// host, as interpolate_psd takes them), `first` its first nonzero frequency.
+struct FiltTask {
+  int off, nin, first;
+  double plateau;  // white-noise level subtracted from the spectrum
+  double sigma;    // the detector's sigma before this filter (the inversion cut)
+};
+
+// interpolate_psd (noise_routines.f90:130-190) at one target: the bracket is
+// where the reference's monotone walk over ascending targets ends, i.e. the
+// last index j in [first, nin - 2] below which every frequency past `first`
+// is under the target (found by bisection: the frequencies are ascending).
+// The arithmetic is the host's, operation by operation; log and exp are
+// CUDA's.
+__device__ __forceinline__ double filt_interp(const FiltTask &T, const double *fr,
+                                              const double *ps, const double *lf,
+                                              const double *lp, double target) {
+  if (target == 0) return 0.0;
+  const double flog = log(target);
+  const int nin = T.nin;
+  int j = T.first;
+  if (j < nin - 2) {
+    // smallest k in [first + 1, nin - 2] with lf[k] >= flog; j = k - 1
+    int lo = j + 1, hi = nin - 2;
+    if (lf[T.off + hi] < flog) {
+      j = nin - 2;
+    } else {
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (lf[T.off + mid] < flog) lo = mid + 1;
+        else hi = mid;
+      }
+      j = lo - 1;
+    }
+  }
+  const double p0 = ps[T.off + j], p1 = ps[T.off + j + 1];
+  if (p0 > 0 && p1 > 0) {
+    const double l0 = lf[T.off + j], l1 = lf[T.off + j + 1];
+    const double r = __ddiv_rn(__dsub_rn(flog, l0), __dsub_rn(l1, l0));
+    return exp(__dadd_rn(__dmul_rn(lp[T.off + j], __dsub_rn(1.0, r)),
+                         __dmul_rn(lp[T.off + j + 1], r)));
+  }
+  const double f0 = fr[T.off + j], f1 = fr[T.off + j + 1];
+  const double r = __ddiv_rn(__dsub_rn(target, f0), __dsub_rn(f1, f0));
+  return __dadd_rn(__dmul_rn(p0, __dsub_rn(1.0, r)), __dmul_rn(p1, r));
+}
+
+// One aliased term of bin j at alias k: spectrum minus the plateau (or its
+// margin-th part), times the sinc^2 window.  Sets bit 0 of *flag for a
+// spectrum value that is not positive (the reference then fills it from its
+// neighbours, which the host does).
+__device__ __forceinline__ double filt_term(const FiltTask &T, const double *fr, const double *ps,
+                                            const double *lf, const double *lp, int k, long j,
+                                            long nof, double fa, double margin, int *flag) {
+  const double f = __dadd_rn(__dmul_rn((double)k, fa), __ddiv_rn(__dmul_rn((double)j, fa),
+                                                                 (double)nof));
+  double sp = filt_interp(T, fr, ps, lf, lp, f);
+  sp = (sp > __dmul_rn(T.plateau, __dadd_rn(1.0, margin))) ? __dsub_rn(sp, T.plateau)
+                                                           : __dmul_rn(sp, margin);
+  if (k == 0 && j == 0) sp = 0.0;  // f[0] == 0: the mean carries no noise
+  else if (sp <= 0) atomicOr(flag, 1);
+  const double kPi = 3.141592653589793238462643383279502884197;
+  const double x = __ddiv_rn(__dmul_rn(kPi, f), fa);
+  const double sx = sin(x);
+  const double g = (x < (double)1e-30f) ? 1.0 : __ddiv_rn(__dmul_rn(sx, sx), __dmul_rn(x, x));
+  return __dmul_rn(sp, g);
+}
+
+__global__ void k_filter_spectra(const FiltTask *tasks, const double *fr, const double *ps,
+                                 const double *lf, const double *lp, long nof, long nh, double fa,
+                                 double margin, double *fcov, int *flag) {
+  const FiltTask T = tasks[blockIdx.y];
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nh;
+       i += (long)gridDim.x * blockDim.x) {
+    double a = 0.0;
+    for (int k = 0; k <= 2; ++k) {
+      if (i == 0) {
+        const double t0 = filt_term(T, fr, ps, lf, lp, k, 0, nof, fa, margin, flag);
+        // aspec[0] = spec[0] at k = 0, then += 2 spec[0] g[0]; t0 = spec * g
+        // with g[0] = 1 at k = 0
+        a = (k == 0) ? t0 : __dadd_rn(a, __dmul_rn(2.0, t0));
+      } else {
+        const double t1 = filt_term(T, fr, ps, lf, lp, k, i, nof, fa, margin, flag);
+        const double t2 = filt_term(T, fr, ps, lf, lp, k, nof - i, nof, fa, margin, flag);
+        a = __dadd_rn(__dadd_rn(a, t1), t2);
+      }
+    }
+    double v = (fabs(a) > __dmul_rn(T.sigma, (double)1e-30f)) ? __ddiv_rn(1.0, __dmul_rn(fa, a))
+                                                               : 0.0;
+    if (i == 0) v = 0.0;
+    if (isnan(v)) atomicOr(flag, 2);
+    fcov[(long)blockIdx.y * nh + i] = v;
+  }
+}
+
+// The Fourier-domain preconditioner 1 / (nshort w + fcov) per PSD and bin
+// (construct_preconditioner, noise_routines.f90:920-1153).
+__global__ void k_fprec(const double *fcov, const double *w, long nh, long npsd, double nshort,
+                        double *fp) {
+  const long n = nh * npsd;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x)
+    fp[i] = __ddiv_rn(1.0, __dadd_rn(__dmul_rn(nshort, w[i / nh]), fcov[i]));
+}
+
+// Power of each PSD's inverse-covariance kernel, summed in the host's order
+// (one thread per PSD): ptot = sum_{k < nof/2} icv_k^2 and the running sums
+// pre[k] = sum_{k' <= k} icv_k'^2 for k < W, from which the band width is
+// chosen.
+__global__ void k_invcov_power(const double *icv, long nof, long npsd, long W, double *ptot,
+                               double *pre) {
+  const long ip = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (ip >= npsd) return;
+  const double *c = icv + ip * nof;
+  double s = 0.0;
+  for (long k = 0; k < nof / 2; ++k) s = __dadd_rn(s, __dmul_rn(c[k], c[k]));
+  ptot[ip] = s;
+  double q = 0.0;
+  for (long k = 0; k < W; ++k) {
+    q = __dadd_rn(q, __dmul_rn(c[k], c[k]));
+    pre[ip * W + k] = q;
+  }
+}
+
+__global__ void k_iota(int *a, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    a[i] = (int)i;
+}
+
+// Scatter chunks of the pixel-sorted pointing: pixel p's entries
+// off[p]..off[p+1] cut into ceil(n / K) chunks (one for an empty pixel).
+// Pass 0 counts per pixel (chunks, partial-sum slots: the chunks of a pixel
+// cut in several, pixels cut in several); pass 1 writes the chunks
+// (pixel, first entry, count, slot or -1) and the multi-chunk pixels (pixel,
+// first slot, chunks, 0) at the exclusive prefix sums of those counts.
+__global__ void k_scatter_chunk_count(const int *off, int npix, int K, int *nck, int *nslot,
+                                      int *nmulti) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+    const int n = off[p + 1] - off[p];
+    const int nc = max(1, (n + K - 1) / K);
+    nck[p] = nc;
+    nslot[p] = nc > 1 ? nc : 0;
+    nmulti[p] = nc > 1 ? 1 : 0;
+  }
+}
+
+__global__ void k_scatter_chunk_fill(const int *off, int npix, int K, const int *ck_off,
+                                     const int *slot_off, const int *multi_off, int4 *ck,
+                                     int4 *multi) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+    const int e0 = off[p], n = off[p + 1] - off[p];
+    const int nc = max(1, (n + K - 1) / K);
+    const int c0 = ck_off[p];
+    if (nc == 1) {
+      ck[c0] = make_int4(p, e0, n, -1);
+      continue;
+    }
+    const int s0 = slot_off[p];
+    multi[multi_off[p]] = make_int4(p, s0, nc, 0);
+    for (int c = 0; c < nc; ++c)
+      ck[c0 + c] = make_int4(p, e0 + c * K, min(K, n - c * K), s0 + c);
+  }
+}
+
 // masked dot products sum_i mask_i a_i b_i for up to 3 pairs
 __global__ void k_dots(const double *a0, const double *b0, const double *a1, const double *b1,
                        const double *a2, const double *b2, int nd, const uint8_t *mask,

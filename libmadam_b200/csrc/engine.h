@@ -440,10 +440,24 @@ class Engine {
   DevBuf<double> p2y_;  // forward solution L^-1 r, full baseline vector
   DevBuf<int> band2_err_;  // a staging wait of the guarded solve ran out
   void check_band_err();
+  // setup trace: with MADAM_B200_TRACE set, each step's host time (after a
+  // synchronisation of the stream) goes to stderr
+  bool trace_on_ = false;
+  double trace_t_ = 0;
+  cudaEvent_t trace_ev_[2] = {nullptr, nullptr};
+  void trace(const char *what);
   long n_band_fail_ = 0;
   std::unique_ptr<FFTPlan> fft_;
   std::future<void> filter_job_;  // host spectra of build_filter
   std::string filter_err_;
+  // filter spectra computed on the device (build_filter); the host copy of
+  // fcov and of the inverse-covariance kernels is made when asked for
+  bool filter_dev_ = false, fcov_host_valid_ = false, invcov_valid_ = false;
+  DevBuf<int> filter_flag_;
+  std::vector<std::pair<long, int>> filter_tasks_;
+  std::vector<double> filter_sigma0_;
+  const std::vector<double> &fcov_host();
+  const std::vector<double> &invcov_host();
   std::unique_ptr<CgpWork> cgp_;
 
   // pixels flagged during the call (host write-back)

@@ -60,6 +60,8 @@ Engine::~Engine() {
   cudaStreamSynchronize(st_);
   g_alloc_stream = nullptr;
   for (auto &e : ev_) cudaEventDestroy(e);
+  for (auto &e : trace_ev_)
+    if (e) cudaEventDestroy(e);
   if (ev_ptr_) cudaEventDestroy(ev_ptr_);
   if (ev_tod_) cudaEventDestroy(ev_tod_);
   if (cst_) cudaStreamDestroy(cst_);
@@ -553,6 +555,35 @@ void Engine::flag_and_compact(bool first_call) {
   }
 }
 
+void Engine::trace(const char *what) {
+  if (!trace_on_) return;
+  // host time since the last point, and the stream's own time between
+  // events recorded at the two points
+  if (!trace_ev_[0]) {
+    MADAM_CUDA(cudaEventCreate(&trace_ev_[0]));
+    MADAM_CUDA(cudaEventCreate(&trace_ev_[1]));
+    MADAM_CUDA(cudaEventRecord(trace_ev_[0], st_));
+  }
+  MADAM_CUDA(cudaEventRecord(trace_ev_[1], st_));
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  float dev_ms = 0;
+  MADAM_CUDA(cudaEventElapsedTime(&dev_ms, trace_ev_[0], trace_ev_[1]));
+  std::swap(trace_ev_[0], trace_ev_[1]);
+  const double t = now_ms();
+  int dev = 0;
+  cudaMemPool_t pool;
+  uint64_t reserved = 0, used = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+  }
+  std::fprintf(stderr,
+               "madam_b200 trace: %-28s %9.3f ms (stream %9.3f ms)  pool %.2f GB reserved, "
+               "%.2f GB used\n",
+               what, t - trace_t_, dev_ms, reserved / 1e9, used / 1e9);
+  trace_t_ = t;
+}
+
 void Engine::build_runs() {
   const long long n = (long long)ndet_ * nsamp_;
   const SampleMap sm = sample_map(istart_d_.get(), kstart_d_.get(), (int)ninterval_, nsamp_,
@@ -593,6 +624,7 @@ void Engine::build_runs() {
   MADAM_CUDA(cudaStreamSynchronize(st_));
   sflag.reset();
   eflag.reset();
+  trace("runs: flags+select");
   if (cnt[0] != cnt[1]) fail("internal: unpaired run boundaries");
   const long long nr0 = cnt[0];
   if (nr0 == 0) return;
@@ -627,17 +659,12 @@ void Engine::build_runs() {
                  nr0, sm, p4, pc, tile_shift_, runs0.get(), keys.get(), lens.get());
   starts.reset();
   ends.reset();
+  trace("runs: split+emit");
   // bucket runs by tile (stable radix sort keeps time order inside a tile)
   idx.alloc(nr);
   idx_sorted.alloc(nr);
   keys_sorted.alloc(nr);
-  {
-    // idx = 0..nr-1
-    std::vector<int> h(nr);
-    for (long long i = 0; i < nr; ++i) h[i] = (int)i;
-    MADAM_CUDA(cudaMemcpyAsync(idx.get(), h.data(), nr * sizeof(int), cudaMemcpyHostToDevice, st_));
-    MADAM_CUDA(cudaStreamSynchronize(st_));
-  }
+  MADAM_LAUNCH(k_iota, grid_for(nr), 256, 0, st_, idx.get(), nr);
   int endbit = 1;
   while ((1L << endbit) <= ntiles_) ++endbit;
   tmpb = 0;
@@ -646,6 +673,7 @@ void Engine::build_runs() {
   tmp.alloc(std::max<size_t>(tmpb, tmp.n));
   MADAM_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tmpb, keys.get(), keys_sorted.get(),
                                              idx.get(), idx_sorted.get(), (int)nr, 0, endbit, st_));
+  trace("runs: iota+sort");
   runs_.alloc(nr);
   lens_sorted.alloc(nr);
   MADAM_LAUNCH(k_gather_runs, grid_for(nr), 256, 0, st_, idx_sorted.get(), runs0.get(),
@@ -710,13 +738,16 @@ void Engine::build_csr() {
   npair_chunks_ = 0;
   have_xcsr_ = false;
   build_sample_csr();
+  trace("csr: sample csr");
   if (fp32_ && nmap_ == 3) {
     // FP32-TOD form: the scatter runs over pointing pairs; the sample CSR
     // stays for the reliable updates' exact scatter (apply_A_exact)
     swap_csr();
     csr_off_.alloc((size_t)nloc_cross_ + 1);
     if (build_pairs()) {
+      trace("csr: pairs");
       build_scatter_chunks();
+      trace("csr: pair scatter chunks");
       have_xcsr_ = true;
       return;
     }
@@ -779,6 +810,7 @@ void Engine::build_sample_csr() {
   keys.reset();
   vals.reset();
   MADAM_CUDA(cudaStreamSynchronize(st_));
+  trace("csr: keys+sort");
   csr_nvalid_ = (long long)nv;
   MADAM_LAUNCH(k_fill_int, grid_for(nloc_cross_ + 1), 256, 0, st_, csr_off_.get(),
                (long long)nloc_cross_ + 1, (int)csr_nvalid_);
@@ -794,42 +826,56 @@ void Engine::build_sample_csr() {
                    csr_nvalid_, point4_.get(), sm, (float4 *)nullptr, sp2_.get(), csr_off_.get());
   }
   MADAM_CUDA(cudaStreamSynchronize(st_));
+  trace("csr: fill");
   build_scatter_chunks();
 }
 
 void Engine::build_scatter_chunks() {
   // scatter chunks: every pixel's entries cut into chunks of at most
   // kScatterChunk; pixels of several chunks combine their partial sums
-  {
-    std::vector<int> offh((size_t)nloc_cross_ + 1);
-    MADAM_CUDA(cudaMemcpy(offh.data(), csr_off_.get(), offh.size() * sizeof(int),
-                          cudaMemcpyDeviceToHost));
-    std::vector<int4> ck, multi;
-    int slot = 0;
-    for (int p = 0; p < (int)nloc_cross_; ++p) {
-      const int e0 = offh[p], n = offh[p + 1] - offh[p];
-      const int nc = std::max(1, (n + kScatterChunk - 1) / kScatterChunk);
-      if (nc == 1) {
-        ck.push_back(make_int4(p, e0, n, -1));
-        continue;
-      }
-      multi.push_back(make_int4(p, slot, nc, 0));
-      for (int c = 0; c < nc; ++c)
-        ck.push_back(make_int4(p, e0 + c * kScatterChunk, std::min(kScatterChunk, n - c * kScatterChunk),
-                               slot++));
-    }
-    nscatter_chunks_ = (long long)ck.size();
-    nscatter_multi_ = (int)multi.size();
-    scatter_chunks_.alloc(std::max<size_t>(1, ck.size()));
-    scatter_multi_.alloc(std::max<size_t>(1, multi.size()));
-    scatter_partial_.alloc((size_t)std::max(1, slot) * nmap_);
-    if (!ck.empty())
-      MADAM_CUDA(cudaMemcpyAsync(scatter_chunks_.get(), ck.data(), ck.size() * sizeof(int4),
-                                 cudaMemcpyHostToDevice, st_));
-    if (!multi.empty())
-      MADAM_CUDA(cudaMemcpyAsync(scatter_multi_.get(), multi.data(), multi.size() * sizeof(int4),
-                                 cudaMemcpyHostToDevice, st_));
+  // (built on the device: counts, three prefix sums, then the fill)
+  const int np = (int)nloc_cross_;
+  nscatter_chunks_ = 0;
+  nscatter_multi_ = 0;
+  if (np <= 0) {
+    scatter_chunks_.alloc(1);
+    scatter_multi_.alloc(1);
+    scatter_partial_.alloc((size_t)nmap_);
+    return;
   }
+  DevBuf<int> cnt, off;
+  cnt.alloc((size_t)3 * np);
+  off.alloc((size_t)3 * (np + 1));
+  int *nck = cnt.get(), *nslot = nck + np, *nmulti = nslot + np;
+  int *ock = off.get(), *oslot = ock + (np + 1), *omulti = oslot + (np + 1);
+  MADAM_LAUNCH(k_scatter_chunk_count, grid_for(np), 256, 0, st_, csr_off_.get(), np,
+               kScatterChunk, nck, nslot, nmulti);
+  size_t tmpb = 0;
+  MADAM_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmpb, nck, ock, np, st_));
+  DevBuf<uint8_t> tmp;
+  tmp.alloc(tmpb);
+  // each total is the last prefix plus the last count
+  for (int q = 0; q < 3; ++q)
+    MADAM_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tmpb, cnt.get() + (size_t)q * np,
+                                             off.get() + (size_t)q * (np + 1), np, st_));
+  int last[6];
+  for (int q = 0; q < 3; ++q) {
+    MADAM_CUDA(cudaMemcpyAsync(&last[2 * q], off.get() + (size_t)q * (np + 1) + (np - 1),
+                               sizeof(int), cudaMemcpyDeviceToHost, st_));
+    MADAM_CUDA(cudaMemcpyAsync(&last[2 * q + 1], cnt.get() + (size_t)q * np + (np - 1),
+                               sizeof(int), cudaMemcpyDeviceToHost, st_));
+  }
+  MADAM_CUDA(cudaStreamSynchronize(st_));
+  const long long nck_tot = (long long)last[0] + last[1];
+  const int nslot_tot = last[2] + last[3];
+  const int nmulti_tot = last[4] + last[5];
+  nscatter_chunks_ = nck_tot;
+  nscatter_multi_ = nmulti_tot;
+  scatter_chunks_.alloc(std::max<long long>(1, nck_tot));
+  scatter_multi_.alloc(std::max(1, nmulti_tot));
+  scatter_partial_.alloc((size_t)std::max(1, nslot_tot) * nmap_);
+  MADAM_LAUNCH(k_scatter_chunk_fill, grid_for(np), 256, 0, st_, csr_off_.get(), np,
+               kScatterChunk, ock, oslot, omulti, scatter_chunks_.get(), scatter_multi_.get());
   MADAM_CUDA(cudaStreamSynchronize(st_));
 }
 
@@ -884,6 +930,7 @@ bool Engine::build_pairs() {
       b = e;
     }
   }
+  trace("pairs: heads+offsets+chunks");
   npairs_ = np;
   gp4_.alloc(std::max(1, np));
   DevBuf<int> pbase;
@@ -897,6 +944,7 @@ bool Engine::build_pairs() {
   if (!ck.empty())
     MADAM_CUDA(cudaMemcpyAsync(pair_chunks_.get(), ck.data(), ck.size() * sizeof(int4),
                                cudaMemcpyHostToDevice, st_));
+  trace("pairs: fill");
   // pixel-sorted pairs (stable radix sort: time order inside a pixel)
   csr_nvalid_ = np;
   MADAM_LAUNCH(k_fill_int, grid_for(nloc_cross_ + 1), 256, 0, st_, csr_off_.get(),
@@ -1183,10 +1231,15 @@ void Engine::build_segments() {
 
 void Engine::build_filter() {
   // init_filter (noise_routines.f90:242-292) + build_filter (367-739).  The
-  // spectra are computed on the host (OpenMP over the PSDs) by a background
-  // job that overlaps the device-side setup; build_filter_finish() waits for
-  // it and uploads the result.
+  // plateau of each PSD is found on the host; the spectra are computed on
+  // the device (k_filter_spectra) and checked in build_filter_finish().  A
+  // PSD table the device form does not cover (frequencies not ascending past
+  // the first nonzero one, fewer than two of them) or a spectrum that is not
+  // positive somewhere (which the reference fills from its neighbours) takes
+  // the host's computation (filter_spectra, OpenMP over the PSDs) instead.
   filter_err_.clear();
+  fcov_host_valid_ = false;
+  filter_dev_ = false;
   if (!par_.kfilter) return;
   long nof_min = 2 * noba_pp_max_;
   if (par_.precond_width_max > nof_min - 1) nof_min = par_.precond_width_max + 1;
@@ -1196,7 +1249,6 @@ void Engine::build_filter() {
   npsdtot_ = 0;
   for (auto &d : dets_) npsdtot_ += d.npsd;
   const long nh = nof_ / 2 + 1;
-  fcov_host_.assign((size_t)nh * npsdtot_, 0.0);
   psddet_.assign(npsdtot_, 0);
   psdstart_.assign(npsdtot_, 0.0);
   psdstop_.assign(npsdtot_, 0.0);
@@ -1212,13 +1264,113 @@ void Engine::build_filter() {
     psdstart_[it] = dets_[d].psdstarts[ip];
     psdstop_[it] = (ip < dets_[d].npsd - 1) ? dets_[d].psdstarts[ip + 1] : fsp(1e30f);
   }
-  filter_job_ = std::async(std::launch::async, [this, tasks, nh]() { filter_spectra(tasks, nh); });
+  filter_tasks_ = tasks;
+  // the device form: plateaus and tables on the host, spectra on the device
+  const double fa = par_.fsample / (double)nshort_;
+  const double margin = par_.radiometers ? fsp(1e-6f) : fsp(1e-3f);
+  std::vector<FiltTask> ft(tasks.size());
+  std::vector<double> tfr, tps, tlf, tlp;
+  bool dev_ok = true;
+  filter_sigma0_.assign(tasks.size(), 0.0);
+  try {
+    for (size_t it = 0; it < tasks.size() && dev_ok; ++it) {
+      const long d = tasks[it].first;
+      const int ip = tasks[it].second;
+      const Detector &det = dets_[d];
+      const std::vector<double> &fq = det.psdfreqs, &pv = det.psds[ip];
+      const long nin = (long)fq.size();
+      if ((long)pv.size() != nin) fail("freq and psd do not have the same shape");
+      long first = 0;
+      while (first < nin && fq[first] == 0) ++first;
+      if (first == nin) fail("input freqs are all zero.");
+      if (nin - first < 2) dev_ok = false;
+      for (long i = first + 1; i < nin && dev_ok; ++i)
+        if (!(fq[i] >= fq[i - 1])) dev_ok = false;
+      if (!dev_ok) break;
+      double plateau;
+      if (par_.noise_weights_from_psd) {
+        plateau = det.plateaus[ip];
+      } else if (par_.radiometers) {
+        const double ff = par_.fsample / 2;
+        interpolate_psd(fq, pv, &ff, &plateau, 1);
+      } else {
+        std::vector<double> fr(1000), dt(1000);
+        for (int i = 0; i < 1000; ++i) fr[i] = 1 + (double)(i * 10) / 1000;
+        interpolate_psd(fq, pv, fr.data(), dt.data(), 1000);
+        plateau = *std::min_element(dt.begin(), dt.end());
+      }
+      ft[it] = FiltTask{(int)tfr.size(), (int)nin, (int)first, plateau, det.sigmas[ip]};
+      for (long i = 0; i < nin; ++i) {
+        tfr.push_back(fq[i]);
+        tps.push_back(pv[i]);
+        tlf.push_back(std::log(fq[i]));
+        tlp.push_back(std::log(pv[i]));
+      }
+    }
+  } catch (const std::exception &e) {
+    filter_err_ = e.what();  // raised where the host's spectra raise it
+    return;
+  }
+  if (!dev_ok || tasks.empty()) {
+    filter_job_ =
+        std::async(std::launch::async, [this, tasks, nh]() { filter_spectra(tasks, nh); });
+    return;
+  }
+  for (size_t it = 0; it < tasks.size(); ++it) {
+    Detector &det = dets_[tasks[it].first];
+    filter_sigma0_[it] = det.sigmas[tasks[it].second];
+    if (!par_.noise_weights_from_psd)
+      det.sigmas[tasks[it].second] = std::sqrt(ft[it].plateau * par_.fsample);
+  }
+  filter_dev_ = true;
+  DevBuf<FiltTask> dft;
+  DevBuf<double> tab;
+  const size_t nt = tfr.size();
+  dft.alloc(ft.size());
+  tab.alloc(4 * nt);
+  MADAM_CUDA(cudaMemcpyAsync(dft.get(), ft.data(), ft.size() * sizeof(FiltTask),
+                             cudaMemcpyHostToDevice, st_));
+  const std::vector<double> *parts[4] = {&tfr, &tps, &tlf, &tlp};
+  for (int q = 0; q < 4; ++q)
+    MADAM_CUDA(cudaMemcpyAsync(tab.get() + q * nt, parts[q]->data(), nt * sizeof(double),
+                               cudaMemcpyHostToDevice, st_));
+  fcov_.alloc((size_t)nh * npsdtot_);
+  filter_flag_.alloc(1);
+  filter_flag_.zero(st_);
+  const unsigned gx = (unsigned)std::min<long>((nh + 255) / 256, 4096);
+  MADAM_LAUNCH(k_filter_spectra, dim3(gx, (unsigned)tasks.size()), 256, 0, st_, dft.get(),
+               tab.get(), tab.get() + nt, tab.get() + 2 * nt, tab.get() + 3 * nt, nof_, nh, fa,
+               margin, fcov_.get(), filter_flag_.get());
+}
+
+// The host copy of the filter's spectra (the covariance output and the
+// "fcov" result read it).
+const std::vector<double> &Engine::fcov_host() {
+  if (!fcov_host_valid_ && filter_dev_ && fcov_.n) {
+    fcov_host_.resize(fcov_.n);
+    MADAM_CUDA(cudaMemcpyAsync(fcov_host_.data(), fcov_.get(), fcov_.n * sizeof(double),
+                               cudaMemcpyDeviceToHost, st_));
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+  }
+  fcov_host_valid_ = true;
+  return fcov_host_;
+}
+
+const std::vector<double> &Engine::invcov_host() {
+  if (invcov_valid_ && invcov_host_.empty() && invcov_.n) {
+    invcov_host_.resize((size_t)nof_ * npsdtot_);
+    MADAM_CUDA(cudaMemcpyAsync(invcov_host_.data(), invcov_.get(),
+                               invcov_host_.size() * sizeof(double), cudaMemcpyDeviceToHost, st_));
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+  }
+  return invcov_host_;
 }
 
 void Engine::filter_spectra(const std::vector<std::pair<long, int>> &tasks, long nh) {
   const double fa = par_.fsample / (double)nshort_;
   const double kPi = 3.141592653589793238462643383279502884197;
   std::string err;
+  fcov_host_.assign((size_t)nh * npsdtot_, 0.0);
 #pragma omp parallel for schedule(dynamic, 1)
   for (long it = 0; it < (long)tasks.size(); ++it) {
     try {
@@ -1292,17 +1444,39 @@ void Engine::filter_spectra(const std::vector<std::pair<long, int>> &tasks, long
 
 void Engine::build_filter_finish() {
   if (!par_.kfilter) return;
-  if (filter_job_.valid()) filter_job_.get();
+  if (filter_dev_) {
+    int flag = 0;
+    MADAM_CUDA(cudaMemcpyAsync(&flag, filter_flag_.get(), sizeof flag, cudaMemcpyDeviceToHost,
+                               st_));
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    if (flag & 1) {
+      // a spectrum that is not positive somewhere: the host's computation
+      // with the reference's fill (from the sigmas the filter started from)
+      for (size_t it = 0; it < filter_tasks_.size(); ++it)
+        dets_[filter_tasks_[it].first].sigmas[filter_tasks_[it].second] = filter_sigma0_[it];
+      filter_dev_ = false;
+      filter_spectra(filter_tasks_, nof_ / 2 + 1);
+    } else if (flag & 2) {
+      fail("NaN in fcov. Check input PSD and sigma.");
+    }
+  } else if (filter_job_.valid()) {
+    filter_job_.get();
+  }
   if (!filter_err_.empty()) fail(filter_err_);
-  fcov_.alloc(fcov_host_.size());
-  MADAM_CUDA(cudaMemcpyAsync(fcov_.get(), fcov_host_.data(), fcov_host_.size() * sizeof(double),
-                             cudaMemcpyHostToDevice, st_));
+  if (!filter_dev_) {
+    fcov_.alloc(fcov_host_.size());
+    MADAM_CUDA(cudaMemcpyAsync(fcov_.get(), fcov_host_.data(),
+                               fcov_host_.size() * sizeof(double), cudaMemcpyHostToDevice, st_));
+    fcov_host_valid_ = true;
+  }
   fft_.reset(new FFTPlan(nof_));
   MADAM_CUDA(cudaStreamSynchronize(st_));
 }
 
 void Engine::construct_preconditioner() {
   // construct_preconditioner (noise_routines.f90:920-1153)
+  invcov_valid_ = false;
+  invcov_host_.clear();
   band_segs_.clear();
   cg_prec_segs_.clear();
   band_widths_.clear();
@@ -1333,16 +1507,18 @@ void Engine::construct_preconditioner() {
   }
   const long nh = nof_ / 2 + 1;
   {
-    std::vector<double> fp((size_t)nh * npsdtot_);
+    std::vector<double> w(npsdtot_);
     long ip = 0;
     for (long d = 0; d < ndet_; ++d)
-      for (int k = 0; k < dets_[d].npsd; ++k, ++ip)
-        for (long i = 0; i < nh; ++i)
-          fp[(size_t)ip * nh + i] =
-              1.0 / ((double)nshort_ * dets_[d].weights[k] + fcov_host_[(size_t)ip * nh + i]);
-    fprec_.alloc(fp.size());
-    MADAM_CUDA(cudaMemcpyAsync(fprec_.get(), fp.data(), fp.size() * sizeof(double),
+      for (int k = 0; k < dets_[d].npsd; ++k, ++ip) w[ip] = dets_[d].weights[k];
+    DevBuf<double> wd;
+    wd.alloc(std::max<long>(1, npsdtot_));
+    MADAM_CUDA(cudaMemcpyAsync(wd.get(), w.data(), npsdtot_ * sizeof(double),
                                cudaMemcpyHostToDevice, st_));
+    fprec_.alloc((size_t)nh * npsdtot_);
+    MADAM_LAUNCH(k_fprec, grid_for((long long)nh * npsdtot_), 256, 0, st_, fcov_.get(), wd.get(),
+                 nh, (long)npsdtot_, (double)nshort_, fprec_.get());
+    MADAM_CUDA(cudaStreamSynchronize(st_));
   }
   if (par_.use_fprecond) {
     MADAM_CUDA(cudaStreamSynchronize(st_));
@@ -1363,10 +1539,23 @@ void Engine::construct_preconditioner() {
     ic[ip].flags = 0;
   }
   convolve(delta_.get(), invcov_.get(), ic, fcov_.get(), tmp_segs_d_);
-  invcov_host_.resize((size_t)nof_ * npsdtot_);
-  MADAM_CUDA(cudaMemcpyAsync(invcov_host_.data(), invcov_.get(),
-                             invcov_host_.size() * sizeof(double), cudaMemcpyDeviceToHost, st_));
-  MADAM_CUDA(cudaStreamSynchronize(st_));
+  invcov_host_.clear();  // copied to the host only when asked for (result "invcov")
+  invcov_valid_ = true;
+  // the kernels' power sums, in the host's order of summation
+  const long pw_w = std::max<long>(1, std::min<long>(nof_, par_.precond_width_max));
+  std::vector<double> ptot(npsdtot_), ppre((size_t)npsdtot_ * pw_w);
+  {
+    DevBuf<double> dpt, dpre;
+    dpt.alloc(std::max<long>(1, npsdtot_));
+    dpre.alloc(std::max<size_t>(1, ppre.size()));
+    MADAM_LAUNCH(k_invcov_power, (unsigned)((npsdtot_ + 63) / 64), 64, 0, st_, invcov_.get(),
+                 nof_, (long)npsdtot_, pw_w, dpt.get(), dpre.get());
+    MADAM_CUDA(cudaMemcpyAsync(ptot.data(), dpt.get(), npsdtot_ * sizeof(double),
+                               cudaMemcpyDeviceToHost, st_));
+    MADAM_CUDA(cudaMemcpyAsync(ppre.data(), dpre.get(), ppre.size() * sizeof(double),
+                               cudaMemcpyDeviceToHost, st_));
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+  }
   // candidate segments
   std::vector<int> cand;
   for (int i = 0; i < (int)segs_.size(); ++i) {
@@ -1383,16 +1572,14 @@ void Engine::construct_preconditioner() {
   std::vector<Try> todo;
   for (int i : cand) {
     const Segment &s = segs_[i];
-    const double *icv = invcov_host_.data() + (size_t)s.psd_prec * nof_;
-    double p_tot = 0;
-    for (long k = 0; k < nof_ / 2; ++k) p_tot += icv[k] * icv[k];
+    const double p_tot = ptot[s.psd_prec];
+    const double *pre = ppre.data() + (size_t)s.psd_prec * pw_w;
     long tr = 1, nband = 0;
     bool ok = false;
     for (;;) {
       nband = std::min(s.noba, tr * par_.precond_width_min);
       nband = std::min(nband, par_.precond_width_max);
-      double pp = 0;
-      for (long k = 0; k < nband; ++k) pp += icv[k] * icv[k];
+      const double pp = nband > 0 ? pre[nband - 1] : 0.0;
       if (pp > plim * p_tot) { ok = true; break; }
       if (nband == s.noba || nband == par_.precond_width_max) break;
       if (tr == 1000) break;
@@ -2724,7 +2911,11 @@ void Engine::run_setup(const Params &par, std::vector<Detector> dets, long ndet,
     MADAM_CUDA(cudaStreamSynchronize(st_));
     setup_marks_[i] = now_ms() - t0;
   };
+  trace_on_ = std::getenv("MADAM_B200_TRACE") != nullptr;
+  trace_t_ = t0;
+  if (trace_on_ && trace_ev_[0]) MADAM_CUDA(cudaEventRecord(trace_ev_[0], st_));
   bind_inputs(timestamps, pix, pixweights, signal, is_device, true);
+  trace("bind_inputs");
   struct TodGuard {
     Engine &e;
     ~TodGuard() { e.sync_tod(); }
@@ -2749,7 +2940,9 @@ void Engine::run_setup(const Params &par, std::vector<Detector> dets, long ndet,
     if (ar_sum_host(err.empty() ? 0.0 : 1.0) > 0)
       fail(err.empty() ? "another rank failed its input checks" : err);
   }
+  trace("pixel_check");
   init_layout(nperiod, periods);
+  trace("init_layout");
   // baseline start times (baseline_times, parameter_control.f90:956-977)
   btime_.assign(noba_short_, 0.0);
   if (is_device) {
@@ -2772,26 +2965,37 @@ void Engine::run_setup(const Params &par, std::vector<Detector> dets, long ndet,
       if (f.valid()) f.wait();
     }
   } filter_guard{filter_job_};
+  trace("baseline_times");
   build_filter();
   mark(2);
+  trace("build_filter");
   flag_and_compact(true);
   mark(3);
+  trace("flag_and_compact");
   build_runs();
   mark(4);
+  trace("build_runs");
   setup_scatter();
   mark(5);
+  trace("setup_scatter");
   if (par_.kfirst) build_csr();
   mark(6);
+  trace("build_csr");
   if (par_.kfirst) {
     map_side_setup();
+    trace("map_side_setup");
     initialize_a();
+    trace("initialize_a");
     check_nan_setup();
     mark(7);
     build_segments();
+    trace("build_segments");
     build_filter_finish();
     mark(8);
+    trace("build_filter_finish");
     construct_preconditioner();
     mark(9);
+    trace("construct_preconditioner");
   }
   MADAM_CUDA(cudaStreamSynchronize(st_));
   timings.setup_ms = now_ms() - t0;
@@ -2904,8 +3108,8 @@ long Engine::result_size(const std::string &name) {
   if (name == "cca") return npc * nmap_ * nmap_;
   if (name == "aa" || name == "yba") return nb * nbasis_;
   if (name == "nna") return nb * nbasis_ * nbasis_;
-  if (name == "fcov") return (long)fcov_host_.size();
-  if (name == "invcov") return (long)invcov_host_.size();
+  if (name == "fcov") return (long)fcov_host().size();
+  if (name == "invcov") return (long)invcov_host().size();
   if (name == "rr_history") return (long)rr_history.size();
   if (name == "band_widths") return (long)band_widths_.size();
   if (name == "scalars") return 24;
@@ -3035,10 +3239,10 @@ void Engine::result_copy(const std::string &name, void *dst, long nbytes) {
     if (sz) MADAM_CUDA(cudaMemcpy(dst, src, sz * sizeof(double), cudaMemcpyDeviceToHost));
   } else if (name == "fcov") {
     need(sizeof(double));
-    std::memcpy(dst, fcov_host_.data(), sz * sizeof(double));
+    std::memcpy(dst, fcov_host().data(), sz * sizeof(double));
   } else if (name == "invcov") {
     need(sizeof(double));
-    std::memcpy(dst, invcov_host_.data(), sz * sizeof(double));
+    std::memcpy(dst, invcov_host().data(), sz * sizeof(double));
   } else if (name == "rr_history") {
     need(sizeof(double));
     std::memcpy(dst, rr_history.data(), sz * sizeof(double));

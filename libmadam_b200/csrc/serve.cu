@@ -73,6 +73,7 @@ struct Job {
   double t_submit = 0, t_start = 0, t_end = 0;
   std::map<std::string, std::vector<char>> results;
   double noiter = 0;
+  double setup_ms = 0, iterate_ms = 0, finalize_ms = 0;  // the engine's phases
 };
 
 // device memory of a job, from the engine's buffers per sample / baseline
@@ -199,6 +200,7 @@ class Server {
       std::string err;
       std::map<std::string, std::vector<char>> res;
       double noiter = 0;
+      Timings tm;
       try {
         if (!eng) eng.reset(new Engine());
         eng->set_fp32(j->fp32);
@@ -235,6 +237,11 @@ class Server {
           res[nm] = std::move(buf);
         }
         noiter = (double)eng->noiter;
+        tm = eng->timings;
+        // an engine keeps its buffers for the worker's next job; one sized
+        // for a large job gives them back, since the budget counts only the
+        // running jobs
+        if (j->bytes > budget_ / 8) eng.reset();
       } catch (const std::exception &e) {
         st = 3;
         err = e.what();
@@ -244,6 +251,9 @@ class Server {
         std::lock_guard<std::mutex> lk(mu_);
         j->results = std::move(res);
         j->noiter = noiter;
+        j->setup_ms = tm.setup_ms;
+        j->iterate_ms = tm.iterate_ms;
+        j->finalize_ms = tm.finalize_ms;
         j->error = err;
         j->t_end = wall_s();
         j->state = st;
@@ -565,6 +575,11 @@ int madam_b200_serve_job_info(void *srv, long job, double *out, long nout) {
   out[3] = (double)j->ndet * j->nsamp;
   out[4] = j->noiter;
   out[5] = (double)j->bytes;
+  if (nout >= 9) {
+    out[6] = j->setup_ms;
+    out[7] = j->iterate_ms;
+    out[8] = j->finalize_ms;
+  }
   return 0;
 }
 

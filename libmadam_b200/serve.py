@@ -138,12 +138,14 @@ class Server:
         return out
 
     def info(self, ticket):
-        """submit / start / end times (s), samples, PCG iterations, admitted bytes."""
-        out = np.zeros(6)
+        """submit / start / end times (s), samples, PCG iterations, admitted
+        bytes, and the setup / PCG / finalisation wall times (ms)."""
+        out = np.zeros(9)
         if self._L.madam_b200_serve_job_info(self._h, ticket.job,
-                                             out.ctypes.data_as(ct.c_void_p), 6):
+                                             out.ctypes.data_as(ct.c_void_p), 9):
             raise RuntimeError("job {} is not finished".format(ticket.job))
-        keys = ("t_submit", "t_start", "t_end", "samples", "iterations", "bytes")
+        keys = ("t_submit", "t_start", "t_end", "samples", "iterations", "bytes", "setup_ms",
+                "iterate_ms", "finalize_ms")
         return dict(zip(keys, out.tolist()))
 
     def stats(self):

@@ -227,17 +227,24 @@ def test_pixel_matrix_modes(W, pars):
 
 def test_good_baseline_fraction(W):
     # flag_bad_baselines (read_data.f90:30-74): without the filter, a baseline
-    # with fewer good samples than the fraction loses all of them
+    # with fewer good (unflagged) samples than the fraction loses all of
+    # them.  The reference compares the reduced pixel numbers with
+    # 12 nside_max^2 (smadam.F90:293), so the rule acts only when every
+    # submap is hit: the pointing here is uniform over the sky, a third of
+    # the samples flagged (pixel -1)
     d = syn.to_numpy(syn.generate(syn.small_config(seed=28)))
     rng = np.random.default_rng(8)
     n = d["pixels"].size
-    d["pixweights"].reshape(-1, 3)[rng.choice(n, n // 3, replace=False)] = 0.0
+    npix0 = 12 * d["pars"]["nside_map"] ** 2
+    d["pixels"] = rng.integers(0, npix0, d["pixels"].shape).astype(d["pixels"].dtype)
+    d["pixels"].reshape(-1)[rng.choice(n, n // 3, replace=False)] = -1
     ro, rp, do, dp = run_both(W, d, dict(kfilter=False, good_baseline_fraction=0.7))
     compare(ro, rp, 3)
-    # some samples were flagged by the rule beyond the zero-weight ones (the
-    # rule's come back past the dummy pixel, read_data.f90:51 and
-    # pointing.f90:178-186)
-    assert (dp["pixels"] >= 12 * d["pars"]["nside_map"] ** 2).sum() > n // 3
+    # the rule flags samples (they come back past the dummy pixel,
+    # read_data.f90:51 and pointing.f90:178-186) that a run without it keeps
+    npix = 12 * d["pars"]["nside_map"] ** 2
+    _, _, _, dp0 = run_both(W, d, dict(kfilter=False, good_baseline_fraction=0.0))
+    assert (dp["pixels"] >= npix).sum() > (dp0["pixels"] >= npix).sum()
 
 
 @pytest.mark.parametrize("radiometers", [True, False])
