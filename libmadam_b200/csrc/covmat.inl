@@ -258,7 +258,9 @@ void Engine::write_covmat() {
       MADAM_CUDA(cudaMemcpyAsync(dcs.get(), cs.data(), nseg * sizeof(ConvSeg),
                                  cudaMemcpyHostToDevice, st_));
       fft_->reserve(nseg);
-      fft_->convolve(st_, dcs.get(), nseg, dspec.get(), dimp.get(), dmm.get());
+      fft_->convolve(st_, dcs.get(), nseg, dspec.get(), (long)(spec.size() / nh), dimp.get(),
+                     dmm.get());
+      fft_->forget_spectra();  // dspec is a temporary
       // the non-zeros of P^T F: sorted (pixel, baseline) keys, run-length
       // encoded
       DevBuf<int> dseg_of, dk0, dn;

@@ -127,7 +127,7 @@ void Engine::apply_preconditioner_batch(const double *r, double *z) {
   MADAM_CUDA(cudaMemcpyAsync(z, r, nt * sizeof(double), cudaMemcpyDeviceToDevice, st_));
   const long nfs = (long)filt_segs_.size() * nrhs_;
   if (par_.use_fprecond) {
-    if (nfs > 0) fft_->convolve(st_, filt_segs_b_d_.get(), nfs, fprec_.get(), r, z);
+    if (nfs > 0) fft_->convolve(st_, filt_segs_b_d_.get(), nfs, fprec_.get(), npsdtot_, r, z);
     return;
   }
   if (band2_guarded_) {
@@ -235,7 +235,8 @@ void Engine::apply_A_batch() {
     MADAM_CUDA(cudaMemcpyAsync(apb_.get(), pb_.get(), nt * sizeof(double),
                                cudaMemcpyDeviceToDevice, st_));
     const long nfs = (long)filt_segs_.size() * nrhs_;
-    if (nfs > 0) fft_->convolve(st_, filt_segs_b_d_.get(), nfs, fcov_.get(), pb_.get(), apb_.get());
+    if (nfs > 0) fft_->convolve(st_, filt_segs_b_d_.get(), nfs, fcov_.get(), npsdtot_, pb_.get(),
+                                apb_.get());
   } else if (par_.diagfilter != 0) {
     for (long k = 0; k < nrhs_; ++k)
       MADAM_LAUNCH(k_diagfilter, grid_for(nb), 256, 0, st_, apb_.get() + k * nb, nna_.get(),

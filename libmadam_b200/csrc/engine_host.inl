@@ -13,13 +13,26 @@ struct CgpWork {
 
 thread_local cudaStream_t g_alloc_stream = nullptr;
 
+// allocations and frees that take longer than a millisecond of host time
+// are reported with MADAM_B200_TRACE set
+static const bool g_trace_alloc = std::getenv("MADAM_B200_TRACE") != nullptr;
+
 void *dev_alloc(size_t bytes) {
   void *p = nullptr;
+  const double t0 = g_trace_alloc ? now_ms() : 0;
   MADAM_CUDA(cudaMallocAsync(&p, bytes, g_alloc_stream));
+  if (g_trace_alloc && now_ms() - t0 > 1.0)
+    std::fprintf(stderr, "madam_b200 trace: slow alloc of %.3f GB: %.3f ms\n", bytes / 1e9,
+                 now_ms() - t0);
   return p;
 }
 
-void dev_free(void *p) { cudaFreeAsync(p, g_alloc_stream); }
+void dev_free(void *p) {
+  const double t0 = g_trace_alloc ? now_ms() : 0;
+  cudaFreeAsync(p, g_alloc_stream);
+  if (g_trace_alloc && now_ms() - t0 > 1.0)
+    std::fprintf(stderr, "madam_b200 trace: slow free: %.3f ms\n", now_ms() - t0);
+}
 
 Engine::Engine() {
   MADAM_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
@@ -1240,6 +1253,7 @@ void Engine::build_filter() {
   filter_err_.clear();
   fcov_host_valid_ = false;
   filter_dev_ = false;
+  if (fft_) fft_->forget_spectra();  // fcov is rewritten
   if (!par_.kfilter) return;
   long nof_min = 2 * noba_pp_max_;
   if (par_.precond_width_max > nof_min - 1) nof_min = par_.precond_width_max + 1;
@@ -1515,6 +1529,7 @@ void Engine::construct_preconditioner() {
     wd.alloc(std::max<long>(1, npsdtot_));
     MADAM_CUDA(cudaMemcpyAsync(wd.get(), w.data(), npsdtot_ * sizeof(double),
                                cudaMemcpyHostToDevice, st_));
+    if (fft_) fft_->forget_spectra();  // fprec is rewritten
     fprec_.alloc((size_t)nh * npsdtot_);
     MADAM_LAUNCH(k_fprec, grid_for((long long)nh * npsdtot_), 256, 0, st_, fcov_.get(), wd.get(),
                  nh, (long)npsdtot_, (double)nshort_, fprec_.get());
@@ -1960,7 +1975,7 @@ void Engine::convolve(const double *x, double *y, const std::vector<ConvSeg> &se
   if (dsegs.n < segs.size()) dsegs.alloc(segs.size());
   MADAM_CUDA(cudaMemcpyAsync(dsegs.get(), segs.data(), segs.size() * sizeof(ConvSeg),
                              cudaMemcpyHostToDevice, st_));
-  fft_->convolve(st_, dsegs.get(), (long)segs.size(), spectra, x, y);
+  fft_->convolve(st_, dsegs.get(), (long)segs.size(), spectra, npsdtot_, x, y);
 }
 
 void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) {
@@ -2004,7 +2019,8 @@ void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) 
   if (par_.kfilter) {
     MADAM_CUDA(cudaMemcpyAsync(ap, p, nb * sizeof(double), cudaMemcpyDeviceToDevice, st_));
     if (!filt_segs_.empty())
-      fft_->convolve(st_, filt_segs_d_.get(), (long)filt_segs_.size(), fcov_.get(), p, ap);
+      fft_->convolve(st_, filt_segs_d_.get(), (long)filt_segs_.size(), fcov_.get(), npsdtot_, p,
+                     ap);
   } else if (par_.diagfilter != 0) {
     MADAM_LAUNCH(k_diagfilter, grid_for(nb), 256, 0, st_, ap, nna_.get(), p, par_.diagfilter, nb);
   } else {
@@ -2115,7 +2131,8 @@ void Engine::apply_A_exact(const double *x, double *ax) {
   if (par_.kfilter) {
     MADAM_CUDA(cudaMemcpyAsync(ax, x, nb * sizeof(double), cudaMemcpyDeviceToDevice, st_));
     if (!filt_segs_.empty())
-      fft_->convolve(st_, filt_segs_d_.get(), (long)filt_segs_.size(), fcov_.get(), x, ax);
+      fft_->convolve(st_, filt_segs_d_.get(), (long)filt_segs_.size(), fcov_.get(), npsdtot_, x,
+                     ax);
   } else if (par_.diagfilter != 0) {
     MADAM_LAUNCH(k_diagfilter, grid_for(nb), 256, 0, st_, ax, nna_.get(), x, par_.diagfilter, nb);
   } else {
@@ -2401,7 +2418,8 @@ void Engine::cg_preconditioner_segments(const double *r, double *z) {
                w.prop.get(), w.zres.get(), w.prec.get(), nna_.get(), invcov_.get(),
                (long long)nof_, w.st.get(), w.done.get());
   for (int iter = 1; iter <= 100; ++iter) {
-    fft_->convolve(st_, w.csegs.get(), w.nseg, fcov_.get(), w.prop.get(), w.aprop.get());
+    fft_->convolve(st_, w.csegs.get(), w.nseg, fcov_.get(), npsdtot_, w.prop.get(),
+                   w.aprop.get());
     MADAM_CUDA(cudaMemsetAsync(w.active.get(), 0, sizeof(int), st_));
     MADAM_LAUNCH(k_cgp_step, ns, 256, 0, st_, w.segs.get(), w.x.get(), w.resid.get(),
                  w.prop.get(), w.aprop.get(), w.zres.get(), w.prec.get(), nna_.get(), w.st.get(),
@@ -2429,7 +2447,8 @@ void Engine::apply_preconditioner(const double *r, double *z) {
   MADAM_CUDA(cudaMemcpyAsync(z, r, nb * sizeof(double), cudaMemcpyDeviceToDevice, st_));
   if (par_.use_fprecond) {
     if (!filt_segs_.empty())
-      fft_->convolve(st_, filt_segs_d_.get(), (long)filt_segs_.size(), fprec_.get(), r, z);
+      fft_->convolve(st_, filt_segs_d_.get(), (long)filt_segs_.size(), fprec_.get(), npsdtot_, r,
+                     z);
     return;
   }
   if (band2_guarded_) {

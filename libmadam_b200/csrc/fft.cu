@@ -164,18 +164,18 @@ __device__ void fft_dif(cplx *s, int L, int nfft, const cplx *tw, bool inverse) 
 
 // Real-spectrum split of the packed transform for the pair (k, N-k), product
 // with the real spectrum H and re-packing for the inverse transform.
-// A = Z[k], B = Z[N-k]; on return A = Z'[k], B = Z'[N-k].  k == 0 handles
-// the DC / Nyquist pair (B is ignored and set equal to A).
-__device__ __forceinline__ void spectral_pair(cplx &A, cplx &B, long long k, long long N,
-                                              const double *H, const cplx *T2) {
-  if (k == 0) {
+// A = Z[k], B = Z[N-k], W = exp(-i pi k / N), Hk = H[k], Hnk = H[N-k]; on
+// return A = Z'[k], B = Z'[N-k].  dc (k == 0) handles the DC / Nyquist pair
+// with Hk = H[0], Hnk = H[N] (B is ignored and set equal to A).
+__device__ __forceinline__ void spectral_pair(cplx &A, cplx &B, bool dc, cplx W, double Hk,
+                                              double Hnk) {
+  if (dc) {
     const double x0 = A.x + A.y, xn = A.x - A.y;
-    const double y0 = x0 * H[0], yn = xn * H[N];
+    const double y0 = x0 * Hk, yn = xn * Hnk;
     A = make_double2(0.5 * (y0 + yn), 0.5 * (y0 - yn));
     B = A;
     return;
   }
-  const cplx W = T2[k];  // exp(-i pi k / N)
   const cplx Bc = cconj(B);
   const cplx E = cscale(cadd(A, Bc), 0.5);
   const cplx D = csub(A, Bc);
@@ -183,8 +183,8 @@ __device__ __forceinline__ void spectral_pair(cplx &A, cplx &B, long long k, lon
   const cplx WO = cmul(W, O);
   const cplx Xk = cadd(E, WO);
   const cplx Xnk = cconj(csub(E, WO));
-  const cplx Yk = cscale(Xk, H[k]);
-  const cplx Ynk = cscale(Xnk, H[N - k]);
+  const cplx Yk = cscale(Xk, Hk);
+  const cplx Ynk = cscale(Xnk, Hnk);
   // re-pack: Z'[k] = 1/2 (Yk + conj Ynk) + i/2 (Yk - conj Ynk) conj(W^k)
   const cplx Wc = cconj(W);
   const cplx e1 = cscale(cadd(Yk, cconj(Ynk)), 0.5);
@@ -259,7 +259,7 @@ __global__ void k_conv_small(const ConvSeg *segs, const double *spectra, long lo
   for (int k = threadIdx.x; k <= N / 2; k += blockDim.x) {
     const int nk = (N - k) % N;
     cplx A = s[k], B = s[nk];
-    spectral_pair(A, B, k, N, H, T2);
+    spectral_pair(A, B, k == 0, T2[k], H[k], H[N - k]);
     s[k] = A;
     if (nk != k) s[nk] = B;
   }
@@ -295,9 +295,8 @@ __device__ __forceinline__ cplx tw_l(const cplx *twL, int q) {
   return INV ? cconj(w) : w;
 }
 
-__device__ __forceinline__ void load_twl(cplx *twL, int L, const cplx *T2, long long N) {
-  const long long step = 2 * N / L;
-  for (int q = threadIdx.x; q < L; q += blockDim.x) twL[q] = T2[q * step];
+__device__ __forceinline__ void load_twl(cplx *twL, int L, const cplx *tw) {
+  for (int q = threadIdx.x; q < L; q += blockDim.x) twL[q] = tw[q];
 }
 
 template <bool INV>
@@ -441,11 +440,13 @@ __device__ __forceinline__ void fft_block(cplx *s, int S, int L, int logL, int n
 // Pass 1: forward column FFTs (length R) of G adjacent columns, twiddled.
 __global__ void __launch_bounds__(512, 2) k_conv_cols_fwd(const ConvSeg *segs, const double *x,
                                                        const double *part, double2 *work, int R,
-                                                       int logR, int C, int G, const cplx *T2) {
+                                                       int logR, int C, int G,
+                                                       const cplx *__restrict__ twrow,
+                                                       const cplx *__restrict__ twr) {
   extern __shared__ double2 sm[];
   const int S = pad8(R) + 1;
   cplx *twL = sm + G * S;
-  load_twl(twL, R, T2, (long long)R * C);
+  load_twl(twL, R, twr);
   const int seg = blockIdx.y;
   const ConvSeg sg = segs[seg];
   const double mean = seg_mean(part, seg, sg.n_in, sg.flags & 1);
@@ -457,22 +458,28 @@ __global__ void __launch_bounds__(512, 2) k_conv_cols_fwd(const ConvSeg *segs, c
     return make_double2(seg_input(x, sg, 2 * m, mean), seg_input(x, sg, 2 * m + 1, mean));
   };
   auto store = [&](int f, int k1, cplx v) {
-    const int n2 = c0 + f;
-    W[(long long)k1 * C + n2] = cmul(v, tw_n(T2, (long long)n2 * k1, N));
+    const long long i = (long long)k1 * C + c0 + f;
+    W[i] = cmul(v, twrow[i]);
   };
   fft_block<false, true>(sm, S, R, logR, G, twL, load, store);
 }
 
 // Pass 2: forward row FFTs of rows k1 and R-k1, spectral product, inverse
-// row FFTs, inverse twiddles.
-__global__ void __launch_bounds__(1024) k_conv_rows(const ConvSeg *segs, const double *spectra,
+// row FFTs, inverse twiddles.  Hrows holds the spectra in rows of the split
+// (Hr[k1][k2] = H[k1 + R k2]); the Nyquist value H[N] comes from spectra.
+__global__ void __launch_bounds__(1024) k_conv_rows(const ConvSeg *segs,
+                                                    const double *__restrict__ Hrows,
+                                                    const double *__restrict__ spectra,
                                                     long long spec_len, double2 *work, int R,
-                                                    int C, int logC, const cplx *T2) {
+                                                    int C, int logC,
+                                                    const cplx *__restrict__ twrow,
+                                                    const cplx *__restrict__ wrow,
+                                                    const cplx *__restrict__ twc) {
   extern __shared__ double2 sm[];
   const int S = pad8(C) + 1;
   cplx *s = sm;  // 2 rows
   cplx *twL = sm + 2 * S;
-  load_twl(twL, C, T2, (long long)R * C);
+  load_twl(twL, C, twc);
   const int seg = blockIdx.y;
   const ConvSeg sg = segs[seg];
   const long long N = (long long)R * C;
@@ -484,14 +491,17 @@ __global__ void __launch_bounds__(1024) k_conv_rows(const ConvSeg *segs, const d
   auto sload = [&](int f, int n2) { return s[f * S + pad8(n2)]; };
   auto sstore = [&](int f, int n2, cplx v) { s[f * S + pad8(n2)] = v; };
   fft_block<false, false>(s, S, C, logC, nrows, twL, gload, sstore);
-  const double *H = spectra + (long long)sg.spec * spec_len;
+  const double *Hr = Hrows + (long long)sg.spec * N;
+  const double *Ha = Hr + (long long)ka * C, *Hb = Hr + (long long)kb * C;
+  const cplx *Wa = wrow + (long long)ka * C;
   auto at = [&](int f, int n2) -> cplx & { return s[f * S + pad8(n2)]; };
   if (ka == 0) {
-    // row 0: (0, k2) <-> (0, C - k2)
+    // row 0: (0, k2) <-> (0, C - k2); k = R k2, N - k = R (C - k2)
     for (int k2 = threadIdx.x; k2 <= C / 2; k2 += blockDim.x) {
       const int p2 = (C - k2) % C;
       cplx A = at(0, k2), B = at(0, p2);
-      spectral_pair(A, B, (long long)R * k2, N, H, T2);
+      const double Hnk = k2 ? Ha[C - k2] : spectra[(long long)sg.spec * spec_len + N];
+      spectral_pair(A, B, k2 == 0, Wa[k2], Ha[k2], Hnk);
       at(0, k2) = A;
       if (p2 != k2) at(0, p2) = B;
     }
@@ -500,7 +510,7 @@ __global__ void __launch_bounds__(1024) k_conv_rows(const ConvSeg *segs, const d
     for (int k2 = threadIdx.x; k2 < C / 2; k2 += blockDim.x) {
       const int p2 = C - 1 - k2;
       cplx A = at(0, k2), B = at(0, p2);
-      spectral_pair(A, B, ka + (long long)R * k2, N, H, T2);
+      spectral_pair(A, B, false, Wa[k2], Ha[k2], Ha[p2]);
       at(0, k2) = A;
       at(0, p2) = B;
     }
@@ -509,15 +519,15 @@ __global__ void __launch_bounds__(1024) k_conv_rows(const ConvSeg *segs, const d
     for (int k2 = threadIdx.x; k2 < C; k2 += blockDim.x) {
       const int p2 = C - 1 - k2;
       cplx A = at(0, k2), B = at(1, p2);
-      spectral_pair(A, B, ka + (long long)R * k2, N, H, T2);
+      spectral_pair(A, B, false, Wa[k2], Ha[k2], Hb[p2]);
       at(0, k2) = A;
       at(1, p2) = B;
     }
   }
   __syncthreads();
   auto gstore = [&](int f, int n2, cplx v) {
-    const int k1 = f ? kb : ka;
-    W[(long long)k1 * C + n2] = cmul(v, cconj(tw_n(T2, (long long)n2 * k1, N)));
+    const long long i = (long long)(f ? kb : ka) * C + n2;
+    W[i] = cmul(v, cconj(twrow[i]));
   };
   fft_block<true, false>(s, S, C, logC, nrows, twL, sload, gstore);
 }
@@ -525,11 +535,11 @@ __global__ void __launch_bounds__(1024) k_conv_rows(const ConvSeg *segs, const d
 // Pass 3: inverse column FFTs and real output.
 __global__ void __launch_bounds__(512, 2) k_conv_cols_inv(const ConvSeg *segs, const double2 *work,
                                                        double *y, int R, int logR, int C, int G,
-                                                       const cplx *T2) {
+                                                       const cplx *__restrict__ twr) {
   extern __shared__ double2 sm[];
   const int S = pad8(R) + 1;
   cplx *twL = sm + G * S;
-  load_twl(twL, R, T2, (long long)R * C);
+  load_twl(twL, R, twr);
   const int seg = blockIdx.y;
   const ConvSeg sg = segs[seg];
   const int c0 = blockIdx.x * G;
@@ -543,6 +553,34 @@ __global__ void __launch_bounds__(512, 2) k_conv_cols_inv(const ConvSeg *segs, c
     if (2 * m + 1 < sg.n_out) y[sg.y_off + 2 * m + 1] = v.y * scale;
   };
   fft_block<true, true>(sm, S, R, logR, G, twL, load, store);
+}
+
+// The row-ordered tables of the four-step split (FFTPlan), from T2.
+__global__ void k_fill_row_tables(const cplx *T2, long long N, int R, int C, cplx *twrow,
+                                  cplx *wrow, cplx *twr, cplx *twc) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long k1 = i / C, n2 = i % C;
+    twrow[i] = tw_n(T2, n2 * k1, N);
+    wrow[i] = T2[k1 + (long long)R * n2];
+    if (i < R) twr[i] = T2[i * (2 * N / R)];
+    if (i < C) twc[i] = T2[i * (2 * N / C)];
+  }
+}
+
+// rows[s][k1][k2] = H[s][k1 + R k2]: the transpose of each spectrum viewed
+// as a C x R matrix, through 32 x 32 shared-memory tiles
+__global__ void k_spectra_rows(const double *H, long long spec_len, int R, int C, double *rows) {
+  __shared__ double t[32][33];
+  const int s = blockIdx.z;
+  const double *h = H + (long long)s * spec_len;
+  double *o = rows + (long long)s * R * C;
+  const int k1b = blockIdx.x * 32, k2b = blockIdx.y * 32;
+  for (int y = threadIdx.y; y < 32; y += blockDim.y)
+    t[y][threadIdx.x] = h[(long long)(k2b + y) * R + k1b + threadIdx.x];
+  __syncthreads();
+  for (int y = threadIdx.y; y < 32; y += blockDim.y)
+    o[(long long)(k1b + y) * C + k2b + threadIdx.x] = t[threadIdx.x][y];
 }
 
 int ilog2(long v) {
@@ -568,9 +606,49 @@ FFTPlan::FFTPlan(long nof_) : nof(nof_), N(nof_ / 2) {
 }
 
 FFTPlan::~FFTPlan() {
-  if (table) dev_free(table);
-  if (work) dev_free(work);
-  if (means) dev_free(means);
+  forget_spectra();
+  for (double *p : {table, work, means, twrow, wrow, twr, twc})
+    if (p) dev_free(p);
+}
+
+void FFTPlan::forget_spectra() {
+  for (RowSpectra &c : cache) {
+    if (c.rows) dev_free(c.rows);
+    c = RowSpectra{};
+  }
+}
+
+void FFTPlan::make_tables(cudaStream_t st) {
+  if (twrow || !R) return;
+  twrow = (double *)dev_alloc((size_t)N * sizeof(double2));
+  wrow = (double *)dev_alloc((size_t)N * sizeof(double2));
+  twr = (double *)dev_alloc((size_t)R * sizeof(double2));
+  twc = (double *)dev_alloc((size_t)C * sizeof(double2));
+  MADAM_LAUNCH(k_fill_row_tables, (unsigned)std::min<long long>(4096, (N + 255) / 256), 256, 0,
+               st, (const cplx *)table, (long long)N, R, C, (cplx *)twrow, (cplx *)wrow,
+               (cplx *)twr, (cplx *)twc);
+}
+
+const double *FFTPlan::row_spectra(cudaStream_t st, const double *spectra, long nspec) {
+  for (const RowSpectra &c : cache)
+    if (c.rows && c.src == spectra && c.nspec == nspec) return c.rows;
+  // a free slot, else the first one is dropped
+  RowSpectra *slot = &cache[0];
+  for (RowSpectra &c : cache)
+    if (!c.rows) {
+      slot = &c;
+      break;
+    }
+  if (slot->rows) dev_free(slot->rows);
+  slot->src = spectra;
+  slot->nspec = nspec;
+  slot->rows = (double *)dev_alloc((size_t)std::max<long>(1, nspec) * N * sizeof(double));
+  if (nspec > 0) {
+    if (nspec > 65535) fail("too many filter spectra");
+    MADAM_LAUNCH(k_spectra_rows, dim3(R / 32, C / 32, (unsigned)nspec), dim3(32, 8), 0, st,
+                 spectra, (long long)N + 1, R, C, slot->rows);
+  }
+  return slot->rows;
 }
 
 void FFTPlan::reserve(long nseg) {
@@ -585,7 +663,7 @@ void FFTPlan::reserve(long nseg) {
 }
 
 void FFTPlan::convolve(cudaStream_t st, const ConvSeg *segs, long nseg, const double *spectra,
-                       const double *x, double *y) {
+                       long nspec, const double *x, double *y) {
   if (nseg == 0) return;
   if (!table) {
     table = (double *)dev_alloc((size_t)2 * N * sizeof(double2));
@@ -627,13 +705,16 @@ void FFTPlan::convolve(cudaStream_t st, const ConvSeg *segs, long nseg, const do
                                       200 * 1024));
       attr = true;
     }
+    make_tables(st);
+    const double *Hrows = row_spectra(st, spectra, nspec);
     dim3 gc(C / G, (unsigned)nseg), gr(R / 2 + 1, (unsigned)nseg);
     MADAM_LAUNCH(k_conv_cols_fwd, gc, tcols, smem_cols, st, segs, x, means, (double2 *)work, R,
-                 logR, C, G, T2);
-    MADAM_LAUNCH(k_conv_rows, gr, trows, smem_rows, st, segs, spectra, spec_len, (double2 *)work, R,
-                 C, logC, T2);
+                 logR, C, G, (const cplx *)twrow, (const cplx *)twr);
+    MADAM_LAUNCH(k_conv_rows, gr, trows, smem_rows, st, segs, Hrows, spectra, spec_len,
+                 (double2 *)work, R, C, logC, (const cplx *)twrow, (const cplx *)wrow,
+                 (const cplx *)twc);
     MADAM_LAUNCH(k_conv_cols_inv, gc, tcols, smem_cols, st, segs, (const double2 *)work, y, R,
-                 logR, C, G, T2);
+                 logR, C, G, (const cplx *)twr);
   }
   MADAM_LAUNCH(k_seg_sum, gm, 256, 0, st, segs, y, 1, means);
   MADAM_LAUNCH(k_seg_sub_mean, gm, 256, 0, st, segs, y, means);

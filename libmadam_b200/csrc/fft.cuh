@@ -23,12 +23,32 @@ struct FFTPlan {
   double *table = nullptr;  // 2N complex twiddles exp(-2 pi i m / (2N))
   double *means = nullptr;  // nseg_max
   long nseg_max = 0;
+  // Four-step tables laid out so that a row of the split reads them
+  // contiguously: twrow[k1][n2] = exp(-2 pi i n2 k1 / N) (the inter-pass
+  // twiddles), wrow[k1][k2] = exp(-i pi (k1 + R k2) / N) (the real split),
+  // and the sub-transform twiddles exp(-2 pi i q / L) for L = R and C.  The
+  // values are those of `table`.
+  double *twrow = nullptr, *wrow = nullptr, *twr = nullptr, *twc = nullptr;
+  // Spectra copied into the rows of the split: rows[s][k1][k2] =
+  // spectra[s][k1 + R k2], one copy per spectra array, kept while the plan
+  // lives (forget_spectra() drops them when an array is rewritten).
+  struct RowSpectra {
+    const double *src;
+    long nspec;
+    double *rows;
+  };
+  RowSpectra cache[4] = {};
   explicit FFTPlan(long nof_);
   ~FFTPlan();
   void reserve(long nseg);
+  void forget_spectra();
   // segs: device table of nseg entries; spectra: [nspec][nof/2+1] (device)
-  void convolve(cudaStream_t st, const ConvSeg *segs, long nseg,
-                const double *spectra, const double *x, double *y);
+  void convolve(cudaStream_t st, const ConvSeg *segs, long nseg, const double *spectra,
+                long nspec, const double *x, double *y);
+
+ private:
+  void make_tables(cudaStream_t st);
+  const double *row_spectra(cudaStream_t st, const double *spectra, long nspec);
 };
 
 }  // namespace madam
