@@ -299,6 +299,24 @@ __device__ __forceinline__ void load_twl(cplx *twL, int L, const cplx *tw) {
   for (int q = threadIdx.x; q < L; q += blockDim.x) twL[q] = tw[q];
 }
 
+// The twiddles of the radix-8 passes p >= 1 (sub-transform size Ns = 8^p)
+// in the order the threads read them: ptw[off_p + (k - 1) Ns + r] =
+// exp(-2 pi i r k L / (8 Ns) / L) for k = 1..7, r < Ns, so that consecutive
+// threads (consecutive r) read consecutive entries with no bank conflicts.
+// At most L - 8 entries; the values are those of tw.
+__device__ __forceinline__ void load_pass_tw(cplx *ptw, int L, int logL, const cplx *tw) {
+  const int n8 = logL / 3;
+  int off = 0;
+  for (int p = 1, Ns = 8; p < n8; ++p, Ns *= 8) {
+    const int step = L / (8 * Ns);
+    for (int e = threadIdx.x; e < 7 * Ns; e += blockDim.x) {
+      const int k = e / Ns + 1, r = e % Ns;
+      ptw[off + e] = tw[r * step * k];
+    }
+    off += 7 * Ns;
+  }
+}
+
 template <bool INV>
 __device__ __forceinline__ cplx mul_mi(cplx a) {  // a * (-i), inverse a * i
   return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
@@ -395,11 +413,12 @@ __device__ __forceinline__ void last_pass(cplx *s, int S, int L, int nfft, const
 // store(f, i, v) takes output element i of the last pass.
 template <bool INV, bool FFAST, typename Load, typename Store>
 __device__ __forceinline__ void fft_block(cplx *s, int S, int L, int logL, int nfft,
-                                          const cplx *twL, Load load, Store store) {
+                                          const cplx *twL, const cplx *ptw, Load load,
+                                          Store store) {
   const int L8 = L >> 3, n8 = logL / 3, rem = logL - 3 * n8;
   const int nb8 = nfft * L8;
   const int t = threadIdx.x;
-  int Ns = 1;
+  int Ns = 1, poff = 0;
   for (int pass = 0; pass < n8; ++pass) {
     const bool first = pass == 0, last = pass == n8 - 1 && rem == 0;
     const bool act = t < nb8;
@@ -414,10 +433,12 @@ __device__ __forceinline__ void fft_block(cplx *s, int S, int L, int logL, int n
     __syncthreads();
     if (act) {
       if (!first) {
-        const int r = j & (Ns - 1);
-        const int qs = r * (L / (8 * Ns));
+        const cplx *pt = ptw + poff + (j & (Ns - 1));
 #pragma unroll
-        for (int k = 1; k < 8; ++k) v[k] = cmul(v[k], tw_l<INV>(twL, qs * k));
+        for (int k = 1; k < 8; ++k) {
+          const cplx w = pt[(k - 1) * Ns];
+          v[k] = cmul(v[k], INV ? cconj(w) : w);
+        }
       }
       dft8<INV>(v);
       if (last) {
@@ -430,6 +451,7 @@ __device__ __forceinline__ void fft_block(cplx *s, int S, int L, int logL, int n
       }
     }
     __syncthreads();
+    if (pass > 0) poff += 7 * Ns;
     Ns *= 8;
   }
   if (rem == 1) last_pass<2, INV, FFAST>(s, S, L, nfft, twL, nb8, store);
@@ -445,8 +467,9 @@ __global__ void __launch_bounds__(512, 2) k_conv_cols_fwd(const ConvSeg *segs, c
                                                        const cplx *__restrict__ twr) {
   extern __shared__ double2 sm[];
   const int S = pad8(R) + 1;
-  cplx *twL = sm + G * S;
+  cplx *twL = sm + G * S, *ptw = twL + R;
   load_twl(twL, R, twr);
+  load_pass_tw(ptw, R, logR, twr);
   const int seg = blockIdx.y;
   const ConvSeg sg = segs[seg];
   const double mean = seg_mean(part, seg, sg.n_in, sg.flags & 1);
@@ -461,7 +484,7 @@ __global__ void __launch_bounds__(512, 2) k_conv_cols_fwd(const ConvSeg *segs, c
     const long long i = (long long)k1 * C + c0 + f;
     W[i] = cmul(v, twrow[i]);
   };
-  fft_block<false, true>(sm, S, R, logR, G, twL, load, store);
+  fft_block<false, true>(sm, S, R, logR, G, twL, ptw, load, store);
 }
 
 // Pass 2: forward row FFTs of rows k1 and R-k1, spectral product, inverse
@@ -478,8 +501,9 @@ __global__ void __launch_bounds__(1024) k_conv_rows(const ConvSeg *segs,
   extern __shared__ double2 sm[];
   const int S = pad8(C) + 1;
   cplx *s = sm;  // 2 rows
-  cplx *twL = sm + 2 * S;
+  cplx *twL = sm + 2 * S, *ptw = twL + C;
   load_twl(twL, C, twc);
+  load_pass_tw(ptw, C, logC, twc);
   const int seg = blockIdx.y;
   const ConvSeg sg = segs[seg];
   const long long N = (long long)R * C;
@@ -490,7 +514,7 @@ __global__ void __launch_bounds__(1024) k_conv_rows(const ConvSeg *segs,
   auto gload = [&](int f, int n2) { return W[(long long)(f ? kb : ka) * C + n2]; };
   auto sload = [&](int f, int n2) { return s[f * S + pad8(n2)]; };
   auto sstore = [&](int f, int n2, cplx v) { s[f * S + pad8(n2)] = v; };
-  fft_block<false, false>(s, S, C, logC, nrows, twL, gload, sstore);
+  fft_block<false, false>(s, S, C, logC, nrows, twL, ptw, gload, sstore);
   const double *Hr = Hrows + (long long)sg.spec * N;
   const double *Ha = Hr + (long long)ka * C, *Hb = Hr + (long long)kb * C;
   const cplx *Wa = wrow + (long long)ka * C;
@@ -529,7 +553,7 @@ __global__ void __launch_bounds__(1024) k_conv_rows(const ConvSeg *segs,
     const long long i = (long long)(f ? kb : ka) * C + n2;
     W[i] = cmul(v, cconj(twrow[i]));
   };
-  fft_block<true, false>(s, S, C, logC, nrows, twL, sload, gstore);
+  fft_block<true, false>(s, S, C, logC, nrows, twL, ptw, sload, gstore);
 }
 
 // Pass 3: inverse column FFTs and real output.
@@ -538,8 +562,9 @@ __global__ void __launch_bounds__(512, 2) k_conv_cols_inv(const ConvSeg *segs, c
                                                        const cplx *__restrict__ twr) {
   extern __shared__ double2 sm[];
   const int S = pad8(R) + 1;
-  cplx *twL = sm + G * S;
+  cplx *twL = sm + G * S, *ptw = twL + R;
   load_twl(twL, R, twr);
+  load_pass_tw(ptw, R, logR, twr);
   const int seg = blockIdx.y;
   const ConvSeg sg = segs[seg];
   const int c0 = blockIdx.x * G;
@@ -552,7 +577,7 @@ __global__ void __launch_bounds__(512, 2) k_conv_cols_inv(const ConvSeg *segs, c
     if (2 * m < sg.n_out) y[sg.y_off + 2 * m] = v.x * scale;
     if (2 * m + 1 < sg.n_out) y[sg.y_off + 2 * m + 1] = v.y * scale;
   };
-  fft_block<true, true>(sm, S, R, logR, G, twL, load, store);
+  fft_block<true, true>(sm, S, R, logR, G, twL, ptw, load, store);
 }
 
 // The row-ordered tables of the four-step split (FFTPlan), from T2.
@@ -690,19 +715,24 @@ void FFTPlan::convolve(cudaStream_t st, const ConvSeg *segs, long nseg, const do
   } else {
     const int logR = ilog2(R), logC = ilog2(C);
     auto padded = [](long L) { return L + L / 8 + 1; };
-    // rows padded one slot in nine, then the sub-transform twiddle table
-    size_t smem_cols = (size_t)(G * padded(R) + R) * sizeof(double2);
-    size_t smem_rows = (size_t)(2 * padded(C) + C) * sizeof(double2);
+    // rows padded one slot in nine, then the sub-transform twiddle table and
+    // the passes' twiddles (8^(log8 L) - 8 entries)
+    auto passes = [](int logL) { return logL >= 6 ? (1L << (3 * (logL / 3))) - 8 : 0L; };
+    size_t smem_cols = (size_t)(G * padded(R) + R + passes(logR)) * sizeof(double2);
+    size_t smem_rows = (size_t)(2 * padded(C) + C + passes(logC)) * sizeof(double2);
+    constexpr size_t kSmemMax = 227 * 1024;
+    if (smem_cols > kSmemMax || smem_rows > kSmemMax)
+      fail("FFT length too large for the four-step filter");
     const unsigned tcols = (unsigned)std::max(32, G * R / 8);
     const unsigned trows = (unsigned)std::max(32, C / 4);
     static bool attr = false;
     if (!attr) {
       MADAM_CUDA(cudaFuncSetAttribute(k_conv_cols_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      200 * 1024));
+                                      (int)kSmemMax));
       MADAM_CUDA(cudaFuncSetAttribute(k_conv_cols_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      200 * 1024));
+                                      (int)kSmemMax));
       MADAM_CUDA(cudaFuncSetAttribute(k_conv_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      200 * 1024));
+                                      (int)kSmemMax));
       attr = true;
     }
     make_tables(st);
