@@ -362,6 +362,10 @@ def run_mc(args, world, rank, local):
                 "iterations": {"min": int(its.min()), "max": int(its.max()),
                                "single_rhs": it1},
                 "batch_iterate_ms": t_it, "batch_setup_ms": tb["setup_ms"],
+                "phases_ms_per_iteration": {
+                    k: tb[k + "_ms"] / max(1, int(its.max()))
+                    for k in ("scatter", "gather", "filter", "precond")},
+                "reliable_updates_ms": tb["other_ms"],
                 "batch_finalize_ms": tb["finalize_ms"],
                 "fp64_batch": {"value": value64, "iterate_ms": t64["iterate_ms"],
                                "iterations_max": int(its64.max()),
@@ -834,7 +838,8 @@ def extra_mc(args, world, rank, local):
     if r is None:
         return None
     keep = ("metric", "value", "unit", "ms_per_step", "clocks", "dtype", "iterations",
-            "batch_iterate_ms", "batch_setup_ms", "fp64_batch", "fp32_vs_fp64",
+            "batch_iterate_ms", "batch_setup_ms", "phases_ms_per_iteration",
+            "reliable_updates_ms", "fp64_batch", "fp32_vs_fp64",
             "reliable_updates", "single_rhs",
             "speedup_vs_one_at_a_time")
     out = {k: r[k] for k in keep}

@@ -334,6 +334,63 @@ __global__ void __launch_bounds__(256) k_scatter_T(
   }
 }
 
+// The FP32-TOD batch's baseline_to_map over the same chunks: lane j holds
+// right-hand sides j, j + 32, ... (all GW of a row in one launch) and adds a
+// chunk's entries in entry order.  The float32 p.detw already sets this
+// form's precision, so the single solve's summation tree is not rebuilt.
+template <int NMAP, int GW>
+__global__ void __launch_bounds__(256) k_scatter_T_seq(
+    const int4 *__restrict__ chunks, long long nchunks, const float4 *__restrict__ sp4,
+    const int2 *__restrict__ sp2, const float *__restrict__ pwT, double *__restrict__ target,
+    double *__restrict__ partial) {
+  constexpr int G = GW / 32;
+  constexpr int U = kScatterChunk / 32;
+  __shared__ float4 rec[8][kScatterChunk];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  float4 *rw = rec[wid];
+  for (long long c = w0; c < nchunks; c += nwarps) {
+    const int4 ck = chunks[c];  // {pixel, first entry, entries, partial slot or -1}
+#pragma unroll
+    for (int r = 0; r < U; ++r) {
+      const int i = r * 32 + lane;
+      if (i < ck.z)
+        rw[i] = NMAP == 3 ? __ldcs(sp4 + ck.y + i)
+                          : make_float4(1.f, 0.f, 0.f, __int_as_float(__ldcs(&sp2[ck.y + i].x)));
+    }
+    __syncwarp();
+    double P[G][NMAP];
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int e = 0; e < NMAP; ++e) P[g][e] = 0.0;
+#pragma unroll 8
+    for (int i = 0; i < ck.z; ++i) {
+      const float4 q = rw[i];
+      const float *pk = pwT + (long long)__float_as_int(q.w) * GW + lane;
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        const double wv = (double)__ldg(pk + g * 32);
+        if (NMAP == 3) {
+          P[g][0] = fma((double)q.x, wv, P[g][0]);
+          P[g][1] = fma((double)q.y, wv, P[g][1]);
+          P[g][2] = fma((double)q.z, wv, P[g][2]);
+        } else {
+          P[g][0] += wv;
+        }
+      }
+    }
+    double *out = ck.w < 0 ? target + (long long)ck.x * NMAP * GW
+                           : partial + (long long)ck.w * NMAP * GW;
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+#pragma unroll
+      for (int e = 0; e < NMAP; ++e) out[e * GW + g * 32 + lane] = P[g][e];
+    __syncwarp();
+  }
+}
+
 // multi-chunk pixels {pixel, first partial slot, chunks}: partial sums added
 // in chunk order; thread per (pixel, component, right-hand side)
 template <int NMAP, int G>

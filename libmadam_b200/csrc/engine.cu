@@ -1139,22 +1139,46 @@ __global__ void k_fprec(const double *fcov, const double *w, long nh, long npsd,
 }
 
 // Power of each PSD's inverse-covariance kernel, summed in the host's order
-// (one thread per PSD): ptot = sum_{k < nof/2} icv_k^2 and the running sums
-// pre[k] = sum_{k' <= k} icv_k'^2 for k < W, from which the band width is
-// chosen.
-__global__ void k_invcov_power(const double *icv, long nof, long npsd, long W, double *ptot,
-                               double *pre) {
-  const long ip = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (ip >= npsd) return;
+// (construct_preconditioner, noise_routines.f90:1039-1060): ptot =
+// sum_{k < nof/2} icv_k^2 and the running sums pre[k] = sum_{k' <= k}
+// icv_k'^2 for k < W, from which the band width is chosen.  One CTA per PSD:
+// the other warps stage the squares of the next 2048 values in shared
+// memory while thread 0 adds the current ones one after the other (the
+// additions stay sequential, so the sums are the host's to the bit).
+constexpr int kPowTile = 2048;
+__global__ void __launch_bounds__(256) k_invcov_power(const double *icv, long nof, long W,
+                                                      double *ptot, double *pre) {
+  __shared__ double sq[2][kPowTile];
+  const long ip = blockIdx.x;
   const double *c = icv + ip * nof;
+  const long nsum = nof / 2, nk = max(nsum, W);
+  const long ntile = (nk + kPowTile - 1) / kPowTile;
+  auto stage = [&](long t, int buf, int t0, int stride) {
+    for (int i = t0; i < kPowTile; i += stride) {
+      const long k = t * kPowTile + i;
+      sq[buf][i] = k < nk ? __dmul_rn(c[k], c[k]) : 0.0;
+    }
+  };
+  stage(0, 0, threadIdx.x, blockDim.x);
+  __syncthreads();
   double s = 0.0;
-  for (long k = 0; k < nof / 2; ++k) s = __dadd_rn(s, __dmul_rn(c[k], c[k]));
-  ptot[ip] = s;
-  double q = 0.0;
-  for (long k = 0; k < W; ++k) {
-    q = __dadd_rn(q, __dmul_rn(c[k], c[k]));
-    pre[ip * W + k] = q;
+  for (long t = 0; t < ntile; ++t) {
+    const int buf = (int)(t & 1);
+    if (threadIdx.x >= 32) {
+      if (t + 1 < ntile) stage(t + 1, buf ^ 1, threadIdx.x - 32, blockDim.x - 32);
+    } else if (threadIdx.x == 0) {
+      const long k0 = t * kPowTile;
+      const int m = (int)min((long)kPowTile, nk - k0);
+      for (int i = 0; i < m; ++i) {
+        s = __dadd_rn(s, sq[buf][i]);
+        const long k = k0 + i;
+        if (k < W) pre[ip * W + k] = s;
+        if (k == nsum - 1) ptot[ip] = s;
+      }
+    }
+    __syncthreads();
   }
+  if (threadIdx.x == 0 && nsum == 0) ptot[ip] = 0.0;
 }
 
 __global__ void k_iota(int *a, long long n) {

@@ -257,6 +257,7 @@ class Engine {
   // --- batched Monte Carlo
   void iterate_batch();
   void apply_A_batch();
+  bool batch_timed_ = false;  // iterate_batch: phase events in apply_A_batch
   void apply_preconditioner_batch(const double *r, double *z);
   void build_batch_tables();
   template <int G>

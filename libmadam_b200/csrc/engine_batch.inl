@@ -176,10 +176,21 @@ void Engine::project_group_T2(long r0, int nr) {
   scatpT_.alloc((size_t)std::max<size_t>(1, scatter_partial_.n / nmap_) * nmap_ * GW);
   apnT_.alloc((size_t)nb * GW);
   const unsigned tb = (unsigned)std::min<long long>(4736, (nb + 31) / 32);
+  if (batch_timed_) MADAM_CUDA(cudaEventRecord(ev_[2], st_));
   MADAM_LAUNCH((k_transpose_rhs<G, T>), dim3(tb, G), 256, 0, st_, pwb_.get(), nb, (int)r0, nr,
                pwT);
   // 1) baseline -> map, combine, ccmultiply
-  if (nloc_cross_ > 0 && nscatter_chunks_ > 0) {
+  if (nloc_cross_ > 0 && nscatter_chunks_ > 0 && f32) {
+    // FP32-TOD form: all GW right-hand sides in one pass, entry-order sums
+    if (nmap_ == 3)
+      MADAM_LAUNCH((k_scatter_T_seq<3, GW>), kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
+                   nscatter_chunks_, sp4_.get(), sp2_.get(), (const float *)pwT, lmapT_.get(),
+                   scatpT_.get());
+    else
+      MADAM_LAUNCH((k_scatter_T_seq<1, GW>), kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
+                   nscatter_chunks_, sp4_.get(), sp2_.get(), (const float *)pwT, lmapT_.get(),
+                   scatpT_.get());
+  } else if (nloc_cross_ > 0 && nscatter_chunks_ > 0) {
     // one launch per 32 right-hand sides (fewer registers, more warps)
     for (int g0 = 0; g0 < GW; g0 += 32) {
       if (nmap_ == 3)
@@ -191,15 +202,15 @@ void Engine::project_group_T2(long r0, int nr) {
                      nscatter_chunks_, sp4_.get(), sp2_.get(), (const T *)pwT, g0,
                      lmapT_.get(), scatpT_.get());
     }
-    if (nscatter_multi_ > 0) {
-      const long long tot = (long long)nscatter_multi_ * nmap_ * GW;
-      if (nmap_ == 3)
-        MADAM_LAUNCH((k_scatter_combine_T<3, G>), grid_for(tot), 256, 0, st_,
-                     scatter_multi_.get(), nscatter_multi_, scatpT_.get(), lmapT_.get());
-      else
-        MADAM_LAUNCH((k_scatter_combine_T<1, G>), grid_for(tot), 256, 0, st_,
-                     scatter_multi_.get(), nscatter_multi_, scatpT_.get(), lmapT_.get());
-    }
+  }
+  if (nloc_cross_ > 0 && nscatter_chunks_ > 0 && nscatter_multi_ > 0) {
+    const long long tot = (long long)nscatter_multi_ * nmap_ * GW;
+    if (nmap_ == 3)
+      MADAM_LAUNCH((k_scatter_combine_T<3, G>), grid_for(tot), 256, 0, st_,
+                   scatter_multi_.get(), nscatter_multi_, scatpT_.get(), lmapT_.get());
+    else
+      MADAM_LAUNCH((k_scatter_combine_T<1, G>), grid_for(tot), 256, 0, st_,
+                   scatter_multi_.get(), nscatter_multi_, scatpT_.get(), lmapT_.get());
   }
   float *mf = f32 ? lmapTf_.get() : nullptr;
   if (nloc_cross_ > 0) {
@@ -211,6 +222,7 @@ void Engine::project_group_T2(long r0, int nr) {
                    cca_.get(), lmapT_.get(), (long long)nloc_cross_, mf);
   }
   // 3) map -> baseline sums, then ap and p.ap per right-hand side
+  if (batch_timed_) MADAM_CUDA(cudaEventRecord(ev_[3], st_));
   const T *mT = f32 ? (const T *)lmapTf_.get() : (const T *)lmapT_.get();
   if (nmap_ == 3)
     MADAM_LAUNCH((k_gather_T<3, G, T>), kRedBlocks, 256, 0, st_, gather_chunks_.get(),
@@ -222,6 +234,7 @@ void Engine::project_group_T2(long r0, int nr) {
                  nsamp_, mT, (int)ndeg_shift_, (int)nloc_, apnT_.get());
   MADAM_LAUNCH(k_gather_finish_T<G>, kRedBlocks, 256, 0, st_, apnT_.get(), nb, bw_.get(),
                nna_.get(), rmask_.get(), pb_.get(), apb_.get(), (int)r0, nr, partb_.get());
+  if (batch_timed_) MADAM_CUDA(cudaEventRecord(ev_[4], st_));
 }
 
 void Engine::apply_A_batch() {
@@ -231,6 +244,7 @@ void Engine::apply_A_batch() {
   const long long pstride = (long long)scatter_partial_.n;
   // noise prior ap = C_a^-1 p (cinvmul, 829-845); the projections add to it
   const long long nt = nb * nrhs_;
+  if (batch_timed_) MADAM_CUDA(cudaEventRecord(ev_[0], st_));
   if (par_.kfilter) {
     MADAM_CUDA(cudaMemcpyAsync(apb_.get(), pb_.get(), nt * sizeof(double),
                                cudaMemcpyDeviceToDevice, st_));
@@ -244,6 +258,7 @@ void Engine::apply_A_batch() {
   } else {
     MADAM_CUDA(cudaMemsetAsync(apb_.get(), 0, nt * sizeof(double), st_));
   }
+  if (batch_timed_) MADAM_CUDA(cudaEventRecord(ev_[1], st_));
   if (ngather_chunks_ > 0) {
     // right-hand-side-minor projections, 64 right-hand sides a pass
     for (long r0 = 0; r0 < nrhs_; r0 += 64) {
@@ -374,18 +389,35 @@ void Engine::iterate_batch() {
   std::vector<double> rr_true(rrinit_b_);
   n_reliable_ = 0;
   long istep = 0;
+  // phase times (CUDA events; the projections' of the last 64-RHS group when
+  // there are several)
+  batch_timed_ = ngather_chunks_ > 0 && nrhs_ <= 64;
   while (istep < par_.iter_max && nact > 0) {
     ++istep;
     apply_A_batch();
     MADAM_LAUNCH(k_update_ar_b, gv, 256, 0, st_, aab_.get(), rb_.get(), rob_.get(), pb_.get(),
                  apb_.get(), nb, scalb_.get(), actb_.get());
+    if (batch_timed_) MADAM_CUDA(cudaEventRecord(ev_[5], st_));
     apply_preconditioner_batch(rb_.get(), zb_.get());
+    if (batch_timed_) MADAM_CUDA(cudaEventRecord(ev_[6], st_));
     MADAM_LAUNCH(k_dots_b, gd, 256, 0, st_, rb_.get(), zb_.get(), rob_.get(), zb_.get(),
                  rb_.get(), rb_.get(), 3, rmask_.get(), nb, actb_.get(), partb_.get());
     MADAM_LAUNCH(k_finish_b, (unsigned)R, 1024, 0, st_, partb_.get(), kRedBlocks, 3,
                  scalb_.get(), 2, 0, actb_.get());
     fetch();
+    if (batch_timed_) {
+      float tm[4];
+      MADAM_CUDA(cudaEventElapsedTime(&tm[0], ev_[0], ev_[1]));
+      MADAM_CUDA(cudaEventElapsedTime(&tm[1], ev_[2], ev_[3]));
+      MADAM_CUDA(cudaEventElapsedTime(&tm[2], ev_[3], ev_[4]));
+      MADAM_CUDA(cudaEventElapsedTime(&tm[3], ev_[5], ev_[6]));
+      timings.filter_ms += tm[0];
+      timings.scatter_ms += tm[1];
+      timings.gather_ms += tm[2];
+      timings.precond_ms += tm[3];
+    }
     if (refine_b) {
+      const double tr0 = now_ms();
       std::vector<long> upd;
       for (long k = 0; k < R; ++k) {
         if (!act_host_[k]) continue;
@@ -413,6 +445,7 @@ void Engine::iterate_batch() {
         fetch();
         for (long k : upd) rr_true[k] = sc[k * S_NSCAL + S_RR];
       }
+      timings.other_ms += now_ms() - tr0;  // the reliable updates
     }
     bool changed = false;
     for (long k = 0; k < R; ++k) {
@@ -434,6 +467,7 @@ void Engine::iterate_batch() {
                  scalb_.get(), 0, actb_.get());
   }
   MADAM_CUDA(cudaStreamSynchronize(st_));
+  batch_timed_ = false;
   check_band_err();
   timings.iterate_ms = now_ms() - t0;
 }

@@ -1563,14 +1563,16 @@ void Engine::construct_preconditioner() {
     DevBuf<double> dpt, dpre;
     dpt.alloc(std::max<long>(1, npsdtot_));
     dpre.alloc(std::max<size_t>(1, ppre.size()));
-    MADAM_LAUNCH(k_invcov_power, (unsigned)((npsdtot_ + 63) / 64), 64, 0, st_, invcov_.get(),
-                 nof_, (long)npsdtot_, pw_w, dpt.get(), dpre.get());
+    if (npsdtot_ > 0)
+      MADAM_LAUNCH(k_invcov_power, (unsigned)npsdtot_, 256, 0, st_, invcov_.get(), nof_, pw_w,
+                   dpt.get(), dpre.get());
     MADAM_CUDA(cudaMemcpyAsync(ptot.data(), dpt.get(), npsdtot_ * sizeof(double),
                                cudaMemcpyDeviceToHost, st_));
     MADAM_CUDA(cudaMemcpyAsync(ppre.data(), dpre.get(), ppre.size() * sizeof(double),
                                cudaMemcpyDeviceToHost, st_));
     MADAM_CUDA(cudaStreamSynchronize(st_));
   }
+  trace("precond: fprec+invcov");
   // candidate segments
   std::vector<int> cand;
   for (int i = 0; i < (int)segs_.size(); ++i) {
@@ -1717,6 +1719,7 @@ void Engine::construct_preconditioner() {
     }
     todo.swap(next);
   }
+  trace("precond: factor");
   // pack the deduplicated factors the apply step uses (prec_ok segments),
   // ordered by register width class so that each class's chunks are contiguous
   struct Pack { const Done2 *dn; std::vector<PRun> rl; int W; };
@@ -1898,7 +1901,9 @@ void Engine::construct_preconditioner() {
   band2_rows_ = nunique;
   band2_ntrans_ = (long)trans.size();
   band2_chunk_ = C;
+  trace("precond: scan tables");
   build_guarded_chunks(pruns, cruns);
+  trace("precond: guarded chunks");
   // plain column store for the wide bands
   long long total = 0;
   band_segs_.clear();
