@@ -507,6 +507,58 @@ __global__ void __launch_bounds__(256) k_gather_T(
   }
 }
 
+// The FP32-TOD batch's map_to_baseline over pointing pairs (as
+// k_gather_pairs): chunks {first baseline, baselines, first pair, pairs},
+// per-baseline pair offsets poff, pair records {sum w, cross pixel (-1:
+// none)}; lane j holds right-hand sides j, j + 32, ... and sums each
+// baseline's pairs in time order from the float32 map rows.
+template <int G>
+__global__ void __launch_bounds__(256) k_gather_T_pairs(
+    const int4 *__restrict__ chunks, long long nchunks, const float4 *__restrict__ gp4,
+    const int *__restrict__ poff, const float *__restrict__ mT, double *__restrict__ apnT) {
+  constexpr int GW = 32 * G;
+  constexpr int U = kGatherChunk / 32;
+  __shared__ float4 rec[8][kGatherChunk];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  float4 *rw = rec[wid];
+  for (long long c = w0; c < nchunks; c += nwarps) {
+    const int4 ck = chunks[c];
+#pragma unroll
+    for (int r = 0; r < U; ++r) {
+      const int i = r * 32 + lane;
+      if (i < ck.w) rw[i] = __ldcs(gp4 + (long long)ck.z + i);
+    }
+    __syncwarp();
+    int a1 = poff[ck.x] - ck.z;
+    for (int j = 0; j < ck.y; ++j) {
+      const int a0 = a1;
+      a1 = poff[ck.x + j + 1] - ck.z;
+      double apn[G];
+#pragma unroll
+      for (int g = 0; g < G; ++g) apn[g] = 0.0;
+#pragma unroll 4
+      for (int s = a0; s < a1; ++s) {
+        const float4 q = rw[s];
+        const int px = __float_as_int(q.w);
+        if (px >= 0) {
+          const float *mm = mT + (long long)px * 3 * GW + lane;
+#pragma unroll
+          for (int g = 0; g < G; ++g) {
+            const double m0 = (double)__ldg(mm + g * 32), m1 = (double)__ldg(mm + GW + g * 32),
+                         m2 = (double)__ldg(mm + 2 * GW + g * 32);
+            apn[g] += fma((double)q.z, m2, fma((double)q.y, m1, (double)q.x * m0));
+          }
+        }
+      }
+#pragma unroll
+      for (int g = 0; g < G; ++g) apnT[(long long)(ck.x + j) * GW + g * 32 + lane] = apn[g];
+    }
+    __syncwarp();
+  }
+}
+
 // ap[r][b] = ap + (nna p - apn detw) for the group's right-hand sides and the
 // p.ap partial sums per block; a block transposes tiles of 32 baselines
 template <int G>

@@ -224,7 +224,12 @@ void Engine::project_group_T2(long r0, int nr) {
   // 3) map -> baseline sums, then ap and p.ap per right-hand side
   if (batch_timed_) MADAM_CUDA(cudaEventRecord(ev_[3], st_));
   const T *mT = f32 ? (const T *)lmapTf_.get() : (const T *)lmapT_.get();
-  if (nmap_ == 3)
+  if (f32 && use_pairs_ && nmap_ == 3 && npair_chunks_ > 0) {
+    // FP32-TOD form: over the pointing pairs (fewer map rows to read); the
+    // chunks cover every baseline, so apnT is written for all of them
+    MADAM_LAUNCH(k_gather_T_pairs<G>, kRedBlocks, 256, 0, st_, pair_chunks_.get(),
+                 npair_chunks_, gp4_.get(), poff_.get(), lmapTf_.get(), apnT_.get());
+  } else if (nmap_ == 3)
     MADAM_LAUNCH((k_gather_T<3, G, T>), kRedBlocks, 256, 0, st_, gather_chunks_.get(),
                  ngather_chunks_, point4_.get(), pixc_.get(), bstart_d_.get(), noba_short_,
                  nsamp_, mT, (int)ndeg_shift_, (int)nloc_, apnT_.get());
