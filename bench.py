@@ -42,12 +42,15 @@ def profiled_traffic(kernel, nsamp):
     """DRAM bytes of one launch of `kernel` at `nsamp` samples, from the committed ncu
     summary (bytes per sample of a smaller capture; traffic grows with the samples)."""
     import re
-    try:
-        with open(os.path.join(ROOT, "profiles", kernel + "_mid.md")) as f:
-            m = re.search(r"dram_bytes_per_sample = ([0-9.]+) B", f.read())
-        return float(m.group(1)) * nsamp if m else None
-    except OSError:
-        return None
+    for size in ("prof", "mid"):
+        try:
+            with open(os.path.join(ROOT, "profiles", "%s_%s.md" % (kernel, size))) as f:
+                m = re.search(r"dram_bytes_per_sample = ([0-9.]+) B", f.read())
+            if m:
+                return float(m.group(1)) * nsamp
+        except OSError:
+            pass
+    return None
 
 
 def peaks():
