@@ -456,6 +456,7 @@ class Engine {
   bool filter_dev_ = false, fcov_host_valid_ = false, invcov_valid_ = false;
   DevBuf<int> filter_flag_;
   std::vector<std::pair<long, int>> filter_tasks_;
+  std::unique_ptr<SpectrumFile> spectrum_file_;  // file_spectrum's table
   std::vector<double> filter_sigma0_;
   const std::vector<double> &fcov_host();
   const std::vector<double> &invcov_host();

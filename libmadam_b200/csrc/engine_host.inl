@@ -261,7 +261,6 @@ void Engine::init_layout(long nperiod, const long *periods) {
   if (p.pixlim_cross < 0) p.pixlim_cross = p.pixlim_map;
   if (p.pixmode_map < 0 || p.pixmode_map > 2) fail("Pixmode_map must be in range [0-2]");
   if (p.pixmode_cross < 0 || p.pixmode_cross > 4) fail("Pixmode_cross must be in range [0-4]");
-  if (!p.file_spectrum.empty()) fail("file_spectrum is not supported");
   if (nmap_ == 1) p.temperature_only = true;
   else if (p.temperature_only) nmap_ = 1;
   if (nmap_ != 1 && nmap_ != 3) fail("only nnz = 1 or nnz = 3 is supported");
@@ -1279,6 +1278,32 @@ void Engine::build_filter() {
     psdstop_[it] = (ip < dets_[d].npsd - 1) ? dets_[d].psdstarts[ip + 1] : fsp(1e30f);
   }
   filter_tasks_ = tasks;
+  spectrum_file_.reset();
+  if (!par_.file_spectrum.empty()) {
+    // read_spectrum (noise_routines.f90:505-596): the file's sigmas replace
+    // the detectors' (and their weights), and its table the PSDs; the
+    // spectra are computed on the host from it (no plateau subtraction, as
+    // get_spectrum_file returns the table's values)
+    try {
+      spectrum_file_.reset(new SpectrumFile(read_spectrum_file(par_.file_spectrum, dets_)));
+    } catch (const std::exception &e) {
+      filter_err_ = e.what();
+      return;
+    }
+    for (long d = 0; d < ndet_; ++d) {
+      Detector &det = dets_[d];
+      const double sg = spectrum_file_->sigma[d];
+      for (int ip = 0; ip < det.npsd; ++ip) {
+        det.sigmas[ip] = sg;
+        det.weights[ip] = 1 / (sg * sg);
+      }
+      if (rank() == 0) std::printf(" %s, SIGMA == %.15g\n", det.name.c_str(), sg);
+    }
+    std::fflush(stdout);
+    filter_job_ =
+        std::async(std::launch::async, [this, tasks, nh]() { filter_spectra(tasks, nh); });
+    return;
+  }
   // the device form: plateaus and tables on the host, spectra on the device
   const double fa = par_.fsample / (double)nshort_;
   const double margin = par_.radiometers ? fsp(1e-6f) : fsp(1e-3f);
@@ -1395,6 +1420,20 @@ void Engine::filter_spectra(const std::vector<std::pair<long, int>> &tasks, long
       std::vector<double> aspec(nh, 0.0), f(nof_), g(nof_), spec(nof_);
       for (int k = 0; k <= 2; ++k) {
         for (long i = 0; i < nof_; ++i) f[i] = k * fa + (double)i * fa / (double)nof_;
+        if (spectrum_file_) {
+          // get_spectrum_file (noise_routines.f90:600-634): the table's
+          // spectrum as it stands
+          spectrum_from_file(*spectrum_file_, (int)d, f.data(), spec.data(), nof_);
+          for (long i = 0; i < nof_; ++i) {
+            const double x = kPi * f[i] / fa;
+            g[i] = (x < fsp(1e-30f)) ? 1.0 : std::sin(x) * std::sin(x) / (x * x);
+          }
+          if (k == 0) aspec[0] = spec[0];
+          else aspec[0] = aspec[0] + 2 * spec[0] * g[0];
+          for (long i = 1; i < nh; ++i)
+            aspec[i] = aspec[i] + spec[i] * g[i] + spec[nof_ - i] * g[nof_ - i];
+          continue;
+        }
         // get_spectrum_interp (noise_routines.f90:638-737)
         interpolate_psd(det.psdfreqs, det.psds[ip], f.data(), spec.data(), nof_);
         double plateau;

@@ -3,6 +3,8 @@
 #include "params.h"
 
 #include <cctype>
+#include <fstream>
+#include <istream>
 #include <cmath>
 #include <cstdlib>
 #include <functional>
@@ -347,6 +349,131 @@ int psd_index_det(const Detector &d, double t) {
   for (int i = 0;; ++i) {
     if (i == d.npsd - 1) return d.psdstarts[i] > t ? -1 : i;
     if (d.psdstarts[i + 1] > t) return i;
+  }
+}
+
+}  // namespace madam
+
+namespace madam {
+
+namespace {
+
+// Fortran list-directed input: every READ starts at a new record, takes its
+// items from as many records as it needs (separated by blanks or commas,
+// strings possibly quoted) and drops the rest of the last record it used.
+class ListInput {
+ public:
+  explicit ListInput(std::istream &in) {
+    std::string line;
+    while (std::getline(in, line)) lines_.push_back(line);
+  }
+  // n items of one READ; false at the end of the file
+  bool read(size_t n, std::vector<std::string> &out) {
+    out.clear();
+    while (out.size() < n) {
+      if (rec_ >= lines_.size()) return false;
+      split(lines_[rec_++], out, n);
+    }
+    return true;
+  }
+
+ private:
+  static void split(const std::string &s, std::vector<std::string> &out, size_t n) {
+    size_t i = 0;
+    while (i < s.size() && out.size() < n) {
+      while (i < s.size() && (std::isspace((unsigned char)s[i]) || s[i] == ',')) ++i;
+      if (i >= s.size()) break;
+      std::string tok;
+      if (s[i] == '\'' || s[i] == '"') {
+        const char q = s[i++];
+        while (i < s.size()) {
+          if (s[i] == q) {
+            if (i + 1 < s.size() && s[i + 1] == q) {
+              tok += q;
+              i += 2;
+              continue;
+            }
+            ++i;
+            break;
+          }
+          tok += s[i++];
+        }
+      } else {
+        while (i < s.size() && !std::isspace((unsigned char)s[i]) && s[i] != ',') tok += s[i++];
+      }
+      out.push_back(tok);
+    }
+  }
+  std::vector<std::string> lines_;
+  size_t rec_ = 0;
+};
+
+bool to_real(std::string t, double &v) {
+  for (char &c : t)
+    if (c == 'd' || c == 'D') c = 'e';
+  char *end = nullptr;
+  v = std::strtod(t.c_str(), &end);
+  return end && *end == '\0' && !t.empty();
+}
+
+bool to_reals(const std::vector<std::string> &tok, std::vector<double> &v) {
+  v.resize(tok.size());
+  for (size_t i = 0; i < tok.size(); ++i)
+    if (!to_real(tok[i], v[i])) return false;
+  return true;
+}
+
+}  // namespace
+
+SpectrumFile read_spectrum_file(const std::string &path, const std::vector<Detector> &dets) {
+  // read_spectrum (noise_routines.f90:505-596): "nobins nodetectors", the
+  // detector names, their sigmas, then one row "freq psd_1 .. psd_n" per bin
+  std::ifstream f(path);
+  if (!f) fail("ERROR, cannot open " + path);
+  ListInput in(f);
+  std::vector<std::string> tok;
+  std::vector<double> v;
+  if (!in.read(2, tok) || !to_reals(tok, v) || v[0] < 2 || v[1] < 1 || v[0] != (long)v[0] ||
+      v[1] != (long)v[1])
+    fail("ERROR, " + path + " is not formatted correctly");
+  const long nolines = (long)v[0], nocols = (long)v[1];
+  std::vector<std::string> names;
+  if (!in.read((size_t)nocols, names))
+    fail("Failed to read detector names from spectrum file");
+  std::vector<double> sig;
+  if (!in.read((size_t)nocols, tok) || !to_reals(tok, sig))
+    fail("Failed to read detector noise levels from spectrum file");
+  std::vector<double> tab;
+  if (!in.read((size_t)(nocols + 1) * nolines, tok) || !to_reals(tok, tab))
+    fail("Failed to read the table from spectrum file");
+  SpectrumFile sf;
+  sf.logf.resize(nolines);
+  for (long l = 0; l < nolines; ++l) sf.logf[l] = std::log(tab[(size_t)l * (nocols + 1)]);
+  for (const Detector &d : dets) {
+    long icol = 0;
+    while (icol < nocols && names[icol].find(d.name) == std::string::npos) ++icol;
+    if (icol == nocols) fail("ERROR: " + d.name + " not in " + path);
+    sf.sigma.push_back(sig[icol]);
+    std::vector<double> ls(nolines);
+    for (long l = 0; l < nolines; ++l)
+      ls[l] = std::log(tab[(size_t)l * (nocols + 1) + 1 + icol]);
+    sf.logspec.push_back(std::move(ls));
+  }
+  return sf;
+}
+
+void spectrum_from_file(const SpectrumFile &sf, int idet, const double *f, double *out,
+                        long nout) {
+  const std::vector<double> &ft = sf.logf, &st = sf.logspec[idet];
+  const long nl = (long)ft.size();
+  long k = 0;
+  for (long i = 0; i < nout; ++i) {
+    const double logf = std::log(f[i]);
+    while (!(logf <= ft[k + 1] || k == nl - 2)) ++k;
+    double p = (logf - ft[k]) / (ft[k + 1] - ft[k]);
+    if (p < 0) p = 0;
+    if (p > 1) p = 1;
+    out[i] = std::exp((1.0 - p) * st[k] + p * st[k + 1]);
   }
 }
 

@@ -113,6 +113,24 @@ void interpolate_psd(const std::vector<double> &freq,
                      const std::vector<double> &psd, const double *target,
                      double *out, long nout);
 
+// The noise spectra of file_spectrum (read_spectrum, noise_routines.f90:
+// 505-596): the log frequencies of the table, and per detector (in the
+// detectors' order) the log spectrum of its column and its sigma.  Columns
+// are matched to detectors as the reference matches them: the first column
+// whose name contains the detector's name.
+struct SpectrumFile {
+  std::vector<double> logf;
+  std::vector<std::vector<double>> logspec;
+  std::vector<double> sigma;
+};
+SpectrumFile read_spectrum_file(const std::string &path, const std::vector<Detector> &dets);
+
+// get_spectrum_file (noise_routines.f90:600-634): the spectrum of one
+// detector at ascending frequencies f (log-log interpolation with the
+// reference's monotone bracket walk and its clamp to the table's ends).
+void spectrum_from_file(const SpectrumFile &sf, int idet, const double *f, double *out,
+                        long nout);
+
 // psd_index_det (noise_routines.f90:211-236); 0-based, -1 if none.
 int psd_index_det(const Detector &d, double t);
 

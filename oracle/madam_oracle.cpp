@@ -39,7 +39,8 @@
 //   src/noise_routines.f90   measure_noise_weights 65-127, interpolate_psd
 //                            130-190, psd_index 193-208, psd_index_det
 //                            211-236, init_filter 242-292, build_filter
-//                            367-739, trim_interval 764-813,
+//                            367-739 (read_spectrum 505-596,
+//                            get_spectrum_file 600-634), trim_interval 764-813,
 //                            convolve_interval 816-857, convolve_pp 861-913,
 //                            construct_preconditioner 920-1153,
 //                            preconditioning_band 1159-1256,
@@ -792,6 +793,11 @@ struct State {
   long nof = -1;
   long npsdtot = 0;
   std::vector<double> fcov;  // (nof/2+1) x npsdtot, real valued
+  // file_spectrum (read_spectrum): log frequencies and, per detector, the
+  // log spectrum of its column
+  bool kread_file = false;
+  std::vector<double> ftable;
+  std::vector<std::vector<double>> spectrum_table;
   std::vector<int> psddet;
   std::vector<double> psdstart, psdstop;
   std::vector<double> fprecond, invcov;
@@ -1050,7 +1056,6 @@ void init_parameters(State &S) {
     fail("Pixmode_map must be in range [0-2]");
   if (p.pixmode_cross < 0 || p.pixmode_cross > 4)
     fail("Pixmode_cross must be in range [0-4]");
-  if (!p.file_spectrum.empty()) fail("file_spectrum is not supported");
   if (S.nmap == 1) p.temperature_only = true;
   else if (p.temperature_only) S.nmap = 1;
   if (S.nmap != 1 && S.nmap != 3) fail("only nnz = 1 or nnz = 3 is supported");
@@ -1241,7 +1246,116 @@ void init_filter(State &S) {
   S.fft = new RealFFT(nof);
 }
 
-// build_filter (noise_routines.f90:367-739) with get_spectrum_interp
+extern int g_rank;
+
+// Fortran list-directed READ: a READ starts at a new record, takes items
+// separated by blanks or commas (strings may be quoted) across as many
+// records as it needs, and drops the rest of its last record.
+struct FortranList {
+  std::vector<std::string> rec;
+  size_t next = 0;
+  bool items(size_t n, std::vector<std::string> &out) {
+    out.clear();
+    while (out.size() < n) {
+      if (next >= rec.size()) return false;
+      const std::string &s = rec[next++];
+      size_t i = 0;
+      while (out.size() < n) {
+        while (i < s.size() && (isspace((unsigned char)s[i]) || s[i] == ',')) ++i;
+        if (i >= s.size()) break;
+        std::string t;
+        if (s[i] == '\'' || s[i] == '"') {
+          char q = s[i++];
+          for (; i < s.size(); ++i) {
+            if (s[i] != q) { t += s[i]; continue; }
+            if (i + 1 < s.size() && s[i + 1] == q) { t += q; ++i; continue; }
+            ++i;
+            break;
+          }
+        } else {
+          while (i < s.size() && !isspace((unsigned char)s[i]) && s[i] != ',') t += s[i++];
+        }
+        out.push_back(t);
+      }
+    }
+    return true;
+  }
+};
+
+static bool fortran_reals(const std::vector<std::string> &t, std::vector<double> &v) {
+  v.assign(t.size(), 0.0);
+  for (size_t i = 0; i < t.size(); ++i) {
+    std::string x = t[i];
+    for (char &c : x) if (c == 'd' || c == 'D') c = 'e';
+    char *e = nullptr;
+    v[i] = strtod(x.c_str(), &e);
+    if (x.empty() || *e) return false;
+  }
+  return true;
+}
+
+// read_spectrum (noise_routines.f90:505-596)
+void read_spectrum(State &S) {
+  const std::string &fn = S.par.file_spectrum;
+  FILE *fp = fopen(fn.c_str(), "r");
+  if (!fp) fail("ERROR, cannot open " + fn);
+  FortranList in;
+  std::string line;
+  int c;
+  while ((c = fgetc(fp)) != EOF) {
+    if (c == '\n') { in.rec.push_back(line); line.clear(); }
+    else line += (char)c;
+  }
+  if (!line.empty()) in.rec.push_back(line);
+  fclose(fp);
+  std::vector<std::string> t, names;
+  std::vector<double> hd, sigmas, dtemp;
+  if (!in.items(2, t) || !fortran_reals(t, hd) || hd[0] < 2 || hd[1] < 1 ||
+      hd[0] != (long)hd[0] || hd[1] != (long)hd[1])
+    fail("ERROR, " + fn + " is not formatted correctly");
+  long nolines = (long)hd[0], nocols = (long)hd[1];
+  if (!in.items(nocols, names)) fail("Failed to read detector names from spectrum file");
+  if (!in.items(nocols, t) || !fortran_reals(t, sigmas))
+    fail("Failed to read detector noise levels from spectrum file");
+  if (!in.items((size_t)(nocols + 1) * nolines, t) || !fortran_reals(t, dtemp))
+    fail("Failed to read the table from spectrum file");
+  S.ftable.assign(nolines, 0.0);
+  for (long l = 0; l < nolines; ++l) S.ftable[l] = log(dtemp[l * (nocols + 1)]);
+  S.spectrum_table.assign(S.ndet, std::vector<double>(nolines));
+  for (long idet = 0; idet < S.ndet; ++idet) {
+    Detector &d = S.dets[idet];
+    long icol = 0;
+    for (;; ++icol) {
+      if (icol >= nocols) fail("ERROR: " + d.name + " not in " + fn);
+      if (names[icol].find(d.name) != std::string::npos) break;
+    }
+    for (int ip = 0; ip < d.npsd; ++ip) {
+      d.sigmas[ip] = sigmas[icol];
+      d.weights[ip] = 1 / (sigmas[icol] * sigmas[icol]);
+    }
+    if (g_rank == 0) printf(" %s, SIGMA == %.15g\n", d.name.c_str(), sigmas[icol]);
+    for (long l = 0; l < nolines; ++l)
+      S.spectrum_table[idet][l] = log(dtemp[l * (nocols + 1) + 1 + icol]);
+  }
+  fflush(stdout);
+}
+
+// get_spectrum_file (noise_routines.f90:600-634)
+void get_spectrum_file(const State &S, long idet, const double *f, double *spectrum, long nof) {
+  const std::vector<double> &ft = S.ftable, &tab = S.spectrum_table[idet];
+  long nolines = (long)ft.size(), k = 0;
+  for (long i = 0; i < nof; ++i) {
+    double logf = log(f[i]);
+    while (!(logf <= ft[k + 1] || k == nolines - 2)) ++k;
+    double p = (logf - ft[k]) / (ft[k + 1] - ft[k]);
+    if (p < 0) p = 0;
+    if (p > 1) p = 1;
+    spectrum[i] = exp((1.0 - p) * tab[k] + p * tab[k + 1]);
+  }
+}
+
+// build_filter (noise_routines.f90:367-739) with get_spectrum_interp, or
+// get_spectrum_file when file_spectrum names the noise spectra
 void build_filter(State &S) {
   if (!S.par.kfilter) return;
   Params &p = S.par;
@@ -1252,6 +1366,8 @@ void build_filter(State &S) {
   S.psddet.assign(S.npsdtot, 0);
   S.psdstart.assign(S.npsdtot, 0);
   S.psdstop.assign(S.npsdtot, 0);
+  S.kread_file = !p.file_spectrum.empty();
+  if (S.kread_file) read_spectrum(S);
   double fa = p.fsample / (double)S.nshort;
   std::vector<std::pair<long, int>> tasks;
   for (long d = 0; d < S.ndet; ++d) {
@@ -1274,6 +1390,18 @@ void build_filter(State &S) {
       for (int k = 0; k <= 2; ++k) {
         for (long i = 0; i < nof; ++i)
           f[i] = k * fa + (double)i * fa / (double)nof;
+        if (S.kread_file) {
+          get_spectrum_file(S, d, f.data(), spec.data(), nof);
+          for (long i = 0; i < nof; ++i) {
+            double x = kPi * f[i] / fa;
+            g[i] = (x < kTiny30) ? 1.0 : std::sin(x) * std::sin(x) / (x * x);
+          }
+          if (k == 0) aspec[0] = spec[0];
+          else aspec[0] = aspec[0] + 2 * spec[0] * g[0];
+          for (long i = 1; i < nh; ++i)
+            aspec[i] = aspec[i] + spec[i] * g[i] + spec[nof - i] * g[nof - i];
+          continue;
+        }
         // get_spectrum_interp
         interpolate_psd(det.psdfreqs, det.psds[ip], f.data(), spec.data(), nof);
         double plateau;

@@ -52,3 +52,21 @@ def test_psd_with_zero_bins_takes_the_fill(W):
     d["psdvals"] = pv.reshape(-1)
     ro, rp, _, _ = run_both(W, d)
     _fcov_check(W, 3, ro, rp)
+
+
+def test_file_spectrum_matches_oracle(W, tmp_path):
+    # read_spectrum / get_spectrum_file (noise_routines.f90:505-634): the
+    # file's spectra and sigmas (columns in another order than the detectors)
+    d = syn.to_numpy(syn.generate(syn.small_config(seed=83)))
+    ndet = len(d["dets"])
+    freq = np.logspace(-4, np.log10(d["pars"]["fsample"] / 2), 80)
+    order = list(range(ndet))[::-1]
+    with open(tmp_path / "spec.txt", "w") as f:
+        f.write("%d %d\n" % (len(freq), ndet))
+        f.write(" ".join(d["dets"][j] for j in order) + "\n")
+        f.write(" ".join("%.17e" % (1e-3 * (1 + 0.2 * j)) for j in order) + "\n")
+        for v in freq:
+            f.write("%.17e " % v + " ".join("%.17e" % (3e-6 * (1 + (v / (0.04 + 0.01 * j)) ** -1.5))
+                                          for j in order) + "\n")
+    ro, rp, _, _ = run_both(W, d, dict(file_spectrum=str(tmp_path / "spec.txt")))
+    _fcov_check(W, 3, ro, rp)
