@@ -272,6 +272,12 @@ class Engine {
   DevBuf<double> binb_, mapb_, binmapb_; // [R][nloc][nmap]
   DevBuf<double> partb_, scalb_;         // [R][3][kRedBlocks], [R][S_NSCAL]
   DevBuf<int> actb_, actu_;              // active / reliably updated right-hand sides
+  // reliable updates of several right-hand sides at once: their A x through
+  // the float64 batched projections on the pixel-sorted samples
+  DevBuf<double> xsb_, pwsb_, apsb_, partsb_, scalsb_;
+  DevBuf<int> actsb_;
+  void true_residual_batch(const std::vector<long> &upd);
+  long nrhs_alt_ = 0;  // the batch size while true_residual_batch runs its own
   std::vector<int> act_host_;
   std::vector<double> noiter_b_, rrinit_b_, rrfinal_b_;
   // band factor tables replicated per right-hand side (offsets k0 + r nb)

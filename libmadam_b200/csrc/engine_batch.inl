@@ -338,6 +338,70 @@ void Engine::apply_A_batch() {
                scalb_.get(), 1, 0, actb_.get());
 }
 
+// The true residuals r_k = y_k - A aa_k of the right-hand sides in upd (the
+// FP32-TOD batch's reliable updates) in one float64 pass: their aa rows go
+// through apply_A_batch as a batch of their own, with the pixel-sorted
+// samples in the scatter and float64 projections (the arithmetic of the
+// single solve's exact operator, apply_A_exact), instead of one single-RHS
+// operator per right-hand side.
+template <class B>
+static void swap_buf(B &a, B &b) {
+  std::swap(a.p, b.p);
+  std::swap(a.n, b.n);
+}
+
+void Engine::true_residual_batch(const std::vector<long> &upd) {
+  const long long nb = (long long)ndet_ * noba_short_;
+  const long ns = (long)upd.size();
+  xsb_.alloc((size_t)ns * nb);
+  pwsb_.alloc((size_t)ns * nb);
+  apsb_.alloc((size_t)ns * nb);
+  partsb_.alloc((size_t)ns * 3 * kRedBlocks);
+  scalsb_.alloc((size_t)ns * S_NSCAL);
+  scalsb_.zero(st_);
+  actsb_.alloc(ns);
+  std::vector<int> one(ns, 1);
+  MADAM_CUDA(cudaMemcpyAsync(actsb_.get(), one.data(), ns * sizeof(int), cudaMemcpyHostToDevice,
+                             st_));
+  for (long i = 0; i < ns; ++i) {
+    MADAM_CUDA(cudaMemcpyAsync(xsb_.get() + i * nb, aab_.get() + upd[i] * nb,
+                               nb * sizeof(double), cudaMemcpyDeviceToDevice, st_));
+    MADAM_LAUNCH(k_mul, grid_for(nb), 256, 0, st_, pwsb_.get() + i * nb, xsb_.get() + i * nb,
+                 bw_.get(), nb);
+  }
+  auto swap_all = [&]() {
+    swap_buf(pb_, xsb_);
+    swap_buf(pwb_, pwsb_);
+    swap_buf(apb_, apsb_);
+    swap_buf(partb_, partsb_);
+    swap_buf(scalb_, scalsb_);
+    swap_buf(actb_, actsb_);
+    if (have_xcsr_) swap_csr();
+    std::swap(nrhs_, nrhs_alt_);
+  };
+  nrhs_alt_ = ns;
+  const bool f32 = fp32_, timed = batch_timed_;
+  fp32_ = false;
+  batch_timed_ = false;
+  swap_all();
+  try {
+    apply_A_batch();
+  } catch (...) {
+    swap_all();
+    fp32_ = f32;
+    batch_timed_ = timed;
+    throw;
+  }
+  swap_all();
+  fp32_ = f32;
+  batch_timed_ = timed;
+  for (long i = 0; i < ns; ++i) {
+    MADAM_LAUNCH(k_residual, grid_for(nb), 256, 0, st_, rb_.get() + upd[i] * nb,
+                 yb_.get() + upd[i] * nb, apsb_.get() + i * nb, nb);
+    ++n_reliable_;
+  }
+}
+
 void Engine::iterate_batch() {
   // iterate_a (smadam_routines.f90:677-983) for every right-hand side
   const double t0 = now_ms();
@@ -436,8 +500,13 @@ void Engine::iterate_batch() {
         // single-solve preconditioner on their slices), and rz, rz2 and rr
         // of those alone (mode 3 keeps rz_old)
         std::vector<int> mask(R, 0);
+        if (upd.size() >= 4 && ngather_chunks_ > 0) {
+          true_residual_batch(upd);
+        } else {
+          for (long k : upd)
+            true_residual(aab_.get() + k * nb, yb_.get() + k * nb, rb_.get() + k * nb);
+        }
         for (long k : upd) {
-          true_residual(aab_.get() + k * nb, yb_.get() + k * nb, rb_.get() + k * nb);
           apply_preconditioner(rb_.get() + k * nb, zb_.get() + k * nb);
           mask[k] = 1;
         }
