@@ -21,6 +21,8 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
+#include <tuple>
 #include <omp.h>
 
 #include "engine.h"

@@ -88,6 +88,10 @@ struct DevBuf {
   void zero(cudaStream_t s) {
     if (n) MADAM_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
   }
+  // at least count elements (kept when already as large)
+  void reserve(size_t count) {
+    if (count > n) alloc(count);
+  }
   T *get() const { return p; }
 };
 
@@ -264,6 +268,14 @@ class Engine {
   void project_group_T(long r0, int nr);
   template <int G, class T>
   void project_group_T2(long r0, int nr);
+  // Launch-shape tuner of the batched projections: the grid of a kernel is
+  // chosen once per (kernel, work items, right-hand-side width) by timing
+  // one launch at each candidate (one to four waves of resident CTAs, and
+  // the reduction grid) and kept for the process; a tuning pass runs only
+  // while tune_batch_ is set (before the timed iterations).
+  template <class L>
+  unsigned tuned_grid(const void *kern, int key, long long items, int GW, L launch);
+  bool tune_batch_ = false;
   DevBuf<double> pwT_, lmapT_, scatpT_, apnT_;  // right-hand-side-minor copies
   DevBuf<float> pwTf_, lmapTf_;                 // their float32 forms (FP32-TOD batch)
   long nrhs_ = 0;                        // right-hand sides of the last batch

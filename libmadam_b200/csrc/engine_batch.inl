@@ -148,6 +148,59 @@ void Engine::apply_preconditioner_batch(const double *r, double *z) {
   }
 }
 
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<int, long long, int>, unsigned> g_tuned;  // (kernel, items, GW) -> grid
+}  // namespace
+
+template <class L>
+unsigned Engine::tuned_grid(const void *kern, int key, long long items, int GW, L launch) {
+  const auto id = std::make_tuple(key, items, GW);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(id);
+    if (it != g_tuned.end()) {
+      launch(it->second);
+      return it->second;
+    }
+  }
+  if (!tune_batch_) {
+    launch((unsigned)kRedBlocks);
+    return (unsigned)kRedBlocks;
+  }
+  int per_sm = 0, dev = 0, nsm = 0;
+  MADAM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0));
+  MADAM_CUDA(cudaGetDevice(&dev));
+  MADAM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  std::vector<unsigned> cand{(unsigned)kRedBlocks};
+  for (int w = 1; w <= 4 && per_sm > 0; ++w) {
+    const unsigned g = (unsigned)(w * per_sm * nsm);
+    if (std::find(cand.begin(), cand.end(), g) == cand.end()) cand.push_back(g);
+  }
+  launch(cand[0]);  // warm: caches and the kernel's first load
+  float best = 1e30f;
+  unsigned best_g = cand[0];
+  for (unsigned g : cand) {
+    MADAM_CUDA(cudaEventRecord(ev_[0], st_));
+    launch(g);
+    MADAM_CUDA(cudaEventRecord(ev_[1], st_));
+    MADAM_CUDA(cudaEventSynchronize(ev_[1]));
+    float ms = 0;
+    MADAM_CUDA(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
+    if (ms < best) {
+      best = ms;
+      best_g = g;
+    }
+  }
+  if (best_g != cand.back()) launch(best_g);  // the outputs of the chosen shape last
+  if (g_trace_alloc)
+    std::fprintf(stderr, "madam_b200 trace: tuned kernel %d (GW %d): grid %u, %.3f ms\n", key,
+                 GW, best_g, best);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tuned[id] = best_g;
+  return best_g;
+}
+
 template <int G>
 void Engine::project_group_T(long r0, int nr) {
   if (fp32_) project_group_T2<G, float>(r0, nr);
@@ -163,18 +216,20 @@ void Engine::project_group_T2(long r0, int nr) {
   const long long nb = (long long)ndet_ * noba_short_;
   const long long ncross = std::max<long>(1, nloc_cross_);
   const bool f32 = std::is_same<T, float>::value;
+  // grow-only: the float32 and float64 passes (reliable updates) and the
+  // 32- and 64-wide groups share these buffers
   T *pwT;
   if (f32) {
-    pwTf_.alloc((size_t)nb * GW);
+    pwTf_.reserve((size_t)nb * GW);
     pwT = (T *)pwTf_.get();
-    lmapTf_.alloc((size_t)ncross * nmap_ * GW);
+    lmapTf_.reserve((size_t)ncross * nmap_ * GW);
   } else {
-    pwT_.alloc((size_t)nb * GW);
+    pwT_.reserve((size_t)nb * GW);
     pwT = (T *)pwT_.get();
   }
-  lmapT_.alloc((size_t)ncross * nmap_ * GW);
-  scatpT_.alloc((size_t)std::max<size_t>(1, scatter_partial_.n / nmap_) * nmap_ * GW);
-  apnT_.alloc((size_t)nb * GW);
+  lmapT_.reserve((size_t)ncross * nmap_ * GW);
+  scatpT_.reserve((size_t)std::max<size_t>(1, scatter_partial_.n / nmap_) * nmap_ * GW);
+  apnT_.reserve((size_t)nb * GW);
   const unsigned tb = (unsigned)std::min<long long>(4736, (nb + 31) / 32);
   if (batch_timed_) MADAM_CUDA(cudaEventRecord(ev_[2], st_));
   MADAM_LAUNCH((k_transpose_rhs<G, T>), dim3(tb, G), 256, 0, st_, pwb_.get(), nb, (int)r0, nr,
@@ -183,13 +238,17 @@ void Engine::project_group_T2(long r0, int nr) {
   if (nloc_cross_ > 0 && nscatter_chunks_ > 0 && f32) {
     // FP32-TOD form: all GW right-hand sides in one pass, entry-order sums
     if (nmap_ == 3)
-      MADAM_LAUNCH((k_scatter_T_seq<3, GW>), kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
-                   nscatter_chunks_, sp4_.get(), sp2_.get(), (const float *)pwT, lmapT_.get(),
-                   scatpT_.get());
+      tuned_grid((const void *)k_scatter_T_seq<3, GW>, 1, nscatter_chunks_, GW, [&](unsigned g) {
+        MADAM_LAUNCH((k_scatter_T_seq<3, GW>), g, 256, 0, st_, scatter_chunks_.get(),
+                     nscatter_chunks_, sp4_.get(), sp2_.get(), (const float *)pwT, lmapT_.get(),
+                     scatpT_.get());
+      });
     else
-      MADAM_LAUNCH((k_scatter_T_seq<1, GW>), kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
-                   nscatter_chunks_, sp4_.get(), sp2_.get(), (const float *)pwT, lmapT_.get(),
-                   scatpT_.get());
+      tuned_grid((const void *)k_scatter_T_seq<1, GW>, 2, nscatter_chunks_, GW, [&](unsigned g) {
+        MADAM_LAUNCH((k_scatter_T_seq<1, GW>), g, 256, 0, st_, scatter_chunks_.get(),
+                     nscatter_chunks_, sp4_.get(), sp2_.get(), (const float *)pwT, lmapT_.get(),
+                     scatpT_.get());
+      });
   } else if (nloc_cross_ > 0 && nscatter_chunks_ > 0) {
     // one launch per 32 right-hand sides (fewer registers, more warps)
     for (int g0 = 0; g0 < GW; g0 += 32) {
@@ -227,12 +286,18 @@ void Engine::project_group_T2(long r0, int nr) {
   if (f32 && use_pairs_ && nmap_ == 3 && npair_chunks_ > 0) {
     // FP32-TOD form: over the pointing pairs (fewer map rows to read); the
     // chunks cover every baseline, so apnT is written for all of them
-    MADAM_LAUNCH(k_gather_T_pairs<G>, kRedBlocks, 256, 0, st_, pair_chunks_.get(),
-                 npair_chunks_, gp4_.get(), poff_.get(), lmapTf_.get(), apnT_.get());
+    tuned_grid((const void *)k_gather_T_pairs<G>, 3, npair_chunks_, GW, [&](unsigned g) {
+      MADAM_LAUNCH(k_gather_T_pairs<G>, g, 256, 0, st_, pair_chunks_.get(), npair_chunks_,
+                   gp4_.get(), poff_.get(), lmapTf_.get(), apnT_.get());
+    });
   } else if (nmap_ == 3)
-    MADAM_LAUNCH((k_gather_T<3, G, T>), kRedBlocks, 256, 0, st_, gather_chunks_.get(),
-                 ngather_chunks_, point4_.get(), pixc_.get(), bstart_d_.get(), noba_short_,
-                 nsamp_, mT, (int)ndeg_shift_, (int)nloc_, apnT_.get());
+    tuned_grid((const void *)k_gather_T<3, G, T>, f32 ? 4 : 5, ngather_chunks_, GW,
+               [&](unsigned g) {
+                 MADAM_LAUNCH((k_gather_T<3, G, T>), g, 256, 0, st_, gather_chunks_.get(),
+                              ngather_chunks_, point4_.get(), pixc_.get(), bstart_d_.get(),
+                              noba_short_, nsamp_, mT, (int)ndeg_shift_, (int)nloc_,
+                              apnT_.get());
+               });
   else
     MADAM_LAUNCH((k_gather_T<1, G, T>), kRedBlocks, 256, 0, st_, gather_chunks_.get(),
                  ngather_chunks_, point4_.get(), pixc_.get(), bstart_d_.get(), noba_short_,
@@ -353,13 +418,13 @@ static void swap_buf(B &a, B &b) {
 void Engine::true_residual_batch(const std::vector<long> &upd) {
   const long long nb = (long long)ndet_ * noba_short_;
   const long ns = (long)upd.size();
-  xsb_.alloc((size_t)ns * nb);
-  pwsb_.alloc((size_t)ns * nb);
-  apsb_.alloc((size_t)ns * nb);
-  partsb_.alloc((size_t)ns * 3 * kRedBlocks);
-  scalsb_.alloc((size_t)ns * S_NSCAL);
+  xsb_.reserve((size_t)ns * nb);
+  pwsb_.reserve((size_t)ns * nb);
+  apsb_.reserve((size_t)ns * nb);
+  partsb_.reserve((size_t)ns * 3 * kRedBlocks);
+  scalsb_.reserve((size_t)ns * S_NSCAL);
   scalsb_.zero(st_);
-  actsb_.alloc(ns);
+  actsb_.reserve(ns);
   std::vector<int> one(ns, 1);
   MADAM_CUDA(cudaMemcpyAsync(actsb_.get(), one.data(), ns * sizeof(int), cudaMemcpyHostToDevice,
                              st_));
@@ -404,7 +469,7 @@ void Engine::true_residual_batch(const std::vector<long> &upd) {
 
 void Engine::iterate_batch() {
   // iterate_a (smadam_routines.f90:677-983) for every right-hand side
-  const double t0 = now_ms();
+  double t0 = now_ms();
   const long long nb = (long long)ndet_ * noba_short_;
   const long long nt = nb * nrhs_;
   const long R = nrhs_;
@@ -453,6 +518,37 @@ void Engine::iterate_batch() {
     nact += act_host_[k];
   }
   upload_act();
+  // launch shapes of the batched projections, tuned once per shape on this
+  // batch's data before the iterations (apply_A_batch's outputs are
+  // overwritten by the first iteration); counted in the setup time
+  if (ngather_chunks_ > 0) {
+    const double tt = now_ms();
+    tune_batch_ = true;
+    try {
+      apply_A_batch();
+    } catch (...) {
+      tune_batch_ = false;
+      throw;
+    }
+    tune_batch_ = false;
+    if (fp32_) {
+      // the float64 pass of the reliable updates: its buffers now, so that
+      // the iterations do not allocate
+      const long long ncr = std::max<long>(1, nloc_cross_);
+      const size_t xpart = have_xcsr_ ? xscatter_partial_.n : scatter_partial_.n;
+      for (auto *b : {&xsb_, &pwsb_, &apsb_}) b->reserve((size_t)R * nb);
+      partsb_.reserve((size_t)R * 3 * kRedBlocks);
+      scalsb_.reserve((size_t)R * S_NSCAL);
+      actsb_.reserve(R);
+      pwT_.reserve((size_t)nb * 64);
+      lmapT_.reserve((size_t)ncr * nmap_ * 64);
+      scatpT_.reserve(std::max<size_t>(1, xpart / nmap_) * nmap_ * 64);
+      apnT_.reserve((size_t)nb * 64);
+    }
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    timings.setup_ms += now_ms() - tt;
+    t0 += now_ms() - tt;
+  }
   // FP32-TOD batch: reliable updates per right-hand side (see iterate())
   const bool refine_b = fp32_;
   std::vector<double> rr_true(rrinit_b_);
@@ -500,15 +596,25 @@ void Engine::iterate_batch() {
         // single-solve preconditioner on their slices), and rz, rz2 and rr
         // of those alone (mode 3 keeps rz_old)
         std::vector<int> mask(R, 0);
+        const double ta = now_ms();
         if (upd.size() >= 4 && ngather_chunks_ > 0) {
           true_residual_batch(upd);
         } else {
           for (long k : upd)
             true_residual(aab_.get() + k * nb, yb_.get() + k * nb, rb_.get() + k * nb);
         }
+        if (g_trace_alloc) MADAM_CUDA(cudaStreamSynchronize(st_));
+        const double tb = now_ms();
         for (long k : upd) {
           apply_preconditioner(rb_.get() + k * nb, zb_.get() + k * nb);
           mask[k] = 1;
+        }
+        if (g_trace_alloc) {
+          MADAM_CUDA(cudaStreamSynchronize(st_));
+          std::fprintf(stderr,
+                       "madam_b200 trace: iteration %ld reliable update of %zu: residual "
+                       "%.2f ms, preconditioner %.2f ms\n",
+                       istep, upd.size(), tb - ta, now_ms() - tb);
         }
         MADAM_CUDA(cudaMemcpyAsync(actu_.get(), mask.data(), R * sizeof(int),
                                    cudaMemcpyHostToDevice, st_));
