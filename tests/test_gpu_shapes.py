@@ -21,7 +21,9 @@ shapes at sizes the oracle solves in seconds:
 
 Tolerances as in the other parity tests, per pixel (parity.close): float64
 maps and baselines 1e-6, float32-TOD 1e-4 (both sides solved to
-parity.CONVERGED_CGLIMIT); hits and masks bit-exact.
+parity.CONVERGED_CGLIMIT, baselines and I map up to the solve's
+undetermined common offset, parity.close_modulo_offset); hits and masks
+bit-exact.
 """
 import numpy as np
 import pytest
@@ -70,15 +72,20 @@ def _oracle(d, pars):
     return r
 
 
-def _check(rp, ro, nmap, rtol, bin_rtol, floor=parity.FLOOR):
+def _check(rp, ro, nmap, rtol, bin_rtol, floor=parity.FLOOR, offset_free=False):
+    # offset_free: the float32-TOD forms, compared up to the solve's
+    # undetermined common offset of baselines and I map
+    # (parity.close_modulo_offset)
     np.testing.assert_array_equal(rp["hits"], ro["hits"])
     np.testing.assert_array_equal(rp["mask"], ro["mask"])
     for c in range(nmap):
         parity.close(rp["binmap"].reshape(-1, nmap)[:, c], ro["binmap"].reshape(-1, nmap)[:, c],
                      bin_rtol, "binmap[%d]" % c)
-        parity.close(rp["map"].reshape(-1, nmap)[:, c], ro["map"].reshape(-1, nmap)[:, c],
-                     rtol, "map[%d]" % c, floor)
-    parity.close(rp["aa"], ro["aa"], rtol, "aa", floor)
+        cmp = parity.close_modulo_offset if (offset_free and c == 0) else parity.close
+        cmp(rp["map"].reshape(-1, nmap)[:, c], ro["map"].reshape(-1, nmap)[:, c],
+            rtol, "map[%d]" % c, floor)
+    (parity.close_modulo_offset if offset_free else parity.close)(rp["aa"], ro["aa"], rtol, "aa",
+                                                                  floor)
 
 
 def test_plain_float64_workload_shape(W):
@@ -110,7 +117,7 @@ def test_precision_form_workload_shape(W):
     sc = W.scalars()
     assert sc["fp32"] == 1.0 and sc["pairs"] > 0
     np.testing.assert_array_equal(dp["pixels"], ro["pixels"])
-    _check(rp, ro, 3, FP32_RTOL, BIN_RTOL)
+    _check(rp, ro, 3, FP32_RTOL, BIN_RTOL, offset_free=True)
     assert sc["noiter"] <= 2.5 * ro["scalars"]["noiter"] + 3  # converges, in more steps
 
 
@@ -161,10 +168,14 @@ def test_batched_monte_carlo_workload_shape(W):
                 assert its[r] <= 2.5 * ref[r]["noiter"] + 3  # converges, in more steps
             else:
                 assert its[r] == ref[r]["noiter"]
+            # the float32 batch up to the solve's undetermined common offset
+            # of baselines and I map (parity.close_modulo_offset)
+            off = parity.close_modulo_offset if fp32 else parity.close
             for c in range(3):
-                parity.close(maps[r][:, c], ref[r]["map"].reshape(-1, 3)[:, c], rtol,
-                             "map_batch[%d][%d]" % (r, c))
-            parity.close(aas[r], ref[r]["aa"], rtol, "aa_batch[%d]" % r)
+                (off if c == 0 else parity.close)(maps[r][:, c],
+                                                  ref[r]["map"].reshape(-1, 3)[:, c], rtol,
+                                                  "map_batch[%d][%d]" % (r, c))
+            off(aas[r], ref[r]["aa"], rtol, "aa_batch[%d]" % r)
     W.clear_caches()
 
 
