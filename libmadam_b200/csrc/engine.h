@@ -276,6 +276,7 @@ class Engine {
   template <class L>
   unsigned tuned_grid(const void *kern, int key, long long items, int GW, L launch);
   bool tune_batch_ = false;
+  bool tuned(int key, long long items, int GW);  // a shape tuned_grid has already timed
   DevBuf<double> pwT_, lmapT_, scatpT_, apnT_;  // right-hand-side-minor copies
   DevBuf<float> pwTf_, lmapTf_;                 // their float32 forms (FP32-TOD batch)
   long nrhs_ = 0;                        // right-hand sides of the last batch

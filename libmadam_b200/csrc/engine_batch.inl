@@ -153,6 +153,11 @@ std::mutex g_tune_mu;
 std::map<std::tuple<int, long long, int>, unsigned> g_tuned;  // (kernel, items, GW) -> grid
 }  // namespace
 
+bool Engine::tuned(int key, long long items, int GW) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  return g_tuned.count(std::make_tuple(key, items, GW)) > 0;
+}
+
 template <class L>
 unsigned Engine::tuned_grid(const void *kern, int key, long long items, int GW, L launch) {
   const auto id = std::make_tuple(key, items, GW);

@@ -2029,17 +2029,23 @@ void Engine::apply_A(const double *p, const double *pw, double *ap, bool timed) 
   if (timed) MADAM_CUDA(cudaEventRecord(ev_[0], st_));
   if (nscatter_chunks_ == 0 && nloc_cross_ > 0) lmap_.zero(st_);  // a rank with no samples
   if (nloc_cross_ > 0 && nscatter_chunks_ > 0) {
+    // the grid from the launch-shape tuner (tuned_grid; the chunks' sums do
+    // not depend on it)
     if (nmap_ == 3) {
-      MADAM_LAUNCH(k_scatter_chunks<3>, kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
-                   nscatter_chunks_, sp4_.get(), sp2_.get(), pw, lmap_.get(),
-                   scatter_partial_.get());
+      tuned_grid((const void *)k_scatter_chunks<3>, 10, nscatter_chunks_, 1, [&](unsigned g) {
+        MADAM_LAUNCH(k_scatter_chunks<3>, g, 256, 0, st_, scatter_chunks_.get(),
+                     nscatter_chunks_, sp4_.get(), sp2_.get(), pw, lmap_.get(),
+                     scatter_partial_.get());
+      });
       if (nscatter_multi_ > 0)
         MADAM_LAUNCH(k_scatter_combine<3>, grid_for(nscatter_multi_), 256, 0, st_,
                      scatter_multi_.get(), nscatter_multi_, scatter_partial_.get(), lmap_.get());
     } else {
-      MADAM_LAUNCH(k_scatter_chunks<1>, kRedBlocks, 256, 0, st_, scatter_chunks_.get(),
-                   nscatter_chunks_, sp4_.get(), sp2_.get(), pw, lmap_.get(),
-                   scatter_partial_.get());
+      tuned_grid((const void *)k_scatter_chunks<1>, 11, nscatter_chunks_, 1, [&](unsigned g) {
+        MADAM_LAUNCH(k_scatter_chunks<1>, g, 256, 0, st_, scatter_chunks_.get(),
+                     nscatter_chunks_, sp4_.get(), sp2_.get(), pw, lmap_.get(),
+                     scatter_partial_.get());
+      });
       if (nscatter_multi_ > 0)
         MADAM_LAUNCH(k_scatter_combine<1>, grid_for(nscatter_multi_), 256, 0, st_,
                      scatter_multi_.get(), nscatter_multi_, scatter_partial_.get(), lmap_.get());
@@ -2514,7 +2520,7 @@ void Engine::apply_preconditioner(const double *r, double *z) {
 void Engine::iterate() {
   // iterate_a (smadam_routines.f90:677-983); nb counts the CG vectors'
   // amplitudes (basis_order + 1 per baseline)
-  const double t0 = now_ms();
+  double t0 = now_ms();
   const long long nb = (long long)ndet_ * noba_short_ * nbasis_;
   const double *bwv = bw_.get();
   const uint8_t *rmv = rmask_.get();
@@ -2557,6 +2563,23 @@ void Engine::iterate() {
   long istep = 0;
   float tm[4];
   pcg_reset();
+  if (nloc_cross_ > 0 && nscatter_chunks_ > 0 && !sharded() &&
+      !tuned(nmap_ == 3 ? 10 : 11, nscatter_chunks_, 1)) {
+    // the scatter's launch shape, tuned once per shape (a pass of A p whose
+    // outputs the first iteration overwrites); counted in the setup time
+    const double tt = now_ms();
+    tune_batch_ = true;
+    try {
+      apply_A(p_.get(), pw_.get(), ap_.get(), false);
+    } catch (...) {
+      tune_batch_ = false;
+      throw;
+    }
+    tune_batch_ = false;
+    MADAM_CUDA(cudaStreamSynchronize(st_));
+    timings.setup_ms += now_ms() - tt;
+    t0 += now_ms() - tt;
+  }
   while (istep < par_.iter_max) {
     ++istep;
     apply_A(p_.get(), pw_.get(), ap_.get(), true);
