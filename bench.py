@@ -349,6 +349,12 @@ def run_mc(args, world, rank, local):
     pp_aa = max(pp(a32[r], a64r[r]) for r in range(R))
     pp_map3 = [max(pp(m32[r][:, c], m64[r][:, c], parity.FLOOR) for r in range(R))
                for c in range(3)]
+    # the same with the solve's undetermined common offset of baselines and
+    # I map removed (the destriping system is singular along it)
+    ppo = lambda a, b: parity.per_pixel_error_modulo_offset(a, b, parity.FP32_FLOOR)[0]
+    pp_map_off = [max((ppo if c == 0 else pp)(m32[r][:, c], m64[r][:, c]) for r in range(R))
+                  for c in range(3)]
+    pp_aa_off = max(ppo(a32[r], a64r[r]) for r in range(R))
     n_rel = int(W.scalars()["reliable_updates"])
     line = None
     if rank == 0:
@@ -376,6 +382,8 @@ def run_mc(args, world, rank, local):
                 "fp32_vs_fp64": {"map_rel_err_iqu": err_map, "baseline_rel_err": err_aa,
                                  "map_per_pixel_err_iqu": pp_map,
                                  "baseline_per_baseline_err": pp_aa,
+                                 "map_per_pixel_err_iqu_modulo_offset": pp_map_off,
+                                 "baseline_per_baseline_err_modulo_offset": pp_aa_off,
                                  "tolerance": 1e-4,
                                  "map_per_pixel_err_iqu_floor_1e-3": pp_map3,
                                  "samples": "the same (float32) samples in both batches",

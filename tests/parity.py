@@ -89,6 +89,16 @@ def close(a, b, rtol, what="", floor=FLOOR):
     return e
 
 
+def per_pixel_error_modulo_offset(a, b, floor=FLOOR):
+    """per_pixel_error after removing the mean of a - b over the elements
+    where either is nonzero (the solve's undetermined common offset)."""
+    a = np.asarray(a, dtype=float).reshape(-1)
+    b = np.asarray(b, dtype=float).reshape(-1)
+    nz = (a != 0) | (b != 0)
+    off = float(np.mean(a[nz] - b[nz])) if nz.any() else 0.0
+    return per_pixel_error(np.where(nz, a - off, a), b, floor)
+
+
 def close_modulo_offset(a, b, rtol, what="", floor=FLOOR):
     """close() after removing the mean of a - b over the elements where
     either is nonzero (the solve's undetermined common offset)."""
