@@ -324,10 +324,8 @@ void Engine::apply_A_batch() {
     MADAM_CUDA(cudaMemcpyAsync(apb_.get(), pb_.get(), nt * sizeof(double),
                                cudaMemcpyDeviceToDevice, st_));
     const long nfs = (long)filt_segs_.size() * nrhs_;
-    // the FP32-TOD batch filters in float32 passes (its reliable updates
-    // recompute the residual with the float64 filter)
     if (nfs > 0) fft_->convolve(st_, filt_segs_b_d_.get(), nfs, fcov_.get(), npsdtot_, pb_.get(),
-                                apb_.get(), fp32_);
+                                apb_.get());
   } else if (par_.diagfilter != 0) {
     for (long k = 0; k < nrhs_; ++k)
       MADAM_LAUNCH(k_diagfilter, grid_for(nb), 256, 0, st_, apb_.get() + k * nb, nna_.get(),

@@ -26,13 +26,6 @@ __device__ __forceinline__ cplx cconj(cplx a) { return make_double2(a.x, -a.y); 
 __device__ __forceinline__ cplx cadd(cplx a, cplx b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ cplx csub(cplx a, cplx b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ cplx cscale(cplx a, double s) { return make_double2(a.x * s, a.y * s); }
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 
 // exp(-2 pi i num / den) computed with sincospi for full double accuracy
 __device__ __forceinline__ cplx twiddle(long long num, long long den) {
@@ -282,25 +275,310 @@ __global__ void k_conv_small(const ConvSeg *segs, const double *spectra, long lo
 }
 
 // ------------------------------------------------------ Stockham FFT --
-// (fft_steps.inl) the four-step passes in float64 and in float32
-#define FFT_NS fs64
-#define FFT_CPLX double2
-#define FFT_REAL double
-#define FFT_MK make_double2
-#include "fft_steps.inl"
-#undef FFT_NS
-#undef FFT_CPLX
-#undef FFT_REAL
-#undef FFT_MK
-#define FFT_NS fs32
-#define FFT_CPLX float2
-#define FFT_REAL float
-#define FFT_MK make_float2
-#include "fft_steps.inl"
-#undef FFT_NS
-#undef FFT_CPLX
-#undef FFT_REAL
-#undef FFT_MK
+// Batched radix-8 Stockham transforms for the four-step passes.  Pass p
+// (sub-transform size Ns = 8^p) takes the eight elements j + k L/8 of a
+// length-L transform into registers, multiplies element k by the twiddle
+// w_L^{(j mod Ns) k L/(8 Ns)}, does an 8-point DFT in registers and writes
+// element k to (j / Ns) 8 Ns + (j mod Ns) + k Ns: natural order in and out,
+// no bit reversal.  A last radix-4 or radix-2 pass finishes lengths that are
+// not powers of 8.  Every thread holds eight values per pass; shared-memory
+// rows are padded one slot in nine (pad8) so that strided accesses spread
+// over the banks.  The first pass may read from global memory and the last
+// pass write to it through the load / store functors.
+__device__ __forceinline__ int pad8(int i) { return i + (i >> 3); }
+
+// twL[q] = exp(-2 pi i q / L), q < L: the sub-transform's twiddles, copied
+// into shared memory by the kernel (load_twl) before its first transform
+template <bool INV>
+__device__ __forceinline__ cplx tw_l(const cplx *twL, int q) {
+  const cplx w = twL[q];
+  return INV ? cconj(w) : w;
+}
+
+__device__ __forceinline__ void load_twl(cplx *twL, int L, const cplx *tw) {
+  for (int q = threadIdx.x; q < L; q += blockDim.x) twL[q] = tw[q];
+}
+
+// The twiddles of the radix-8 passes p >= 1 (sub-transform size Ns = 8^p)
+// in the order the threads read them: ptw[off_p + (k - 1) Ns + r] =
+// exp(-2 pi i r k L / (8 Ns) / L) for k = 1..7, r < Ns, so that consecutive
+// threads (consecutive r) read consecutive entries with no bank conflicts.
+// At most L - 8 entries; the values are those of tw.
+__device__ __forceinline__ void load_pass_tw(cplx *ptw, int L, int logL, const cplx *tw) {
+  const int n8 = logL / 3;
+  int off = 0;
+  for (int p = 1, Ns = 8; p < n8; ++p, Ns *= 8) {
+    const int step = L / (8 * Ns);
+    for (int e = threadIdx.x; e < 7 * Ns; e += blockDim.x) {
+      const int k = e / Ns + 1, r = e % Ns;
+      ptw[off + e] = tw[r * step * k];
+    }
+    off += 7 * Ns;
+  }
+}
+
+template <bool INV>
+__device__ __forceinline__ cplx mul_mi(cplx a) {  // a * (-i), inverse a * i
+  return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+}
+
+template <bool INV>
+__device__ __forceinline__ cplx mul_w8(cplx a) {  // a * exp(-+ 2 pi i / 8)
+  const double c = 0.70710678118654752440;
+  return INV ? make_double2(c * (a.x - a.y), c * (a.x + a.y))
+             : make_double2(c * (a.x + a.y), c * (a.y - a.x));
+}
+
+template <bool INV>
+__device__ __forceinline__ cplx mul_w83(cplx a) {  // a * exp(-+ 6 pi i / 8)
+  const double c = 0.70710678118654752440;
+  return INV ? make_double2(-c * (a.x + a.y), c * (a.x - a.y))
+             : make_double2(c * (a.y - a.x), -c * (a.x + a.y));
+}
+
+// 8-point DFT in registers, natural order in and out
+template <bool INV>
+__device__ __forceinline__ void dft8(cplx *v) {
+  const cplx a0 = cadd(v[0], v[4]), b0 = csub(v[0], v[4]);
+  const cplx a1 = cadd(v[1], v[5]), b1 = mul_w8<INV>(csub(v[1], v[5]));
+  const cplx a2 = cadd(v[2], v[6]), b2 = mul_mi<INV>(csub(v[2], v[6]));
+  const cplx a3 = cadd(v[3], v[7]), b3 = mul_w83<INV>(csub(v[3], v[7]));
+  const cplx c0 = cadd(a0, a2), d0 = csub(a0, a2), c1 = cadd(a1, a3);
+  const cplx d1 = mul_mi<INV>(csub(a1, a3));
+  v[0] = cadd(c0, c1);
+  v[4] = csub(c0, c1);
+  v[2] = cadd(d0, d1);
+  v[6] = csub(d0, d1);
+  const cplx e0 = cadd(b0, b2), f0 = csub(b0, b2), e1 = cadd(b1, b3);
+  const cplx f1 = mul_mi<INV>(csub(b1, b3));
+  v[1] = cadd(e0, e1);
+  v[5] = csub(e0, e1);
+  v[3] = cadd(f0, f1);
+  v[7] = csub(f0, f1);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(cplx *v) {
+  const cplx c0 = cadd(v[0], v[2]), d0 = csub(v[0], v[2]), c1 = cadd(v[1], v[3]);
+  const cplx d1 = mul_mi<INV>(csub(v[1], v[3]));
+  v[0] = cadd(c0, c1);
+  v[2] = csub(c0, c1);
+  v[1] = cadd(d0, d1);
+  v[3] = csub(d0, d1);
+}
+
+// Last radix-R pass (R = 2 or 4, Ns = L / R): butterflies j < L / R over the
+// elements j + k L / R; each thread takes 8 / R butterflies.
+template <int R, bool INV, bool FFAST, typename Store>
+__device__ __forceinline__ void last_pass(cplx *s, int S, int L, int nfft, const cplx *twL,
+                                          int nb8, Store store) {
+  constexpr int PER = 8 / R;
+  const int Lr = L / R, t = threadIdx.x;
+  cplx v[PER][R];
+  int ff[PER], jj[PER];
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    const int q = t + u * nb8;
+    ff[u] = -1;
+    jj[u] = 0;
+    if (q < nfft * Lr) {
+      ff[u] = FFAST ? q % nfft : q / Lr;
+      jj[u] = FFAST ? q / nfft : q % Lr;
+#pragma unroll
+      for (int k = 0; k < R; ++k) v[u][k] = s[ff[u] * S + pad8(jj[u] + k * Lr)];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < PER; ++u) {
+    if (ff[u] < 0) continue;
+#pragma unroll
+    for (int k = 1; k < R; ++k) v[u][k] = cmul(v[u][k], tw_l<INV>(twL, jj[u] * k));
+    if (R == 4) {
+      dft4<INV>(v[u]);
+    } else {
+      const cplx a = v[u][0], b = v[u][1];
+      v[u][0] = cadd(a, b);
+      v[u][1] = csub(a, b);
+    }
+#pragma unroll
+    for (int k = 0; k < R; ++k) store(ff[u], jj[u] + k * Lr, v[u][k]);
+  }
+  __syncthreads();
+}
+
+// nfft transforms of length L (>= 64) at s + f * S; blockDim.x >= nfft L / 8.
+// FFAST: consecutive threads take consecutive transforms f (else consecutive
+// j).  load(f, i) gives input element i of transform f for the first pass;
+// store(f, i, v) takes output element i of the last pass.
+template <bool INV, bool FFAST, typename Load, typename Store>
+__device__ __forceinline__ void fft_block(cplx *s, int S, int L, int logL, int nfft,
+                                          const cplx *twL, const cplx *ptw, Load load,
+                                          Store store) {
+  const int L8 = L >> 3, n8 = logL / 3, rem = logL - 3 * n8;
+  const int nb8 = nfft * L8;
+  const int t = threadIdx.x;
+  int Ns = 1, poff = 0;
+  for (int pass = 0; pass < n8; ++pass) {
+    const bool first = pass == 0, last = pass == n8 - 1 && rem == 0;
+    const bool act = t < nb8;
+    const int f = FFAST ? t % nfft : t / L8;
+    const int j = FFAST ? t / nfft : t % L8;
+    cplx v[8];
+    if (act) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        v[k] = first ? load(f, j + k * L8) : s[f * S + pad8(j + k * L8)];
+    }
+    __syncthreads();
+    if (act) {
+      if (!first) {
+        const cplx *pt = ptw + poff + (j & (Ns - 1));
+#pragma unroll
+        for (int k = 1; k < 8; ++k) {
+          const cplx w = pt[(k - 1) * Ns];
+          v[k] = cmul(v[k], INV ? cconj(w) : w);
+        }
+      }
+      dft8<INV>(v);
+      if (last) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) store(f, j + k * L8, v[k]);
+      } else {
+        const int base = (j / Ns) * Ns * 8 + (j & (Ns - 1));
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s[f * S + pad8(base + k * Ns)] = v[k];
+      }
+    }
+    __syncthreads();
+    if (pass > 0) poff += 7 * Ns;
+    Ns *= 8;
+  }
+  if (rem == 1) last_pass<2, INV, FFAST>(s, S, L, nfft, twL, nb8, store);
+  else if (rem == 2) last_pass<4, INV, FFAST>(s, S, L, nfft, twL, nb8, store);
+}
+
+// ------------------------------------------------------- four-step path --
+// Pass 1: forward column FFTs (length R) of G adjacent columns, twiddled.
+__global__ void __launch_bounds__(512, 2) k_conv_cols_fwd(const ConvSeg *segs, const double *x,
+                                                       const double *part, double2 *work, int R,
+                                                       int logR, int C, int G,
+                                                       const cplx *__restrict__ twrow,
+                                                       const cplx *__restrict__ twr) {
+  extern __shared__ double2 sm[];
+  const int S = pad8(R) + 1;
+  cplx *twL = sm + G * S, *ptw = twL + R;
+  load_twl(twL, R, twr);
+  load_pass_tw(ptw, R, logR, twr);
+  const int seg = blockIdx.y;
+  const ConvSeg sg = segs[seg];
+  const double mean = seg_mean(part, seg, sg.n_in, sg.flags & 1);
+  const int c0 = blockIdx.x * G;
+  const long long N = (long long)R * C;
+  double2 *W = work + (long long)seg * N;
+  auto load = [&](int f, int n1) {
+    const long long m = (long long)C * n1 + c0 + f;
+    return make_double2(seg_input(x, sg, 2 * m, mean), seg_input(x, sg, 2 * m + 1, mean));
+  };
+  auto store = [&](int f, int k1, cplx v) {
+    const long long i = (long long)k1 * C + c0 + f;
+    W[i] = cmul(v, twrow[i]);
+  };
+  fft_block<false, true>(sm, S, R, logR, G, twL, ptw, load, store);
+}
+
+// Pass 2: forward row FFTs of rows k1 and R-k1, spectral product, inverse
+// row FFTs, inverse twiddles.  Hrows holds the spectra in rows of the split
+// (Hr[k1][k2] = H[k1 + R k2]); the Nyquist value H[N] comes from spectra.
+__global__ void __launch_bounds__(1024) k_conv_rows(const ConvSeg *segs,
+                                                    const double *__restrict__ Hrows,
+                                                    const double *__restrict__ spectra,
+                                                    long long spec_len, double2 *work, int R,
+                                                    int C, int logC,
+                                                    const cplx *__restrict__ twrow,
+                                                    const cplx *__restrict__ wrow,
+                                                    const cplx *__restrict__ twc) {
+  extern __shared__ double2 sm[];
+  const int S = pad8(C) + 1;
+  cplx *s = sm;  // 2 rows
+  cplx *twL = sm + 2 * S, *ptw = twL + C;
+  load_twl(twL, C, twc);
+  load_pass_tw(ptw, C, logC, twc);
+  const int seg = blockIdx.y;
+  const ConvSeg sg = segs[seg];
+  const long long N = (long long)R * C;
+  double2 *W = work + (long long)seg * N;
+  const int j = blockIdx.x;            // 0 .. R/2
+  const int ka = j, kb = (R - j) % R;  // row pair (equal for j = 0, R/2)
+  const int nrows = (ka == kb) ? 1 : 2;
+  auto gload = [&](int f, int n2) { return W[(long long)(f ? kb : ka) * C + n2]; };
+  auto sload = [&](int f, int n2) { return s[f * S + pad8(n2)]; };
+  auto sstore = [&](int f, int n2, cplx v) { s[f * S + pad8(n2)] = v; };
+  fft_block<false, false>(s, S, C, logC, nrows, twL, ptw, gload, sstore);
+  const double *Hr = Hrows + (long long)sg.spec * N;
+  const double *Ha = Hr + (long long)ka * C, *Hb = Hr + (long long)kb * C;
+  const cplx *Wa = wrow + (long long)ka * C;
+  auto at = [&](int f, int n2) -> cplx & { return s[f * S + pad8(n2)]; };
+  if (ka == 0) {
+    // row 0: (0, k2) <-> (0, C - k2); k = R k2, N - k = R (C - k2)
+    for (int k2 = threadIdx.x; k2 <= C / 2; k2 += blockDim.x) {
+      const int p2 = (C - k2) % C;
+      cplx A = at(0, k2), B = at(0, p2);
+      const double Hnk = k2 ? Ha[C - k2] : spectra[(long long)sg.spec * spec_len + N];
+      spectral_pair(A, B, k2 == 0, Wa[k2], Ha[k2], Hnk);
+      at(0, k2) = A;
+      if (p2 != k2) at(0, p2) = B;
+    }
+  } else if (ka == kb) {
+    // row R/2: (R/2, k2) <-> (R/2, C - 1 - k2)
+    for (int k2 = threadIdx.x; k2 < C / 2; k2 += blockDim.x) {
+      const int p2 = C - 1 - k2;
+      cplx A = at(0, k2), B = at(0, p2);
+      spectral_pair(A, B, false, Wa[k2], Ha[k2], Ha[p2]);
+      at(0, k2) = A;
+      at(0, p2) = B;
+    }
+  } else {
+    // rows ka, kb = R - ka: (ka, k2) <-> (kb, C - 1 - k2)
+    for (int k2 = threadIdx.x; k2 < C; k2 += blockDim.x) {
+      const int p2 = C - 1 - k2;
+      cplx A = at(0, k2), B = at(1, p2);
+      spectral_pair(A, B, false, Wa[k2], Ha[k2], Hb[p2]);
+      at(0, k2) = A;
+      at(1, p2) = B;
+    }
+  }
+  __syncthreads();
+  auto gstore = [&](int f, int n2, cplx v) {
+    const long long i = (long long)(f ? kb : ka) * C + n2;
+    W[i] = cmul(v, cconj(twrow[i]));
+  };
+  fft_block<true, false>(s, S, C, logC, nrows, twL, ptw, sload, gstore);
+}
+
+// Pass 3: inverse column FFTs and real output.
+__global__ void __launch_bounds__(512, 2) k_conv_cols_inv(const ConvSeg *segs, const double2 *work,
+                                                       double *y, int R, int logR, int C, int G,
+                                                       const cplx *__restrict__ twr) {
+  extern __shared__ double2 sm[];
+  const int S = pad8(R) + 1;
+  cplx *twL = sm + G * S, *ptw = twL + R;
+  load_twl(twL, R, twr);
+  load_pass_tw(ptw, R, logR, twr);
+  const int seg = blockIdx.y;
+  const ConvSeg sg = segs[seg];
+  const int c0 = blockIdx.x * G;
+  const long long N = (long long)R * C;
+  const double2 *W = work + (long long)seg * N;
+  const double scale = 1.0 / (double)N;
+  auto load = [&](int f, int k1) { return W[(long long)k1 * C + c0 + f]; };
+  auto store = [&](int f, int n1, cplx v) {
+    const long long m = (long long)C * n1 + c0 + f;
+    if (2 * m < sg.n_out) y[sg.y_off + 2 * m] = v.x * scale;
+    if (2 * m + 1 < sg.n_out) y[sg.y_off + 2 * m + 1] = v.y * scale;
+  };
+  fft_block<true, true>(sm, S, R, logR, G, twL, ptw, load, store);
+}
 
 // The row-ordered tables of the four-step split (FFTPlan), from T2.
 __global__ void k_fill_row_tables(const cplx *T2, long long N, int R, int C, cplx *twrow,
@@ -313,18 +591,6 @@ __global__ void k_fill_row_tables(const cplx *T2, long long N, int R, int C, cpl
     if (i < R) twr[i] = T2[i * (2 * N / R)];
     if (i < C) twc[i] = T2[i * (2 * N / C)];
   }
-}
-
-// float32 copies of tables (complex and real)
-__global__ void k_d2f_c(const double2 *a, float2 *b, long long n) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    b[i] = make_float2((float)a[i].x, (float)a[i].y);
-}
-__global__ void k_d2f(const double *a, float *b, long long n) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x)
-    b[i] = (float)a[i];
 }
 
 // rows[s][k1][k2] = H[s][k1 + R k2]: the transpose of each spectrum viewed
@@ -368,13 +634,11 @@ FFTPlan::~FFTPlan() {
   forget_spectra();
   for (double *p : {table, work, means, twrow, wrow, twr, twc})
     if (p) dev_free(p);
-  if (tw32) dev_free(tw32);
 }
 
 void FFTPlan::forget_spectra() {
   for (RowSpectra &c : cache) {
     if (c.rows) dev_free(c.rows);
-    if (c.rows32) dev_free(c.rows32);
     c = RowSpectra{};
   }
 }
@@ -388,18 +652,11 @@ void FFTPlan::make_tables(cudaStream_t st) {
   MADAM_LAUNCH(k_fill_row_tables, (unsigned)std::min<long long>(4096, (N + 255) / 256), 256, 0,
                st, (const cplx *)table, (long long)N, R, C, (cplx *)twrow, (cplx *)wrow,
                (cplx *)twr, (cplx *)twc);
-  tw32 = (float *)dev_alloc((size_t)(2 * N + R + C) * sizeof(float2));
-  float2 *t = (float2 *)tw32;
-  const unsigned g = (unsigned)std::min<long long>(4096, (N + 255) / 256);
-  MADAM_LAUNCH(k_d2f_c, g, 256, 0, st, (const double2 *)twrow, t, (long long)N);
-  MADAM_LAUNCH(k_d2f_c, g, 256, 0, st, (const double2 *)wrow, t + N, (long long)N);
-  MADAM_LAUNCH(k_d2f_c, g, 256, 0, st, (const double2 *)twr, t + 2 * N, (long long)R);
-  MADAM_LAUNCH(k_d2f_c, g, 256, 0, st, (const double2 *)twc, t + 2 * N + R, (long long)C);
 }
 
-FFTPlan::RowSpectra &FFTPlan::row_spectra(cudaStream_t st, const double *spectra, long nspec) {
-  for (RowSpectra &c : cache)
-    if (c.rows && c.src == spectra && c.nspec == nspec) return c;
+const double *FFTPlan::row_spectra(cudaStream_t st, const double *spectra, long nspec) {
+  for (const RowSpectra &c : cache)
+    if (c.rows && c.src == spectra && c.nspec == nspec) return c.rows;
   // a free slot, else the first one is dropped
   RowSpectra *slot = &cache[0];
   for (RowSpectra &c : cache)
@@ -408,8 +665,6 @@ FFTPlan::RowSpectra &FFTPlan::row_spectra(cudaStream_t st, const double *spectra
       break;
     }
   if (slot->rows) dev_free(slot->rows);
-  if (slot->rows32) dev_free(slot->rows32);
-  slot->rows32 = nullptr;
   slot->src = spectra;
   slot->nspec = nspec;
   slot->rows = (double *)dev_alloc((size_t)std::max<long>(1, nspec) * N * sizeof(double));
@@ -418,7 +673,7 @@ FFTPlan::RowSpectra &FFTPlan::row_spectra(cudaStream_t st, const double *spectra
     MADAM_LAUNCH(k_spectra_rows, dim3(R / 32, C / 32, (unsigned)nspec), dim3(32, 8), 0, st,
                  spectra, (long long)N + 1, R, C, slot->rows);
   }
-  return *slot;
+  return slot->rows;
 }
 
 void FFTPlan::reserve(long nseg) {
@@ -433,7 +688,7 @@ void FFTPlan::reserve(long nseg) {
 }
 
 void FFTPlan::convolve(cudaStream_t st, const ConvSeg *segs, long nseg, const double *spectra,
-                       long nspec, const double *x, double *y, bool f32) {
+                       long nspec, const double *x, double *y) {
   if (nseg == 0) return;
   if (!table) {
     table = (double *)dev_alloc((size_t)2 * N * sizeof(double2));
@@ -472,41 +727,24 @@ void FFTPlan::convolve(cudaStream_t st, const ConvSeg *segs, long nseg, const do
     const unsigned trows = (unsigned)std::max(32, C / 4);
     static bool attr = false;
     if (!attr) {
-      for (const void *k : {(const void *)fs64::k_conv_cols_fwd, (const void *)fs64::k_conv_cols_inv,
-                            (const void *)fs64::k_conv_rows, (const void *)fs32::k_conv_cols_fwd,
-                            (const void *)fs32::k_conv_cols_inv, (const void *)fs32::k_conv_rows})
-        MADAM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kSmemMax));
+      MADAM_CUDA(cudaFuncSetAttribute(k_conv_cols_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kSmemMax));
+      MADAM_CUDA(cudaFuncSetAttribute(k_conv_cols_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kSmemMax));
+      MADAM_CUDA(cudaFuncSetAttribute(k_conv_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)kSmemMax));
       attr = true;
     }
     make_tables(st);
-    RowSpectra &rs = row_spectra(st, spectra, nspec);
+    const double *Hrows = row_spectra(st, spectra, nspec);
     dim3 gc(C / G, (unsigned)nseg), gr(R / 2 + 1, (unsigned)nseg);
-    if (!f32) {
-      MADAM_LAUNCH(fs64::k_conv_cols_fwd, gc, tcols, smem_cols, st, segs, x, means,
-                   (double2 *)work, R, logR, C, G, (const double2 *)twrow, (const double2 *)twr);
-      MADAM_LAUNCH(fs64::k_conv_rows, gr, trows, smem_rows, st, segs, rs.rows, spectra, spec_len,
-                   (double2 *)work, R, C, logC, (const double2 *)twrow, (const double2 *)wrow,
-                   (const double2 *)twc);
-      MADAM_LAUNCH(fs64::k_conv_cols_inv, gc, tcols, smem_cols, st, segs, (const double2 *)work,
-                   y, R, logR, C, G, (const double2 *)twr);
-    } else {
-      if (!rs.rows32) {
-        const long long nr = (long long)std::max<long>(1, nspec) * N;
-        rs.rows32 = (float *)dev_alloc((size_t)nr * sizeof(float));
-        MADAM_LAUNCH(k_d2f, (unsigned)std::min<long long>(4096, (nr + 255) / 256), 256, 0, st,
-                     rs.rows, rs.rows32, nr);
-      }
-      const float2 *t = (const float2 *)tw32;
-      const float2 *trow = t, *wr = t + N, *tr = t + 2 * N, *tc = t + 2 * N + R;
-      // float2 elements: half the shared memory of the float64 passes
-      MADAM_LAUNCH(fs32::k_conv_cols_fwd, gc, tcols, smem_cols / 2, st, segs, x, means,
-                   (float2 *)work, R, logR, C, G, trow, tr);
-      MADAM_LAUNCH(fs32::k_conv_rows, gr, trows, smem_rows / 2, st, segs, rs.rows32, spectra,
-                   spec_len, (float2 *)work, R, C, logC, trow, wr, tc);
-      MADAM_LAUNCH(fs32::k_conv_cols_inv, gc, tcols, smem_cols / 2, st, segs,
-                   (const float2 *)work, y, R, logR, C, G, tr);
-    }
+    MADAM_LAUNCH(k_conv_cols_fwd, gc, tcols, smem_cols, st, segs, x, means, (double2 *)work, R,
+                 logR, C, G, (const cplx *)twrow, (const cplx *)twr);
+    MADAM_LAUNCH(k_conv_rows, gr, trows, smem_rows, st, segs, Hrows, spectra, spec_len,
+                 (double2 *)work, R, C, logC, (const cplx *)twrow, (const cplx *)wrow,
+                 (const cplx *)twc);
+    MADAM_LAUNCH(k_conv_cols_inv, gc, tcols, smem_cols, st, segs, (const double2 *)work, y, R,
+                 logR, C, G, (const cplx *)twr);
   }
   MADAM_LAUNCH(k_seg_sum, gm, 256, 0, st, segs, y, 1, means);
   MADAM_LAUNCH(k_seg_sub_mean, gm, 256, 0, st, segs, y, means);

@@ -29,9 +29,6 @@ struct FFTPlan {
   // and the sub-transform twiddles exp(-2 pi i q / L) for L = R and C.  The
   // values are those of `table`.
   double *twrow = nullptr, *wrow = nullptr, *twr = nullptr, *twc = nullptr;
-  // the same four tables rounded to float32 (float2 [N | N | R | C]), for
-  // the float32 passes of the FP32-TOD batch's filter
-  float *tw32 = nullptr;
   // Spectra copied into the rows of the split: rows[s][k1][k2] =
   // spectra[s][k1 + R k2], one copy per spectra array, kept while the plan
   // lives (forget_spectra() drops them when an array is rewritten).
@@ -39,22 +36,19 @@ struct FFTPlan {
     const double *src;
     long nspec;
     double *rows;
-    float *rows32;  // the rows rounded to float32, made when first asked for
   };
   RowSpectra cache[4] = {};
   explicit FFTPlan(long nof_);
   ~FFTPlan();
   void reserve(long nseg);
   void forget_spectra();
-  // segs: device table of nseg entries; spectra: [nspec][nof/2+1] (device).
-  // f32: the four-step passes in float32 (the segment means, the input and
-  // the output stay float64); the FP32-TOD batch's filter
+  // segs: device table of nseg entries; spectra: [nspec][nof/2+1] (device)
   void convolve(cudaStream_t st, const ConvSeg *segs, long nseg, const double *spectra,
-                long nspec, const double *x, double *y, bool f32 = false);
+                long nspec, const double *x, double *y);
 
  private:
   void make_tables(cudaStream_t st);
-  RowSpectra &row_spectra(cudaStream_t st, const double *spectra, long nspec);
+  const double *row_spectra(cudaStream_t st, const double *spectra, long nspec);
 };
 
 }  // namespace madam
