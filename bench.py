@@ -874,7 +874,7 @@ def main():
                     help="serving: requests in the stream (the serving workload names 2000; "
                          "the headline line runs this many)")
     ap.add_argument("--rate", type=float, default=20.0)
-    ap.add_argument("--workers", type=int, default=4)
+    ap.add_argument("--workers", type=int, default=6)
     ap.add_argument("--nrhs", type=int, default=64)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
