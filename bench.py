@@ -520,6 +520,10 @@ def run_serve(args, world, rank, local):
                     tickets[i] = 0
                     done[i] = True
                     cond.notify_all()
+            if fin and int(done.sum()) % 8 < len(fin):
+                # the client's freed inputs go back to the device (torch keeps
+                # them cached otherwise, out of the server's reach)
+                torch.cuda.empty_cache()
             if not fin:
                 time.sleep(0.001)
 

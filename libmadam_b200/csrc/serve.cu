@@ -74,6 +74,7 @@ struct Job {
   std::map<std::string, std::vector<char>> results;
   double noiter = 0;
   double setup_ms = 0, iterate_ms = 0, finalize_ms = 0;  // the engine's phases
+  bool retried = false;  // requeued once after running out of device memory
 };
 
 // device memory of a job, from the engine's buffers per sample / baseline
@@ -246,6 +247,34 @@ class Server {
         st = 3;
         err = e.what();
         eng.reset();  // a failed job leaves no state behind
+        cudaGetLastError();  // an allocation failure is not left pending for the next job
+      }
+      // the pool keeps the memory of finished jobs for the next ones, but no
+      // more than the budget: the rest goes back to the device for other
+      // users of the GPU
+      {
+        int dev = 0;
+        cudaMemPool_t pool;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess)
+          cudaMemPoolTrimTo(pool, budget_);
+        cudaGetLastError();
+      }
+      // a job that ran out of device memory (other users of the GPU hold
+      // more than the budget assumed) goes back to the head of the queue
+      // once, to start when the running jobs leave room
+      const bool retry = st == 3 && !j->retried && err.find("out of memory") != std::string::npos;
+      if (retry) {
+        {
+          std::lock_guard<std::mutex> lk(mu_);
+          j->retried = true;
+          j->state = 0;
+          in_flight_ -= j->bytes;
+          --running_;
+          queue_.push_front(j);
+        }
+        cv_work_.notify_all();
+        continue;
       }
       {
         std::lock_guard<std::mutex> lk(mu_);
