@@ -79,7 +79,9 @@ int madam_b200_destripe_with_cache_batch_fp32(int comm, long ndet, long nsamp, l
  * refused) and returns its id, or -1 (message in err).  The caller's buffers
  * must stay valid until the job is done.  Jobs start first come, first
  * served, when their estimated footprint fits the budget beside the running
- * jobs, and overlap on the device; their products do not depend on what else
+ * jobs, and overlap on the device (the library's memory pool is trimmed to
+ * the budget after each job, and a job that runs out of device memory is
+ * requeued once); their products do not depend on what else
  * runs (beyond rounding).  A job's setup runs on its worker; its PCG then
  * iterates in shared rounds with the other jobs past their setup, driven by
  * one stepper thread: per round each job's A p and preconditioner, the CG
