@@ -150,17 +150,24 @@ void Engine::apply_preconditioner_batch(const double *r, double *z) {
 
 namespace {
 std::mutex g_tune_mu;
-std::map<std::tuple<int, long long, int>, unsigned> g_tuned;  // (kernel, items, GW) -> grid
+// (device, kernel, items, GW) -> grid
+std::map<std::tuple<int, int, long long, int>, unsigned> g_tuned;
+int current_device() {
+  int d = 0;
+  cudaGetDevice(&d);
+  return d;
+}
 }  // namespace
 
 bool Engine::tuned(int key, long long items, int GW) {
+  const auto id = std::make_tuple(current_device(), key, items, GW);
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  return g_tuned.count(std::make_tuple(key, items, GW)) > 0;
+  return g_tuned.count(id) > 0;
 }
 
 template <class L>
 unsigned Engine::tuned_grid(const void *kern, int key, long long items, int GW, L launch) {
-  const auto id = std::make_tuple(key, items, GW);
+  const auto id = std::make_tuple(current_device(), key, items, GW);
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tuned.find(id);
