@@ -1350,7 +1350,7 @@ void Engine::build_filter() {
     filter_err_ = e.what();  // raised where the host's spectra raise it
     return;
   }
-  if (!dev_ok || tasks.empty()) {
+  if (!dev_ok || tasks.empty() || tasks.size() > 65535) {  // (a grid dimension per PSD)
     filter_job_ =
         std::async(std::launch::async, [this, tasks, nh]() { filter_spectra(tasks, nh); });
     return;
