@@ -71,3 +71,16 @@ def test_two_ranks_match_one():
 
 def test_two_ranks_with_subsets_and_no_filter():
     SU.run_ranks(_rank, 2, (dict(subsets=True, kfilter=False, diagfilter=0.5),))
+
+
+def test_two_ranks_with_file_spectrum(tmp_path):
+    """Every rank reads the spectrum file for the detectors it holds
+    (get_spectrum_file, noise_routines.f90:600-634); the sharded run still
+    gives the lone run's maps and baselines."""
+    from libmadam_b200 import synthetic as syn
+    from test_oracle_spectrum import _table, _write
+    d = syn.to_numpy(syn.generate(syn.small_config(seed=101)))
+    freq, psd, sig = _table(d)
+    path = tmp_path / "spec.txt"
+    _write(path, list(d["dets"]), sig, freq, psd)
+    SU.run_ranks(_rank, 2, (dict(file_spectrum=str(path)),))
