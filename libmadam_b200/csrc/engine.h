@@ -247,7 +247,7 @@ class Engine {
   int guard_chunk_len(long long npos) const;
   void iterate();
   void pcg_reset();
-  bool pcg_judge(long istep, double rz, double rr);
+  bool pcg_stop_test(long istep, double rz, double rr);
   long pcg_istep_ = 0;
   double pcg_t0_ = 0, run_t0_ = 0, pcg_rr_true_ = 0;
   bool pcg_reliable_ = false;

@@ -2602,7 +2602,7 @@ void Engine::iterate() {
     timings.filter_ms += tm[1];
     timings.gather_ms += tm[2];
     timings.precond_ms += tm[3];
-    if (pcg_judge(istep, scal_host_[S_RZ], scal_host_[S_RR])) break;
+    if (pcg_stop_test(istep, scal_host_[S_RZ], scal_host_[S_RR])) break;
     MADAM_LAUNCH(k_update_p, grid_for(nb), 256, 0, st_, p_.get(), z_.get(), pw_.get(), bwv,
                  nb, scal_.get(), 0);
   }
@@ -2629,11 +2629,11 @@ void Engine::pcg_reset() {
   n_reliable_ = 0;
 }
 
-bool Engine::pcg_judge(long istep, double rz, double rr) {
+bool Engine::pcg_stop_test(long istep, double rz, double rr) {
   if (pcg_reliable_ && ((rr / rrinit < par_.cglimit && istep > par_.iter_min) ||
                         rr < kReliableDrop * pcg_rr_true_)) {
     // reliable update: the residual the float32 projections carried is
-    // replaced by the true one, so that convergence is judged, and the
+    // replaced by the true one, so that convergence is tested, and the
     // iteration continues, on the float64 system
     const long long nb = (long long)ndet_ * noba_short_ * nbasis_;
     true_residual(aa_.get(), yba_.get(), r_.get());
@@ -2742,7 +2742,7 @@ PcgJob Engine::pcg_job() {
 }
 
 bool Engine::pcg_after(double rz, double rr) {
-  return pcg_judge(pcg_istep_, rz, rr) || pcg_istep_ >= par_.iter_max;
+  return pcg_stop_test(pcg_istep_, rz, rr) || pcg_istep_ >= par_.iter_max;
 }
 
 void Engine::pcg_end() {
