@@ -136,6 +136,7 @@ static int destripe_impl(bool fp32, int comm, char *parstring, long ndet, char *
       madam::fail("temperature_only=T but pointing weights are polarized");
     if (ndet > 10000) madam::fail("ndet > NDETMAX");
     if (ndet <= 0 || nsamp <= 0 || nnz <= 0) madam::fail("empty data");
+    if (nnz != 1 && nnz != 3) madam::fail("only nnz = 1 or nnz = 3 is supported");
     auto dets = madam::read_detectors(par, detstring, ndet, detweights, npsd, npsdtot, psdstarts,
                                       npsdbin, psdfreqs, npsdval, psdvals);
     const bool dev = madam::inputs_on_device(-1, {timestamps, pix, pixweights, signal});

@@ -549,6 +549,7 @@ static long serve_submit(bool fp32, void *srv, char *parstring, long ndet, char 
     if (j->par.temperature_only && nnz != 1)
       madam::fail("temperature_only=T but pointing weights are polarized");
     if (ndet <= 0 || nsamp <= 0 || nnz <= 0) madam::fail("empty data");
+    if (nnz != 1 && nnz != 3) madam::fail("only nnz = 1 or nnz = 3 is supported");
     j->dets = madam::read_detectors(j->par, detstring, ndet, detweights, npsd, npsdtot,
                                     psdstarts, npsdbin, psdfreqs, npsdval, psdvals);
     j->ndet = ndet;

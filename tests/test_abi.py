@@ -66,6 +66,12 @@ def test_parameter_errors_are_reported_not_aborted():
                    np.ones(1, np.int64), np.zeros(1), np.array([1.0, 2.0]), np.ones(2))
     status, msg = _lib.last_error()
     assert status == 1 and "polarized" in msg
+    # nnz = 2: the reference's general pixel matrix is undefined (float32
+    # weights handed to the float64 dsyr, smadam_routines.f90:227)
+    with pytest.raises(RuntimeError, match="only nnz = 1 or nnz = 3 is supported"):
+        W.destripe(None, {}, ["a"], np.ones(1), np.zeros(4), np.zeros(4, np.int32),
+                   np.ones(8, np.float32), np.zeros(4), np.array([0]), np.ones(1, np.int64),
+                   np.zeros(1), np.array([1.0, 2.0]), np.ones(2))
     del d
 
 
