@@ -12,6 +12,9 @@
  * periods int64[nperiod] (start offsets); npsd int64[ndet];
  * psdstarts float64[npsdtot]; psdfreqs float64[npsdbin];
  * psdvals float64[npsdval].  Host or CUDA device pointers are accepted.
+ * nnz is 1 (temperature) or 3 (I, Q, U); other values are refused, since
+ * the reference's general pixel matrix (src/smadam_routines.f90:227) hands
+ * its float32 weights to the float64 BLAS dsyr and so has no defined result.
  * pix is rewritten in place (flagged samples become 12*nside_max^2) and
  * signal is destriped in place when write_tod or subsets are set, as in the
  * reference.  `comm` is a Fortran MPI handle in the reference; here it is 0
