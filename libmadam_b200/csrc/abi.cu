@@ -139,12 +139,19 @@ static int destripe_impl(bool fp32, int comm, char *parstring, long ndet, char *
     if (nnz != 1 && nnz != 3) madam::fail("only nnz = 1 or nnz = 3 is supported");
     auto dets = madam::read_detectors(par, detstring, ndet, detweights, npsd, npsdtot, psdstarts,
                                       npsdbin, psdfreqs, npsdval, psdvals);
+    // a lone rank reads file_spectrum once before any device work, so that
+    // a bad file fails fast (build_filter reads it again where the reference
+    // does, noise_routines.f90:430-432; sharded ranks wait for that read,
+    // which reports its error on every rank after the same collectives)
+    madam::Comm *cm = madam::comm_lookup(comm);
+    if (par.kfilter && !par.file_spectrum.empty() && (!cm || cm->nranks == 1))
+      (void)madam::read_spectrum_file(par.file_spectrum, dets);
     const bool dev = madam::inputs_on_device(-1, {timestamps, pix, pixweights, signal});
     Engine &e = engine();
     e.clear_subchunk_results();
     // comm: a communicator of madam_b200_comm_init_* (a sharded run), else a
     // single rank (the reference's MPI handle has no meaning here)
-    e.set_comm(madam::comm_lookup(comm));
+    e.set_comm(cm);
     // subchunk passes (smadam.F90:192-196): isubchunk = 1 .. nsubchunk, then
     // 0 (the full data) last, starting from the isubchunk parameter
     const int nsub = par.nsubchunk >= 2 ? (int)par.nsubchunk : 0;

@@ -144,3 +144,30 @@ def test_library_handles_avoid_mpi_fortran_handles():
     first = int(re.search(r"kFirstHandle = (0x[0-9A-Fa-f]+)", src).group(1), 16)
     # Open MPI: small indices; MPICH built-ins 0x44000000.., created ones negative
     assert 1 << 16 < first < 0x44000000 - (1 << 20)
+
+
+@pytest.mark.parametrize("case, msg", [
+    ("nofile", "cannot open"),
+    ("header", "is not formatted correctly"),
+    ("missing", "ERROR: a not in"),
+    ("short", "Failed to read the table from spectrum file"),
+])
+def test_bad_spectrum_file_fails_before_device_work(tmp_path, case, msg):
+    """A lone rank reads file_spectrum (read_spectrum,
+    noise_routines.f90:505-596) before any device work: its errors need no
+    GPU."""
+    from libmadam_b200 import libmadam_wrapper as W
+    path = tmp_path / "spec.txt"
+    rows = ["%g %g" % (f, 1e-6 / f) for f in (0.01, 0.1, 1.0)]
+    text = ["3 1", "b" if case == "missing" else "a_det", "1e-3"] + rows
+    if case == "header":
+        text[0] = "three one"
+    elif case == "short":
+        text = text[:-1]
+    if case != "nofile":
+        path.write_text("\n".join(text) + "\n")
+    with pytest.raises(RuntimeError, match=msg):
+        W.destripe(None, {"kfilter": True, "file_spectrum": str(path)}, ["a"], np.ones(1),
+                   np.zeros(4), np.zeros(4, np.int32), np.ones(4, np.float32), np.zeros(4),
+                   np.array([0]), np.ones(1, np.int64), np.zeros(1), np.array([1.0, 2.0]),
+                   np.ones(2))
