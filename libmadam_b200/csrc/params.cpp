@@ -367,22 +367,35 @@ class ListInput {
     std::string line;
     while (std::getline(in, line)) lines_.push_back(line);
   }
-  // n items of one READ; false at the end of the file
+  // n items of one READ; false at the end of the file, and where the READ
+  // would leave items undefined: a null value ("r*" with no constant) or a
+  // slash that ends the READ early
   bool read(size_t n, std::vector<std::string> &out) {
     out.clear();
     while (out.size() < n) {
       if (rec_ >= lines_.size()) return false;
-      split(lines_[rec_++], out, n);
+      if (!split(lines_[rec_++], out, n)) return false;
     }
     return true;
   }
 
  private:
-  static void split(const std::string &s, std::vector<std::string> &out, size_t n) {
+  static bool split(const std::string &s, std::vector<std::string> &out, size_t n) {
     size_t i = 0;
     while (i < s.size() && out.size() < n) {
       while (i < s.size() && (std::isspace((unsigned char)s[i]) || s[i] == ',')) ++i;
       if (i >= s.size()) break;
+      if (s[i] == '/') return false;
+      // a repeat count "r*c": r copies of the constant c
+      size_t r = 1, j = i;
+      while (j < s.size() && std::isdigit((unsigned char)s[j])) ++j;
+      if (j > i && j < s.size() && s[j] == '*') {
+        if (j - i > 9) return false;
+        r = std::stoul(s.substr(i, j - i));
+        i = j + 1;
+        if (r == 0 || i >= s.size() || std::isspace((unsigned char)s[i]) || s[i] == ',')
+          return false;
+      }
       std::string tok;
       if (s[i] == '\'' || s[i] == '"') {
         const char q = s[i++];
@@ -401,8 +414,9 @@ class ListInput {
       } else {
         while (i < s.size() && !std::isspace((unsigned char)s[i]) && s[i] != ',') tok += s[i++];
       }
-      out.push_back(tok);
+      for (size_t k = 0; k < r && out.size() < n; ++k) out.push_back(tok);
     }
+    return true;
   }
   std::vector<std::string> lines_;
   size_t rec_ = 0;

@@ -1254,6 +1254,8 @@ extern int g_rank;
 struct FortranList {
   std::vector<std::string> rec;
   size_t next = 0;
+  // false at the end of the file, at a null value ("r*" alone) and at a
+  // slash, both of which leave items of the READ undefined
   bool items(size_t n, std::vector<std::string> &out) {
     out.clear();
     while (out.size() < n) {
@@ -1263,6 +1265,16 @@ struct FortranList {
       while (out.size() < n) {
         while (i < s.size() && (isspace((unsigned char)s[i]) || s[i] == ',')) ++i;
         if (i >= s.size()) break;
+        if (s[i] == '/') return false;
+        size_t rep = 1, j = i;  // "r*c": r copies of c
+        while (j < s.size() && isdigit((unsigned char)s[j])) ++j;
+        if (j > i && j < s.size() && s[j] == '*') {
+          if (j - i > 9) return false;
+          rep = strtoul(s.substr(i, j - i).c_str(), nullptr, 10);
+          i = j + 1;
+          if (rep == 0 || i >= s.size() || isspace((unsigned char)s[i]) || s[i] == ',')
+            return false;
+        }
         std::string t;
         if (s[i] == '\'' || s[i] == '"') {
           char q = s[i++];
@@ -1275,7 +1287,7 @@ struct FortranList {
         } else {
           while (i < s.size() && !isspace((unsigned char)s[i]) && s[i] != ',') t += s[i++];
         }
-        out.push_back(t);
+        for (size_t k = 0; k < rep && out.size() < n; ++k) out.push_back(t);
       }
     }
     return true;

@@ -151,6 +151,8 @@ def test_library_handles_avoid_mpi_fortran_handles():
     ("header", "is not formatted correctly"),
     ("missing", "ERROR: a not in"),
     ("short", "Failed to read the table from spectrum file"),
+    ("slash", "Failed to read detector noise levels"),
+    ("null", "Failed to read detector noise levels"),
 ])
 def test_bad_spectrum_file_fails_before_device_work(tmp_path, case, msg):
     """A lone rank reads file_spectrum (read_spectrum,
@@ -164,6 +166,10 @@ def test_bad_spectrum_file_fails_before_device_work(tmp_path, case, msg):
         text[0] = "three one"
     elif case == "short":
         text = text[:-1]
+    elif case == "slash":
+        text[2] = "/ 1e-3"
+    elif case == "null":
+        text[2] = "1* 1e-3"
     if case != "nofile":
         path.write_text("\n".join(text) + "\n")
     with pytest.raises(RuntimeError, match=msg):
@@ -171,3 +177,25 @@ def test_bad_spectrum_file_fails_before_device_work(tmp_path, case, msg):
                    np.zeros(4), np.zeros(4, np.int32), np.ones(4, np.float32), np.zeros(4),
                    np.array([0]), np.ones(1, np.int64), np.zeros(1), np.array([1.0, 2.0]),
                    np.ones(2))
+
+
+def test_spectrum_file_with_repeat_counts_is_read():
+    """Repeat counts ("r*c") and quoted names read as the reference's
+    list-directed READ reads them: the call gets past the file (and then
+    needs a GPU)."""
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    import tempfile
+    from libmadam_b200 import libmadam_wrapper as W
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "spec.txt")
+        with open(path, "w") as f:
+            f.write("3, 2  header words\n'x_a', \"b\"\n2*1d-3\n")
+            for fr in (0.01, 0.1, 1.0):
+                f.write("%g 2*%g\n" % (fr, 1e-6 / fr))
+        with pytest.raises(RuntimeError, match="CUDA"):
+            W.destripe(None, {"kfilter": True, "file_spectrum": path}, ["a"], np.ones(1),
+                       np.zeros(4), np.zeros(4, np.int32), np.ones(4, np.float32), np.zeros(4),
+                       np.array([0]), np.ones(1, np.int64), np.zeros(1), np.array([1.0, 2.0]),
+                       np.ones(2))

@@ -120,3 +120,39 @@ def test_spectrum_file_errors(tmp_path, case, msg):
     path.write_text("\n".join(text) + "\n")
     with pytest.raises(O.OracleError, match=msg):
         _run(d, dict(d["pars"], file_spectrum=str(path)))
+
+
+def test_repeat_counts(tmp_path):
+    """List-directed repeat counts ("r*c", r copies of c) in the sigmas and
+    the table give the file written out in full."""
+    d = syn.to_numpy(syn.generate(syn.small_config(seed=93)))
+    freq, psd, _ = _table(d)
+    ndet = len(d["dets"])
+    sig = np.full(ndet, 2e-3)
+    psd = np.repeat(psd[:, :1], ndet, 1)  # one spectrum for every detector
+    full, short = tmp_path / "full.txt", tmp_path / "short.txt"
+    names = list(d["dets"])
+    _write(full, names, sig, freq, psd)
+    text = full.read_text().splitlines()
+    text[2] = "%d*%.17e" % (ndet, sig[0])
+    for b in range(len(freq)):
+        text[3 + b] = "%.17e %d*%.17e" % (freq[b], ndet, psd[b, 0])
+    short.write_text("\n".join(text) + "\n")
+    _run(d, dict(d["pars"], file_spectrum=str(full)))
+    ref = O.result("fcov")
+    _run(d, dict(d["pars"], file_spectrum=str(short)))
+    np.testing.assert_array_equal(O.result("fcov"), ref)
+
+
+@pytest.mark.parametrize("line", ["1.0 / 2.0", "2*", "0*1.0"])
+def test_undefined_sigmas_are_refused(tmp_path, line):
+    """A slash or a null value leaves items of the READ undefined."""
+    d = syn.to_numpy(syn.generate(syn.small_config(seed=94)))
+    freq, psd, sig = _table(d)
+    path = tmp_path / "spec.txt"
+    _write(path, list(d["dets"]), sig, freq, psd)
+    text = path.read_text().splitlines()
+    text[2] = line + " " + " ".join("%g" % s for s in sig)
+    path.write_text("\n".join(text) + "\n")
+    with pytest.raises(O.OracleError, match="Failed to read detector noise levels"):
+        _run(d, dict(d["pars"], file_spectrum=str(path)))
