@@ -916,10 +916,15 @@ def main():
             # the headline line carries the precision form (float32 TOD at
             # nside 1024), the batched Monte Carlo form (64 realisations) and
             # the serving stream, each measured in the same run with its own
-            # clocks record
-            line["precision_form"] = extra_precision(args, world, rank, local)
-            line["batched_mc"] = extra_mc(args, world, rank, local)
-            line["serving"] = extra_serve(args, world, rank, local)
+            # clocks record; a form that fails is reported in its key and
+            # does not take the headline line with it
+            for key, fn in (("precision_form", extra_precision), ("batched_mc", extra_mc),
+                            ("serving", extra_serve)):
+                try:
+                    line[key] = fn(args, world, rank, local)
+                except Exception as e:  # noqa: BLE001
+                    line[key] = {"error": "{}: {}".format(type(e).__name__, e)}
+                    torch.cuda.empty_cache()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
