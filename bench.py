@@ -399,6 +399,23 @@ def run_mc(args, world, rank, local):
     return line
 
 
+def serve_requests(n, rate, seed):
+    """The serving stream's request mix: per request nside in {128, 256, 512,
+    1024}, 2-32 detectors, log-uniform 2^18-2^24 samples per detector, fknee
+    0.02-0.2 Hz, base_first in {0.25, 0.5, 1, 2} s, float32 TOD for half of
+    them, its own seed; and Poisson arrival times at `rate` per second."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(n):
+        specs.append(dict(
+            nside=int(rng.choice([128, 256, 512, 1024])), ndet=int(rng.integers(2, 33)),
+            nsamp=int(2 ** rng.uniform(18, 24)), fknee=float(rng.uniform(0.02, 0.2)),
+            base_first=float(rng.choice([0.25, 0.5, 1.0, 2.0])), f32=bool(rng.random() < 0.5),
+            seed=7000 + i))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+    return specs, arrivals
+
+
 def run_serve(args, world, rank, local):
     """Serving stream with the request mix of the serving workload: requests
     draw nside in {128, 256, 512, 1024}, 2-32 detectors, log-uniform 2^18-2^24
@@ -421,15 +438,7 @@ def run_serve(args, world, rank, local):
     import torch
     from libmadam_b200 import synthetic as syn
     from libmadam_b200.serve import Server
-    rng = np.random.default_rng(5005 + rank)
-    specs = []
-    for i in range(args.requests):
-        specs.append(dict(
-            nside=int(rng.choice([128, 256, 512, 1024])), ndet=int(rng.integers(2, 33)),
-            nsamp=int(2 ** rng.uniform(18, 24)), fknee=float(rng.uniform(0.02, 0.2)),
-            base_first=float(rng.choice([0.25, 0.5, 1.0, 2.0])), f32=bool(rng.random() < 0.5),
-            seed=7000 + i))
-    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, args.requests))
+    specs, arrivals = serve_requests(args.requests, args.rate, 5005 + rank)
     free, _ = torch.cuda.mem_get_info()
     gen_cap = 0.45 * free
     cond = threading.Condition()

@@ -71,3 +71,31 @@ def test_bench_measures_these_workloads():
     assert bench.config_for("2")[0] == syn.config2()
     assert bench.config_for("1")[0] == syn.config1()
     assert bench.config_for("3")[0] == syn.config3()
+
+
+def test_serving_request_mix():
+    """The serving stream: 2000 requests, Poisson arrivals at 20 per second,
+    nside 128-1024, 2-32 detectors, 2^18-2^24 samples per detector,
+    base_first 0.25-2 s, half of them float32 TOD."""
+    import importlib.util
+    import os
+
+    import numpy as np
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    spec = importlib.util.spec_from_file_location("bench_module", os.path.join(root, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    specs, arrivals = bench.serve_requests(2000, 20.0, 5005)
+    assert len(specs) == 2000 and len(arrivals) == 2000
+    assert {s["nside"] for s in specs} == {128, 256, 512, 1024}
+    nd = np.array([s["ndet"] for s in specs])
+    assert nd.min() == 2 and nd.max() == 32
+    ns = np.log2([s["nsamp"] for s in specs])
+    assert ns.min() >= 18 and ns.max() < 24 and abs(ns.mean() - 21) < 0.2
+    assert {s["base_first"] for s in specs} == {0.25, 0.5, 1.0, 2.0}
+    assert abs(np.mean([s["f32"] for s in specs]) - 0.5) < 0.05
+    gaps = np.diff(np.concatenate([[0.0], arrivals]))
+    assert (gaps > 0).all() and abs(gaps.mean() - 0.05) < 0.005
+    assert len({s["seed"] for s in specs}) == 2000
+    again, _ = bench.serve_requests(2000, 20.0, 5005)
+    assert again == specs
