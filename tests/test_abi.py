@@ -199,3 +199,18 @@ def test_spectrum_file_with_repeat_counts_is_read():
                        np.zeros(4), np.zeros(4, np.int32), np.ones(4, np.float32), np.zeros(4),
                        np.array([0]), np.ones(1, np.int64), np.zeros(1), np.array([1.0, 2.0]),
                        np.ones(2))
+
+
+def test_server_arguments_and_no_cpu_fallback():
+    """The job server checks its arguments, and without a GPU it refuses to
+    open rather than serving on the CPU."""
+    from libmadam_b200.serve import Server
+    with pytest.raises(RuntimeError, match="nworkers must be in 1..64"):
+        Server(workers=0)
+    with pytest.raises(RuntimeError, match=r"mem_fraction must be in \(0, 1\]"):
+        Server(workers=2, mem_fraction=0.0)
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        return
+    with pytest.raises(RuntimeError, match="CUDA"):
+        Server(workers=2)
