@@ -81,6 +81,14 @@ def test_destripe_with_cache_without_cache_fails():
     with pytest.raises(RuntimeError, match="empty caches"):
         W.destripe_with_cache(None, np.zeros(4), np.zeros(4, np.int32), np.ones(4, np.float32),
                               np.zeros(4), b"")
+    # the batched Monte Carlo calls read the same caches
+    for fn in (W.destripe_with_cache_batch, W.destripe_with_cache_batch_fp32):
+        with pytest.raises(RuntimeError, match="empty caches"):
+            fn(None, np.zeros(4), np.zeros(4, np.int32), np.ones(4, np.float32),
+               np.zeros((2, 4)))
+    # no run, no results
+    with pytest.raises(KeyError):
+        W.get_result("map")
 
 
 def test_void_entry_points_do_not_abort():
